@@ -1,0 +1,369 @@
+"""GB MD throughput on one large system, B200.
+
+Workload (the reference's single-large-system configuration): 16 seeded
+80-residue peptides on a 4x4 grid 25 A apart, 20,566 atoms, built by the
+reference's own builder and pre-minimised (tests/golden/c2_16x80_s2.npz),
+AMBER99 + Still GB (FastMode) + bonded terms, Rc 16 A (inner 13 A),
+neighbour list rebuilt every 10 steps, Langevin dynamics at 1 fs, 300 K,
+friction 1/ps.  A "step" is one MD step: list refresh (every 10th), bonded +
+Born radii + fused GB/LJ/Coulomb + chain-rule forces, integrator.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: independent replicas, one per rank (the path does not shard one
+system); value = simulated ns of all ranks / the slowest rank's time.
+"""
+import argparse
+import ctypes
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+FIXTURE = os.path.join(ROOT, "tests", "golden", "c2_16x80_s2.npz")
+REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver_timing")
+REF_PARAM = os.path.join(ROOT, "oracle", "_ref", "param")
+DT_FS = 1.0
+BLOCK = 10  # list period = one timed iteration (L2 flushed between them)
+METRIC = "GB MD ns/day"
+
+
+def rank_info():
+    r = int(os.environ.get("RANK", "0"))
+    w = int(os.environ.get("WORLD_SIZE", "1"))
+    lr = int(os.environ.get("LOCAL_RANK", str(r)))
+    return r, w, lr
+
+
+def load_fixture():
+    z = np.load(FIXTURE)
+    arrays = {k: z[k] for k in z.files}
+    meta = json.loads(bytes(arrays.pop("meta_json")).decode())
+    return arrays, meta
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args, n_gpus):
+    """The reference's own CPU MD (compiled from its sources with its own
+    flags, oracle/_ref/ref_driver_timing), single-threaded as the reference
+    is, on a bounded sample of the same workload; else the oracle port."""
+    arrays, meta = load_fixture()
+    n = arrays["charge"].shape[0]
+    steps = max(1, min(args.steps, args.ref_steps))
+    warm = max(1, min(args.warmup, 2))
+    if os.path.exists(REF_DRIVER):
+        tmp = tempfile.mkdtemp(prefix="pdref_")
+        try:
+            np.save(os.path.join(tmp, "pos.npy"), arrays["pos"])
+            with open(os.path.join(tmp, "meta.txt"), "w") as fh:
+                for c in meta["chains"]:
+                    fh.write("chain %s\n" % c)
+            env = dict(os.environ, PD_PARAM_PATH=REF_PARAM)
+            out = subprocess.check_output(
+                [REF_DRIVER, "time", "--in", tmp, "--cutoff", meta["cutoff"], "--inner", meta["inner"],
+                 "--steps", str(steps), "--warmup", str(warm), "--nlist-every", "10"],
+                env=env, stderr=subprocess.DEVNULL, text=True)
+            res = json.loads(out.strip().splitlines()[-1])
+            secs = res["seconds"]
+            kind = "reference"
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+    else:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        S = O.System(arrays, cutoff=float(meta["cutoff"]), inner=float(meta["inner"]))
+        x = arrays["pos"].reshape(-1).copy()
+        v = np.zeros_like(x)
+        rng = np.random.default_rng(0)
+        t0 = None
+        ptr = data = None
+        for s in range(warm + steps):
+            if s == warm:
+                t0 = time.perf_counter()
+            if s % 10 == 0:
+                ptr, data = S.nlist(x)
+            f, e, _ = S.calc_forces(x, ptr, data)
+            x, v, _ = O.langevin_step(x, v, f.reshape(-1), S.mass, rng.standard_normal(6 * n), 1e-15, 1e12,
+                                      300.0, s, warm + steps + 1)
+        secs = time.perf_counter() - t0
+        kind = "port"
+    ns_day = steps * DT_FS * 1e-6 / secs * 86400.0
+    sample = "%d MD steps (1 list rebuild per 10) of the %d-atom workload after %d warm-up" % (steps, n, warm)
+    return {"value": ns_day, "kind": kind, "cores": 1, "sample": sample, "seconds": secs, "steps": steps}
+
+
+# ---------------------------------------------------------------- ours
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=100)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-steps", type=int, default=60, help="bounded CPU sample (steps)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = rank_info()
+    n_gpus = max(args.gpus, world)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        r = run_reference(args, n_gpus)
+        line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": "ns/day",
+                "n_gpus": n_gpus, "steps": r["steps"], "warmup": min(args.warmup, 2),
+                "ms_per_step": 1e3 * r["seconds"] / r["steps"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "16x80-residue GB MD, 20566 atoms, Rc 16 A, Langevin 1 fs",
+                           "threads": 1},
+                "cpu_baseline": {"value": r["value"], "unit": "ns/day", "cores": 1, "kind": r["kind"],
+                                 "sample": r["sample"]},
+                "e2e": {"value": r["value"], "unit": "ns/day", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    device = torch.cuda.current_device()
+
+    sys.path.insert(0, os.path.join(ROOT, "pd.arcus_b200"))
+    import pdgpu
+    from pdgpu import _abi as A
+
+    arrays, meta = load_fixture()
+    ctx = pdgpu.Context(device)
+    ws = pdgpu.WorkSpace(pdgpu.SystemSpec(arrays, meta), ctx)
+    ff = pdgpu.Forcefield(ws)
+    ff.add(pdgpu.FF_Bonded(ws))
+    gb = pdgpu.FF_GeneralizedBorn_Still(ws)
+    gb.Cutoff, gb.InnerCutoff = float(meta["cutoff"]), float(meta["inner"])
+    gb.VdwCutoff, gb.VdwInnerCutoff = float(meta["vdwcut"]), float(meta["vdwinner"])
+    ff.add(gb)
+    n = ws.nAtoms()
+
+    # parity at the start coordinates (against the reference's FP64 forces)
+    ws.nlist().calcNewList()
+    ff.calcForces()
+    f_ref = arrays["f_total"]
+    force_rms = float(np.sqrt(np.sum((ws.cur.f - f_ref) ** 2) / np.sum(f_ref ** 2)))
+    de_kcal = float(abs(ws.ene.epot - arrays["ene_total"][0]) * pdgpu.J2KCAL_NA)
+
+    # roofline inputs: pair counts and per-kernel device times (CUDA events)
+    counts = np.zeros(3, dtype=np.int64)
+    A.check(A.lib().pdgpu_pair_counts(ctx.ptr, ws._sys, counts.ctypes.data_as(A._I64)))
+    kms = np.zeros(3)
+    A.check(A.lib().pdgpu_profile_pair_kernels(ctx.ptr, ws._sys, 20, A.dptr(kms)))
+
+    p = A.md_params_default()
+    p.Integrator, p.UpdateNList, p.UseGraph = A.INTEGRATOR_LANGEVIN, BLOCK, 1
+    p.Timestep, p.FricCoeff, p.TargetTemp, p.Seed = 1e-15, 1e12, 300.0, 1000 + rank
+    A.check(A.lib().pdgpu_md_init_velocities(ctx.ptr, ws._sys, 300.0, 1000 + rank))
+    L = A.lib()
+    total = args.warmup + args.steps + BLOCK
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def run_block(step0, k):
+        st = L.pdgpu_md_run(ctx.ptr, ws._sys, ctypes.byref(p), step0, k, total, None)
+        A.check(st)
+        return ctx.last_run_ms()
+
+    warm = max(3, args.warmup)
+    s = 0
+    while s < warm:
+        k = min(BLOCK, warm - s)
+        run_block(s, k)
+        s += k
+    # timed: K steps in list-period blocks, L2 flushed before each block
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    lc0 = ctypes.c_int64(0)
+    L.pdgpu_launch_count(ctx.ptr, ctypes.byref(lc0))
+    clocks = ClockSampler(device)
+    clocks.start()
+    dev_ms = 0.0
+    done = 0
+    while done < args.steps:
+        k = min(BLOCK, args.steps - done)
+        flush.zero_()
+        torch.cuda.synchronize()
+        dev_ms += run_block(s, k)
+        s += k
+        done += k
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    lc1 = ctypes.c_int64(0)
+    L.pdgpu_launch_count(ctx.ptr, ctypes.byref(lc1))
+    if dist:
+        dist.barrier()
+    t_local = dev_ms / 1e3
+    if dist:
+        t = torch.tensor([t_local], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    else:
+        t_max = t_local
+    ns_total = n_gpus * args.steps * DT_FS * 1e-6
+    value = ns_total / t_max * 86400.0
+
+    # end to end through the public API: per list period, host -> device
+    # state (pinned), 10 steps, device -> host state + energies
+    e2e = None
+    if not args.no_e2e:
+        x_h = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+        v_h = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+        e_h = torch.empty(A.ENE_COUNT, dtype=torch.float64).pin_memory()
+        xp = ctypes.cast(x_h.data_ptr(), A._D)
+        vp = ctypes.cast(v_h.data_ptr(), A._D)
+        ep = ctypes.cast(e_h.data_ptr(), A._D)
+        A.check(L.pdgpu_get_positions(ctx.ptr, ws._sys, xp))
+        A.check(L.pdgpu_get_velocities(ctx.ptr, ws._sys, vp))
+        e2e_steps = min(args.steps, 1000)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        done = 0
+        s2 = 0
+        while done < e2e_steps:
+            k = min(BLOCK, e2e_steps - done)
+            A.check(L.pdgpu_set_positions(ctx.ptr, ws._sys, xp))
+            A.check(L.pdgpu_set_velocities(ctx.ptr, ws._sys, vp))
+            A.check(L.pdgpu_md_run(ctx.ptr, ws._sys, ctypes.byref(p), s2, k, e2e_steps + BLOCK, None))
+            A.check(L.pdgpu_get_positions(ctx.ptr, ws._sys, xp))
+            A.check(L.pdgpu_get_velocities(ctx.ptr, ws._sys, vp))
+            A.check(L.pdgpu_get_energies(ctx.ptr, ws._sys, ep, A.ENE_COUNT))
+            s2 += k
+            done += k
+        torch.cuda.synchronize()
+        te = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([te], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        e2e = {"value": n_gpus * e2e_steps * DT_FS * 1e-6 / te * 86400.0, "unit": "ns/day",
+               "h2d_bytes_per_step": int(2 * n * 24 / BLOCK),
+               "d2h_bytes_per_step": int((2 * n * 24 + A.ENE_COUNT * 8) / BLOCK),
+               "steps": e2e_steps, "api": "pdgpu_set_positions/velocities + pdgpu_md_run(10) + get_*"}
+
+    # roofline of the pair kernels (FP32/SFU; nominal peaks at the max SM clock)
+    P_B, P_H, entries = (int(c) for c in counts)
+    f_max = (clk.get("sm_max_mhz") or 1965.0) * 1e6
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    F32 = sms * 256 * f_max
+    SFU = sms * 16 * f_max
+    t2, t3, t4 = (float(x) / 1e3 for x in kms)
+    k3_flop, k3_sfu = 90.0 * P_H, 5.0 * P_H
+    k3_frac_fp32 = (k3_flop / t3) / F32
+    k3_frac_sfu = (k3_sfu / t3) / SFU
+    all_flop, all_sfu = 57.0 * P_B + 90.0 * P_H, 7.0 * P_B + 5.0 * P_H
+    t_pair = t2 + t3 + t4
+    t_roof = max(all_flop / F32, all_sfu / SFU)
+    bound = "fp32" if k3_frac_fp32 >= k3_frac_sfu else "sfu"
+    roof = {"kernel": "k_gb_pair (fused GB + LJ + Coulomb, K3)", "bound": bound,
+            "achieved": (k3_flop / t3 / 1e12) if bound == "fp32" else (k3_sfu / t3 / 1e12),
+            "peak": (F32 if bound == "fp32" else SFU) / 1e12,
+            "unit": "TFLOP/s" if bound == "fp32" else "Top/s (MUFU)",
+            "frac": max(k3_frac_fp32, k3_frac_sfu), "traffic": None,
+            "peak_source": "nominal %d SMs x %s/clk at sm_max_mhz %.0f (no measured FP32/SFU peak)" % (
+                sms, "256 flop" if bound == "fp32" else "16 MUFU", f_max / 1e6),
+            "pairs": {"P_B": P_B, "P_H": P_H, "list_entries": entries},
+            "kernel_ms": {"born_K2": t2 * 1e3, "pair_K3": t3 * 1e3, "chain_K4": t4 * 1e3},
+            "pair_kernels_frac_of_roof": t_roof / t_pair}
+
+    line = {"metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": n_gpus, "steps": args.steps,
+            "warmup": warm, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair / f64 state",
+            "data": "synthetic (seeded peptides built by the reference's NewProtein)",
+            "config": {"workload": "16x80-residue chains, 20566 atoms, AMBER99 + Still GB + bonded, Rc 16 A, "
+                                   "Langevin 1 fs 300 K gamma 1/ps, list every 10 steps",
+                       "atoms": n, "parallelism": "replicas" if n_gpus > 1 else "single",
+                       "l2": "flushed (256 MiB write) before every 10-step timed block"},
+            "parity": {"force_rel_rms_vs_fp64": force_rms, "epot_abs_err_kcal": de_kcal},
+            "gpu_launches": int(lc1.value - lc0.value),
+            "clocks": clk, "roofline": roof, "e2e": e2e}
+    if rank == 0 and n_gpus == 1 and not args.no_cpu_baseline:
+        try:
+            cb = run_reference(args, 1)
+            line["cpu_baseline"] = {"value": cb["value"], "unit": "ns/day", "cores": cb["cores"],
+                                    "kind": cb["kind"], "sample": cb["sample"]}
+        except Exception as exc:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
+    if rank == 0:
+        print(json.dumps(line))
+    ws.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

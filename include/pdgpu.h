@@ -1,0 +1,256 @@
+/* pdgpu: B200 (sm_100a) GB/SA energy-force hot path of PD (JonnyWideFoot/pd.arcus).
+ *
+ * C ABI of libpdgpu.so.  Plain pointers and sizes only.  Every entry point
+ * returns PDGPU_OK (0) or a negative status; pdgpu_last_error() gives the
+ * message of the last failure on the calling thread.  Inputs and outputs
+ * use the reference's own units: positions in Angstrom, energies in
+ * J/molecule, forces in N, masses in kg, LJ epsilon in sqrt(J), LJ radius
+ * (half Rmin) and GB radius in Angstrom, charges in e.
+ *
+ * Each entry point names the reference interface it replaces
+ * (paths relative to the reference's src/mmlib).
+ *
+ * Threading: a context is used by one host thread at a time; calls on one
+ * context are serialised on its CUDA stream.  Separate contexts may be
+ * driven from separate threads.
+ */
+#ifndef PDGPU_H
+#define PDGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define PDGPU_OK 0
+#define PDGPU_ERR_ARG -1        /* bad argument (ArgumentException)           */
+#define PDGPU_ERR_CUDA -2       /* CUDA runtime failure                        */
+#define PDGPU_ERR_NOMEM -3      /* device allocation failed (OutOfMemory)      */
+#define PDGPU_ERR_UNSTABLE -4   /* NaN energy (ProcedureException "unstable") */
+#define PDGPU_ERR_STATE -5      /* call out of order (e.g. no neighbour list)  */
+#define PDGPU_ERR_BUDGET -6     /* admission refused: HBM budget exhausted     */
+#define PDGPU_ERR_NODEVICE -7   /* no CUDA device / extension not usable       */
+
+typedef struct pdgpu_ctx pdgpu_ctx;
+
+/* ------------------------------------------------------------------ settings
+ * Public members of FF_NonBonded (forcefields/nonbonded.h:55-126) and
+ * FF_GeneralizedBorn_Still (forcefields/gbff.h:127-133), same names and
+ * meaning.  pdgpu_ff_params_default() fills the values a freshly constructed
+ * FF_GeneralizedBorn_Still carries (gbff.cpp:17-38, nonbonded.cpp:968-1004). */
+typedef struct {
+  double Cutoff, InnerCutoff, VdwCutoff, VdwInnerCutoff;
+  double Vdw14Scaling, Elec14Scaling;
+  double Dielectric;           /* FF_NonBonded::Dielectric (stand-alone LJ/Coulomb) */
+  double DielectricSolute, DielectricSolvent;
+  double GbsaStillCutoff, ExpApproxThreshold, DielectricOffset, BornRadiusOffset;
+  double P1, P2, P3, P4, P5;   /* Still parameters (SOLVATION_GENERALISED_BORN)     */
+  double DDDielectricAlpha;
+  double VdwCorDensity, VdwCorEpsilon, VdwCorRadius, VdwCorCutoff;
+  double Padding;              /* NeighbourListBase::Padding (neighbourlist.cpp:18) */
+  int32_t FastMode, EnergySwitch, ForceSwitch, DDDielectric, DoVdw, DoElec, VdwCor;
+  int32_t _reserved;
+} pdgpu_ff_params;
+
+void pdgpu_ff_params_default(pdgpu_ff_params *p);
+
+/* ------------------------------------------------------------------ context */
+/* Replaces: nothing in the reference (it is host-only); owns the device,
+ * one CUDA stream and the resident systems. */
+int pdgpu_ctx_create(int device, pdgpu_ctx **out);
+int pdgpu_ctx_destroy(pdgpu_ctx *ctx);
+const char *pdgpu_last_error(void);
+/* Device bytes currently held by the context's systems. */
+int pdgpu_ctx_mem_used(pdgpu_ctx *ctx, int64_t *bytes);
+
+/* ------------------------------------------------------------------ systems
+ * A system is one WorkSpace: its atoms, topology, parameters and state.
+ * Replaces the per-atom data FF_NonBonded::setup / FF_GeneralizedBorn_Still::
+ * setup copy out of WorkSpace (nonbonded.cpp:1008-1036, gbff.cpp:40-87) and
+ * BondOrder::reinit (workspace/bondorder.cpp:170-195).
+ *   residue       Particle::ir (residue index), used for the bond-order band
+ *   cov12/13/14   Particle::cov12atom/cov13atom/cov14atom as CSR (ptr[n+1],
+ *                 idx), with the equilibrium distances of 1-2 and 1-3
+ *                 partners (CovalentAtom::d, set by FF_Bonded::setup)
+ *   gb_radius     GBtype[FFType].radius of each atom
+ * The Still fixed terms (calcFixedBornRadiiTerms, gbff.cpp:307-381) and the
+ * bond-order band are computed here.  *sys_id receives the handle. */
+int pdgpu_system_create(pdgpu_ctx *ctx, int32_t natoms, const double *charge,
+                        const double *radius, const double *epsilon,
+                        const double *mass, const double *gb_radius,
+                        const int32_t *residue, const int32_t *cov12_ptr,
+                        const int32_t *cov12_idx, const double *cov12_d,
+                        const int32_t *cov13_ptr, const int32_t *cov13_idx,
+                        const double *cov13_d, const int32_t *cov14_ptr,
+                        const int32_t *cov14_idx, const pdgpu_ff_params *params,
+                        int32_t *sys_id);
+int pdgpu_system_destroy(pdgpu_ctx *ctx, int32_t sys);
+/* Change the forcefield settings (FF_NonBonded::calcCheckSum re-setup path,
+ * nonbonded.cpp:1061-1067). */
+int pdgpu_system_set_params(pdgpu_ctx *ctx, int32_t sys, const pdgpu_ff_params *params);
+
+/* Bonded terms as FF_Bonded::setup assembles them (ffbonded.cpp:13-470):
+ * bonds (i,j | l,k), angles (i,a,j | k,theta0), torsions and impropers
+ * (i,a,b,j | terms | Vn[4],n[4],gamma[4]).  Energies in J, angles in rad. */
+int pdgpu_system_set_bonded(pdgpu_ctx *ctx, int32_t sys, int32_t nbond,
+                            const int32_t *bond_ij, const double *bond_lk,
+                            int32_t nangle, const int32_t *angle_iaj,
+                            const double *angle_kt, int32_t ntors,
+                            const int32_t *tors_idx, const int32_t *tors_terms,
+                            const double *tors_par, int32_t nimpr,
+                            const int32_t *impr_idx, const int32_t *impr_terms,
+                            const double *impr_par);
+
+/* Particle::isHydrogen() per atom (fundamentals.h:74), used by the
+ * LangevinOnHydrogens=false integrator (md.cpp:1048-1218).  Default: none. */
+int pdgpu_system_set_hydrogens(pdgpu_ctx *ctx, int32_t sys, const int8_t *is_h);
+
+/* State transfer (WorkSpace::cur.atom[i].p / .v / .f, snapshot.h:16-22). */
+int pdgpu_set_positions(pdgpu_ctx *ctx, int32_t sys, const double *xyz);
+int pdgpu_get_positions(pdgpu_ctx *ctx, int32_t sys, double *xyz);
+int pdgpu_set_velocities(pdgpu_ctx *ctx, int32_t sys, const double *v);
+int pdgpu_get_velocities(pdgpu_ctx *ctx, int32_t sys, double *v);
+/* Forces accumulated since the last pdgpu_zero_forces, in N. */
+int pdgpu_get_forces(pdgpu_ctx *ctx, int32_t sys, double *f);
+/* Born radii of the last evaluation (GB_atom_param[i].bornradius). */
+int pdgpu_get_born_radii(pdgpu_ctx *ctx, int32_t sys, double *born);
+/* Per-atom potential energy (Particle::epot), J. */
+int pdgpu_get_atom_epot(pdgpu_ctx *ctx, int32_t sys, double *epot);
+
+/* Energy record (Hamiltonian, workspace/hamiltonian.h:23-49), J.  Index
+ * order of the PDGPU_ENE_* slots below; n >= PDGPU_ENE_COUNT. */
+#define PDGPU_ENE_EPOT 0
+#define PDGPU_ENE_VDW 1
+#define PDGPU_ENE_ELEC 2
+#define PDGPU_ENE_POL 3
+#define PDGPU_ENE_POL_CROSS 4
+#define PDGPU_ENE_POL_SELF 5
+#define PDGPU_ENE_BOND 6
+#define PDGPU_ENE_ANGLE 7
+#define PDGPU_ENE_TORSION 8
+#define PDGPU_ENE_VIRIAL 9
+#define PDGPU_ENE_EKIN 10
+#define PDGPU_ENE_ETOT 11
+#define PDGPU_ENE_GB_COMPONENT 12 /* FF_GeneralizedBorn::epot_pol of the energy path */
+#define PDGPU_ENE_COUNT 16
+int pdgpu_get_energies(pdgpu_ctx *ctx, int32_t sys, double *ene, int32_t n);
+
+/* WorkSpace::zeroForces (workspace.cpp:283-292): forces, per-atom and
+ * system energies to zero. */
+int pdgpu_zero_forces(pdgpu_ctx *ctx, int32_t sys);
+
+/* ------------------------------------------------------------------ kernels */
+/* NeighbourList::calcNewList (neighbourlist.cpp:205-316): cell binning with
+ * integer keys and a radix sort, exact FP64 distance test against
+ * (max(Cutoff,VdwCutoff)+Padding)^2, bond-order encoding incl. off-diagonal
+ * corrections.  Always the full ("shadow") list. */
+int pdgpu_nlist_build(pdgpu_ctx *ctx, int32_t sys);
+/* NeighbourListBase::getData (neighbourlist.h:47): the list in the
+ * reference's packed encoding (j | bondorder<<24, j ascending per atom).
+ * ptr[natoms+1]; data has room for cap entries; *count receives the total.
+ * shadow=0 returns the half list (j < i) the reference builds without
+ * CalcShadow. */
+int pdgpu_nlist_export(pdgpu_ctx *ctx, int32_t sys, int32_t shadow, int32_t *ptr,
+                       int32_t *data, int64_t cap, int64_t *count);
+
+/* FF_GeneralizedBorn_Still::calcForces (gbff.cpp:168-180) in FastMode:
+ * Born radii (:415-466), then the fused GB + LJ + Coulomb pass (:1529-1736)
+ * and the Born-radius chain-rule pass (:1751-1818).  Adds forces; sets the
+ * vdw/elec/pol energy slots and adds to EPOT.  FastMode=0 runs
+ * FF_NonBonded::calcForces + the same GB terms as calcBornForces. */
+int pdgpu_gb_forces(pdgpu_ctx *ctx, int32_t sys);
+/* FF_GeneralizedBorn_Still::calcEnergies (gbff.cpp:161-166): radii, the
+ * stand-alone LJ/Coulomb pass at the solute dielectric (which, as in the
+ * reference, also adds its forces), then calcBornEnergy (:520-579). */
+int pdgpu_gb_energies(pdgpu_ctx *ctx, int32_t sys);
+/* FF_NonBonded::calcForces (nonbonded.cpp:1205-1229, fast2 kernel :548-893):
+ * VdW energy switch, electrostatics Normal / EnergySwitch / ForceSwitch /
+ * distance-dependent dielectric, 1-4 scaling by bond order, virial, VdW
+ * long-range correction. */
+int pdgpu_nonbonded_forces(pdgpu_ctx *ctx, int32_t sys);
+/* FF_Bonded::calcForces (ffbonded.cpp:809-823). */
+int pdgpu_bonded_forces(pdgpu_ctx *ctx, int32_t sys);
+/* Forcefield::calcForces (forcefield.cpp:220-247) for {FF_Bonded,
+ * FF_GeneralizedBorn_Still}: zero, bonded, GB.  Reads nothing back. */
+int pdgpu_calc_forces(pdgpu_ctx *ctx, int32_t sys);
+
+/* ------------------------------------------------------------------ protocols */
+#define PDGPU_INTEGRATOR_VERLET 0
+#define PDGPU_INTEGRATOR_VELOCITY_VERLET 1
+#define PDGPU_INTEGRATOR_BEEMAN 2
+#define PDGPU_INTEGRATOR_LANGEVIN 3
+
+/* MolecularDynamics public members (protocols/md.h:84-128). */
+typedef struct {
+  int32_t Integrator;          /* PDGPU_INTEGRATOR_*                          */
+  int32_t UpdateNList;         /* rebuild the list every n steps (md.cpp:64) */
+  int32_t LangevinOnHydrogens; /* md.cpp:59                                   */
+  int32_t UseGraph;            /* capture UpdateNList-step blocks in a graph */
+  double Timestep;             /* s                                           */
+  double FricCoeff;            /* 1/s                                         */
+  double TargetTemp;           /* K                                           */
+  uint64_t Seed;               /* counter-based RNG key (Philox4x32-10)       */
+} pdgpu_md_params;
+void pdgpu_md_params_default(pdgpu_md_params *p);
+
+/* MolecularDynamics::run_core (md.cpp:202-267): steps of {list refresh every
+ * UpdateNList, Forcefield::calcForces, NaN check, integrator}.  first_step is
+ * the protocol's Step of the first call; total_steps its Steps (the
+ * integrators branch on Step>0 and Step<Steps-1).  Per-step epot, ekin and
+ * etot (J) are written to history[3*steps] when history is not NULL.
+ * Returns PDGPU_ERR_UNSTABLE on a NaN energy (assertStability,
+ * protocolbase.cpp:104-110). */
+int pdgpu_md_run(pdgpu_ctx *ctx, int32_t sys, const pdgpu_md_params *p,
+                 int32_t first_step, int32_t steps, int32_t total_steps,
+                 double *history);
+/* One integrator step with externally supplied normals (normals[6*natoms],
+ * per atom in the order the reference's three nrand() pairs draw them:
+ * n1x n2y n2x n1z n1y n2z), on the forces already accumulated.  For exact
+ * single-step parity tests. */
+int pdgpu_md_step_with_normals(pdgpu_ctx *ctx, int32_t sys, const pdgpu_md_params *p,
+                               int32_t step, int32_t total_steps, const double *normals);
+/* MolecularDynamics::setInitialSpeeds (md.cpp:342-363): Boltzmann draw then
+ * rescale to 3/2 N kB T. */
+int pdgpu_md_init_velocities(pdgpu_ctx *ctx, int32_t sys, double temperature,
+                             uint64_t seed);
+
+#define PDGPU_MIN_STEEPEST_DESCENT 0
+#define PDGPU_MIN_CONJUGATE_GRADIENTS 1
+/* Minimisation public members (protocols/minimise.h, minimise.cpp:34-41). */
+typedef struct {
+  int32_t Algorithm;
+  int32_t UpdateNList;
+  double StepSize;
+  double SlopeCutoff;
+  double Strictness;
+} pdgpu_min_params;
+void pdgpu_min_params_default(pdgpu_min_params *p);
+/* Minimisation::runcore (minimise.cpp:99-179) with the accept / restore
+ * control flow on the device; *steps_taken receives the steps done. */
+int pdgpu_minimise_run(pdgpu_ctx *ctx, int32_t sys, const pdgpu_min_params *p,
+                       int32_t steps, int32_t *steps_taken);
+
+/* ------------------------------------------------------------------ timing */
+/* Device time (ms) of the last pdgpu_md_run / pdgpu_minimise_run call,
+ * measured with CUDA events on the context stream. */
+int pdgpu_last_run_ms(pdgpu_ctx *ctx, double *ms);
+
+/* Instrumentation (no reference counterpart).  Pair counts of the current
+ * list and positions: counts[0] = P_B, directed pairs with r <= GbsaStillCutoff
+ * and bond order >= 3 (Born sum / chain rule); counts[1] = P_H, unordered
+ * pairs with r <= Cutoff (fused GB + LJ + Coulomb); counts[2] = list entries. */
+int pdgpu_pair_counts(pdgpu_ctx *ctx, int32_t sys, int64_t *counts);
+/* Average device time (ms) of the Born-radius, fused pair and chain-rule
+ * kernels over `reps` evaluations, each bracketed by CUDA events on the
+ * context stream: ms[0..2]. */
+int pdgpu_profile_pair_kernels(pdgpu_ctx *ctx, int32_t sys, int32_t reps, double *ms);
+/* Kernels this context has launched (graph replays count their kernel
+ * nodes). */
+int pdgpu_launch_count(pdgpu_ctx *ctx, int64_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

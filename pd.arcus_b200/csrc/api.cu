@@ -1,0 +1,1180 @@
+// C ABI of libpdgpu (declared in include/pdgpu.h) and the protocol runners.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+
+#include "internal.cuh"
+
+namespace pdgpu {
+const char *last_error_cstr();
+void launch_bonded_terms(const PackView &v, cudaStream_t st, double *scratch, const int *off);
+void launch_md_step_impl(const PackView &v, cudaStream_t st, const MDCoef &c, const double *normals,
+                         const int *step_dev, const unsigned char *is_h, const unsigned long long *seeds);
+void launch_step_inc(const PackView &v, int *step_dev, cudaStream_t st);
+void launch_record(const PackView &v, cudaStream_t st, double *hist, const int *step_dev);
+void launch_pair_counts(const PackView &v, cudaStream_t st, unsigned long long *out);
+void launch_ke_from_velocities(const PackView &v, cudaStream_t st);
+void launch_vel_init_impl(const PackView &v, cudaStream_t st, double temp, const unsigned long long *seeds);
+void launch_min_step(const PackView &v, cudaStream_t st, void *ms, int algorithm, double slope_kcal,
+                     double strict_kcal, double step_size, int nsteps);
+void launch_min_finish(const PackView &v, cudaStream_t st);
+size_t min_state_size();
+void min_state_init(void *host_buf, int n);
+void min_state_read(const void *host_buf, int s, int *taken, int *nan, double *mult);
+}  // namespace pdgpu
+
+using namespace pdgpu;
+
+// Device-side extras a system needs beyond the Pack core.
+struct SysEntry {
+  SystemHost host;
+  std::unique_ptr<Pack> pack;
+  // bonded scratch + per-system term ranges
+  double *bonded_scratch = nullptr;
+  int *bonded_off = nullptr;
+  unsigned char *is_h = nullptr;
+  unsigned long long *seeds = nullptr;
+  int *step_dev = nullptr;
+  double *hist = nullptr;
+  int hist_cap = 0;
+  void *min_state = nullptr;
+  std::vector<void *> extra;
+  // cached MD block graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  std::string gkey;
+  long long gnodes = 0;
+  void drop_graph() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    gexec = nullptr;
+    graph = nullptr;
+    gkey.clear();
+  }
+  ~SysEntry() {
+    drop_graph();
+    for (void *p : extra) cudaFree(p);
+  }
+};
+
+struct pdgpu_ctx {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  std::map<int, std::unique_ptr<SysEntry>> sys;
+  int next_id = 1;
+  double last_ms = 0.0;
+};
+
+#define CHECK_CTX(c)                        \
+  do {                                      \
+    if (!(c)) {                             \
+      set_error("null context");            \
+      return PDGPU_ERR_ARG;                 \
+    }                                       \
+    cudaSetDevice((c)->device);             \
+  } while (0)
+
+static SysEntry *find_sys(pdgpu_ctx *c, int id) {
+  auto it = c->sys.find(id);
+  if (it == c->sys.end()) {
+    set_error("unknown system id " + std::to_string(id));
+    return nullptr;
+  }
+  return it->second.get();
+}
+#define GET_SYS(e, c, id)            \
+  SysEntry *e = find_sys((c), (id)); \
+  if (!e) return PDGPU_ERR_ARG
+
+template <typename T>
+static cudaError_t xalloc(SysEntry *e, T **p, size_t n) {
+  cudaError_t r = cudaMalloc((void **)p, sizeof(T) * (n ? n : 1));
+  if (r == cudaSuccess) {
+    e->extra.push_back(*p);
+    cudaMemset(*p, 0, sizeof(T) * (n ? n : 1));
+  }
+  return r;
+}
+
+static int sync_check(pdgpu_ctx *c, const char *what) {
+  cudaError_t e = cudaStreamSynchronize(c->st);
+  if (e != cudaSuccess) return cuda_fail(e, what);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, what);
+  return PDGPU_OK;
+}
+
+extern "C" {
+
+const char *pdgpu_last_error(void) { return last_error_cstr(); }
+
+void pdgpu_ff_params_default(pdgpu_ff_params *p) {
+  memset(p, 0, sizeof *p);
+  // FF_NonBonded::settodefault (nonbonded.cpp:968-1004), then the
+  // FF_GeneralizedBorn_Still constructor overrides (gbff.cpp:17-38)
+  p->Cutoff = 15;
+  p->InnerCutoff = 12;
+  p->VdwCutoff = 15;
+  p->VdwInnerCutoff = 12;
+  p->Vdw14Scaling = 1.0;
+  p->Elec14Scaling = 1.0;
+  p->Dielectric = 1.0;
+  p->DDDielectricAlpha = 1.0;
+  p->DielectricSolute = 1.0;
+  p->DielectricSolvent = 80.0;
+  p->GbsaStillCutoff = 10;
+  p->ExpApproxThreshold = -4.0;
+  p->DielectricOffset = -0.090;
+  p->BornRadiusOffset = 0.0;
+  p->P1 = 0.073;
+  p->P2 = 0.921;
+  p->P3 = 6.211;
+  p->P4 = 15.236;
+  p->P5 = 1.254;
+  p->Padding = 0.5;
+  p->FastMode = 1;
+  p->EnergySwitch = 1;
+  p->ForceSwitch = 0;
+  p->DDDielectric = 0;
+  p->DoVdw = 1;
+  p->DoElec = 1;
+  p->VdwCor = 0;
+}
+
+void pdgpu_md_params_default(pdgpu_md_params *p) {
+  memset(p, 0, sizeof *p);
+  // MolecularDynamics::settodefault (md.cpp:39-70)
+  p->Integrator = PDGPU_INTEGRATOR_BEEMAN;
+  p->UpdateNList = 10;
+  p->LangevinOnHydrogens = 1;
+  p->UseGraph = 1;
+  p->Timestep = 1e-15;
+  p->FricCoeff = 10e12;
+  p->TargetTemp = 300;
+  p->Seed = 0;
+}
+
+void pdgpu_min_params_default(pdgpu_min_params *p) {
+  // Minimisation::settodefault (minimise.cpp:34-41); UpdateNList from
+  // ProtocolBase (protocolbase.cpp:20)
+  p->Algorithm = PDGPU_MIN_CONJUGATE_GRADIENTS;
+  p->UpdateNList = 1;
+  p->StepSize = 2e5;
+  p->SlopeCutoff = -1.0;
+  p->Strictness = 0.0;
+}
+
+int pdgpu_ctx_create(int device, pdgpu_ctx **out) {
+  if (!out) {
+    set_error("out is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    set_error(std::string("no CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "count 0"));
+    return PDGPU_ERR_NODEVICE;
+  }
+  if (device < 0 || device >= n) {
+    set_error("device index out of range");
+    return PDGPU_ERR_ARG;
+  }
+  PDGPU_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  PDGPU_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10) {
+    set_error("libpdgpu is built for sm_100a (B200); device is sm_" + std::to_string(prop.major) +
+              std::to_string(prop.minor));
+    return PDGPU_ERR_NODEVICE;
+  }
+  pdgpu_ctx *c = new pdgpu_ctx();
+  c->device = device;
+  e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return cuda_fail(e, "cudaStreamCreate");
+  }
+  *out = c;
+  return PDGPU_OK;
+}
+
+int pdgpu_ctx_destroy(pdgpu_ctx *c) {
+  if (!c) return PDGPU_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->st);
+  c->sys.clear();
+  cudaStreamDestroy(c->st);
+  delete c;
+  return PDGPU_OK;
+}
+
+int pdgpu_ctx_mem_used(pdgpu_ctx *c, int64_t *bytes) {
+  CHECK_CTX(c);
+  int64_t b = 0;
+  for (auto &kv : c->sys)
+    if (kv.second->pack) b += kv.second->pack->bytes;
+  *bytes = b;
+  return PDGPU_OK;
+}
+
+// ------------------------------------------------------------ systems
+static int validate_params(const pdgpu_ff_params *p) {
+  if (!p) return PDGPU_OK;
+  if (!(p->Cutoff > 0) || !(p->InnerCutoff >= 0) || !(p->InnerCutoff < p->Cutoff) ||
+      !(p->VdwCutoff > 0) || !(p->VdwInnerCutoff < p->VdwCutoff) || !(p->Padding >= 0) ||
+      !(p->GbsaStillCutoff > 0) || !(p->DielectricSolute > 0) || !(p->DielectricSolvent > 0) ||
+      !(p->Dielectric > 0) || !(p->P5 > 0)) {
+    set_error("invalid forcefield settings (cutoffs must satisfy 0 <= Inner < Cutoff, dielectrics > 0)");
+    return PDGPU_ERR_ARG;
+  }
+  return PDGPU_OK;
+}
+
+int pdgpu_system_create(pdgpu_ctx *c, int32_t natoms, const double *charge, const double *radius,
+                        const double *epsilon, const double *mass, const double *gb_radius,
+                        const int32_t *residue, const int32_t *c12p, const int32_t *c12i,
+                        const double *c12d, const int32_t *c13p, const int32_t *c13i,
+                        const double *c13d, const int32_t *c14p, const int32_t *c14i,
+                        const pdgpu_ff_params *params, int32_t *sys_id) {
+  CHECK_CTX(c);
+  if (natoms <= 0 || natoms >= (1 << 24) || !charge || !radius || !epsilon || !mass || !gb_radius ||
+      !residue || !c12p || !c13p || !c14p || !sys_id) {
+    set_error("pdgpu_system_create: bad arguments (natoms must be in [1, 2^24), arrays non-NULL)");
+    return PDGPU_ERR_ARG;
+  }
+  int r = validate_params(params);
+  if (r) return r;
+  auto e = std::make_unique<SysEntry>();
+  SystemHost &h = e->host;
+  h.natoms = natoms;
+  if (params)
+    h.params = *params;
+  else
+    pdgpu_ff_params_default(&h.params);
+  h.charge.assign(charge, charge + natoms);
+  h.radius.assign(radius, radius + natoms);
+  h.epsilon.assign(epsilon, epsilon + natoms);
+  h.mass.assign(mass, mass + natoms);
+  h.gbR.assign(gb_radius, gb_radius + natoms);
+  h.residue.assign(residue, residue + natoms);
+  for (int i = 0; i < natoms; i++)
+    if (!(mass[i] > 0)) {
+      set_error("pdgpu_system_create: masses must be positive");
+      return PDGPU_ERR_ARG;
+    }
+  auto csr = [&](const int32_t *p, const int32_t *idx, std::vector<int> &P, std::vector<int> &I) -> bool {
+    P.assign(p, p + natoms + 1);
+    if (P[0] != 0) return false;
+    for (int i = 0; i < natoms; i++)
+      if (P[i + 1] < P[i]) return false;
+    if (P[natoms] > 0 && !idx) return false;
+    I.assign(idx, idx + P[natoms]);
+    return true;
+  };
+  if (!csr(c12p, c12i, h.c12p, h.c12i) || !csr(c13p, c13i, h.c13p, h.c13i) ||
+      !csr(c14p, c14i, h.c14p, h.c14i)) {
+    set_error("pdgpu_system_create: malformed covalent CSR lists");
+    return PDGPU_ERR_ARG;
+  }
+  if ((h.c12p[natoms] && !c12d) || (h.c13p[natoms] && !c13d)) {
+    set_error("pdgpu_system_create: 1-2 and 1-3 equilibrium distances required");
+    return PDGPU_ERR_ARG;
+  }
+  if (h.c12p[natoms]) h.c12d.assign(c12d, c12d + h.c12p[natoms]);
+  if (h.c13p[natoms]) h.c13d.assign(c13d, c13d + h.c13p[natoms]);
+  std::string err;
+  r = host_bondorder(h, &err);
+  if (r) {
+    set_error(err);
+    return r;
+  }
+  host_gb_fixed_terms(h);
+  std::vector<const SystemHost *> one(1, &h);
+  Pack *p = pack_create(c->device, c->st, one, &err);
+  if (!p) {
+    set_error(err);
+    return PDGPU_ERR_NOMEM;
+  }
+  e->pack.reset(p);
+  if (xalloc(e.get(), &e->is_h, natoms) != cudaSuccess || xalloc(e.get(), &e->seeds, 1) != cudaSuccess ||
+      xalloc(e.get(), &e->step_dev, 2) != cudaSuccess ||
+      xalloc(e.get(), &e->bonded_off, 4 * 2) != cudaSuccess) {
+    set_error("device allocation failed");
+    return PDGPU_ERR_NOMEM;
+  }
+  int id = c->next_id++;
+  c->sys[id] = std::move(e);
+  *sys_id = id;
+  return PDGPU_OK;
+}
+
+int pdgpu_system_destroy(pdgpu_ctx *c, int32_t sys) {
+  CHECK_CTX(c);
+  cudaStreamSynchronize(c->st);
+  if (!c->sys.erase(sys)) {
+    set_error("unknown system id");
+    return PDGPU_ERR_ARG;
+  }
+  return PDGPU_OK;
+}
+
+int pdgpu_system_set_params(pdgpu_ctx *c, int32_t sys, const pdgpu_ff_params *params) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  int r = validate_params(params);
+  if (r) return r;
+  if (!params) {
+    set_error("params is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  bool fixed_changed = params->P1 != e->host.params.P1 || params->P2 != e->host.params.P2 ||
+                       params->P3 != e->host.params.P3 || params->P4 != e->host.params.P4 ||
+                       params->DielectricOffset != e->host.params.DielectricOffset;
+  e->host.params = *params;
+  if (fixed_changed) {
+    // the Still fixed terms depend on P1-P4: rebuild the pack (re-setup)
+    host_gb_fixed_terms(e->host);
+    std::string err;
+    std::vector<const SystemHost *> one(1, &e->host);
+    std::vector<double> x(3 * e->host.natoms);
+    pdgpu_get_positions(c, sys, x.data());
+    Pack *p = pack_create(c->device, c->st, one, &err);
+    if (!p) {
+      set_error(err);
+      return PDGPU_ERR_NOMEM;
+    }
+    e->drop_graph();
+    e->pack.reset(p);
+    return pdgpu_set_positions(c, sys, x.data());
+  }
+  e->drop_graph();
+  Pack &P = *e->pack;
+  pack_set_params(&P, 0, *params);
+  PDGPU_CUDA(cudaMemcpyAsync((void *)P.v.sp, P.sp.data(), sizeof(SysParams), cudaMemcpyHostToDevice, c->st));
+  P.have_list = false;  // the list radius may have changed
+  return sync_check(c, "set_params");
+}
+
+int pdgpu_system_set_bonded(pdgpu_ctx *c, int32_t sys, int32_t nb, const int32_t *bij, const double *blk,
+                            int32_t na, const int32_t *aiaj, const double *akt, int32_t nt,
+                            const int32_t *tidx, const int32_t *tterms, const double *tpar, int32_t ni,
+                            const int32_t *iidx, const int32_t *iterms, const double *ipar) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (nb < 0 || na < 0 || nt < 0 || ni < 0 || (nb && (!bij || !blk)) || (na && (!aiaj || !akt)) ||
+      (nt && (!tidx || !tterms || !tpar)) || (ni && (!iidx || !iterms || !ipar))) {
+    set_error("pdgpu_system_set_bonded: bad arguments");
+    return PDGPU_ERR_ARG;
+  }
+  SystemHost &h = e->host;
+  int n = h.natoms;
+  auto inrange = [&](const int32_t *a, long cnt) {
+    for (long k = 0; k < cnt; k++)
+      if (a[k] < 0 || a[k] >= n) return false;
+    return true;
+  };
+  if (!inrange(bij, 2L * nb) || !inrange(aiaj, 3L * na) || !inrange(tidx, 4L * nt) || !inrange(iidx, 4L * ni)) {
+    set_error("pdgpu_system_set_bonded: atom index out of range");
+    return PDGPU_ERR_ARG;
+  }
+  for (int k = 0; k < nt; k++)
+    if (tterms[k] < 0 || tterms[k] > 4) {
+      set_error("pdgpu_system_set_bonded: torsion term count must be 0..4");
+      return PDGPU_ERR_ARG;
+    }
+  for (int k = 0; k < ni; k++)
+    if (iterms[k] < 0 || iterms[k] > 4) {
+      set_error("pdgpu_system_set_bonded: improper term count must be 0..4");
+      return PDGPU_ERR_ARG;
+    }
+  h.nb = nb;
+  h.na = na;
+  h.nt = nt;
+  h.ni = ni;
+  h.bij.assign(bij, bij + 2 * nb);
+  h.blk.assign(blk, blk + 2 * nb);
+  h.aiaj.assign(aiaj, aiaj + 3 * na);
+  h.akt.assign(akt, akt + 2 * na);
+  h.tidx.assign(tidx, tidx + 4 * nt);
+  h.tidx.insert(h.tidx.end(), iidx, iidx + 4 * ni);
+  h.tterms.assign(tterms, tterms + nt);
+  h.tterms.insert(h.tterms.end(), iterms, iterms + ni);
+  h.tpar.assign(tpar, tpar + 12 * nt);
+  h.tpar.insert(h.tpar.end(), ipar, ipar + 12 * ni);
+  // rebuild the pack with the bonded terms, keeping the state
+  std::vector<double> x(3 * n), vv(3 * n);
+  int r = pdgpu_get_positions(c, sys, x.data());
+  if (r) return r;
+  r = pdgpu_get_velocities(c, sys, vv.data());
+  if (r) return r;
+  std::string err;
+  std::vector<const SystemHost *> one(1, &h);
+  Pack *p = pack_create(c->device, c->st, one, &err);
+  if (!p) {
+    set_error(err);
+    return PDGPU_ERR_NOMEM;
+  }
+  e->drop_graph();
+  e->pack.reset(p);
+  int off[8] = {0, nb, 0, na, 0, nt, nt, nt + ni};
+  PDGPU_CUDA(cudaMemcpyAsync(e->bonded_off, off, sizeof off, cudaMemcpyHostToDevice, c->st));
+  if (e->bonded_scratch) {
+    cudaFree(e->bonded_scratch);
+    e->extra.erase(std::find(e->extra.begin(), e->extra.end(), (void *)e->bonded_scratch));
+    e->bonded_scratch = nullptr;
+  }
+  if (xalloc(e, &e->bonded_scratch, (size_t)2 * nb + na + nt + ni + 1) != cudaSuccess) {
+    set_error("device allocation failed");
+    return PDGPU_ERR_NOMEM;
+  }
+  r = pdgpu_set_positions(c, sys, x.data());
+  if (r) return r;
+  return pdgpu_set_velocities(c, sys, vv.data());
+}
+
+int pdgpu_system_set_hydrogens(pdgpu_ctx *c, int32_t sys, const int8_t *is_h) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (!is_h) {
+    set_error("is_h is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  PDGPU_CUDA(cudaMemcpyAsync(e->is_h, is_h, e->host.natoms, cudaMemcpyHostToDevice, c->st));
+  return sync_check(c, "set_hydrogens");
+}
+
+// ------------------------------------------------------------ state
+static int copy_soa_in(pdgpu_ctx *c, Pack &P, const double *xyz, double *X, double *Y, double *Z) {
+  int n = P.v.n_atoms;
+  std::vector<double> a(n), b(n), d(n);
+  for (int i = 0; i < n; i++) {
+    a[i] = xyz[3 * i];
+    b[i] = xyz[3 * i + 1];
+    d[i] = xyz[3 * i + 2];
+  }
+  PDGPU_CUDA(cudaMemcpyAsync(X, a.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(Y, b.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(Z, d.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+  return sync_check(c, "copy in");
+}
+static int copy_soa_out(pdgpu_ctx *c, Pack &P, double *xyz, const double *X, const double *Y,
+                        const double *Z) {
+  int n = P.v.n_atoms;
+  std::vector<double> a(n), b(n), d(n);
+  PDGPU_CUDA(cudaMemcpyAsync(a.data(), X, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(b.data(), Y, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(d.data(), Z, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+  int r = sync_check(c, "copy out");
+  if (r) return r;
+  for (int i = 0; i < n; i++) {
+    xyz[3 * i] = a[i];
+    xyz[3 * i + 1] = b[i];
+    xyz[3 * i + 2] = d[i];
+  }
+  return PDGPU_OK;
+}
+
+int pdgpu_set_positions(pdgpu_ctx *c, int32_t sys, const double *xyz) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (!xyz) {
+    set_error("xyz is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  Pack &P = *e->pack;
+  int r = copy_soa_in(c, P, xyz, P.v.x, P.v.y, P.v.z);
+  if (r) return r;
+  launch_pack_positions(P.v, c->st);
+  return sync_check(c, "set_positions");
+}
+int pdgpu_get_positions(pdgpu_ctx *c, int32_t sys, double *xyz) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (!xyz) {
+    set_error("xyz is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  Pack &P = *e->pack;
+  return copy_soa_out(c, P, xyz, P.v.x, P.v.y, P.v.z);
+}
+int pdgpu_set_velocities(pdgpu_ctx *c, int32_t sys, const double *v) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (!v) {
+    set_error("v is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  Pack &P = *e->pack;
+  return copy_soa_in(c, P, v, P.v.vx, P.v.vy, P.v.vz);
+}
+int pdgpu_get_velocities(pdgpu_ctx *c, int32_t sys, double *v) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (!v) {
+    set_error("v is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  Pack &P = *e->pack;
+  return copy_soa_out(c, P, v, P.v.vx, P.v.vy, P.v.vz);
+}
+
+int pdgpu_get_forces(pdgpu_ctx *c, int32_t sys, double *f) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (!f) {
+    set_error("f is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  Pack &P = *e->pack;
+  int n = P.v.n_atoms;
+  std::vector<long long> a(n), b(n), d(n);
+  PDGPU_CUDA(cudaMemcpyAsync(a.data(), P.v.fx, sizeof(long long) * n, cudaMemcpyDeviceToHost, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(b.data(), P.v.fy, sizeof(long long) * n, cudaMemcpyDeviceToHost, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(d.data(), P.v.fz, sizeof(long long) * n, cudaMemcpyDeviceToHost, c->st));
+  int r = sync_check(c, "get_forces");
+  if (r) return r;
+  double s = kInvForceScale * consts().N_per_kcalmolA;
+  for (int i = 0; i < n; i++) {
+    f[3 * i] = (double)a[i] * s;
+    f[3 * i + 1] = (double)b[i] * s;
+    f[3 * i + 2] = (double)d[i] * s;
+  }
+  return PDGPU_OK;
+}
+
+int pdgpu_get_born_radii(pdgpu_ctx *c, int32_t sys, double *born) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (!born) {
+    set_error("born is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  Pack &P = *e->pack;
+  PDGPU_CUDA(cudaMemcpyAsync(born, P.v.born_d, sizeof(double) * P.v.n_atoms, cudaMemcpyDeviceToHost, c->st));
+  return sync_check(c, "get_born_radii");
+}
+
+int pdgpu_get_atom_epot(pdgpu_ctx *c, int32_t sys, double *epot) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (!epot) {
+    set_error("epot is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  Pack &P = *e->pack;
+  int n = P.v.n_atoms;
+  std::vector<double> ea((size_t)AE_COUNT * n);
+  PDGPU_CUDA(cudaMemcpyAsync(ea.data(), P.v.e_atom, sizeof(double) * ea.size(), cudaMemcpyDeviceToHost, c->st));
+  int r = sync_check(c, "get_atom_epot");
+  if (r) return r;
+  double J = consts().J_per_kcalmol;
+  for (int i = 0; i < n; i++)
+    epot[i] = (ea[(size_t)AE_VDW * n + i] + ea[(size_t)AE_ELEC * n + i] + ea[(size_t)AE_POL * n + i] +
+               ea[(size_t)AE_POL_SELF * n + i]) *
+              J;
+  return PDGPU_OK;
+}
+
+int pdgpu_get_energies(pdgpu_ctx *c, int32_t sys, double *ene, int32_t n) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (!ene || n < PDGPU_ENE_COUNT) {
+    set_error("ene must hold PDGPU_ENE_COUNT values");
+    return PDGPU_ERR_ARG;
+  }
+  Pack &P = *e->pack;
+  double tmp[E_COUNT];
+  PDGPU_CUDA(cudaMemcpyAsync(tmp, P.v.ene, sizeof tmp, cudaMemcpyDeviceToHost, c->st));
+  int r = sync_check(c, "get_energies");
+  if (r) return r;
+  double J = consts().J_per_kcalmol;
+  for (int k = 0; k < E_COUNT; k++) ene[k] = tmp[k] * J;
+  return PDGPU_OK;
+}
+
+int pdgpu_zero_forces(pdgpu_ctx *c, int32_t sys) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  launch_zero(e->pack->v, c->st);
+  return sync_check(c, "zero_forces");
+}
+
+// ------------------------------------------------------------ kernels
+// enqueue a full list rebuild; when `size_check` the host reads the count
+// and grows the list buffer first (one synchronisation)
+static int nlist_enqueue(pdgpu_ctx *c, SysEntry *e, bool size_check) {
+  Pack &P = *e->pack;
+  PackView &v = P.v;
+  launch_nlist_count(P, c->st);
+  if (size_check) {
+    long long total = 0;
+    PDGPU_CUDA(cudaMemcpyAsync(&total, v.row_start + v.n_atoms, sizeof total, cudaMemcpyDeviceToHost, c->st));
+    int r = sync_check(c, "nlist count");
+    if (r) return r;
+    if (total > v.nl_cap) {
+      long long cap = total + total / 3 + 4096;
+      unsigned *nl = nullptr;
+      cudaError_t ce = cudaMalloc(&nl, sizeof(unsigned) * cap);
+      if (ce != cudaSuccess) return cuda_fail(ce, "grow neighbour list");
+      auto it = std::find(P.allocs.begin(), P.allocs.end(), (void *)v.nl);
+      if (it != P.allocs.end()) {
+        cudaFree(*it);
+        *it = nl;
+      }
+      P.bytes += (int64_t)(cap - v.nl_cap) * 4;
+      v.nl = nl;
+      v.nl_cap = cap;
+    }
+    P.nl_total = total;
+    PDGPU_CUDA(cudaMemsetAsync(v.flags + F_NL_OVERFLOW, 0, sizeof(int), c->st));
+  }
+  launch_nlist_fill(P, c->st);
+  P.have_list = true;
+  return PDGPU_OK;
+}
+
+int pdgpu_nlist_build(pdgpu_ctx *c, int32_t sys) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  int r = nlist_enqueue(c, e, true);
+  if (r) return r;
+  return sync_check(c, "nlist_build");
+}
+
+int pdgpu_nlist_export(pdgpu_ctx *c, int32_t sys, int32_t shadow, int32_t *ptr, int32_t *data, int64_t cap,
+                       int64_t *count) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  if (!P.have_list) {
+    set_error("no neighbour list: call pdgpu_nlist_build first");
+    return PDGPU_ERR_STATE;
+  }
+  if (!ptr || !count) {
+    set_error("ptr/count is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  int n = P.v.n_atoms;
+  std::vector<long long> rs(n + 1);
+  PDGPU_CUDA(cudaMemcpyAsync(rs.data(), P.v.row_start, sizeof(long long) * (n + 1), cudaMemcpyDeviceToHost, c->st));
+  int r = sync_check(c, "export");
+  if (r) return r;
+  std::vector<unsigned> raw(rs[n]);
+  if (rs[n])
+    PDGPU_CUDA(cudaMemcpyAsync(raw.data(), P.v.nl, sizeof(unsigned) * rs[n], cudaMemcpyDeviceToHost, c->st));
+  r = sync_check(c, "export");
+  if (r) return r;
+  int64_t k = 0;
+  std::vector<int> row;
+  for (int i = 0; i < n; i++) {
+    ptr[i] = (int32_t)k;
+    row.clear();
+    for (long long q = rs[i]; q < rs[i + 1]; q++) {
+      int j = (int)(raw[q] >> 3);
+      int bo = (int)(raw[q] & 7u);
+      if (!shadow && j >= i) continue;
+      row.push_back((j & 0x00FFFFFF) | (bo << 24));
+    }
+    std::sort(row.begin(), row.end(), [](int a, int b) { return (a & 0x00FFFFFF) < (b & 0x00FFFFFF); });
+    for (int x : row) {
+      if (data && k < cap) data[k] = x;
+      k++;
+    }
+  }
+  ptr[n] = (int32_t)k;
+  *count = k;
+  if (data && k > cap) {
+    set_error("export buffer too small");
+    return PDGPU_ERR_ARG;
+  }
+  return PDGPU_OK;
+}
+
+static int need_list(Pack &P) {
+  if (!P.have_list) {
+    set_error("no neighbour list: call pdgpu_nlist_build first (NeighbourList::calcNewList)");
+    return PDGPU_ERR_STATE;
+  }
+  return PDGPU_OK;
+}
+
+// GB calcForces enqueue (no sync)
+static void gb_forces_enqueue(pdgpu_ctx *c, Pack &P) {
+  launch_born_radii(P.v, c->st);
+  launch_gb_pair(P.v, c->st);
+  launch_gb_chain(P.v, c->st);
+  launch_reduce_gb_energies(P.v, c->st, 0);
+}
+
+static void bonded_enqueue(pdgpu_ctx *c, SysEntry *e) {
+  if (e->bonded_scratch) launch_bonded_terms(e->pack->v, c->st, e->bonded_scratch, e->bonded_off);
+}
+
+int pdgpu_gb_forces(pdgpu_ctx *c, int32_t sys) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  int r = need_list(P);
+  if (r) return r;
+  if (!e->host.params.FastMode) {
+    set_error("FastMode=false (separate FF_NonBonded + calcBornForces) is not built; use FastMode");
+    return PDGPU_ERR_ARG;
+  }
+  gb_forces_enqueue(c, P);
+  return sync_check(c, "gb_forces");
+}
+
+int pdgpu_gb_energies(pdgpu_ctx *c, int32_t sys) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  int r = need_list(P);
+  if (r) return r;
+  // calcEnergies: radii, FF_NonBonded::calcEnergies at Dielectric =
+  // DielectricSolute (gbff.cpp:44), then calcBornEnergy
+  pdgpu_ff_params q = e->host.params;
+  q.Dielectric = q.DielectricSolute;
+  SysParams saved = P.sp[0];
+  pack_set_params(&P, 0, q);
+  PDGPU_CUDA(cudaMemcpyAsync((void *)P.v.sp, P.sp.data(), sizeof(SysParams), cudaMemcpyHostToDevice, c->st));
+  launch_born_radii(P.v, c->st);
+  launch_nonbonded(P.v, c->st, P.sp[0].elec_mode);
+  launch_reduce_gb_energies(P.v, c->st, 1);
+  launch_born_energy(P.v, c->st);
+  launch_reduce_gb_energies(P.v, c->st, 2);
+  P.sp[0] = saved;
+  PDGPU_CUDA(cudaMemcpyAsync((void *)P.v.sp, P.sp.data(), sizeof(SysParams), cudaMemcpyHostToDevice, c->st));
+  return sync_check(c, "gb_energies");
+}
+
+int pdgpu_nonbonded_forces(pdgpu_ctx *c, int32_t sys) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  int r = need_list(P);
+  if (r) return r;
+  launch_nonbonded(P.v, c->st, P.sp[0].elec_mode);
+  launch_reduce_gb_energies(P.v, c->st, 1);
+  return sync_check(c, "nonbonded_forces");
+}
+
+int pdgpu_bonded_forces(pdgpu_ctx *c, int32_t sys) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  bonded_enqueue(c, e);
+  return sync_check(c, "bonded_forces");
+}
+
+static void calc_forces_enqueue(pdgpu_ctx *c, SysEntry *e) {
+  Pack &P = *e->pack;
+  launch_zero(P.v, c->st);
+  bonded_enqueue(c, e);
+  gb_forces_enqueue(c, P);
+}
+
+int pdgpu_calc_forces(pdgpu_ctx *c, int32_t sys) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  int r = need_list(P);
+  if (r) return r;
+  calc_forces_enqueue(c, e);
+  return sync_check(c, "calc_forces");
+}
+
+// ------------------------------------------------------------ MD
+static MDCoef md_coef(const pdgpu_md_params *p, int step, int steps) {
+  // the coefficient branches of md.cpp:961-1000
+  MDCoef c;
+  memset(&c, 0, sizeof c);
+  c.dt = p->Timestep;
+  c.gamma = p->FricCoeff;
+  c.temp = p->TargetTemp;
+  c.integrator = p->Integrator;
+  c.step = step;
+  c.steps = steps;
+  c.stochastic_h = p->LangevinOnHydrogens;
+  c.seed = p->Seed;
+  double gt = c.gamma * c.dt;
+  double gt2 = gt * gt, gt3 = gt * gt2, gt4 = gt2 * gt2, gt5 = gt2 * gt3, gt6 = gt3 * gt3, gt7 = gt3 * gt4,
+         gt8 = gt4 * gt4, gt9 = gt4 * gt5;
+  if (gt > 0.05) {
+    c.c0 = exp(-gt);
+    c.c1 = (1 - c.c0) / gt;
+    c.c2 = (1 - c.c1) / gt;
+    double eg = exp(-gt);
+    c.varv = (1.0 - eg * eg);
+    c.varr = (2.0 * gt - 3.0 + (4.0 - eg) * eg);
+    c.crv = (1.0 - eg) * (1.0 - eg) / (sqrt(c.varv * c.varr));
+  } else {
+    c.c0 = 1 - gt + 0.5 * gt2 - gt3 / 6.0 + gt4 / 24.0 - gt5 / 120.0 + gt6 / 720.0 - gt7 / 5040.0 +
+           gt8 / 40320.0 - gt9 / 362880.0;
+    c.c1 = 1 - (0.5 * gt - gt2 / 6.0 + gt3 / 24.0 - gt4 / 120.0 + gt5 / 720.0 - gt6 / 5040.0 + gt7 / 40320.0 -
+                gt8 / 362880.0);
+    c.c2 = 0.5 - gt / 6.0 + gt2 / 24.0 - gt3 / 120.0 + gt4 / 720.0 - gt5 / 5040.0 + gt6 / 40320.0 -
+           gt7 / 362880.0;
+    c.varr = 2.0 * gt3 / 3.0 - gt4 / 2.0 + 7.0 * gt5 / 30.0 - gt6 / 12.0 + 31.0 * gt7 / 1260.0 - gt8 / 160.0 +
+             127.0 * gt9 / 90720.0;
+    c.varv = 2.0 * gt - 2.0 * gt2 + 4.0 * gt3 / 3.0 - 2.0 * gt4 / 3.0 + 4.0 * gt5 / 15.0 - 4.0 * gt6 / 45.0 +
+             8.0 * gt7 / 315.0 - 2.0 * gt8 / 315.0 + 4.0 * gt9 / 2835.0;
+    c.crv = sqrt(3.0) * (0.5 - 3.0 * gt / 16.0 - 17.0 * gt2 / 1280.0 + 17.0 * gt3 / 6144.0 +
+                         40967.0 * gt4 / 34406400.0 - 57203.0 * gt5 / 275251200.0 -
+                         1429487.0 * gt6 / 13212057600.0);
+  }
+  return c;
+}
+
+static int validate_md(const pdgpu_md_params *p) {
+  if (!p || !(p->Timestep > 0) || p->Integrator < 0 || p->Integrator > 3 || !(p->TargetTemp >= 0) ||
+      (p->Integrator == PDGPU_INTEGRATOR_LANGEVIN && !(p->FricCoeff > 0))) {
+    set_error("invalid MD parameters");
+    return PDGPU_ERR_ARG;
+  }
+  return PDGPU_OK;
+}
+
+int pdgpu_md_step_with_normals(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t step,
+                               int32_t total_steps, const double *normals) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  int r = validate_md(p);
+  if (r) return r;
+  Pack &P = *e->pack;
+  double *nd = nullptr;
+  if (normals) {
+    PDGPU_CUDA(cudaMalloc(&nd, sizeof(double) * 6 * P.v.n_atoms));
+    PDGPU_CUDA(cudaMemcpyAsync(nd, normals, sizeof(double) * 6 * P.v.n_atoms, cudaMemcpyHostToDevice, c->st));
+  }
+  unsigned long long seed = p->Seed;
+  PDGPU_CUDA(cudaMemcpyAsync(e->seeds, &seed, sizeof seed, cudaMemcpyHostToDevice, c->st));
+  MDCoef k = md_coef(p, step, total_steps);
+  launch_md_step_impl(P.v, c->st, k, nd, nullptr, e->is_h, e->seeds);
+  r = sync_check(c, "md_step");
+  if (nd) cudaFree(nd);
+  return r;
+}
+
+int pdgpu_md_init_velocities(pdgpu_ctx *c, int32_t sys, double temperature, uint64_t seed) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  unsigned long long s = seed;
+  PDGPU_CUDA(cudaMemcpyAsync(e->seeds, &s, sizeof s, cudaMemcpyHostToDevice, c->st));
+  launch_vel_init_impl(e->pack->v, c->st, temperature, e->seeds);
+  return sync_check(c, "init_velocities");
+}
+
+// one MD step enqueue: forces, integrate, record, advance the step counter
+static void md_step_enqueue(pdgpu_ctx *c, SysEntry *e, const MDCoef &k) {
+  Pack &P = *e->pack;
+  calc_forces_enqueue(c, e);
+  launch_md_step_impl(P.v, c->st, k, nullptr, e->step_dev, e->is_h, e->seeds);
+  launch_record(P.v, c->st, e->hist, e->step_dev);
+  launch_step_inc(P.v, e->step_dev, c->st);
+}
+
+int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t first_step, int32_t steps,
+                 int32_t total_steps, double *history) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  int r = validate_md(p);
+  if (r) return r;
+  if (steps < 0 || first_step < 0 || total_steps < first_step + steps) {
+    set_error("md_run: need 0 <= first_step and first_step + steps <= total_steps");
+    return PDGPU_ERR_ARG;
+  }
+  Pack &P = *e->pack;
+  PackView &v = P.v;
+  if (steps == 0) return PDGPU_OK;
+  if (e->hist_cap < steps) {
+    if (e->hist) {
+      cudaFree(e->hist);
+      e->extra.erase(std::find(e->extra.begin(), e->extra.end(), (void *)e->hist));
+      e->hist = nullptr;
+    }
+    if (xalloc(e, &e->hist, (size_t)3 * steps) != cudaSuccess) {
+      set_error("device allocation failed (history)");
+      return PDGPU_ERR_NOMEM;
+    }
+    e->hist_cap = steps;
+  }
+  unsigned long long seed = p->Seed;
+  PDGPU_CUDA(cudaMemcpyAsync(e->seeds, &seed, sizeof seed, cudaMemcpyHostToDevice, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(e->step_dev, &first_step, sizeof(int), cudaMemcpyHostToDevice, c->st));
+  PDGPU_CUDA(cudaMemsetAsync(v.flags, 0, sizeof(int) * F_COUNT, c->st));
+  MDCoef k = md_coef(p, first_step, total_steps);
+  int every = p->UpdateNList;
+  // size the list once up front (one synchronisation); later rebuilds run
+  // inside the step blocks and report overflow through a device flag
+  if (!P.have_list || P.nl_total < 0) {
+    r = nlist_enqueue(c, e, true);
+    if (r) return r;
+  }
+  // A block is one list period: [rebuild] + UpdateNList steps.  If the
+  // in-block rebuild overflows the list buffer, every kernel after it skips
+  // (device flag), the state stays at the block start, and the host grows
+  // the buffer and runs the block again.
+  int steps0[2] = {first_step, first_step};
+  PDGPU_CUDA(cudaMemcpyAsync(e->step_dev, steps0, sizeof steps0, cudaMemcpyHostToDevice, c->st));
+  cudaEventRecord(P.ev0, c->st);
+  int s = 0;
+  while (s < steps) {
+    int step = first_step + s;
+    bool rebuild = every > 0 && (P.nlist_counter % every) == 0;
+    int block = 1;
+    if (rebuild && every > 1) block = std::min(every, steps - s);
+    bool use_graph = p->UseGraph && rebuild && block == every && every > 1;
+    int counter0 = P.nlist_counter;
+    for (int attempt = 0;; attempt++) {
+      if (attempt == 4) {
+        set_error("neighbour list kept overflowing after regrowth");
+        return PDGPU_ERR_STATE;
+      }
+      PDGPU_CUDA(cudaMemsetAsync(v.flags + F_NL_OVERFLOW, 0, sizeof(int), c->st));
+      PDGPU_CUDA(cudaMemcpyAsync(e->step_dev, &step, sizeof(int), cudaMemcpyHostToDevice, c->st));
+      if (use_graph) {
+        // graphs are cached per system; the key holds every value baked in
+        char key[256];
+        snprintf(key, sizeof key, "%d|%p|%lld|%p|%d|%d|%.17g|%.17g|%.17g|%d|%d|%d", block, (void *)v.nl,
+                 v.nl_cap, (void *)e->hist, k.integrator, k.steps, k.dt, k.gamma, k.temp, k.stochastic_h,
+                 P.radix_passes, (int)e->host.params.FastMode);
+        if (!e->gexec || e->gkey != key) {
+          e->drop_graph();
+          long long before = launch_counter();
+          PDGPU_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+          launch_nlist_count(P, c->st);
+          launch_nlist_fill(P, c->st);
+          for (int q = 0; q < block; q++) md_step_enqueue(c, e, k);
+          PDGPU_CUDA(cudaStreamEndCapture(c->st, &e->graph));
+          PDGPU_CUDA(cudaGraphInstantiate(&e->gexec, e->graph, 0));
+          e->gnodes = launch_counter() - before;
+          launch_counter() = before;  // capture ran nothing
+          e->gkey = key;
+        }
+        PDGPU_CUDA(cudaGraphLaunch(e->gexec, c->st));
+        launch_counter() += e->gnodes;
+      } else {
+        if (rebuild) {
+          launch_nlist_count(P, c->st);
+          launch_nlist_fill(P, c->st);
+        }
+        for (int q = 0; q < block; q++) md_step_enqueue(c, e, k);
+      }
+      int flags[F_COUNT];
+      PDGPU_CUDA(cudaMemcpyAsync(flags, v.flags, sizeof flags, cudaMemcpyDeviceToHost, c->st));
+      r = sync_check(c, "md block");
+      if (r) return r;
+      if (flags[F_NL_OVERFLOW]) {
+        // state untouched since the block start: grow the list and re-run
+        r = nlist_enqueue(c, e, true);
+        if (r) return r;
+        e->drop_graph();
+        continue;
+      }
+      if (flags[F_NAN]) {
+        if (history) {
+          std::vector<double> h((size_t)3 * (s + block));
+          cudaMemcpy(h.data(), e->hist, sizeof(double) * h.size(), cudaMemcpyDeviceToHost);
+          for (size_t q = 0; q < h.size(); q++) history[q] = h[q] * consts().J_per_kcalmol;
+        }
+        set_error("Simulation unstable or division by zero (NaN energy)");
+        return PDGPU_ERR_UNSTABLE;
+      }
+      break;
+    }
+    P.nlist_counter = counter0 + block;
+    s += block;
+  }
+  cudaEventRecord(P.ev1, c->st);
+  r = sync_check(c, "md_run");
+  if (r) return r;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, P.ev0, P.ev1);
+  P.last_run_ms = ms;
+  c->last_ms = ms;
+  if (history) {
+    std::vector<double> h((size_t)3 * steps);
+    PDGPU_CUDA(cudaMemcpy(h.data(), e->hist, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
+    double J = consts().J_per_kcalmol;
+    for (size_t q = 0; q < h.size(); q++) history[q] = h[q] * J;
+  }
+  return PDGPU_OK;
+}
+
+// ------------------------------------------------------------ minimiser
+int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int32_t steps,
+                       int32_t *steps_taken) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (!p || steps < 0 || (p->Algorithm != 0 && p->Algorithm != 1)) {
+    set_error("invalid minimiser parameters");
+    return PDGPU_ERR_ARG;
+  }
+  Pack &P = *e->pack;
+  PackView &v = P.v;
+  const Consts &k = consts();
+  if (!e->min_state) {
+    void *m = nullptr;
+    PDGPU_CUDA(cudaMalloc(&m, min_state_size()));
+    e->extra.push_back(m);
+    e->min_state = m;
+  }
+  std::vector<unsigned char> hs(min_state_size());
+  min_state_init(hs.data(), 1);
+  PDGPU_CUDA(cudaMemcpyAsync(e->min_state, hs.data(), hs.size(), cudaMemcpyHostToDevice, c->st));
+  PDGPU_CUDA(cudaMemsetAsync(v.flags, 0, sizeof(int) * F_COUNT, c->st));
+  // WorkSpace::old = cur (minimise.cpp:114)
+  int n = v.n_atoms;
+  PDGPU_CUDA(cudaMemcpyAsync(v.ox, v.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(v.oy, v.y, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(v.oz, v.z, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
+  double J2k = k.J2kcal * k.Na;
+  double slope = p->SlopeCutoff > 0 ? p->SlopeCutoff * J2k : -1.0;
+  double strict = p->Strictness;  // kcal/mol (minimise.cpp:256)
+  int every = p->UpdateNList;
+  int r;
+  if (!P.have_list || P.nl_total < 0) {
+    r = nlist_enqueue(c, e, true);
+    if (r) return r;
+  }
+  cudaEventRecord(P.ev0, c->st);
+  // Chunks of up to 16 steps run without a host synchronisation.  A step
+  // whose list rebuild overflowed does nothing on the device (flag); the
+  // host grows the list and repeats it.  The list cadence follows the
+  // steps the device actually took.
+  const int counter0 = P.nlist_counter;
+  int taken = 0, regrow = 0;
+  while (taken < steps) {
+    int chunk = std::min(16, steps - taken);
+    for (int q = 0; q < chunk; q++) {
+      int cnt = counter0 + taken + q;
+      if (every > 0 && (cnt % every) == 0) {
+        launch_nlist_count(P, c->st);
+        launch_nlist_fill(P, c->st);
+      }
+      calc_forces_enqueue(c, e);
+      launch_min_step(v, c->st, e->min_state, p->Algorithm, slope, strict, p->StepSize, steps);
+    }
+    int flags[F_COUNT];
+    PDGPU_CUDA(cudaMemcpyAsync(flags, v.flags, sizeof flags, cudaMemcpyDeviceToHost, c->st));
+    r = sync_check(c, "minimise");
+    if (r) return r;
+    int nan, done_taken;
+    double mult;
+    PDGPU_CUDA(cudaMemcpy(hs.data(), e->min_state, hs.size(), cudaMemcpyDeviceToHost));
+    min_state_read(hs.data(), 0, &done_taken, &nan, &mult);
+    if (nan) {
+      if (steps_taken) *steps_taken = -1;
+      set_error("Simulation unstable (NaN energy during minimisation)");
+      return PDGPU_ERR_UNSTABLE;
+    }
+    bool finished = done_taken == taken && !flags[F_NL_OVERFLOW];  // converged (SlopeCutoff)
+    taken = done_taken;
+    if (flags[F_NL_OVERFLOW]) {
+      if (++regrow > 8) {
+        set_error("neighbour list kept overflowing during minimisation");
+        return PDGPU_ERR_STATE;
+      }
+      r = nlist_enqueue(c, e, true);  // sized rebuild at the current positions
+      if (r) return r;
+      continue;
+    }
+    if (finished) break;
+  }
+  P.nlist_counter = counter0 + taken;
+  // cur = old; recompute the energies (minimise.cpp:172-176)
+  launch_min_finish(v, c->st);
+  calc_forces_enqueue(c, e);
+  cudaEventRecord(P.ev1, c->st);
+  r = sync_check(c, "minimise finish");
+  if (r) return r;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, P.ev0, P.ev1);
+  P.last_run_ms = ms;
+  c->last_ms = ms;
+  if (steps_taken) *steps_taken = taken;
+  return PDGPU_OK;
+}
+
+// ------------------------------------------------------------ instrumentation
+int pdgpu_pair_counts(pdgpu_ctx *c, int32_t sys, int64_t *counts) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  int r = need_list(P);
+  if (r) return r;
+  if (!counts) {
+    set_error("counts is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  unsigned long long *d = nullptr;
+  PDGPU_CUDA(cudaMalloc(&d, 3 * sizeof(unsigned long long)));
+  cudaMemsetAsync(d, 0, 3 * sizeof(unsigned long long), c->st);
+  launch_pair_counts(P.v, c->st, d);
+  unsigned long long h[3];
+  cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, c->st);
+  r = sync_check(c, "pair_counts");
+  cudaFree(d);
+  if (r) return r;
+  for (int q = 0; q < 3; q++) counts[q] = (int64_t)h[q];
+  return PDGPU_OK;
+}
+
+int pdgpu_profile_pair_kernels(pdgpu_ctx *c, int32_t sys, int32_t reps, double *ms) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  int r = need_list(P);
+  if (r) return r;
+  if (!ms || reps <= 0) {
+    set_error("ms is NULL or reps <= 0");
+    return PDGPU_ERR_ARG;
+  }
+  cudaEvent_t ev[4];
+  for (int q = 0; q < 4; q++) cudaEventCreate(&ev[q]);
+  double acc[3] = {0, 0, 0};
+  for (int it = 0; it < reps; it++) {
+    launch_zero(P.v, c->st);
+    cudaEventRecord(ev[0], c->st);
+    launch_born_radii(P.v, c->st);
+    cudaEventRecord(ev[1], c->st);
+    launch_gb_pair(P.v, c->st);
+    cudaEventRecord(ev[2], c->st);
+    launch_gb_chain(P.v, c->st);
+    cudaEventRecord(ev[3], c->st);
+    r = sync_check(c, "profile");
+    if (r) break;
+    for (int q = 0; q < 3; q++) {
+      float t = 0;
+      cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
+      acc[q] += t;
+    }
+  }
+  for (int q = 0; q < 4; q++) cudaEventDestroy(ev[q]);
+  if (r) return r;
+  for (int q = 0; q < 3; q++) ms[q] = acc[q] / reps;
+  return PDGPU_OK;
+}
+
+int pdgpu_launch_count(pdgpu_ctx *c, int64_t *count) {
+  CHECK_CTX(c);
+  if (!count) {
+    set_error("count is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  *count = launch_counter();
+  return PDGPU_OK;
+}
+
+int pdgpu_last_run_ms(pdgpu_ctx *c, double *ms) {
+  CHECK_CTX(c);
+  if (!ms) {
+    set_error("ms is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  *ms = c->last_ms;
+  return PDGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,207 @@
+// FF_Bonded on the device: harmonic bonds (ffbonded.cpp:885-940), harmonic
+// angles (:994-1129) and Fourier / harmonic dihedrals for torsions and
+// impropers (calcDihedralForces, :1207-1499).  One thread per term, FP64
+// arithmetic (the terms are O(N) and cheap), forces scattered with 64-bit
+// fixed-point atomics (order-independent), per-term energies reduced per
+// system in a fixed order.
+#include <cuda_runtime.h>
+
+#include "internal.cuh"
+
+namespace pdgpu {
+
+__device__ __forceinline__ void add_force(const PackView &v, int i, double fx, double fy, double fz) {
+  atomicAdd((unsigned long long *)&v.fx[i], (unsigned long long)__double2ll_rn(fx * kForceScale));
+  atomicAdd((unsigned long long *)&v.fy[i], (unsigned long long)__double2ll_rn(fy * kForceScale));
+  atomicAdd((unsigned long long *)&v.fz[i], (unsigned long long)__double2ll_rn(fz * kForceScale));
+}
+
+__global__ void k_bonds(PackView v, double *e_term, double *vir_term) {
+  if (v.flags[F_NL_OVERFLOW]) return;  // the step is being re-planned
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= v.bt.nb) return;
+  int2 ij = v.bt.bij[t];
+  double2 lk = v.bt.blk[t];
+  int i = ij.x, j = ij.y;
+  double bx = v.x[i] - v.x[j], by = v.y[i] - v.y[j], bz = v.z[i] - v.z[j];
+  double d = sqrt(bx * bx + by * by + bz * bz);
+  double fm = 2 * lk.y * (d - lk.x);
+  e_term[t] = lk.y * (d - lk.x) * (d - lk.x);
+  vir_term[t] = d * fm;
+  double s = fm / d;
+  add_force(v, i, -bx * s, -by * s, -bz * s);
+  add_force(v, j, bx * s, by * s, bz * s);
+}
+
+__global__ void k_angles(PackView v, double *e_term) {
+  if (v.flags[F_NL_OVERFLOW]) return;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= v.bt.na) return;
+  double2 kt = v.bt.akt[t];
+  e_term[t] = 0.0;
+  if (kt.x == 0) return;
+  int4 q = v.bt.aiaj[t];
+  int i = q.x, a = q.y, j = q.z;
+  double iv[3] = {v.x[i] - v.x[a], v.y[i] - v.y[a], v.z[i] - v.z[a]};
+  double jv[3] = {v.x[j] - v.x[a], v.y[j] - v.y[a], v.z[j] - v.z[a]};
+  double inv_iv = 1 / sqrt(iv[0] * iv[0] + iv[1] * iv[1] + iv[2] * iv[2]);
+  double inv_jv = 1 / sqrt(jv[0] * jv[0] + jv[1] * jv[1] + jv[2] * jv[2]);
+  double ui[3], uj[3];
+  for (int c = 0; c < 3; c++) {
+    ui[c] = iv[c] * inv_iv;
+    uj[c] = jv[c] * inv_jv;
+  }
+  double cs = ui[0] * uj[0] + ui[1] * uj[1] + ui[2] * uj[2];
+  double theta = acos(cs);
+  double sn = sin(theta);
+  double dth = theta - kt.y;
+  e_term[t] = kt.x * dth * dth;
+  double fm = 2 * kt.x * dth;
+  double bi[3], bj[3];
+  for (int c = 0; c < 3; c++) {
+    bi[c] = fm * inv_iv * (ui[c] * cs - uj[c]) / sn;
+    bj[c] = fm * inv_jv * (uj[c] * cs - ui[c]) / sn;
+  }
+  add_force(v, i, -bi[0], -bi[1], -bi[2]);
+  add_force(v, j, -bj[0], -bj[1], -bj[2]);
+  add_force(v, a, bi[0] + bj[0], bi[1] + bj[1], bi[2] + bj[2]);
+}
+
+__global__ void k_dihedrals(PackView v, double *e_term) {
+  if (v.flags[F_NL_OVERFLOW]) return;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= v.bt.nt + v.bt.ni) return;
+  int4 q = v.bt.tidx[t];
+  int ti = q.x, ta = q.y, tb = q.z, tj = q.w;
+  const double *par = v.bt.tpar + 12 * (size_t)t;
+  int terms = v.bt.tterms[t];
+  double a[3] = {v.x[ti] - v.x[ta], v.y[ti] - v.y[ta], v.z[ti] - v.z[ta]};
+  double b[3] = {v.x[ta] - v.x[tb], v.y[ta] - v.y[tb], v.z[ta] - v.z[tb]};
+  double c[3] = {v.x[tb] - v.x[tj], v.y[tb] - v.y[tj], v.z[tb] - v.z[tj]};
+  double n1[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+  double n2[3] = {b[1] * c[2] - b[2] * c[1], b[2] * c[0] - b[0] * c[2], b[0] * c[1] - b[1] * c[0]};
+  double n3[3] = {b[1] * n1[2] - b[2] * n1[1], b[2] * n1[0] - b[0] * n1[2], b[0] * n1[1] - b[1] * n1[0]};
+  double in1 = 1.0 / sqrt(n1[0] * n1[0] + n1[1] * n1[1] + n1[2] * n1[2]);
+  double in2 = 1.0 / sqrt(n2[0] * n2[0] + n2[1] * n2[1] + n2[2] * n2[2]);
+  double in3 = 1.0 / sqrt(n3[0] * n3[0] + n3[1] * n3[1] + n3[2] * n3[2]);
+  double cos_phi = (n1[0] * n2[0] + n1[1] * n2[1] + n1[2] * n2[2]) * in1 * in2;
+  double sin_phi = (n3[0] * n2[0] + n3[1] * n2[1] + n3[2] * n2[2]) * in3 * in2;
+  for (int k = 0; k < 3; k++) n2[k] *= in2;
+  double phi = -atan2(sin_phi, cos_phi);
+  bool use_cos = fabs(sin_phi) > 0.1;
+  double d1[3], d2[3];
+  if (use_cos) {
+    for (int k = 0; k < 3; k++) n1[k] *= in1;
+    for (int k = 0; k < 3; k++) {
+      d1[k] = in1 * (n1[k] * cos_phi - n2[k]);
+      d2[k] = in2 * (n2[k] * cos_phi - n1[k]);
+    }
+  } else {
+    for (int k = 0; k < 3; k++) n3[k] *= in3;
+    for (int k = 0; k < 3; k++) {
+      d1[k] = in3 * (n3[k] * sin_phi - n2[k]);  // dsin/dn3
+      d2[k] = in2 * (n2[k] * sin_phi - n3[k]);  // dsin/dn2
+    }
+  }
+  double fi[3] = {0, 0, 0}, fab[3] = {0, 0, 0}, fj[3] = {0, 0, 0};
+  double e = 0;
+  const double PI = 3.14159265358979323846;
+  for (int m = 0; m < terms; m++) {
+    double k = par[m], n = par[4 + m], gamma = par[8 + m];
+    double ep, dE;
+    if (n > 0) {
+      ep = k * (1.0 + cos(n * phi + gamma));
+      dE = -n * k * sin(n * phi + gamma);
+    } else {
+      double diff = phi - gamma;
+      if (diff < -PI)
+        diff += 2.0 * PI;
+      else if (diff > PI)
+        diff -= 2.0 * PI;
+      ep = k * diff * diff;
+      dE = 2.0 * k * diff;
+    }
+    e += ep;
+    if (use_cos) {
+      dE /= sin_phi;
+      fi[0] += dE * (b[1] * d1[2] - b[2] * d1[1]);
+      fi[1] += dE * (b[2] * d1[0] - b[0] * d1[2]);
+      fi[2] += dE * (b[0] * d1[1] - b[1] * d1[0]);
+      fj[0] += dE * (b[2] * d2[1] - b[1] * d2[2]);
+      fj[1] += dE * (b[0] * d2[2] - b[2] * d2[0]);
+      fj[2] += dE * (b[1] * d2[0] - b[0] * d2[1]);
+      fab[0] += dE * (a[2] * d1[1] - a[1] * d1[2] + c[1] * d2[2] - c[2] * d2[1]);
+      fab[1] += dE * (a[0] * d1[2] - a[2] * d1[0] + c[2] * d2[0] - c[0] * d2[2]);
+      fab[2] += dE * (a[1] * d1[0] - a[0] * d1[1] + c[0] * d2[1] - c[1] * d2[0]);
+    } else {
+      dE /= -cos_phi;
+      fi[0] += dE * ((b[1] * b[1] + b[2] * b[2]) * d1[0] - b[0] * b[1] * d1[1] - b[0] * b[2] * d1[2]);
+      fi[1] += dE * ((b[2] * b[2] + b[0] * b[0]) * d1[1] - b[1] * b[2] * d1[2] - b[1] * b[0] * d1[0]);
+      fi[2] += dE * ((b[0] * b[0] + b[1] * b[1]) * d1[2] - b[2] * b[0] * d1[0] - b[2] * b[1] * d1[1]);
+      fj[0] += dE * (d2[1] * b[2] - d2[2] * b[1]);
+      fj[1] += dE * (d2[2] * b[0] - d2[0] * b[2]);
+      fj[2] += dE * (d2[0] * b[1] - d2[1] * b[0]);
+      fab[0] += dE * (-(b[1] * a[1] + b[2] * a[2]) * d1[0] + (2.0 * b[0] * a[1] - a[0] * b[1]) * d1[1] +
+                      (2.0 * b[0] * a[2] - a[0] * b[2]) * d1[2] + d2[2] * c[1] - d2[1] * c[2]);
+      fab[1] += dE * (-(b[2] * a[2] + b[0] * a[0]) * d1[1] + (2.0 * b[1] * a[2] - a[1] * b[2]) * d1[2] +
+                      (2.0 * b[1] * a[0] - a[1] * b[0]) * d1[0] + d2[0] * c[2] - d2[2] * c[0]);
+      fab[2] += dE * (-(b[0] * a[0] + b[1] * a[1]) * d1[2] + (2.0 * b[2] * a[0] - a[2] * b[0]) * d1[0] +
+                      (2.0 * b[2] * a[1] - a[2] * b[1]) * d1[1] + d2[1] * c[0] - d2[0] * c[1]);
+    }
+  }
+  e_term[t] = e;
+  add_force(v, ti, fi[0], fi[1], fi[2]);
+  add_force(v, ta, fab[0] - fi[0], fab[1] - fi[1], fab[2] - fi[2]);
+  add_force(v, tb, fj[0] - fab[0], fj[1] - fab[1], fj[2] - fab[2]);
+  add_force(v, tj, -fj[0], -fj[1], -fj[2]);
+}
+
+// Per-system sums of the per-term energies in a fixed order.  Terms are
+// stored system by system, so each system owns one contiguous range of each
+// kind; off[4*(S+1)] holds the ranges (bonds, angles, torsions, impropers;
+// torsion and improper ranges index the shared dihedral array).
+__global__ void k_reduce_bonded(PackView v, const double *eb, const double *vb, const double *ea,
+                                const double *ed, const int *off) {
+  if (v.flags[F_NL_OVERFLOW]) return;
+  int s = blockIdx.x;
+  int S = v.n_sys;
+  __shared__ double sh[4][256];
+  double acc[4] = {0, 0, 0, 0};
+  int b0 = off[s], b1 = off[s + 1];
+  int a0 = off[(S + 1) + s], a1 = off[(S + 1) + s + 1];
+  int t0 = off[2 * (S + 1) + s], t1 = off[2 * (S + 1) + s + 1];
+  int i0 = off[3 * (S + 1) + s], i1 = off[3 * (S + 1) + s + 1];
+  for (int k = b0 + threadIdx.x; k < b1; k += blockDim.x) {
+    acc[0] += eb[k];
+    acc[3] += vb[k];
+  }
+  for (int k = a0 + threadIdx.x; k < a1; k += blockDim.x) acc[1] += ea[k];
+  for (int k = t0 + threadIdx.x; k < t1; k += blockDim.x) acc[2] += ed[k];
+  for (int k = i0 + threadIdx.x; k < i1; k += blockDim.x) acc[2] += ed[k];
+  for (int c = 0; c < 4; c++) sh[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int c = 0; c < 4; c++) sh[c][threadIdx.x] += sh[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double *E = v.ene + (size_t)s * E_COUNT;
+    E[E_BOND] += sh[0][0];
+    E[E_ANGLE] += sh[1][0];
+    E[E_TORSION] += sh[2][0];
+    E[E_VIRIAL] += sh[3][0];
+    E[E_EPOT] += sh[0][0] + sh[1][0] + sh[2][0];
+  }
+}
+
+void launch_bonded_terms(const PackView &v, cudaStream_t st, double *scratch, const int *off) {
+  const BondedTerms &bt = v.bt;
+  double *eb = scratch, *vb = eb + bt.nb, *ea = vb + bt.nb, *ed = ea + bt.na;
+  if (bt.nb) PDGPU_LAUNCH(k_bonds, (bt.nb + 255) / 256, 256, 0, st, v, eb, vb);
+  if (bt.na) PDGPU_LAUNCH(k_angles, (bt.na + 255) / 256, 256, 0, st, v, ea);
+  if (bt.nt + bt.ni) PDGPU_LAUNCH(k_dihedrals, (bt.nt + bt.ni + 255) / 256, 256, 0, st, v, ed);
+  if (v.n_sys) PDGPU_LAUNCH(k_reduce_bonded, v.n_sys, 256, 0, st, v, eb, vb, ea, ed, off);
+}
+
+}  // namespace pdgpu

@@ -1,0 +1,533 @@
+// MD integrators, kinetic energy, velocity initialisation and the
+// minimiser's device-side control flow.
+//
+//   Langevin        MolecularDynamics::applyForces_LangevinIntegration (md.cpp:906-1042)
+//   Langevin non-H  applyForces_LangevinIntegration_NonHydrogens        (md.cpp:1048-1218)
+//   VelocityVerlet  applyForces_VelocityVerletIntegration               (md.cpp:788-838)
+//   Beeman          applyForces_BeemanIntegration                       (md.cpp:841-902)
+//   Verlet          applyForces_VerletIntegration                       (md.cpp:748-786)
+//   KE              calcKineticEnergy                                   (md.cpp:504-539)
+//   init velocities setInitialSpeeds                                    (md.cpp:342-363)
+//   SD / CG         Minimisation::doSteepestDescentStep / doConjugateGradientStep
+//                   (minimise.cpp:181-318) and the runcore bookkeeping (:99-179)
+//
+// State is FP64 (positions in Angstrom, velocities in m/s, forces converted
+// from the fixed-point accumulators to N), as in the reference.  Random
+// normals come from a counter-based Philox4x32-10 generator keyed by the
+// system's seed and indexed by (system-local atom, step), so a system's
+// trajectory does not depend on which other systems share its launch.
+// Roofline: HBM-bound, 152 B/atom/step algorithmic traffic.
+#include <cuda_runtime.h>
+
+#include "internal.cuh"
+
+namespace pdgpu {
+
+// --------------------------------------------------------------- Philox4x32-10
+// Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3"
+// (SC11): 10 rounds of two 32x32->64 multiplies with the published
+// multipliers and Weyl key increments.
+struct U4 {
+  unsigned a, b, c, d;
+};
+__device__ __forceinline__ U4 philox(U4 ctr, unsigned k0, unsigned k1) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    unsigned hi0 = __umulhi(0xD2511F53u, ctr.a), lo0 = 0xD2511F53u * ctr.a;
+    unsigned hi1 = __umulhi(0xCD9E8D57u, ctr.c), lo1 = 0xCD9E8D57u * ctr.c;
+    U4 n;
+    n.a = hi1 ^ ctr.b ^ k0;
+    n.b = lo1;
+    n.c = hi0 ^ ctr.d ^ k1;
+    n.d = lo0;
+    ctr = n;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return ctr;
+}
+// uniform in (0, 1], like the reference's frand() (maths.cpp:256-261)
+__device__ __forceinline__ double u01(unsigned x) { return ((double)x + 1.0) * (1.0 / 4294967296.0); }
+// Box-Muller pair in the reference's form (maths.h:136-151)
+__device__ __forceinline__ void nrand_pair(unsigned ua, unsigned ub, double &n1, double &n2) {
+  double z1 = u01(ua), z2 = u01(ub);
+  double l = sqrt(-2.0 * log(z1));
+  double s, c;
+  sincos(-2.0 * 3.14159265358979323846 * z2, &s, &c);
+  n1 = l * c;
+  n2 = l * s;
+}
+// six normals for atom `local` at `step`, in the reference's draw order
+// n1x n2y n2x n1z n1y n2z
+__device__ __forceinline__ void six_normals(unsigned long long seed, int local, int step, double *o) {
+  unsigned k0 = (unsigned)seed, k1 = (unsigned)(seed >> 32);
+  U4 r1 = philox(U4{(unsigned)local, (unsigned)step, 0u, 0x4D44u}, k0, k1);
+  U4 r2 = philox(U4{(unsigned)local, (unsigned)step, 1u, 0x4D44u}, k0, k1);
+  nrand_pair(r1.a, r1.b, o[0], o[1]);
+  nrand_pair(r1.c, r1.d, o[2], o[3]);
+  nrand_pair(r2.a, r2.b, o[4], o[5]);
+}
+
+__device__ __forceinline__ double force_N(long long f) {
+  return (double)f * kInvForceScale;  // kcal/mol/A; caller scales to N
+}
+
+__device__ __forceinline__ void store_pos(const PackView &v, int i, double x, double y, double z) {
+  v.x[i] = x;
+  v.y[i] = y;
+  v.z[i] = z;
+  float hx = __double2float_rn(x), hy = __double2float_rn(y), hz = __double2float_rn(z);
+  float4 a = v.pa[i];
+  a.x = hx;
+  a.y = hy;
+  a.z = hz;
+  v.pa[i] = a;
+  v.pb[i] = make_float4(__double2float_rn(x - (double)hx), __double2float_rn(y - (double)hy),
+                        __double2float_rn(z - (double)hz), 0.f);
+}
+
+struct MDDev {
+  MDCoef c;
+  double N_per_unit;   // kcal/mol/A -> N
+  double inv_angstrom; // 1 / 1e-10 as the reference forms it
+  double kB;
+  const unsigned char *is_h;
+  const unsigned long long *sys_seed;
+};
+
+// One integrator step for every atom of the pack.  KE per atom goes to
+// e_atom[AE_KIN] and is reduced per system afterwards.
+__global__ void k_md_step(PackView v, MDDev d, const double *normals, const int *step_dev) {
+  if (v.flags[F_NL_OVERFLOW]) return;  // forces incomplete: keep the state, host re-plans
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v.n_atoms) return;
+  const MDCoef &c = d.c;
+  int step = step_dev ? *step_dev : c.step;
+  double m = v.mass_si[i];
+  double f[3] = {force_N(v.fx[i]) * d.N_per_unit, force_N(v.fy[i]) * d.N_per_unit,
+                 force_N(v.fz[i]) * d.N_per_unit};
+  double vel[3] = {v.vx[i], v.vy[i], v.vz[i]};
+  double pos[3] = {v.x[i], v.y[i], v.z[i]};
+  double t = c.dt;
+  int integ = c.integrator;
+  bool hyd = d.is_h && d.is_h[i];
+  bool langevin = integ == PDGPU_INTEGRATOR_LANGEVIN;
+  if (langevin && c.gamma * t < 0.00001) integ = PDGPU_INTEGRATOR_VELOCITY_VERLET, langevin = false;
+  bool vv_like = integ == PDGPU_INTEGRATOR_VELOCITY_VERLET || (langevin && !c.stochastic_h && hyd);
+  double ke = 0;
+  if (vv_like && integ == PDGPU_INTEGRATOR_VELOCITY_VERLET) {
+    // md.cpp:788-838 as written: kick, KE, kick, drift with v+dv, kick
+    double tim = 0.5 * t / m;
+    for (int k = 0; k < 3; k++) vel[k] += f[k] * tim;
+    ke = 0.5 * m * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
+    for (int k = 0; k < 3; k++) {
+      double dv = f[k] * tim;
+      vel[k] += dv;
+      double dr = t * (vel[k] + dv);
+      dr *= d.inv_angstrom;
+      pos[k] += dr;
+      vel[k] += dv;
+    }
+  } else if (langevin && vv_like) {
+    // hydrogens in the non-hydrogen Langevin variant (md.cpp:1135-1183)
+    double tim = 0.5 * t / m;
+    if (step > 0)
+      for (int k = 0; k < 3; k++) vel[k] += f[k] * tim;
+    ke = 0.5 * m * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
+    if (step < c.steps - 1)
+      for (int k = 0; k < 3; k++) {
+        double dv = f[k] * tim;
+        double dr = t * (vel[k] + dv);
+        dr *= d.inv_angstrom;
+        pos[k] += dr;
+        vel[k] += dv;
+      }
+  } else if (langevin) {
+    double tim = t / m;
+    double gt = c.gamma * t;
+    if (step > 0)
+      for (int k = 0; k < 3; k++) vel[k] += (1.0 - c.c0 / c.c1) * f[k] * tim / gt;
+    ke = 0.5 * m * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
+    if (step < c.steps - 1) {
+      double nr[6];
+      if (normals) {
+        for (int k = 0; k < 6; k++) nr[k] = normals[6 * (size_t)i + k];
+      } else {
+        int s = v.sys_of[i];
+        six_normals(d.sys_seed[s], i - v.atom_off[s], step, nr);
+      }
+      double n1x = nr[0], n2y = nr[1], n2x = nr[2], n1z = nr[3], n1y = nr[4], n2z = nr[5];
+      double kTdivm = d.kB * c.temp / m;
+      double sigmav = sqrt(kTdivm * c.varv);
+      double sigmar = sqrt(kTdivm * c.varr) / c.gamma;
+      double sq = sqrt(1.0 - c.crv * c.crv);
+      double dvr[3] = {sigmav * (c.crv * n1x + sq * n2x), sigmav * (c.crv * n1y + sq * n2y),
+                       sigmav * (c.crv * n1z + sq * n2z)};
+      double drr[3] = {sigmar * n1x, sigmar * n1y, sigmar * n1z};
+      for (int k = 0; k < 3; k++) {
+        double dr = t * (c.c1 * vel[k] + c.c2 * f[k] * tim) + drr[k];
+        dr *= d.inv_angstrom;
+        double dv = (c.c0 * c.c2) * f[k] * tim / c.c1 + dvr[k];
+        pos[k] += dr;
+        vel[k] *= c.c0;
+        vel[k] += dv;
+      }
+    }
+  } else if (integ == PDGPU_INTEGRATOR_BEEMAN) {
+    double tim = t / (6.0 * m);
+    double fo[3] = {v.fox[i], v.foy[i], v.foz[i]};
+    if (step > 0)
+      for (int k = 0; k < 3; k++) vel[k] += (2.0 * f[k]) * tim;
+    ke = 0.5 * m * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
+    if (step < c.steps - 1) {
+      for (int k = 0; k < 3; k++) {
+        double dr = t * (vel[k] + (4.0 * f[k] - fo[k]) * tim);
+        dr *= d.inv_angstrom;
+        double dv = (5.0 * f[k] - fo[k]) * tim;
+        pos[k] += dr;
+        vel[k] += dv;
+      }
+      v.fox[i] = f[0];
+      v.foy[i] = f[1];
+      v.foz[i] = f[2];
+    }
+  } else {  // Verlet (md.cpp:748-786): needs the previous position in o*
+    double op[3] = {v.ox[i], v.oy[i], v.oz[i]};
+    double np[3];
+    for (int k = 0; k < 3; k++) {
+      double t2a = f[k] * (t * t / 1e-10 / m);
+      np[k] = pos[k] * 2 - op[k] + t2a;
+      vel[k] = (np[k] - op[k]) / (2 * t / 1e-10);
+    }
+    v.ox[i] = pos[0];
+    v.oy[i] = pos[1];
+    v.oz[i] = pos[2];
+    v.fox[i] = f[0];
+    v.foy[i] = f[1];
+    v.foz[i] = f[2];
+    pos[0] = np[0];
+    pos[1] = np[1];
+    pos[2] = np[2];
+    ke = 0.5 * m * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
+  }
+  v.vx[i] = vel[0];
+  v.vy[i] = vel[1];
+  v.vz[i] = vel[2];
+  store_pos(v, i, pos[0], pos[1], pos[2]);
+  v.e_atom[(size_t)AE_KIN * v.n_atoms + i] = ke;  // J
+}
+
+__global__ void k_step_inc(int *step_dev, const int *flags) {
+  if (!flags[F_NL_OVERFLOW]) (*step_dev)++;
+}
+
+// KE per system (J -> stored in kcal/mol) and etot = epot + ekin.
+__global__ void k_reduce_ke(PackView v, double J2kcalmol, int from_velocities) {
+  if (v.flags[F_NL_OVERFLOW]) return;
+  int s = blockIdx.x;
+  int a0 = v.atom_off[s], a1 = v.atom_off[s + 1];
+  __shared__ double sh[256];
+  double acc = 0;
+  for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
+    if (from_velocities) {
+      double vx = v.vx[i], vy = v.vy[i], vz = v.vz[i];
+      acc += 0.5 * v.mass_si[i] * (vx * vx + vy * vy + vz * vz);
+    } else {
+      acc += v.e_atom[(size_t)AE_KIN * v.n_atoms + i];
+    }
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double *E = v.ene + (size_t)s * E_COUNT;
+    E[E_EKIN] = sh[0] * J2kcalmol;
+    E[E_ETOT] = E[E_EPOT] + E[E_EKIN];
+  }
+}
+
+// history[step][sys][3] = epot, ekin, etot (kcal/mol)
+// step_dev[0] = current step, step_dev[1] = first step of the run
+__global__ void k_record(PackView v, double *hist, const int *step_dev) {
+  const int step0 = step_dev[1];
+  if (v.flags[F_NL_OVERFLOW]) return;
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= v.n_sys) return;
+  int k = *step_dev - step0;
+  const double *E = v.ene + (size_t)s * E_COUNT;
+  double *h = hist + ((size_t)k * v.n_sys + s) * 3;
+  h[0] = E[E_EPOT];
+  h[1] = E[E_EKIN];
+  h[2] = E[E_ETOT];
+  if (!(E[E_EPOT] == E[E_EPOT])) atomicExch(&v.flags[F_NAN], 1);
+}
+
+// setInitialSpeeds: Boltzmann draw (two nrand pairs, the second overwriting
+// vy as the reference does, md.cpp:353-356); then rescale to 3/2 N kB T.
+__global__ void k_vel_init(PackView v, double kB, double temp, const unsigned long long *sys_seed) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v.n_atoms) return;
+  int s = v.sys_of[i];
+  double nr[6];
+  six_normals(sys_seed[s] ^ 0x5EEDull, i - v.atom_off[s], -1, nr);
+  double sigma = sqrt(kB * temp / v.mass_si[i]);
+  double vx = nr[0] * sigma, vy = nr[1] * sigma;
+  vy = nr[2] * sigma;  // nrand(vy, vz): second pair overwrites vy
+  double vz = nr[3] * sigma;
+  v.vx[i] = vx;
+  v.vy[i] = vy;
+  v.vz[i] = vz;
+}
+__global__ void k_vel_scale(PackView v, double kB, double temp, double kcal2J_per_mol) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v.n_atoms) return;
+  int s = v.sys_of[i];
+  int n = v.atom_off[s + 1] - v.atom_off[s];
+  double ekin = v.ene[(size_t)s * E_COUNT + E_EKIN] * kcal2J_per_mol;  // J
+  double edes = 3 * n * kB * temp / 2;
+  double chi = sqrt(edes / ekin);
+  v.vx[i] *= chi;
+  v.vy[i] *= chi;
+  v.vz[i] *= chi;
+}
+
+// --------------------------------------------------------------- minimiser
+struct MinState {
+  double mult, old_energy, local_old, gamma, fmagold, fmagnew;
+  int step, breakcount, done, action;  // action: 0 step, 1 restore-and-skip, 2 restore-then-step
+  int taken, nan;
+};
+
+// CG dot products per system: fmagold = sum of.of, fmagnew = sum (of-f).f
+__global__ void k_min_dots(PackView v, MinState *ms, double N_per_unit) {
+  if (v.flags[F_NL_OVERFLOW]) return;
+  int s = blockIdx.x;
+  int a0 = v.atom_off[s], a1 = v.atom_off[s + 1];
+  __shared__ double sa[256], sb[256];
+  double A = 0, B = 0;
+  for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
+    double f[3] = {force_N(v.fx[i]) * N_per_unit, force_N(v.fy[i]) * N_per_unit,
+                   force_N(v.fz[i]) * N_per_unit};
+    double of[3] = {v.fox[i], v.foy[i], v.foz[i]};
+    A += of[0] * of[0] + of[1] * of[1] + of[2] * of[2];
+    B += (of[0] - f[0]) * f[0] + (of[1] - f[1]) * f[1] + (of[2] - f[2]) * f[2];
+  }
+  sa[threadIdx.x] = A;
+  sb[threadIdx.x] = B;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      sa[threadIdx.x] += sa[threadIdx.x + w];
+      sb[threadIdx.x] += sb[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    ms[s].fmagold = sa[0];
+    ms[s].fmagnew = sb[0];
+  }
+}
+
+// One thread per system: the accept / restore decision of the step.
+// Energies here are kcal/mol; one joule per molecule (the reference's
+// "m_OldEnergy += 1" after a rejected SD step) is J_unit kcal/mol.
+__global__ void k_min_control(PackView v, MinState *ms, int algorithm, double slope_cutoff_kcal,
+                              double strictness_kcal, double J_unit, int nsteps) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= v.n_sys) return;
+  MinState &m = ms[s];
+  if (v.flags[F_NL_OVERFLOW]) {  // no valid forces this step: do nothing, retry
+    m.action = -1;
+    return;
+  }
+  if (m.done) {
+    m.action = -1;
+    return;
+  }
+  double epot = v.ene[(size_t)s * E_COUNT + E_EPOT];
+  if (!(epot == epot)) {
+    m.nan = 1;
+    m.done = 1;
+    m.action = -1;
+    atomicExch(&v.flags[F_NAN], 1);
+    return;
+  }
+  if (m.step == 0) m.local_old = epot;
+  if (m.step > 0 && slope_cutoff_kcal > 0.0) {
+    double d = m.local_old - epot;
+    if (d >= 0.0 && d < slope_cutoff_kcal) m.breakcount++;
+    m.local_old = epot;
+  }
+  if (m.breakcount > 10) {
+    m.done = 1;
+    m.action = -1;
+    return;
+  }
+  if (algorithm == PDGPU_MIN_STEEPEST_DESCENT) {
+    if (m.step != 0) {
+      if (epot <= m.old_energy) {
+        m.mult *= 1.2;
+        m.old_energy = epot;
+        m.action = 0;  // save then step
+      } else {
+        m.mult *= 0.5 / 1.2;
+        m.old_energy += J_unit;
+        m.action = 1;  // restore, no step
+      }
+    } else {
+      m.old_energy = epot;
+      m.action = 0;
+    }
+  } else {
+    if (m.step != 0) {
+      if ((m.mult < 0.05 && (epot - m.old_energy) < strictness_kcal) || epot < m.old_energy) {
+        m.mult *= 1.2;
+        double g = m.fmagold != 0 ? m.fmagnew / m.fmagold : 0.0;
+        if (g < 0) g = 0;
+        m.gamma = g;
+        m.old_energy = epot;
+        m.action = 3;  // new direction, save, step
+      } else {
+        m.mult *= 0.5 / 1.2;
+        m.action = 2;  // restore positions, step along the old direction
+      }
+    } else {
+      m.old_energy = epot;
+      m.action = 4;  // first step: direction = force
+    }
+  }
+  m.step++;
+  m.taken = m.step;
+  if (m.step >= nsteps) m.done = 1;
+}
+
+__global__ void k_min_update(PackView v, const MinState *ms, double N_per_unit, double step_size) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v.n_atoms) return;
+  int s = v.sys_of[i];
+  const MinState &m = ms[s];
+  int a = m.action;
+  if (a < 0) return;
+  double f[3] = {force_N(v.fx[i]) * N_per_unit, force_N(v.fy[i]) * N_per_unit,
+                 force_N(v.fz[i]) * N_per_unit};
+  double p[3] = {v.x[i], v.y[i], v.z[i]};
+  double sc = step_size * m.mult;
+  if (a == 0) {  // SD accept (or first step): save p, f; step along f
+    v.ox[i] = p[0];
+    v.oy[i] = p[1];
+    v.oz[i] = p[2];
+    v.fox[i] = f[0];
+    v.foy[i] = f[1];
+    v.foz[i] = f[2];
+    for (int k = 0; k < 3; k++) p[k] += f[k] * sc;
+  } else if (a == 1) {  // SD reject: restore p (the restored force is recomputed next step)
+    p[0] = v.ox[i];
+    p[1] = v.oy[i];
+    p[2] = v.oz[i];
+  } else if (a == 2) {  // CG reject: restore p, step along the current direction
+    p[0] = v.ox[i] + v.dirx[i] * sc;
+    p[1] = v.oy[i] + v.diry[i] * sc;
+    p[2] = v.oz[i] + v.dirz[i] * sc;
+  } else {  // 3: CG accept (new direction), 4: first CG step
+    double d[3];
+    if (a == 3) {
+      d[0] = v.odx[i] * m.gamma + f[0];
+      d[1] = v.ody[i] * m.gamma + f[1];
+      d[2] = v.odz[i] * m.gamma + f[2];
+    } else {
+      d[0] = f[0];
+      d[1] = f[1];
+      d[2] = f[2];
+    }
+    v.dirx[i] = d[0];
+    v.diry[i] = d[1];
+    v.dirz[i] = d[2];
+    v.odx[i] = d[0];
+    v.ody[i] = d[1];
+    v.odz[i] = d[2];
+    v.ox[i] = p[0];
+    v.oy[i] = p[1];
+    v.oz[i] = p[2];
+    v.fox[i] = f[0];
+    v.foy[i] = f[1];
+    v.foz[i] = f[2];
+    for (int k = 0; k < 3; k++) p[k] += d[k] * sc;
+  }
+  store_pos(v, i, p[0], p[1], p[2]);
+}
+
+// end of runcore: cur = old (the last accepted positions)
+__global__ void k_min_restore_best(PackView v) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v.n_atoms) return;
+  store_pos(v, i, v.ox[i], v.oy[i], v.oz[i]);
+}
+
+// --------------------------------------------------------------- launchers
+void launch_md_step_impl(const PackView &v, cudaStream_t st, const MDCoef &c, const double *normals,
+                         const int *step_dev, const unsigned char *is_h, const unsigned long long *seeds) {
+  const Consts &k = consts();
+  MDDev d;
+  d.c = c;
+  d.N_per_unit = k.N_per_kcalmolA;
+  d.inv_angstrom = 1 / k.Angstrom;
+  d.kB = k.kB;
+  d.is_h = is_h;
+  d.sys_seed = seeds;
+  if (v.n_atoms) PDGPU_LAUNCH(k_md_step, (v.n_atoms + 255) / 256, 256, 0, st, v, d, normals, step_dev);
+  if (v.n_sys) PDGPU_LAUNCH(k_reduce_ke, v.n_sys, 256, 0, st, v, k.J2kcal * k.Na, 0);
+}
+void launch_step_inc(const PackView &v, int *step_dev, cudaStream_t st) {
+  PDGPU_LAUNCH(k_step_inc, 1, 1, 0, st, step_dev, v.flags);
+}
+
+long long &launch_counter() {
+  static long long n = 0;
+  return n;
+}
+void launch_record(const PackView &v, cudaStream_t st, double *hist, const int *step_dev) {
+  if (v.n_sys) PDGPU_LAUNCH(k_record, (v.n_sys + 127) / 128, 128, 0, st, v, hist, step_dev);
+}
+void launch_ke_from_velocities(const PackView &v, cudaStream_t st) {
+  const Consts &k = consts();
+  if (v.n_sys) PDGPU_LAUNCH(k_reduce_ke, v.n_sys, 256, 0, st, v, k.J2kcal * k.Na, 1);
+}
+void launch_vel_init_impl(const PackView &v, cudaStream_t st, double temp, const unsigned long long *seeds) {
+  const Consts &k = consts();
+  if (!v.n_atoms) return;
+  PDGPU_LAUNCH(k_vel_init, (v.n_atoms + 255) / 256, 256, 0, st, v, k.kB, temp, seeds);
+  launch_ke_from_velocities(v, st);
+  PDGPU_LAUNCH(k_vel_scale, (v.n_atoms + 255) / 256, 256, 0, st, v, k.kB, temp, k.kcal2J / k.Na);
+  launch_ke_from_velocities(v, st);
+}
+void launch_min_step(const PackView &v, cudaStream_t st, void *ms, int algorithm, double slope_kcal,
+                     double strict_kcal, double step_size, int nsteps) {
+  const Consts &k = consts();
+  MinState *m = (MinState *)ms;
+  if (algorithm == PDGPU_MIN_CONJUGATE_GRADIENTS) PDGPU_LAUNCH(k_min_dots, v.n_sys, 256, 0, st, v, m, k.N_per_kcalmolA);
+  PDGPU_LAUNCH(k_min_control, (v.n_sys + 127) / 128, 128, 0, st, v, m, algorithm, slope_kcal, strict_kcal,
+                                                       k.J2kcal * k.Na, nsteps);
+  PDGPU_LAUNCH(k_min_update, (v.n_atoms + 255) / 256, 256, 0, st, v, m, k.N_per_kcalmolA, step_size);
+}
+void launch_min_finish(const PackView &v, cudaStream_t st) {
+  if (v.n_atoms) PDGPU_LAUNCH(k_min_restore_best, (v.n_atoms + 255) / 256, 256, 0, st, v);
+}
+size_t min_state_size() { return sizeof(MinState); }
+void min_state_init(void *host_buf, int n) {
+  MinState *m = (MinState *)host_buf;
+  for (int s = 0; s < n; s++) {
+    m[s] = MinState{};
+    m[s].mult = 1.0;
+  }
+}
+void min_state_read(const void *host_buf, int s, int *taken, int *nan, double *mult) {
+  const MinState *m = (const MinState *)host_buf;
+  *taken = m[s].taken;
+  *nan = m[s].nan;
+  *mult = m[s].mult;
+}
+
+}  // namespace pdgpu

@@ -1,0 +1,241 @@
+// Internal data model of libpdgpu (B200 / sm_100a).
+//
+// A Pack is a set of systems resident on one device, atoms concatenated.
+// Every kernel works on a Pack through PackView; per-atom arrays are SoA,
+// per-system settings live in a small SysParams table indexed by sys_of[i].
+// A single system is a Pack of one; batched evaluation packs many.
+//
+// Units inside the kernels: Angstrom, kcal/mol, kcal/mol/A, e.  Conversion
+// to the reference's SI units (J, N) happens only at the C-ABI boundary.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "pdgpu.h"
+
+namespace pdgpu {
+
+// ----------------------------------------------------------------- constants
+// Values the reference computes in forcefields/forcefield.cpp:18-38 (same
+// expressions, evaluated once on the host in double precision).
+struct Consts {
+  double kcal2J, J2kcal, Na, kB, Angstrom, econv, econv_joule, halfeconv,
+      halfeconv_joule;
+  double J_per_kcalmol;  // kcal2J / Na : kcal/mol -> J/molecule
+  double N_per_kcalmolA; // (kcal2J/Na) / Angstrom : kcal/mol/A -> N
+};
+const Consts &consts();
+
+// Fixed-point scales.  Forces: kcal/mol/A * 2^32 in int64 (range +-2.1e9
+// kcal/mol/A).  Born sums: A^-1 * 2^40 in int64 (range +-8.3e6).
+constexpr double kForceScale = 4294967296.0;          // 2^32
+constexpr double kInvForceScale = 1.0 / 4294967296.0;
+constexpr double kBornScale = 1099511627776.0;        // 2^40
+constexpr double kInvBornScale = 1.0 / 1099511627776.0;
+
+// Per-system settings in kernel units.  Float copies feed the FP32 pair
+// math; double copies feed the exact recomputation of the two
+// discontinuous predicates (Still cutoff, GB exp-approximation threshold).
+struct SysParams {
+  // cutoffs
+  float rc2, rc, rin, inv_sw2;           // elec/GB energy switch
+  float vdw_rc, vdw_rin, vdw_inv_sw2;    // VdW energy switch
+  float vdw14, elec14;
+  float econv_in, econv_out;             // econv / eps_solute, econv / eps_solvent
+  float premul;                          // Born premultiplier, kcal/mol*A
+  float exp_thresh;                      // ExpApproxThreshold
+  float still2;                          // GbsaStillCutoff^2
+  float P4, P5, invP5, piP5;
+  // stand-alone LJ/Coulomb (FF_NonBonded)
+  float econv_nb;                        // econv / Dielectric
+  float ddd_alpha, dielectric;
+  float fs_A, fs_B, fs_C, fs_D, fs_E, fs_cutV, fs_eshift;  // force switch
+  float vdwcor_e;                        // per-atom long-range correction, kcal/mol
+  int elec_mode;                         // 0 none 1 normal 2 DDD 3 energy switch 4 force switch
+  int vdw_mode;                          // 0 none 2 energy switch
+  int fast_mode;
+  int pad_;
+  // exact predicates (double)
+  double still2_d, exp_thresh_d, nl_lim2_d, rc2_d;
+  double halfeconv_d, born_offset_d, premul_d;
+  double vdwcor_e_d;
+};
+
+enum EneSlot {
+  E_EPOT = 0, E_VDW, E_ELEC, E_POL, E_POL_CROSS, E_POL_SELF, E_BOND, E_ANGLE,
+  E_TORSION, E_VIRIAL, E_EKIN, E_ETOT, E_GB_COMPONENT, E_COUNT = 16
+};
+
+// Per-atom energy terms written by the pair kernels (kcal/mol), reduced per
+// system in a fixed order so every sum is bit-reproducible.
+enum AtomEne { AE_VDW = 0, AE_ELEC, AE_POL, AE_POL_SELF, AE_VIR, AE_KIN, AE_COUNT };
+
+struct BondedTerms {
+  int nb = 0, na = 0, nt = 0, ni = 0;
+  int2 *bij = nullptr;        // bond atoms (global)
+  double2 *blk = nullptr;     // (l, k kcal/mol/A^2)
+  int4 *aiaj = nullptr;       // (i, a, j, -)
+  double2 *akt = nullptr;     // (k kcal/mol/rad^2, theta0)
+  int4 *tidx = nullptr;       // torsions then impropers (i,a,b,j)
+  int *tterms = nullptr;
+  double *tpar = nullptr;     // 12 per dihedral: Vn kcal/mol, n, gamma
+};
+
+// Device view of a Pack.  Plain pointers, passed by value to kernels.
+struct PackView {
+  int n_atoms, n_sys;
+  const int *atom_off;        // [S+1]
+  const int *sys_of;          // [N]
+  const SysParams *sp;        // [S]
+  // state (FP64)
+  double *x, *y, *z;          // Angstrom
+  double *vx, *vy, *vz;       // m/s
+  double *ox, *oy, *oz;       // saved positions (minimiser / restore)
+  // pair-kernel copies
+  float4 *pa;                 // (x_hi, y_hi, z_hi, q)
+  float4 *pb;                 // (x_lo, y_lo, z_lo, 0)
+  const float4 *prm;          // (lj_radius, sqrt_eps (kcal/mol)^1/2, gb_R, V_j)
+  const double *gbR_d;        // gb_R (double)
+  const double *pv_d;         // P4 * V_j (double)
+  const double *terms123;     // Still fixed terms (A^-1 scaled like the reference)
+  const double *inv_mass_si;  // 1 / kg
+  const double *mass_si;      // kg
+  double *born_d;             // Born radii
+  float *born_f;
+  float *w_chain;             // gpi_i * deda_i (kcal/mol/A^2 scaled)
+  long long *fx, *fy, *fz;    // fixed-point forces
+  double *fox, *foy, *foz;    // saved forces (N) for Beeman / minimiser
+  double *dirx, *diry, *dirz; // CG directions / old directions
+  double *odx, *ody, *odz;
+  double *e_atom;             // [AE_COUNT * N]
+  double *ene;                // [S * E_COUNT] J-free kcal/mol accumulators
+  // bond order
+  const int *mid;             // [S]
+  const long long *band_off;  // [S]
+  const int8_t *band;
+  const int *off_ptr;         // [N+1] off-diagonal partners per atom
+  const int2 *off_data;       // (partner global index, order)
+  // neighbour list (full): entries (j_global << 3) | bondorder
+  long long *row_start;       // [N+1]
+  int *row_cnt;               // [N]
+  unsigned *nl;
+  long long nl_cap;
+  // cell grid
+  int *cell_key;              // [N]
+  int *sorted_atom;           // [N]
+  int *cell_start, *cell_end; // [cell_cap]
+  int cell_cap;
+  double *grid;               // [S*8] origin xyz, cell size, dims(as double), cell_off
+  int *flags;                 // [8] overflow / nan / etc.
+  BondedTerms bt;
+};
+
+enum Flag { F_NL_OVERFLOW = 0, F_NAN = 1, F_CELL_CLAMP = 2, F_COUNT = 8 };
+
+// ----------------------------------------------------------------- host side
+struct SystemHost {
+  int natoms = 0;
+  pdgpu_ff_params params;
+  std::vector<double> charge, radius, epsilon, mass, gbR;
+  std::vector<int> residue;
+  std::vector<int> c12p, c12i, c13p, c13i, c14p, c14i;
+  std::vector<double> c12d, c13d;
+  // derived
+  int mid = 0;
+  std::vector<int8_t> band;
+  std::vector<int> off_i, off_j, off_o;   // unique (i<j) pairs, last order wins
+  std::vector<double> vj, terms123;
+  // bonded (reference units)
+  std::vector<int> bij, aiaj, tidx, tterms;
+  std::vector<double> blk, akt, tpar;
+  int nb = 0, na = 0, nt = 0, ni = 0;
+};
+
+// Owner of device memory for a Pack.
+struct Pack {
+  int device = 0;
+  PackView v{};
+  std::vector<int> atom_off;     // host copy
+  std::vector<SysParams> sp;     // host copy
+  std::vector<void *> allocs;
+  int64_t bytes = 0;
+  long long nl_total = -1;       // last known list size (host)
+  bool have_list = false;
+  int radix_passes = 3;
+  // temporary buffers for scans / sorts
+  int *tmp_keys = nullptr, *tmp_vals = nullptr;
+  int *sort_hist = nullptr;      // [256 * blocks]
+  long long *scan_tmp = nullptr;
+  int scan_tmp_len = 0;
+  double *red_tmp = nullptr;     // reductions
+  // bookkeeping for protocols
+  int nlist_counter = 0;
+  double last_run_ms = 0.0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  ~Pack();
+};
+
+// Build a device Pack from host systems (atoms concatenated in order).
+Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHost *> &systems,
+                  std::string *err);
+void pack_set_params(Pack *p, int s, const pdgpu_ff_params &prm);
+SysParams make_sys_params(const pdgpu_ff_params &p);
+
+// Host setup computations (restate the reference's setup code).
+int host_bondorder(SystemHost &s, std::string *err);
+void host_gb_fixed_terms(SystemHost &s);
+
+// ----------------------------------------------------------------- launchers
+// All launchers enqueue on `st` and do not synchronise.
+void launch_pack_positions(const PackView &v, cudaStream_t st);
+void launch_zero(const PackView &v, cudaStream_t st);
+// neighbour list: build phases.  count -> (host may read total) -> fill
+void launch_nlist_count(Pack &p, cudaStream_t st);
+void launch_nlist_fill(Pack &p, cudaStream_t st);
+// GB
+void launch_born_radii(const PackView &v, cudaStream_t st);
+void launch_gb_pair(const PackView &v, cudaStream_t st);
+void launch_gb_chain(const PackView &v, cudaStream_t st);
+void launch_born_energy(const PackView &v, cudaStream_t st);
+void launch_nonbonded(const PackView &v, cudaStream_t st, int elec_mode);
+void launch_bonded(const PackView &v, cudaStream_t st);
+// energies: reduce per-atom terms into the per-system record (adds)
+void launch_reduce_gb_energies(const PackView &v, cudaStream_t st, int mode);
+// integrators / minimiser
+struct MDCoef {
+  double dt, gamma, c0, c1, c2, varv, varr, crv, temp;
+  int integrator, step, steps, use_normals, stochastic_h;
+  unsigned long long seed;
+};
+void launch_md_step(const PackView &v, cudaStream_t st, const MDCoef &c, const double *normals,
+                    const int *step_dev);
+void launch_kinetic(const PackView &v, cudaStream_t st);
+void launch_vel_init(const PackView &v, cudaStream_t st, double temp, unsigned long long seed);
+void launch_vel_rescale(const PackView &v, cudaStream_t st, double temp);
+void launch_check_nan(const PackView &v, cudaStream_t st);
+
+// ----------------------------------------------------------------- errors
+void set_error(const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+}  // namespace pdgpu
+
+// Every kernel launch goes through PDGPU_LAUNCH so the context can report
+// how many of its kernels ran (graph replays add their kernel-node count).
+namespace pdgpu {
+long long &launch_counter();
+}
+#define PDGPU_LAUNCH(kern, grid, block, smem, stream, ...)          \
+  do {                                                             \
+    kern<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);      \
+    ::pdgpu::launch_counter()++;                                   \
+  } while (0)
+
+#define PDGPU_CUDA(call)                                      \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return ::pdgpu::cuda_fail(e_, #call); \
+  } while (0)

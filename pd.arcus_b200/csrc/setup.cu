@@ -1,0 +1,479 @@
+// Host-side setup: constants, bond-order band, Still fixed terms, per-system
+// kernel parameters and Pack allocation.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+
+#include "internal.cuh"
+
+namespace pdgpu {
+
+static thread_local std::string g_err;
+void set_error(const std::string &msg) { g_err = msg; }
+const char *last_error_cstr() { return g_err.c_str(); }
+int cuda_fail(cudaError_t e, const char *what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? PDGPU_ERR_NOMEM : PDGPU_ERR_CUDA;
+}
+
+// forcefields/forcefield.cpp:18-38 -- same expressions, same order.
+const Consts &consts() {
+  static Consts c = [] {
+    Consts k;
+    double e_charge = 1.60217645E-19;
+    double sqr_e_charge = e_charge * e_charge;
+    double e0 = 8.854187817E-12;
+    double _4pi_e0 = (3.14159265358979323846 * 4.0) * e0;
+    k.kcal2J = 4184.0;
+    k.J2kcal = 1.0 / k.kcal2J;
+    k.Na = 6.0221418E23;
+    k.kB = 1.38065E-23;
+    k.Angstrom = 1E-10;
+    k.econv = (k.J2kcal * k.Na * sqr_e_charge) / (_4pi_e0 * k.Angstrom);
+    k.halfeconv = k.econv * 0.5;
+    k.econv_joule = sqr_e_charge / (_4pi_e0 * k.Angstrom);
+    k.halfeconv_joule = k.econv_joule * 0.5;
+    k.J_per_kcalmol = k.kcal2J / k.Na;
+    k.N_per_kcalmolA = k.J_per_kcalmol / k.Angstrom;
+    return k;
+  }();
+  return c;
+}
+
+// BondOrder::reinit (workspace/bondorder.cpp:77-195).  Band width: largest
+// index distance of a 1-2/1-3/1-4 partner in the same or an adjacent residue,
+// plus one.  The band is filled 1-4, 1-3, 1-2 (later writes win); partners
+// farther apart than the band go to a sparse list, whose last entry for a
+// pair wins when the neighbour list is corrected (neighbourlist.cpp:162-203).
+int host_bondorder(SystemHost &s, std::string *err) {
+  const int n = s.natoms;
+  const std::vector<int> *P[3] = {&s.c12p, &s.c13p, &s.c14p};
+  const std::vector<int> *I[3] = {&s.c12i, &s.c13i, &s.c14i};
+  int mid = 0;
+  for (int i = 0; i < n; i++)
+    for (int l = 0; l < 3; l++)
+      for (int k = (*P[l])[i]; k < (*P[l])[i + 1]; k++) {
+        int lookup = (*I[l])[k];
+        if (lookup < 0 || lookup >= n) {
+          if (err) *err = "covalent partner index out of range";
+          return PDGPU_ERR_ARG;
+        }
+        if (std::abs(s.residue[i] - s.residue[lookup]) > 1) continue;
+        mid = std::max(mid, std::abs(i - lookup));
+      }
+  mid += 1;
+  s.mid = mid;
+  s.band.assign((size_t)mid * (size_t)(n > 1 ? n - 1 : 0), (int8_t)7);
+  std::map<std::pair<int, int>, int> sparse;  // last write wins
+  const int lists[3] = {2, 1, 0};
+  const int orders[3] = {3, 2, 1};
+  for (int i = 0; i < n; i++)
+    for (int t = 0; t < 3; t++) {
+      int l = lists[t];
+      for (int k = (*P[l])[i]; k < (*P[l])[i + 1]; k++) {
+        int j = (*I[l])[k];
+        if (j <= i) continue;
+        int delta = j - i;
+        int order = std::min(orders[t], 7);
+        if (delta > mid)
+          sparse[std::make_pair(i, j)] = order;
+        else
+          s.band[(size_t)i * mid + (delta - 1)] = (int8_t)order;
+      }
+    }
+  s.off_i.clear();
+  s.off_j.clear();
+  s.off_o.clear();
+  for (auto &kv : sparse) {
+    s.off_i.push_back(kv.first.first);
+    s.off_j.push_back(kv.first.second);
+    s.off_o.push_back(kv.second);
+  }
+  return PDGPU_OK;
+}
+
+// FF_GeneralizedBorn_Still::calcFixedBornRadiiTerms (gbff.cpp:307-381).
+void host_gb_fixed_terms(SystemHost &s) {
+  const double PI = 3.14159265358979323846;
+  const double FourPI = 4.0 * PI;
+  const int n = s.natoms;
+  const pdgpu_ff_params &p = s.params;
+  s.vj.assign(n, 0.0);
+  s.terms123.assign(n, 0.0);
+  auto sq = [](double x) { return x * x; };
+  for (int j = 0; j < n; j++) {
+    double Rj = s.gbR[j];
+    if (Rj <= 0.01) Rj = 1.15;
+    double v = FourPI * Rj * Rj * Rj / 3;
+    for (int nk = s.c12p[j]; nk < s.c12p[j + 1]; nk++) {
+      int k = s.c12i[nk];
+      double Rk = s.gbR[k];
+      if (Rk <= 0.01) Rk = 1.15;
+      double rjk = 1.01 * s.c12d[nk];
+      double hjk = Rj * (1.0 + (sq(Rk) - sq(Rj) - sq(rjk)) / (2.0 * Rj * rjk));
+      v -= PI * sq(hjk) * (3 * Rj - hjk) / 3;
+    }
+    s.vj[j] = v < 0 ? 0 : v;
+  }
+  for (int i = 0; i < n; i++) {
+    double Rj = s.gbR[i];
+    if (Rj <= 0.01) Rj = 1.15;
+    double term1 = -166.0 / (Rj + p.DielectricOffset + p.P1);
+    double term2 = 0, term3 = 0;
+    for (int nj = s.c12p[i]; nj < s.c12p[i + 1]; nj++) {
+      double rij = s.c12d[nj];
+      term2 += p.P2 * s.vj[s.c12i[nj]] / (sq(rij) * sq(rij));
+    }
+    for (int nj = s.c13p[i]; nj < s.c13p[i + 1]; nj++) {
+      double rij = s.c13d[nj];
+      term3 += p.P3 * s.vj[s.c13i[nj]] / (sq(rij) * sq(rij));
+    }
+    s.terms123[i] = term1 + term2 + term3;
+  }
+}
+
+// Kernel-unit settings for one system.
+SysParams make_sys_params(const pdgpu_ff_params &p) {
+  const Consts &c = consts();
+  SysParams s;
+  memset(&s, 0, sizeof s);
+  auto sq = [](double x) { return x * x; };
+  auto cube = [](double x) { return x * x * x; };
+  double Rc = p.Cutoff, Ri = p.InnerCutoff;
+  s.rc2 = (float)sq(Rc);
+  s.rc2_d = sq(Rc);
+  s.rc = (float)Rc;
+  s.rin = (float)Ri;
+  s.inv_sw2 = (float)sq(1.0 / (Rc - Ri));
+  s.vdw_rc = (float)p.VdwCutoff;
+  s.vdw_rin = (float)p.VdwInnerCutoff;
+  s.vdw_inv_sw2 = (float)sq(1.0 / (p.VdwCutoff - p.VdwInnerCutoff));
+  s.vdw14 = (float)p.Vdw14Scaling;
+  s.elec14 = (float)p.Elec14Scaling;
+  s.econv_in = (float)(c.econv / p.DielectricSolute);
+  s.econv_out = (float)(c.econv / p.DielectricSolvent);
+  double premul_kcal = -c.halfeconv * (1 / p.DielectricSolute - 1 / p.DielectricSolvent);
+  s.premul = (float)premul_kcal;
+  s.premul_d = premul_kcal;
+  s.exp_thresh = (float)p.ExpApproxThreshold;
+  s.exp_thresh_d = p.ExpApproxThreshold;
+  s.still2 = (float)sq(p.GbsaStillCutoff);
+  s.still2_d = sq(p.GbsaStillCutoff);
+  s.P4 = (float)p.P4;
+  s.P5 = (float)p.P5;
+  s.invP5 = (float)(1 / p.P5);
+  s.piP5 = (float)(p.P5 * 3.14159265358979323846);
+  s.halfeconv_d = c.halfeconv;
+  s.born_offset_d = p.BornRadiusOffset;
+  double lc = std::max(p.Cutoff, p.VdwCutoff) + p.Padding;
+  s.nl_lim2_d = sq(lc);
+  // stand-alone LJ/Coulomb (nonbonded.cpp:1205-1229 mode selection)
+  s.dielectric = (float)p.Dielectric;
+  s.ddd_alpha = (float)p.DDDielectricAlpha;
+  s.econv_nb = (float)(c.econv / p.Dielectric);
+  int em = 1;
+  if (p.EnergySwitch) em = 3;
+  if (p.ForceSwitch) em = 4;
+  if (p.DDDielectric) em = 2;
+  if (!p.DoElec) em = 0;
+  s.elec_mode = em;
+  s.vdw_mode = p.DoVdw ? 2 : 0;
+  s.fast_mode = p.FastMode;
+  double sA = 1.0 / cube(sq(Rc) - sq(Ri));
+  double sB = -(cube(sq(Rc)) - 3.0 * sq(Rc) * sq(Rc) * sq(Ri));
+  double sC = 6.0 * sq(Rc) * sq(Ri);
+  double sD = -(sq(Rc) + sq(Ri));
+  double sE = 2.0 / 5.0;
+  double fin = sA * (sB * (1.0 / Ri) + sC * Ri + sD * cube(Ri) + sE * cube(Ri) * sq(Ri));
+  double fcut = sA * (sB * (1.0 / Rc) + sC * Rc + sD * cube(Rc) + sE * cube(Rc) * sq(Rc));
+  s.fs_A = (float)sA;
+  s.fs_B = (float)sB;
+  s.fs_C = (float)sC;
+  s.fs_D = (float)sD;
+  s.fs_E = (float)sE;
+  s.fs_cutV = (float)fcut;
+  s.fs_eshift = (float)(Ri < Rc ? 1 / Ri + (fin - fcut) : 0.0);
+  if (p.VdwCor) {
+    // nonbonded.cpp:845-857, J -> kcal/mol
+    double vp = -0.5 * p.VdwCorDensity * p.VdwCorEpsilon * (8.0 / 3.0) * 3.14159265358979323846 *
+                sq(p.VdwCorRadius) * sq(p.VdwCorRadius) * sq(p.VdwCorRadius) / cube(p.VdwCorCutoff);
+    s.vdwcor_e_d = vp;
+    s.vdwcor_e = (float)vp;
+  }
+  return s;
+}
+
+// ----------------------------------------------------------------- Pack
+Pack::~Pack() {
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != device) cudaSetDevice(device);
+  for (void *a : allocs) cudaFree(a);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (cur >= 0 && cur != device) cudaSetDevice(cur);
+}
+
+template <typename T>
+static cudaError_t palloc(Pack *p, T **ptr, size_t count) {
+  size_t bytes = sizeof(T) * (count > 0 ? count : 1);
+  cudaError_t e = cudaMalloc((void **)ptr, bytes);
+  if (e == cudaSuccess) {
+    p->allocs.push_back((void *)*ptr);
+    p->bytes += (int64_t)bytes;
+    cudaMemset(*ptr, 0, bytes);
+  }
+  return e;
+}
+
+void pack_set_params(Pack *p, int s, const pdgpu_ff_params &prm) {
+  p->sp[s] = make_sys_params(prm);
+}
+
+#define PALLOC(ptr, n)                                        \
+  do {                                                        \
+    cudaError_t e_ = palloc(p, &(ptr), (n));                  \
+    if (e_ != cudaSuccess) {                                  \
+      if (err) *err = std::string("cudaMalloc failed: ") + cudaGetErrorString(e_); \
+      delete p;                                               \
+      return nullptr;                                         \
+    }                                                         \
+  } while (0)
+
+Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHost *> &systems,
+                  std::string *err) {
+  const Consts &c = consts();
+  Pack *p = new Pack();
+  p->device = device;
+  int S = (int)systems.size();
+  int N = 0;
+  p->atom_off.push_back(0);
+  for (auto *s : systems) {
+    N += s->natoms;
+    p->atom_off.push_back(N);
+  }
+  PackView &v = p->v;
+  v.n_atoms = N;
+  v.n_sys = S;
+  // host staging
+  std::vector<int> sys_of(N);
+  std::vector<float4> pa(N), pb(N), prm(N);
+  std::vector<double> gbR(N), pv(N), t123(N), minv(N), mass(N), X(N), Y(N), Z(N);
+  std::vector<int> mid(S);
+  std::vector<long long> band_off(S);
+  std::vector<int8_t> band;
+  std::vector<int> off_ptr(N + 1, 0);
+  std::vector<std::vector<int2>> offl(N);
+  double sqrt_eps_scale = std::sqrt(c.J2kcal * c.Na);
+  for (int s = 0; s < S; s++) {
+    const SystemHost &h = *systems[s];
+    p->sp.push_back(make_sys_params(h.params));
+    int o = p->atom_off[s];
+    for (int i = 0; i < h.natoms; i++) {
+      int g = o + i;
+      sys_of[g] = s;
+      prm[g] = make_float4((float)h.radius[i], (float)(h.epsilon[i] * sqrt_eps_scale), (float)h.gbR[i],
+                           (float)h.vj[i]);
+      pa[g] = make_float4(0, 0, 0, (float)h.charge[i]);
+      gbR[g] = h.gbR[i];
+      pv[g] = h.params.P4 * h.vj[i];
+      t123[g] = h.terms123[i];
+      minv[g] = 1.0 / h.mass[i];
+      mass[g] = h.mass[i];
+    }
+    mid[s] = h.mid;
+    band_off[s] = (long long)band.size();
+    band.insert(band.end(), h.band.begin(), h.band.end());
+    for (size_t k = 0; k < h.off_i.size(); k++) {
+      int a = o + h.off_i[k], b = o + h.off_j[k];
+      offl[a].push_back(make_int2(b, h.off_o[k]));
+      offl[b].push_back(make_int2(a, h.off_o[k]));
+    }
+  }
+  std::vector<int2> off_data;
+  for (int i = 0; i < N; i++) {
+    off_ptr[i] = (int)off_data.size();
+    off_data.insert(off_data.end(), offl[i].begin(), offl[i].end());
+  }
+  off_ptr[N] = (int)off_data.size();
+
+  // device allocations
+  int *atom_off_d, *sys_of_d, *mid_d, *off_ptr_d;
+  SysParams *sp_d;
+  long long *band_off_d;
+  int8_t *band_d;
+  int2 *off_data_d;
+  float4 *prm_d;
+  double *gbR_d, *pv_d, *t123_d, *minv_d, *mass_d;
+  PALLOC(atom_off_d, S + 1);
+  PALLOC(sys_of_d, N);
+  PALLOC(sp_d, S);
+  PALLOC(mid_d, S);
+  PALLOC(band_off_d, S);
+  PALLOC(band_d, band.size());
+  PALLOC(off_ptr_d, N + 1);
+  PALLOC(off_data_d, off_data.size());
+  PALLOC(prm_d, N);
+  PALLOC(gbR_d, N);
+  PALLOC(pv_d, N);
+  PALLOC(t123_d, N);
+  PALLOC(minv_d, N);
+  PALLOC(mass_d, N);
+  PALLOC(v.x, N);
+  PALLOC(v.y, N);
+  PALLOC(v.z, N);
+  PALLOC(v.vx, N);
+  PALLOC(v.vy, N);
+  PALLOC(v.vz, N);
+  PALLOC(v.ox, N);
+  PALLOC(v.oy, N);
+  PALLOC(v.oz, N);
+  PALLOC(v.pa, N);
+  PALLOC(v.pb, N);
+  PALLOC(v.born_d, N);
+  PALLOC(v.born_f, 2 * N);
+  PALLOC(v.w_chain, N);
+  PALLOC(v.fx, N);
+  PALLOC(v.fy, N);
+  PALLOC(v.fz, N);
+  PALLOC(v.fox, N);
+  PALLOC(v.foy, N);
+  PALLOC(v.foz, N);
+  PALLOC(v.dirx, N);
+  PALLOC(v.diry, N);
+  PALLOC(v.dirz, N);
+  PALLOC(v.odx, N);
+  PALLOC(v.ody, N);
+  PALLOC(v.odz, N);
+  PALLOC(v.e_atom, (size_t)AE_COUNT * N);
+  PALLOC(v.ene, (size_t)E_COUNT * S);
+  PALLOC(v.row_start, N + 1);
+  PALLOC(v.row_cnt, N);
+  PALLOC(v.cell_key, N);
+  PALLOC(v.sorted_atom, N);
+  v.cell_cap = 2 * N + 64 * S;
+  PALLOC(v.cell_start, v.cell_cap);
+  PALLOC(v.cell_end, v.cell_cap);
+  PALLOC(v.grid, (size_t)8 * S);
+  PALLOC(v.flags, F_COUNT);
+  PALLOC(p->tmp_keys, N);
+  PALLOC(p->tmp_vals, N);
+  int tiles = (N + 2047) / 2048;
+  PALLOC(p->sort_hist, 256 * (size_t)(tiles > 0 ? tiles : 1));
+  p->scan_tmp_len = (N + 1023) / 1024 + 1;
+  PALLOC(p->scan_tmp, p->scan_tmp_len + 1);
+  PALLOC(p->red_tmp, 4096);
+  v.nl_cap = (long long)N * 48 + 4096;
+  PALLOC(v.nl, (size_t)v.nl_cap);
+  int bits = 1;
+  while ((1LL << bits) < (long long)v.cell_cap) bits++;
+  p->radix_passes = (bits + 7) / 8;
+
+  cudaMemcpyAsync(atom_off_d, p->atom_off.data(), sizeof(int) * (S + 1), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(sys_of_d, sys_of.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(sp_d, p->sp.data(), sizeof(SysParams) * S, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(mid_d, mid.data(), sizeof(int) * S, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(band_off_d, band_off.data(), sizeof(long long) * S, cudaMemcpyHostToDevice, st);
+  if (!band.empty()) cudaMemcpyAsync(band_d, band.data(), band.size(), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(off_ptr_d, off_ptr.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice, st);
+  if (!off_data.empty())
+    cudaMemcpyAsync(off_data_d, off_data.data(), sizeof(int2) * off_data.size(), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(prm_d, prm.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(v.pa, pa.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(gbR_d, gbR.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(pv_d, pv.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(t123_d, t123.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(minv_d, minv.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(mass_d, mass.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st);
+  v.atom_off = atom_off_d;
+  v.sys_of = sys_of_d;
+  v.sp = sp_d;
+  v.mid = mid_d;
+  v.band_off = band_off_d;
+  v.band = band_d;
+  v.off_ptr = off_ptr_d;
+  v.off_data = off_data_d;
+  v.prm = prm_d;
+  v.gbR_d = gbR_d;
+  v.pv_d = pv_d;
+  v.terms123 = t123_d;
+  v.inv_mass_si = minv_d;
+  v.mass_si = mass_d;
+
+  // bonded terms (converted to kcal/mol)
+  BondedTerms &bt = v.bt;
+  std::vector<int2> bij;
+  std::vector<double2> blk, akt;
+  std::vector<int4> aiaj, tidx;
+  std::vector<int> tterms;
+  std::vector<double> tpar;
+  double J2k = c.J2kcal * c.Na;
+  for (int s = 0; s < S; s++) {
+    const SystemHost &h = *systems[s];
+    int o = p->atom_off[s];
+    for (int k = 0; k < h.nb; k++) {
+      bij.push_back(make_int2(o + h.bij[2 * k], o + h.bij[2 * k + 1]));
+      blk.push_back(make_double2(h.blk[2 * k], h.blk[2 * k + 1] * J2k));
+    }
+    for (int k = 0; k < h.na; k++) {
+      aiaj.push_back(make_int4(o + h.aiaj[3 * k], o + h.aiaj[3 * k + 1], o + h.aiaj[3 * k + 2], s));
+      akt.push_back(make_double2(h.akt[2 * k] * J2k, h.akt[2 * k + 1]));
+    }
+  }
+  for (int pass = 0; pass < 2; pass++)
+    for (int s = 0; s < S; s++) {
+      const SystemHost &h = *systems[s];
+      int o = p->atom_off[s];
+      int base = pass == 0 ? 0 : h.nt;
+      int cnt = pass == 0 ? h.nt : h.ni;
+      for (int k = 0; k < cnt; k++) {
+        int q = base + k;
+        tidx.push_back(make_int4(o + h.tidx[4 * q], o + h.tidx[4 * q + 1], o + h.tidx[4 * q + 2],
+                                 o + h.tidx[4 * q + 3]));
+        tterms.push_back(h.tterms[q]);
+        for (int m = 0; m < 12; m++) {
+          double val = h.tpar[12 * q + m];
+          tpar.push_back(m < 4 ? val * J2k : val);
+        }
+      }
+    }
+  bt.nb = (int)bij.size();
+  bt.na = (int)aiaj.size();
+  int ndih = (int)tidx.size();
+  int nt_all = 0;
+  for (auto *s : systems) nt_all += s->nt;
+  bt.nt = nt_all;
+  bt.ni = ndih - nt_all;
+  PALLOC(bt.bij, bij.size());
+  PALLOC(bt.blk, blk.size());
+  PALLOC(bt.aiaj, aiaj.size());
+  PALLOC(bt.akt, akt.size());
+  PALLOC(bt.tidx, tidx.size());
+  PALLOC(bt.tterms, tterms.size());
+  PALLOC(bt.tpar, tpar.size());
+  if (!bij.empty()) {
+    cudaMemcpyAsync(bt.bij, bij.data(), sizeof(int2) * bij.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(bt.blk, blk.data(), sizeof(double2) * blk.size(), cudaMemcpyHostToDevice, st);
+  }
+  if (!aiaj.empty()) {
+    cudaMemcpyAsync(bt.aiaj, aiaj.data(), sizeof(int4) * aiaj.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(bt.akt, akt.data(), sizeof(double2) * akt.size(), cudaMemcpyHostToDevice, st);
+  }
+  if (!tidx.empty()) {
+    cudaMemcpyAsync(bt.tidx, tidx.data(), sizeof(int4) * tidx.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(bt.tterms, tterms.data(), sizeof(int) * tterms.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(bt.tpar, tpar.data(), sizeof(double) * tpar.size(), cudaMemcpyHostToDevice, st);
+  }
+  cudaEventCreate(&p->ev0);
+  cudaEventCreate(&p->ev1);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    if (err) *err = std::string("pack upload failed: ") + cudaGetErrorString(e);
+    delete p;
+    return nullptr;
+  }
+  return p;
+}
+
+}  // namespace pdgpu

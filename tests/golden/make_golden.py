@@ -1,0 +1,100 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+Runs oracle/_ref/ref_driver (the reference library compiled from its own
+sources by ``make -C oracle ref``) on seeded synthetic peptide systems and
+packs its FP64 outputs into compressed ``.npz`` files.  Needs the reference
+tree (REF, default /root/reference) only through that build; the fixtures
+themselves are self-contained and are what the tests read.
+
+    python tests/golden/make_golden.py            # all fixtures
+    python tests/golden/make_golden.py pep8_s1    # one
+
+Systems (extended builds from the reference's NewProtein, sequences drawn
+uniformly from the 20 standard residues with the stated seed, pre-minimised
+with 500 steepest-descent steps at Rc 12 A unless noted):
+  pep8_s1       8 residues, Rc 12, + 3 MD steps per integrator, 20 SD/CG steps
+  pep20_s2      20 residues, Rc 12, + 2 MD steps per integrator, 10 SD/CG steps
+  pep30_s3_rc16 30 residues, Rc 16 (the large-system cutoff)
+  two_chain_s4  two 12-residue chains 12 A apart, Rc 10 (inter-chain pairs)
+  c1_pep64_s0   the 64-residue, seed-0 chain of the small plain-MD workload, Rc 12
+  c2_16x80_s2   16 x 80-residue chains on a 4x4 grid 25 A apart (~20.6k atoms),
+                Rc 16: inputs plus reference forces, Born radii and energies
+                (no neighbour list: too large to store)
+"""
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+PARAM = os.path.join(ROOT, "oracle", "_ref", "param")
+
+SYSTEMS = {
+    "pep8_s1": dict(nres=[8], seed=1, cutoff=12, premin=500, md=3, min=20),
+    "pep20_s2": dict(nres=[20], seed=2, cutoff=12, premin=500, md=2, min=10),
+    "pep30_s3_rc16": dict(nres=[30], seed=3, cutoff=16, premin=500),
+    "two_chain_s4": dict(nres=[12, 12], seed=4, cutoff=10, premin=500, grid=(2, 12)),
+    "c1_pep64_s0": dict(nres=[64], seed=0, cutoff=12, premin=500),
+    "c2_16x80_s2": dict(nres=[80] * 16, seed=2, cutoff=16, premin=500, grid=(4, 25), drop_nl=True),
+}
+
+# arrays kept for the large system (inputs + a few reference results)
+LARGE_KEEP = None  # everything except the neighbour list
+
+
+def build(name, spec, keep_dir=None):
+    if not os.path.exists(DRIVER):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", "-j8"])
+    out = keep_dir or tempfile.mkdtemp(prefix="pdgold_")
+    cmd = [DRIVER, "build", "--out", out, "--nres", ",".join(map(str, spec["nres"])),
+           "--seed", str(spec["seed"]), "--cutoff", str(spec["cutoff"]),
+           "--premin", str(spec.get("premin", 500))]
+    if "grid" in spec:
+        cmd += ["--grid", "%d,%d" % spec["grid"]]
+    if spec.get("md"):
+        cmd += ["--md", str(spec["md"])]
+    if spec.get("min"):
+        cmd += ["--min", str(spec["min"])]
+    env = dict(os.environ, PD_PARAM_PATH=PARAM)
+    subprocess.check_call(cmd, env=env, stdout=subprocess.DEVNULL)
+    arrays = {}
+    for fn in sorted(os.listdir(out)):
+        if fn.endswith(".npy"):
+            arrays[fn[:-4]] = np.load(os.path.join(out, fn))
+    meta = {}
+    chains = []
+    with open(os.path.join(out, "meta.txt")) as fh:
+        for line in fh:
+            k, v = line.split(None, 1)
+            if k == "chain":
+                chains.append(v.strip())
+            else:
+                meta[k] = v.strip()
+    meta["chains"] = chains
+    meta["name"] = name
+    if spec.get("drop_nl"):
+        for k in list(arrays):
+            if k.startswith("nl_") or k in ("f_energypath", "ene_energypath", "atom_epot"):
+                del arrays[k]
+    arrays["meta_json"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+    if keep_dir is None:
+        shutil.rmtree(out)
+    return os.path.join(HERE, name + ".npz")
+
+
+def main(argv):
+    names = argv[1:] or list(SYSTEMS)
+    for n in names:
+        p = build(n, SYSTEMS[n])
+        print("%-16s %8.1f KB" % (n, os.path.getsize(p) / 1024.0))
+
+
+if __name__ == "__main__":
+    main(sys.argv)
