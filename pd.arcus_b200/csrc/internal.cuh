@@ -62,6 +62,7 @@ struct SysParams {
   double still2_d, exp_thresh_d, nl_lim2_d, rc2_d;
   double halfeconv_d, born_offset_d, premul_d;
   double vdwcor_e_d;
+  double P5_d, invP5_d;                  // Still P5 for the FP64 Born sums
 };
 
 enum EneSlot {

@@ -118,8 +118,8 @@ __global__ void __launch_bounds__(256) k_born(PackView v) {
   const double xi = v.x[i], yi = v.y[i], zi = v.z[i];
   const double Ri = v.gbR_d[i];
   const double still2 = P.still2_d;
-  const double invP5 = 1.0 / (double)P.P5;  // only the branch test uses it
-  const double P5 = (double)P.P5;
+  const double invP5 = P.invP5_d;
+  const double P5 = P.P5_d;
   long long b = v.row_start[i], e = v.row_start[i + 1];
   double acc = 0.0;
   for (long long k = b + lane; k < e; k += 32) {

@@ -163,6 +163,8 @@ SysParams make_sys_params(const pdgpu_ff_params &p) {
   s.P4 = (float)p.P4;
   s.P5 = (float)p.P5;
   s.invP5 = (float)(1 / p.P5);
+  s.P5_d = p.P5;
+  s.invP5_d = 1 / p.P5;
   s.piP5 = (float)(p.P5 * 3.14159265358979323846);
   s.halfeconv_d = c.halfeconv;
   s.born_offset_d = p.BornRadiusOffset;

@@ -137,6 +137,7 @@ class WorkSpace:
         self._params_key = None
         self._nlist = NeighbourList(self)
         self._pos_dirty = True
+        self._ff = None  # the Forcefield whose components set this workspace up
 
     def nAtoms(self):
         return self.spec.natoms
@@ -249,8 +250,10 @@ class NeighbourList:
 
     def calcNewList(self):
         ws = self.ws
+        if ws._sys is None and ws._ff is not None:
+            ws._ff.ensuresetup()
         if ws._sys is None:
-            raise A.PdgpuError(A.ERR_STATE, "set up a forcefield on this workspace first")
+            raise A.PdgpuError(A.ERR_STATE, "add a forcefield component to this workspace first")
         if ws._pos_dirty:
             ws._push_positions()
         A.check(A.lib().pdgpu_nlist_build(ws.ctx.ptr, ws._sys))
@@ -386,6 +389,7 @@ class Forcefield:
         if comp.getWSpace() is not self.wspace:
             raise ValueError("You cannot add this force field component because they use different workspaces.")
         self.components.append(comp)
+        self.wspace._ff = self
 
     def getWSpace(self):
         return self.wspace
