@@ -9,11 +9,8 @@
 
 namespace pdgpu {
 const char *last_error_cstr();
-void launch_bonded_terms(const PackView &v, cudaStream_t st, double *scratch, const int *off);
 void launch_md_step_impl(const PackView &v, cudaStream_t st, const MDCoef &c, const double *normals,
                          const int *step_dev, const unsigned char *is_h, const unsigned long long *seeds);
-void launch_step_inc(const PackView &v, int *step_dev, cudaStream_t st);
-void launch_record(const PackView &v, cudaStream_t st, double *hist, const int *step_dev);
 void launch_pair_counts(const PackView &v, cudaStream_t st, unsigned long long *out);
 void launch_ke_from_velocities(const PackView &v, cudaStream_t st);
 void launch_vel_init_impl(const PackView &v, cudaStream_t st, double temp, const unsigned long long *seeds);
@@ -32,8 +29,6 @@ struct SysEntry {
   SystemHost host;
   std::unique_ptr<Pack> pack;
   // bonded scratch + per-system term ranges
-  double *bonded_scratch = nullptr;
-  int *bonded_off = nullptr;
   unsigned char *is_h = nullptr;
   unsigned long long *seeds = nullptr;
   int *step_dev = nullptr;
@@ -299,8 +294,7 @@ int pdgpu_system_create(pdgpu_ctx *c, int32_t natoms, const double *charge, cons
   }
   e->pack.reset(p);
   if (xalloc(e.get(), &e->is_h, natoms) != cudaSuccess || xalloc(e.get(), &e->seeds, 1) != cudaSuccess ||
-      xalloc(e.get(), &e->step_dev, 2) != cudaSuccess ||
-      xalloc(e.get(), &e->bonded_off, 4 * 2) != cudaSuccess) {
+      xalloc(e.get(), &e->step_dev, 3) != cudaSuccess) {
     set_error("device allocation failed");
     return PDGPU_ERR_NOMEM;
   }
@@ -418,17 +412,6 @@ int pdgpu_system_set_bonded(pdgpu_ctx *c, int32_t sys, int32_t nb, const int32_t
   }
   e->drop_graph();
   e->pack.reset(p);
-  int off[8] = {0, nb, 0, na, 0, nt, nt, nt + ni};
-  PDGPU_CUDA(cudaMemcpyAsync(e->bonded_off, off, sizeof off, cudaMemcpyHostToDevice, c->st));
-  if (e->bonded_scratch) {
-    cudaFree(e->bonded_scratch);
-    e->extra.erase(std::find(e->extra.begin(), e->extra.end(), (void *)e->bonded_scratch));
-    e->bonded_scratch = nullptr;
-  }
-  if (xalloc(e, &e->bonded_scratch, (size_t)2 * nb + na + nt + ni + 1) != cudaSuccess) {
-    set_error("device allocation failed");
-    return PDGPU_ERR_NOMEM;
-  }
   r = pdgpu_set_positions(c, sys, x.data());
   if (r) return r;
   return pdgpu_set_velocities(c, sys, vv.data());
@@ -705,12 +688,10 @@ static void gb_forces_enqueue(pdgpu_ctx *c, Pack &P) {
   launch_born_radii(P.v, c->st);
   launch_gb_pair(P.v, c->st);
   launch_gb_chain(P.v, c->st);
-  launch_reduce_gb_energies(P.v, c->st, 0);
+  launch_energy(P.v, c->st, EM_PAIR_GB);
 }
 
-static void bonded_enqueue(pdgpu_ctx *c, SysEntry *e) {
-  if (e->bonded_scratch) launch_bonded_terms(e->pack->v, c->st, e->bonded_scratch, e->bonded_off);
-}
+static bool has_bonded(const Pack &P) { return P.v.bt.nb + P.v.bt.na + P.v.bt.nt + P.v.bt.ni > 0; }
 
 int pdgpu_gb_forces(pdgpu_ctx *c, int32_t sys) {
   CHECK_CTX(c);
@@ -741,9 +722,8 @@ int pdgpu_gb_energies(pdgpu_ctx *c, int32_t sys) {
   PDGPU_CUDA(cudaMemcpyAsync((void *)P.v.sp, P.sp.data(), sizeof(SysParams), cudaMemcpyHostToDevice, c->st));
   launch_born_radii(P.v, c->st);
   launch_nonbonded(P.v, c->st, P.sp[0].elec_mode);
-  launch_reduce_gb_energies(P.v, c->st, 1);
   launch_born_energy(P.v, c->st);
-  launch_reduce_gb_energies(P.v, c->st, 2);
+  launch_energy(P.v, c->st, EM_PAIR_NB | EM_BORN_ENERGY);
   P.sp[0] = saved;
   PDGPU_CUDA(cudaMemcpyAsync((void *)P.v.sp, P.sp.data(), sizeof(SysParams), cudaMemcpyHostToDevice, c->st));
   return sync_check(c, "gb_energies");
@@ -756,22 +736,31 @@ int pdgpu_nonbonded_forces(pdgpu_ctx *c, int32_t sys) {
   int r = need_list(P);
   if (r) return r;
   launch_nonbonded(P.v, c->st, P.sp[0].elec_mode);
-  launch_reduce_gb_energies(P.v, c->st, 1);
+  launch_energy(P.v, c->st, EM_PAIR_NB);
   return sync_check(c, "nonbonded_forces");
 }
 
 int pdgpu_bonded_forces(pdgpu_ctx *c, int32_t sys) {
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
-  bonded_enqueue(c, e);
+  Pack &P = *e->pack;
+  if (has_bonded(P)) {
+    launch_bonded_terms(P.v, c->st);
+    launch_energy(P.v, c->st, EM_BONDED);
+  }
   return sync_check(c, "bonded_forces");
 }
 
-static void calc_forces_enqueue(pdgpu_ctx *c, SysEntry *e) {
+// Forcefield::calcForces for {FF_Bonded, FF_GeneralizedBorn_Still}: the
+// Born-radius kernel zeroes forces and record first; one energy reduction.
+// extra_mode adds EM_KINETIC / EM_RECORD inside an MD step.
+static void calc_forces_enqueue(pdgpu_ctx *c, SysEntry *e, bool reduce = true) {
   Pack &P = *e->pack;
-  launch_zero(P.v, c->st);
-  bonded_enqueue(c, e);
-  gb_forces_enqueue(c, P);
+  launch_born_radii(P.v, c->st, true);
+  if (has_bonded(P)) launch_bonded_terms(P.v, c->st);
+  launch_gb_pair(P.v, c->st);
+  launch_gb_chain(P.v, c->st);
+  if (reduce) launch_energy(P.v, c->st, EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0));
 }
 
 int pdgpu_calc_forces(pdgpu_ctx *c, int32_t sys) {
@@ -865,13 +854,14 @@ int pdgpu_md_init_velocities(pdgpu_ctx *c, int32_t sys, double temperature, uint
   return sync_check(c, "init_velocities");
 }
 
-// one MD step enqueue: forces, integrate, record, advance the step counter
+// one MD step enqueue: forces, integrate, one energy reduction that also
+// records the step and advances the device step counter (7 launches)
 static void md_step_enqueue(pdgpu_ctx *c, SysEntry *e, const MDCoef &k) {
   Pack &P = *e->pack;
-  calc_forces_enqueue(c, e);
+  calc_forces_enqueue(c, e, false);
   launch_md_step_impl(P.v, c->st, k, nullptr, e->step_dev, e->is_h, e->seeds);
-  launch_record(P.v, c->st, e->hist, e->step_dev);
-  launch_step_inc(P.v, e->step_dev, c->st);
+  launch_energy(P.v, c->st, EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0) | EM_KINETIC | EM_RECORD, e->hist,
+                e->step_dev);
 }
 
 int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t first_step, int32_t steps,
@@ -915,7 +905,7 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
   // in-block rebuild overflows the list buffer, every kernel after it skips
   // (device flag), the state stays at the block start, and the host grows
   // the buffer and runs the block again.
-  int steps0[2] = {first_step, first_step};
+  int steps0[3] = {first_step, first_step, 0};
   PDGPU_CUDA(cudaMemcpyAsync(e->step_dev, steps0, sizeof steps0, cudaMemcpyHostToDevice, c->st));
   cudaEventRecord(P.ev0, c->st);
   int s = 0;

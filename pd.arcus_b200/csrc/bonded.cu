@@ -16,10 +16,7 @@ __device__ __forceinline__ void add_force(const PackView &v, int i, double fx, d
   atomicAdd((unsigned long long *)&v.fz[i], (unsigned long long)__double2ll_rn(fz * kForceScale));
 }
 
-__global__ void k_bonds(PackView v, double *e_term, double *vir_term) {
-  if (v.flags[F_NL_OVERFLOW]) return;  // the step is being re-planned
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= v.bt.nb) return;
+__device__ __forceinline__ void bond_term(const PackView &v, int t, double *e_term, double *vir_term) {
   int2 ij = v.bt.bij[t];
   double2 lk = v.bt.blk[t];
   int i = ij.x, j = ij.y;
@@ -33,10 +30,7 @@ __global__ void k_bonds(PackView v, double *e_term, double *vir_term) {
   add_force(v, j, bx * s, by * s, bz * s);
 }
 
-__global__ void k_angles(PackView v, double *e_term) {
-  if (v.flags[F_NL_OVERFLOW]) return;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= v.bt.na) return;
+__device__ __forceinline__ void angle_term(const PackView &v, int t, double *e_term) {
   double2 kt = v.bt.akt[t];
   e_term[t] = 0.0;
   if (kt.x == 0) return;
@@ -67,10 +61,7 @@ __global__ void k_angles(PackView v, double *e_term) {
   add_force(v, a, bi[0] + bj[0], bi[1] + bj[1], bi[2] + bj[2]);
 }
 
-__global__ void k_dihedrals(PackView v, double *e_term) {
-  if (v.flags[F_NL_OVERFLOW]) return;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= v.bt.nt + v.bt.ni) return;
+__device__ __forceinline__ void dihedral_term(const PackView &v, int t, double *e_term) {
   int4 q = v.bt.tidx[t];
   int ti = q.x, ta = q.y, tb = q.z, tj = q.w;
   const double *par = v.bt.tpar + 12 * (size_t)t;
@@ -156,52 +147,29 @@ __global__ void k_dihedrals(PackView v, double *e_term) {
   add_force(v, tj, -fj[0], -fj[1], -fj[2]);
 }
 
-// Per-system sums of the per-term energies in a fixed order.  Terms are
-// stored system by system, so each system owns one contiguous range of each
-// kind; off[4*(S+1)] holds the ranges (bonds, angles, torsions, impropers;
-// torsion and improper ranges index the shared dihedral array).
-__global__ void k_reduce_bonded(PackView v, const double *eb, const double *vb, const double *ea,
-                                const double *ed, const int *off) {
-  if (v.flags[F_NL_OVERFLOW]) return;
-  int s = blockIdx.x;
-  int S = v.n_sys;
-  __shared__ double sh[4][256];
-  double acc[4] = {0, 0, 0, 0};
-  int b0 = off[s], b1 = off[s + 1];
-  int a0 = off[(S + 1) + s], a1 = off[(S + 1) + s + 1];
-  int t0 = off[2 * (S + 1) + s], t1 = off[2 * (S + 1) + s + 1];
-  int i0 = off[3 * (S + 1) + s], i1 = off[3 * (S + 1) + s + 1];
-  for (int k = b0 + threadIdx.x; k < b1; k += blockDim.x) {
-    acc[0] += eb[k];
-    acc[3] += vb[k];
+// One launch for every bonded term: threads [0, nb) bonds, then angles,
+// then torsions and impropers.  Per-term energies feed the energy reduction.
+__global__ void k_bonded_all(PackView v) {
+  if (v.flags[F_NL_OVERFLOW]) return;  // the step is being re-planned
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const BondedTerms &b = v.bt;
+  if (t < b.nb) {
+    bond_term(v, t, b.e_bond, b.vir_bond);
+    return;
   }
-  for (int k = a0 + threadIdx.x; k < a1; k += blockDim.x) acc[1] += ea[k];
-  for (int k = t0 + threadIdx.x; k < t1; k += blockDim.x) acc[2] += ed[k];
-  for (int k = i0 + threadIdx.x; k < i1; k += blockDim.x) acc[2] += ed[k];
-  for (int c = 0; c < 4; c++) sh[c][threadIdx.x] = acc[c];
-  __syncthreads();
-  for (int w = 128; w > 0; w >>= 1) {
-    if (threadIdx.x < w)
-      for (int c = 0; c < 4; c++) sh[c][threadIdx.x] += sh[c][threadIdx.x + w];
-    __syncthreads();
+  t -= b.nb;
+  if (t < b.na) {
+    angle_term(v, t, b.e_angle);
+    return;
   }
-  if (threadIdx.x == 0) {
-    double *E = v.ene + (size_t)s * E_COUNT;
-    E[E_BOND] += sh[0][0];
-    E[E_ANGLE] += sh[1][0];
-    E[E_TORSION] += sh[2][0];
-    E[E_VIRIAL] += sh[3][0];
-    E[E_EPOT] += sh[0][0] + sh[1][0] + sh[2][0];
-  }
+  t -= b.na;
+  if (t < b.nt + b.ni) dihedral_term(v, t, b.e_dih);
 }
 
-void launch_bonded_terms(const PackView &v, cudaStream_t st, double *scratch, const int *off) {
-  const BondedTerms &bt = v.bt;
-  double *eb = scratch, *vb = eb + bt.nb, *ea = vb + bt.nb, *ed = ea + bt.na;
-  if (bt.nb) PDGPU_LAUNCH(k_bonds, (bt.nb + 255) / 256, 256, 0, st, v, eb, vb);
-  if (bt.na) PDGPU_LAUNCH(k_angles, (bt.na + 255) / 256, 256, 0, st, v, ea);
-  if (bt.nt + bt.ni) PDGPU_LAUNCH(k_dihedrals, (bt.nt + bt.ni + 255) / 256, 256, 0, st, v, ed);
-  if (v.n_sys) PDGPU_LAUNCH(k_reduce_bonded, v.n_sys, 256, 0, st, v, eb, vb, ea, ed, off);
+void launch_bonded_terms(const PackView &v, cudaStream_t st) {
+  const BondedTerms &b = v.bt;
+  int n = b.nb + b.na + b.nt + b.ni;
+  if (n) PDGPU_LAUNCH(k_bonded_all, (n + 127) / 128, 128, 0, st, v);
 }
 
 }  // namespace pdgpu

@@ -1,0 +1,158 @@
+// Energy record (Hamiltonian, workspace/hamiltonian.h:23-49) from the
+// per-atom and per-term energies the force kernels write.
+//
+// Two stages, both in a fixed order so every total is bit-reproducible:
+//   k_energy_partial  grid (chunks, systems): each block sums one 1024-item
+//                     chunk of each range of one system (per-atom terms and
+//                     the bond / angle / dihedral term arrays)
+//   k_energy_final    one block per system: sums the chunk partials in
+//                     chunk order, applies them to the record with the
+//                     reference's semantics (the GB and stand-alone
+//                     LJ/Coulomb components assign epot_vdw / epot_elec,
+//                     everything else accumulates), and in a step loop
+//                     records the step's energies and advances the step.
+#include <cuda_runtime.h>
+
+#include "internal.cuh"
+
+namespace pdgpu {
+
+constexpr int kChunk = 1024;
+// partial slots
+enum { P_VDW = 0, P_ELEC, P_POL, P_SELF, P_NBVIR, P_KIN, P_BOND, P_BVIR, P_ANGLE, P_DIH, P_COUNT };
+
+__device__ __forceinline__ double block_sum(double x, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) sh[w] = x;
+  __syncthreads();
+  double r = 0;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) r += sh[k];
+  return r;  // valid in thread 0
+}
+
+__global__ void k_energy_partial(PackView v, int mode, int C) {
+  if (v.flags[F_NL_OVERFLOW]) return;
+  const int c = blockIdx.x, s = blockIdx.y, N = v.n_atoms;
+  __shared__ double sh[32];
+  double acc[P_COUNT];
+#pragma unroll
+  for (int k = 0; k < P_COUNT; k++) acc[k] = 0.0;
+  int a0 = v.atom_off[s] + c * kChunk, a1 = min(a0 + kChunk, v.atom_off[s + 1]);
+  bool atoms = mode & (EM_PAIR_GB | EM_PAIR_NB | EM_BORN_ENERGY | EM_KINETIC);
+  if (atoms)
+    for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
+      if (mode & (EM_PAIR_GB | EM_PAIR_NB)) {
+        acc[P_VDW] += v.e_atom[(size_t)AE_VDW * N + i];
+        acc[P_ELEC] += v.e_atom[(size_t)AE_ELEC * N + i];
+      }
+      if (mode & (EM_PAIR_GB | EM_BORN_ENERGY)) {
+        acc[P_POL] += v.e_atom[(size_t)AE_POL * N + i];
+        acc[P_SELF] += v.e_atom[(size_t)AE_POL_SELF * N + i];
+      }
+      if (mode & EM_PAIR_NB) acc[P_NBVIR] += v.e_atom[(size_t)AE_VIR * N + i];
+      if (mode & EM_KINETIC) acc[P_KIN] += v.e_atom[(size_t)AE_KIN * N + i];
+    }
+  if (mode & EM_BONDED) {
+    const int S1 = v.n_sys + 1;
+    const int *off = v.bt.term_off;
+    int b0 = off[s] + c * kChunk, b1 = min(b0 + kChunk, off[s + 1]);
+    for (int t = b0 + threadIdx.x; t < b1; t += blockDim.x) {
+      acc[P_BOND] += v.bt.e_bond[t];
+      acc[P_BVIR] += v.bt.vir_bond[t];
+    }
+    int g0 = off[S1 + s] + c * kChunk, g1 = min(g0 + kChunk, off[S1 + s + 1]);
+    for (int t = g0 + threadIdx.x; t < g1; t += blockDim.x) acc[P_ANGLE] += v.bt.e_angle[t];
+    // torsions and impropers share the dihedral array: two ranges
+    for (int r = 2; r < 4; r++) {
+      int d0 = off[r * S1 + s] + c * kChunk, d1 = min(d0 + kChunk, off[r * S1 + s + 1]);
+      for (int t = d0 + threadIdx.x; t < d1; t += blockDim.x) acc[P_DIH] += v.bt.e_dih[t];
+    }
+  }
+  double *out = v.e_part + ((size_t)s * C + c) * P_COUNT;
+#pragma unroll
+  for (int k = 0; k < P_COUNT; k++) {
+    double t = block_sum(acc[k], sh);
+    if (threadIdx.x == 0) out[k] = t;
+  }
+}
+
+// hist: [step][sys][3] (epot, ekin, etot); step_dev[0] current step,
+// step_dev[1] first step of the run, step_dev[2] finished-block counter.
+__global__ void k_energy_final(PackView v, int mode, int C, double J2kcalmol, double *hist, int *step_dev) {
+  if (v.flags[F_NL_OVERFLOW]) return;
+  const int s = blockIdx.x;
+  __shared__ double tot[P_COUNT];
+  if (threadIdx.x < P_COUNT) {
+    double t = 0;
+    const double *p = v.e_part + (size_t)s * C * P_COUNT + threadIdx.x;
+    for (int c = 0; c < C; c++) t += p[(size_t)c * P_COUNT];
+    tot[threadIdx.x] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double *E = v.ene + (size_t)s * E_COUNT;
+    if (mode & (EM_PAIR_GB | EM_PAIR_NB)) {
+      E[E_VDW] = tot[P_VDW];
+      E[E_ELEC] = tot[P_ELEC];
+      E[E_EPOT] += tot[P_VDW] + tot[P_ELEC];
+    }
+    if (mode & EM_PAIR_GB) {
+      E[E_POL] += tot[P_POL] + tot[P_SELF];
+      E[E_POL_CROSS] += tot[P_POL];
+      E[E_POL_SELF] += tot[P_SELF];
+      E[E_EPOT] += tot[P_POL] + tot[P_SELF];
+    }
+    if (mode & EM_PAIR_NB) E[E_VIRIAL] += tot[P_NBVIR];
+    if (mode & EM_BORN_ENERGY) {
+      // the energy-only path adds the Born energy to epot alone
+      // (gbff.cpp:574-578); the component's own totals go to extra slots
+      E[E_EPOT] += tot[P_POL] + tot[P_SELF];
+      E[E_GB_COMPONENT] = tot[P_POL] + tot[P_SELF];
+      E[E_GB_COMPONENT + 1] = tot[P_POL];
+      E[E_GB_COMPONENT + 2] = tot[P_SELF];
+    }
+    if (mode & EM_BONDED) {
+      E[E_BOND] += tot[P_BOND];
+      E[E_ANGLE] += tot[P_ANGLE];
+      E[E_TORSION] += tot[P_DIH];
+      E[E_VIRIAL] += tot[P_BVIR];
+      E[E_EPOT] += tot[P_BOND] + tot[P_ANGLE] + tot[P_DIH];
+    }
+    if (mode & EM_KINETIC) {
+      E[E_EKIN] = tot[P_KIN] * J2kcalmol;
+      E[E_ETOT] = E[E_EPOT] + E[E_EKIN];
+    }
+    if (!(E[E_EPOT] == E[E_EPOT])) atomicExch(&v.flags[F_NAN], 1);
+    if (mode & EM_RECORD) {
+      int k = step_dev[0] - step_dev[1];
+      double *h = hist + ((size_t)k * v.n_sys + s) * 3;
+      h[0] = E[E_EPOT];
+      h[1] = E[E_EKIN];
+      h[2] = E[E_ETOT];
+      // the last system to finish advances the step (every block has read
+      // step_dev[0] before it counts itself finished)
+      __threadfence();
+      int done = atomicAdd(&step_dev[2], 1);
+      if (done == v.n_sys - 1) {
+        step_dev[2] = 0;
+        __threadfence();
+        atomicAdd(&step_dev[0], 1);
+      }
+    }
+  }
+}
+
+int energy_chunks(const PackView &v) { return v.e_chunks; }
+
+void launch_energy(const PackView &v, cudaStream_t st, int mode, double *hist, int *step_dev) {
+  if (!v.n_sys) return;
+  const Consts &k = consts();
+  int C = v.e_chunks;
+  PDGPU_LAUNCH(k_energy_partial, dim3(C, v.n_sys), 256, 0, st, v, mode, C);
+  PDGPU_LAUNCH(k_energy_final, v.n_sys, 32, 0, st, v, mode, C, k.J2kcal * k.Na, hist, step_dev);
+}
+
+}  // namespace pdgpu

@@ -217,52 +217,12 @@ __global__ void k_md_step(PackView v, MDDev d, const double *normals, const int 
   v.e_atom[(size_t)AE_KIN * v.n_atoms + i] = ke;  // J
 }
 
-__global__ void k_step_inc(int *step_dev, const int *flags) {
-  if (!flags[F_NL_OVERFLOW]) (*step_dev)++;
-}
-
-// KE per system (J -> stored in kcal/mol) and etot = epot + ekin.
-__global__ void k_reduce_ke(PackView v, double J2kcalmol, int from_velocities) {
-  if (v.flags[F_NL_OVERFLOW]) return;
-  int s = blockIdx.x;
-  int a0 = v.atom_off[s], a1 = v.atom_off[s + 1];
-  __shared__ double sh[256];
-  double acc = 0;
-  for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
-    if (from_velocities) {
-      double vx = v.vx[i], vy = v.vy[i], vz = v.vz[i];
-      acc += 0.5 * v.mass_si[i] * (vx * vx + vy * vy + vz * vz);
-    } else {
-      acc += v.e_atom[(size_t)AE_KIN * v.n_atoms + i];
-    }
-  }
-  sh[threadIdx.x] = acc;
-  __syncthreads();
-  for (int w = 128; w > 0; w >>= 1) {
-    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    double *E = v.ene + (size_t)s * E_COUNT;
-    E[E_EKIN] = sh[0] * J2kcalmol;
-    E[E_ETOT] = E[E_EPOT] + E[E_EKIN];
-  }
-}
-
-// history[step][sys][3] = epot, ekin, etot (kcal/mol)
-// step_dev[0] = current step, step_dev[1] = first step of the run
-__global__ void k_record(PackView v, double *hist, const int *step_dev) {
-  const int step0 = step_dev[1];
-  if (v.flags[F_NL_OVERFLOW]) return;
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= v.n_sys) return;
-  int k = *step_dev - step0;
-  const double *E = v.ene + (size_t)s * E_COUNT;
-  double *h = hist + ((size_t)k * v.n_sys + s) * 3;
-  h[0] = E[E_EPOT];
-  h[1] = E[E_EKIN];
-  h[2] = E[E_ETOT];
-  if (!(E[E_EPOT] == E[E_EPOT])) atomicExch(&v.flags[F_NAN], 1);
+// per-atom kinetic energy from the current velocities (J)
+__global__ void k_kinetic_atoms(PackView v) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v.n_atoms) return;
+  double vx = v.vx[i], vy = v.vy[i], vz = v.vz[i];
+  v.e_atom[(size_t)AE_KIN * v.n_atoms + i] = 0.5 * v.mass_si[i] * (vx * vx + vy * vy + vz * vz);
 }
 
 // setInitialSpeeds: Boltzmann draw (two nrand pairs, the second overwriting
@@ -301,11 +261,13 @@ struct MinState {
   int taken, nan;
 };
 
-// CG dot products per system: fmagold = sum of.of, fmagnew = sum (of-f).f
-__global__ void k_min_dots(PackView v, MinState *ms, double N_per_unit) {
+// CG dot products, stage 1: per (chunk, system) partials of
+// fmagold = sum of.of and fmagnew = sum (of-f).f into e_part slots 0 and 1;
+// k_min_control adds the chunk partials in chunk order.
+__global__ void k_min_dots(PackView v, double N_per_unit, int C) {
   if (v.flags[F_NL_OVERFLOW]) return;
-  int s = blockIdx.x;
-  int a0 = v.atom_off[s], a1 = v.atom_off[s + 1];
+  const int c = blockIdx.x, s = blockIdx.y;
+  int a0 = v.atom_off[s] + c * 1024, a1 = min(a0 + 1024, v.atom_off[s + 1]);
   __shared__ double sa[256], sb[256];
   double A = 0, B = 0;
   for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
@@ -326,8 +288,9 @@ __global__ void k_min_dots(PackView v, MinState *ms, double N_per_unit) {
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    ms[s].fmagold = sa[0];
-    ms[s].fmagnew = sb[0];
+    double *o = v.e_part + ((size_t)s * C + c) * 10;
+    o[0] = sa[0];
+    o[1] = sb[0];
   }
 }
 
@@ -335,10 +298,20 @@ __global__ void k_min_dots(PackView v, MinState *ms, double N_per_unit) {
 // Energies here are kcal/mol; one joule per molecule (the reference's
 // "m_OldEnergy += 1" after a rejected SD step) is J_unit kcal/mol.
 __global__ void k_min_control(PackView v, MinState *ms, int algorithm, double slope_cutoff_kcal,
-                              double strictness_kcal, double J_unit, int nsteps) {
+                              double strictness_kcal, double J_unit, int nsteps, int C) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= v.n_sys) return;
   MinState &m = ms[s];
+  if (algorithm == PDGPU_MIN_CONJUGATE_GRADIENTS && !v.flags[F_NL_OVERFLOW]) {
+    double A = 0, B = 0;
+    for (int c = 0; c < C; c++) {
+      const double *o = v.e_part + ((size_t)s * C + c) * 10;
+      A += o[0];
+      B += o[1];
+    }
+    m.fmagold = A;
+    m.fmagnew = B;
+  }
   if (v.flags[F_NL_OVERFLOW]) {  // no valid forces this step: do nothing, retry
     m.action = -1;
     return;
@@ -478,22 +451,16 @@ void launch_md_step_impl(const PackView &v, cudaStream_t st, const MDCoef &c, co
   d.is_h = is_h;
   d.sys_seed = seeds;
   if (v.n_atoms) PDGPU_LAUNCH(k_md_step, (v.n_atoms + 255) / 256, 256, 0, st, v, d, normals, step_dev);
-  if (v.n_sys) PDGPU_LAUNCH(k_reduce_ke, v.n_sys, 256, 0, st, v, k.J2kcal * k.Na, 0);
-}
-void launch_step_inc(const PackView &v, int *step_dev, cudaStream_t st) {
-  PDGPU_LAUNCH(k_step_inc, 1, 1, 0, st, step_dev, v.flags);
 }
 
 long long &launch_counter() {
   static long long n = 0;
   return n;
 }
-void launch_record(const PackView &v, cudaStream_t st, double *hist, const int *step_dev) {
-  if (v.n_sys) PDGPU_LAUNCH(k_record, (v.n_sys + 127) / 128, 128, 0, st, v, hist, step_dev);
-}
 void launch_ke_from_velocities(const PackView &v, cudaStream_t st) {
-  const Consts &k = consts();
-  if (v.n_sys) PDGPU_LAUNCH(k_reduce_ke, v.n_sys, 256, 0, st, v, k.J2kcal * k.Na, 1);
+  if (!v.n_atoms) return;
+  PDGPU_LAUNCH(k_kinetic_atoms, (v.n_atoms + 255) / 256, 256, 0, st, v);
+  launch_energy(v, st, EM_KINETIC);
 }
 void launch_vel_init_impl(const PackView &v, cudaStream_t st, double temp, const unsigned long long *seeds) {
   const Consts &k = consts();
@@ -507,9 +474,11 @@ void launch_min_step(const PackView &v, cudaStream_t st, void *ms, int algorithm
                      double strict_kcal, double step_size, int nsteps) {
   const Consts &k = consts();
   MinState *m = (MinState *)ms;
-  if (algorithm == PDGPU_MIN_CONJUGATE_GRADIENTS) PDGPU_LAUNCH(k_min_dots, v.n_sys, 256, 0, st, v, m, k.N_per_kcalmolA);
+  int C = v.e_chunks;
+  if (algorithm == PDGPU_MIN_CONJUGATE_GRADIENTS)
+    PDGPU_LAUNCH(k_min_dots, dim3(C, v.n_sys), 256, 0, st, v, k.N_per_kcalmolA, C);
   PDGPU_LAUNCH(k_min_control, (v.n_sys + 127) / 128, 128, 0, st, v, m, algorithm, slope_kcal, strict_kcal,
-                                                       k.J2kcal * k.Na, nsteps);
+               k.J2kcal * k.Na, nsteps, C);
   PDGPU_LAUNCH(k_min_update, (v.n_atoms + 255) / 256, 256, 0, st, v, m, k.N_per_kcalmolA, step_size);
 }
 void launch_min_finish(const PackView &v, cudaStream_t st) {

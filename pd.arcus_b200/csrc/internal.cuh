@@ -74,8 +74,20 @@ enum EneSlot {
 // system in a fixed order so every sum is bit-reproducible.
 enum AtomEne { AE_VDW = 0, AE_ELEC, AE_POL, AE_POL_SELF, AE_VIR, AE_KIN, AE_COUNT };
 
+// What one energy reduction applies to the record (launch_energy).
+enum EnergyMode {
+  EM_PAIR_GB = 1,      // fused GB + LJ + Coulomb: vdw, elec, pol, pol_cross, pol_self
+  EM_PAIR_NB = 2,      // stand-alone LJ / Coulomb: vdw, elec, virial
+  EM_BORN_ENERGY = 4,  // energy-only Born term
+  EM_BONDED = 8,       // bond, angle, torsion, bond virial
+  EM_KINETIC = 16,     // ekin, etot
+  EM_RECORD = 32       // history row + step counter advance (step loops)
+};
+
 struct BondedTerms {
   int nb = 0, na = 0, nt = 0, ni = 0;
+  const int *term_off = nullptr;  // [4*(S+1)]: bond, angle, torsion, improper ranges per system
+  double *e_bond = nullptr, *vir_bond = nullptr, *e_angle = nullptr, *e_dih = nullptr;
   int2 *bij = nullptr;        // bond atoms (global)
   double2 *blk = nullptr;     // (l, k kcal/mol/A^2)
   int4 *aiaj = nullptr;       // (i, a, j, -)
@@ -113,6 +125,8 @@ struct PackView {
   double *odx, *ody, *odz;
   double *e_atom;             // [AE_COUNT * N]
   double *ene;                // [S * E_COUNT] J-free kcal/mol accumulators
+  double *e_part;             // [S * e_chunks * 10] reduction partials
+  int e_chunks;               // 1024-item chunks of the largest per-system range
   // bond order
   const int *mid;             // [S]
   const long long *band_off;  // [S]
@@ -196,15 +210,18 @@ void launch_zero(const PackView &v, cudaStream_t st);
 // neighbour list: build phases.  count -> (host may read total) -> fill
 void launch_nlist_count(Pack &p, cudaStream_t st);
 void launch_nlist_fill(Pack &p, cudaStream_t st);
-// GB
-void launch_born_radii(const PackView &v, cudaStream_t st);
+// GB (zero_first: also zero the forces and the potential-energy record,
+// WorkSpace::zeroForces, so the step needs no separate zeroing launch)
+void launch_born_radii(const PackView &v, cudaStream_t st, bool zero_first = false);
 void launch_gb_pair(const PackView &v, cudaStream_t st);
 void launch_gb_chain(const PackView &v, cudaStream_t st);
 void launch_born_energy(const PackView &v, cudaStream_t st);
 void launch_nonbonded(const PackView &v, cudaStream_t st, int elec_mode);
-void launch_bonded(const PackView &v, cudaStream_t st);
-// energies: reduce per-atom terms into the per-system record (adds)
-void launch_reduce_gb_energies(const PackView &v, cudaStream_t st, int mode);
+void launch_bonded_terms(const PackView &v, cudaStream_t st);
+// energies: per-atom / per-term energies into the per-system record
+// (mode = EnergyMode bits); hist/step_dev only with EM_RECORD
+void launch_energy(const PackView &v, cudaStream_t st, int mode, double *hist = nullptr,
+                   int *step_dev = nullptr);
 // integrators / minimiser
 struct MDCoef {
   double dt, gamma, c0, c1, c2, varv, varr, crv, temp;

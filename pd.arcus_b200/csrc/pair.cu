@@ -109,12 +109,21 @@ void launch_zero(const PackView &v, cudaStream_t st) {
 }
 
 // --------------------------------------------------------------- K2 radii
-__global__ void __launch_bounds__(256) k_born(PackView v) {
+__global__ void __launch_bounds__(256) k_born(PackView v, int zero_first) {
   if (v.flags[F_NL_OVERFLOW]) return;  // list incomplete: the host re-plans
   int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (i >= v.n_atoms) return;
-  const SysParams &P = v.sp[v.sys_of[i]];
+  const int s = v.sys_of[i];
+  const SysParams &P = v.sp[s];
+  if (zero_first && lane < 3) {
+    // WorkSpace::zeroForces for this atom (and the record, by the first atom)
+    long long *f = lane == 0 ? v.fx : (lane == 1 ? v.fy : v.fz);
+    f[i] = 0;
+    if (i == v.atom_off[s])
+      for (int k = lane; k < E_COUNT; k += 3)
+        if (k != E_EKIN) v.ene[(size_t)s * E_COUNT + k] = 0.0;
+  }
   const double xi = v.x[i], yi = v.y[i], zi = v.z[i];
   const double Ri = v.gbR_d[i];
   const double still2 = P.still2_d;
@@ -149,19 +158,23 @@ __global__ void __launch_bounds__(256) k_born(PackView v) {
   }
 }
 
-void launch_born_radii(const PackView &v, cudaStream_t st) {
-  if (v.n_atoms) PDGPU_LAUNCH(k_born, (v.n_atoms + 7) / 8, 256, 0, st, v);
+void launch_born_radii(const PackView &v, cudaStream_t st, bool zero_first) {
+  if (v.n_atoms) PDGPU_LAUNCH(k_born, (v.n_atoms + 7) / 8, 256, 0, st, v, (int)zero_first);
 }
 
 // --------------------------------------------------------------- K3 pair
 // Exact FP64 re-evaluation of the reference's GB branch predicate
 // uGB = -srij*0.25/aiaj > ExpApproxThreshold, with srij formed as in
 // gbff.cpp:1553-1556 (dddx = p_i - p_j; sqr+sqr+sqr).
-__device__ __noinline__ bool gb_branch_exact(const PackView &v, const SysParams &P, int i, int j) {
-  double srij = ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]);
-  double aiaj = v.born_d[i] * v.born_d[j];
+// (Plain pointer arguments: taking the address of the kernel's PackView
+// parameter would copy it to local memory in every thread.)
+__device__ __noinline__ bool gb_branch_exact(const double *__restrict__ x, const double *__restrict__ y,
+                                             const double *__restrict__ z, const double *__restrict__ born,
+                                             int i, int j, double thr) {
+  double srij = ref_d2(x[i], y[i], z[i], x[j], y[j], z[j]);
+  double aiaj = born[i] * born[j];
   double uGB = -srij * 0.25 / aiaj;
-  return uGB > P.exp_thresh_d;
+  return uGB > thr;
 }
 
 __global__ void __launch_bounds__(256) k_gb_pair(PackView v) {
@@ -197,7 +210,7 @@ __global__ void __launch_bounds__(256) k_gb_pair(PackView v) {
     float aiaj = ai * aj;
     float u = -0.25f * r2 * (inv_ai * jbf.y);
     bool gb = u > thr;
-    if (fabsf(u - thr) <= band) gb = gb_branch_exact(v, P, i, j);
+    if (fabsf(u - thr) <= band) gb = gb_branch_exact(v.x, v.y, v.z, v.born_d, i, j, P.exp_thresh_d);
     float p14 = (bo == 3) ? P.elec14 : 1.0f;
     float S = 1.f, dSdd = 0.f;
     if (r >= P.rin) {
@@ -570,62 +583,6 @@ __global__ void k_pair_counts(PackView v, unsigned long long *out) {
 
 void launch_pair_counts(const PackView &v, cudaStream_t st, unsigned long long *out) {
   if (v.n_atoms) PDGPU_LAUNCH(k_pair_counts, (v.n_atoms + 7) / 8, 256, 0, st, v, out);
-}
-
-// --------------------------------------------------------------- reductions
-// One block per system; fixed-order tree in double.  mode selects which
-// per-atom terms feed which slots:
-//   0 GB forces path: VDW=, ELEC=, POL/POL_CROSS/POL_SELF +=, EPOT += all
-//   1 stand-alone LJ/Coulomb: VDW=, ELEC=, VIRIAL +=, EPOT += vdw+elec
-//   2 Born energy (energy path): EPOT += pol, GB_COMPONENT = pol
-__global__ void k_reduce_atoms(PackView v, int mode) {
-  if (v.flags[F_NL_OVERFLOW]) return;
-  int s = blockIdx.x;
-  int a0 = v.atom_off[s], a1 = v.atom_off[s + 1];
-  const int N = v.n_atoms;
-  __shared__ double sh[AE_COUNT][256];
-  double acc[AE_COUNT];
-#pragma unroll
-  for (int k = 0; k < AE_COUNT; k++) acc[k] = 0.0;
-  for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x)
-#pragma unroll
-    for (int k = 0; k < AE_COUNT; k++) acc[k] += v.e_atom[(size_t)k * N + i];
-#pragma unroll
-  for (int k = 0; k < AE_COUNT; k++) sh[k][threadIdx.x] = acc[k];
-  __syncthreads();
-  for (int w = 128; w > 0; w >>= 1) {
-    if (threadIdx.x < w)
-#pragma unroll
-      for (int k = 0; k < AE_COUNT; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    double *E = v.ene + (size_t)s * E_COUNT;
-    double vdw = sh[AE_VDW][0], el = sh[AE_ELEC][0], pol = sh[AE_POL][0], self = sh[AE_POL_SELF][0];
-    if (mode == 0) {
-      E[E_VDW] = vdw;
-      E[E_ELEC] = el;
-      E[E_POL] += pol + self;
-      E[E_POL_CROSS] += pol;
-      E[E_POL_SELF] += self;
-      E[E_EPOT] += vdw + el + pol + self;
-    } else if (mode == 1) {
-      E[E_VDW] = vdw;
-      E[E_ELEC] = el;
-      E[E_VIRIAL] += sh[AE_VIR][0];
-      E[E_EPOT] += vdw + el;
-    } else {
-      E[E_EPOT] += pol + self;
-      E[E_GB_COMPONENT] = pol + self;
-      E[E_GB_COMPONENT + 1] = pol;
-      E[E_GB_COMPONENT + 2] = self;
-    }
-    if (!(E[E_EPOT] == E[E_EPOT])) atomicExch(&v.flags[F_NAN], 1);
-  }
-}
-
-void launch_reduce_gb_energies(const PackView &v, cudaStream_t st, int mode) {
-  if (v.n_sys) PDGPU_LAUNCH(k_reduce_atoms, v.n_sys, 256, 0, st, v, mode);
 }
 
 }  // namespace pdgpu

@@ -447,6 +447,31 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   for (auto *s : systems) nt_all += s->nt;
   bt.nt = nt_all;
   bt.ni = ndih - nt_all;
+  // per-system term ranges: bonds, angles, torsions, impropers (the last two
+  // index the shared dihedral array: all torsions first, then impropers)
+  std::vector<int> toff(4 * (S + 1), 0);
+  int max_range = 0;
+  for (int s = 0; s < S; s++) {
+    const SystemHost &h = *systems[s];
+    toff[s + 1] = toff[s] + h.nb;
+    toff[(S + 1) + s + 1] = toff[(S + 1) + s] + h.na;
+    toff[2 * (S + 1) + s + 1] = toff[2 * (S + 1) + s] + h.nt;
+    max_range = std::max(max_range, std::max(std::max(h.nb, h.na), std::max(h.nt, h.ni)));
+    max_range = std::max(max_range, h.natoms);
+  }
+  toff[3 * (S + 1)] = nt_all;
+  for (int s = 0; s < S; s++) toff[3 * (S + 1) + s + 1] = toff[3 * (S + 1) + s] + systems[s]->ni;
+  int *toff_d;
+  PALLOC(toff_d, toff.size());
+  cudaMemcpyAsync(toff_d, toff.data(), sizeof(int) * toff.size(), cudaMemcpyHostToDevice, st);
+  bt.term_off = toff_d;
+  PALLOC(bt.e_bond, bt.nb);
+  PALLOC(bt.vir_bond, bt.nb);
+  PALLOC(bt.e_angle, bt.na);
+  PALLOC(bt.e_dih, ndih);
+  v.e_chunks = (max_range + 1023) / 1024;
+  if (v.e_chunks < 1) v.e_chunks = 1;
+  PALLOC(v.e_part, (size_t)S * v.e_chunks * 10);
   PALLOC(bt.bij, bij.size());
   PALLOC(bt.blk, blk.size());
   PALLOC(bt.aiaj, aiaj.size());
