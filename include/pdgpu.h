@@ -155,6 +155,37 @@ int pdgpu_nlist_build(pdgpu_ctx *ctx, int32_t sys);
 int pdgpu_nlist_export(pdgpu_ctx *ctx, int32_t sys, int32_t shadow, int32_t *ptr,
                        int32_t *data, int64_t cap, int64_t *count);
 
+/* Neighbour-list build that allocates no device memory.  No counterpart in
+ * the reference: it exists for callers that cannot call cudaMalloc -- code
+ * running while a stream is captured into a CUDA graph, or a host framework
+ * that hands out all device memory from its own pool and forbids
+ * allocation after start-up.  Same pair set and bond orders as
+ * pdgpu_nlist_build, for one system given in device memory:
+ *   x, y, z        positions (Angstrom), natoms each (SoA)
+ *   list_cutoff    max(Cutoff, VdwCutoff) + Padding
+ *   max_index_delta, band   BondOrder band width and band (int8,
+ *                  max_index_delta * (natoms-1)), as BondOrder::getDiagData
+ *   offdiag_ptr, offdiag_pairs  optional off-band partners: CSR over atoms
+ *                  (natoms+1) of (partner, order) int pairs, both directions;
+ *                  both NULL when there are none
+ *   row_start      out: natoms+1 int64 row offsets
+ *   entries        out: capacity uint32, the reference's packed entries
+ *                  (j | bondorder<<24), rows in cell-scan order
+ *   count          out (host): entries needed; PDGPU_ERR_ARG if > capacity
+ *   stream         cudaStream_t to run on (NULL: the default stream)
+ * All scratch lives in one static device array sized for 65,536 atoms
+ * (about 2.9 MB, held on every GPU that loads the library until exit);
+ * larger systems are refused with PDGPU_ERR_ARG.  Calls share that array:
+ * calls that overlap on the GPU race and must be serialised by the caller.
+ * The first call on each device looks up the array's device address; make
+ * that first call outside any stream capture.  The call synchronises
+ * `stream` once to read the entry count. */
+int pdgpu_nlist_build_noalloc(const double *x, const double *y, const double *z, int32_t natoms,
+                              double list_cutoff, int32_t max_index_delta, const int8_t *band,
+                              const int32_t *offdiag_ptr, const int32_t *offdiag_pairs,
+                              int64_t *row_start, uint32_t *entries, int64_t capacity,
+                              int64_t *count, void *stream);
+
 /* FF_GeneralizedBorn_Still::calcForces (gbff.cpp:168-180) in FastMode:
  * Born radii (:415-466), then the fused GB + LJ + Coulomb pass (:1529-1736)
  * and the Born-radius chain-rule pass (:1751-1818).  Adds forces; sets the
