@@ -218,6 +218,8 @@ def main():
     # roofline inputs: pair counts and per-kernel device times (CUDA events)
     counts = np.zeros(3, dtype=np.int64)
     A.check(A.lib().pdgpu_pair_counts(ctx.ptr, ws._sys, counts.ctypes.data_as(A._I64)))
+    lpa = np.zeros(3, dtype=np.int32)
+    A.check(A.lib().pdgpu_autotune(ctx.ptr, ws._sys, A.iptr(lpa)))
     kms = np.zeros(3)
     A.check(A.lib().pdgpu_profile_pair_kernels(ctx.ptr, ws._sys, 20, A.dptr(kms)))
 
@@ -336,6 +338,7 @@ def main():
                 sms, "256 flop" if bound == "fp32" else "16 MUFU", f_max / 1e6),
             "pairs": {"P_B": P_B, "P_H": P_H, "list_entries": entries},
             "kernel_ms": {"born_K2": t2 * 1e3, "pair_K3": t3 * 1e3, "chain_K4": t4 * 1e3},
+            "lanes_per_atom": {"born_K2": int(lpa[0]), "pair_K3": int(lpa[1]), "chain_K4": int(lpa[2])},
             "pair_kernels_frac_of_roof": t_roof / t_pair}
 
     line = {"metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": n_gpus, "steps": args.steps,

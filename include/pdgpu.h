@@ -280,6 +280,11 @@ int pdgpu_profile_pair_kernels(pdgpu_ctx *ctx, int32_t sys, int32_t reps, double
 /* Kernels this context has launched (graph replays count their kernel
  * nodes). */
 int pdgpu_launch_count(pdgpu_ctx *ctx, int64_t *count);
+/* Autotuner (no reference counterpart): re-time the lanes-per-atom choice
+ * (4, 8, 16 or 32 lanes walk one atom's neighbour row) of the Born-radius,
+ * fused pair and chain-rule kernels on the current list; lpa[0..2] receive
+ * the picks.  The first force evaluation of a system tunes automatically. */
+int pdgpu_autotune(pdgpu_ctx *ctx, int32_t sys, int32_t *lpa);
 
 #ifdef __cplusplus
 }

@@ -683,6 +683,73 @@ static int need_list(Pack &P) {
   return PDGPU_OK;
 }
 
+// Autotuner: lanes per atom (4, 8, 16, 32) of the Born, fused-pair and
+// chain-rule kernels, chosen once per pack by timing each candidate on the
+// current list with CUDA events.  The timed launches write their forces and
+// energies into scratch buffers; the Born radii and chain weights they also
+// write are the values the next evaluation computes anyway.
+static int ensure_tuned(pdgpu_ctx *c, Pack &P) {
+  if (P.tuned || P.v.n_atoms == 0 || !P.have_list) return PDGPU_OK;
+  const int N = P.v.n_atoms;
+  PackView t = P.v;
+  long long *f = nullptr;
+  double *ea = nullptr, *en = nullptr;
+  PDGPU_CUDA(cudaMalloc(&f, sizeof(long long) * 3 * (size_t)N));
+  if (cudaMalloc(&ea, sizeof(double) * AE_COUNT * (size_t)N) != cudaSuccess ||
+      cudaMalloc(&en, sizeof(double) * E_COUNT * (size_t)P.v.n_sys) != cudaSuccess) {
+    cudaFree(f);
+    cudaFree(ea);
+    set_error("autotune scratch allocation failed");
+    return PDGPU_ERR_NOMEM;
+  }
+  t.fx = f;
+  t.fy = f + N;
+  t.fz = f + 2 * N;
+  t.e_atom = ea;
+  t.ene = en;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  static const int cand[4] = {4, 8, 16, 32};
+  int r = PDGPU_OK;
+  for (int kern = 0; kern < 3 && r == PDGPU_OK; kern++) {
+    float best = 1e30f;
+    int pick = 8;
+    for (int q = 0; q < 4; q++) {
+      float tot = 0;
+      for (int rep = 0; rep < 4; rep++) {
+        cudaEventRecord(a, c->st);
+        if (kern == 0) launch_born_radii_lpa(t, c->st, false, cand[q]);
+        if (kern == 1) launch_gb_pair_lpa(t, c->st, cand[q]);
+        if (kern == 2) launch_gb_chain_lpa(t, c->st, cand[q]);
+        cudaEventRecord(b, c->st);
+        r = sync_check(c, "autotune");
+        if (r) break;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        if (rep > 0) tot += ms;  // the first launch warms the caches
+      }
+      if (r) break;
+      if (tot < best) {
+        best = tot;
+        pick = cand[q];
+      }
+    }
+    P.v.lpa[kern] = t.lpa[kern] = pick;
+    // leave valid inputs for the next kernel's timing
+    if (kern == 0) launch_born_radii_lpa(t, c->st, false, pick);
+    if (kern == 1) launch_gb_pair_lpa(t, c->st, pick);
+  }
+  if (r == PDGPU_OK) r = sync_check(c, "autotune");
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(f);
+  cudaFree(ea);
+  cudaFree(en);
+  if (r == PDGPU_OK) P.tuned = true;
+  return r;
+}
+
 // GB calcForces enqueue (no sync)
 static void gb_forces_enqueue(pdgpu_ctx *c, Pack &P) {
   launch_born_radii(P.v, c->st);
@@ -699,6 +766,7 @@ int pdgpu_gb_forces(pdgpu_ctx *c, int32_t sys) {
   Pack &P = *e->pack;
   int r = need_list(P);
   if (r) return r;
+  if ((r = ensure_tuned(c, P))) return r;
   if (!e->host.params.FastMode) {
     set_error("FastMode=false (separate FF_NonBonded + calcBornForces) is not built; use FastMode");
     return PDGPU_ERR_ARG;
@@ -769,6 +837,7 @@ int pdgpu_calc_forces(pdgpu_ctx *c, int32_t sys) {
   Pack &P = *e->pack;
   int r = need_list(P);
   if (r) return r;
+  if ((r = ensure_tuned(c, P))) return r;
   calc_forces_enqueue(c, e);
   return sync_check(c, "calc_forces");
 }
@@ -901,6 +970,7 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
     r = nlist_enqueue(c, e, true);
     if (r) return r;
   }
+  if ((r = ensure_tuned(c, P))) return r;
   // A block is one list period: [rebuild] + UpdateNList steps.  If the
   // in-block rebuild overflows the list buffer, every kernel after it skips
   // (device flag), the state stays at the block start, and the host grows
@@ -926,9 +996,9 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
       if (use_graph) {
         // graphs are cached per system; the key holds every value baked in
         char key[256];
-        snprintf(key, sizeof key, "%d|%p|%lld|%p|%d|%d|%.17g|%.17g|%.17g|%d|%d|%d", block, (void *)v.nl,
+        snprintf(key, sizeof key, "%d|%p|%lld|%p|%d|%d|%.17g|%.17g|%.17g|%d|%d|%d|%d%d%d", block, (void *)v.nl,
                  v.nl_cap, (void *)e->hist, k.integrator, k.steps, k.dt, k.gamma, k.temp, k.stochastic_h,
-                 P.radix_passes, (int)e->host.params.FastMode);
+                 P.radix_passes, (int)e->host.params.FastMode, v.lpa[0], v.lpa[1], v.lpa[2]);
         if (!e->gexec || e->gkey != key) {
           e->drop_graph();
           long long before = launch_counter();
@@ -1028,6 +1098,7 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
     r = nlist_enqueue(c, e, true);
     if (r) return r;
   }
+  if ((r = ensure_tuned(c, P))) return r;
   cudaEventRecord(P.ev0, c->st);
   // Chunks of up to 16 steps run without a host synchronisation.  A step
   // whose list rebuild overflowed does nothing on the device (flag); the
@@ -1117,6 +1188,7 @@ int pdgpu_profile_pair_kernels(pdgpu_ctx *c, int32_t sys, int32_t reps, double *
   Pack &P = *e->pack;
   int r = need_list(P);
   if (r) return r;
+  if ((r = ensure_tuned(c, P))) return r;
   if (!ms || reps <= 0) {
     set_error("ms is NULL or reps <= 0");
     return PDGPU_ERR_ARG;
@@ -1144,6 +1216,20 @@ int pdgpu_profile_pair_kernels(pdgpu_ctx *c, int32_t sys, int32_t reps, double *
   for (int q = 0; q < 4; q++) cudaEventDestroy(ev[q]);
   if (r) return r;
   for (int q = 0; q < 3; q++) ms[q] = acc[q] / reps;
+  return PDGPU_OK;
+}
+
+int pdgpu_autotune(pdgpu_ctx *c, int32_t sys, int32_t *lpa) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  int r = need_list(P);
+  if (r) return r;
+  P.tuned = false;
+  if ((r = ensure_tuned(c, P))) return r;
+  e->drop_graph();
+  if (lpa)
+    for (int q = 0; q < 3; q++) lpa[q] = P.v.lpa[q];
   return PDGPU_OK;
 }
 

@@ -77,13 +77,15 @@ __device__ __forceinline__ void store_pos(const PackView &v, int i, double x, do
   v.y[i] = y;
   v.z[i] = z;
   float hx = __double2float_rn(x), hy = __double2float_rn(y), hz = __double2float_rn(z);
-  float4 a = v.pa[i];
+  float4 a = v.pq[2 * (size_t)i];
   a.x = hx;
   a.y = hy;
   a.z = hz;
-  v.pa[i] = a;
-  v.pb[i] = make_float4(__double2float_rn(x - (double)hx), __double2float_rn(y - (double)hy),
-                        __double2float_rn(z - (double)hz), 0.f);
+  v.pq[2 * (size_t)i] = a;
+  // the Born radius slot (.w) is refreshed by the next Born-radius pass
+  v.pq[2 * (size_t)i + 1] = make_float4(__double2float_rn(x - (double)hx), __double2float_rn(y - (double)hy),
+                                        __double2float_rn(z - (double)hz), 0.f);
+  v.xyzp[i] = make_double4(x, y, z, v.pv_d[i]);
 }
 
 struct MDDev {

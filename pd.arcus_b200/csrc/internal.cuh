@@ -107,9 +107,10 @@ struct PackView {
   double *x, *y, *z;          // Angstrom
   double *vx, *vy, *vz;       // m/s
   double *ox, *oy, *oz;       // saved positions (minimiser / restore)
-  // pair-kernel copies
-  float4 *pa;                 // (x_hi, y_hi, z_hi, q)
-  float4 *pb;                 // (x_lo, y_lo, z_lo, 0)
+  // pair-kernel records: one 32-byte sector per atom per gather
+  float4 *pq;                 // [2N]: (x_hi, y_hi, z_hi, q), (x_lo, y_lo, z_lo, born radius)
+  double4 *xyzp;              // [N]: (x, y, z, P4*V_j) for the FP64 Born sums
+  float4 *chainp;             // [N]: (gb_R, V_j, gpi*deda, 0) for the chain-rule pass
   const float4 *prm;          // (lj_radius, sqrt_eps (kcal/mol)^1/2, gb_R, V_j)
   const double *gbR_d;        // gb_R (double)
   const double *pv_d;         // P4 * V_j (double)
@@ -117,8 +118,6 @@ struct PackView {
   const double *inv_mass_si;  // 1 / kg
   const double *mass_si;      // kg
   double *born_d;             // Born radii
-  float *born_f;
-  float *w_chain;             // gpi_i * deda_i (kcal/mol/A^2 scaled)
   long long *fx, *fy, *fz;    // fixed-point forces
   double *fox, *foy, *foz;    // saved forces (N) for Beeman / minimiser
   double *dirx, *diry, *dirz; // CG directions / old directions
@@ -127,6 +126,7 @@ struct PackView {
   double *ene;                // [S * E_COUNT] J-free kcal/mol accumulators
   double *e_part;             // [S * e_chunks * 10] reduction partials
   int e_chunks;               // 1024-item chunks of the largest per-system range
+  int lpa[3];                 // lanes per atom of the Born, fused-pair and chain kernels
   // bond order
   const int *mid;             // [S]
   const long long *band_off;  // [S]
@@ -188,6 +188,7 @@ struct Pack {
   double *red_tmp = nullptr;     // reductions
   // bookkeeping for protocols
   int nlist_counter = 0;
+  bool tuned = false;            // lanes-per-atom chosen by the autotuner
   double last_run_ms = 0.0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   ~Pack();
@@ -215,6 +216,10 @@ void launch_nlist_fill(Pack &p, cudaStream_t st);
 void launch_born_radii(const PackView &v, cudaStream_t st, bool zero_first = false);
 void launch_gb_pair(const PackView &v, cudaStream_t st);
 void launch_gb_chain(const PackView &v, cudaStream_t st);
+// explicit lanes-per-atom variants (4, 8, 16, 32), used by the autotuner
+void launch_born_radii_lpa(const PackView &v, cudaStream_t st, bool zero_first, int lpa);
+void launch_gb_pair_lpa(const PackView &v, cudaStream_t st, int lpa);
+void launch_gb_chain_lpa(const PackView &v, cudaStream_t st, int lpa);
 void launch_born_energy(const PackView &v, cudaStream_t st);
 void launch_nonbonded(const PackView &v, cudaStream_t st, int elec_mode);
 void launch_bonded_terms(const PackView &v, cudaStream_t st);

@@ -6,11 +6,16 @@
 //      k_born_energy calcBornEnergy                   (gbff.cpp:520-579)
 //      k_nonbonded   FF_NonBonded_CalcForces_T_fast2  (nonbonded.cpp:548-893)
 //
-// Layout: one warp per atom i walks i's full neighbour row (lanes stride the
-// row; rows are contiguous uint32 (j<<3|bondorder) entries).  Every atom
+// Layout: a group of LPA lanes (4, 8, 16 or 32; chosen per system by the
+// autotuner) walks atom i's full neighbour row, so one warp serves 32/LPA
+// atoms.  Rows are contiguous uint32 (j<<3|bondorder) entries.  Every atom
 // accumulates only its own force, so no atomics touch j; per-lane partials
-// are converted to 64-bit fixed point and summed with shuffles, so every
-// result is bit-reproducible run to run and independent of lane order.
+// are converted to 64-bit fixed point and summed with shuffles inside the
+// group, so every result is bit-reproducible run to run and independent of
+// lane order.  Each neighbour costs one 32-byte record gather per kernel plus
+// one 16-byte parameter gather.  The fused pass evaluates the GB and the
+// vacuum Coulomb terms without branches (both computed, one selected), so
+// the lanes of a group stay converged.
 //
 // Precision: pair arithmetic in FP32 on coordinates split as hi+lo floats
 // (dx = (xi_hi - xj_hi) + (xi_lo - xj_lo), i.e. the FP64 difference rounded
@@ -31,14 +36,10 @@
 
 namespace pdgpu {
 
-__device__ __forceinline__ long long warp_sum_ll(long long x) {
+template <int W, typename T>
+__device__ __forceinline__ T group_sum(T x) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-  return x;
-}
-__device__ __forceinline__ double warp_sum_d(double x) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  for (int o = W / 2; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
   return x;
 }
 __device__ __forceinline__ long long to_fixed_force(float f) {
@@ -66,20 +67,34 @@ __device__ __forceinline__ double ref_d2(double ax, double ay, double az, double
   return __dadd_rn(__dadd_rn(__dmul_rn(g, g), __dmul_rn(h, h)), __dmul_rn(k, k));
 }
 
+// hi + lo coordinate difference of records a (hi) / b (lo): p_i - p_j
+struct Dx {
+  float x, y, z, r2;
+};
+__device__ __forceinline__ Dx diff(const float4 &ia, const float4 &ib, const float4 &ja, const float4 &jb) {
+  Dx d;
+  d.x = (ia.x - ja.x) + (ib.x - jb.x);
+  d.y = (ia.y - ja.y) + (ib.y - jb.y);
+  d.z = (ia.z - ja.z) + (ib.z - jb.z);
+  d.r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+  return d;
+}
+
 // --------------------------------------------------------------- positions
-// FP64 state -> (hi, lo) float copies used by the pair kernels.
+// FP64 state -> the pair-kernel records (hi/lo floats, FP64 AoS copy).
 __global__ void k_pack_positions(PackView v) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= v.n_atoms) return;
   double x = v.x[i], y = v.y[i], z = v.z[i];
   float hx = __double2float_rn(x), hy = __double2float_rn(y), hz = __double2float_rn(z);
-  float4 a = v.pa[i];
+  float4 a = v.pq[2 * (size_t)i];
   a.x = hx;
   a.y = hy;
   a.z = hz;
-  v.pa[i] = a;
-  v.pb[i] = make_float4(__double2float_rn(x - (double)hx), __double2float_rn(y - (double)hy),
-                        __double2float_rn(z - (double)hz), 0.f);
+  v.pq[2 * (size_t)i] = a;
+  v.pq[2 * (size_t)i + 1] = make_float4(__double2float_rn(x - (double)hx), __double2float_rn(y - (double)hy),
+                                        __double2float_rn(z - (double)hz), 0.f);
+  v.xyzp[i] = make_double4(x, y, z, v.pv_d[i]);
 }
 
 void launch_pack_positions(const PackView &v, cudaStream_t st) {
@@ -108,58 +123,76 @@ void launch_zero(const PackView &v, cudaStream_t st) {
   if (n) PDGPU_LAUNCH(k_zero, (n + 255) / 256, 256, 0, st, v);
 }
 
+// grid of `lpa`-lane groups, 256-thread blocks
+static inline int pair_blocks(int n_atoms, int lpa) { return (int)(((long long)n_atoms * lpa + 255) / 256); }
+
+#define PDGPU_LPA_DISPATCH(lpa, KERN, grid, ...)                                   \
+  switch (lpa) {                                                                   \
+    case 4: PDGPU_LAUNCH((KERN<4>), grid(4), 256, 0, st, __VA_ARGS__); break;       \
+    case 16: PDGPU_LAUNCH((KERN<16>), grid(16), 256, 0, st, __VA_ARGS__); break;    \
+    case 32: PDGPU_LAUNCH((KERN<32>), grid(32), 256, 0, st, __VA_ARGS__); break;    \
+    default: PDGPU_LAUNCH((KERN<8>), grid(8), 256, 0, st, __VA_ARGS__); break;      \
+  }
+
 // --------------------------------------------------------------- K2 radii
+template <int LPA>
 __global__ void __launch_bounds__(256) k_born(PackView v, int zero_first) {
   if (v.flags[F_NL_OVERFLOW]) return;  // list incomplete: the host re-plans
-  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
-  if (i >= v.n_atoms) return;
-  const int s = v.sys_of[i];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / LPA, sub = t % LPA;
+  const bool valid = i < v.n_atoms;
+  const int ii = valid ? i : 0;
+  const int s = v.sys_of[ii];
   const SysParams &P = v.sp[s];
-  if (zero_first && lane < 3) {
+  if (valid && zero_first && sub < 3) {
     // WorkSpace::zeroForces for this atom (and the record, by the first atom)
-    long long *f = lane == 0 ? v.fx : (lane == 1 ? v.fy : v.fz);
+    long long *f = sub == 0 ? v.fx : (sub == 1 ? v.fy : v.fz);
     f[i] = 0;
     if (i == v.atom_off[s])
-      for (int k = lane; k < E_COUNT; k += 3)
+      for (int k = sub; k < E_COUNT; k += 3)
         if (k != E_EKIN) v.ene[(size_t)s * E_COUNT + k] = 0.0;
   }
-  const double xi = v.x[i], yi = v.y[i], zi = v.z[i];
-  const double Ri = v.gbR_d[i];
-  const double still2 = P.still2_d;
-  const double invP5 = P.invP5_d;
-  const double P5 = P.P5_d;
-  long long b = v.row_start[i], e = v.row_start[i + 1];
+  const double4 me = v.xyzp[ii];
+  const double Ri = v.gbR_d[ii];
+  const double still2 = P.still2_d, invP5 = P.invP5_d, P5 = P.P5_d;
+  const long long e = valid ? v.row_start[i + 1] : 0;
   double acc = 0.0;
-  for (long long k = b + lane; k < e; k += 32) {
+#pragma unroll 2
+  for (long long k = (valid ? v.row_start[i] : 0) + sub; k < e; k += LPA) {
     unsigned ent = v.nl[k];
-    if ((ent & 7u) <= 2u) continue;  // 1-2 and 1-3 partners carry no Born term
     int j = (int)(ent >> 3);
-    double d2 = ref_d2(xi, yi, zi, v.x[j], v.y[j], v.z[j]);
-    if (d2 > still2) continue;
-    double Rs = Ri + v.gbR_d[j];
-    double s2 = Rs * Rs;
-    double inv = rcp_d(d2);
-    double term = v.pv_d[j] * inv * inv;
-    if (!(d2 > s2 * invP5)) {
-      // close-contact switching factor CCF (rare; exact division + FP64 cos)
-      double rdivR = d2 / s2;
-      double c = 0.5 - 0.5 * cos(rdivR * P5 * 3.14159265358979323846);
-      if (!(rdivR > invP5)) term *= c * c;
+    double4 pj = v.xyzp[j];
+    double Rj = v.gbR_d[j];
+    if ((ent & 7u) > 2u) {  // 1-2 and 1-3 partners carry no Born term
+      double d2 = ref_d2(me.x, me.y, me.z, pj.x, pj.y, pj.z);
+      if (!(d2 > still2)) {
+        double Rs = Ri + Rj;
+        double s2 = Rs * Rs;
+        double inv = rcp_d(d2);
+        double term = pj.w * inv * inv;  // P4 * V_j / r^4
+        if (!(d2 > s2 * invP5)) {
+          // close-contact switching factor CCF (rare; exact division + FP64 cos)
+          double rdivR = d2 / s2;
+          double c = 0.5 - 0.5 * cospi(rdivR * P5);  // cos(rdivR * P5 * pi)
+          if (!(rdivR > invP5)) term *= c * c;
+        }
+        acc += term;
+      }
     }
-    acc += term;
   }
-  long long fixed = warp_sum_ll(__double2ll_rn(acc * kBornScale));
-  if (lane == 0) {
+  long long fixed = group_sum<LPA>(__double2ll_rn(acc * kBornScale));
+  if (valid && sub == 0) {
     double Gpol = v.terms123[i] + (double)fixed * kInvBornScale;
     double a = -P.halfeconv_d / Gpol + P.born_offset_d;
     v.born_d[i] = a;
-    reinterpret_cast<float2 *>(v.born_f)[i] = make_float2((float)a, (float)(1.0 / a));
+    reinterpret_cast<float *>(&v.pq[2 * (size_t)i + 1])[3] = (float)a;
   }
 }
 
-void launch_born_radii(const PackView &v, cudaStream_t st, bool zero_first) {
-  if (v.n_atoms) PDGPU_LAUNCH(k_born, (v.n_atoms + 7) / 8, 256, 0, st, v, (int)zero_first);
+void launch_born_radii_lpa(const PackView &v, cudaStream_t st, bool zero_first, int lpa) {
+  if (!v.n_atoms) return;
+  auto grid = [&](int l) { return pair_blocks(v.n_atoms, l); };
+  PDGPU_LPA_DISPATCH(lpa, k_born, grid, v, (int)zero_first);
 }
 
 // --------------------------------------------------------------- K3 pair
@@ -168,121 +201,111 @@ void launch_born_radii(const PackView &v, cudaStream_t st, bool zero_first) {
 // gbff.cpp:1553-1556 (dddx = p_i - p_j; sqr+sqr+sqr).
 // (Plain pointer arguments: taking the address of the kernel's PackView
 // parameter would copy it to local memory in every thread.)
-__device__ __noinline__ bool gb_branch_exact(const double *__restrict__ x, const double *__restrict__ y,
-                                             const double *__restrict__ z, const double *__restrict__ born,
-                                             int i, int j, double thr) {
+__device__ __forceinline__ bool gb_branch_exact(const double *__restrict__ x, const double *__restrict__ y,
+                                                const double *__restrict__ z, const double *__restrict__ born,
+                                                int i, int j, double thr) {
   double srij = ref_d2(x[i], y[i], z[i], x[j], y[j], z[j]);
   double aiaj = born[i] * born[j];
   double uGB = -srij * 0.25 / aiaj;
   return uGB > thr;
 }
 
+template <int LPA>
 __global__ void __launch_bounds__(256) k_gb_pair(PackView v) {
   if (v.flags[F_NL_OVERFLOW]) return;
-  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
-  if (i >= v.n_atoms) return;
-  const SysParams &P = v.sp[v.sys_of[i]];
-  const float4 ia = v.pa[i], ib = v.pb[i], ip = v.prm[i];
-  const float2 ab = reinterpret_cast<const float2 *>(v.born_f)[i];
-  const float ai = ab.x, inv_ai = ab.y;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / LPA, sub = t % LPA;
+  const bool valid = i < v.n_atoms;
+  const int ii = valid ? i : 0;
+  const SysParams &P = v.sp[v.sys_of[ii]];
+  const float4 ia = v.pq[2 * (size_t)ii], ib = v.pq[2 * (size_t)ii + 1], ip = v.prm[ii];
+  const float ai = ib.w;
   const float qi = ia.w, radi = ip.x, epsi = ip.y;
+  // every setting in registers for the whole row
   const float thr = P.exp_thresh;
+  const double thr_d = P.exp_thresh_d;
   const float band = 4e-6f * fabsf(thr);
+  const float rc2 = P.rc2, rin = P.rin, inv_sw2 = P.inv_sw2;
+  const float elec14 = P.elec14, vdw14 = P.vdw14, econv_in = P.econv_in, econv_out = P.econv_out;
+  const float premul = P.premul, vdw_rc = P.vdw_rc, vdw_rin = P.vdw_rin, vdw_inv_sw2 = P.vdw_inv_sw2;
   float fx = 0.f, fy = 0.f, fz = 0.f;  // -dE/dr_i, kcal/mol/A
   float e_vdw = 0.f, e_el = 0.f, e_pol = 0.f, deda = 0.f;
-  long long b = v.row_start[i], e = v.row_start[i + 1];
-  for (long long k = b + lane; k < e; k += 32) {
-    unsigned ent = v.nl[k];
-    int j = (int)(ent >> 3);
-    int bo = (int)(ent & 7u);
-    float4 ja = v.pa[j], jb = v.pb[j];
-    float dx = (ia.x - ja.x) + (ib.x - jb.x);
-    float dy = (ia.y - ja.y) + (ib.y - jb.y);
-    float dz = (ia.z - ja.z) + (ib.z - jb.z);
-    float r2 = dx * dx + dy * dy + dz * dz;
-    if (r2 > P.rc2) continue;
-    float invr = rsqrtf(r2);
-    float r = r2 * invr;
-    float2 jbf = reinterpret_cast<const float2 *>(v.born_f)[j];
-    float aj = jbf.x;
-    float qiqj = qi * ja.w;
-    float aiaj = ai * aj;
-    float u = -0.25f * r2 * (inv_ai * jbf.y);
-    bool gb = u > thr;
-    if (fabsf(u - thr) <= band) gb = gb_branch_exact(v.x, v.y, v.z, v.born_d, i, j, P.exp_thresh_d);
-    float p14 = (bo == 3) ? P.elec14 : 1.0f;
-    float S = 1.f, dSdd = 0.f;
-    if (r >= P.rin) {
-      float d = r - P.rin;
-      float s = 1.f - P.inv_sw2 * d * d;
-      dSdd = -4.f * P.inv_sw2 * d * s;
-      S = s * s;
-    }
-    float fscal = 0.f;  // dE/dr / r for this pair (dE/d(r_i) = fscal * (p_i - p_j))
-    float elec = 0.f, elf = 0.f;
-    if (gb) {
-      float t = __expf(u);
-      float m = t * aiaj;
-      float fgb = rsqrtf(r2 + m);
-      float l = fgb * fgb;
-      float epol = P.premul * qiqj * fgb;
-      float dedr = -epol * (r - 0.25f * r * t) * l;
-      float dedal = -epol * t * (1.f - u) * l;
-      if (bo >= 3) {
-        elec = P.econv_in * p14 * qiqj * invr;
-        elf = -elec * invr;
-      }
-      // the switch applies to the whole GB branch (gbff.cpp:1602-1614)
-      elf = S * elf + elec * dSdd;
-      elec *= S;
-      dedr = S * dedr + dSdd * epol;
-      dedal *= S;
-      epol *= S;
-      fscal += dedr * 2.f * invr;
-      e_pol += epol;
-      deda += dedal * aj;
-    } else if (bo >= 3) {
-      elec = P.econv_out * p14 * qiqj * invr;
-      elf = -elec * invr;
-      elf = S * elf + elec * dSdd;
-      elec *= S;
-    }
-    if (bo >= 3) {
-      float vdwf = 0.f, vdw = 0.f;
-      if (r < P.vdw_rc) {
-        float rr = (radi + v.prm[j].x) * invr;
-        float rr2 = rr * rr;
-        float B = rr2 * rr2 * rr2;
-        float A = B * B;
-        float eps = epsi * v.prm[j].y * ((bo == 3) ? P.vdw14 : 1.0f);
+  const long long e = valid ? v.row_start[i + 1] : 0;
+#pragma unroll 2
+  for (long long k = (valid ? v.row_start[i] : 0) + sub; k < e; k += LPA) {
+    const unsigned ent = v.nl[k];
+    const int j = (int)(ent >> 3);
+    const float4 ja = v.pq[2 * (size_t)j], jb = v.pq[2 * (size_t)j + 1], jp = v.prm[j];
+    const Dx d = diff(ia, ib, ja, jb);
+    if (d.r2 <= rc2) {
+      const int bo = (int)(ent & 7u);
+      const bool nb = bo >= 3;   // LJ and vacuum Coulomb apply (1-4 scaled)
+      const bool b14 = bo == 3;
+      const float invr = rsqrtf(d.r2);
+      const float r = d.r2 * invr;
+      const float aj = jb.w;
+      const float qiqj = qi * ja.w;
+      const float aiaj = ai * aj;
+      const float u = __fdividef(-0.25f * d.r2, aiaj);
+      bool gb = u > thr;
+      if (fabsf(u - thr) <= band) gb = gb_branch_exact(v.x, v.y, v.z, v.born_d, i, j, thr_d);
+      // energy switch (applies to GB and Coulomb, gbff.cpp:1602-1614)
+      const float dr = r - rin;
+      const float sw = 1.f - inv_sw2 * dr * dr;
+      const bool on = r >= rin;
+      const float S = on ? sw * sw : 1.f;
+      const float dSdd = on ? -4.f * inv_sw2 * dr * sw : 0.f;
+      // GB cross term (all bond orders), evaluated for every pair, kept
+      // when the exp approximation applies
+      const float tg = __expf(u);
+      const float fgb = rsqrtf(d.r2 + tg * aiaj);
+      const float l = fgb * fgb;
+      const float epol0 = premul * qiqj * fgb;
+      const float dedr0 = -epol0 * (r - 0.25f * r * tg) * l;
+      const float dedal0 = -epol0 * tg * (1.f - u) * l;
+      const float epol = gb ? epol0 * S : 0.f;
+      const float dedr = gb ? S * dedr0 + dSdd * epol0 : 0.f;
+      const float dedal = gb ? dedal0 * S : 0.f;
+      // vacuum Coulomb at the solute (GB branch) or solvent dielectric
+      const float ec = nb ? (gb ? econv_in : econv_out) * (b14 ? elec14 : 1.f) * qiqj * invr : 0.f;
+      const float elf = S * (-ec * invr) + ec * dSdd;
+      const float elec = ec * S;
+      // Lennard-Jones 12-6 with its own switch
+      float vdw = 0.f, vdwf = 0.f;
+      if (nb && r < vdw_rc) {
+        const float rr = (radi + jp.x) * invr;
+        const float rr2 = rr * rr;
+        const float B = rr2 * rr2 * rr2;
+        const float A = B * B;
+        const float eps = epsi * jp.y * (b14 ? vdw14 : 1.0f);
         vdw = (2.f * eps) * (0.5f * A - B);
         vdwf = -(12.f * eps * invr) * (A - B);
-        if (r > P.vdw_rin) {
-          float d = r - P.vdw_rin;
-          float s = 1.f - P.vdw_inv_sw2 * d * d;
-          float ds = -4.f * P.vdw_inv_sw2 * d * s;
-          s = s * s;
-          vdwf = s * vdwf + vdw * ds;
-          vdw *= s;
-        }
+        const float vd = r - vdw_rin;
+        const float vs = 1.f - vdw_inv_sw2 * vd * vd;
+        const bool von = r > vdw_rin;
+        const float vS = von ? vs * vs : 1.f;
+        const float vdS = von ? -4.f * vdw_inv_sw2 * vd * vs : 0.f;
+        vdwf = vS * vdwf + vdw * vdS;
+        vdw *= vS;
       }
+      const float fscal = dedr * 2.f * invr + (vdwf + elf) * invr;
+      e_pol += epol;
+      deda += dedal * aj;
       e_vdw += vdw;
       e_el += elec;
-      fscal += (vdwf + elf) * invr;
+      fx -= fscal * d.x;
+      fy -= fscal * d.y;
+      fz -= fscal * d.z;
     }
-    fx -= fscal * dx;
-    fy -= fscal * dy;
-    fz -= fscal * dz;
   }
-  long long sx = warp_sum_ll(to_fixed_force(fx));
-  long long sy = warp_sum_ll(to_fixed_force(fy));
-  long long sz = warp_sum_ll(to_fixed_force(fz));
-  double dv = warp_sum_d((double)e_vdw);
-  double de = warp_sum_d((double)e_el);
-  double dp = warp_sum_d((double)e_pol);
-  double dd = warp_sum_d((double)deda);
-  if (lane == 0) {
+  const long long sx = group_sum<LPA>(to_fixed_force(fx));
+  const long long sy = group_sum<LPA>(to_fixed_force(fy));
+  const long long sz = group_sum<LPA>(to_fixed_force(fz));
+  const double dv = group_sum<LPA>((double)e_vdw);
+  const double de = group_sum<LPA>((double)e_el);
+  const double dp = group_sum<LPA>((double)e_pol);
+  const double dd = group_sum<LPA>((double)deda);
+  if (valid && sub == 0) {
     atomicAdd((unsigned long long *)&v.fx[i], (unsigned long long)sx);
     atomicAdd((unsigned long long *)&v.fy[i], (unsigned long long)sy);
     atomicAdd((unsigned long long *)&v.fz[i], (unsigned long long)sz);
@@ -296,107 +319,115 @@ __global__ void __launch_bounds__(256) k_gb_pair(PackView v) {
     v.e_atom[(size_t)AE_POL_SELF * N + i] = eself;
     double deda_i = dd - eself / ai_d;
     double gpi = ai_d * ai_d / 166.0;  // gbff.cpp:1755 uses the literal 166.0
-    v.w_chain[i] = (float)(gpi * deda_i);
+    reinterpret_cast<float *>(&v.chainp[i])[2] = (float)(gpi * deda_i);
   }
 }
 
-void launch_gb_pair(const PackView &v, cudaStream_t st) {
-  if (v.n_atoms) PDGPU_LAUNCH(k_gb_pair, (v.n_atoms + 7) / 8, 256, 0, st, v);
+void launch_gb_pair_lpa(const PackView &v, cudaStream_t st, int lpa) {
+  if (!v.n_atoms) return;
+  auto grid = [&](int l) { return pair_blocks(v.n_atoms, l); };
+  PDGPU_LPA_DISPATCH(lpa, k_gb_pair, grid, v);
 }
 
 // --------------------------------------------------------------- K4 chain
+template <int LPA>
 __global__ void __launch_bounds__(256) k_gb_chain(PackView v) {
   if (v.flags[F_NL_OVERFLOW]) return;
-  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
-  if (i >= v.n_atoms) return;
-  const SysParams &P = v.sp[v.sys_of[i]];
-  const float4 ia = v.pa[i], ib = v.pb[i], ip = v.prm[i];
-  const float wi = v.w_chain[i];
-  const float Vi = ip.w, Ri = ip.z;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / LPA, sub = t % LPA;
+  const bool valid = i < v.n_atoms;
+  const int ii = valid ? i : 0;
+  const SysParams &P = v.sp[v.sys_of[ii]];
+  const float4 ia = v.pq[2 * (size_t)ii], ib = v.pq[2 * (size_t)ii + 1], ic = v.chainp[ii];
+  const float Ri = ic.x, Vi = ic.y, wi = ic.z;
   const float s_hi = P.still2 * (1.f + 4e-6f), s_lo = P.still2 * (1.f - 4e-6f);
+  const float invP5 = P.invP5, piP5 = P.piP5, P4 = P.P4;
+  const double still2_d = P.still2_d;
   float fx = 0.f, fy = 0.f, fz = 0.f;
-  long long b = v.row_start[i], e = v.row_start[i + 1];
-  for (long long k = b + lane; k < e; k += 32) {
-    unsigned ent = v.nl[k];
-    if ((ent & 7u) <= 2u) continue;
-    int j = (int)(ent >> 3);
-    float4 ja = v.pa[j], jb = v.pb[j];
-    float dx = (ia.x - ja.x) + (ib.x - jb.x);
-    float dy = (ia.y - ja.y) + (ib.y - jb.y);
-    float dz = (ia.z - ja.z) + (ib.z - jb.z);
-    float r2 = dx * dx + dy * dy + dz * dz;
-    if (r2 > s_hi) continue;
-    if (r2 > s_lo) {
-      double d2 = ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]);
-      if (d2 > P.still2_d) continue;
+  const long long e = valid ? v.row_start[i + 1] : 0;
+#pragma unroll 2
+  for (long long k = (valid ? v.row_start[i] : 0) + sub; k < e; k += LPA) {
+    const unsigned ent = v.nl[k];
+    const int j = (int)(ent >> 3);
+    const float4 ja = v.pq[2 * (size_t)j], jb = v.pq[2 * (size_t)j + 1], jc = v.chainp[j];
+    if ((ent & 7u) > 2u) {
+      const Dx d = diff(ia, ib, ja, jb);
+      bool in = d.r2 <= s_lo;
+      if (!in && d.r2 <= s_hi) {
+        double d2 = ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]);
+        in = !(d2 > still2_d);
+      }
+      if (in) {
+        const float Rs = Ri + jc.x;
+        const float rdivR = __fdividef(d.r2, Rs * Rs);
+        float X = 4.f;
+        if (!(rdivR > invP5)) {
+          const float th = rdivR * piP5;
+          float sn, cs;
+          __sincosf(th, &sn, &cs);
+          const float sq = 0.5f - 0.5f * cs;
+          X = 4.f * sq * sq - 2.f * sq * sn * th;
+        }
+        const float ir2 = __frcp_rn(d.r2);
+        const float ir6 = ir2 * ir2 * ir2;
+        const float tt = P4 * X * ir6 * (wi * jc.y + jc.z * Vi);
+        fx += tt * d.x;
+        fy += tt * d.y;
+        fz += tt * d.z;
+      }
     }
-    float4 jp = v.prm[j];
-    float Rs = Ri + jp.z;
-    float rdivR = r2 / (Rs * Rs);
-    float X = 4.f;
-    if (!(rdivR > P.invP5)) {
-      float th = rdivR * P.piP5;
-      float sn, cs;
-      __sincosf(th, &sn, &cs);
-      float sq = 0.5f - 0.5f * cs;
-      X = 4.f * sq * sq - 2.f * sq * sn * th;
-    }
-    float ir2 = __frcp_rn(r2);
-    float ir6 = ir2 * ir2 * ir2;
-    float wj = v.w_chain[j];
-    float t = P.P4 * X * ir6 * (wi * jp.w + wj * Vi);
-    fx += t * dx;
-    fy += t * dy;
-    fz += t * dz;
   }
-  long long sx = warp_sum_ll(to_fixed_force(fx));
-  long long sy = warp_sum_ll(to_fixed_force(fy));
-  long long sz = warp_sum_ll(to_fixed_force(fz));
-  if (lane == 0) {
+  const long long sx = group_sum<LPA>(to_fixed_force(fx));
+  const long long sy = group_sum<LPA>(to_fixed_force(fy));
+  const long long sz = group_sum<LPA>(to_fixed_force(fz));
+  if (valid && sub == 0) {
     atomicAdd((unsigned long long *)&v.fx[i], (unsigned long long)sx);
     atomicAdd((unsigned long long *)&v.fy[i], (unsigned long long)sy);
     atomicAdd((unsigned long long *)&v.fz[i], (unsigned long long)sz);
   }
 }
 
-void launch_gb_chain(const PackView &v, cudaStream_t st) {
-  if (v.n_atoms) PDGPU_LAUNCH(k_gb_chain, (v.n_atoms + 7) / 8, 256, 0, st, v);
+void launch_gb_chain_lpa(const PackView &v, cudaStream_t st, int lpa) {
+  if (!v.n_atoms) return;
+  auto grid = [&](int l) { return pair_blocks(v.n_atoms, l); };
+  PDGPU_LPA_DISPATCH(lpa, k_gb_chain, grid, v);
 }
+
+void launch_born_radii(const PackView &v, cudaStream_t st, bool zero_first) {
+  launch_born_radii_lpa(v, st, zero_first, v.lpa[0]);
+}
+void launch_gb_pair(const PackView &v, cudaStream_t st) { launch_gb_pair_lpa(v, st, v.lpa[1]); }
+void launch_gb_chain(const PackView &v, cudaStream_t st) { launch_gb_chain_lpa(v, st, v.lpa[2]); }
 
 // --------------------------------------------------------------- Born energy
 // Energy-only Born term: all pairs r <= Rc, no exp threshold, energy switch.
 __global__ void __launch_bounds__(256) k_born_energy(PackView v) {
+  if (v.flags[F_NL_OVERFLOW]) return;
   int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (i >= v.n_atoms) return;
   const SysParams &P = v.sp[v.sys_of[i]];
-  const float4 ia = v.pa[i], ib = v.pb[i];
-  const float2 ab = reinterpret_cast<const float2 *>(v.born_f)[i];
+  const float4 ia = v.pq[2 * (size_t)i], ib = v.pq[2 * (size_t)i + 1];
   float acc = 0.f;
   long long b = v.row_start[i], e = v.row_start[i + 1];
   for (long long k = b + lane; k < e; k += 32) {
     unsigned ent = v.nl[k];
     int j = (int)(ent >> 3);
-    float4 ja = v.pa[j], jb = v.pb[j];
-    float dx = (ia.x - ja.x) + (ib.x - jb.x);
-    float dy = (ia.y - ja.y) + (ib.y - jb.y);
-    float dz = (ia.z - ja.z) + (ib.z - jb.z);
-    float r2 = dx * dx + dy * dy + dz * dz;
-    if (r2 > P.rc2) continue;
-    float r = sqrtf(r2);
+    float4 ja = v.pq[2 * (size_t)j], jb = v.pq[2 * (size_t)j + 1];
+    Dx d = diff(ia, ib, ja, jb);
+    if (d.r2 > P.rc2) continue;
+    float r = sqrtf(d.r2);
     float S = 1.f;
     if (!(r < P.rin)) {
-      float d = r - P.rin;
-      float s = 1.f - P.inv_sw2 * d * d;
+      float dd = r - P.rin;
+      float s = 1.f - P.inv_sw2 * dd * dd;
       S = s * s;
     }
-    float2 jbf = reinterpret_cast<const float2 *>(v.born_f)[j];
-    float aiaj = ab.x * jbf.x;
-    float t = __expf(-r2 * 0.25f * (ab.y * jbf.y));
-    acc += S * ia.w * ja.w * rsqrtf(r2 + aiaj * t);
+    float aiaj = ib.w * jb.w;
+    float t = __expf(__fdividef(-d.r2 * 0.25f, aiaj));
+    acc += S * ia.w * ja.w * rsqrtf(d.r2 + aiaj * t);
   }
-  double sum = warp_sum_d((double)acc);
+  double sum = group_sum<32>((double)acc);
   if (lane == 0) {
     const int N = v.n_atoms;
     double ai = v.born_d[i];
@@ -454,11 +485,12 @@ __device__ __forceinline__ void nb_elec(const SysParams &P, float r, float r2, f
 
 template <int EM>
 __global__ void __launch_bounds__(256) k_nonbonded(PackView v) {
+  if (v.flags[F_NL_OVERFLOW]) return;
   int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (i >= v.n_atoms) return;
   const SysParams &P = v.sp[v.sys_of[i]];
-  const float4 ia = v.pa[i], ib = v.pb[i], ip = v.prm[i];
+  const float4 ia = v.pq[2 * (size_t)i], ib = v.pq[2 * (size_t)i + 1], ip = v.prm[i];
   float fx = 0.f, fy = 0.f, fz = 0.f, e_vdw = 0.f, e_el = 0.f, vir = 0.f;
   long long b = v.row_start[i], e = v.row_start[i + 1];
   for (long long k = b + lane; k < e; k += 32) {
@@ -466,11 +498,9 @@ __global__ void __launch_bounds__(256) k_nonbonded(PackView v) {
     int bo = (int)(ent & 7u);
     if (bo < 3) continue;  // the 1-4 scaling table zeroes 1-2 and 1-3 pairs
     int j = (int)(ent >> 3);
-    float4 ja = v.pa[j], jb = v.pb[j];
-    float dx = (ia.x - ja.x) + (ib.x - jb.x);
-    float dy = (ia.y - ja.y) + (ib.y - jb.y);
-    float dz = (ia.z - ja.z) + (ib.z - jb.z);
-    float r2 = dx * dx + dy * dy + dz * dz;
+    float4 ja = v.pq[2 * (size_t)j], jb = v.pq[2 * (size_t)j + 1];
+    Dx d = diff(ia, ib, ja, jb);
+    float r2 = d.r2;
     if (EM == 1 || EM == 2) {
       // unswitched Coulomb is discontinuous at Rc: decide boundary pairs
       // with the reference's FP64 expression (fv = p_j - p_i; innerdot)
@@ -496,9 +526,9 @@ __global__ void __launch_bounds__(256) k_nonbonded(PackView v) {
       vdw = (2.f * eps) * (0.5f * A - B);
       vdwf = -(12.f * eps * invr) * (A - B);
       if (r > P.vdw_rin) {
-        float d = r - P.vdw_rin;
-        float s = 1.f - P.vdw_inv_sw2 * d * d;
-        float ds = -4.f * P.vdw_inv_sw2 * d * s;
+        float dd = r - P.vdw_rin;
+        float s = 1.f - P.vdw_inv_sw2 * dd * dd;
+        float ds = -4.f * P.vdw_inv_sw2 * dd * s;
         s = s * s;
         vdwf = s * vdwf + vdw * ds;
         vdw *= s;
@@ -512,16 +542,16 @@ __global__ void __launch_bounds__(256) k_nonbonded(PackView v) {
     e_el += pot;
     vir += r * fm;
     float s = fm * invr;  // force on i along (p_j - p_i): f_i += s * (p_j - p_i)
-    fx -= s * dx;
-    fy -= s * dy;
-    fz -= s * dz;
+    fx -= s * d.x;
+    fy -= s * d.y;
+    fz -= s * d.z;
   }
-  long long sx = warp_sum_ll(to_fixed_force(fx));
-  long long sy = warp_sum_ll(to_fixed_force(fy));
-  long long sz = warp_sum_ll(to_fixed_force(fz));
-  double dv = warp_sum_d((double)e_vdw);
-  double de = warp_sum_d((double)e_el);
-  double dw = warp_sum_d((double)vir);
+  long long sx = group_sum<32>(to_fixed_force(fx));
+  long long sy = group_sum<32>(to_fixed_force(fy));
+  long long sz = group_sum<32>(to_fixed_force(fz));
+  double dv = group_sum<32>((double)e_vdw);
+  double de = group_sum<32>((double)e_el);
+  double dw = group_sum<32>((double)vir);
   if (lane == 0) {
     atomicAdd((unsigned long long *)&v.fx[i], (unsigned long long)sx);
     atomicAdd((unsigned long long *)&v.fy[i], (unsigned long long)sy);
@@ -556,24 +586,18 @@ __global__ void k_pair_counts(PackView v, unsigned long long *out) {
   int lane = threadIdx.x & 31;
   if (i >= v.n_atoms) return;
   const SysParams &P = v.sp[v.sys_of[i]];
-  const float4 ia = v.pa[i], ib = v.pb[i];
+  const float4 ia = v.pq[2 * (size_t)i], ib = v.pq[2 * (size_t)i + 1];
   unsigned long long pb = 0, ph = 0;
   long long b = v.row_start[i], e = v.row_start[i + 1];
   for (long long k = b + lane; k < e; k += 32) {
     unsigned ent = v.nl[k];
     int j = (int)(ent >> 3);
-    float4 ja = v.pa[j], jb = v.pb[j];
-    float dx = (ia.x - ja.x) + (ib.x - jb.x);
-    float dy = (ia.y - ja.y) + (ib.y - jb.y);
-    float dz = (ia.z - ja.z) + (ib.z - jb.z);
-    float r2 = dx * dx + dy * dy + dz * dz;
-    if (j < i && r2 <= P.rc2) ph++;
+    Dx d = diff(ia, ib, v.pq[2 * (size_t)j], v.pq[2 * (size_t)j + 1]);
+    if (j < i && d.r2 <= P.rc2) ph++;
     if ((ent & 7u) > 2u && ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]) <= P.still2_d) pb++;
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    pb += __shfl_xor_sync(0xffffffffu, pb, o);
-    ph += __shfl_xor_sync(0xffffffffu, ph, o);
-  }
+  pb = group_sum<32>(pb);
+  ph = group_sum<32>(ph);
   if (lane == 0) {
     atomicAdd(&out[0], pb);
     atomicAdd(&out[1], ph);

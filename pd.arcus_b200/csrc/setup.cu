@@ -260,7 +260,8 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   v.n_sys = S;
   // host staging
   std::vector<int> sys_of(N);
-  std::vector<float4> pa(N), pb(N), prm(N);
+  std::vector<float4> pq(2 * (size_t)N, make_float4(0, 0, 0, 0)), chainp(N), prm(N);
+  std::vector<double4> xyzp(N);
   std::vector<double> gbR(N), pv(N), t123(N), minv(N), mass(N), X(N), Y(N), Z(N);
   std::vector<int> mid(S);
   std::vector<long long> band_off(S);
@@ -277,9 +278,11 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
       sys_of[g] = s;
       prm[g] = make_float4((float)h.radius[i], (float)(h.epsilon[i] * sqrt_eps_scale), (float)h.gbR[i],
                            (float)h.vj[i]);
-      pa[g] = make_float4(0, 0, 0, (float)h.charge[i]);
+      pq[2 * (size_t)g] = make_float4(0, 0, 0, (float)h.charge[i]);
+      chainp[g] = make_float4((float)h.gbR[i], (float)h.vj[i], 0.f, 0.f);
       gbR[g] = h.gbR[i];
       pv[g] = h.params.P4 * h.vj[i];
+      xyzp[g] = make_double4(0, 0, 0, pv[g]);
       t123[g] = h.terms123[i];
       minv[g] = 1.0 / h.mass[i];
       mass[g] = h.mass[i];
@@ -331,11 +334,10 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   PALLOC(v.ox, N);
   PALLOC(v.oy, N);
   PALLOC(v.oz, N);
-  PALLOC(v.pa, N);
-  PALLOC(v.pb, N);
+  PALLOC(v.pq, 2 * (size_t)N);
+  PALLOC(v.xyzp, N);
+  PALLOC(v.chainp, N);
   PALLOC(v.born_d, N);
-  PALLOC(v.born_f, 2 * N);
-  PALLOC(v.w_chain, N);
   PALLOC(v.fx, N);
   PALLOC(v.fy, N);
   PALLOC(v.fz, N);
@@ -382,7 +384,9 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   if (!off_data.empty())
     cudaMemcpyAsync(off_data_d, off_data.data(), sizeof(int2) * off_data.size(), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(prm_d, prm.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(v.pa, pa.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(v.pq, pq.data(), sizeof(float4) * pq.size(), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(v.xyzp, xyzp.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(v.chainp, chainp.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(gbR_d, gbR.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(pv_d, pv.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(t123_d, t123.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st);
@@ -469,6 +473,7 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   PALLOC(bt.vir_bond, bt.nb);
   PALLOC(bt.e_angle, bt.na);
   PALLOC(bt.e_dih, ndih);
+  v.lpa[0] = v.lpa[1] = v.lpa[2] = 8;
   v.e_chunks = (max_range + 1023) / 1024;
   if (v.e_chunks < 1) v.e_chunks = 1;
   PALLOC(v.e_part, (size_t)S * v.e_chunks * 10);
