@@ -88,7 +88,8 @@ int pdgpu_system_create(pdgpu_ctx *ctx, int32_t natoms, const double *charge,
                         int32_t *sys_id);
 int pdgpu_system_destroy(pdgpu_ctx *ctx, int32_t sys);
 /* Change the forcefield settings (FF_NonBonded::calcCheckSum re-setup path,
- * nonbonded.cpp:1061-1067). */
+ * nonbonded.cpp:1061-1067).  Topology and settings calls (set_params,
+ * set_bonded, set_hydrogens, set_torsions) take single systems only. */
 int pdgpu_system_set_params(pdgpu_ctx *ctx, int32_t sys, const pdgpu_ff_params *params);
 
 /* Bonded terms as FF_Bonded::setup assembles them (ffbonded.cpp:13-470):
@@ -107,6 +108,49 @@ int pdgpu_system_set_bonded(pdgpu_ctx *ctx, int32_t sys, int32_t nbond,
  * LangevinOnHydrogens=false integrator (md.cpp:1048-1218).  Default: none. */
 int pdgpu_system_set_hydrogens(pdgpu_ctx *ctx, int32_t sys, const int8_t *is_h);
 
+/* ------------------------------------------------------------------ batches
+ * Many independent systems of uneven size packed into one device pack
+ * behind per-system offset tables, so that every kernel of an evaluation,
+ * MD step or minimiser step covers all of them in one launch.  No reference
+ * counterpart: the reference evaluates one WorkSpace at a time.  A batch
+ * handle is used with the same calls as a system handle; per-atom arrays
+ * then cover all packed atoms in member order (system s owns atoms
+ * atom_offset[s] .. atom_offset[s+1]-1), and per-system outputs (energies,
+ * MD history, minimiser steps) hold one record per member.  The batch takes
+ * its members' topology, settings, positions, velocities and RNG keys at
+ * creation and is independent of them afterwards.  Each member's results
+ * equal the ones it gets alone (same pair list, same per-system reductions,
+ * RNG streams keyed by the system's own key). */
+int pdgpu_batch_create(pdgpu_ctx *ctx, const int32_t *sys_ids, int32_t nsys, int32_t *batch_id);
+/* Member count and atom offsets (atom_offset[nsys+1]; either may be NULL). */
+int pdgpu_batch_info(pdgpu_ctx *ctx, int32_t batch, int32_t *nsys, int32_t *atom_offset);
+/* RNG keys of the handle's systems (seeds[nsys]); used by MD (Langevin
+ * noise, initial velocities) and trial moves instead of Seed + s.  NULL
+ * returns to the default keys (the MD Seed + member index). */
+int pdgpu_set_seeds(pdgpu_ctx *ctx, int32_t sys, const uint64_t *seeds);
+
+/* ------------------------------------------------------------------ trial moves
+ * Backbone phi/psi rotations for Monte Carlo trial conformations
+ * (MoleculeBase::setResiduePhiPsi, system/molecule.cpp:677-744, as the
+ * MonteCarlo protocol's movers use it, protocols/montecarlo.cpp:16-159).
+ * set_torsions lists a system's rotations from the N terminus: axis[2*k],
+ * axis[2*k+1] are the bonded atoms bi, bj of the k-th bond (N-CA for phi,
+ * CA-C for psi); as in MoleculeBase::rotateBond (molecule.cpp:1099-1175)
+ * rotation k turns the atoms reached from bj without crossing bi about the
+ * axis bj - bi.  Consecutive rotations of a chain must nest (each moves a
+ * subset of what the previous one moves); a rotation that moves only atoms
+ * no earlier rotation moves starts the next chain.  save_base_positions
+ * keeps the current positions as the base; perturb_torsions sets the
+ * positions to the base with rotation k turned by angles[k] (rad; all
+ * rotations of all members in member order) or, with angles NULL, by
+ * sigma * N(0,1) drawn from Philox keyed by the system's RNG key with
+ * `trial` as the counter.  The result equals rotating the bonds one by one
+ * from the N terminus (setResiduePhiPsi with phi+dphi, psi+dpsi). */
+int pdgpu_system_set_torsions(pdgpu_ctx *ctx, int32_t sys, int32_t nrot, const int32_t *axis);
+int pdgpu_save_base_positions(pdgpu_ctx *ctx, int32_t sys);
+int pdgpu_perturb_torsions(pdgpu_ctx *ctx, int32_t sys, double sigma, uint64_t trial,
+                           const double *angles);
+
 /* State transfer (WorkSpace::cur.atom[i].p / .v / .f, snapshot.h:16-22). */
 int pdgpu_set_positions(pdgpu_ctx *ctx, int32_t sys, const double *xyz);
 int pdgpu_get_positions(pdgpu_ctx *ctx, int32_t sys, double *xyz);
@@ -120,7 +164,8 @@ int pdgpu_get_born_radii(pdgpu_ctx *ctx, int32_t sys, double *born);
 int pdgpu_get_atom_epot(pdgpu_ctx *ctx, int32_t sys, double *epot);
 
 /* Energy record (Hamiltonian, workspace/hamiltonian.h:23-49), J.  Index
- * order of the PDGPU_ENE_* slots below; n >= PDGPU_ENE_COUNT. */
+ * order of the PDGPU_ENE_* slots below; n >= PDGPU_ENE_COUNT.  For a batch,
+ * system s fills ene[s*PDGPU_ENE_COUNT ...] and n >= nsys*PDGPU_ENE_COUNT. */
 #define PDGPU_ENE_EPOT 0
 #define PDGPU_ENE_VDW 1
 #define PDGPU_ENE_ELEC 2
@@ -230,7 +275,8 @@ void pdgpu_md_params_default(pdgpu_md_params *p);
  * UpdateNList, Forcefield::calcForces, NaN check, integrator}.  first_step is
  * the protocol's Step of the first call; total_steps its Steps (the
  * integrators branch on Step>0 and Step<Steps-1).  Per-step epot, ekin and
- * etot (J) are written to history[3*steps] when history is not NULL.
+ * etot (J) are written to history[3*steps*nsys] ([step][system][3]) when
+ * history is not NULL.
  * Returns PDGPU_ERR_UNSTABLE on a NaN energy (assertStability,
  * protocolbase.cpp:104-110). */
 int pdgpu_md_run(pdgpu_ctx *ctx, int32_t sys, const pdgpu_md_params *p,
@@ -259,7 +305,9 @@ typedef struct {
 } pdgpu_min_params;
 void pdgpu_min_params_default(pdgpu_min_params *p);
 /* Minimisation::runcore (minimise.cpp:99-179) with the accept / restore
- * control flow on the device; *steps_taken receives the steps done. */
+ * control flow on the device; steps_taken[nsys] receives the steps each
+ * system did (-1: NaN energy; a single system then returns
+ * PDGPU_ERR_UNSTABLE). */
 int pdgpu_minimise_run(pdgpu_ctx *ctx, int32_t sys, const pdgpu_min_params *p,
                        int32_t steps, int32_t *steps_taken);
 

@@ -400,3 +400,52 @@ def load_system_dir(path):
                 meta[k] = v.strip()
     meta["chains"] = chains
     return arrays, meta
+
+
+# ------------------------------------------------------------------ trial moves
+def backbone_axes(backbone_ncac):
+    """Rotation bonds of every residue's phi then psi, residues in order, as
+    MoleculeBase::setResiduePhiPsi applies them (system/molecule.cpp:702-711):
+    (N, CA) then (CA, C).  Returns an (R, 2) int array."""
+    bb = np.asarray(backbone_ncac).reshape(-1, 3)
+    ax = []
+    for n, ca, c in bb:
+        ax.append((n, ca))
+        ax.append((ca, c))
+    return np.asarray(ax, dtype=np.int32)
+
+
+def moved_atoms(cov12_ptr, cov12_idx, bi, bj):
+    """Atoms MoleculeBase::rotateBond(bi, bj) moves (molecule.cpp:1099-1175):
+    the covalent graph walked from bj without stepping onto bi."""
+    seen = {bi, bj}
+    queue = [bj]
+    for a in queue:
+        for nb in cov12_idx[cov12_ptr[a]:cov12_ptr[a + 1]]:
+            nb = int(nb)
+            if nb not in seen:
+                seen.add(nb)
+                queue.append(nb)
+    return np.asarray(queue, dtype=np.int64)
+
+
+def axis_rotation(axis, angle):
+    """matrix3x3::setToAxisRot (maths/maths_matrix3x3.cpp:161-185): the
+    right-handed rotation by `angle` about `axis`, applied to column vectors."""
+    u = np.asarray(axis, dtype=np.float64) / np.linalg.norm(axis)
+    c, s, t = np.cos(angle), np.sin(angle), 1.0 - np.cos(angle)
+    x, y, z = u
+    return np.array([[t * x * x + c, t * x * y - s * z, t * x * z + s * y],
+                     [t * x * y + s * z, t * y * y + c, t * y * z - s * x],
+                     [t * x * z - s * y, t * y * z + s * x, t * z * z + c]])
+
+
+def apply_torsions(pos, cov12_ptr, cov12_idx, axes, angles):
+    """Rotate the bonds one by one in list order, each about its current
+    axis (rotateBond: translate to bi, rotate, translate back)."""
+    x = np.array(pos, dtype=np.float64).reshape(-1, 3)
+    for (bi, bj), th in zip(axes, angles):
+        m = moved_atoms(cov12_ptr, cov12_idx, int(bi), int(bj))
+        R = axis_rotation(x[bj] - x[bi], th)
+        x[m] = (x[m] - x[bi]) @ R.T + x[bi]
+    return x

@@ -355,6 +355,18 @@ static void dump_topology(Built &b, const Settings &st) {
   put_d("cov13_d", c13d);
   put_i("cov14_ptr", c14p);
   put_i("cov14_idx", c14i);
+  // backbone N, CA, C of every residue (-1 where absent), for phi/psi moves
+  {
+    int nres = 0;
+    for (size_t i = 0; i < n; i++) nres = std::max(nres, ws.atom[i].ir + 1);
+    std::vector<int32_t> bb(3 * (size_t)nres, -1);
+    for (size_t i = 0; i < n; i++) {
+      const std::string &nm = ws.atom[i].pdbname;
+      int k = nm == "N" ? 0 : (nm == "CA" ? 1 : (nm == "C" ? 2 : -1));
+      if (k >= 0 && bb[3 * ws.atom[i].ir + k] < 0) bb[3 * ws.atom[i].ir + k] = (int32_t)i;
+    }
+    put_i("backbone_ncac", bb, shp(nres, 3));
+  }
 
   // bond-order band matrix + off-diagonal list, as the reference built them
   const BondOrder &bo = ws.bondorder();
@@ -483,6 +495,57 @@ static void dump_single_point(Built &b, const std::string &pre) {
   put_d(pre + "ene_energypath", e);
 }
 
+// Monte Carlo trial conformations: from the base coordinates, every
+// residue's phi and psi turned by its own normal deviate (sigma, radians)
+// through MoleculeBase::setResiduePhiPsi (molecule.cpp:702-711), residues
+// in order; then the single-point forces of each trial.  The deviates come
+// from splitmix64 + Box-Muller and are stored with the results.
+static uint64_t splitmix64(uint64_t &x) {
+  uint64_t z = (x += 0x9E3779B97F4A7C15ULL);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+static double normal01(uint64_t &x) {
+  double u1 = ((splitmix64(x) >> 11) + 1.0) * (1.0 / 9007199254740992.0);
+  double u2 = (splitmix64(x) >> 11) * (1.0 / 9007199254740992.0);
+  return sqrt(-2.0 * log(u1)) * cos(2.0 * 3.14159265358979323846 * u2);
+}
+static void dump_trials(Built &b, const std::vector<double> &base, int ntrials, double sigma, uint64_t seed) {
+  WorkSpace &ws = *b.ws;
+  size_t n = ws.nAtoms();
+  int nres = ws.nResidues();
+  std::vector<double> ang, pos, f, ene;
+  uint64_t state = seed * 0x2545F4914F6CDD1DULL + 12345;
+  for (int t = 0; t < ntrials; t++) {
+    set_pos(ws, base);
+    for (int ir = 0; ir < nres; ir++) {
+      double dphi = sigma * normal01(state), dpsi = sigma * normal01(state);
+      double fphi, fpsi;
+      ws.calcResiduePhiPsi(ir, fphi, fpsi);
+      ws.setResiduePhiPsi(ir, fphi + dphi, fpsi + dpsi);
+      ang.push_back(dphi);
+      ang.push_back(dpsi);
+    }
+    std::vector<double> p = get_pos(ws);
+    pos.insert(pos.end(), p.begin(), p.end());
+    ws.nlist().calcNewList();
+    b.ff->calcForces();
+    std::vector<double> ft = get_f(ws), et = ene_vec(ws.ene);
+    f.insert(f.end(), ft.begin(), ft.end());
+    ene.insert(ene.end(), et.begin(), et.end());
+  }
+  std::vector<size_t> s3(3);
+  s3[0] = ntrials;
+  s3[1] = n;
+  s3[2] = 3;
+  put_d("trial_angles", ang, shp(ntrials, 2 * nres));
+  put_d("trial_pos", pos, s3);
+  put_d("trial_f", f, s3);
+  put_d("trial_ene", ene, shp(ntrials, 10));
+  set_pos(ws, base);
+}
+
 // One integrator step with the normals the reference's nrand() will draw,
 // recorded by replaying the same srand() seed (rand() is only called by the
 // Langevin step inside applyForces).
@@ -573,7 +636,7 @@ static void usage() {
   fprintf(stderr,
           "ref_driver build --out DIR --nres N[,N..] --seed S [--cutoff R] "
           "[--inner R] [--grid NX,SPACING] [--premin STEPS] [--param F] "
-          "[--md STEPS] [--min STEPS] [--slowmode]\n"
+          "[--md STEPS] [--min STEPS] [--slowmode] [--trials K --trial-sigma DEG]\n"
           "ref_driver time --in DIR --cutoff R --inner R --steps K "
           "[--warmup W] [--nlist-every M] [--param F]\n");
   exit(1);
@@ -596,7 +659,8 @@ int main(int argc, char **argv) {
   Settings st;
   std::vector<int> nres;
   uint64_t seed = 0;
-  int premin = 500, mdsteps = 0, minsteps = 0, steps = 10, warmup = 1;
+  int premin = 500, mdsteps = 0, minsteps = 0, steps = 10, warmup = 1, ntrials = 0;
+  double trial_sigma_deg = 15.0;
   int nlist_every = 10;
   int gridx = 0;
   double spacing = 25.0;
@@ -614,6 +678,8 @@ int main(int argc, char **argv) {
     else if (k == "--premin") { premin = atoi(v); a++; }
     else if (k == "--md") { mdsteps = atoi(v); a++; }
     else if (k == "--min") { minsteps = atoi(v); a++; }
+    else if (k == "--trials") { ntrials = atoi(v); a++; }
+    else if (k == "--trial-sigma") { trial_sigma_deg = atof(v); a++; }
     else if (k == "--steps") { steps = atoi(v); a++; }
     else if (k == "--warmup") { warmup = atoi(v); a++; }
     else if (k == "--nlist-every") { nlist_every = atoi(v); a++; }
@@ -676,6 +742,7 @@ int main(int argc, char **argv) {
     put_d("pos", allpos, shp(b.ws->nAtoms(), 3));
     dump_topology(b, st);
     dump_single_point(b, "");
+    if (ntrials > 0) dump_trials(b, allpos, ntrials, trial_sigma_deg * 3.14159265358979323846 / 180.0, seed);
     if (minsteps > 0) {
       set_pos(*b.ws, allpos);
       dump_minimise(b, Minimisation::SteepestDescent, minsteps, "minsd_");

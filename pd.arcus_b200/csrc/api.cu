@@ -24,13 +24,21 @@ void min_state_read(const void *host_buf, int s, int *taken, int *nan, double *m
 
 using namespace pdgpu;
 
-// Device-side extras a system needs beyond the Pack core.
+// A handle: one system (a WorkSpace), or a batch of many packed into one
+// device Pack.  `host` is the first member; a batch shares its members'
+// host data with the systems it was made from.
 struct SysEntry {
-  SystemHost host;
+  std::shared_ptr<SystemHost> host;
+  std::vector<std::shared_ptr<SystemHost>> members;
   std::unique_ptr<Pack> pack;
-  // bonded scratch + per-system term ranges
-  unsigned char *is_h = nullptr;
-  unsigned long long *seeds = nullptr;
+  unsigned long long *seeds = nullptr;  // [S] RNG keys
+  bool custom_seeds = false;
+  int nsys() const { return (int)members.size(); }
+  std::vector<const SystemHost *> member_ptrs() const {
+    std::vector<const SystemHost *> m;
+    for (auto &h : members) m.push_back(h.get());
+    return m;
+  }
   int *step_dev = nullptr;
   double *hist = nullptr;
   int hist_cap = 0;
@@ -99,6 +107,60 @@ static int sync_check(pdgpu_ctx *c, const char *what) {
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, what);
   return PDGPU_OK;
+}
+
+// Device side of a new handle: the pack of its members, the RNG keys and
+// the step counters.
+static int entry_finish(pdgpu_ctx *c, SysEntry *e) {
+  std::string err;
+  Pack *p = pack_create(c->device, c->st, e->member_ptrs(), &err);
+  if (!p) {
+    set_error(err);
+    return PDGPU_ERR_NOMEM;
+  }
+  e->pack.reset(p);
+  if (xalloc(e, &e->seeds, e->nsys()) != cudaSuccess || xalloc(e, &e->step_dev, 3) != cudaSuccess) {
+    set_error("device allocation failed");
+    return PDGPU_ERR_NOMEM;
+  }
+  return PDGPU_OK;
+}
+
+extern "C" int pdgpu_get_positions(pdgpu_ctx *c, int32_t sys, double *xyz);
+extern "C" int pdgpu_set_positions(pdgpu_ctx *c, int32_t sys, const double *xyz);
+extern "C" int pdgpu_get_velocities(pdgpu_ctx *c, int32_t sys, double *v);
+extern "C" int pdgpu_set_velocities(pdgpu_ctx *c, int32_t sys, const double *v);
+
+// Topology and settings are edited on single systems; a batch takes its
+// members' topology, settings and state when it is created.
+static int need_single(SysEntry *e, const char *what) {
+  if (e->nsys() != 1) {
+    set_error(std::string(what) + ": not allowed on a batch (edit the member systems, then re-create the batch)");
+    return PDGPU_ERR_STATE;
+  }
+  return PDGPU_OK;
+}
+
+// Re-create a handle's pack after its host topology changed (re-setup),
+// keeping positions and velocities.
+static int rebuild_pack(pdgpu_ctx *c, SysEntry *e, int sys) {
+  int n = e->pack->v.n_atoms;
+  std::vector<double> x(3 * (size_t)n), vv(3 * (size_t)n);
+  int r = pdgpu_get_positions(c, sys, x.data());
+  if (r) return r;
+  r = pdgpu_get_velocities(c, sys, vv.data());
+  if (r) return r;
+  std::string err;
+  Pack *p = pack_create(c->device, c->st, e->member_ptrs(), &err);
+  if (!p) {
+    set_error(err);
+    return PDGPU_ERR_NOMEM;
+  }
+  e->drop_graph();
+  e->pack.reset(p);
+  r = pdgpu_set_positions(c, sys, x.data());
+  if (r) return r;
+  return pdgpu_set_velocities(c, sys, vv.data());
 }
 
 extern "C" {
@@ -242,7 +304,9 @@ int pdgpu_system_create(pdgpu_ctx *c, int32_t natoms, const double *charge, cons
   int r = validate_params(params);
   if (r) return r;
   auto e = std::make_unique<SysEntry>();
-  SystemHost &h = e->host;
+  e->host = std::make_shared<SystemHost>();
+  e->members.push_back(e->host);
+  SystemHost &h = *e->host;
   h.natoms = natoms;
   if (params)
     h.params = *params;
@@ -286,22 +350,87 @@ int pdgpu_system_create(pdgpu_ctx *c, int32_t natoms, const double *charge, cons
     return r;
   }
   host_gb_fixed_terms(h);
-  std::vector<const SystemHost *> one(1, &h);
-  Pack *p = pack_create(c->device, c->st, one, &err);
-  if (!p) {
-    set_error(err);
-    return PDGPU_ERR_NOMEM;
-  }
-  e->pack.reset(p);
-  if (xalloc(e.get(), &e->is_h, natoms) != cudaSuccess || xalloc(e.get(), &e->seeds, 1) != cudaSuccess ||
-      xalloc(e.get(), &e->step_dev, 3) != cudaSuccess) {
-    set_error("device allocation failed");
-    return PDGPU_ERR_NOMEM;
-  }
+  r = entry_finish(c, e.get());
+  if (r) return r;
   int id = c->next_id++;
   c->sys[id] = std::move(e);
   *sys_id = id;
   return PDGPU_OK;
+}
+
+int pdgpu_batch_create(pdgpu_ctx *c, const int32_t *sys_ids, int32_t nsys, int32_t *batch_id) {
+  CHECK_CTX(c);
+  if (!sys_ids || nsys <= 0 || !batch_id) {
+    set_error("pdgpu_batch_create: bad arguments");
+    return PDGPU_ERR_ARG;
+  }
+  auto e = std::make_unique<SysEntry>();
+  long long total = 0;
+  std::vector<SysEntry *> src;
+  for (int k = 0; k < nsys; k++) {
+    GET_SYS(m, c, sys_ids[k]);
+    if (m->nsys() != 1) {
+      set_error("pdgpu_batch_create: members must be single systems, not batches");
+      return PDGPU_ERR_ARG;
+    }
+    e->members.push_back(m->host);
+    src.push_back(m);
+    total += m->host->natoms;
+  }
+  if (total >= (1 << 24)) {
+    set_error("pdgpu_batch_create: a batch holds fewer than 2^24 atoms");
+    return PDGPU_ERR_ARG;
+  }
+  e->host = e->members[0];
+  int r = entry_finish(c, e.get());
+  if (r) return r;
+  // the batch starts from its members' current positions, velocities and
+  // RNG keys (device to device, no host round trip)
+  Pack &B = *e->pack;
+  std::vector<unsigned long long> keys(nsys);
+  for (int k = 0; k < nsys; k++) {
+    const PackView &s = src[k]->pack->v;
+    size_t o = B.atom_off[k], n = s.n_atoms;
+    double *dst[6] = {B.v.x, B.v.y, B.v.z, B.v.vx, B.v.vy, B.v.vz};
+    const double *from[6] = {s.x, s.y, s.z, s.vx, s.vy, s.vz};
+    for (int q = 0; q < 6; q++)
+      PDGPU_CUDA(cudaMemcpyAsync(dst[q] + o, from[q], sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
+    PDGPU_CUDA(cudaMemcpyAsync(&keys[k], src[k]->seeds, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->st));
+  }
+  r = sync_check(c, "batch_create");
+  if (r) return r;
+  PDGPU_CUDA(cudaMemcpyAsync(e->seeds, keys.data(), sizeof(unsigned long long) * nsys, cudaMemcpyHostToDevice,
+                             c->st));
+  e->custom_seeds = false;
+  launch_pack_positions(B.v, c->st);
+  r = sync_check(c, "batch_create");
+  if (r) return r;
+  int id = c->next_id++;
+  c->sys[id] = std::move(e);
+  *batch_id = id;
+  return PDGPU_OK;
+}
+
+int pdgpu_batch_info(pdgpu_ctx *c, int32_t batch, int32_t *nsys, int32_t *atom_offset) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, batch);
+  if (nsys) *nsys = e->nsys();
+  if (atom_offset)
+    for (int s = 0; s <= e->nsys(); s++) atom_offset[s] = e->pack->atom_off[s];
+  return PDGPU_OK;
+}
+
+int pdgpu_set_seeds(pdgpu_ctx *c, int32_t sys, const uint64_t *seeds) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (!seeds) {
+    e->custom_seeds = false;
+    return PDGPU_OK;
+  }
+  PDGPU_CUDA(cudaMemcpyAsync(e->seeds, seeds, sizeof(unsigned long long) * e->nsys(), cudaMemcpyHostToDevice,
+                             c->st));
+  e->custom_seeds = true;
+  return sync_check(c, "set_seeds");
 }
 
 int pdgpu_system_destroy(pdgpu_ctx *c, int32_t sys) {
@@ -323,25 +452,16 @@ int pdgpu_system_set_params(pdgpu_ctx *c, int32_t sys, const pdgpu_ff_params *pa
     set_error("params is NULL");
     return PDGPU_ERR_ARG;
   }
-  bool fixed_changed = params->P1 != e->host.params.P1 || params->P2 != e->host.params.P2 ||
-                       params->P3 != e->host.params.P3 || params->P4 != e->host.params.P4 ||
-                       params->DielectricOffset != e->host.params.DielectricOffset;
-  e->host.params = *params;
+  r = need_single(e, "pdgpu_system_set_params");
+  if (r) return r;
+  SystemHost &h = *e->host;
+  bool fixed_changed = params->P1 != h.params.P1 || params->P2 != h.params.P2 || params->P3 != h.params.P3 ||
+                       params->P4 != h.params.P4 || params->DielectricOffset != h.params.DielectricOffset;
+  h.params = *params;
   if (fixed_changed) {
     // the Still fixed terms depend on P1-P4: rebuild the pack (re-setup)
-    host_gb_fixed_terms(e->host);
-    std::string err;
-    std::vector<const SystemHost *> one(1, &e->host);
-    std::vector<double> x(3 * e->host.natoms);
-    pdgpu_get_positions(c, sys, x.data());
-    Pack *p = pack_create(c->device, c->st, one, &err);
-    if (!p) {
-      set_error(err);
-      return PDGPU_ERR_NOMEM;
-    }
-    e->drop_graph();
-    e->pack.reset(p);
-    return pdgpu_set_positions(c, sys, x.data());
+    host_gb_fixed_terms(h);
+    return rebuild_pack(c, e, sys);
   }
   e->drop_graph();
   Pack &P = *e->pack;
@@ -362,7 +482,9 @@ int pdgpu_system_set_bonded(pdgpu_ctx *c, int32_t sys, int32_t nb, const int32_t
     set_error("pdgpu_system_set_bonded: bad arguments");
     return PDGPU_ERR_ARG;
   }
-  SystemHost &h = e->host;
+  int r = need_single(e, "pdgpu_system_set_bonded");
+  if (r) return r;
+  SystemHost &h = *e->host;
   int n = h.natoms;
   auto inrange = [&](const int32_t *a, long cnt) {
     for (long k = 0; k < cnt; k++)
@@ -398,23 +520,7 @@ int pdgpu_system_set_bonded(pdgpu_ctx *c, int32_t sys, int32_t nb, const int32_t
   h.tpar.assign(tpar, tpar + 12 * nt);
   h.tpar.insert(h.tpar.end(), ipar, ipar + 12 * ni);
   // rebuild the pack with the bonded terms, keeping the state
-  std::vector<double> x(3 * n), vv(3 * n);
-  int r = pdgpu_get_positions(c, sys, x.data());
-  if (r) return r;
-  r = pdgpu_get_velocities(c, sys, vv.data());
-  if (r) return r;
-  std::string err;
-  std::vector<const SystemHost *> one(1, &h);
-  Pack *p = pack_create(c->device, c->st, one, &err);
-  if (!p) {
-    set_error(err);
-    return PDGPU_ERR_NOMEM;
-  }
-  e->drop_graph();
-  e->pack.reset(p);
-  r = pdgpu_set_positions(c, sys, x.data());
-  if (r) return r;
-  return pdgpu_set_velocities(c, sys, vv.data());
+  return rebuild_pack(c, e, sys);
 }
 
 int pdgpu_system_set_hydrogens(pdgpu_ctx *c, int32_t sys, const int8_t *is_h) {
@@ -424,8 +530,106 @@ int pdgpu_system_set_hydrogens(pdgpu_ctx *c, int32_t sys, const int8_t *is_h) {
     set_error("is_h is NULL");
     return PDGPU_ERR_ARG;
   }
-  PDGPU_CUDA(cudaMemcpyAsync(e->is_h, is_h, e->host.natoms, cudaMemcpyHostToDevice, c->st));
+  int r = need_single(e, "pdgpu_system_set_hydrogens");
+  if (r) return r;
+  e->host->is_h.assign(is_h, is_h + e->host->natoms);
+  PDGPU_CUDA(cudaMemcpyAsync(e->pack->is_h, is_h, e->host->natoms, cudaMemcpyHostToDevice, c->st));
   return sync_check(c, "set_hydrogens");
+}
+
+int pdgpu_system_set_torsions(pdgpu_ctx *c, int32_t sys, int32_t nrot, const int32_t *axis) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  int r = need_single(e, "pdgpu_system_set_torsions");
+  if (r) return r;
+  SystemHost &h = *e->host;
+  const int n = h.natoms;
+  if (nrot < 0 || (nrot && !axis)) {
+    set_error("pdgpu_system_set_torsions: bad arguments");
+    return PDGPU_ERR_ARG;
+  }
+  // The atoms each rotation moves: MoleculeBase::rotateBond(bi, bj)
+  // (system/molecule.cpp:1099-1175) walks the covalent graph from bj and
+  // never steps onto bi.  Consecutive rotations must nest (each moves a
+  // subset of what the previous one moves) or start a new nest on atoms no
+  // earlier rotation moves; each atom records the last rotation moving it.
+  std::vector<int> last(n, -1), queue;
+  std::vector<unsigned char> start(nrot, 0), mark(n, 0);
+  for (int k = 0; k < nrot; k++) {
+    int bi = axis[2 * k], bj = axis[2 * k + 1];
+    if (bi < 0 || bi >= n || bj < 0 || bj >= n) {
+      set_error("pdgpu_system_set_torsions: axis atom out of range");
+      return PDGPU_ERR_ARG;
+    }
+    bool bonded = false;
+    for (int q = h.c12p[bi]; q < h.c12p[bi + 1]; q++) bonded |= h.c12i[q] == bj;
+    if (!bonded) {
+      set_error("pdgpu_system_set_torsions: rotation " + std::to_string(k) + " is not about a covalent bond");
+      return PDGPU_ERR_ARG;
+    }
+    queue.assign(1, bj);
+    std::fill(mark.begin(), mark.end(), 0);
+    mark[bi] = mark[bj] = 1;
+    for (size_t q = 0; q < queue.size(); q++) {
+      int a = queue[q];
+      for (int t = h.c12p[a]; t < h.c12p[a + 1]; t++) {
+        int nb = h.c12i[t];
+        if (!mark[nb]) {
+          mark[nb] = 1;
+          queue.push_back(nb);
+        }
+      }
+    }
+    bool inner = true, fresh = true;
+    for (int a : queue) {
+      inner &= k > 0 && last[a] == k - 1;
+      fresh &= last[a] == -1;
+    }
+    if (!inner && !fresh) {
+      set_error("pdgpu_system_set_torsions: rotation " + std::to_string(k) +
+                " neither nests inside the previous one nor moves only atoms no earlier rotation moves");
+      return PDGPU_ERR_ARG;
+    }
+    start[k] = !inner;
+    for (int a : queue) last[a] = k;
+  }
+  h.rot_axis.assign(axis, axis + 2 * nrot);
+  h.rot_start = start;
+  if (nrot)
+    h.rot_last = last;
+  else
+    h.rot_last.clear();
+  return rebuild_pack(c, e, sys);
+}
+
+int pdgpu_save_base_positions(pdgpu_ctx *c, int32_t sys) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  PackView &v = e->pack->v;
+  size_t n = v.n_atoms;
+  PDGPU_CUDA(cudaMemcpyAsync(v.bx, v.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(v.by, v.y, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(v.bz, v.z, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
+  return sync_check(c, "save_base_positions");
+}
+
+int pdgpu_perturb_torsions(pdgpu_ctx *c, int32_t sys, double sigma, uint64_t trial, const double *angles) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  if (!(sigma >= 0)) {
+    set_error("pdgpu_perturb_torsions: sigma must be >= 0");
+    return PDGPU_ERR_ARG;
+  }
+  double *ang = nullptr;
+  size_t R = P.rot_total;
+  if (angles && R) {
+    PDGPU_CUDA(cudaMallocAsync((void **)&ang, sizeof(double) * R, c->st));
+    PDGPU_CUDA(cudaMemcpyAsync(ang, angles, sizeof(double) * R, cudaMemcpyHostToDevice, c->st));
+  }
+  launch_torsion_moves(P.v, c->st, sigma, trial, e->seeds, ang);
+  if (ang) cudaFreeAsync(ang, c->st);
+  return sync_check(c, "perturb_torsions");
 }
 
 // ------------------------------------------------------------ state
@@ -767,7 +971,7 @@ int pdgpu_gb_forces(pdgpu_ctx *c, int32_t sys) {
   int r = need_list(P);
   if (r) return r;
   if ((r = ensure_tuned(c, P))) return r;
-  if (!e->host.params.FastMode) {
+  if (!e->host->params.FastMode) {
     set_error("FastMode=false (separate FF_NonBonded + calcBornForces) is not built; use FastMode");
     return PDGPU_ERR_ARG;
   }
@@ -783,18 +987,23 @@ int pdgpu_gb_energies(pdgpu_ctx *c, int32_t sys) {
   if (r) return r;
   // calcEnergies: radii, FF_NonBonded::calcEnergies at Dielectric =
   // DielectricSolute (gbff.cpp:44), then calcBornEnergy
-  pdgpu_ff_params q = e->host.params;
-  q.Dielectric = q.DielectricSolute;
-  SysParams saved = P.sp[0];
-  pack_set_params(&P, 0, q);
-  PDGPU_CUDA(cudaMemcpyAsync((void *)P.v.sp, P.sp.data(), sizeof(SysParams), cudaMemcpyHostToDevice, c->st));
+  const int S = e->nsys();
+  std::vector<SysParams> saved = P.sp;
+  for (int s = 0; s < S; s++) {
+    pdgpu_ff_params q = e->members[s]->params;
+    q.Dielectric = q.DielectricSolute;
+    pack_set_params(&P, s, q);
+  }
+  PDGPU_CUDA(cudaMemcpyAsync((void *)P.v.sp, P.sp.data(), sizeof(SysParams) * S, cudaMemcpyHostToDevice, c->st));
   launch_born_radii(P.v, c->st);
   launch_nonbonded(P.v, c->st, P.sp[0].elec_mode);
   launch_born_energy(P.v, c->st);
   launch_energy(P.v, c->st, EM_PAIR_NB | EM_BORN_ENERGY);
-  P.sp[0] = saved;
-  PDGPU_CUDA(cudaMemcpyAsync((void *)P.v.sp, P.sp.data(), sizeof(SysParams), cudaMemcpyHostToDevice, c->st));
-  return sync_check(c, "gb_energies");
+  r = sync_check(c, "gb_energies");
+  P.sp = saved;
+  PDGPU_CUDA(cudaMemcpyAsync((void *)P.v.sp, P.sp.data(), sizeof(SysParams) * S, cudaMemcpyHostToDevice, c->st));
+  int r2 = sync_check(c, "gb_energies");
+  return r ? r : r2;
 }
 
 int pdgpu_nonbonded_forces(pdgpu_ctx *c, int32_t sys) {
@@ -843,6 +1052,16 @@ int pdgpu_calc_forces(pdgpu_ctx *c, int32_t sys) {
 }
 
 // ------------------------------------------------------------ MD
+// RNG keys: those given to pdgpu_set_seeds, else base + s for system s
+static int default_seeds(pdgpu_ctx *c, SysEntry *e, unsigned long long base) {
+  if (e->custom_seeds) return PDGPU_OK;
+  std::vector<unsigned long long> k(e->nsys());
+  for (int s = 0; s < e->nsys(); s++) k[s] = base + (unsigned long long)s;
+  PDGPU_CUDA(cudaMemcpyAsync(e->seeds, k.data(), sizeof(unsigned long long) * k.size(), cudaMemcpyHostToDevice,
+                             c->st));
+  return PDGPU_OK;
+}
+
 static MDCoef md_coef(const pdgpu_md_params *p, int step, int steps) {
   // the coefficient branches of md.cpp:961-1000
   MDCoef c;
@@ -905,10 +1124,9 @@ int pdgpu_md_step_with_normals(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params 
     PDGPU_CUDA(cudaMalloc(&nd, sizeof(double) * 6 * P.v.n_atoms));
     PDGPU_CUDA(cudaMemcpyAsync(nd, normals, sizeof(double) * 6 * P.v.n_atoms, cudaMemcpyHostToDevice, c->st));
   }
-  unsigned long long seed = p->Seed;
-  PDGPU_CUDA(cudaMemcpyAsync(e->seeds, &seed, sizeof seed, cudaMemcpyHostToDevice, c->st));
+  if ((r = default_seeds(c, e, p->Seed))) return r;
   MDCoef k = md_coef(p, step, total_steps);
-  launch_md_step_impl(P.v, c->st, k, nd, nullptr, e->is_h, e->seeds);
+  launch_md_step_impl(P.v, c->st, k, nd, nullptr, P.is_h, e->seeds);
   r = sync_check(c, "md_step");
   if (nd) cudaFree(nd);
   return r;
@@ -917,8 +1135,8 @@ int pdgpu_md_step_with_normals(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params 
 int pdgpu_md_init_velocities(pdgpu_ctx *c, int32_t sys, double temperature, uint64_t seed) {
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
-  unsigned long long s = seed;
-  PDGPU_CUDA(cudaMemcpyAsync(e->seeds, &s, sizeof s, cudaMemcpyHostToDevice, c->st));
+  int r = default_seeds(c, e, seed);
+  if (r) return r;
   launch_vel_init_impl(e->pack->v, c->st, temperature, e->seeds);
   return sync_check(c, "init_velocities");
 }
@@ -928,7 +1146,7 @@ int pdgpu_md_init_velocities(pdgpu_ctx *c, int32_t sys, double temperature, uint
 static void md_step_enqueue(pdgpu_ctx *c, SysEntry *e, const MDCoef &k) {
   Pack &P = *e->pack;
   calc_forces_enqueue(c, e, false);
-  launch_md_step_impl(P.v, c->st, k, nullptr, e->step_dev, e->is_h, e->seeds);
+  launch_md_step_impl(P.v, c->st, k, nullptr, e->step_dev, P.is_h, e->seeds);
   launch_energy(P.v, c->st, EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0) | EM_KINETIC | EM_RECORD, e->hist,
                 e->step_dev);
 }
@@ -946,20 +1164,20 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
   Pack &P = *e->pack;
   PackView &v = P.v;
   if (steps == 0) return PDGPU_OK;
+  const int S = e->nsys();
   if (e->hist_cap < steps) {
     if (e->hist) {
       cudaFree(e->hist);
       e->extra.erase(std::find(e->extra.begin(), e->extra.end(), (void *)e->hist));
       e->hist = nullptr;
     }
-    if (xalloc(e, &e->hist, (size_t)3 * steps) != cudaSuccess) {
+    if (xalloc(e, &e->hist, (size_t)3 * steps * S) != cudaSuccess) {
       set_error("device allocation failed (history)");
       return PDGPU_ERR_NOMEM;
     }
     e->hist_cap = steps;
   }
-  unsigned long long seed = p->Seed;
-  PDGPU_CUDA(cudaMemcpyAsync(e->seeds, &seed, sizeof seed, cudaMemcpyHostToDevice, c->st));
+  if ((r = default_seeds(c, e, p->Seed))) return r;
   PDGPU_CUDA(cudaMemcpyAsync(e->step_dev, &first_step, sizeof(int), cudaMemcpyHostToDevice, c->st));
   PDGPU_CUDA(cudaMemsetAsync(v.flags, 0, sizeof(int) * F_COUNT, c->st));
   MDCoef k = md_coef(p, first_step, total_steps);
@@ -998,7 +1216,7 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
         char key[256];
         snprintf(key, sizeof key, "%d|%p|%lld|%p|%d|%d|%.17g|%.17g|%.17g|%d|%d|%d|%d%d%d", block, (void *)v.nl,
                  v.nl_cap, (void *)e->hist, k.integrator, k.steps, k.dt, k.gamma, k.temp, k.stochastic_h,
-                 P.radix_passes, (int)e->host.params.FastMode, v.lpa[0], v.lpa[1], v.lpa[2]);
+                 P.radix_passes, (int)e->host->params.FastMode, v.lpa[0], v.lpa[1], v.lpa[2]);
         if (!e->gexec || e->gkey != key) {
           e->drop_graph();
           long long before = launch_counter();
@@ -1034,7 +1252,7 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
       }
       if (flags[F_NAN]) {
         if (history) {
-          std::vector<double> h((size_t)3 * (s + block));
+          std::vector<double> h((size_t)3 * (s + block) * S);
           cudaMemcpy(h.data(), e->hist, sizeof(double) * h.size(), cudaMemcpyDeviceToHost);
           for (size_t q = 0; q < h.size(); q++) history[q] = h[q] * consts().J_per_kcalmol;
         }
@@ -1054,7 +1272,7 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
   P.last_run_ms = ms;
   c->last_ms = ms;
   if (history) {
-    std::vector<double> h((size_t)3 * steps);
+    std::vector<double> h((size_t)3 * steps * S);
     PDGPU_CUDA(cudaMemcpy(h.data(), e->hist, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
     double J = consts().J_per_kcalmol;
     for (size_t q = 0; q < h.size(); q++) history[q] = h[q] * J;
@@ -1074,14 +1292,15 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
   Pack &P = *e->pack;
   PackView &v = P.v;
   const Consts &k = consts();
+  const int S = e->nsys();
   if (!e->min_state) {
     void *m = nullptr;
-    PDGPU_CUDA(cudaMalloc(&m, min_state_size()));
+    PDGPU_CUDA(cudaMalloc(&m, min_state_size() * S));
     e->extra.push_back(m);
     e->min_state = m;
   }
-  std::vector<unsigned char> hs(min_state_size());
-  min_state_init(hs.data(), 1);
+  std::vector<unsigned char> hs(min_state_size() * S);
+  min_state_init(hs.data(), S);
   PDGPU_CUDA(cudaMemcpyAsync(e->min_state, hs.data(), hs.size(), cudaMemcpyHostToDevice, c->st));
   PDGPU_CUDA(cudaMemsetAsync(v.flags, 0, sizeof(int) * F_COUNT, c->st));
   // WorkSpace::old = cur (minimise.cpp:114)
@@ -1103,13 +1322,16 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
   // Chunks of up to 16 steps run without a host synchronisation.  A step
   // whose list rebuild overflowed does nothing on the device (flag); the
   // host grows the list and repeats it.  The list cadence follows the
-  // steps the device actually took.
+  // iterations the device actually took; every system still running takes
+  // one step per iteration, and a finished system (converged, out of
+  // steps, NaN) sits the rest out.
   const int counter0 = P.nlist_counter;
-  int taken = 0, regrow = 0;
-  while (taken < steps) {
-    int chunk = std::min(16, steps - taken);
+  int iter = 0, regrow = 0;
+  std::vector<int> taken(S, 0);
+  while (iter < steps) {
+    int chunk = std::min(16, steps - iter);
     for (int q = 0; q < chunk; q++) {
-      int cnt = counter0 + taken + q;
+      int cnt = counter0 + iter + q;
       if (every > 0 && (cnt % every) == 0) {
         launch_nlist_count(P, c->st);
         launch_nlist_fill(P, c->st);
@@ -1121,17 +1343,27 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
     PDGPU_CUDA(cudaMemcpyAsync(flags, v.flags, sizeof flags, cudaMemcpyDeviceToHost, c->st));
     r = sync_check(c, "minimise");
     if (r) return r;
-    int nan, done_taken;
-    double mult;
     PDGPU_CUDA(cudaMemcpy(hs.data(), e->min_state, hs.size(), cudaMemcpyDeviceToHost));
-    min_state_read(hs.data(), 0, &done_taken, &nan, &mult);
-    if (nan) {
+    int advanced = 0, nan_count = 0;
+    for (int s = 0; s < S; s++) {
+      int nan, done_taken;
+      double mult;
+      min_state_read(hs.data(), s, &done_taken, &nan, &mult);
+      advanced = std::max(advanced, done_taken - taken[s]);
+      taken[s] = done_taken;
+      if (nan) {
+        taken[s] = -1;
+        nan_count++;
+      }
+    }
+    if (S == 1 && nan_count) {
       if (steps_taken) *steps_taken = -1;
       set_error("Simulation unstable (NaN energy during minimisation)");
       return PDGPU_ERR_UNSTABLE;
     }
-    bool finished = done_taken == taken && !flags[F_NL_OVERFLOW];  // converged (SlopeCutoff)
-    taken = done_taken;
+    // every system finished early (converged on SlopeCutoff, or NaN)
+    bool finished = advanced < chunk && !flags[F_NL_OVERFLOW];
+    iter += advanced;
     if (flags[F_NL_OVERFLOW]) {
       if (++regrow > 8) {
         set_error("neighbour list kept overflowing during minimisation");
@@ -1143,7 +1375,7 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
     }
     if (finished) break;
   }
-  P.nlist_counter = counter0 + taken;
+  P.nlist_counter = counter0 + iter;
   // cur = old; recompute the energies (minimise.cpp:172-176)
   launch_min_finish(v, c->st);
   calc_forces_enqueue(c, e);
@@ -1154,7 +1386,8 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
   cudaEventElapsedTime(&ms, P.ev0, P.ev1);
   P.last_run_ms = ms;
   c->last_ms = ms;
-  if (steps_taken) *steps_taken = taken;
+  if (steps_taken)
+    for (int s = 0; s < S; s++) steps_taken[s] = taken[s];
   return PDGPU_OK;
 }
 

@@ -23,40 +23,7 @@
 
 namespace pdgpu {
 
-// --------------------------------------------------------------- Philox4x32-10
-// Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3"
-// (SC11): 10 rounds of two 32x32->64 multiplies with the published
-// multipliers and Weyl key increments.
-struct U4 {
-  unsigned a, b, c, d;
-};
-__device__ __forceinline__ U4 philox(U4 ctr, unsigned k0, unsigned k1) {
-#pragma unroll
-  for (int r = 0; r < 10; r++) {
-    unsigned hi0 = __umulhi(0xD2511F53u, ctr.a), lo0 = 0xD2511F53u * ctr.a;
-    unsigned hi1 = __umulhi(0xCD9E8D57u, ctr.c), lo1 = 0xCD9E8D57u * ctr.c;
-    U4 n;
-    n.a = hi1 ^ ctr.b ^ k0;
-    n.b = lo1;
-    n.c = hi0 ^ ctr.d ^ k1;
-    n.d = lo0;
-    ctr = n;
-    k0 += 0x9E3779B9u;
-    k1 += 0xBB67AE85u;
-  }
-  return ctr;
-}
-// uniform in (0, 1], like the reference's frand() (maths.cpp:256-261)
-__device__ __forceinline__ double u01(unsigned x) { return ((double)x + 1.0) * (1.0 / 4294967296.0); }
-// Box-Muller pair in the reference's form (maths.h:136-151)
-__device__ __forceinline__ void nrand_pair(unsigned ua, unsigned ub, double &n1, double &n2) {
-  double z1 = u01(ua), z2 = u01(ub);
-  double l = sqrt(-2.0 * log(z1));
-  double s, c;
-  sincos(-2.0 * 3.14159265358979323846 * z2, &s, &c);
-  n1 = l * c;
-  n2 = l * s;
-}
+// (Philox4x32-10 and the Box-Muller pair live in internal.cuh)
 // six normals for atom `local` at `step`, in the reference's draw order
 // n1x n2y n2x n1z n1y n2z
 __device__ __forceinline__ void six_normals(unsigned long long seed, int local, int step, double *o) {

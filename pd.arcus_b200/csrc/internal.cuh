@@ -127,6 +127,13 @@ struct PackView {
   double *e_part;             // [S * e_chunks * 10] reduction partials
   int e_chunks;               // 1024-item chunks of the largest per-system range
   int lpa[3];                 // lanes per atom of the Born, fused-pair and chain kernels
+  // backbone torsion moves (Monte Carlo trial conformations)
+  const int2 *rot_axis;       // [R]: axis atoms (global) of every phi/psi rotation
+  const int *rot_off;         // [S+1]: rotation range of each system
+  const unsigned char *rot_start; // [R]: 1 where a nest of rotations (a chain) begins
+  const int *rot_last;        // [N]: last rotation (global) that moves the atom, -1 none
+  double *rot_xf;             // [R*12]: prefix-composed affine transforms
+  double *bx, *by, *bz;       // base positions the trial moves start from
   // bond order
   const int *mid;             // [S]
   const long long *band_off;  // [S]
@@ -167,6 +174,11 @@ struct SystemHost {
   std::vector<int> bij, aiaj, tidx, tterms;
   std::vector<double> blk, akt, tpar;
   int nb = 0, na = 0, nt = 0, ni = 0;
+  // backbone torsion moves: axis atom pairs (local), nest starts and the
+  // last rotation (local index, -1 none) that moves each atom
+  std::vector<int> rot_axis, rot_last;
+  std::vector<unsigned char> rot_start;
+  std::vector<int8_t> is_h;
 };
 
 // Owner of device memory for a Pack.
@@ -187,6 +199,8 @@ struct Pack {
   int scan_tmp_len = 0;
   double *red_tmp = nullptr;     // reductions
   // bookkeeping for protocols
+  unsigned char *is_h = nullptr; // Particle::isHydrogen per atom
+  long long rot_total = 0;       // backbone rotations over all systems
   int nlist_counter = 0;
   bool tuned = false;            // lanes-per-atom chosen by the autotuner
   double last_run_ms = 0.0;
@@ -239,6 +253,46 @@ void launch_kinetic(const PackView &v, cudaStream_t st);
 void launch_vel_init(const PackView &v, cudaStream_t st, double temp, unsigned long long seed);
 void launch_vel_rescale(const PackView &v, cudaStream_t st, double temp);
 void launch_check_nan(const PackView &v, cudaStream_t st);
+// backbone phi/psi trial moves from the base positions (angles: optional
+// explicit per-rotation angles, else sigma * N(0,1) from Philox keyed by
+// the system's key with the trial number as counter)
+void launch_torsion_moves(const PackView &v, cudaStream_t st, double sigma, unsigned long long trial,
+                          const unsigned long long *keys, const double *angles);
+
+// ----------------------------------------------------------------- random
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
+// easy as 1, 2, 3", SC11): 10 rounds of two 32x32->64 multiplies with the
+// published multipliers and Weyl key increments.
+struct U4 {
+  unsigned a, b, c, d;
+};
+__device__ __forceinline__ U4 philox(U4 ctr, unsigned k0, unsigned k1) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    unsigned hi0 = __umulhi(0xD2511F53u, ctr.a), lo0 = 0xD2511F53u * ctr.a;
+    unsigned hi1 = __umulhi(0xCD9E8D57u, ctr.c), lo1 = 0xCD9E8D57u * ctr.c;
+    U4 n;
+    n.a = hi1 ^ ctr.b ^ k0;
+    n.b = lo1;
+    n.c = hi0 ^ ctr.d ^ k1;
+    n.d = lo0;
+    ctr = n;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return ctr;
+}
+// uniform in (0, 1], like the reference's frand() (maths.cpp:256-261)
+__device__ __forceinline__ double u01(unsigned x) { return ((double)x + 1.0) * (1.0 / 4294967296.0); }
+// Box-Muller pair in the reference's form (maths.h:136-151)
+__device__ __forceinline__ void nrand_pair(unsigned ua, unsigned ub, double &n1, double &n2) {
+  double z1 = u01(ua), z2 = u01(ub);
+  double l = sqrt(-2.0 * log(z1));
+  double s, c;
+  sincos(-2.0 * 3.14159265358979323846 * z2, &s, &c);
+  n1 = l * c;
+  n2 = l * s;
+}
 
 // ----------------------------------------------------------------- errors
 void set_error(const std::string &msg);

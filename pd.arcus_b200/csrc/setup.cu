@@ -473,6 +473,49 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   PALLOC(bt.vir_bond, bt.nb);
   PALLOC(bt.e_angle, bt.na);
   PALLOC(bt.e_dih, ndih);
+  // backbone torsion moves and hydrogen flags
+  {
+    std::vector<int2> rax;
+    std::vector<unsigned char> rst;
+    std::vector<int> roff(S + 1, 0), rlast(N, -1);
+    std::vector<unsigned char> ish(N, 0);
+    for (int s = 0; s < S; s++) {
+      const SystemHost &h = *systems[s];
+      int o = p->atom_off[s], r0 = (int)rax.size();
+      for (size_t k = 0; k + 1 < h.rot_axis.size(); k += 2) {
+        rax.push_back(make_int2(o + h.rot_axis[k], o + h.rot_axis[k + 1]));
+        rst.push_back(h.rot_start[k / 2]);
+      }
+      roff[s + 1] = (int)rax.size();
+      for (int i = 0; i < h.natoms && !h.rot_last.empty(); i++)
+        rlast[o + i] = h.rot_last[i] < 0 ? -1 : r0 + h.rot_last[i];
+      for (int i = 0; i < h.natoms && !h.is_h.empty(); i++) ish[o + i] = (unsigned char)h.is_h[i];
+    }
+    int2 *rax_d;
+    int *roff_d, *rlast_d;
+    unsigned char *rst_d;
+    PALLOC(rax_d, rax.size());
+    PALLOC(rst_d, rst.size());
+    PALLOC(roff_d, S + 1);
+    PALLOC(rlast_d, N);
+    PALLOC(v.rot_xf, 12 * rax.size());
+    PALLOC(p->is_h, N);
+    if (!rax.empty()) {
+      cudaMemcpyAsync(rax_d, rax.data(), sizeof(int2) * rax.size(), cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(rst_d, rst.data(), rst.size(), cudaMemcpyHostToDevice, st);
+    }
+    cudaMemcpyAsync(roff_d, roff.data(), sizeof(int) * (S + 1), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(rlast_d, rlast.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(p->is_h, ish.data(), N, cudaMemcpyHostToDevice, st);
+    v.rot_axis = rax_d;
+    v.rot_off = roff_d;
+    v.rot_start = rst_d;
+    v.rot_last = rlast_d;
+    p->rot_total = (long long)rax.size();
+    PALLOC(v.bx, N);
+    PALLOC(v.by, N);
+    PALLOC(v.bz, N);
+  }
   v.lpa[0] = v.lpa[1] = v.lpa[2] = 8;
   v.e_chunks = (max_range + 1023) / 1024;
   if (v.e_chunks < 1) v.e_chunks = 1;

@@ -9,6 +9,7 @@ from ._abi import (PdgpuError, UnstableError, lib, last_error, ff_params_default
 from .core import (Context, SystemSpec, WorkSpace, NeighbourList, Hamiltonian,  # noqa: F401
                    ForcefieldBase, Forcefield, FF_Bonded, FF_NonBonded, FF_GeneralizedBorn_Still,
                    ProtocolBase, Energy, Minimisation, MolecularDynamics, J2KCAL_NA)
+from .batch import Batch  # noqa: F401
 
 # the reference's pre-rename aliases used by its example scripts (src/RENAME.log)
 GB_Still = FF_GeneralizedBorn_Still

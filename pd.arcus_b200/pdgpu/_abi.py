@@ -86,6 +86,12 @@ PROTOTYPES = {
                                                ctypes.c_int32, _I, _D, ctypes.c_int32, _I, _I, _D,
                                                ctypes.c_int32, _I, _I, _D]),
     "pdgpu_system_set_hydrogens": (ctypes.c_int, [_CTX, ctypes.c_int32, _I8]),
+    "pdgpu_batch_create": (ctypes.c_int, [_CTX, _I, ctypes.c_int32, _I]),
+    "pdgpu_batch_info": (ctypes.c_int, [_CTX, ctypes.c_int32, _I, _I]),
+    "pdgpu_set_seeds": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64)]),
+    "pdgpu_system_set_torsions": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32, _I]),
+    "pdgpu_save_base_positions": (ctypes.c_int, [_CTX, ctypes.c_int32]),
+    "pdgpu_perturb_torsions": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_double, ctypes.c_uint64, _D]),
     "pdgpu_set_positions": (ctypes.c_int, [_CTX, ctypes.c_int32, _D]),
     "pdgpu_get_positions": (ctypes.c_int, [_CTX, ctypes.c_int32, _D]),
     "pdgpu_set_velocities": (ctypes.c_int, [_CTX, ctypes.c_int32, _D]),

@@ -219,6 +219,50 @@ class WorkSpace:
         self.cur.f[:] = 0
         self.ene.zero()
 
+    # -- backbone phi/psi trial moves (MoleculeBase::setResiduePhiPsi,
+    #    system/molecule.cpp:702-711, applied as increments)
+    def _device(self):
+        if self._sys is None and self._ff is not None:
+            self._ff.ensuresetup()
+        if self._sys is None:
+            raise A.PdgpuError(A.ERR_STATE, "add a forcefield component to this workspace first")
+        if self._pos_dirty:
+            self._push_positions()
+        return self._sys
+
+    def backboneAxes(self):
+        """(N, CA) then (CA, C) of every residue in order: the bonds
+        setResiduePhiPsi turns for phi and psi."""
+        bb = np.asarray(self.spec["backbone_ncac"]).reshape(-1, 3)
+        ax = []
+        for n, ca, c in bb:
+            if n >= 0 and ca >= 0:
+                ax.append((n, ca))
+            if ca >= 0 and c >= 0:
+                ax.append((ca, c))
+        return np.asarray(ax, dtype=np.int32).reshape(-1, 2)
+
+    def setTorsionMoves(self, axes=None):
+        """Register the rotatable bonds of trial moves (default: every
+        residue's phi and psi); returns the rotation count."""
+        sid = self._device()
+        ax = self.backboneAxes() if axes is None else np.asarray(axes, dtype=np.int32).reshape(-1, 2)
+        ax = np.ascontiguousarray(ax, dtype=np.int32)
+        A.check(A.lib().pdgpu_system_set_torsions(self.ctx.ptr, sid, len(ax), A.iptr(ax)))
+        self.nRotations = len(ax)
+        return len(ax)
+
+    def saveBasePositions(self):
+        A.check(A.lib().pdgpu_save_base_positions(self.ctx.ptr, self._device()))
+
+    def perturbTorsions(self, sigma=0.0, trial=0, angles=None):
+        """Positions = base with rotation k turned by angles[k] (rad), or by
+        sigma * N(0,1) from the counter-based RNG (key: Seed, counter: trial)."""
+        sid = self._device()
+        ang = None if angles is None else A.dptr(A.cd(angles))
+        A.check(A.lib().pdgpu_perturb_torsions(self.ctx.ptr, sid, float(sigma), int(trial), ang))
+        self._pull_positions()
+
     def close(self):
         if self._sys is not None and self.ctx.ptr:
             A.lib().pdgpu_system_destroy(self.ctx.ptr, self._sys)

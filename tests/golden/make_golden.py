@@ -13,9 +13,11 @@ Systems (extended builds from the reference's NewProtein, sequences drawn
 uniformly from the 20 standard residues with the stated seed, pre-minimised
 with 500 steepest-descent steps at Rc 12 A unless noted):
   pep8_s1       8 residues, Rc 12, + 3 MD steps per integrator, 20 SD/CG steps
-  pep20_s2      20 residues, Rc 12, + 2 MD steps per integrator, 10 SD/CG steps
+  pep20_s2      20 residues, Rc 12, + 2 MD steps per integrator, 10 SD/CG steps,
+                4 phi/psi trial conformations (sigma 15 deg) with their forces
   pep30_s3_rc16 30 residues, Rc 16 (the large-system cutoff)
-  two_chain_s4  two 12-residue chains 12 A apart, Rc 10 (inter-chain pairs)
+  two_chain_s4  two 12-residue chains 12 A apart, Rc 10 (inter-chain pairs),
+                3 phi/psi trial conformations
   c1_pep64_s0   the 64-residue, seed-0 chain of the small plain-MD workload, Rc 12
   c2_16x80_s2   16 x 80-residue chains on a 4x4 grid 25 A apart (~20.6k atoms),
                 Rc 16: inputs plus reference forces, Born radii and energies
@@ -37,9 +39,9 @@ PARAM = os.path.join(ROOT, "oracle", "_ref", "param")
 
 SYSTEMS = {
     "pep8_s1": dict(nres=[8], seed=1, cutoff=12, premin=500, md=3, min=20),
-    "pep20_s2": dict(nres=[20], seed=2, cutoff=12, premin=500, md=2, min=10),
+    "pep20_s2": dict(nres=[20], seed=2, cutoff=12, premin=500, md=2, min=10, trials=4),
     "pep30_s3_rc16": dict(nres=[30], seed=3, cutoff=16, premin=500),
-    "two_chain_s4": dict(nres=[12, 12], seed=4, cutoff=10, premin=500, grid=(2, 12)),
+    "two_chain_s4": dict(nres=[12, 12], seed=4, cutoff=10, premin=500, grid=(2, 12), trials=3),
     "c1_pep64_s0": dict(nres=[64], seed=0, cutoff=12, premin=500),
     "c2_16x80_s2": dict(nres=[80] * 16, seed=2, cutoff=16, premin=500, grid=(4, 25), drop_nl=True),
 }
@@ -61,6 +63,8 @@ def build(name, spec, keep_dir=None):
         cmd += ["--md", str(spec["md"])]
     if spec.get("min"):
         cmd += ["--min", str(spec["min"])]
+    if spec.get("trials"):
+        cmd += ["--trials", str(spec["trials"]), "--trial-sigma", "15"]
     env = dict(os.environ, PD_PARAM_PATH=PARAM)
     subprocess.check_call(cmd, env=env, stdout=subprocess.DEVNULL)
     arrays = {}
@@ -89,10 +93,67 @@ def build(name, spec, keep_dir=None):
     return os.path.join(HERE, name + ".npz")
 
 
+# Peptide libraries for the batched workloads: separate single-chain systems
+# stored in one file, arrays prefixed "pNN_".  Lengths are drawn with numpy's
+# seeded generator; each peptide is pre-minimised with 200 SD steps.
+#   lib16_amber_s3  16 peptides, lengths floor(exp(U(ln 20, ln 200))), amber99aa, Rc 12,
+#                   2 phi/psi trial conformations each (sigma 15 deg) with their forces
+#   lib16_opls_s4   16 peptides, lengths U{30..150}, oplsaal, Rc 12
+LIBRARIES = {
+    "lib16_amber_s3": dict(n=16, seed=3, dist="loguniform", lo=20, hi=200, param="amber99aa.ff", trials=2),
+    "lib16_opls_s4": dict(n=16, seed=4, dist="uniform", lo=30, hi=150, param="oplsaal.ff"),
+}
+LIB_KEEP_OUT = ("nl_", "f_energypath", "ene_energypath", "atom_epot", "f_gb", "ene_gb", "f_bonded", "ene_bonded")
+
+
+def _lib_member(args):
+    name, k, nres, seed, param, trials = args
+    out = tempfile.mkdtemp(prefix="pdlib_")
+    cmd = [DRIVER, "build", "--out", out, "--nres", str(nres), "--seed", str(seed), "--cutoff", "12",
+           "--premin", "200", "--param", param]
+    if trials:
+        cmd += ["--trials", str(trials), "--trial-sigma", "15"]
+    env = dict(os.environ, PD_PARAM_PATH=PARAM)
+    subprocess.check_call(cmd, env=env, stdout=subprocess.DEVNULL)
+    arrays = {}
+    for fn in sorted(os.listdir(out)):
+        if fn.endswith(".npy") and not fn.startswith(LIB_KEEP_OUT):
+            arrays["p%02d_%s" % (k, fn[:-4])] = np.load(os.path.join(out, fn))
+    meta = {}
+    with open(os.path.join(out, "meta.txt")) as fh:
+        for line in fh:
+            kk, v = line.split(None, 1)
+            meta.setdefault(kk, []).append(v.strip()) if kk == "chain" else meta.__setitem__(kk, v.strip())
+    shutil.rmtree(out)
+    return k, arrays, meta
+
+
+def build_library(name, spec):
+    import multiprocessing as mp
+    if not os.path.exists(DRIVER):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", "-j8"])
+    rng = np.random.default_rng(spec["seed"])
+    if spec["dist"] == "loguniform":
+        lens = np.floor(np.exp(rng.uniform(np.log(spec["lo"]), np.log(spec["hi"]), spec["n"]))).astype(int)
+    else:
+        lens = rng.integers(spec["lo"], spec["hi"] + 1, spec["n"])
+    jobs = [(name, k, int(lens[k]), spec["seed"] * 100 + k, spec["param"], spec.get("trials", 0))
+            for k in range(spec["n"])]
+    arrays, metas = {}, {}
+    with mp.get_context("spawn").Pool(min(8, os.cpu_count() or 1)) as pool:
+        for k, a, m in pool.imap_unordered(_lib_member, jobs):
+            arrays.update(a)
+            metas[k] = m
+    meta = {"name": name, "members": [metas[k] for k in range(spec["n"])], "param": spec["param"]}
+    arrays["meta_json"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+    return os.path.join(HERE, name + ".npz")
+
+
 def main(argv):
-    names = argv[1:] or list(SYSTEMS)
+    names = argv[1:] or (list(SYSTEMS) + list(LIBRARIES))
     for n in names:
-        p = build(n, SYSTEMS[n])
+        p = build(n, SYSTEMS[n]) if n in SYSTEMS else build_library(n, LIBRARIES[n])
         print("%-16s %8.1f KB" % (n, os.path.getsize(p) / 1024.0))
 
 

@@ -146,3 +146,31 @@ def test_off_diagonal_bond_order_correction():
     assert bo[(0, 5)] == 1 and bo[(5, 0)] == 1
     assert bo[(1, 4)] == 3 and bo[(4, 1)] == 3
     assert bo[(0, 1)] == 7 and bo[(2, 3)] == 7
+
+
+@pytest.mark.parametrize("name", [n for n in SMALL if n in ("pep20_s2", "two_chain_s4")])
+def test_trial_moves_match_reference(name):
+    """Backbone phi/psi trial conformations: the oracle's bond-by-bond
+    restatement of MoleculeBase::rotateBond reproduces the reference's
+    setResiduePhiPsi results from the recorded angles.  Not bit-exact: the
+    reference rotates with matrix3x3 products in its own order (~1e-13 A)."""
+    arrays, meta = load_fixture(name)
+    ax = O.backbone_axes(arrays["backbone_ncac"])
+    assert ax.shape[0] == arrays["trial_angles"].shape[1]
+    for t in range(arrays["trial_angles"].shape[0]):
+        x = O.apply_torsions(arrays["pos"], arrays["cov12_ptr"], arrays["cov12_idx"], ax, arrays["trial_angles"][t])
+        assert np.abs(x - arrays["trial_pos"][t]).max() < 1e-10
+        assert np.abs(arrays["trial_pos"][t] - arrays["pos"]).max() > 1.0  # the move did something
+
+
+@pytest.mark.parametrize("name", [n for n in SMALL if n in ("pep20_s2", "two_chain_s4")])
+def test_trial_forces_match_oracle(name):
+    """The reference's single-point forces of each trial conformation agree
+    with the oracle's at the same positions."""
+    S, arrays, meta = _system(name)
+    for t in range(arrays["trial_pos"].shape[0]):
+        x = arrays["trial_pos"][t]
+        ptr, data = S.nlist(x)
+        f, e, _ = S.calc_forces(x, ptr, data)
+        assert rel_rms(f, arrays["trial_f"][t]) < 1e-12
+        assert e["epot"] == pytest.approx(arrays["trial_ene"][t][0], rel=1e-12, abs=1e-30)
