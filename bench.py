@@ -1,12 +1,26 @@
-"""GB MD throughput on one large system, B200.
+"""GB MD throughput on one large system, B200, plus the batched workloads.
 
-Workload (the reference's single-large-system configuration): 16 seeded
-80-residue peptides on a 4x4 grid 25 A apart, 20,566 atoms, built by the
-reference's own builder and pre-minimised (tests/golden/c2_16x80_s2.npz),
+Headline workload (the reference's single-large-system configuration): 16
+seeded 80-residue peptides on a 4x4 grid 25 A apart, 20,566 atoms, built by
+the reference's own builder and pre-minimised (tests/golden/c2_16x80_s2.npz),
 AMBER99 + Still GB (FastMode) + bonded terms, Rc 16 A (inner 13 A),
 neighbour list rebuilt every 10 steps, Langevin dynamics at 1 fs, 300 K,
 friction 1/ps.  A "step" is one MD step: list refresh (every 10th), bonded +
 Born radii + fused GB/LJ/Coulomb + chain-rule forces, integrator.
+
+Extra keys of the same JSON line:
+  batched_sp  512 peptide systems (32 copies of each of the 16 reference-built
+              AMBER99 peptides of tests/golden/lib16_amber_s3.npz, lengths
+              log-uniform 20-200 residues, each copy with its own RNG key)
+              x 64 backbone phi/psi trials (sigma 15 deg) drawn on the device:
+              32,768 energy+force evaluations, Rc 12 A, in 64 batched
+              evaluations of all 512 systems; against the plain path (one
+              system per launch sequence) on a sample.
+  batched_md  256 peptide systems (16 copies of each of the 16 OPLS-AA
+              peptides of tests/golden/lib16_opls_s4.npz, 30-150 residues),
+              Langevin 1 fs, gamma 1/ps, 300 K, Rc 12 A, list every 10 steps,
+              all systems in one CUDA-graph step loop; aggregate ns/day against
+              one system alone.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -29,6 +43,8 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 FIXTURE = os.path.join(ROOT, "tests", "golden", "c2_16x80_s2.npz")
+LIB_SP = os.path.join(ROOT, "tests", "golden", "lib16_amber_s3.npz")
+LIB_MD = os.path.join(ROOT, "tests", "golden", "lib16_opls_s4.npz")
 REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver_timing")
 REF_PARAM = os.path.join(ROOT, "oracle", "_ref", "param")
 DT_FS = 1.0
@@ -48,6 +64,169 @@ def load_fixture():
     arrays = {k: z[k] for k in z.files}
     meta = json.loads(bytes(arrays.pop("meta_json")).decode())
     return arrays, meta
+
+
+def load_library(path):
+    z = np.load(path)
+    meta = json.loads(bytes(z["meta_json"]).decode())
+    out = []
+    for k, m in enumerate(meta["members"]):
+        pre = "p%02d_" % k
+        out.append(({f[len(pre):]: z[f] for f in z.files if f.startswith(pre)}, m))
+    return out
+
+
+def make_ws(pdgpu, arrays, meta, ctx):
+    """WorkSpace + {FF_Bonded, FF_GeneralizedBorn_Still} at the fixture's cutoffs."""
+    ws = pdgpu.WorkSpace(pdgpu.SystemSpec(arrays, meta), ctx)
+    ff = pdgpu.Forcefield(ws)
+    ff.add(pdgpu.FF_Bonded(ws))
+    gb = pdgpu.FF_GeneralizedBorn_Still(ws)
+    gb.Cutoff, gb.InnerCutoff = float(meta["cutoff"]), float(meta["inner"])
+    gb.VdwCutoff, gb.VdwInnerCutoff = float(meta["vdwcut"]), float(meta["vdwinner"])
+    ff.add(gb)
+    ff.ensuresetup()
+    return ws, ff
+
+
+def pctl(xs, q):
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
+
+
+# ---------------------------------------------------------------- batched workloads
+def bench_batched_sp(pdgpu, A, ctx, torch, copies=32, trials=64, plain_trials=2):
+    """Batched single-point evaluations of Monte Carlo trial conformations."""
+    lib = load_library(LIB_SP)
+    L = A.lib()
+    sigma = np.deg2rad(15.0)
+    members = []
+    for c in range(copies):
+        for k, (a, m) in enumerate(lib):
+            ws, ff = make_ws(pdgpu, a, m, ctx)
+            ws.setTorsionMoves()
+            members.append((ws, ff, a, m, c * len(lib) + k))
+    nsys = len(members)
+    b = pdgpu.Batch([ws for ws, *_ in members])
+    b.setSeeds(np.array([1_000_003 * (s + 1) for *_, s in members], dtype=np.uint64))
+    b.saveBasePositions()
+    # parity: the reference's first recorded trial of every peptide
+    ang = [a["trial_angles"][0] for ws, ff, a, m, s in members]
+    b.perturbTorsions(angles=ang)
+    f, e = b.evaluate()
+    worst = 0.0
+    for s, (ws, ff, a, m, _) in enumerate(members[:len(lib)]):
+        fs = b.split(f)[s]
+        ref = a["trial_f"][0]
+        worst = max(worst, float(np.sqrt(np.sum((fs - ref) ** 2) / np.sum(ref ** 2))))
+    lat = []
+    lc0 = ctypes.c_int64(0)
+    L.pdgpu_launch_count(ctx.ptr, ctypes.byref(lc0))
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter()
+    for t in range(trials):
+        t0 = time.perf_counter()
+        b.perturbTorsions(sigma=sigma, trial=t)
+        b.calcNewList()
+        b.calcForces()
+        e = b.energies()
+        lat.append(time.perf_counter() - t0)
+    t_all = time.perf_counter() - t_wall
+    lc1 = ctypes.c_int64(0)
+    L.pdgpu_launch_count(ctx.ptr, ctypes.byref(lc1))
+    evals = nsys * trials
+    # plain path: one system per launch sequence (perturb, list, forces,
+    # read); an untimed first evaluation per system tunes its kernels
+    plain = []
+    torch.cuda.synchronize()
+    t_plain = 0.0
+    n_plain = 0
+    for ws, ff, a, m, s in members:
+        sid = ws._sys
+        A.check(L.pdgpu_save_base_positions(ctx.ptr, sid))
+        A.check(L.pdgpu_nlist_build(ctx.ptr, sid))
+        A.check(L.pdgpu_calc_forces(ctx.ptr, sid))
+        for t in range(plain_trials):
+            t0 = time.perf_counter()
+            A.check(L.pdgpu_perturb_torsions(ctx.ptr, sid, sigma, t, None))
+            A.check(L.pdgpu_nlist_build(ctx.ptr, sid))
+            A.check(L.pdgpu_calc_forces(ctx.ptr, sid))
+            ebuf = np.zeros(A.ENE_COUNT)
+            A.check(L.pdgpu_get_energies(ctx.ptr, sid, A.dptr(ebuf), A.ENE_COUNT))
+            plain.append(time.perf_counter() - t0)
+            t_plain += plain[-1]
+            n_plain += 1
+    atoms = int(b.nAtoms)
+    b.close()
+    for ws, *_ in members:
+        ws.close()
+    return {"metric": "batched GB evals/s", "value": evals / t_all, "unit": "evals/s",
+            "evals": evals, "systems": nsys, "trials_per_system": trials, "atoms_packed": atoms,
+            "batch_latency_ms": {"p50": 1e3 * pctl(lat, 50), "p99": 1e3 * pctl(lat, 99)},
+            "plain_one_system_per_launch": {"value": n_plain / t_plain, "unit": "evals/s", "sample_evals": n_plain,
+                                            "latency_ms": {"p50": 1e3 * pctl(plain, 50), "p99": 1e3 * pctl(plain, 99)}},
+            "speedup_vs_plain": (evals / t_all) / (n_plain / t_plain),
+            "gpu_launches": int(lc1.value - lc0.value),
+            "parity": {"force_rel_rms_vs_fp64_max": worst,
+                       "case": "reference trial 0 of each of the 16 peptides, angles from the reference run"},
+            "timing": "wall clock around perturb + list + forces + energies read-back, per batched evaluation"}
+
+
+def bench_batched_md(pdgpu, A, ctx, torch, copies=16, steps=5000, plain_steps=200):
+    """All systems advanced together in one CUDA-graph step loop."""
+    lib = load_library(LIB_MD)
+    L = A.lib()
+    members = []
+    for c in range(copies):
+        for k, (a, m) in enumerate(lib):
+            ws, ff = make_ws(pdgpu, a, m, ctx)
+            members.append((ws, ff, a, m))
+    nsys = len(members)
+    p = A.md_params_default()
+    p.Integrator, p.UpdateNList, p.UseGraph = A.INTEGRATOR_LANGEVIN, 10, 1
+    p.Timestep, p.FricCoeff, p.TargetTemp, p.Seed = 1e-15, 1e12, 300.0, 77
+    b = pdgpu.Batch([ws for ws, *_ in members])
+    b.calcNewList()
+    total = steps + 20
+    A.check(L.pdgpu_md_init_velocities(ctx.ptr, b._id, 300.0, 77))
+    hist = np.zeros(3 * 20 * nsys)
+    A.check(L.pdgpu_md_run(ctx.ptr, b._id, ctypes.byref(p), 0, 20, total, A.dptr(hist)))  # warm-up + graph
+    lc0 = ctypes.c_int64(0)
+    L.pdgpu_launch_count(ctx.ptr, ctypes.byref(lc0))
+    hist = np.zeros(3 * steps * nsys)
+    A.check(L.pdgpu_md_run(ctx.ptr, b._id, ctypes.byref(p), 20, steps, total, A.dptr(hist)))
+    ms = ctx.last_run_ms()
+    lc1 = ctypes.c_int64(0)
+    L.pdgpu_launch_count(ctx.ptr, ctypes.byref(lc1))
+    h = hist.reshape(steps, nsys, 3) * pdgpu.J2KCAL_NA
+    nat = np.diff(b.offsets)
+    ek_per_atom = h[-100:, :, 1].mean(axis=0) / nat  # kcal/mol per atom
+    t_kin = ek_per_atom / (1.5 * 0.0019872041)        # K
+    agg = nsys * steps * 1e-6 / (ms / 1e3) * 86400.0
+    # one system alone (the plain path), the median-sized peptide
+    order = np.argsort([a["charge"].shape[0] for ws, ff, a, m in members[:len(lib)]])
+    ws, ff, a, m = members[int(order[len(order) // 2])]
+    one = pdgpu.Batch([ws])
+    one.calcNewList()
+    A.check(L.pdgpu_md_init_velocities(ctx.ptr, one._id, 300.0, 78))
+    A.check(L.pdgpu_md_run(ctx.ptr, one._id, ctypes.byref(p), 0, 20, plain_steps + 20, None))
+    A.check(L.pdgpu_md_run(ctx.ptr, one._id, ctypes.byref(p), 20, plain_steps, plain_steps + 20, None))
+    ms1 = ctx.last_run_ms()
+    one_nsday = plain_steps * 1e-6 / (ms1 / 1e3) * 86400.0
+    atoms = int(b.nAtoms)
+    one.close()
+    b.close()
+    for ws, *_ in members:
+        ws.close()
+    return {"metric": "batched GB MD aggregate ns/day", "value": agg, "unit": "ns/day", "systems": nsys,
+            "steps": steps, "atoms_packed": atoms, "ms_per_step": ms / steps,
+            "plain_one_system": {"value": one_nsday, "unit": "ns/day", "atoms": int(a["charge"].shape[0]),
+                                 "steps": plain_steps},
+            "speedup_vs_plain_sequential": agg / one_nsday,
+            "kinetic_temperature_K": {"median": float(np.median(t_kin)), "min": float(t_kin.min()),
+                                      "max": float(t_kin.max())},
+            "finite": bool(np.all(np.isfinite(h))),
+            "gpu_launches": int(lc1.value - lc0.value),
+            "timing": "CUDA events around the device step loop (pdgpu_last_run_ms)"}
 
 
 # ---------------------------------------------------------------- clocks
@@ -162,6 +341,8 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=60, help="bounded CPU sample (steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched workloads")
+    ap.add_argument("--batched-md-steps", type=int, default=5000)
     args = ap.parse_args()
     rank, world, local = rank_info()
     n_gpus = max(args.gpus, world)
@@ -352,6 +533,9 @@ def main():
             "parity": {"force_rel_rms_vs_fp64": force_rms, "epot_abs_err_kcal": de_kcal},
             "gpu_launches": int(lc1.value - lc0.value),
             "clocks": clk, "roofline": roof, "e2e": e2e}
+    if not args.no_batched:
+        line["batched_sp"] = bench_batched_sp(pdgpu, A, ctx, torch)
+        line["batched_md"] = bench_batched_md(pdgpu, A, ctx, torch, steps=args.batched_md_steps)
     if rank == 0 and n_gpus == 1 and not args.no_cpu_baseline:
         try:
             cb = run_reference(args, 1)

@@ -333,6 +333,11 @@ int pdgpu_launch_count(pdgpu_ctx *ctx, int64_t *count);
  * fused pair and chain-rule kernels on the current list; lpa[0..2] receive
  * the picks.  The first force evaluation of a system tunes automatically. */
 int pdgpu_autotune(pdgpu_ctx *ctx, int32_t sys, int32_t *lpa);
+/* Fix the lanes per atom (lpa[0..2], each 4, 8, 16 or 32) instead of
+ * tuning; NULL re-enables tuning at the next evaluation.  Results are
+ * bit-identical run to run for given lanes per atom; with the same lanes a
+ * system's results are bit-identical alone and in any batch. */
+int pdgpu_set_lanes(pdgpu_ctx *ctx, int32_t sys, const int32_t *lpa);
 
 #ifdef __cplusplus
 }

@@ -248,6 +248,13 @@ int pdgpu_ctx_create(int device, pdgpu_ctx **out) {
   }
   pdgpu_ctx *c = new pdgpu_ctx();
   c->device = device;
+  // keep freed pack memory in the device pool (packs come and go with
+  // batches and served jobs); the threshold only stops trimming at syncs
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    unsigned long long keep = ~0ULL;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete c;
@@ -716,18 +723,22 @@ int pdgpu_get_forces(pdgpu_ctx *c, int32_t sys, double *f) {
   }
   Pack &P = *e->pack;
   int n = P.v.n_atoms;
-  std::vector<long long> a(n), b(n), d(n);
-  PDGPU_CUDA(cudaMemcpyAsync(a.data(), P.v.fx, sizeof(long long) * n, cudaMemcpyDeviceToHost, c->st));
-  PDGPU_CUDA(cudaMemcpyAsync(b.data(), P.v.fy, sizeof(long long) * n, cudaMemcpyDeviceToHost, c->st));
-  PDGPU_CUDA(cudaMemcpyAsync(d.data(), P.v.fz, sizeof(long long) * n, cudaMemcpyDeviceToHost, c->st));
+  std::vector<long long> a(3 * (size_t)n);
+  std::vector<double> g(3 * (size_t)n);
+  const long long *fs[3] = {P.v.fx, P.v.fy, P.v.fz};
+  const double *gs[3] = {P.v.gx, P.v.gy, P.v.gz};
+  for (int k = 0; k < 3; k++) {
+    PDGPU_CUDA(cudaMemcpyAsync(a.data() + (size_t)k * n, fs[k], sizeof(long long) * n, cudaMemcpyDeviceToHost,
+                               c->st));
+    PDGPU_CUDA(cudaMemcpyAsync(g.data() + (size_t)k * n, gs[k], sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+  }
   int r = sync_check(c, "get_forces");
   if (r) return r;
-  double s = kInvForceScale * consts().N_per_kcalmolA;
-  for (int i = 0; i < n; i++) {
-    f[3 * i] = (double)a[i] * s;
-    f[3 * i + 1] = (double)b[i] * s;
-    f[3 * i + 2] = (double)d[i] * s;
-  }
+  // the integrator's sum (fixed-point scattered terms + FP64 pair forces)
+  double s = consts().N_per_kcalmolA;
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < 3; k++)
+      f[3 * i + k] = ((double)a[(size_t)k * n + i] * kInvForceScale + g[(size_t)k * n + i]) * s;
   return PDGPU_OK;
 }
 
@@ -803,11 +814,11 @@ static int nlist_enqueue(pdgpu_ctx *c, SysEntry *e, bool size_check) {
     if (total > v.nl_cap) {
       long long cap = total + total / 3 + 4096;
       unsigned *nl = nullptr;
-      cudaError_t ce = cudaMalloc(&nl, sizeof(unsigned) * cap);
+      cudaError_t ce = cudaMallocAsync((void **)&nl, sizeof(unsigned) * cap, c->st);
       if (ce != cudaSuccess) return cuda_fail(ce, "grow neighbour list");
       auto it = std::find(P.allocs.begin(), P.allocs.end(), (void *)v.nl);
       if (it != P.allocs.end()) {
-        cudaFree(*it);
+        cudaFreeAsync(*it, c->st);
         *it = nl;
       }
       P.bytes += (int64_t)(cap - v.nl_cap) * 4;
@@ -896,9 +907,9 @@ static int ensure_tuned(pdgpu_ctx *c, Pack &P) {
   if (P.tuned || P.v.n_atoms == 0 || !P.have_list) return PDGPU_OK;
   const int N = P.v.n_atoms;
   PackView t = P.v;
-  long long *f = nullptr;
+  double *f = nullptr;
   double *ea = nullptr, *en = nullptr;
-  PDGPU_CUDA(cudaMalloc(&f, sizeof(long long) * 3 * (size_t)N));
+  PDGPU_CUDA(cudaMalloc(&f, sizeof(double) * 3 * (size_t)N));
   if (cudaMalloc(&ea, sizeof(double) * AE_COUNT * (size_t)N) != cudaSuccess ||
       cudaMalloc(&en, sizeof(double) * E_COUNT * (size_t)P.v.n_sys) != cudaSuccess) {
     cudaFree(f);
@@ -906,9 +917,9 @@ static int ensure_tuned(pdgpu_ctx *c, Pack &P) {
     set_error("autotune scratch allocation failed");
     return PDGPU_ERR_NOMEM;
   }
-  t.fx = f;
-  t.fy = f + N;
-  t.fz = f + 2 * N;
+  t.gx = f;
+  t.gy = f + N;
+  t.gz = f + 2 * N;
   t.e_atom = ea;
   t.ene = en;
   cudaEvent_t a, b;
@@ -1463,6 +1474,25 @@ int pdgpu_autotune(pdgpu_ctx *c, int32_t sys, int32_t *lpa) {
   e->drop_graph();
   if (lpa)
     for (int q = 0; q < 3; q++) lpa[q] = P.v.lpa[q];
+  return PDGPU_OK;
+}
+
+int pdgpu_set_lanes(pdgpu_ctx *c, int32_t sys, const int32_t *lpa) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  e->drop_graph();
+  if (!lpa) {
+    P.tuned = false;
+    return PDGPU_OK;
+  }
+  for (int q = 0; q < 3; q++)
+    if (lpa[q] != 4 && lpa[q] != 8 && lpa[q] != 16 && lpa[q] != 32) {
+      set_error("lanes per atom must be 4, 8, 16 or 32");
+      return PDGPU_ERR_ARG;
+    }
+  for (int q = 0; q < 3; q++) P.v.lpa[q] = lpa[q];
+  P.tuned = true;
   return PDGPU_OK;
 }
 

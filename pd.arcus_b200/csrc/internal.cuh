@@ -118,7 +118,8 @@ struct PackView {
   const double *inv_mass_si;  // 1 / kg
   const double *mass_si;      // kg
   double *born_d;             // Born radii
-  long long *fx, *fy, *fz;    // fixed-point forces
+  long long *fx, *fy, *fz;    // fixed-point forces of the scattering terms (bonded)
+  double *gx, *gy, *gz;       // pair forces (kcal/mol/A), each atom owned by one lane group
   double *fox, *foy, *foz;    // saved forces (N) for Beeman / minimiser
   double *dirx, *diry, *dirz; // CG directions / old directions
   double *odx, *ody, *odz;
@@ -187,7 +188,8 @@ struct Pack {
   PackView v{};
   std::vector<int> atom_off;     // host copy
   std::vector<SysParams> sp;     // host copy
-  std::vector<void *> allocs;
+  std::vector<void *> allocs;    // stream-ordered (pooled) allocations on `st`
+  cudaStream_t st = nullptr;
   int64_t bytes = 0;
   long long nl_total = -1;       // last known list size (host)
   bool have_list = false;

@@ -9,10 +9,12 @@
 // Layout: a group of LPA lanes (4, 8, 16 or 32; chosen per system by the
 // autotuner) walks atom i's full neighbour row, so one warp serves 32/LPA
 // atoms.  Rows are contiguous uint32 (j<<3|bondorder) entries.  Every atom
-// accumulates only its own force, so no atomics touch j; per-lane partials
-// are converted to 64-bit fixed point and summed with shuffles inside the
-// group, so every result is bit-reproducible run to run and independent of
-// lane order.  Each neighbour costs one 32-byte record gather per kernel plus
+// accumulates only its own force, so no atomics touch j: per-lane FP32
+// partials are summed in FP64 with a fixed shuffle tree inside the group and
+// added to the atom's FP64 pair force by the group's first lane, kernel
+// after kernel in stream order.  Results are bit-reproducible run to run for
+// a given lanes-per-atom, and FP64 keeps the range of clashing trial
+// structures.  Each neighbour costs one 32-byte record gather per kernel plus
 // one 16-byte parameter gather.  The fused pass evaluates the GB and the
 // vacuum Coulomb terms without branches (both computed, one selected), so
 // the lanes of a group stay converged.
@@ -41,12 +43,6 @@ __device__ __forceinline__ T group_sum(T x) {
 #pragma unroll
   for (int o = W / 2; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
   return x;
-}
-__device__ __forceinline__ long long to_fixed_force(float f) {
-  // kcal/mol/A -> 2^32 fixed point; saturate far outside any physical range
-  float s = f * (float)kForceScale;
-  s = fminf(fmaxf(s, -9.0e18f), 9.0e18f);
-  return __float2ll_rn(s);
 }
 
 // Reciprocal of a double by one FP32 seed and two Newton-Raphson steps
@@ -108,6 +104,9 @@ __global__ void k_zero(PackView v) {
     v.fx[i] = 0;
     v.fy[i] = 0;
     v.fz[i] = 0;
+    v.gx[i] = 0.0;
+    v.gy[i] = 0.0;
+    v.gz[i] = 0.0;
 #pragma unroll
     for (int k = 0; k < AE_COUNT; k++) v.e_atom[(size_t)k * v.n_atoms + i] = 0.0;
   }
@@ -147,7 +146,9 @@ __global__ void __launch_bounds__(256) k_born(PackView v, int zero_first) {
   if (valid && zero_first && sub < 3) {
     // WorkSpace::zeroForces for this atom (and the record, by the first atom)
     long long *f = sub == 0 ? v.fx : (sub == 1 ? v.fy : v.fz);
+    double *g = sub == 0 ? v.gx : (sub == 1 ? v.gy : v.gz);
     f[i] = 0;
+    g[i] = 0.0;
     if (i == v.atom_off[s])
       for (int k = sub; k < E_COUNT; k += 3)
         if (k != E_EKIN) v.ene[(size_t)s * E_COUNT + k] = 0.0;
@@ -298,17 +299,17 @@ __global__ void __launch_bounds__(256) k_gb_pair(PackView v) {
       fz -= fscal * d.z;
     }
   }
-  const long long sx = group_sum<LPA>(to_fixed_force(fx));
-  const long long sy = group_sum<LPA>(to_fixed_force(fy));
-  const long long sz = group_sum<LPA>(to_fixed_force(fz));
+  const double sx = group_sum<LPA>((double)fx);
+  const double sy = group_sum<LPA>((double)fy);
+  const double sz = group_sum<LPA>((double)fz);
   const double dv = group_sum<LPA>((double)e_vdw);
   const double de = group_sum<LPA>((double)e_el);
   const double dp = group_sum<LPA>((double)e_pol);
   const double dd = group_sum<LPA>((double)deda);
   if (valid && sub == 0) {
-    atomicAdd((unsigned long long *)&v.fx[i], (unsigned long long)sx);
-    atomicAdd((unsigned long long *)&v.fy[i], (unsigned long long)sy);
-    atomicAdd((unsigned long long *)&v.fz[i], (unsigned long long)sz);
+    v.gx[i] += sx;
+    v.gy[i] += sy;
+    v.gz[i] += sz;
     const int N = v.n_atoms;
     double ai_d = v.born_d[i];
     double qd = (double)qi;
@@ -377,13 +378,13 @@ __global__ void __launch_bounds__(256) k_gb_chain(PackView v) {
       }
     }
   }
-  const long long sx = group_sum<LPA>(to_fixed_force(fx));
-  const long long sy = group_sum<LPA>(to_fixed_force(fy));
-  const long long sz = group_sum<LPA>(to_fixed_force(fz));
+  const double sx = group_sum<LPA>((double)fx);
+  const double sy = group_sum<LPA>((double)fy);
+  const double sz = group_sum<LPA>((double)fz);
   if (valid && sub == 0) {
-    atomicAdd((unsigned long long *)&v.fx[i], (unsigned long long)sx);
-    atomicAdd((unsigned long long *)&v.fy[i], (unsigned long long)sy);
-    atomicAdd((unsigned long long *)&v.fz[i], (unsigned long long)sz);
+    v.gx[i] += sx;
+    v.gy[i] += sy;
+    v.gz[i] += sz;
   }
 }
 
@@ -546,16 +547,16 @@ __global__ void __launch_bounds__(256) k_nonbonded(PackView v) {
     fy -= s * d.y;
     fz -= s * d.z;
   }
-  long long sx = group_sum<32>(to_fixed_force(fx));
-  long long sy = group_sum<32>(to_fixed_force(fy));
-  long long sz = group_sum<32>(to_fixed_force(fz));
+  double sx = group_sum<32>((double)fx);
+  double sy = group_sum<32>((double)fy);
+  double sz = group_sum<32>((double)fz);
   double dv = group_sum<32>((double)e_vdw);
   double de = group_sum<32>((double)e_el);
   double dw = group_sum<32>((double)vir);
   if (lane == 0) {
-    atomicAdd((unsigned long long *)&v.fx[i], (unsigned long long)sx);
-    atomicAdd((unsigned long long *)&v.fy[i], (unsigned long long)sy);
-    atomicAdd((unsigned long long *)&v.fz[i], (unsigned long long)sz);
+    v.gx[i] += sx;
+    v.gy[i] += sy;
+    v.gz[i] += sz;
     const int N = v.n_atoms;
     v.e_atom[(size_t)AE_VDW * N + i] = 0.5 * dv + P.vdwcor_e_d;
     v.e_atom[(size_t)AE_ELEC * N + i] = 0.5 * de;

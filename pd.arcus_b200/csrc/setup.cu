@@ -211,7 +211,7 @@ Pack::~Pack() {
   int cur = -1;
   cudaGetDevice(&cur);
   if (cur != device) cudaSetDevice(device);
-  for (void *a : allocs) cudaFree(a);
+  for (void *a : allocs) cudaFreeAsync(a, st);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (cur >= 0 && cur != device) cudaSetDevice(cur);
@@ -219,12 +219,15 @@ Pack::~Pack() {
 
 template <typename T>
 static cudaError_t palloc(Pack *p, T **ptr, size_t count) {
+  // stream-ordered allocation from the device's memory pool: packs are
+  // created and freed often (batches, served jobs) and the pool keeps the
+  // memory instead of returning it to the driver each time
   size_t bytes = sizeof(T) * (count > 0 ? count : 1);
-  cudaError_t e = cudaMalloc((void **)ptr, bytes);
+  cudaError_t e = cudaMallocAsync((void **)ptr, bytes, p->st);
   if (e == cudaSuccess) {
     p->allocs.push_back((void *)*ptr);
     p->bytes += (int64_t)bytes;
-    cudaMemset(*ptr, 0, bytes);
+    e = cudaMemsetAsync(*ptr, 0, bytes, p->st);
   }
   return e;
 }
@@ -248,6 +251,7 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   const Consts &c = consts();
   Pack *p = new Pack();
   p->device = device;
+  p->st = st;
   int S = (int)systems.size();
   int N = 0;
   p->atom_off.push_back(0);
@@ -338,6 +342,9 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   PALLOC(v.xyzp, N);
   PALLOC(v.chainp, N);
   PALLOC(v.born_d, N);
+  PALLOC(v.gx, N);
+  PALLOC(v.gy, N);
+  PALLOC(v.gz, N);
   PALLOC(v.fx, N);
   PALLOC(v.fy, N);
   PALLOC(v.fz, N);

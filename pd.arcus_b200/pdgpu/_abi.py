@@ -121,6 +121,7 @@ PROTOTYPES = {
     "pdgpu_profile_pair_kernels": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32, _D]),
     "pdgpu_launch_count": (ctypes.c_int, [_CTX, _I64]),
     "pdgpu_autotune": (ctypes.c_int, [_CTX, ctypes.c_int32, _I]),
+    "pdgpu_set_lanes": (ctypes.c_int, [_CTX, ctypes.c_int32, _I]),
     "pdgpu_nlist_build_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                  ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

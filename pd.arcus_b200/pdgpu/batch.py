@@ -78,6 +78,12 @@ class Batch:
         A.check(A.lib().pdgpu_get_energies(self.ctx.ptr, self._id, A.dptr(e), len(e)))
         return e.reshape(self.nSystems, A.ENE_COUNT)
 
+    def setLanes(self, lpa=None):
+        """Fix the lanes per atom of the Born, fused and chain kernels
+        (None: autotune)."""
+        arr = None if lpa is None else A.iptr(np.ascontiguousarray(lpa, dtype=np.int32))
+        A.check(A.lib().pdgpu_set_lanes(self.ctx.ptr, self._id, arr))
+
     def setSeeds(self, seeds=None):
         if seeds is None:
             A.check(A.lib().pdgpu_set_seeds(self.ctx.ptr, self._id, None))

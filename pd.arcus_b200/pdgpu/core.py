@@ -230,6 +230,12 @@ class WorkSpace:
             self._push_positions()
         return self._sys
 
+    def setLanes(self, lpa=None):
+        """Fix the lanes per atom of the Born, fused and chain kernels
+        (None: autotune at the next evaluation)."""
+        arr = None if lpa is None else A.iptr(np.ascontiguousarray(lpa, dtype=np.int32))
+        A.check(A.lib().pdgpu_set_lanes(self.ctx.ptr, self._device(), arr))
+
     def backboneAxes(self):
         """(N, CA) then (CA, C) of every residue in order: the bonds
         setResiduePhiPsi turns for phi and psi."""

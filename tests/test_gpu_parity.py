@@ -191,6 +191,7 @@ def test_md_graph_and_eager_agree(gpu_ctx):
     outs = []
     for use_graph in (True, False):
         ws, ff, a, _ = make("c1_pep64_s0", gpu_ctx)
+        ws.setLanes((8, 8, 8))  # the same kernel variants in both runs
         md = pdgpu.MolecularDynamics(ff)
         md.Integrator = pdgpu.MolecularDynamics.Langevin
         md.FricCoeff = 1e12
@@ -203,7 +204,8 @@ def test_md_graph_and_eager_agree(gpu_ctx):
         assert np.all(np.isfinite(md.history))
     assert np.array_equal(outs[0][0], outs[1][0])
     assert np.array_equal(outs[0][1], outs[1][1])
-    assert np.array_equal(outs[0][2], outs[1][2])
+    bad = np.argwhere(outs[0][2] != outs[1][2])
+    assert len(bad) == 0, (bad[:10].tolist(), outs[0][2][tuple(bad[0])], outs[1][2][tuple(bad[0])])
 
 
 def test_langevin_temperature_is_sane(gpu_ctx):
