@@ -5,62 +5,9 @@
 #include <map>
 #include <memory>
 
-#include "internal.cuh"
-
-namespace pdgpu {
-const char *last_error_cstr();
-void launch_md_step_impl(const PackView &v, cudaStream_t st, const MDCoef &c, const double *normals,
-                         const int *step_dev, const unsigned char *is_h, const unsigned long long *seeds);
-void launch_pair_counts(const PackView &v, cudaStream_t st, unsigned long long *out);
-void launch_ke_from_velocities(const PackView &v, cudaStream_t st);
-void launch_vel_init_impl(const PackView &v, cudaStream_t st, double temp, const unsigned long long *seeds);
-void launch_min_step(const PackView &v, cudaStream_t st, void *ms, int algorithm, double slope_kcal,
-                     double strict_kcal, double step_size, int nsteps);
-void launch_min_finish(const PackView &v, cudaStream_t st);
-size_t min_state_size();
-void min_state_init(void *host_buf, int n);
-void min_state_read(const void *host_buf, int s, int *taken, int *nan, double *mult);
-}  // namespace pdgpu
+#include "entry.cuh"
 
 using namespace pdgpu;
-
-// A handle: one system (a WorkSpace), or a batch of many packed into one
-// device Pack.  `host` is the first member; a batch shares its members'
-// host data with the systems it was made from.
-struct SysEntry {
-  std::shared_ptr<SystemHost> host;
-  std::vector<std::shared_ptr<SystemHost>> members;
-  std::unique_ptr<Pack> pack;
-  unsigned long long *seeds = nullptr;  // [S] RNG keys
-  bool custom_seeds = false;
-  int nsys() const { return (int)members.size(); }
-  std::vector<const SystemHost *> member_ptrs() const {
-    std::vector<const SystemHost *> m;
-    for (auto &h : members) m.push_back(h.get());
-    return m;
-  }
-  int *step_dev = nullptr;
-  double *hist = nullptr;
-  int hist_cap = 0;
-  void *min_state = nullptr;
-  std::vector<void *> extra;
-  // cached MD block graph
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t gexec = nullptr;
-  std::string gkey;
-  long long gnodes = 0;
-  void drop_graph() {
-    if (gexec) cudaGraphExecDestroy(gexec);
-    if (graph) cudaGraphDestroy(graph);
-    gexec = nullptr;
-    graph = nullptr;
-    gkey.clear();
-  }
-  ~SysEntry() {
-    drop_graph();
-    for (void *p : extra) cudaFree(p);
-  }
-};
 
 struct pdgpu_ctx {
   int device = 0;
@@ -79,27 +26,37 @@ struct pdgpu_ctx {
     cudaSetDevice((c)->device);             \
   } while (0)
 
-static SysEntry *find_sys(pdgpu_ctx *c, int id) {
+// Look a handle up; with `device` its device side is created on first use.
+static int get_sys(pdgpu_ctx *c, int id, bool device, SysEntry **out) {
   auto it = c->sys.find(id);
   if (it == c->sys.end()) {
     set_error("unknown system id " + std::to_string(id));
-    return nullptr;
+    return PDGPU_ERR_ARG;
   }
-  return it->second.get();
+  SysEntry *e = it->second.get();
+  if (device && !e->pack) {
+    int r = entry_materialize(c->device, e);
+    if (r) {
+      e->free_device();
+      return r;
+    }
+  }
+  *out = e;
+  return PDGPU_OK;
 }
-#define GET_SYS(e, c, id)            \
-  SysEntry *e = find_sys((c), (id)); \
-  if (!e) return PDGPU_ERR_ARG
+#define GET_SYS(e, c, id)                  \
+  SysEntry *e = nullptr;                   \
+  do {                                     \
+    int r_ = get_sys((c), (id), true, &e); \
+    if (r_) return r_;                     \
+  } while (0)
+#define GET_SYS_HOST(e, c, id)              \
+  SysEntry *e = nullptr;                    \
+  do {                                      \
+    int r_ = get_sys((c), (id), false, &e); \
+    if (r_) return r_;                      \
+  } while (0)
 
-template <typename T>
-static cudaError_t xalloc(SysEntry *e, T **p, size_t n) {
-  cudaError_t r = cudaMalloc((void **)p, sizeof(T) * (n ? n : 1));
-  if (r == cudaSuccess) {
-    e->extra.push_back(*p);
-    cudaMemset(*p, 0, sizeof(T) * (n ? n : 1));
-  }
-  return r;
-}
 
 static int sync_check(pdgpu_ctx *c, const char *what) {
   cudaError_t e = cudaStreamSynchronize(c->st);
@@ -109,11 +66,10 @@ static int sync_check(pdgpu_ctx *c, const char *what) {
   return PDGPU_OK;
 }
 
-// Device side of a new handle: the pack of its members, the RNG keys and
-// the step counters.
-static int entry_finish(pdgpu_ctx *c, SysEntry *e) {
+namespace pdgpu {
+int entry_materialize(int device, SysEntry *e) {
   std::string err;
-  Pack *p = pack_create(c->device, c->st, e->member_ptrs(), &err);
+  Pack *p = pack_create(device, e->st, e->member_ptrs(), &err);
   if (!p) {
     set_error(err);
     return PDGPU_ERR_NOMEM;
@@ -125,6 +81,7 @@ static int entry_finish(pdgpu_ctx *c, SysEntry *e) {
   }
   return PDGPU_OK;
 }
+}  // namespace pdgpu
 
 extern "C" int pdgpu_get_positions(pdgpu_ctx *c, int32_t sys, double *xyz);
 extern "C" int pdgpu_set_positions(pdgpu_ctx *c, int32_t sys, const double *xyz);
@@ -144,6 +101,7 @@ static int need_single(SysEntry *e, const char *what) {
 // Re-create a handle's pack after its host topology changed (re-setup),
 // keeping positions and velocities.
 static int rebuild_pack(pdgpu_ctx *c, SysEntry *e, int sys) {
+  if (!e->pack) return PDGPU_OK;  // built from the host data on first use
   int n = e->pack->v.n_atoms;
   std::vector<double> x(3 * (size_t)n), vv(3 * (size_t)n);
   int r = pdgpu_get_positions(c, sys, x.data());
@@ -151,7 +109,7 @@ static int rebuild_pack(pdgpu_ctx *c, SysEntry *e, int sys) {
   r = pdgpu_get_velocities(c, sys, vv.data());
   if (r) return r;
   std::string err;
-  Pack *p = pack_create(c->device, c->st, e->member_ptrs(), &err);
+  Pack *p = pack_create(c->device, e->st, e->member_ptrs(), &err);
   if (!p) {
     set_error(err);
     return PDGPU_ERR_NOMEM;
@@ -269,6 +227,7 @@ int pdgpu_ctx_destroy(pdgpu_ctx *c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->st);
   c->sys.clear();
+  cudaStreamSynchronize(c->st);
   cudaStreamDestroy(c->st);
   delete c;
   return PDGPU_OK;
@@ -357,8 +316,7 @@ int pdgpu_system_create(pdgpu_ctx *c, int32_t natoms, const double *charge, cons
     return r;
   }
   host_gb_fixed_terms(h);
-  r = entry_finish(c, e.get());
-  if (r) return r;
+  e->st = c->st;  // the device side is created on first use
   int id = c->next_id++;
   c->sys[id] = std::move(e);
   *sys_id = id;
@@ -389,7 +347,8 @@ int pdgpu_batch_create(pdgpu_ctx *c, const int32_t *sys_ids, int32_t nsys, int32
     return PDGPU_ERR_ARG;
   }
   e->host = e->members[0];
-  int r = entry_finish(c, e.get());
+  e->st = c->st;
+  int r = entry_materialize(c->device, e.get());
   if (r) return r;
   // the batch starts from its members' current positions, velocities and
   // RNG keys (device to device, no host round trip)
@@ -452,7 +411,7 @@ int pdgpu_system_destroy(pdgpu_ctx *c, int32_t sys) {
 
 int pdgpu_system_set_params(pdgpu_ctx *c, int32_t sys, const pdgpu_ff_params *params) {
   CHECK_CTX(c);
-  GET_SYS(e, c, sys);
+  GET_SYS_HOST(e, c, sys);
   int r = validate_params(params);
   if (r) return r;
   if (!params) {
@@ -470,6 +429,7 @@ int pdgpu_system_set_params(pdgpu_ctx *c, int32_t sys, const pdgpu_ff_params *pa
     host_gb_fixed_terms(h);
     return rebuild_pack(c, e, sys);
   }
+  if (!e->pack) return PDGPU_OK;
   e->drop_graph();
   Pack &P = *e->pack;
   pack_set_params(&P, 0, *params);
@@ -483,7 +443,7 @@ int pdgpu_system_set_bonded(pdgpu_ctx *c, int32_t sys, int32_t nb, const int32_t
                             const int32_t *tidx, const int32_t *tterms, const double *tpar, int32_t ni,
                             const int32_t *iidx, const int32_t *iterms, const double *ipar) {
   CHECK_CTX(c);
-  GET_SYS(e, c, sys);
+  GET_SYS_HOST(e, c, sys);
   if (nb < 0 || na < 0 || nt < 0 || ni < 0 || (nb && (!bij || !blk)) || (na && (!aiaj || !akt)) ||
       (nt && (!tidx || !tterms || !tpar)) || (ni && (!iidx || !iterms || !ipar))) {
     set_error("pdgpu_system_set_bonded: bad arguments");
@@ -532,7 +492,7 @@ int pdgpu_system_set_bonded(pdgpu_ctx *c, int32_t sys, int32_t nb, const int32_t
 
 int pdgpu_system_set_hydrogens(pdgpu_ctx *c, int32_t sys, const int8_t *is_h) {
   CHECK_CTX(c);
-  GET_SYS(e, c, sys);
+  GET_SYS_HOST(e, c, sys);
   if (!is_h) {
     set_error("is_h is NULL");
     return PDGPU_ERR_ARG;
@@ -540,13 +500,14 @@ int pdgpu_system_set_hydrogens(pdgpu_ctx *c, int32_t sys, const int8_t *is_h) {
   int r = need_single(e, "pdgpu_system_set_hydrogens");
   if (r) return r;
   e->host->is_h.assign(is_h, is_h + e->host->natoms);
+  if (!e->pack) return PDGPU_OK;
   PDGPU_CUDA(cudaMemcpyAsync(e->pack->is_h, is_h, e->host->natoms, cudaMemcpyHostToDevice, c->st));
   return sync_check(c, "set_hydrogens");
 }
 
 int pdgpu_system_set_torsions(pdgpu_ctx *c, int32_t sys, int32_t nrot, const int32_t *axis) {
   CHECK_CTX(c);
-  GET_SYS(e, c, sys);
+  GET_SYS_HOST(e, c, sys);
   int r = need_single(e, "pdgpu_system_set_torsions");
   if (r) return r;
   SystemHost &h = *e->host;
@@ -778,17 +739,19 @@ int pdgpu_get_atom_epot(pdgpu_ctx *c, int32_t sys, double *epot) {
 int pdgpu_get_energies(pdgpu_ctx *c, int32_t sys, double *ene, int32_t n) {
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
-  if (!ene || n < PDGPU_ENE_COUNT) {
-    set_error("ene must hold PDGPU_ENE_COUNT values");
+  const int S = e->nsys();
+  if (!ene || n < PDGPU_ENE_COUNT * S) {
+    set_error("ene must hold PDGPU_ENE_COUNT values per system");
     return PDGPU_ERR_ARG;
   }
+  static_assert(E_COUNT == PDGPU_ENE_COUNT, "energy record layout");
   Pack &P = *e->pack;
-  double tmp[E_COUNT];
-  PDGPU_CUDA(cudaMemcpyAsync(tmp, P.v.ene, sizeof tmp, cudaMemcpyDeviceToHost, c->st));
+  std::vector<double> tmp((size_t)E_COUNT * S);
+  PDGPU_CUDA(cudaMemcpyAsync(tmp.data(), P.v.ene, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost, c->st));
   int r = sync_check(c, "get_energies");
   if (r) return r;
   double J = consts().J_per_kcalmol;
-  for (int k = 0; k < E_COUNT; k++) ene[k] = tmp[k] * J;
+  for (size_t k = 0; k < tmp.size(); k++) ene[k] = tmp[k] * J;
   return PDGPU_OK;
 }
 
@@ -973,7 +936,9 @@ static void gb_forces_enqueue(pdgpu_ctx *c, Pack &P) {
   launch_energy(P.v, c->st, EM_PAIR_GB);
 }
 
-static bool has_bonded(const Pack &P) { return P.v.bt.nb + P.v.bt.na + P.v.bt.nt + P.v.bt.ni > 0; }
+}  // extern "C"
+bool pdgpu::has_bonded(const Pack &P) { return P.v.bt.nb + P.v.bt.na + P.v.bt.nt + P.v.bt.ni > 0; }
+extern "C" {
 
 int pdgpu_gb_forces(pdgpu_ctx *c, int32_t sys) {
   CHECK_CTX(c);
@@ -1042,14 +1007,16 @@ int pdgpu_bonded_forces(pdgpu_ctx *c, int32_t sys) {
 // Forcefield::calcForces for {FF_Bonded, FF_GeneralizedBorn_Still}: the
 // Born-radius kernel zeroes forces and record first; one energy reduction.
 // extra_mode adds EM_KINETIC / EM_RECORD inside an MD step.
-static void calc_forces_enqueue(pdgpu_ctx *c, SysEntry *e, bool reduce = true) {
+}  // extern "C"
+void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce) {
   Pack &P = *e->pack;
-  launch_born_radii(P.v, c->st, true);
-  if (has_bonded(P)) launch_bonded_terms(P.v, c->st);
-  launch_gb_pair(P.v, c->st);
-  launch_gb_chain(P.v, c->st);
-  if (reduce) launch_energy(P.v, c->st, EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0));
+  launch_born_radii(P.v, st, true);
+  if (has_bonded(P)) launch_bonded_terms(P.v, st);
+  launch_gb_pair(P.v, st);
+  launch_gb_chain(P.v, st);
+  if (reduce) launch_energy(P.v, st, EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0));
 }
+extern "C" {
 
 int pdgpu_calc_forces(pdgpu_ctx *c, int32_t sys) {
   CHECK_CTX(c);
@@ -1058,7 +1025,7 @@ int pdgpu_calc_forces(pdgpu_ctx *c, int32_t sys) {
   int r = need_list(P);
   if (r) return r;
   if ((r = ensure_tuned(c, P))) return r;
-  calc_forces_enqueue(c, e);
+  calc_forces_enqueue(c->st, e, true);
   return sync_check(c, "calc_forces");
 }
 
@@ -1073,7 +1040,8 @@ static int default_seeds(pdgpu_ctx *c, SysEntry *e, unsigned long long base) {
   return PDGPU_OK;
 }
 
-static MDCoef md_coef(const pdgpu_md_params *p, int step, int steps) {
+}  // extern "C"
+MDCoef pdgpu::md_coef(const pdgpu_md_params *p, int step, int steps) {
   // the coefficient branches of md.cpp:961-1000
   MDCoef c;
   memset(&c, 0, sizeof c);
@@ -1113,8 +1081,10 @@ static MDCoef md_coef(const pdgpu_md_params *p, int step, int steps) {
   }
   return c;
 }
+extern "C" {
 
-static int validate_md(const pdgpu_md_params *p) {
+}  // extern "C"
+int pdgpu::validate_md(const pdgpu_md_params *p) {
   if (!p || !(p->Timestep > 0) || p->Integrator < 0 || p->Integrator > 3 || !(p->TargetTemp >= 0) ||
       (p->Integrator == PDGPU_INTEGRATOR_LANGEVIN && !(p->FricCoeff > 0))) {
     set_error("invalid MD parameters");
@@ -1122,6 +1092,7 @@ static int validate_md(const pdgpu_md_params *p) {
   }
   return PDGPU_OK;
 }
+extern "C" {
 
 int pdgpu_md_step_with_normals(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t step,
                                int32_t total_steps, const double *normals) {
@@ -1154,13 +1125,15 @@ int pdgpu_md_init_velocities(pdgpu_ctx *c, int32_t sys, double temperature, uint
 
 // one MD step enqueue: forces, integrate, one energy reduction that also
 // records the step and advances the device step counter (7 launches)
-static void md_step_enqueue(pdgpu_ctx *c, SysEntry *e, const MDCoef &k) {
+}  // extern "C"
+void pdgpu::md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k) {
   Pack &P = *e->pack;
-  calc_forces_enqueue(c, e, false);
-  launch_md_step_impl(P.v, c->st, k, nullptr, e->step_dev, P.is_h, e->seeds);
-  launch_energy(P.v, c->st, EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0) | EM_KINETIC | EM_RECORD, e->hist,
+  calc_forces_enqueue(st, e, false);
+  launch_md_step_impl(P.v, st, k, nullptr, e->step_dev, P.is_h, e->seeds);
+  launch_energy(P.v, st, EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0) | EM_KINETIC | EM_RECORD, e->hist,
                 e->step_dev);
 }
+extern "C" {
 
 int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t first_step, int32_t steps,
                  int32_t total_steps, double *history) {
@@ -1230,15 +1203,14 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
                  P.radix_passes, (int)e->host->params.FastMode, v.lpa[0], v.lpa[1], v.lpa[2]);
         if (!e->gexec || e->gkey != key) {
           e->drop_graph();
-          long long before = launch_counter();
+          begin_capture_count();
           PDGPU_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
           launch_nlist_count(P, c->st);
           launch_nlist_fill(P, c->st);
-          for (int q = 0; q < block; q++) md_step_enqueue(c, e, k);
+          for (int q = 0; q < block; q++) md_step_enqueue(c->st, e, k);
           PDGPU_CUDA(cudaStreamEndCapture(c->st, &e->graph));
           PDGPU_CUDA(cudaGraphInstantiate(&e->gexec, e->graph, 0));
-          e->gnodes = launch_counter() - before;
-          launch_counter() = before;  // capture ran nothing
+          e->gnodes = end_capture_count();
           e->gkey = key;
         }
         PDGPU_CUDA(cudaGraphLaunch(e->gexec, c->st));
@@ -1248,7 +1220,7 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
           launch_nlist_count(P, c->st);
           launch_nlist_fill(P, c->st);
         }
-        for (int q = 0; q < block; q++) md_step_enqueue(c, e, k);
+        for (int q = 0; q < block; q++) md_step_enqueue(c->st, e, k);
       }
       int flags[F_COUNT];
       PDGPU_CUDA(cudaMemcpyAsync(flags, v.flags, sizeof flags, cudaMemcpyDeviceToHost, c->st));
@@ -1305,9 +1277,8 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
   const Consts &k = consts();
   const int S = e->nsys();
   if (!e->min_state) {
-    void *m = nullptr;
-    PDGPU_CUDA(cudaMalloc(&m, min_state_size() * S));
-    e->extra.push_back(m);
+    unsigned char *m = nullptr;
+    PDGPU_CUDA(xalloc(e, &m, min_state_size() * S));
     e->min_state = m;
   }
   std::vector<unsigned char> hs(min_state_size() * S);
@@ -1347,7 +1318,7 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
         launch_nlist_count(P, c->st);
         launch_nlist_fill(P, c->st);
       }
-      calc_forces_enqueue(c, e);
+      calc_forces_enqueue(c->st, e, true);
       launch_min_step(v, c->st, e->min_state, p->Algorithm, slope, strict, p->StepSize, steps);
     }
     int flags[F_COUNT];
@@ -1389,7 +1360,7 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
   P.nlist_counter = counter0 + iter;
   // cur = old; recompute the energies (minimise.cpp:172-176)
   launch_min_finish(v, c->st);
-  calc_forces_enqueue(c, e);
+  calc_forces_enqueue(c->st, e, true);
   cudaEventRecord(P.ev1, c->st);
   r = sync_check(c, "minimise finish");
   if (r) return r;
@@ -1502,7 +1473,7 @@ int pdgpu_launch_count(pdgpu_ctx *c, int64_t *count) {
     set_error("count is NULL");
     return PDGPU_ERR_ARG;
   }
-  *count = launch_counter();
+  *count = launch_counter().load();
   return PDGPU_OK;
 }
 

@@ -1,0 +1,99 @@
+// Handles behind the C ABI: a system, a batch of systems, or a served job.
+// Shared by the ABI (api.cu) and the request loop (serve.cu).
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace pdgpu {
+const char *last_error_cstr();
+void launch_md_step_impl(const PackView &v, cudaStream_t st, const MDCoef &c, const double *normals,
+                         const int *step_dev, const unsigned char *is_h, const unsigned long long *seeds);
+void launch_pair_counts(const PackView &v, cudaStream_t st, unsigned long long *out);
+void launch_ke_from_velocities(const PackView &v, cudaStream_t st);
+void launch_vel_init_impl(const PackView &v, cudaStream_t st, double temp, const unsigned long long *seeds);
+void launch_min_step(const PackView &v, cudaStream_t st, void *ms, int algorithm, double slope_kcal,
+                     double strict_kcal, double step_size, int nsteps);
+void launch_min_finish(const PackView &v, cudaStream_t st);
+size_t min_state_size();
+void min_state_init(void *host_buf, int n);
+void min_state_read(const void *host_buf, int s, int *taken, int *nan, double *mult);
+}  // namespace pdgpu
+
+// A handle: one system (a WorkSpace), or a batch of many packed into one
+// device Pack.  `host` is the first member; a batch shares its members'
+// host data with the systems it was made from.  The device side (`pack` and
+// the small buffers) is created on first use and lives on stream `st`;
+// every allocation is stream-ordered so that creating and dropping handles
+// never synchronises the device.
+struct SysEntry {
+  std::shared_ptr<pdgpu::SystemHost> host;
+  std::vector<std::shared_ptr<pdgpu::SystemHost>> members;
+  std::unique_ptr<pdgpu::Pack> pack;
+  cudaStream_t st = nullptr;
+  unsigned long long *seeds = nullptr;  // [S] RNG keys
+  bool custom_seeds = false;
+  int nsys() const { return (int)members.size(); }
+  std::vector<const pdgpu::SystemHost *> member_ptrs() const {
+    std::vector<const pdgpu::SystemHost *> m;
+    for (auto &h : members) m.push_back(h.get());
+    return m;
+  }
+  int *step_dev = nullptr;
+  double *hist = nullptr;
+  int hist_cap = 0;
+  void *min_state = nullptr;
+  std::vector<void *> extra;
+  // cached MD block graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  std::string gkey;
+  long long gnodes = 0;
+  void drop_graph() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    gexec = nullptr;
+    graph = nullptr;
+    gkey.clear();
+  }
+  void free_device() {
+    drop_graph();
+    for (void *p : extra) cudaFreeAsync(p, st);
+    extra.clear();
+    seeds = nullptr;
+    step_dev = nullptr;
+    hist = nullptr;
+    hist_cap = 0;
+    min_state = nullptr;
+    pack.reset();
+  }
+  ~SysEntry() { free_device(); }
+};
+
+// stream-ordered, zero-filled allocation owned by the entry
+template <typename T>
+static inline cudaError_t xalloc(SysEntry *e, T **p, size_t n) {
+  size_t bytes = sizeof(T) * (n ? n : 1);
+  cudaError_t r = cudaMallocAsync((void **)p, bytes, e->st);
+  if (r == cudaSuccess) {
+    e->extra.push_back(*p);
+    r = cudaMemsetAsync(*p, 0, bytes, e->st);
+  }
+  return r;
+}
+
+namespace pdgpu {
+// Device side of a handle: the pack of its members, the RNG keys and the
+// step counters (enqueued on e->st, no synchronisation).
+int entry_materialize(int device, SysEntry *e);
+bool has_bonded(const Pack &P);
+// Forcefield::calcForces for {FF_Bonded, FF_GeneralizedBorn_Still}: zero,
+// Born radii, bonded, fused pair, chain rule; one energy reduction if reduce.
+void calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce);
+// one MD step: forces, integrator, energy record (+ step counter advance)
+void md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k);
+MDCoef md_coef(const pdgpu_md_params *p, int step, int steps);
+int validate_md(const pdgpu_md_params *p);
+}  // namespace pdgpu

@@ -423,8 +423,21 @@ void launch_md_step_impl(const PackView &v, cudaStream_t st, const MDCoef &c, co
   if (v.n_atoms) PDGPU_LAUNCH(k_md_step, (v.n_atoms + 255) / 256, 256, 0, st, v, d, normals, step_dev);
 }
 
-long long &launch_counter() {
-  static long long n = 0;
+std::atomic<long long> &launch_counter() {
+  static std::atomic<long long> n{0};
+  return n;
+}
+static thread_local long long tl_captured = -1;  // -1: this thread is not capturing
+void count_launch() {
+  if (tl_captured >= 0)
+    tl_captured++;
+  else
+    launch_counter()++;
+}
+void begin_capture_count() { tl_captured = 0; }
+long long end_capture_count() {
+  long long n = tl_captured;
+  tl_captured = -1;
   return n;
 }
 void launch_ke_from_velocities(const PackView &v, cudaStream_t st) {

@@ -9,6 +9,8 @@
 // to the reference's SI units (J, N) happens only at the C-ABI boundary.
 #pragma once
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include <stdint.h>
 
 #include <string>
@@ -302,15 +304,20 @@ int cuda_fail(cudaError_t e, const char *what);
 
 }  // namespace pdgpu
 
-// Every kernel launch goes through PDGPU_LAUNCH so the context can report
+// Every kernel launch goes through PDGPU_LAUNCH so the library can report
 // how many of its kernels ran (graph replays add their kernel-node count).
+// Launches a thread makes while it captures a graph are counted for the
+// graph, not as runs.
 namespace pdgpu {
-long long &launch_counter();
+std::atomic<long long> &launch_counter();
+void count_launch();
+void begin_capture_count();
+long long end_capture_count();
 }
 #define PDGPU_LAUNCH(kern, grid, block, smem, stream, ...)          \
   do {                                                             \
     kern<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);      \
-    ::pdgpu::launch_counter()++;                                   \
+    ::pdgpu::count_launch();                                       \
   } while (0)
 
 #define PDGPU_CUDA(call)                                      \
