@@ -311,6 +311,81 @@ void pdgpu_min_params_default(pdgpu_min_params *p);
 int pdgpu_minimise_run(pdgpu_ctx *ctx, int32_t sys, const pdgpu_min_params *p,
                        int32_t steps, int32_t *steps_taken);
 
+/* ------------------------------------------------------------------ serving
+ * A request loop for single-point, minimisation and MD jobs of different
+ * sizes (no reference counterpart; each job runs the reference's protocol:
+ * Energy::runcore energy.cpp:14-20, Minimisation::runcore minimise.cpp:
+ * 99-179, MolecularDynamics::run_core md.cpp:202-267).  A worker thread owns
+ * the device side of every admitted job: each job has its own stream and
+ * keeps its coordinates, neighbour list, Born radii and protocol state on
+ * the device until it finishes; jobs that arrive while others run are
+ * admitted as soon as a stream slot is free and their memory fits under the
+ * HBM budget (first fit in arrival order), and their kernels overlap with
+ * the running jobs'.  All jobs use the same fixed lanes per atom, so a
+ * job's results are bit-identical alone and in any mix.  The server is
+ * driven from one host thread (the context's). */
+typedef struct pdgpu_server pdgpu_server;
+typedef struct {
+  int64_t hbm_budget;   /* device bytes the admitted jobs may hold together   */
+  int32_t max_active;   /* jobs on the device at once (one stream each)       */
+  int32_t lanes[3];     /* lanes per atom: Born, fused pair, chain (4..32)    */
+} pdgpu_serve_params;
+void pdgpu_serve_params_default(pdgpu_serve_params *p);
+
+#define PDGPU_JOB_ENERGY 0    /* list + Forcefield::calcForces + energies          */
+#define PDGPU_JOB_MINIMISE 1  /* Minimisation::runcore, `steps` steps               */
+#define PDGPU_JOB_MD 2        /* MolecularDynamics::run_core, `steps` steps from
+                                 velocities drawn at init_temp with md.Seed         */
+typedef struct {
+  int32_t kind;
+  int32_t steps;
+  pdgpu_md_params md;
+  pdgpu_min_params min;
+  double init_temp;
+} pdgpu_job;
+
+#define PDGPU_JOB_QUEUED 0
+#define PDGPU_JOB_RUNNING 1
+#define PDGPU_JOB_DONE 2
+#define PDGPU_JOB_FAILED 3
+typedef struct {
+  int32_t state;        /* PDGPU_JOB_*                                          */
+  int32_t status;       /* pdgpu status of a failed job                        */
+  int32_t kind;
+  int32_t natoms;
+  int32_t steps_done;   /* MD steps / minimiser steps (-1: NaN) / 1 for energy */
+  int32_t _reserved;
+  double t_queue_ms;    /* submit -> admitted (-1 if not yet)                  */
+  double t_run_ms;      /* admitted -> finished                                 */
+  double t_total_ms;    /* submit -> finished: the job's latency               */
+} pdgpu_job_info;
+
+typedef struct {
+  int64_t submitted, completed, failed;
+  int32_t active, queued, peak_active, _reserved;
+  int64_t bytes_in_use, peak_bytes;
+} pdgpu_serve_stats;
+
+int pdgpu_serve_create(pdgpu_ctx *ctx, const pdgpu_serve_params *p, pdgpu_server **out);
+/* Queue a job on system `sys` (its topology and settings; a single system)
+ * starting from positions xyz[3*natoms].  PDGPU_ERR_BUDGET if the job alone
+ * cannot fit the budget. */
+int pdgpu_serve_submit(pdgpu_server *srv, int32_t sys, const pdgpu_job *job, const double *xyz,
+                       int64_t *job_id);
+/* Block until the job finishes (timeout_s < 0: no limit); returns the job's
+ * status. */
+int pdgpu_serve_wait(pdgpu_server *srv, int64_t job_id, double timeout_s);
+int pdgpu_serve_info(pdgpu_server *srv, int64_t job_id, pdgpu_job_info *info);
+/* Final positions (A), forces (N), energy record (J, PDGPU_ENE_COUNT) and,
+ * for MD, the per-step epot/ekin/etot history (J, 3*steps); any may be NULL. */
+int pdgpu_serve_result(pdgpu_server *srv, int64_t job_id, double *xyz, double *f, double *ene,
+                       double *history);
+/* Forget a finished job (its host buffers return to the pool). */
+int pdgpu_serve_release(pdgpu_server *srv, int64_t job_id);
+int pdgpu_serve_get_stats(pdgpu_server *srv, pdgpu_serve_stats *stats);
+/* Let the admitted jobs finish, fail the queued ones, stop the worker. */
+int pdgpu_serve_destroy(pdgpu_server *srv);
+
 /* ------------------------------------------------------------------ timing */
 /* Device time (ms) of the last pdgpu_md_run / pdgpu_minimise_run call,
  * measured with CUDA events on the context stream. */

@@ -67,9 +67,9 @@ static int sync_check(pdgpu_ctx *c, const char *what) {
 }
 
 namespace pdgpu {
-int entry_materialize(int device, SysEntry *e) {
+int entry_materialize(int device, SysEntry *e, bool sync) {
   std::string err;
-  Pack *p = pack_create(device, e->st, e->member_ptrs(), &err);
+  Pack *p = pack_create(device, e->st, e->member_ptrs(), &err, sync);
   if (!p) {
     set_error(err);
     return PDGPU_ERR_NOMEM;
@@ -87,6 +87,24 @@ extern "C" int pdgpu_get_positions(pdgpu_ctx *c, int32_t sys, double *xyz);
 extern "C" int pdgpu_set_positions(pdgpu_ctx *c, int32_t sys, const double *xyz);
 extern "C" int pdgpu_get_velocities(pdgpu_ctx *c, int32_t sys, double *v);
 extern "C" int pdgpu_set_velocities(pdgpu_ctx *c, int32_t sys, const double *v);
+
+namespace pdgpu {
+int ctx_device(pdgpu_ctx *c) { return c->device; }
+// the host data of a single system (for the request loop's job templates)
+int ctx_system_host(pdgpu_ctx *c, int sys, std::shared_ptr<SystemHost> *out) {
+  auto it = c->sys.find(sys);
+  if (it == c->sys.end()) {
+    set_error("unknown system id " + std::to_string(sys));
+    return PDGPU_ERR_ARG;
+  }
+  if (it->second->nsys() != 1) {
+    set_error("a job runs on a single system, not a batch");
+    return PDGPU_ERR_ARG;
+  }
+  *out = it->second->host;
+  return PDGPU_OK;
+}
+}  // namespace pdgpu
 
 // Topology and settings are edited on single systems; a batch takes its
 // members' topology, settings and state when it is created.
@@ -765,6 +783,27 @@ int pdgpu_zero_forces(pdgpu_ctx *c, int32_t sys) {
 // ------------------------------------------------------------ kernels
 // enqueue a full list rebuild; when `size_check` the host reads the count
 // and grows the list buffer first (one synchronisation)
+}  // extern "C"
+// Grow the list buffer (stream-ordered) to hold `total` entries plus slack.
+int pdgpu::nlist_reserve(Pack &P, long long total, cudaStream_t st) {
+  PackView &v = P.v;
+  if (total <= v.nl_cap) return PDGPU_OK;
+  long long cap = total + total / 3 + 4096;
+  unsigned *nl = nullptr;
+  cudaError_t ce = cudaMallocAsync((void **)&nl, sizeof(unsigned) * cap, st);
+  if (ce != cudaSuccess) return cuda_fail(ce, "grow neighbour list");
+  auto it = std::find(P.allocs.begin(), P.allocs.end(), (void *)v.nl);
+  if (it != P.allocs.end()) {
+    cudaFreeAsync(*it, st);
+    *it = nl;
+  }
+  P.bytes += (int64_t)(cap - v.nl_cap) * 4;
+  v.nl = nl;
+  v.nl_cap = cap;
+  return PDGPU_OK;
+}
+extern "C" {
+
 static int nlist_enqueue(pdgpu_ctx *c, SysEntry *e, bool size_check) {
   Pack &P = *e->pack;
   PackView &v = P.v;
@@ -774,20 +813,8 @@ static int nlist_enqueue(pdgpu_ctx *c, SysEntry *e, bool size_check) {
     PDGPU_CUDA(cudaMemcpyAsync(&total, v.row_start + v.n_atoms, sizeof total, cudaMemcpyDeviceToHost, c->st));
     int r = sync_check(c, "nlist count");
     if (r) return r;
-    if (total > v.nl_cap) {
-      long long cap = total + total / 3 + 4096;
-      unsigned *nl = nullptr;
-      cudaError_t ce = cudaMallocAsync((void **)&nl, sizeof(unsigned) * cap, c->st);
-      if (ce != cudaSuccess) return cuda_fail(ce, "grow neighbour list");
-      auto it = std::find(P.allocs.begin(), P.allocs.end(), (void *)v.nl);
-      if (it != P.allocs.end()) {
-        cudaFreeAsync(*it, c->st);
-        *it = nl;
-      }
-      P.bytes += (int64_t)(cap - v.nl_cap) * 4;
-      v.nl = nl;
-      v.nl_cap = cap;
-    }
+    r = nlist_reserve(P, total, c->st);
+    if (r) return r;
     P.nl_total = total;
     PDGPU_CUDA(cudaMemsetAsync(v.flags + F_NL_OVERFLOW, 0, sizeof(int), c->st));
   }

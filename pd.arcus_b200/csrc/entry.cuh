@@ -86,8 +86,8 @@ static inline cudaError_t xalloc(SysEntry *e, T **p, size_t n) {
 
 namespace pdgpu {
 // Device side of a handle: the pack of its members, the RNG keys and the
-// step counters (enqueued on e->st, no synchronisation).
-int entry_materialize(int device, SysEntry *e);
+// step counters, enqueued on e->st (with `sync`, waited for).
+int entry_materialize(int device, SysEntry *e, bool sync = true);
 bool has_bonded(const Pack &P);
 // Forcefield::calcForces for {FF_Bonded, FF_GeneralizedBorn_Still}: zero,
 // Born radii, bonded, fused pair, chain rule; one energy reduction if reduce.
@@ -95,5 +95,7 @@ void calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce);
 // one MD step: forces, integrator, energy record (+ step counter advance)
 void md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k);
 MDCoef md_coef(const pdgpu_md_params *p, int step, int steps);
+// grow a pack's list buffer to hold `total` entries (stream-ordered)
+int nlist_reserve(Pack &P, long long total, cudaStream_t st);
 int validate_md(const pdgpu_md_params *p);
 }  // namespace pdgpu

@@ -213,8 +213,10 @@ struct Pack {
 };
 
 // Build a device Pack from host systems (atoms concatenated in order).
+// With `sync` the call waits for the uploads on `st` (reporting their
+// errors); without, everything stays enqueued on `st`.
 Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHost *> &systems,
-                  std::string *err);
+                  std::string *err, bool sync = true);
 void pack_set_params(Pack *p, int s, const pdgpu_ff_params &prm);
 SysParams make_sys_params(const pdgpu_ff_params &p);
 

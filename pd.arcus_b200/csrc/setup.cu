@@ -247,7 +247,7 @@ void pack_set_params(Pack *p, int s, const pdgpu_ff_params &prm) {
   } while (0)
 
 Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHost *> &systems,
-                  std::string *err) {
+                  std::string *err, bool sync) {
   const Consts &c = consts();
   Pack *p = new Pack();
   p->device = device;
@@ -549,7 +549,7 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   }
   cudaEventCreate(&p->ev0);
   cudaEventCreate(&p->ev1);
-  cudaError_t e = cudaStreamSynchronize(st);
+  cudaError_t e = sync ? cudaStreamSynchronize(st) : cudaGetLastError();
   if (e != cudaSuccess) {
     if (err) *err = std::string("pack upload failed: ") + cudaGetErrorString(e);
     delete p;

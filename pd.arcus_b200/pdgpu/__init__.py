@@ -10,6 +10,7 @@ from .core import (Context, SystemSpec, WorkSpace, NeighbourList, Hamiltonian,  
                    ForcefieldBase, Forcefield, FF_Bonded, FF_NonBonded, FF_GeneralizedBorn_Still,
                    ProtocolBase, Energy, Minimisation, MolecularDynamics, J2KCAL_NA)
 from .batch import Batch  # noqa: F401
+from .serve import Server  # noqa: F401
 
 # the reference's pre-rename aliases used by its example scripts (src/RENAME.log)
 GB_Still = FF_GeneralizedBorn_Still

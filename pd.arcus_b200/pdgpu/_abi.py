@@ -63,6 +63,30 @@ class MinParams(ctypes.Structure):
                 ("Strictness", ctypes.c_double)]
 
 
+class ServeParams(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_int64), ("max_active", ctypes.c_int32), ("lanes", ctypes.c_int32 * 3)]
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("steps", ctypes.c_int32), ("md", MDParams), ("min", MinParams),
+                ("init_temp", ctypes.c_double)]
+
+
+class JobInfo(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int32), ("status", ctypes.c_int32), ("kind", ctypes.c_int32),
+                ("natoms", ctypes.c_int32), ("steps_done", ctypes.c_int32), ("_reserved", ctypes.c_int32),
+                ("t_queue_ms", ctypes.c_double), ("t_run_ms", ctypes.c_double), ("t_total_ms", ctypes.c_double)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("active", ctypes.c_int32), ("queued", ctypes.c_int32), ("peak_active", ctypes.c_int32),
+                ("_reserved", ctypes.c_int32), ("bytes_in_use", ctypes.c_int64), ("peak_bytes", ctypes.c_int64)]
+
+
+JOB_ENERGY, JOB_MINIMISE, JOB_MD = 0, 1, 2
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int32)
 _I8 = ctypes.POINTER(ctypes.c_int8)
@@ -122,6 +146,15 @@ PROTOTYPES = {
     "pdgpu_launch_count": (ctypes.c_int, [_CTX, _I64]),
     "pdgpu_autotune": (ctypes.c_int, [_CTX, ctypes.c_int32, _I]),
     "pdgpu_set_lanes": (ctypes.c_int, [_CTX, ctypes.c_int32, _I]),
+    "pdgpu_serve_params_default": (None, [ctypes.POINTER(ServeParams)]),
+    "pdgpu_serve_create": (ctypes.c_int, [_CTX, ctypes.POINTER(ServeParams), ctypes.POINTER(ctypes.c_void_p)]),
+    "pdgpu_serve_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(Job), _D, _I64]),
+    "pdgpu_serve_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double]),
+    "pdgpu_serve_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(JobInfo)]),
+    "pdgpu_serve_result": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, _D, _D, _D, _D]),
+    "pdgpu_serve_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
+    "pdgpu_serve_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServeStats)]),
+    "pdgpu_serve_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "pdgpu_nlist_build_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                  ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

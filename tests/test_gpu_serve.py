@@ -1,0 +1,163 @@
+"""GPU: the request loop (pdgpu_serve_*).
+
+A served job must give the same results alone and in a mix of overlapping
+jobs -- bit for bit, since every job runs the same kernels with the same
+fixed lanes per atom on its own device state -- and the same results as
+the plain calls (pdgpu_nlist_build + pdgpu_calc_forces, pdgpu_minimise_run,
+pdgpu_md_run) with those lanes.  Single-point forces also match the
+reference's FP64 forces (relative force RMS 1e-5).
+"""
+import numpy as np
+import pytest
+
+from conftest import build_workspace, load_library, rel_rms
+
+pytestmark = pytest.mark.gpu
+
+LANES = (8, 8, 8)
+
+
+def _members(ctx, count):
+    return [build_workspace(a, m, ctx) + (a, m) for a, m in load_library("lib16_amber_s3")[:count]]
+
+
+def _jobs(pdgpu):
+    S = pdgpu.Server
+    md = pdgpu.md_params_default()
+    md.Integrator = pdgpu.MolecularDynamics.Langevin
+    md.FricCoeff = 1e12
+    md.UpdateNList = 10
+    mn = pdgpu.min_params_default()
+    mn.Algorithm = pdgpu.Minimisation.SteepestDescent
+    jobs = []
+    for k in range(6):
+        if k % 3 == 0:
+            jobs.append(S.job(S.ENERGY))
+        elif k % 3 == 1:
+            jobs.append(S.job(S.MINIMISE, 30, minimiser=mn))
+        else:
+            m = pdgpu.md_params_default()
+            ctypes_copy(m, md)
+            m.Seed = 100 + k
+            jobs.append(S.job(S.MD, 40, md=m, init_temp=300.0))
+    return jobs
+
+
+def ctypes_copy(dst, src):
+    for name, _ in type(src)._fields_:
+        setattr(dst, name, getattr(src, name))
+
+
+def _run(server, members, jobs, together):
+    ids = []
+    if together:
+        ids = [server.submit(ws, j) for (ws, *_), j in zip(members, jobs)]
+        for jid in ids:
+            assert server.wait(jid, 120.0) == 0
+    else:
+        for (ws, *_), j in zip(members, jobs):
+            jid = server.submit(ws, j)
+            assert server.wait(jid, 120.0) == 0
+            ids.append(jid)
+    out = [server.result(jid) for jid in ids]
+    infos = [server.info(jid) for jid in ids]
+    for jid in ids:
+        server.release(jid)
+    return out, infos
+
+
+def test_serve_alone_equals_mixed(gpu_ctx):
+    import pdgpu
+    members = _members(gpu_ctx, 6)
+    jobs = _jobs(pdgpu)
+    srv = pdgpu.Server(gpu_ctx, max_active=8, lanes=LANES)
+    alone, _ = _run(srv, members, jobs, together=False)
+    mixed, infos = _run(srv, members, jobs, together=True)
+    st = srv.stats()
+    srv.close()
+    assert st["peak_active"] >= 2  # the mix really overlapped on the device
+    assert st["failed"] == 0 and st["completed"] == 12
+    for a, b, info in zip(alone, mixed, infos):
+        for key in a:
+            assert np.array_equal(a[key], b[key]), key
+        assert info["state"] == 2  # PDGPU_JOB_DONE
+        assert info["t_total_ms"] >= info["t_run_ms"] >= 0.0
+
+
+def test_serve_matches_plain_calls_and_reference(gpu_ctx):
+    import pdgpu
+    members = _members(gpu_ctx, 6)
+    jobs = _jobs(pdgpu)
+    srv = pdgpu.Server(gpu_ctx, max_active=8, lanes=LANES)
+    served, infos = _run(srv, members, jobs, together=True)
+    srv.close()
+    for (ws, ff, a, m), job, res, info in zip(members, jobs, served, infos):
+        one = pdgpu.Batch([ws])
+        one.setLanes(LANES)
+        if job.kind == pdgpu.Server.ENERGY:
+            f, e = one.evaluate()
+            assert np.array_equal(res["forces"], f)
+            assert np.array_equal(res["energies"], e[0])
+            assert rel_rms(res["forces"], a["f_total"]) <= 1e-5
+            assert info["steps_done"] == 1
+        elif job.kind == pdgpu.Server.MINIMISE:
+            taken = one.minimise(job.min, job.steps)
+            assert info["steps_done"] == taken[0] == job.steps
+            assert np.array_equal(res["positions"], one.positions())
+            assert np.array_equal(res["forces"], one.forces())
+            assert np.array_equal(res["energies"], one.energies()[0])
+        else:
+            one.calcNewList()
+            h = one.runMD(job.md, job.steps, init_velocities=job.init_temp)
+            assert np.array_equal(res["positions"], one.positions())
+            assert np.array_equal(res["history"], h[:, 0, :])
+            assert info["steps_done"] == job.steps
+        one.close()
+
+
+def test_serve_budget_admission(gpu_ctx):
+    import pdgpu
+    members = _members(gpu_ctx, 6)
+    ws = max(members, key=lambda m: m[0].nAtoms())[0]
+    est = ws.nAtoms() * (1024 + 256 * 4) + 4 * 1024 * 1024  # the server's admission estimate
+    budget = int(2.5 * est)  # room for two such jobs at a time
+    srv = pdgpu.Server(gpu_ctx, hbm_budget=budget, max_active=8, lanes=LANES)
+    job = pdgpu.Server.job(pdgpu.Server.MINIMISE, 20)
+    ids = [srv.submit(ws, job) for _ in range(6)]
+    for jid in ids:
+        assert srv.wait(jid, 120.0) == 0
+    st = srv.stats()
+    assert st["completed"] == len(ids)
+    assert st["peak_bytes"] <= budget
+    assert st["peak_active"] <= 2
+    # a job that cannot fit at all is refused at submission
+    tiny = pdgpu.Server(gpu_ctx, hbm_budget=1024 * 1024, max_active=2, lanes=LANES)
+    with pytest.raises(pdgpu.PdgpuError):
+        tiny.submit(members[0][0], job)
+    tiny.close()
+    srv.close()
+
+
+def test_serve_failed_job_does_not_disturb_others(gpu_ctx):
+    """A job whose energy turns NaN fails alone (assertStability,
+    protocolbase.cpp:104-110); the jobs running beside it are unaffected."""
+    import pdgpu
+    members = _members(gpu_ctx, 3)
+    srv = pdgpu.Server(gpu_ctx, max_active=4, lanes=LANES)
+    md = pdgpu.md_params_default()
+    md.Integrator = pdgpu.MolecularDynamics.Langevin
+    md.FricCoeff = 1e12
+    job = pdgpu.Server.job(pdgpu.Server.MD, 20, md=md)
+    ref_ids = [srv.submit(ws, job) for ws, *_ in members[1:]]
+    ref = [srv.result(j) if srv.wait(j, 120.0) == 0 else None for j in ref_ids]
+    bad_pos = members[0][0].cur.p.copy()
+    bad_pos[5] = np.nan
+    bad = srv.submit(members[0][0], job, positions=bad_pos)
+    ok_ids = [srv.submit(ws, job) for ws, *_ in members[1:]]
+    assert srv.wait(bad, 120.0) == pdgpu._abi.ERR_UNSTABLE
+    for j, r in zip(ok_ids, ref):
+        assert srv.wait(j, 120.0) == 0
+        got = srv.result(j)
+        assert np.array_equal(got["positions"], r["positions"])
+    assert srv.info(bad)["state"] == 3
+    srv.close()
