@@ -21,6 +21,14 @@ Extra keys of the same JSON line:
               Langevin 1 fs, gamma 1/ps, 300 K, Rc 12 A, list every 10 steps,
               all systems in one CUDA-graph step loop; aggregate ns/day against
               one system alone.
+  serving     a seeded Poisson request stream (200 requests/s) of jobs on
+              systems of 500-30,000 atoms (log-uniform; multi-chain systems
+              composed from the AMBER99 library peptides, chain axes along z
+              on a 25 A grid): 60% single-point, 30% 200-step steepest-descent
+              minimisation, 10% 2,000-step Langevin MD at 1 fs, Rc 12 A,
+              through the request loop with a 120 GB HBM budget; p50/p99
+              latency and jobs/s beside the plain sequential GPU path (the
+              same jobs one after another through the plain calls).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -229,6 +237,178 @@ def bench_batched_md(pdgpu, A, ctx, torch, copies=16, steps=5000, plain_steps=20
             "timing": "CUDA events around the device step loop (pdgpu_last_run_ms)"}
 
 
+# ---------------------------------------------------------------- serving
+PER_ATOM = ("charge", "radius", "epsilon", "mass", "gb_radius", "is_h")
+
+
+def compose(parts, spacing=25.0):
+    """One multi-chain system from several library peptides: per-atom arrays
+    concatenated, index arrays shifted, each chain's principal axis turned
+    onto z and the chains set on a square grid `spacing` apart in x-y."""
+    out = {k: [] for k in PER_ATOM + ("ir", "pos", "cov12_d", "cov13_d", "bond_lk", "angle_kt", "tors_terms",
+                                      "tors_par", "impr_terms", "impr_par", "backbone_ncac", "bond_ij",
+                                      "angle_iaj", "tors_idx", "impr_idx")}
+    csr = {k: ([0], []) for k in ("cov12", "cov13", "cov14")}
+    g = int(np.ceil(np.sqrt(len(parts))))
+    off = 0
+    res_off = 0
+    for k, a in enumerate(parts):
+        n = a["charge"].shape[0]
+        for f in PER_ATOM:
+            out[f].append(a[f])
+        out["ir"].append(a["ir"] + res_off)
+        p = a["pos"] - a["pos"].mean(axis=0)
+        _, _, vt = np.linalg.svd(p, full_matrices=False)
+        ax = vt[0]
+        # rotation taking the principal axis onto z
+        z = np.array([0.0, 0.0, 1.0])
+        v = np.cross(ax, z)
+        c = float(np.dot(ax, z))
+        if np.linalg.norm(v) < 1e-12:
+            R = np.eye(3) if c > 0 else np.diag([1.0, -1.0, -1.0])
+        else:
+            vx = np.array([[0, -v[2], v[1]], [v[2], 0, -v[0]], [-v[1], v[0], 0]])
+            R = np.eye(3) + vx + vx @ vx * (1.0 / (1.0 + c))
+        out["pos"].append(p @ R.T + np.array([(k % g) * spacing, (k // g) * spacing, 0.0]))
+        for name in ("cov12", "cov13", "cov14"):
+            ptr, idx = csr[name]
+            ptr.extend((a[name + "_ptr"][1:] + ptr[-1]).tolist())
+            idx.append(a[name + "_idx"] + off)
+        out["cov12_d"].append(a["cov12_d"])
+        out["cov13_d"].append(a["cov13_d"])
+        for f in ("bond_ij", "angle_iaj", "tors_idx", "impr_idx"):
+            out[f].append(a[f] + off)
+        for f in ("bond_lk", "angle_kt", "tors_terms", "tors_par", "impr_terms", "impr_par"):
+            out[f].append(a[f])
+        bb = a["backbone_ncac"].copy()
+        out["backbone_ncac"].append(np.where(bb >= 0, bb + off, -1))
+        off += n
+        res_off += int(a["ir"].max()) + 1
+    res = {k: np.concatenate(v) for k, v in out.items()}
+    for name in ("cov12", "cov13", "cov14"):
+        ptr, idx = csr[name]
+        res[name + "_ptr"] = np.asarray(ptr, dtype=np.int32)
+        res[name + "_idx"] = np.concatenate(idx).astype(np.int32)
+    res["ff_params"] = parts[0]["ff_params"]
+    return res
+
+
+def bench_serving(pdgpu, A, ctx, torch, n_requests=300, rate=200.0, budget=120e9, max_active=32, seed=5):
+    lib = load_library(LIB_SP)
+    meta = lib[0][1]
+    rng = np.random.default_rng(seed)
+    # templates: sizes log-uniform in [500, 30000]
+    n_tmpl = 24
+    targets = np.exp(np.linspace(np.log(500), np.log(30000), n_tmpl))
+    templates = []
+    for t in targets:
+        parts, tot = [], 0
+        while tot < 0.9 * t:
+            a = lib[int(rng.integers(len(lib)))][0]
+            if parts and tot + a["charge"].shape[0] > 1.15 * t:
+                cand = [x for x, _ in lib if tot + x["charge"].shape[0] <= 1.15 * t]
+                if not cand:
+                    break
+                a = cand[int(rng.integers(len(cand)))]
+            parts.append(a)
+            tot += a["charge"].shape[0]
+        arrays = compose(parts)
+        ws, ff = make_ws(pdgpu, arrays, meta, ctx)
+        ws.setLanes((8, 8, 8))
+        templates.append(ws)
+    sizes = np.array([ws.nAtoms() for ws in templates])
+    # the request stream
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+    want = np.exp(rng.uniform(np.log(500), np.log(30000), n_requests))
+    tmpl = [int(np.argmin(np.abs(np.log(sizes) - np.log(w)))) for w in want]
+    u = rng.uniform(size=n_requests)
+    kinds = np.where(u < 0.6, A.JOB_ENERGY, np.where(u < 0.9, A.JOB_MINIMISE, A.JOB_MD))
+    md = A.md_params_default()
+    md.Integrator, md.UpdateNList, md.UseGraph = A.INTEGRATOR_LANGEVIN, 10, 1
+    md.Timestep, md.FricCoeff, md.TargetTemp = 1e-15, 1e12, 300.0
+    mn = A.min_params_default()
+    mn.Algorithm = A.MIN_STEEPEST_DESCENT
+    S = pdgpu.Server
+    jobs = []
+    for k in range(n_requests):
+        if kinds[k] == A.JOB_ENERGY:
+            jobs.append(S.job(S.ENERGY))
+        elif kinds[k] == A.JOB_MINIMISE:
+            jobs.append(S.job(S.MINIMISE, 200, minimiser=mn))
+        else:
+            m = A.md_params_default()
+            for name, _ in A.MDParams._fields_:
+                setattr(m, name, getattr(md, name))
+            m.Seed = 1000 + k
+            jobs.append(S.job(S.MD, 2000, md=m, init_temp=300.0))
+    L = A.lib()
+    # served: submit at the arrival times, the worker overlaps the jobs
+    srv = pdgpu.Server(ctx, hbm_budget=budget, max_active=max_active, lanes=(8, 8, 8))
+    lc0 = L_count(L, ctx)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ids = []
+    for k in range(n_requests):
+        while time.perf_counter() - t0 < arrivals[k]:
+            time.sleep(min(2e-4, max(0.0, arrivals[k] - (time.perf_counter() - t0))))
+        ids.append(srv.submit(templates[tmpl[k]], jobs[k]))
+    for jid in ids:
+        A.check(srv.wait(jid, 600.0))
+    makespan = time.perf_counter() - t0
+    lc1 = L_count(L, ctx)
+    lat = [srv.info(j)["t_total_ms"] for j in ids]
+    st = srv.stats()
+    for jid in ids:
+        srv.release(jid)
+    srv.close()
+    by_kind = {}
+    for k, name in ((A.JOB_ENERGY, "energy"), (A.JOB_MINIMISE, "minimise_200"), (A.JOB_MD, "md_2000")):
+        sel = [lat[i] for i in range(n_requests) if kinds[i] == k]
+        by_kind[name] = {"count": len(sel), "p50_ms": pctl(sel, 50), "p99_ms": pctl(sel, 99)}
+    # plain sequential path: the same jobs, one after another, plain calls
+    ebuf = np.zeros(A.ENE_COUNT)
+    plat = []
+    t0 = time.perf_counter()
+    for k in range(n_requests):
+        now = time.perf_counter() - t0
+        if now < arrivals[k]:
+            time.sleep(arrivals[k] - now)
+        ws = templates[tmpl[k]]
+        sid = ws._sys
+        A.check(L.pdgpu_set_positions(ctx.ptr, sid, A.dptr(A.cd(ws.cur.p))))
+        j = jobs[k]
+        if j.kind == A.JOB_ENERGY:
+            A.check(L.pdgpu_nlist_build(ctx.ptr, sid))
+            A.check(L.pdgpu_calc_forces(ctx.ptr, sid))
+        elif j.kind == A.JOB_MINIMISE:
+            taken = np.zeros(1, dtype=np.int32)
+            A.check(L.pdgpu_minimise_run(ctx.ptr, sid, ctypes.byref(j.min), j.steps, A.iptr(taken)))
+        else:
+            A.check(L.pdgpu_md_init_velocities(ctx.ptr, sid, j.init_temp, j.md.Seed))
+            A.check(L.pdgpu_md_run(ctx.ptr, sid, ctypes.byref(j.md), 0, j.steps, j.steps, None))
+        A.check(L.pdgpu_get_energies(ctx.ptr, sid, A.dptr(ebuf), A.ENE_COUNT))
+        plat.append(1e3 * ((time.perf_counter() - t0) - arrivals[k]))
+    plain_makespan = time.perf_counter() - t0
+    for ws in templates:
+        ws.close()
+    return {"metric": "served GB jobs/s", "value": n_requests / makespan, "unit": "jobs/s",
+            "requests": n_requests, "arrival_rate_per_s": rate,
+            "latency_ms": {"p50": pctl(lat, 50), "p99": pctl(lat, 99)}, "by_kind": by_kind,
+            "plain_sequential": {"value": n_requests / plain_makespan, "unit": "jobs/s",
+                                 "latency_ms": {"p50": pctl(plat, 50), "p99": pctl(plat, 99)}},
+            "speedup_jobs_per_s_vs_plain": (n_requests / makespan) / (n_requests / plain_makespan),
+            "system_atoms": {"min": int(sizes.min()), "max": int(sizes.max()), "templates": n_tmpl},
+            "hbm_budget_bytes": int(budget), "max_active": max_active, "peak_active": st["peak_active"],
+            "peak_bytes": st["peak_bytes"], "failed": st["failed"], "gpu_launches": int(lc1 - lc0),
+            "timing": "wall clock: latency = finish - arrival per job; jobs/s = requests / makespan"}
+
+
+def L_count(L, ctx):
+    c = ctypes.c_int64(0)
+    L.pdgpu_launch_count(ctx.ptr, ctypes.byref(c))
+    return c.value
+
+
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
@@ -343,6 +523,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched workloads")
     ap.add_argument("--batched-md-steps", type=int, default=5000)
+    ap.add_argument("--serve-requests", type=int, default=300)
     args = ap.parse_args()
     rank, world, local = rank_info()
     n_gpus = max(args.gpus, world)
@@ -536,6 +717,7 @@ def main():
     if not args.no_batched:
         line["batched_sp"] = bench_batched_sp(pdgpu, A, ctx, torch)
         line["batched_md"] = bench_batched_md(pdgpu, A, ctx, torch, steps=args.batched_md_steps)
+        line["serving"] = bench_serving(pdgpu, A, ctx, torch, n_requests=args.serve_requests)
     if rank == 0 and n_gpus == 1 and not args.no_cpu_baseline:
         try:
             cb = run_reference(args, 1)
