@@ -578,10 +578,11 @@ def main():
     de_kcal = float(abs(ws.ene.epot - arrays["ene_total"][0]) * pdgpu.J2KCAL_NA)
 
     # roofline inputs: pair counts and per-kernel device times (CUDA events)
-    counts = np.zeros(3, dtype=np.int64)
+    counts = np.zeros(5, dtype=np.int64)
     A.check(A.lib().pdgpu_pair_counts(ctx.ptr, ws._sys, counts.ctypes.data_as(A._I64)))
     lpa = np.zeros(3, dtype=np.int32)
     A.check(A.lib().pdgpu_autotune(ctx.ptr, ws._sys, A.iptr(lpa)))
+    path = ws.setPairPath(-2)  # the layout the autotuner chose
     kms = np.zeros(3)
     A.check(A.lib().pdgpu_profile_pair_kernels(ctx.ptr, ws._sys, 20, A.dptr(kms)))
 
@@ -678,7 +679,7 @@ def main():
                "steps": e2e_steps, "api": "pdgpu_set_positions/velocities + pdgpu_md_run(10) + get_*"}
 
     # roofline of the pair kernels (FP32/SFU; nominal peaks at the max SM clock)
-    P_B, P_H, entries = (int(c) for c in counts)
+    P_B, P_H, entries, tile_pairs, n_tiles = (int(c) for c in counts)
     f_max = (clk.get("sm_max_mhz") or 1965.0) * 1e6
     sms = torch.cuda.get_device_properties(device).multi_processor_count
     F32 = sms * 256 * f_max
@@ -691,7 +692,11 @@ def main():
     t_pair = t2 + t3 + t4
     t_roof = max(all_flop / F32, all_sfu / SFU)
     bound = "fp32" if k3_frac_fp32 >= k3_frac_sfu else "sfu"
-    roof = {"kernel": "k_gb_pair (fused GB + LJ + Coulomb, K3)", "bound": bound,
+    k3_name = ("k_gb_tile + k_gb_finish (fused GB + LJ + Coulomb on 32x8 cluster-pair tiles, K3)" if path == 1
+               else "k_gb_pair (fused GB + LJ + Coulomb on neighbour-list rows, K3)")
+    roof = {"kernel": k3_name, "bound": bound, "pair_path": "tiles" if path == 1 else "rows",
+            "tiles": {"tiles": n_tiles, "pair_slots": 256 * n_tiles, "list_pairs_held": tile_pairs,
+                      "slot_occupancy": tile_pairs / max(1, 256 * n_tiles)},
             "achieved": (k3_flop / t3 / 1e12) if bound == "fp32" else (k3_sfu / t3 / 1e12),
             "peak": (F32 if bound == "fp32" else SFU) / 1e12,
             "unit": "TFLOP/s" if bound == "fp32" else "Top/s (MUFU)",

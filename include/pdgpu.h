@@ -321,14 +321,18 @@ int pdgpu_minimise_run(pdgpu_ctx *ctx, int32_t sys, const pdgpu_min_params *p,
  * the device until it finishes; jobs that arrive while others run are
  * admitted as soon as a stream slot is free and their memory fits under the
  * HBM budget (first fit in arrival order), and their kernels overlap with
- * the running jobs'.  All jobs use the same fixed lanes per atom, so a
- * job's results are bit-identical alone and in any mix.  The server is
+ * the running jobs'.  All jobs use the same pair-pass layout (and fixed
+ * lanes per atom on the row layout), so a job's results are bit-identical
+ * alone and in any mix.  A job's memory estimate before admission is
+ * natoms * 2048 bytes + 40 bytes per possible 32 x 8 tile + 4 MiB; once its
+ * list is sized it is charged max(estimate, real size).  The server is
  * driven from one host thread (the context's). */
 typedef struct pdgpu_server pdgpu_server;
 typedef struct {
   int64_t hbm_budget;   /* device bytes the admitted jobs may hold together   */
   int32_t max_active;   /* jobs on the device at once (one stream each)       */
   int32_t lanes[3];     /* lanes per atom: Born, fused pair, chain (4..32)    */
+  int32_t tiles;        /* 1: cluster-pair tile passes, 0: list-row passes    */
 } pdgpu_serve_params;
 void pdgpu_serve_params_default(pdgpu_serve_params *p);
 
@@ -394,7 +398,9 @@ int pdgpu_last_run_ms(pdgpu_ctx *ctx, double *ms);
 /* Instrumentation (no reference counterpart).  Pair counts of the current
  * list and positions: counts[0] = P_B, directed pairs with r <= GbsaStillCutoff
  * and bond order >= 3 (Born sum / chain rule); counts[1] = P_H, unordered
- * pairs with r <= Cutoff (fused GB + LJ + Coulomb); counts[2] = list entries. */
+ * pairs with r <= Cutoff (fused GB + LJ + Coulomb); counts[2] = list entries;
+ * counts[3] = unordered list pairs held by the cluster-pair tiles (counts[2]
+ * / 2 when they agree); counts[4] = tiles (32 x 8 pair slots each). */
 int pdgpu_pair_counts(pdgpu_ctx *ctx, int32_t sys, int64_t *counts);
 /* Average device time (ms) of the Born-radius, fused pair and chain-rule
  * kernels over `reps` evaluations, each bracketed by CUDA events on the
@@ -413,6 +419,13 @@ int pdgpu_autotune(pdgpu_ctx *ctx, int32_t sys, int32_t *lpa);
  * bit-identical run to run for given lanes per atom; with the same lanes a
  * system's results are bit-identical alone and in any batch. */
 int pdgpu_set_lanes(pdgpu_ctx *ctx, int32_t sys, const int32_t *lpa);
+/* Pair-pass layout (no reference counterpart): 0 = neighbour-list rows
+ * (lanes per atom as tuned or set), 1 = cluster-pair tiles (32 x 8 atom
+ * blocks of the same pair set, each unordered pair once; results do not
+ * depend on lanes, row order or the batch a system sits in), -1 = let the
+ * autotuner time both at the next evaluation, -2 = only report.  *current
+ * (may be NULL) receives the layout in use. */
+int pdgpu_pair_path(pdgpu_ctx *ctx, int32_t sys, int32_t set, int32_t *current);
 
 #ifdef __cplusplus
 }

@@ -702,22 +702,27 @@ int pdgpu_get_forces(pdgpu_ctx *c, int32_t sys, double *f) {
   }
   Pack &P = *e->pack;
   int n = P.v.n_atoms;
-  std::vector<long long> a(3 * (size_t)n);
+  std::vector<long long> a(3 * (size_t)n), h(3 * (size_t)n);
   std::vector<double> g(3 * (size_t)n);
   const long long *fs[3] = {P.v.fx, P.v.fy, P.v.fz};
   const double *gs[3] = {P.v.gx, P.v.gy, P.v.gz};
+  const long long *hs[3] = {P.v.hx, P.v.hy, P.v.hz};
   for (int k = 0; k < 3; k++) {
-    PDGPU_CUDA(cudaMemcpyAsync(a.data() + (size_t)k * n, fs[k], sizeof(long long) * n, cudaMemcpyDeviceToHost,
-                               c->st));
-    PDGPU_CUDA(cudaMemcpyAsync(g.data() + (size_t)k * n, gs[k], sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+    size_t o = (size_t)k * n;
+    PDGPU_CUDA(cudaMemcpyAsync(a.data() + o, fs[k], sizeof(long long) * n, cudaMemcpyDeviceToHost, c->st));
+    PDGPU_CUDA(cudaMemcpyAsync(g.data() + o, gs[k], sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+    PDGPU_CUDA(cudaMemcpyAsync(h.data() + o, hs[k], sizeof(long long) * n, cudaMemcpyDeviceToHost, c->st));
   }
   int r = sync_check(c, "get_forces");
   if (r) return r;
-  // the integrator's sum (fixed-point scattered terms + FP64 pair forces)
+  // the integrator's sum: fixed-point scattered terms, FP64 pair forces,
+  // fixed-point j side of the tile passes
   double s = consts().N_per_kcalmolA;
   for (int i = 0; i < n; i++)
-    for (int k = 0; k < 3; k++)
-      f[3 * i + k] = ((double)a[(size_t)k * n + i] * kInvForceScale + g[(size_t)k * n + i]) * s;
+    for (int k = 0; k < 3; k++) {
+      size_t q = (size_t)k * n + i;
+      f[3 * i + k] = ((double)a[q] * kInvForceScale + g[q] + (double)h[q] * kInvJScale) * s;
+    }
   return PDGPU_OK;
 }
 
@@ -897,9 +902,11 @@ static int ensure_tuned(pdgpu_ctx *c, Pack &P) {
   if (P.tuned || P.v.n_atoms == 0 || !P.have_list) return PDGPU_OK;
   const int N = P.v.n_atoms;
   PackView t = P.v;
+  t.tile_mode = 0;
+  // scratch for every array the timed launches accumulate into
   double *f = nullptr;
   double *ea = nullptr, *en = nullptr;
-  PDGPU_CUDA(cudaMalloc(&f, sizeof(double) * 3 * (size_t)N));
+  PDGPU_CUDA(cudaMalloc(&f, sizeof(double) * 12 * (size_t)N));
   if (cudaMalloc(&ea, sizeof(double) * AE_COUNT * (size_t)N) != cudaSuccess ||
       cudaMalloc(&en, sizeof(double) * E_COUNT * (size_t)P.v.n_sys) != cudaSuccess) {
     cudaFree(f);
@@ -907,9 +914,16 @@ static int ensure_tuned(pdgpu_ctx *c, Pack &P) {
     set_error("autotune scratch allocation failed");
     return PDGPU_ERR_NOMEM;
   }
+  cudaMemsetAsync(f, 0, sizeof(double) * 12 * (size_t)N, c->st);
   t.gx = f;
   t.gy = f + N;
   t.gz = f + 2 * N;
+  t.hx = (long long *)(f + 3 * (size_t)N);
+  t.hy = (long long *)(f + 4 * (size_t)N);
+  t.hz = (long long *)(f + 5 * (size_t)N);
+  t.ej = (long long *)(f + 6 * (size_t)N);
+  t.deda = f + 10 * (size_t)N;
+  t.bsum = (long long *)(f + 11 * (size_t)N);
   t.e_atom = ea;
   t.ene = en;
   cudaEvent_t a, b;
@@ -917,6 +931,7 @@ static int ensure_tuned(pdgpu_ctx *c, Pack &P) {
   cudaEventCreate(&b);
   static const int cand[4] = {4, 8, 16, 32};
   int r = PDGPU_OK;
+  float row_total = 0.f;
   for (int kern = 0; kern < 3 && r == PDGPU_OK; kern++) {
     float best = 1e30f;
     int pick = 8;
@@ -941,9 +956,28 @@ static int ensure_tuned(pdgpu_ctx *c, Pack &P) {
       }
     }
     P.v.lpa[kern] = t.lpa[kern] = pick;
+    row_total += best;
     // leave valid inputs for the next kernel's timing
     if (kern == 0) launch_born_radii_lpa(t, c->st, false, pick);
     if (kern == 1) launch_gb_pair_lpa(t, c->st, pick);
+  }
+  // the cluster-pair tile path against the tuned row path (three passes)
+  if (r == PDGPU_OK && P.v.n_sc > 0) {
+    t.tile_mode = 1;
+    launch_tiles_build(t, c->st);
+    float tot = 0;
+    for (int rep = 0; rep < 4 && r == PDGPU_OK; rep++) {
+      cudaEventRecord(a, c->st);
+      launch_born_radii_tile(t, c->st, false);
+      launch_gb_pair_tile(t, c->st);
+      launch_gb_chain_tile(t, c->st);
+      cudaEventRecord(b, c->st);
+      r = sync_check(c, "autotune tiles");
+      float ms = 0;
+      cudaEventElapsedTime(&ms, a, b);
+      if (rep > 0) tot += ms;
+    }
+    P.v.tile_mode = (r == PDGPU_OK && tot < row_total) ? 1 : 0;
   }
   if (r == PDGPU_OK) r = sync_check(c, "autotune");
   cudaEventDestroy(a);
@@ -1412,15 +1446,17 @@ int pdgpu_pair_counts(pdgpu_ctx *c, int32_t sys, int64_t *counts) {
     return PDGPU_ERR_ARG;
   }
   unsigned long long *d = nullptr;
-  PDGPU_CUDA(cudaMalloc(&d, 3 * sizeof(unsigned long long)));
-  cudaMemsetAsync(d, 0, 3 * sizeof(unsigned long long), c->st);
+  PDGPU_CUDA(cudaMalloc(&d, 5 * sizeof(unsigned long long)));
+  cudaMemsetAsync(d, 0, 5 * sizeof(unsigned long long), c->st);
   launch_pair_counts(P.v, c->st, d);
-  unsigned long long h[3];
+  if (!P.v.tile_mode) launch_tiles_build(P.v, c->st);  // the tiles of the current list, for the counts
+  launch_tile_counts(P.v, c->st, d + 3);
+  unsigned long long h[5];
   cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, c->st);
   r = sync_check(c, "pair_counts");
   cudaFree(d);
   if (r) return r;
-  for (int q = 0; q < 3; q++) counts[q] = (int64_t)h[q];
+  for (int q = 0; q < 5; q++) counts[q] = (int64_t)h[q];
   return PDGPU_OK;
 }
 
@@ -1490,7 +1526,32 @@ int pdgpu_set_lanes(pdgpu_ctx *c, int32_t sys, const int32_t *lpa) {
       return PDGPU_ERR_ARG;
     }
   for (int q = 0; q < 3; q++) P.v.lpa[q] = lpa[q];
+  P.v.tile_mode = 0;  // the row path, with these lanes
   P.tuned = true;
+  return PDGPU_OK;
+}
+
+int pdgpu_pair_path(pdgpu_ctx *c, int32_t sys, int32_t set, int32_t *current) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  if (set < -2 || set > 1) {
+    set_error("pdgpu_pair_path: set must be -2 (query), -1 (tune), 0 (rows) or 1 (tiles)");
+    return PDGPU_ERR_ARG;
+  }
+  if (set != -2) {
+    e->drop_graph();
+    if (set == -1) {
+      P.tuned = false;
+    } else {
+      P.v.tile_mode = set;
+      P.tuned = true;
+      if (set == 1 && P.have_list) launch_tiles_build(P.v, c->st);  // tiles for the current list
+      int r = sync_check(c, "pair_path");
+      if (r) return r;
+    }
+  }
+  if (current) *current = P.v.tile_mode;
   return PDGPU_OK;
 }
 

@@ -36,9 +36,11 @@ __device__ __forceinline__ void six_normals(unsigned long long seed, int local, 
 }
 
 // Total force on atom i along one axis in kcal/mol/A (the caller scales to
-// N): the fixed-point scattered terms plus the atom's FP64 pair force, added
-// in this order.
-__device__ __forceinline__ double force_N(long long f, double g) { return (double)f * kInvForceScale + g; }
+// N): the fixed-point scattered terms, the atom's FP64 pair force and the
+// fixed-point j side of the tile passes, added in this order.
+__device__ __forceinline__ double force_N(long long f, double g, long long h) {
+  return (double)f * kInvForceScale + g + (double)h * kInvJScale;
+}
 
 __device__ __forceinline__ void store_pos(const PackView &v, int i, double x, double y, double z) {
   v.x[i] = x;
@@ -74,8 +76,8 @@ __global__ void k_md_step(PackView v, MDDev d, const double *normals, const int 
   const MDCoef &c = d.c;
   int step = step_dev ? *step_dev : c.step;
   double m = v.mass_si[i];
-  double f[3] = {force_N(v.fx[i], v.gx[i]) * d.N_per_unit, force_N(v.fy[i], v.gy[i]) * d.N_per_unit,
-                 force_N(v.fz[i], v.gz[i]) * d.N_per_unit};
+  double f[3] = {force_N(v.fx[i], v.gx[i], v.hx[i]) * d.N_per_unit, force_N(v.fy[i], v.gy[i], v.hy[i]) * d.N_per_unit,
+                 force_N(v.fz[i], v.gz[i], v.hz[i]) * d.N_per_unit};
   double vel[3] = {v.vx[i], v.vy[i], v.vz[i]};
   double pos[3] = {v.x[i], v.y[i], v.z[i]};
   double t = c.dt;
@@ -241,8 +243,8 @@ __global__ void k_min_dots(PackView v, double N_per_unit, int C) {
   __shared__ double sa[256], sb[256];
   double A = 0, B = 0;
   for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
-    double f[3] = {force_N(v.fx[i], v.gx[i]) * N_per_unit, force_N(v.fy[i], v.gy[i]) * N_per_unit,
-                   force_N(v.fz[i], v.gz[i]) * N_per_unit};
+    double f[3] = {force_N(v.fx[i], v.gx[i], v.hx[i]) * N_per_unit, force_N(v.fy[i], v.gy[i], v.hy[i]) * N_per_unit,
+                   force_N(v.fz[i], v.gz[i], v.hz[i]) * N_per_unit};
     double of[3] = {v.fox[i], v.foy[i], v.foz[i]};
     A += of[0] * of[0] + of[1] * of[1] + of[2] * of[2];
     B += (of[0] - f[0]) * f[0] + (of[1] - f[1]) * f[1] + (of[2] - f[2]) * f[2];
@@ -354,8 +356,8 @@ __global__ void k_min_update(PackView v, const MinState *ms, double N_per_unit, 
   const MinState &m = ms[s];
   int a = m.action;
   if (a < 0) return;
-  double f[3] = {force_N(v.fx[i], v.gx[i]) * N_per_unit, force_N(v.fy[i], v.gy[i]) * N_per_unit,
-                 force_N(v.fz[i], v.gz[i]) * N_per_unit};
+  double f[3] = {force_N(v.fx[i], v.gx[i], v.hx[i]) * N_per_unit, force_N(v.fy[i], v.gy[i], v.hy[i]) * N_per_unit,
+                 force_N(v.fz[i], v.gz[i], v.hz[i]) * N_per_unit};
   double p[3] = {v.x[i], v.y[i], v.z[i]};
   double sc = step_size * m.mult;
   if (a == 0) {  // SD accept (or first step): save p, f; step along f

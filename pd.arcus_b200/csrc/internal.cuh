@@ -35,6 +35,8 @@ const Consts &consts();
 // kcal/mol/A).  Born sums: A^-1 * 2^40 in int64 (range +-8.3e6).
 constexpr double kForceScale = 4294967296.0;          // 2^32
 constexpr double kInvForceScale = 1.0 / 4294967296.0;
+constexpr double kJScale = 16777216.0;                // 2^24: j-side tile forces and energies
+constexpr double kInvJScale = 1.0 / 16777216.0;
 constexpr double kBornScale = 1099511627776.0;        // 2^40
 constexpr double kInvBornScale = 1.0 / 1099511627776.0;
 
@@ -154,6 +156,25 @@ struct PackView {
   int *cell_start, *cell_end; // [cell_cap]
   int cell_cap;
   double *grid;               // [S*8] origin xyz, cell size, dims(as double), cell_off
+  unsigned long long *bbox;   // [6*S] ordered-integer box: min x,y,z then max x,y,z (each [S])
+  // cluster-pair tiles (tiles.cu): i-clusters of 32 atoms, j-clusters of 8
+  int tile_mode;              // 1: the pair passes run on the tiles, 0: on the list rows
+  int n_sc, n_jc;
+  const int *sc_atom0, *sc_sys;  // [n_sc] first atom, system
+  const int *jc_atom0, *jc_sys;  // [n_jc]
+  const int *jc_off;          // [S+1] j-cluster range of each system
+  double *sc_bb, *jc_bb;      // [6*n] FP64 boxes (min xyz, max xyz)
+  int *tile_e0, *tile_e1;     // [n_sc] tile range of each i-cluster
+  int *tile_jc;               // [tile_cap] j-cluster of each tile
+  unsigned *tile_mask;        // [8*tile_cap] list bits: word t = j atom t, bit l = i lane l
+  int *tile_spec;             // [tile_cap] bond-order masks index, -1 none
+  unsigned *spec_mask;        // [16*spec_cap] bond order <= 2 (8 words), == 3 (8 words)
+  int *tile_count;            // [2] tiles, bond-order mask sets allocated
+  long long tile_cap, spec_cap;
+  long long *bsum;            // [N] Born sums of the tile pass, fixed point 2^40
+  long long *hx, *hy, *hz;    // [N] j-side pair forces, fixed point 2^24 kcal/mol/A
+  long long *ej;              // [4*N] j-side LJ, Coulomb, GB energies and dE/da, fixed point 2^24
+  double *deda;               // [N] i-side dE/da of the tile pass
   int *flags;                 // [8] overflow / nan / etc.
   BondedTerms bt;
 };
@@ -237,6 +258,13 @@ void launch_born_radii(const PackView &v, cudaStream_t st, bool zero_first = fal
 void launch_gb_pair(const PackView &v, cudaStream_t st);
 void launch_gb_chain(const PackView &v, cudaStream_t st);
 // explicit lanes-per-atom variants (4, 8, 16, 32), used by the autotuner
+// cluster-pair tile versions of the three passes (tiles.cu); the plain
+// launchers above pick them when v.tile_mode is set
+void launch_tiles_build(const PackView &v, cudaStream_t st);
+void launch_tile_counts(const PackView &v, cudaStream_t st, unsigned long long *out);
+void launch_born_radii_tile(const PackView &v, cudaStream_t st, bool zero_first);
+void launch_gb_pair_tile(const PackView &v, cudaStream_t st);
+void launch_gb_chain_tile(const PackView &v, cudaStream_t st);
 void launch_born_radii_lpa(const PackView &v, cudaStream_t st, bool zero_first, int lpa);
 void launch_gb_pair_lpa(const PackView &v, cudaStream_t st, int lpa);
 void launch_gb_chain_lpa(const PackView &v, cudaStream_t st, int lpa);

@@ -20,43 +20,74 @@
 namespace pdgpu {
 
 // --------------------------------------------------------------- grid plan
-// One block per system: bounding box, cell size, dims.  Cells per system are
-// capped at 2*natoms+64 (the key space is allocated from atom_off); a sparse
-// system gets larger cells, which is still exact (more candidates only).
-__global__ void k_grid_plan(PackView v) {
-  int s = blockIdx.x;
-  int a0 = v.atom_off[s], a1 = v.atom_off[s + 1];
-  __shared__ double smin[3][256], smax[3][256];
-  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
-  for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
-    double p[3] = {v.x[i], v.y[i], v.z[i]};
+// Bounding boxes: every atom folds its coordinates into its system's box
+// with 64-bit atomic min/max on an order-preserving integer image of the
+// double (one warp-reduced atomic per warp when the warp lies in one
+// system).  NaN coordinates are ignored for the box (their pairs are
+// decided by the distance test alone, as in the reference).
+__device__ __forceinline__ unsigned long long ordered_key(double d) {
+  unsigned long long u = (unsigned long long)__double_as_longlong(d);
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ULL);
+}
+__device__ __forceinline__ double ordered_value(unsigned long long k) {
+  unsigned long long u = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFULL) : ~k;
+  return __longlong_as_double((long long)u);
+}
+
+__global__ void k_bbox(PackView v) {
+  const int lane = threadIdx.x & 31;
+  const int S = v.n_sys;
+  for (int base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; base < v.n_atoms;
+       base += gridDim.x * blockDim.x) {
+    int i = base + lane;
+    bool valid = i < v.n_atoms;
+    int s = valid ? v.sys_of[i] : -1;
+    double p[3] = {valid ? v.x[i] : 0.0, valid ? v.y[i] : 0.0, valid ? v.z[i] : 0.0};
+    double mn[3], mx[3];
     for (int k = 0; k < 3; k++) {
-      // NaN coordinates are ignored for the box (their pairs are decided by
-      // the distance test alone, as in the reference)
-      if (p[k] == p[k]) {
-        mn[k] = fmin(mn[k], p[k]);
-        mx[k] = fmax(mx[k], p[k]);
-      }
+      bool ok = valid && p[k] == p[k];
+      mn[k] = ok ? p[k] : 1e308;
+      mx[k] = ok ? p[k] : -1e308;
+    }
+    int s0 = __shfl_sync(0xffffffffu, s, 0);
+    bool uniform = __all_sync(0xffffffffu, s == s0 || s < 0);
+    if (uniform) {
+      for (int o = 16; o > 0; o >>= 1)
+        for (int k = 0; k < 3; k++) {
+          mn[k] = fmin(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+          mx[k] = fmax(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+        }
+      if (lane == 0 && s0 >= 0)
+        for (int k = 0; k < 3; k++) {
+          if (mn[k] <= mx[k]) {
+            atomicMin(&v.bbox[k * S + s0], ordered_key(mn[k]));
+            atomicMax(&v.bbox[(3 + k) * S + s0], ordered_key(mx[k]));
+          }
+        }
+    } else if (s >= 0) {
+      for (int k = 0; k < 3; k++)
+        if (mn[k] <= mx[k]) {
+          atomicMin(&v.bbox[k * S + s], ordered_key(mn[k]));
+          atomicMax(&v.bbox[(3 + k) * S + s], ordered_key(mx[k]));
+        }
     }
   }
-  for (int k = 0; k < 3; k++) {
-    smin[k][threadIdx.x] = mn[k];
-    smax[k][threadIdx.x] = mx[k];
-  }
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w)
-      for (int k = 0; k < 3; k++) {
-        smin[k][threadIdx.x] = fmin(smin[k][threadIdx.x], smin[k][threadIdx.x + w]);
-        smax[k][threadIdx.x] = fmax(smax[k][threadIdx.x], smax[k][threadIdx.x + w]);
-      }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
+}
+
+// One thread per system: cell size and dims from the box.  Cells per system
+// are capped at 2*natoms+64 (the key space is allocated from atom_off); a
+// sparse system gets larger cells, which is still exact (more candidates
+// only).
+__global__ void k_grid_plan(PackView v) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= v.n_sys) return;
+  const int S = v.n_sys;
+  int a0 = v.atom_off[s], a1 = v.atom_off[s + 1];
+  {
     double lo[3], ext[3];
     for (int k = 0; k < 3; k++) {
-      lo[k] = smin[k][0];
-      double hi = smax[k][0];
+      lo[k] = ordered_value(v.bbox[k * S + s]);
+      double hi = ordered_value(v.bbox[(3 + k) * S + s]);
       if (!(hi >= lo[k])) {  // empty or all-NaN system
         lo[k] = 0;
         hi = 0;
@@ -341,7 +372,13 @@ void launch_nlist_count(Pack &p, cudaStream_t st) {
   PackView &v = p.v;
   int N = v.n_atoms;
   if (N == 0) return;
-  PDGPU_LAUNCH(k_grid_plan, v.n_sys, 256, 0, st, v);
+  // boxes start empty: min keys at the top of the range, max keys at 0
+  cudaMemsetAsync(v.bbox, 0xFF, sizeof(unsigned long long) * 3 * v.n_sys, st);
+  cudaMemsetAsync(v.bbox + 3 * v.n_sys, 0, sizeof(unsigned long long) * 3 * v.n_sys, st);
+  int bb_blocks = (N + 255) / 256;
+  if (bb_blocks > 592) bb_blocks = 592;
+  PDGPU_LAUNCH(k_bbox, bb_blocks, 256, 0, st, v);
+  PDGPU_LAUNCH(k_grid_plan, (v.n_sys + 127) / 128, 128, 0, st, v);
   int *ka = v.cell_key, *va = v.sorted_atom, *kb = p.tmp_keys, *vb = p.tmp_vals;
   PDGPU_LAUNCH(k_cell_keys, (N + 255) / 256, 256, 0, st, v, ka, va);
   int ntiles = (N + kTile - 1) / kTile;
@@ -380,6 +417,8 @@ void launch_nlist_fill(Pack &p, cudaStream_t st) {
   int warps_per_block = 8;
   int blocks = (N + warps_per_block - 1) / warps_per_block;
   PDGPU_LAUNCH((k_nlist_scan<true>), blocks, 32 * warps_per_block, 0, st, v);
+  // the same pair set re-cut into cluster-pair tiles for the tile passes
+  if (v.tile_mode) launch_tiles_build(v, st);
 }
 
 }  // namespace pdgpu

@@ -39,7 +39,8 @@ constexpr size_t kOffCellEnd = kOffCellStart + align256(sizeof(int) * kCellCap);
 constexpr size_t kOffHist = kOffCellEnd + align256(sizeof(int) * kCellCap);
 constexpr size_t kOffScan = kOffHist + align256(sizeof(int) * 256 * kTiles);
 constexpr size_t kOffGrid = kOffScan + align256(sizeof(long long) * kScanLen);
-constexpr size_t kOffFlags = kOffGrid + align256(sizeof(double) * 8);
+constexpr size_t kOffBbox = kOffGrid + align256(sizeof(double) * 8);
+constexpr size_t kOffFlags = kOffBbox + align256(sizeof(unsigned long long) * 6);
 constexpr size_t kOffSmall = kOffFlags + align256(sizeof(int) * F_COUNT);  // atom_off[2], mid, band_off
 constexpr size_t kOffParams = kOffSmall + 256;
 constexpr size_t kScratchBytes = kOffParams + align256(sizeof(SysParams));
@@ -132,6 +133,7 @@ extern "C" int pdgpu_nlist_build_noalloc(const double *x, const double *y, const
   v.cell_end = (int *)(base + kOffCellEnd);
   v.cell_cap = 2 * natoms + 64;
   v.grid = (double *)(base + kOffGrid);
+  v.bbox = (unsigned long long *)(base + kOffBbox);
   v.flags = (int *)(base + kOffFlags);
   p.tmp_keys = (int *)(base + kOffTmpKeys);
   p.tmp_vals = (int *)(base + kOffTmpVals);

@@ -34,47 +34,9 @@
 // r<=Rc), K4 36 flop + 4 SFU (as K2).
 #include <cuda_runtime.h>
 
-#include "internal.cuh"
+#include "pairmath.cuh"
 
 namespace pdgpu {
-
-template <int W, typename T>
-__device__ __forceinline__ T group_sum(T x) {
-#pragma unroll
-  for (int o = W / 2; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-  return x;
-}
-
-// Reciprocal of a double by one FP32 seed and two Newton-Raphson steps
-// (quadratic convergence: 2^-23 -> 2^-46 -> below double rounding).
-__device__ __forceinline__ double rcp_d(double a) {
-  double y = (double)__frcp_rn(__double2float_rn(a));
-  double e = fma(-a, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-a, y, 1.0);
-  return fma(y, e, y);
-}
-
-// The reference's squared distance with its operand order and no
-// contraction: sqrdist(v1,v2) = (g*g + h*h) + j*j, g = v1.x - v2.x.
-__device__ __forceinline__ double ref_d2(double ax, double ay, double az, double bx, double by,
-                                         double bz) {
-  double g = __dsub_rn(ax, bx), h = __dsub_rn(ay, by), k = __dsub_rn(az, bz);
-  return __dadd_rn(__dadd_rn(__dmul_rn(g, g), __dmul_rn(h, h)), __dmul_rn(k, k));
-}
-
-// hi + lo coordinate difference of records a (hi) / b (lo): p_i - p_j
-struct Dx {
-  float x, y, z, r2;
-};
-__device__ __forceinline__ Dx diff(const float4 &ia, const float4 &ib, const float4 &ja, const float4 &jb) {
-  Dx d;
-  d.x = (ia.x - ja.x) + (ib.x - jb.x);
-  d.y = (ia.y - ja.y) + (ib.y - jb.y);
-  d.z = (ia.z - ja.z) + (ib.z - jb.z);
-  d.r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-  return d;
-}
 
 // --------------------------------------------------------------- positions
 // FP64 state -> the pair-kernel records (hi/lo floats, FP64 AoS copy).
@@ -107,6 +69,11 @@ __global__ void k_zero(PackView v) {
     v.gx[i] = 0.0;
     v.gy[i] = 0.0;
     v.gz[i] = 0.0;
+    v.hx[i] = 0;
+    v.hy[i] = 0;
+    v.hz[i] = 0;
+    v.bsum[i] = 0;
+    for (int k = 0; k < 4; k++) v.ej[(size_t)k * v.n_atoms + i] = 0;
 #pragma unroll
     for (int k = 0; k < AE_COUNT; k++) v.e_atom[(size_t)k * v.n_atoms + i] = 0.0;
   }
@@ -122,113 +89,110 @@ void launch_zero(const PackView &v, cudaStream_t st) {
   if (n) PDGPU_LAUNCH(k_zero, (n + 255) / 256, 256, 0, st, v);
 }
 
-// grid of `lpa`-lane groups, 256-thread blocks
-static inline int pair_blocks(int n_atoms, int lpa) { return (int)(((long long)n_atoms * lpa + 255) / 256); }
-
-#define PDGPU_LPA_DISPATCH(lpa, KERN, grid, ...)                                   \
-  switch (lpa) {                                                                   \
-    case 4: PDGPU_LAUNCH((KERN<4>), grid(4), 256, 0, st, __VA_ARGS__); break;       \
-    case 16: PDGPU_LAUNCH((KERN<16>), grid(16), 256, 0, st, __VA_ARGS__); break;    \
-    case 32: PDGPU_LAUNCH((KERN<32>), grid(32), 256, 0, st, __VA_ARGS__); break;    \
-    default: PDGPU_LAUNCH((KERN<8>), grid(8), 256, 0, st, __VA_ARGS__); break;      \
-  }
-
 // --------------------------------------------------------------- K2 radii
+// Born-radius sums in FP32 per term (hi/lo coordinate differences), each
+// term converted to 64-bit fixed point (2^40) before it is added, so the
+// sum is exact in integers: independent of the order of the row, of the
+// lanes per atom and of the batch the system sits in.  The Still cutoff
+// (r <= GbsaStillCutoff, a jump in the sum) is decided in FP64 with the
+// reference's expression when the FP32 distance lies within a guard band;
+// the close-contact factor CCF is continuous at its threshold.  The
+// inversion a_i = -halfeconv / Gpol_i is FP64.
 template <int LPA>
 __global__ void __launch_bounds__(256) k_born(PackView v, int zero_first) {
   if (v.flags[F_NL_OVERFLOW]) return;  // list incomplete: the host re-plans
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / LPA, sub = t % LPA;
-  const bool valid = i < v.n_atoms;
-  const int ii = valid ? i : 0;
-  const int s = v.sys_of[ii];
-  const SysParams &P = v.sp[s];
-  if (valid && zero_first && sub < 3) {
-    // WorkSpace::zeroForces for this atom (and the record, by the first atom)
-    long long *f = sub == 0 ? v.fx : (sub == 1 ? v.fy : v.fz);
-    double *g = sub == 0 ? v.gx : (sub == 1 ? v.gy : v.gz);
-    f[i] = 0;
-    g[i] = 0.0;
-    if (i == v.atom_off[s])
-      for (int k = sub; k < E_COUNT; k += 3)
-        if (k != E_EKIN) v.ene[(size_t)s * E_COUNT + k] = 0.0;
-  }
-  const double4 me = v.xyzp[ii];
-  const double Ri = v.gbR_d[ii];
-  const double still2 = P.still2_d, invP5 = P.invP5_d, P5 = P.P5_d;
-  const long long e = valid ? v.row_start[i + 1] : 0;
-  double acc = 0.0;
+  const int sub = threadIdx.x % LPA;
+  constexpr int G = 256 / LPA;  // atoms per block and pass
+  for (int i0 = blockIdx.x * G; i0 < v.n_atoms; i0 += gridDim.x * G) {
+    const int i = i0 + (int)threadIdx.x / LPA;
+    const bool valid = i < v.n_atoms;
+    const int ii = valid ? i : 0;
+    const int s = v.sys_of[ii];
+    const SysParams &P = v.sp[s];
+    if (valid && zero_first && sub < 3) {
+      // WorkSpace::zeroForces for this atom (and the record, by the first atom)
+      long long *f = sub == 0 ? v.fx : (sub == 1 ? v.fy : v.fz);
+      double *g = sub == 0 ? v.gx : (sub == 1 ? v.gy : v.gz);
+      long long *h = sub == 0 ? v.hx : (sub == 1 ? v.hy : v.hz);
+      f[i] = 0;
+      g[i] = 0.0;
+      h[i] = 0;
+      if (i == v.atom_off[s])
+        for (int k = sub; k < E_COUNT; k += 3)
+          if (k != E_EKIN) v.ene[(size_t)s * E_COUNT + k] = 0.0;
+    }
+    const float4 ia = v.pq[2 * (size_t)ii], ib = v.pq[2 * (size_t)ii + 1];
+    const float Ri = v.chainp[ii].x;
+    const float s_hi = P.still2 * (1.f + 4e-6f), s_lo = P.still2 * (1.f - 4e-6f);
+    const float invP5 = P.invP5, piP5 = P.piP5, P4s = P.P4 * (float)kBornScale;
+    const double still2_d = P.still2_d;
+    long long acc = 0;
+    const long long e = valid ? v.row_start[i + 1] : 0;
 #pragma unroll 2
-  for (long long k = (valid ? v.row_start[i] : 0) + sub; k < e; k += LPA) {
-    unsigned ent = v.nl[k];
-    int j = (int)(ent >> 3);
-    double4 pj = v.xyzp[j];
-    double Rj = v.gbR_d[j];
-    if ((ent & 7u) > 2u) {  // 1-2 and 1-3 partners carry no Born term
-      double d2 = ref_d2(me.x, me.y, me.z, pj.x, pj.y, pj.z);
-      if (!(d2 > still2)) {
-        double Rs = Ri + Rj;
-        double s2 = Rs * Rs;
-        double inv = rcp_d(d2);
-        double term = pj.w * inv * inv;  // P4 * V_j / r^4
-        if (!(d2 > s2 * invP5)) {
-          // close-contact switching factor CCF (rare; exact division + FP64 cos)
-          double rdivR = d2 / s2;
-          double c = 0.5 - 0.5 * cospi(rdivR * P5);  // cos(rdivR * P5 * pi)
-          if (!(rdivR > invP5)) term *= c * c;
-        }
-        acc += term;
+    for (long long k = (valid ? v.row_start[i] : 0) + sub; k < e; k += LPA) {
+      const unsigned ent = v.nl[k];
+      if ((ent & 7u) > 2u) {  // 1-2 and 1-3 partners carry no Born term
+        const int j = (int)(ent >> 3);
+        const float4 ja = v.pq[2 * (size_t)j], jb = v.pq[2 * (size_t)j + 1], jc = v.chainp[j];
+        const Dx d = diff(ia, ib, ja, jb);
+        bool in = d.r2 <= s_lo;
+        if (!in && d.r2 <= s_hi) in = !(ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]) > still2_d);
+        if (in) acc += __float2ll_rn(born_term_noV(d, Ri, jc.x, invP5, piP5, P4s) * jc.y);
       }
     }
+    const long long fixed = group_sum<LPA>(acc);
+    if (valid && sub == 0) {
+      double Gpol = v.terms123[i] + (double)fixed * kInvBornScale;
+      double a = -P.halfeconv_d / Gpol + P.born_offset_d;
+      v.born_d[i] = a;
+      reinterpret_cast<float *>(&v.pq[2 * (size_t)i + 1])[3] = (float)a;
+    }
   }
-  long long fixed = group_sum<LPA>(__double2ll_rn(acc * kBornScale));
-  if (valid && sub == 0) {
-    double Gpol = v.terms123[i] + (double)fixed * kInvBornScale;
-    double a = -P.halfeconv_d / Gpol + P.born_offset_d;
-    v.born_d[i] = a;
-    reinterpret_cast<float *>(&v.pq[2 * (size_t)i + 1])[3] = (float)a;
+}
+
+// Blocks for a persistent pass over the atoms: every SM holds the same
+// number of resident blocks, each walking atoms block-strided.
+template <typename K>
+static int persistent_blocks(K kern, int n_atoms, int lpa) {
+  static int sms = 0, occ = 0;  // per kernel instantiation
+  if (!occ) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, 0) != cudaSuccess || occ <= 0) occ = 1;
   }
+  long long need = ((long long)n_atoms * lpa + 255) / 256;
+  long long cap = (long long)sms * occ;
+  return (int)(need < cap ? need : cap);
 }
 
 void launch_born_radii_lpa(const PackView &v, cudaStream_t st, bool zero_first, int lpa) {
   if (!v.n_atoms) return;
-  auto grid = [&](int l) { return pair_blocks(v.n_atoms, l); };
-  PDGPU_LPA_DISPATCH(lpa, k_born, grid, v, (int)zero_first);
+  switch (lpa) {
+    case 4: PDGPU_LAUNCH(k_born<4>, persistent_blocks(k_born<4>, v.n_atoms, 4), 256, 0, st, v, (int)zero_first); break;
+    case 16: PDGPU_LAUNCH(k_born<16>, persistent_blocks(k_born<16>, v.n_atoms, 16), 256, 0, st, v, (int)zero_first); break;
+    case 32: PDGPU_LAUNCH(k_born<32>, persistent_blocks(k_born<32>, v.n_atoms, 32), 256, 0, st, v, (int)zero_first); break;
+    default: PDGPU_LAUNCH(k_born<8>, persistent_blocks(k_born<8>, v.n_atoms, 8), 256, 0, st, v, (int)zero_first); break;
+  }
 }
 
 // --------------------------------------------------------------- K3 pair
-// Exact FP64 re-evaluation of the reference's GB branch predicate
-// uGB = -srij*0.25/aiaj > ExpApproxThreshold, with srij formed as in
-// gbff.cpp:1553-1556 (dddx = p_i - p_j; sqr+sqr+sqr).
-// (Plain pointer arguments: taking the address of the kernel's PackView
-// parameter would copy it to local memory in every thread.)
-__device__ __forceinline__ bool gb_branch_exact(const double *__restrict__ x, const double *__restrict__ y,
-                                                const double *__restrict__ z, const double *__restrict__ born,
-                                                int i, int j, double thr) {
-  double srij = ref_d2(x[i], y[i], z[i], x[j], y[j], z[j]);
-  double aiaj = born[i] * born[j];
-  double uGB = -srij * 0.25 / aiaj;
-  return uGB > thr;
-}
-
 template <int LPA>
-__global__ void __launch_bounds__(256) k_gb_pair(PackView v) {
+__global__ void __launch_bounds__(256, 4) k_gb_pair(PackView v) {
   if (v.flags[F_NL_OVERFLOW]) return;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / LPA, sub = t % LPA;
+  const int sub = threadIdx.x % LPA;
+  constexpr int G = 256 / LPA;
+  for (int i0 = blockIdx.x * G; i0 < v.n_atoms; i0 += gridDim.x * G) {
+  const int i = i0 + (int)threadIdx.x / LPA;
   const bool valid = i < v.n_atoms;
   const int ii = valid ? i : 0;
   const SysParams &P = v.sp[v.sys_of[ii]];
   const float4 ia = v.pq[2 * (size_t)ii], ib = v.pq[2 * (size_t)ii + 1], ip = v.prm[ii];
   const float ai = ib.w;
   const float qi = ia.w, radi = ip.x, epsi = ip.y;
-  // every setting in registers for the whole row
-  const float thr = P.exp_thresh;
-  const double thr_d = P.exp_thresh_d;
-  const float band = 4e-6f * fabsf(thr);
-  const float rc2 = P.rc2, rin = P.rin, inv_sw2 = P.inv_sw2;
-  const float elec14 = P.elec14, vdw14 = P.vdw14, econv_in = P.econv_in, econv_out = P.econv_out;
-  const float premul = P.premul, vdw_rc = P.vdw_rc, vdw_rin = P.vdw_rin, vdw_inv_sw2 = P.vdw_inv_sw2;
+  GbSettings gs;  // every setting in registers for the whole row
+  gs.load(P);
   float fx = 0.f, fy = 0.f, fz = 0.f;  // -dE/dr_i, kcal/mol/A
   float e_vdw = 0.f, e_el = 0.f, e_pol = 0.f, deda = 0.f;
   const long long e = valid ? v.row_start[i + 1] : 0;
@@ -238,65 +202,17 @@ __global__ void __launch_bounds__(256) k_gb_pair(PackView v) {
     const int j = (int)(ent >> 3);
     const float4 ja = v.pq[2 * (size_t)j], jb = v.pq[2 * (size_t)j + 1], jp = v.prm[j];
     const Dx d = diff(ia, ib, ja, jb);
-    if (d.r2 <= rc2) {
+    if (d.r2 <= gs.rc2) {
       const int bo = (int)(ent & 7u);
-      const bool nb = bo >= 3;   // LJ and vacuum Coulomb apply (1-4 scaled)
-      const bool b14 = bo == 3;
-      const float invr = rsqrtf(d.r2);
-      const float r = d.r2 * invr;
-      const float aj = jb.w;
-      const float qiqj = qi * ja.w;
-      const float aiaj = ai * aj;
-      const float u = __fdividef(-0.25f * d.r2, aiaj);
-      bool gb = u > thr;
-      if (fabsf(u - thr) <= band) gb = gb_branch_exact(v.x, v.y, v.z, v.born_d, i, j, thr_d);
-      // energy switch (applies to GB and Coulomb, gbff.cpp:1602-1614)
-      const float dr = r - rin;
-      const float sw = 1.f - inv_sw2 * dr * dr;
-      const bool on = r >= rin;
-      const float S = on ? sw * sw : 1.f;
-      const float dSdd = on ? -4.f * inv_sw2 * dr * sw : 0.f;
-      // GB cross term (all bond orders), evaluated for every pair, kept
-      // when the exp approximation applies
-      const float tg = __expf(u);
-      const float fgb = rsqrtf(d.r2 + tg * aiaj);
-      const float l = fgb * fgb;
-      const float epol0 = premul * qiqj * fgb;
-      const float dedr0 = -epol0 * (r - 0.25f * r * tg) * l;
-      const float dedal0 = -epol0 * tg * (1.f - u) * l;
-      const float epol = gb ? epol0 * S : 0.f;
-      const float dedr = gb ? S * dedr0 + dSdd * epol0 : 0.f;
-      const float dedal = gb ? dedal0 * S : 0.f;
-      // vacuum Coulomb at the solute (GB branch) or solvent dielectric
-      const float ec = nb ? (gb ? econv_in : econv_out) * (b14 ? elec14 : 1.f) * qiqj * invr : 0.f;
-      const float elf = S * (-ec * invr) + ec * dSdd;
-      const float elec = ec * S;
-      // Lennard-Jones 12-6 with its own switch
-      float vdw = 0.f, vdwf = 0.f;
-      if (nb && r < vdw_rc) {
-        const float rr = (radi + jp.x) * invr;
-        const float rr2 = rr * rr;
-        const float B = rr2 * rr2 * rr2;
-        const float A = B * B;
-        const float eps = epsi * jp.y * (b14 ? vdw14 : 1.0f);
-        vdw = (2.f * eps) * (0.5f * A - B);
-        vdwf = -(12.f * eps * invr) * (A - B);
-        const float vd = r - vdw_rin;
-        const float vs = 1.f - vdw_inv_sw2 * vd * vd;
-        const bool von = r > vdw_rin;
-        const float vS = von ? vs * vs : 1.f;
-        const float vdS = von ? -4.f * vdw_inv_sw2 * vd * vs : 0.f;
-        vdwf = vS * vdwf + vdw * vdS;
-        vdw *= vS;
-      }
-      const float fscal = dedr * 2.f * invr + (vdwf + elf) * invr;
-      e_pol += epol;
-      deda += dedal * aj;
-      e_vdw += vdw;
-      e_el += elec;
-      fx -= fscal * d.x;
-      fy -= fscal * d.y;
-      fz -= fscal * d.z;
+      // LJ and vacuum Coulomb apply from bond order 3 (1-4, scaled) on
+      const GbPair t = gb_pair_term(gs, d, bo >= 3, bo == 3, ai, jb.w, qi, ja.w, radi, jp.x, epsi, jp.y, v, i, j);
+      e_pol += t.epol;
+      deda += t.dedal * jb.w;
+      e_vdw += t.vdw;
+      e_el += t.elec;
+      fx -= t.fscal * d.x;
+      fy -= t.fscal * d.y;
+      fz -= t.fscal * d.z;
     }
   }
   const double sx = group_sum<LPA>((double)fx);
@@ -322,20 +238,27 @@ __global__ void __launch_bounds__(256) k_gb_pair(PackView v) {
     double gpi = ai_d * ai_d / 166.0;  // gbff.cpp:1755 uses the literal 166.0
     reinterpret_cast<float *>(&v.chainp[i])[2] = (float)(gpi * deda_i);
   }
+  }
 }
 
 void launch_gb_pair_lpa(const PackView &v, cudaStream_t st, int lpa) {
   if (!v.n_atoms) return;
-  auto grid = [&](int l) { return pair_blocks(v.n_atoms, l); };
-  PDGPU_LPA_DISPATCH(lpa, k_gb_pair, grid, v);
+  switch (lpa) {
+    case 4: PDGPU_LAUNCH(k_gb_pair<4>, persistent_blocks(k_gb_pair<4>, v.n_atoms, 4), 256, 0, st, v); break;
+    case 16: PDGPU_LAUNCH(k_gb_pair<16>, persistent_blocks(k_gb_pair<16>, v.n_atoms, 16), 256, 0, st, v); break;
+    case 32: PDGPU_LAUNCH(k_gb_pair<32>, persistent_blocks(k_gb_pair<32>, v.n_atoms, 32), 256, 0, st, v); break;
+    default: PDGPU_LAUNCH(k_gb_pair<8>, persistent_blocks(k_gb_pair<8>, v.n_atoms, 8), 256, 0, st, v); break;
+  }
 }
 
 // --------------------------------------------------------------- K4 chain
 template <int LPA>
 __global__ void __launch_bounds__(256) k_gb_chain(PackView v) {
   if (v.flags[F_NL_OVERFLOW]) return;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / LPA, sub = t % LPA;
+  const int sub = threadIdx.x % LPA;
+  constexpr int G = 256 / LPA;
+  for (int i0 = blockIdx.x * G; i0 < v.n_atoms; i0 += gridDim.x * G) {
+  const int i = i0 + (int)threadIdx.x / LPA;
   const bool valid = i < v.n_atoms;
   const int ii = valid ? i : 0;
   const SysParams &P = v.sp[v.sys_of[ii]];
@@ -359,19 +282,7 @@ __global__ void __launch_bounds__(256) k_gb_chain(PackView v) {
         in = !(d2 > still2_d);
       }
       if (in) {
-        const float Rs = Ri + jc.x;
-        const float rdivR = __fdividef(d.r2, Rs * Rs);
-        float X = 4.f;
-        if (!(rdivR > invP5)) {
-          const float th = rdivR * piP5;
-          float sn, cs;
-          __sincosf(th, &sn, &cs);
-          const float sq = 0.5f - 0.5f * cs;
-          X = 4.f * sq * sq - 2.f * sq * sn * th;
-        }
-        const float ir2 = __frcp_rn(d.r2);
-        const float ir6 = ir2 * ir2 * ir2;
-        const float tt = P4 * X * ir6 * (wi * jc.y + jc.z * Vi);
+        const float tt = chain_term(d, Ri, jc.x, Vi, jc.y, wi, jc.z, invP5, piP5, P4);
         fx += tt * d.x;
         fy += tt * d.y;
         fz += tt * d.z;
@@ -386,19 +297,37 @@ __global__ void __launch_bounds__(256) k_gb_chain(PackView v) {
     v.gy[i] += sy;
     v.gz[i] += sz;
   }
+  }
 }
 
 void launch_gb_chain_lpa(const PackView &v, cudaStream_t st, int lpa) {
   if (!v.n_atoms) return;
-  auto grid = [&](int l) { return pair_blocks(v.n_atoms, l); };
-  PDGPU_LPA_DISPATCH(lpa, k_gb_chain, grid, v);
+  switch (lpa) {
+    case 4: PDGPU_LAUNCH(k_gb_chain<4>, persistent_blocks(k_gb_chain<4>, v.n_atoms, 4), 256, 0, st, v); break;
+    case 16: PDGPU_LAUNCH(k_gb_chain<16>, persistent_blocks(k_gb_chain<16>, v.n_atoms, 16), 256, 0, st, v); break;
+    case 32: PDGPU_LAUNCH(k_gb_chain<32>, persistent_blocks(k_gb_chain<32>, v.n_atoms, 32), 256, 0, st, v); break;
+    default: PDGPU_LAUNCH(k_gb_chain<8>, persistent_blocks(k_gb_chain<8>, v.n_atoms, 8), 256, 0, st, v); break;
+  }
 }
 
 void launch_born_radii(const PackView &v, cudaStream_t st, bool zero_first) {
-  launch_born_radii_lpa(v, st, zero_first, v.lpa[0]);
+  if (v.tile_mode)
+    launch_born_radii_tile(v, st, zero_first);
+  else
+    launch_born_radii_lpa(v, st, zero_first, v.lpa[0]);
 }
-void launch_gb_pair(const PackView &v, cudaStream_t st) { launch_gb_pair_lpa(v, st, v.lpa[1]); }
-void launch_gb_chain(const PackView &v, cudaStream_t st) { launch_gb_chain_lpa(v, st, v.lpa[2]); }
+void launch_gb_pair(const PackView &v, cudaStream_t st) {
+  if (v.tile_mode)
+    launch_gb_pair_tile(v, st);
+  else
+    launch_gb_pair_lpa(v, st, v.lpa[1]);
+}
+void launch_gb_chain(const PackView &v, cudaStream_t st) {
+  if (v.tile_mode)
+    launch_gb_chain_tile(v, st);
+  else
+    launch_gb_chain_lpa(v, st, v.lpa[2]);
+}
 
 // --------------------------------------------------------------- Born energy
 // Energy-only Born term: all pairs r <= Rc, no exp threshold, energy switch.

@@ -118,7 +118,7 @@ struct Job {
 
 size_t res_doubles(const Job &j) {
   size_t n = (size_t)j.natoms;
-  size_t d = 9 * n + E_COUNT;
+  size_t d = 12 * n + E_COUNT;
   if (j.spec.kind == PDGPU_JOB_MD) d += 3 * (size_t)j.spec.steps;
   return d;
 }
@@ -271,9 +271,12 @@ void pdgpu_server::enqueue_results(Job *j) {
   cudaMemcpyAsync(r + 6 * n, v.gx, sizeof(double) * n, cudaMemcpyDeviceToHost, j->st);
   cudaMemcpyAsync(r + 7 * n, v.gy, sizeof(double) * n, cudaMemcpyDeviceToHost, j->st);
   cudaMemcpyAsync(r + 8 * n, v.gz, sizeof(double) * n, cudaMemcpyDeviceToHost, j->st);
-  cudaMemcpyAsync(r + 9 * n, v.ene, sizeof(double) * E_COUNT, cudaMemcpyDeviceToHost, j->st);
+  cudaMemcpyAsync(r + 9 * n, v.hx, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
+  cudaMemcpyAsync(r + 10 * n, v.hy, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
+  cudaMemcpyAsync(r + 11 * n, v.hz, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
+  cudaMemcpyAsync(r + 12 * n, v.ene, sizeof(double) * E_COUNT, cudaMemcpyDeviceToHost, j->st);
   if (j->spec.kind == PDGPU_JOB_MD && j->md_done > 0)
-    cudaMemcpyAsync(r + 9 * n + E_COUNT, j->e->hist, sizeof(double) * 3 * (size_t)j->md_done,
+    cudaMemcpyAsync(r + 12 * n + E_COUNT, j->e->hist, sizeof(double) * 3 * (size_t)j->md_done,
                     cudaMemcpyDeviceToHost, j->st);
   j->have_results = true;
   record(j, PH_FINISH);
@@ -318,6 +321,7 @@ void pdgpu_server::admit(Job *j) {
   }
   Pack &P = *e->pack;
   for (int q = 0; q < 3; q++) P.v.lpa[q] = prm.lanes[q];
+  P.v.tile_mode = prm.tiles ? 1 : 0;
   P.tuned = true;
   size_t n = (size_t)j->natoms;
   std::memcpy(j->res, j->x0.data(), sizeof(double) * 3 * n);
@@ -565,6 +569,7 @@ void pdgpu_serve_params_default(pdgpu_serve_params *p) {
   p->hbm_budget = 120LL * 1000 * 1000 * 1000;
   p->max_active = 32;
   p->lanes[0] = p->lanes[1] = p->lanes[2] = 8;
+  p->tiles = 1;
 }
 
 int pdgpu_serve_create(pdgpu_ctx *ctx, const pdgpu_serve_params *p, pdgpu_server **out) {
@@ -639,9 +644,14 @@ int pdgpu_serve_submit(pdgpu_server *s, int32_t sys, const pdgpu_job *job, const
     j->x0[n + i] = xyz[3 * i + 1];
     j->x0[2 * n + i] = xyz[3 * i + 2];
   }
-  // device bytes before the list is sized: per-atom arrays plus a list of
-  // 256 entries per atom (the pack is charged its real size once sized)
-  j->est_bytes = (int64_t)n * (1024 + 256 * 4) + (int64_t)4 * 1024 * 1024;
+  // device bytes before the list is sized: per-atom arrays, a list of 256
+  // entries per atom and the worst-case tile store (40 bytes per tile of
+  // 32 x 8 atoms); the pack is charged its real size once sized
+  {
+    int64_t nsc = ((int64_t)n + 31) / 32, njc = ((int64_t)n + 7) / 8, tiles = 0;
+    for (int64_t k = 0; k < nsc; k++) tiles += njc - 4 * k;
+    j->est_bytes = (int64_t)n * (1024 + 256 * 4) + tiles * 40 + nsc * 16 * 64 + (int64_t)4 * 1024 * 1024;
+  }
   if (j->est_bytes > s->prm.hbm_budget) {
     set_error("pdgpu_serve_submit: the job alone exceeds the HBM budget");
     return PDGPU_ERR_BUDGET;
@@ -735,15 +745,20 @@ int pdgpu_serve_result(pdgpu_server *s, int64_t job_id, double *xyz, double *f, 
       xyz[3 * i + 2] = r[2 * n + i];
     }
   if (f) {
+    // as the integrator sums them: fixed point, FP64 pair, tile j side
     const long long *fx = (const long long *)(r + 3 * n);
+    const long long *hx = (const long long *)(r + 9 * n);
     for (size_t i = 0; i < n; i++)
       for (int c = 0; c < 3; c++)
-        f[3 * i + c] = ((double)fx[c * n + i] * kInvForceScale + r[(6 + c) * n + i]) * k.N_per_kcalmolA;
+        f[3 * i + c] = ((double)fx[c * n + i] * kInvForceScale + r[(6 + c) * n + i] +
+                        (double)hx[c * n + i] * kInvJScale) *
+                       k.N_per_kcalmolA;
   }
   if (ene)
-    for (int q = 0; q < E_COUNT; q++) ene[q] = r[9 * n + q] * k.J_per_kcalmol;
+    for (int q = 0; q < E_COUNT; q++) ene[q] = r[12 * n + q] * k.J_per_kcalmol;
   if (history && j->spec.kind == PDGPU_JOB_MD)
-    for (size_t q = 0; q < 3 * (size_t)j->steps_done; q++) history[q] = r[9 * n + E_COUNT + q] * k.J_per_kcalmol;
+    for (size_t q = 0; q < 3 * (size_t)j->steps_done; q++)
+      history[q] = r[12 * n + E_COUNT + q] * k.J_per_kcalmol;
   return PDGPU_OK;
 }
 

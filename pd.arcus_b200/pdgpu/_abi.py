@@ -64,7 +64,8 @@ class MinParams(ctypes.Structure):
 
 
 class ServeParams(ctypes.Structure):
-    _fields_ = [("hbm_budget", ctypes.c_int64), ("max_active", ctypes.c_int32), ("lanes", ctypes.c_int32 * 3)]
+    _fields_ = [("hbm_budget", ctypes.c_int64), ("max_active", ctypes.c_int32), ("lanes", ctypes.c_int32 * 3),
+                ("tiles", ctypes.c_int32)]
 
 
 class Job(ctypes.Structure):
@@ -146,6 +147,7 @@ PROTOTYPES = {
     "pdgpu_launch_count": (ctypes.c_int, [_CTX, _I64]),
     "pdgpu_autotune": (ctypes.c_int, [_CTX, ctypes.c_int32, _I]),
     "pdgpu_set_lanes": (ctypes.c_int, [_CTX, ctypes.c_int32, _I]),
+    "pdgpu_pair_path": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32, _I]),
     "pdgpu_serve_params_default": (None, [ctypes.POINTER(ServeParams)]),
     "pdgpu_serve_create": (ctypes.c_int, [_CTX, ctypes.POINTER(ServeParams), ctypes.POINTER(ctypes.c_void_p)]),
     "pdgpu_serve_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(Job), _D, _I64]),

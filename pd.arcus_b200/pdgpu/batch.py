@@ -84,6 +84,13 @@ class Batch:
         arr = None if lpa is None else A.iptr(np.ascontiguousarray(lpa, dtype=np.int32))
         A.check(A.lib().pdgpu_set_lanes(self.ctx.ptr, self._id, arr))
 
+    def setPairPath(self, path):
+        """0: neighbour-list rows, 1: cluster-pair tiles, -1: autotune;
+        returns the layout in use."""
+        cur = ctypes.c_int32(0)
+        A.check(A.lib().pdgpu_pair_path(self.ctx.ptr, self._id, int(path), ctypes.byref(cur)))
+        return cur.value
+
     def setSeeds(self, seeds=None):
         if seeds is None:
             A.check(A.lib().pdgpu_set_seeds(self.ctx.ptr, self._id, None))

@@ -236,6 +236,13 @@ class WorkSpace:
         arr = None if lpa is None else A.iptr(np.ascontiguousarray(lpa, dtype=np.int32))
         A.check(A.lib().pdgpu_set_lanes(self.ctx.ptr, self._device(), arr))
 
+    def setPairPath(self, path):
+        """Pair-pass layout: 0 neighbour-list rows, 1 cluster-pair tiles,
+        -1 autotune, -2 report only; returns the layout in use."""
+        cur = ctypes.c_int32(0)
+        A.check(A.lib().pdgpu_pair_path(self.ctx.ptr, self._device(), int(path), ctypes.byref(cur)))
+        return cur.value
+
     def backboneAxes(self):
         """(N, CA) then (CA, C) of every residue in order: the bonds
         setResiduePhiPsi turns for phi and psi."""

@@ -3,7 +3,8 @@ results (tests/golden/, produced by the compiled reference) and the oracle.
 
 Tolerances (stated per quantity, against the FP64 reference):
   neighbour list        bit-exact (sorted pair sets and bond-order bits)
-  Born radii            relative 1e-9 (FP64 sums, fixed-point lane reduction)
+  Born radii            relative 2e-6 (FP32 terms, each added in 64-bit fixed
+                        point; FP64 inversion)
   forces                relative force RMS 1e-5 (FP32 pair arithmetic)
   pair energies         relative 1e-5 of the term, or 1e-3 kcal/mol
   bonded forces/energy  relative 1e-9 (FP64 terms, fixed-point scatter)
@@ -63,7 +64,7 @@ def test_gb_bonded_forces_and_energies(name, gpu_ctx):
     ws.nlist().calcNewList()
     ff.calcForces()
     born = ws.born_radii()
-    assert np.max(np.abs(born - a["born"]) / np.abs(a["born"])) <= 1e-9
+    assert np.max(np.abs(born - a["born"]) / np.abs(a["born"])) <= 2e-6
     assert rel_rms(ws.cur.f, a["f_total"]) <= 1e-5
     et = a["ene_total"]
     e = ws.ene
@@ -173,7 +174,7 @@ def test_full_size_large_system(gpu_ctx):
     ws.nlist().calcNewList()
     ff.calcForces()
     born = ws.born_radii()
-    assert np.max(np.abs(born - a["born"]) / np.abs(a["born"])) <= 1e-9
+    assert np.max(np.abs(born - a["born"]) / np.abs(a["born"])) <= 2e-6
     assert rel_rms(ws.cur.f, a["f_total"]) <= 1e-5
     et = a["ene_total"]
     for field, idx in (("epot_vdw", 1), ("epot_elec", 2), ("epot_pol", 3), ("epot", 0)):

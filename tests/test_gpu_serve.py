@@ -1,11 +1,11 @@
 """GPU: the request loop (pdgpu_serve_*).
 
 A served job must give the same results alone and in a mix of overlapping
-jobs -- bit for bit, since every job runs the same kernels with the same
-fixed lanes per atom on its own device state -- and the same results as
-the plain calls (pdgpu_nlist_build + pdgpu_calc_forces, pdgpu_minimise_run,
-pdgpu_md_run) with those lanes.  Single-point forces also match the
-reference's FP64 forces (relative force RMS 1e-5).
+jobs -- bit for bit, since every job runs the same kernels (the
+cluster-pair tile layout) on its own device state -- and the same results
+as the plain calls (pdgpu_nlist_build + pdgpu_calc_forces,
+pdgpu_minimise_run, pdgpu_md_run) on that layout.  Single-point forces also
+match the reference's FP64 forces (relative force RMS 1e-5).
 """
 import numpy as np
 import pytest
@@ -93,7 +93,7 @@ def test_serve_matches_plain_calls_and_reference(gpu_ctx):
     srv.close()
     for (ws, ff, a, m), job, res, info in zip(members, jobs, served, infos):
         one = pdgpu.Batch([ws])
-        one.setLanes(LANES)
+        one.setPairPath(1)  # the server's layout: cluster-pair tiles
         if job.kind == pdgpu.Server.ENERGY:
             f, e = one.evaluate()
             assert np.array_equal(res["forces"], f)
@@ -119,7 +119,11 @@ def test_serve_budget_admission(gpu_ctx):
     import pdgpu
     members = _members(gpu_ctx, 6)
     ws = max(members, key=lambda m: m[0].nAtoms())[0]
-    est = ws.nAtoms() * (1024 + 256 * 4) + 4 * 1024 * 1024  # the server's admission estimate
+    n = ws.nAtoms()
+    nsc, njc = (n + 31) // 32, (n + 7) // 8
+    tiles = sum(njc - 4 * k for k in range(nsc))
+    # the server's admission estimate (include/pdgpu.h, pdgpu_serve_submit)
+    est = n * (1024 + 256 * 4) + tiles * 40 + nsc * 16 * 64 + 4 * 1024 * 1024
     budget = int(2.5 * est)  # room for two such jobs at a time
     srv = pdgpu.Server(gpu_ctx, hbm_budget=budget, max_active=8, lanes=LANES)
     job = pdgpu.Server.job(pdgpu.Server.MINIMISE, 20)
