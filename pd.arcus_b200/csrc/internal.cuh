@@ -159,17 +159,15 @@ struct PackView {
   unsigned long long *bbox;   // [6*S] ordered-integer box: min x,y,z then max x,y,z (each [S])
   // cluster-pair tiles (tiles.cu): i-clusters of 32 atoms, j-clusters of 8
   int tile_mode;              // 1: the pair passes run on the tiles, 0: on the list rows
-  int n_sc, n_jc;
+  int n_sc;                   // i-clusters over all systems
+  int max_sys_atoms;          // largest system (sizes the tile build's shared memory)
   const int *sc_atom0, *sc_sys;  // [n_sc] first atom, system
-  const int *jc_atom0, *jc_sys;  // [n_jc]
-  const int *jc_off;          // [S+1] j-cluster range of each system
-  double *sc_bb, *jc_bb;      // [6*n] FP64 boxes (min xyz, max xyz)
   int *tile_e0, *tile_e1;     // [n_sc] tile range of each i-cluster
-  int *tile_jc;               // [tile_cap] j-cluster of each tile
-  unsigned *tile_mask;        // [8*tile_cap] list bits: word t = j atom t, bit l = i lane l
-  int *tile_spec;             // [tile_cap] bond-order masks index, -1 none
-  unsigned *spec_mask;        // [16*spec_cap] bond order <= 2 (8 words), == 3 (8 words)
-  int *tile_count;            // [2] tiles, bond-order mask sets allocated
+  int *tile_b0;               // [tile_cap] first atom of each tile's j-cluster
+  unsigned *tile_rows;        // [8*tile_cap] byte l = i lane l's list bits over the 8 j atoms
+  int *tile_spec;             // [tile_cap] bond-order rows index, -1 none
+  unsigned *spec_rows;        // [16*spec_cap] bytes 0..31 bond order <= 2, 32..63 == 3
+  int *tile_count;            // [2] tiles, bond-order row sets allocated
   long long tile_cap, spec_cap;
   long long *bsum;            // [N] Born sums of the tile pass, fixed point 2^40
   long long *hx, *hy, *hz;    // [N] j-side pair forces, fixed point 2^24 kcal/mol/A

@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(256) k_born(PackView v, int zero_first) {
         const Dx d = diff(ia, ib, ja, jb);
         bool in = d.r2 <= s_lo;
         if (!in && d.r2 <= s_hi) in = !(ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]) > still2_d);
-        if (in) acc += __float2ll_rn(born_term_noV(d, Ri, jc.x, invP5, piP5, P4s) * jc.y);
+        if (in) acc += __float2ll_rn(__fmul_rn(born_term_noV(d, Ri, jc.x, invP5, piP5, P4s), jc.y));
       }
     }
     const long long fixed = group_sum<LPA>(acc);

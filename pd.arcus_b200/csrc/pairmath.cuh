@@ -23,16 +23,19 @@ __device__ __forceinline__ double ref_d2(double ax, double ay, double az, double
   return __dadd_rn(__dadd_rn(__dmul_rn(g, g), __dmul_rn(h, h)), __dmul_rn(k, k));
 }
 
-// hi + lo coordinate difference of records a (hi) / b (lo): p_i - p_j
+// hi + lo coordinate difference of records a (hi) / b (lo): p_i - p_j.
+// The square is spelled out with explicit FMAs so every kernel (row or
+// tile, i or j side) gets the same bits for a pair: d(j,i) = -d(i,j)
+// exactly, and the square does not depend on how a compiler contracts.
 struct Dx {
   float x, y, z, r2;
 };
 __device__ __forceinline__ Dx diff(const float4 &ia, const float4 &ib, const float4 &ja, const float4 &jb) {
   Dx d;
-  d.x = (ia.x - ja.x) + (ib.x - jb.x);
-  d.y = (ia.y - ja.y) + (ib.y - jb.y);
-  d.z = (ia.z - ja.z) + (ib.z - jb.z);
-  d.r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+  d.x = __fadd_rn(__fsub_rn(ia.x, ja.x), __fsub_rn(ib.x, jb.x));
+  d.y = __fadd_rn(__fsub_rn(ia.y, ja.y), __fsub_rn(ib.y, jb.y));
+  d.z = __fadd_rn(__fsub_rn(ia.z, ja.z), __fsub_rn(ib.z, jb.z));
+  d.r2 = __fmaf_rn(d.z, d.z, __fmaf_rn(d.y, d.y, __fmul_rn(d.x, d.x)));
   return d;
 }
 
@@ -179,15 +182,17 @@ __device__ __forceinline__ float chain_term(const Dx &d, float Ri, float Rj, flo
 // the caller multiplies by the partner's V.  CCF is symmetric in i and j.
 __device__ __forceinline__ float born_term_noV(const Dx &d, float Ri, float Rj, float invP5, float piP5,
                                                float P4scaled) {
-  const float Rs = Ri + Rj;
+  // explicit roundings: the i and j sides of a pair, in any kernel, get
+  // the same bits
+  const float Rs = __fadd_rn(Ri, Rj);
   const float ir2 = __frcp_rn(d.r2);
-  float term = P4scaled * ir2 * ir2;
-  const float rdivR = __fdividef(d.r2, Rs * Rs);
+  float term = __fmul_rn(__fmul_rn(P4scaled, ir2), ir2);
+  const float rdivR = __fdividef(d.r2, __fmul_rn(Rs, Rs));
   if (!(rdivR > invP5)) {
     // CCF = (1/2 - 1/2 cos(pi P5 r^2/(Ri+Rj)^2))^2 = sin^4(pi P5 r^2/(2 (Ri+Rj)^2))
-    const float sh = __sinf(0.5f * piP5 * rdivR);
-    const float c = sh * sh;
-    term *= c * c;
+    const float sh = __sinf(__fmul_rn(__fmul_rn(0.5f, piP5), rdivR));
+    const float c = __fmul_rn(sh, sh);
+    term = __fmul_rn(term, __fmul_rn(c, c));
   }
   return term;
 }

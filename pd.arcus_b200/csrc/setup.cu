@@ -308,25 +308,23 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   off_ptr[N] = (int)off_data.size();
 
   // cluster-pair tiles: i-clusters of 32 and j-clusters of 8 atoms per
-  // system in atom order; capacities are worst cases (no overflow path)
-  std::vector<int> sc_atom0, sc_sys, jc_atom0, jc_sys, jc_off(S + 1, 0);
+  // system in atom order; capacities are worst cases (no overflow path):
+  // every j-cluster at or after an i-cluster, and for the bond-order rows
+  // every tile within MaxIndexDelta of it plus one per off-diagonal pair
+  std::vector<int> sc_atom0, sc_sys;
   long long tile_cap = 0, spec_cap = 0;
+  int max_sys = 0;
   for (int s = 0; s < S; s++) {
     int o = p->atom_off[s], n = systems[s]->natoms;
+    max_sys = std::max(max_sys, n);
     int nsc = (n + 31) / 32, njc = (n + 7) / 8;
     for (int k = 0; k < nsc; k++) {
       sc_atom0.push_back(o + 32 * k);
       sc_sys.push_back(s);
-      tile_cap += njc - 4 * k;  // j-clusters at or after the i-cluster
-    }
-    jc_off[s] = (int)jc_atom0.size();
-    for (int k = 0; k < njc; k++) {
-      jc_atom0.push_back(o + 8 * k);
-      jc_sys.push_back(s);
+      tile_cap += njc - 4 * k;
     }
     spec_cap += (long long)nsc * ((32 + systems[s]->mid) / 8 + 3);
   }
-  jc_off[S] = (int)jc_atom0.size();
   spec_cap += (long long)off_data.size();
 
   // device allocations
@@ -405,24 +403,19 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   p->radix_passes = (bits + 7) / 8;
   // cluster-pair tiles and the accumulators of the tile passes
   {
-    int *sc_atom0_d, *sc_sys_d, *jc_atom0_d, *jc_sys_d, *jc_off_d;
+    int *sc_atom0_d, *sc_sys_d;
     v.n_sc = (int)sc_atom0.size();
-    v.n_jc = (int)jc_atom0.size();
+    v.max_sys_atoms = max_sys;
     v.tile_cap = tile_cap;
     v.spec_cap = spec_cap;
     PALLOC(sc_atom0_d, sc_atom0.size());
     PALLOC(sc_sys_d, sc_sys.size());
-    PALLOC(jc_atom0_d, jc_atom0.size());
-    PALLOC(jc_sys_d, jc_sys.size());
-    PALLOC(jc_off_d, S + 1);
-    PALLOC(v.sc_bb, 6 * sc_atom0.size());
-    PALLOC(v.jc_bb, 6 * jc_atom0.size());
     PALLOC(v.tile_e0, sc_atom0.size());
     PALLOC(v.tile_e1, sc_atom0.size());
-    PALLOC(v.tile_jc, (size_t)tile_cap);
-    PALLOC(v.tile_mask, 8 * (size_t)tile_cap);
+    PALLOC(v.tile_b0, (size_t)tile_cap);
+    PALLOC(v.tile_rows, 8 * (size_t)tile_cap);
     PALLOC(v.tile_spec, (size_t)tile_cap);
-    PALLOC(v.spec_mask, 16 * (size_t)spec_cap);
+    PALLOC(v.spec_rows, 16 * (size_t)spec_cap);
     PALLOC(v.tile_count, 2);
     PALLOC(v.bsum, N);
     PALLOC(v.hx, N);
@@ -433,15 +426,9 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
     if (!sc_atom0.empty()) {
       cudaMemcpyAsync(sc_atom0_d, sc_atom0.data(), sizeof(int) * sc_atom0.size(), cudaMemcpyHostToDevice, st);
       cudaMemcpyAsync(sc_sys_d, sc_sys.data(), sizeof(int) * sc_sys.size(), cudaMemcpyHostToDevice, st);
-      cudaMemcpyAsync(jc_atom0_d, jc_atom0.data(), sizeof(int) * jc_atom0.size(), cudaMemcpyHostToDevice, st);
-      cudaMemcpyAsync(jc_sys_d, jc_sys.data(), sizeof(int) * jc_sys.size(), cudaMemcpyHostToDevice, st);
     }
-    cudaMemcpyAsync(jc_off_d, jc_off.data(), sizeof(int) * (S + 1), cudaMemcpyHostToDevice, st);
     v.sc_atom0 = sc_atom0_d;
     v.sc_sys = sc_sys_d;
-    v.jc_atom0 = jc_atom0_d;
-    v.jc_sys = jc_sys_d;
-    v.jc_off = jc_off_d;
     v.tile_mode = 0;
   }
 
