@@ -964,8 +964,17 @@ static int ensure_tuned(pdgpu_ctx *c, Pack &P) {
   // the cluster-pair tile path against the tuned row path (three passes)
   if (r == PDGPU_OK && P.v.n_sc > 0) {
     t.tile_mode = 1;
-    launch_tiles_build(t, c->st);
-    float tot = 0;
+    // the tile build comes with every list rebuild: counted at the MD
+    // default cadence (one rebuild per 10 evaluations)
+    float build = 0;
+    for (int rep = 0; rep < 2 && r == PDGPU_OK; rep++) {
+      cudaEventRecord(a, c->st);
+      launch_tiles_build(t, c->st);
+      cudaEventRecord(b, c->st);
+      r = sync_check(c, "autotune tile build");
+      cudaEventElapsedTime(&build, a, b);
+    }
+    float tot = 0.1f * 3.f * build;  // three timed repetitions below
     for (int rep = 0; rep < 4 && r == PDGPU_OK; rep++) {
       cudaEventRecord(a, c->st);
       launch_born_radii_tile(t, c->st, false);

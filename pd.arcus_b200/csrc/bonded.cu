@@ -47,7 +47,7 @@ __device__ __forceinline__ void angle_term(const PackView &v, int t, double *e_t
   }
   double cs = ui[0] * uj[0] + ui[1] * uj[1] + ui[2] * uj[2];
   double theta = acos(cs);
-  double sn = sin(theta);
+  double sn = sqrt(fmax(0.0, 1.0 - cs * cs));  // sin(acos(cs)) without a second transcendental
   double dth = theta - kt.y;
   e_term[t] = kt.x * dth * dth;
   double fm = 2 * kt.x * dth;
@@ -78,7 +78,17 @@ __device__ __forceinline__ void dihedral_term(const PackView &v, int t, double *
   double cos_phi = (n1[0] * n2[0] + n1[1] * n2[1] + n1[2] * n2[2]) * in1 * in2;
   double sin_phi = (n3[0] * n2[0] + n3[1] * n2[1] + n3[2] * n2[2]) * in3 * in2;
   for (int k = 0; k < 3; k++) n2[k] *= in2;
-  double phi = -atan2(sin_phi, cos_phi);
+  // phi = -atan2(sin_phi, cos_phi) (ffbonded.cpp:1261); the Fourier terms
+  // with integer periodicity 1..6 need only cos(n phi) and sin(n phi), from
+  // powers of cos(phi) + i sin(phi); phi itself only for the others
+  const double hinv = 1.0 / sqrt(cos_phi * cos_phi + sin_phi * sin_phi);
+  const double c1 = cos_phi * hinv, s1 = -sin_phi * hinv;
+  bool need_phi = false;
+  for (int m = 0; m < terms; m++) {
+    double n = par[4 + m];
+    need_phi |= !(n > 0 && n <= 6 && n == floor(n));
+  }
+  double phi = need_phi ? -atan2(sin_phi, cos_phi) : 0.0;
   bool use_cos = fabs(sin_phi) > 0.1;
   double d1[3], d2[3];
   if (use_cos) {
@@ -100,9 +110,24 @@ __device__ __forceinline__ void dihedral_term(const PackView &v, int t, double *
   for (int m = 0; m < terms; m++) {
     double k = par[m], n = par[4 + m], gamma = par[8 + m];
     double ep, dE;
-    if (n > 0) {
-      ep = k * (1.0 + cos(n * phi + gamma));
-      dE = -n * k * sin(n * phi + gamma);
+    if (n > 0 && n <= 6 && n == floor(n)) {
+      // cos(n phi + gamma), sin(n phi + gamma) from (c1 + i s1)^n
+      double cn = c1, sn = s1;
+      for (int p = 1; p < (int)n; p++) {
+        double t = cn * c1 - sn * s1;
+        sn = sn * c1 + cn * s1;
+        cn = t;
+      }
+      double sg, cg;
+      sincos(gamma, &sg, &cg);
+      double cv = cn * cg - sn * sg, sv = sn * cg + cn * sg;
+      ep = k * (1.0 + cv);
+      dE = -n * k * sv;
+    } else if (n > 0) {
+      double sv, cv;
+      sincos(n * phi + gamma, &sv, &cv);
+      ep = k * (1.0 + cv);
+      dE = -n * k * sv;
     } else {
       double diff = phi - gamma;
       if (diff < -PI)

@@ -1,16 +1,14 @@
 // Energy record (Hamiltonian, workspace/hamiltonian.h:23-49) from the
 // per-atom and per-term energies the force kernels write.
 //
-// Two stages, both in a fixed order so every total is bit-reproducible:
-//   k_energy_partial  grid (chunks, systems): each block sums one 1024-item
-//                     chunk of each range of one system (per-atom terms and
-//                     the bond / angle / dihedral term arrays)
-//   k_energy_final    one block per system: sums the chunk partials in
-//                     chunk order, applies them to the record with the
-//                     reference's semantics (the GB and stand-alone
-//                     LJ/Coulomb components assign epot_vdw / epot_elec,
-//                     everything else accumulates), and in a step loop
-//                     records the step's energies and advances the step.
+// One kernel, two stages, both in a fixed order so every total is
+// bit-reproducible: each block of the grid (chunks, systems) sums one
+// 1024-item chunk of each range of one system (per-atom terms and the bond
+// / angle / dihedral term arrays); the last block of a system to finish
+// adds the chunk partials in chunk order, applies them to the record with
+// the reference's semantics (the GB and stand-alone LJ/Coulomb components
+// assign epot_vdw / epot_elec, everything else accumulates), and in a step
+// loop records the step's energies and advances the step.
 #include <cuda_runtime.h>
 
 #include "internal.cuh"
@@ -18,25 +16,20 @@
 namespace pdgpu {
 
 constexpr int kChunk = 1024;
+constexpr int kEnergyThreads = 256;
 // partial slots
 enum { P_VDW = 0, P_ELEC, P_POL, P_SELF, P_NBVIR, P_KIN, P_BOND, P_BVIR, P_ANGLE, P_DIH, P_COUNT };
 
-__device__ __forceinline__ double block_sum(double x, double *sh) {
-  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __syncthreads();
-  if (lane == 0) sh[w] = x;
-  __syncthreads();
-  double r = 0;
-  if (threadIdx.x == 0)
-    for (int k = 0; k < (int)(blockDim.x >> 5); k++) r += sh[k];
-  return r;  // valid in thread 0
-}
-
-__global__ void k_energy_partial(PackView v, int mode, int C) {
+// hist: [step][sys][3] (epot, ekin, etot); step_dev[0] current step,
+// step_dev[1] first step of the run, step_dev[2] finished-system counter.
+__global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode, int C, double J2kcalmol,
+                                                           double *hist, int *step_dev) {
   if (v.flags[F_NL_OVERFLOW]) return;
   const int c = blockIdx.x, s = blockIdx.y, N = v.n_atoms;
-  __shared__ double sh[32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ double sh[kEnergyThreads / 32][P_COUNT];
+  __shared__ double tot[P_COUNT];
+  __shared__ int last;
   double acc[P_COUNT];
 #pragma unroll
   for (int k = 0; k < P_COUNT; k++) acc[k] = 0.0;
@@ -71,28 +64,35 @@ __global__ void k_energy_partial(PackView v, int mode, int C) {
       for (int t = d0 + threadIdx.x; t < d1; t += blockDim.x) acc[P_DIH] += v.bt.e_dih[t];
     }
   }
-  double *out = v.e_part + ((size_t)s * C + c) * P_COUNT;
+  // block partials: warp trees, then the warps in order
 #pragma unroll
-  for (int k = 0; k < P_COUNT; k++) {
-    double t = block_sum(acc[k], sh);
-    if (threadIdx.x == 0) out[k] = t;
-  }
-}
-
-// hist: [step][sys][3] (epot, ekin, etot); step_dev[0] current step,
-// step_dev[1] first step of the run, step_dev[2] finished-block counter.
-__global__ void k_energy_final(PackView v, int mode, int C, double J2kcalmol, double *hist, int *step_dev) {
-  if (v.flags[F_NL_OVERFLOW]) return;
-  const int s = blockIdx.x;
-  __shared__ double tot[P_COUNT];
+  for (int k = 0; k < P_COUNT; k++)
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < P_COUNT; k++) sh[warp][k] = acc[k];
+  __syncthreads();
+  double *part = v.e_part + (size_t)s * C * P_COUNT;
   if (threadIdx.x < P_COUNT) {
-    double t = 0;
-    const double *p = v.e_part + (size_t)s * C * P_COUNT + threadIdx.x;
-    for (int c = 0; c < C; c++) t += p[(size_t)c * P_COUNT];
+    double t = 0.0;
+    for (int w = 0; w < kEnergyThreads / 32; w++) t += sh[w][threadIdx.x];
+    part[(size_t)c * P_COUNT + threadIdx.x] = t;
+  }
+  // the last block of this system to finish forms the record
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&v.e_done[s], 1) == C - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x < P_COUNT) {
+    double t = 0.0;
+    for (int q = 0; q < C; q++) t += __ldcg(part + (size_t)q * P_COUNT + threadIdx.x);
     tot[threadIdx.x] = t;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
+    v.e_done[s] = 0;
     double *E = v.ene + (size_t)s * E_COUNT;
     if (mode & (EM_PAIR_GB | EM_PAIR_NB)) {
       E[E_VDW] = tot[P_VDW];
@@ -151,8 +151,7 @@ void launch_energy(const PackView &v, cudaStream_t st, int mode, double *hist, i
   if (!v.n_sys) return;
   const Consts &k = consts();
   int C = v.e_chunks;
-  PDGPU_LAUNCH(k_energy_partial, dim3(C, v.n_sys), 256, 0, st, v, mode, C);
-  PDGPU_LAUNCH(k_energy_final, v.n_sys, 32, 0, st, v, mode, C, k.J2kcal * k.Na, hist, step_dev);
+  PDGPU_LAUNCH(k_energy, dim3(C, v.n_sys), kEnergyThreads, 0, st, v, mode, C, k.J2kcal * k.Na, hist, step_dev);
 }
 
 }  // namespace pdgpu

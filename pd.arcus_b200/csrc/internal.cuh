@@ -130,6 +130,7 @@ struct PackView {
   double *e_atom;             // [AE_COUNT * N]
   double *ene;                // [S * E_COUNT] J-free kcal/mol accumulators
   double *e_part;             // [S * e_chunks * 10] reduction partials
+  int *e_done;                // [S] blocks of the energy reduction finished (reset by the last)
   int e_chunks;               // 1024-item chunks of the largest per-system range
   int lpa[3];                 // lanes per atom of the Born, fused-pair and chain kernels
   // backbone torsion moves (Monte Carlo trial conformations)

@@ -569,7 +569,7 @@ void pdgpu_serve_params_default(pdgpu_serve_params *p) {
   p->hbm_budget = 120LL * 1000 * 1000 * 1000;
   p->max_active = 32;
   p->lanes[0] = p->lanes[1] = p->lanes[2] = 8;
-  p->tiles = 1;
+  p->tiles = 0;  // list rows: minimisation rebuilds the list every step
 }
 
 int pdgpu_serve_create(pdgpu_ctx *ctx, const pdgpu_serve_params *p, pdgpu_server **out) {

@@ -578,6 +578,7 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   v.e_chunks = (max_range + 1023) / 1024;
   if (v.e_chunks < 1) v.e_chunks = 1;
   PALLOC(v.e_part, (size_t)S * v.e_chunks * 10);
+  PALLOC(v.e_done, S);
   PALLOC(bt.bij, bij.size());
   PALLOC(bt.blk, blk.size());
   PALLOC(bt.aiaj, aiaj.size());

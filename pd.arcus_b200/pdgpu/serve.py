@@ -19,7 +19,7 @@ from . import _abi as A
 class Server:
     ENERGY, MINIMISE, MD = A.JOB_ENERGY, A.JOB_MINIMISE, A.JOB_MD
 
-    def __init__(self, ctx, hbm_budget=None, max_active=None, lanes=(8, 8, 8), tiles=True):
+    def __init__(self, ctx, hbm_budget=None, max_active=None, lanes=(8, 8, 8), tiles=False):
         self.ctx = ctx
         p = A.ServeParams()
         A.lib().pdgpu_serve_params_default(ctypes.byref(p))

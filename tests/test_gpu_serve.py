@@ -1,11 +1,12 @@
 """GPU: the request loop (pdgpu_serve_*).
 
 A served job must give the same results alone and in a mix of overlapping
-jobs -- bit for bit, since every job runs the same kernels (the
-cluster-pair tile layout) on its own device state -- and the same results
-as the plain calls (pdgpu_nlist_build + pdgpu_calc_forces,
-pdgpu_minimise_run, pdgpu_md_run) on that layout.  Single-point forces also
-match the reference's FP64 forces (relative force RMS 1e-5).
+jobs -- bit for bit, since every job runs the same kernels (list rows with
+fixed lanes per atom, or the cluster-pair tiles) on its own device state --
+and the same results as the plain calls (pdgpu_nlist_build +
+pdgpu_calc_forces, pdgpu_minimise_run, pdgpu_md_run) on that layout.
+Single-point forces also match the reference's FP64 forces (relative force
+RMS 1e-5).
 """
 import numpy as np
 import pytest
@@ -66,11 +67,12 @@ def _run(server, members, jobs, together):
     return out, infos
 
 
-def test_serve_alone_equals_mixed(gpu_ctx):
+@pytest.mark.parametrize("tiles", [False, True])
+def test_serve_alone_equals_mixed(gpu_ctx, tiles):
     import pdgpu
     members = _members(gpu_ctx, 6)
     jobs = _jobs(pdgpu)
-    srv = pdgpu.Server(gpu_ctx, max_active=8, lanes=LANES)
+    srv = pdgpu.Server(gpu_ctx, max_active=8, lanes=LANES, tiles=tiles)
     alone, _ = _run(srv, members, jobs, together=False)
     mixed, infos = _run(srv, members, jobs, together=True)
     st = srv.stats()
@@ -93,7 +95,7 @@ def test_serve_matches_plain_calls_and_reference(gpu_ctx):
     srv.close()
     for (ws, ff, a, m), job, res, info in zip(members, jobs, served, infos):
         one = pdgpu.Batch([ws])
-        one.setPairPath(1)  # the server's layout: cluster-pair tiles
+        one.setLanes(LANES)  # the server's layout: list rows with these lanes
         if job.kind == pdgpu.Server.ENERGY:
             f, e = one.evaluate()
             assert np.array_equal(res["forces"], f)
