@@ -293,7 +293,8 @@ def compose(parts, spacing=25.0):
     return res
 
 
-def bench_serving(pdgpu, A, ctx, torch, n_requests=300, rate=200.0, budget=120e9, max_active=32, seed=5):
+def bench_serving(pdgpu, A, ctx, torch, n_requests=300, rate=200.0, budget=120e9, max_active=32, seed=5,
+                  policy=1, tiles=False):
     lib = load_library(LIB_SP)
     meta = lib[0][1]
     rng = np.random.default_rng(seed)
@@ -343,7 +344,8 @@ def bench_serving(pdgpu, A, ctx, torch, n_requests=300, rate=200.0, budget=120e9
             jobs.append(S.job(S.MD, 2000, md=m, init_temp=300.0))
     L = A.lib()
     # served: submit at the arrival times, the worker overlaps the jobs
-    srv = pdgpu.Server(ctx, hbm_budget=budget, max_active=max_active, lanes=(8, 8, 8))
+    srv = pdgpu.Server(ctx, hbm_budget=budget, max_active=max_active, lanes=(8, 8, 8), tiles=tiles,
+                       policy=policy)
     lc0 = L_count(L, ctx)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -399,6 +401,9 @@ def bench_serving(pdgpu, A, ctx, torch, n_requests=300, rate=200.0, budget=120e9
             "speedup_jobs_per_s_vs_plain": (n_requests / makespan) / (n_requests / plain_makespan),
             "system_atoms": {"min": int(sizes.min()), "max": int(sizes.max()), "templates": n_tmpl},
             "hbm_budget_bytes": int(budget), "max_active": max_active, "peak_active": st["peak_active"],
+            "admission": "least work first" if policy == 1 else "arrival order",
+            "pair_path": "tiles" if tiles else "rows (8 lanes per atom)",
+            "device_max_connections": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS"),
             "peak_bytes": st["peak_bytes"], "failed": st["failed"], "gpu_launches": int(lc1 - lc0),
             "timing": "wall clock: latency = finish - arrival per job; jobs/s = requests / makespan"}
 
@@ -524,6 +529,9 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched workloads")
     ap.add_argument("--batched-md-steps", type=int, default=5000)
     ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--serve-policy", type=int, default=1, help="0 arrival order, 1 least work first")
+    ap.add_argument("--serve-max-active", type=int, default=32)
+    ap.add_argument("--serve-tiles", action="store_true")
     args = ap.parse_args()
     rank, world, local = rank_info()
     n_gpus = max(args.gpus, world)
@@ -722,7 +730,9 @@ def main():
     if not args.no_batched:
         line["batched_sp"] = bench_batched_sp(pdgpu, A, ctx, torch)
         line["batched_md"] = bench_batched_md(pdgpu, A, ctx, torch, steps=args.batched_md_steps)
-        line["serving"] = bench_serving(pdgpu, A, ctx, torch, n_requests=args.serve_requests)
+        line["serving"] = bench_serving(pdgpu, A, ctx, torch, n_requests=args.serve_requests,
+                                        policy=args.serve_policy, max_active=args.serve_max_active,
+                                        tiles=args.serve_tiles)
     if rank == 0 and n_gpus == 1 and not args.no_cpu_baseline:
         try:
             cb = run_reference(args, 1)

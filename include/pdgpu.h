@@ -320,8 +320,9 @@ int pdgpu_minimise_run(pdgpu_ctx *ctx, int32_t sys, const pdgpu_min_params *p,
  * keeps its coordinates, neighbour list, Born radii and protocol state on
  * the device until it finishes; jobs that arrive while others run are
  * admitted as soon as a stream slot is free and their memory fits under the
- * HBM budget (first fit in arrival order), and their kernels overlap with
- * the running jobs'.  All jobs use the same pair-pass layout (and fixed
+ * HBM budget (in arrival order, or least work -- atoms x steps -- first
+ * with jobs queued for more than a second ahead of the rest), and their
+ * kernels overlap with the running jobs'.  All jobs use the same pair-pass layout (and fixed
  * lanes per atom on the row layout), so a job's results are bit-identical
  * alone and in any mix.  A job's memory estimate before admission is
  * natoms * 2048 bytes + 40 bytes per possible 32 x 8 tile + 4 MiB; once its
@@ -333,6 +334,8 @@ typedef struct {
   int32_t max_active;   /* jobs on the device at once (one stream each)       */
   int32_t lanes[3];     /* lanes per atom: Born, fused pair, chain (4..32)    */
   int32_t tiles;        /* 1: cluster-pair tile passes, 0: list-row passes    */
+  int32_t policy;       /* admission order: 0 arrival, 1 least work first     */
+  int32_t _reserved;
 } pdgpu_serve_params;
 void pdgpu_serve_params_default(pdgpu_serve_params *p);
 

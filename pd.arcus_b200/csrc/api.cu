@@ -901,6 +901,8 @@ static int need_list(Pack &P) {
 static int ensure_tuned(pdgpu_ctx *c, Pack &P) {
   if (P.tuned || P.v.n_atoms == 0 || !P.have_list) return PDGPU_OK;
   const int N = P.v.n_atoms;
+  int re = pack_ensure_tiles(&P);  // the tile layout is timed too
+  if (re) return re;
   PackView t = P.v;
   t.tile_mode = 0;
   // scratch for every array the timed launches accumulate into
@@ -1458,7 +1460,14 @@ int pdgpu_pair_counts(pdgpu_ctx *c, int32_t sys, int64_t *counts) {
   PDGPU_CUDA(cudaMalloc(&d, 5 * sizeof(unsigned long long)));
   cudaMemsetAsync(d, 0, 5 * sizeof(unsigned long long), c->st);
   launch_pair_counts(P.v, c->st, d);
-  if (!P.v.tile_mode) launch_tiles_build(P.v, c->st);  // the tiles of the current list, for the counts
+  if (!P.v.tile_mode) {  // the tiles of the current list, for the counts
+    int re = pack_ensure_tiles(&P);
+    if (re) {
+      cudaFree(d);
+      return re;
+    }
+    launch_tiles_build(P.v, c->st);
+  }
   launch_tile_counts(P.v, c->st, d + 3);
   unsigned long long h[5];
   cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, c->st);
@@ -1555,7 +1564,11 @@ int pdgpu_pair_path(pdgpu_ctx *c, int32_t sys, int32_t set, int32_t *current) {
     } else {
       P.v.tile_mode = set;
       P.tuned = true;
-      if (set == 1 && P.have_list) launch_tiles_build(P.v, c->st);  // tiles for the current list
+      if (set == 1) {
+        int re = pack_ensure_tiles(&P);
+        if (re) return re;
+        if (P.have_list) launch_tiles_build(P.v, c->st);  // tiles for the current list
+      }
       int r = sync_check(c, "pair_path");
       if (r) return r;
     }

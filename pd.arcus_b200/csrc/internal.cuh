@@ -238,6 +238,8 @@ struct Pack {
 Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHost *> &systems,
                   std::string *err, bool sync = true);
 void pack_set_params(Pack *p, int s, const pdgpu_ff_params &prm);
+// allocate the cluster-pair tile store of a pack (once; enqueued on p->st)
+int pack_ensure_tiles(Pack *p);
 SysParams make_sys_params(const pdgpu_ff_params &p);
 
 // Host setup computations (restate the reference's setup code).

@@ -13,8 +13,9 @@
 // next phase is enqueued when the event has completed.  Kernels of different
 // jobs therefore overlap on the device, and a job that arrives while others
 // run is admitted as soon as a stream slot and its memory estimate fit under
-// the HBM budget (first fit in arrival order).  Every job runs the kernels
-// the plain calls run, with fixed lanes per atom, so its results do not
+// the HBM budget (in arrival order, or least work first with jobs that
+// waited over a second ahead of the rest).  Every job runs the kernels the
+// plain calls run, with one fixed pair-pass layout, so its results do not
 // depend on what else is on the device.
 #include <algorithm>
 #include <chrono>
@@ -72,6 +73,8 @@ class PinnedPool {
 };
 
 enum Phase { PH_QUEUED, PH_SIZE, PH_MIN, PH_MD, PH_FINISH, PH_DONE, PH_FAILED };
+
+constexpr double kAgeMs = 1000.0;  // least-work admission: a job queued this long goes first
 
 // what the device writes back between phases (page-locked)
 struct PinHead {
@@ -323,6 +326,10 @@ void pdgpu_server::admit(Job *j) {
   for (int q = 0; q < 3; q++) P.v.lpa[q] = prm.lanes[q];
   P.v.tile_mode = prm.tiles ? 1 : 0;
   P.tuned = true;
+  if (prm.tiles && (r = pack_ensure_tiles(&P))) {
+    fail(j, r, last_error_cstr());
+    return;
+  }
   size_t n = (size_t)j->natoms;
   std::memcpy(j->res, j->x0.data(), sizeof(double) * 3 * n);
   cudaMemcpyAsync(P.v.x, j->res, sizeof(double) * n, cudaMemcpyHostToDevice, j->st);
@@ -533,13 +540,29 @@ void pdgpu_server::run() {
         a++;
       }
     }
-    for (size_t q = 0; q < queue.size() && !free_slots.empty();) {
-      Job *j = queue[q];
-      if (bytes_in_use + j->est_bytes > prm.hbm_budget) {
-        q++;
-        continue;
+    // Admission order: arrival (policy 0), or jobs that have waited longer
+    // than kAgeMs first (in arrival order) and then the least work (atoms x
+    // steps) first (policy 1); a job is admitted when a slot is free and its
+    // estimate fits the budget.
+    while (!free_slots.empty()) {
+      const auto now = Clock::now();
+      int pick = -1;
+      double best = 0;
+      for (size_t q = 0; q < queue.size(); q++) {
+        Job *c = queue[q];
+        if (bytes_in_use + c->est_bytes > prm.hbm_budget) continue;
+        double waited = ms_between(c->t_submit, now);
+        double key = (prm.policy == 0 || waited > kAgeMs)
+                         ? -1e30 + (double)q
+                         : (double)c->natoms * (double)std::max(1, c->spec.steps);
+        if (pick < 0 || key < best) {
+          pick = (int)q;
+          best = key;
+        }
       }
-      queue.erase(queue.begin() + q);
+      if (pick < 0) break;
+      Job *j = queue[pick];
+      queue.erase(queue.begin() + pick);
       admit(j);
       progressed = true;
       if (j->phase == PH_FAILED)
@@ -569,7 +592,8 @@ void pdgpu_serve_params_default(pdgpu_serve_params *p) {
   p->hbm_budget = 120LL * 1000 * 1000 * 1000;
   p->max_active = 32;
   p->lanes[0] = p->lanes[1] = p->lanes[2] = 8;
-  p->tiles = 0;  // list rows: minimisation rebuilds the list every step
+  p->tiles = 0;   // list rows: minimisation rebuilds the list every step
+  p->policy = 1;  // least work first: short jobs do not queue behind long MD runs
 }
 
 int pdgpu_serve_create(pdgpu_ctx *ctx, const pdgpu_serve_params *p, pdgpu_server **out) {

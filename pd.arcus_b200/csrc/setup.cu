@@ -232,6 +232,21 @@ static cudaError_t palloc(Pack *p, T **ptr, size_t count) {
   return e;
 }
 
+// The cluster-pair tile store (worst-case capacity), allocated the first
+// time a pack uses or times the tile layout.
+int pack_ensure_tiles(Pack *p) {
+  PackView &v = p->v;
+  if (v.tile_b0 || v.n_sc == 0) return PDGPU_OK;
+  if (palloc(p, &v.tile_b0, (size_t)v.tile_cap) != cudaSuccess ||
+      palloc(p, &v.tile_rows, 8 * (size_t)v.tile_cap) != cudaSuccess ||
+      palloc(p, &v.tile_spec, (size_t)v.tile_cap) != cudaSuccess ||
+      palloc(p, &v.spec_rows, 16 * (size_t)v.spec_cap) != cudaSuccess) {
+    set_error("device allocation failed (cluster-pair tiles)");
+    return PDGPU_ERR_NOMEM;
+  }
+  return PDGPU_OK;
+}
+
 void pack_set_params(Pack *p, int s, const pdgpu_ff_params &prm) {
   p->sp[s] = make_sys_params(prm);
 }
@@ -412,11 +427,7 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
     PALLOC(sc_sys_d, sc_sys.size());
     PALLOC(v.tile_e0, sc_atom0.size());
     PALLOC(v.tile_e1, sc_atom0.size());
-    PALLOC(v.tile_b0, (size_t)tile_cap);
-    PALLOC(v.tile_rows, 8 * (size_t)tile_cap);
-    PALLOC(v.tile_spec, (size_t)tile_cap);
-    PALLOC(v.spec_rows, 16 * (size_t)spec_cap);
-    PALLOC(v.tile_count, 2);
+    PALLOC(v.tile_count, 2);  // the tile store itself: pack_ensure_tiles, on first use
     PALLOC(v.bsum, N);
     PALLOC(v.hx, N);
     PALLOC(v.hy, N);

@@ -19,7 +19,9 @@ from . import _abi as A
 class Server:
     ENERGY, MINIMISE, MD = A.JOB_ENERGY, A.JOB_MINIMISE, A.JOB_MD
 
-    def __init__(self, ctx, hbm_budget=None, max_active=None, lanes=(8, 8, 8), tiles=False):
+    ARRIVAL, LEAST_WORK = 0, 1
+
+    def __init__(self, ctx, hbm_budget=None, max_active=None, lanes=(8, 8, 8), tiles=False, policy=1):
         self.ctx = ctx
         p = A.ServeParams()
         A.lib().pdgpu_serve_params_default(ctypes.byref(p))
@@ -30,6 +32,7 @@ class Server:
         for q in range(3):
             p.lanes[q] = int(lanes[q])
         p.tiles = int(bool(tiles))
+        p.policy = int(policy)
         self.params = p
         self.ptr = ctypes.c_void_p()
         A.check(A.lib().pdgpu_serve_create(ctx.ptr, ctypes.byref(p), ctypes.byref(self.ptr)))
