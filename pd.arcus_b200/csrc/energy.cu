@@ -16,9 +16,10 @@
 namespace pdgpu {
 
 constexpr int kChunk = 1024;
-constexpr int kEnergyThreads = 256;
+constexpr int kEnergyThreads = 320;  // ten warps: one per partial slot in the final sum
 // partial slots
 enum { P_VDW = 0, P_ELEC, P_POL, P_SELF, P_NBVIR, P_KIN, P_BOND, P_BVIR, P_ANGLE, P_DIH, P_COUNT };
+static_assert(kEnergyThreads / 32 >= P_COUNT, "one warp per partial slot");
 
 // hist: [step][sys][3] (epot, ekin, etot); step_dev[0] current step,
 // step_dev[1] first step of the run, step_dev[2] finished-system counter.
@@ -85,10 +86,13 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode,
   __syncthreads();
   if (!last) return;
   __threadfence();
-  if (threadIdx.x < P_COUNT) {
+  // warp w adds slot w over the chunks: lane l takes chunks l, l+32, ...
+  // (loads in parallel), then a fixed shuffle tree
+  if (warp < P_COUNT) {
     double t = 0.0;
-    for (int q = 0; q < C; q++) t += __ldcg(part + (size_t)q * P_COUNT + threadIdx.x);
-    tot[threadIdx.x] = t;
+    for (int q = lane; q < C; q += 32) t += __ldcg(part + (size_t)q * P_COUNT + warp);
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) tot[warp] = t;
   }
   __syncthreads();
   if (threadIdx.x == 0) {

@@ -233,9 +233,9 @@ struct MinState {
   int taken, nan;
 };
 
-// CG dot products, stage 1: per (chunk, system) partials of
-// fmagold = sum of.of and fmagnew = sum (of-f).f into e_part slots 0 and 1;
-// k_min_control adds the chunk partials in chunk order.
+// CG dot products: per (chunk, system) partials of fmagold = sum of.of and
+// fmagnew = sum (of-f).f into e_part slots 0 and 1; the last block of each
+// system adds them in a fixed order for k_min_control.
 __global__ void k_min_dots(PackView v, double N_per_unit, int C) {
   if (v.flags[F_NL_OVERFLOW]) return;
   const int c = blockIdx.x, s = blockIdx.y;
@@ -259,11 +259,28 @@ __global__ void k_min_dots(PackView v, double N_per_unit, int C) {
     }
     __syncthreads();
   }
+  double *part = v.e_part + (size_t)s * C * 10;
   if (threadIdx.x == 0) {
-    double *o = v.e_part + ((size_t)s * C + c) * 10;
-    o[0] = sa[0];
-    o[1] = sb[0];
+    part[(size_t)c * 10] = sa[0];
+    part[(size_t)c * 10 + 1] = sb[0];
   }
+  // the last block of the system adds the chunk partials (lanes strided over
+  // the chunks, then a fixed shuffle tree) into slots 2 and 3 of chunk 0
+  __shared__ int last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&v.e_done[s], 1) == C - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < 2) {
+    double t = 0.0;
+    for (int q = lane; q < C; q += 32) t += __ldcg(part + (size_t)q * 10 + warp);
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) part[2 + warp] = t;
+  }
+  if (threadIdx.x == 0) v.e_done[s] = 0;
 }
 
 // One thread per system: the accept / restore decision of the step.
@@ -275,14 +292,9 @@ __global__ void k_min_control(PackView v, MinState *ms, int algorithm, double sl
   if (s >= v.n_sys) return;
   MinState &m = ms[s];
   if (algorithm == PDGPU_MIN_CONJUGATE_GRADIENTS && !v.flags[F_NL_OVERFLOW]) {
-    double A = 0, B = 0;
-    for (int c = 0; c < C; c++) {
-      const double *o = v.e_part + ((size_t)s * C + c) * 10;
-      A += o[0];
-      B += o[1];
-    }
-    m.fmagold = A;
-    m.fmagnew = B;
+    const double *o = v.e_part + (size_t)s * C * 10;  // totals of k_min_dots
+    m.fmagold = o[2];
+    m.fmagnew = o[3];
   }
   if (v.flags[F_NL_OVERFLOW]) {  // no valid forces this step: do nothing, retry
     m.action = -1;
