@@ -527,6 +527,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched workloads")
+    ap.add_argument("--pair-path", default="auto", choices=["auto", "rows", "tiles"],
+                    help="pair-pass layout of the headline run (default: the autotuner's choice)")
     ap.add_argument("--batched-md-steps", type=int, default=5000)
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--serve-policy", type=int, default=1, help="0 arrival order, 1 least work first")
@@ -590,7 +592,9 @@ def main():
     A.check(A.lib().pdgpu_pair_counts(ctx.ptr, ws._sys, counts.ctypes.data_as(A._I64)))
     lpa = np.zeros(3, dtype=np.int32)
     A.check(A.lib().pdgpu_autotune(ctx.ptr, ws._sys, A.iptr(lpa)))
-    path = ws.setPairPath(-2)  # the layout the autotuner chose
+    if args.pair_path != "auto":  # a fixed layout (profiling runs)
+        ws.setPairPath(1 if args.pair_path == "tiles" else 0)
+    path = ws.setPairPath(-2)  # the layout in use (the autotuner's choice by default)
     kms = np.zeros(3)
     A.check(A.lib().pdgpu_profile_pair_kernels(ctx.ptr, ws._sys, 20, A.dptr(kms)))
 

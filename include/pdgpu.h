@@ -201,10 +201,11 @@ int pdgpu_nlist_export(pdgpu_ctx *ctx, int32_t sys, int32_t shadow, int32_t *ptr
                        int32_t *data, int64_t cap, int64_t *count);
 
 /* Neighbour-list build that allocates no device memory.  No counterpart in
- * the reference: it exists for callers that cannot call cudaMalloc -- code
- * running while a stream is captured into a CUDA graph, or a host framework
- * that hands out all device memory from its own pool and forbids
- * allocation after start-up.  Same pair set and bond orders as
+ * the reference: it exists for callers that cannot call cudaMalloc, such
+ * as a host framework (a simulation engine or an inference server) that
+ * reserves all device memory for its own pool at start-up and forbids
+ * allocation afterwards, so the caller owns every input and output buffer
+ * and the library may add none of its own.  Same pair set and bond orders as
  * pdgpu_nlist_build, for one system given in device memory:
  *   x, y, z        positions (Angstrom), natoms each (SoA)
  *   list_cutoff    max(Cutoff, VdwCutoff) + Padding

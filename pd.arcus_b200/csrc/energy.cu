@@ -3,7 +3,7 @@
 //
 // One kernel, two stages, both in a fixed order so every total is
 // bit-reproducible: each block of the grid (chunks, systems) sums one
-// 1024-item chunk of each range of one system (per-atom terms and the bond
+// kReduceChunk-item chunk of each range of one system (per-atom terms and the bond
 // / angle / dihedral term arrays); the last block of a system to finish
 // adds the chunk partials in chunk order, applies them to the record with
 // the reference's semantics (the GB and stand-alone LJ/Coulomb components
@@ -15,7 +15,7 @@
 
 namespace pdgpu {
 
-constexpr int kChunk = 1024;
+constexpr int kChunk = kReduceChunk;
 constexpr int kEnergyThreads = 320;  // ten warps: one per partial slot in the final sum
 // partial slots
 enum { P_VDW = 0, P_ELEC, P_POL, P_SELF, P_NBVIR, P_KIN, P_BOND, P_BVIR, P_ANGLE, P_DIH, P_COUNT };

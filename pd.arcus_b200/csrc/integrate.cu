@@ -239,7 +239,7 @@ struct MinState {
 __global__ void k_min_dots(PackView v, double N_per_unit, int C) {
   if (v.flags[F_NL_OVERFLOW]) return;
   const int c = blockIdx.x, s = blockIdx.y;
-  int a0 = v.atom_off[s] + c * 1024, a1 = min(a0 + 1024, v.atom_off[s + 1]);
+  int a0 = v.atom_off[s] + c * kReduceChunk, a1 = min(a0 + kReduceChunk, v.atom_off[s + 1]);
   __shared__ double sa[256], sb[256];
   double A = 0, B = 0;
   for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
@@ -434,7 +434,8 @@ void launch_md_step_impl(const PackView &v, cudaStream_t st, const MDCoef &c, co
   d.kB = k.kB;
   d.is_h = is_h;
   d.sys_seed = seeds;
-  if (v.n_atoms) PDGPU_LAUNCH(k_md_step, (v.n_atoms + 255) / 256, 256, 0, st, v, d, normals, step_dev);
+  // 64-thread blocks: a 20k-atom system spreads over every SM
+  if (v.n_atoms) PDGPU_LAUNCH(k_md_step, (v.n_atoms + 63) / 64, 64, 0, st, v, d, normals, step_dev);
 }
 
 std::atomic<long long> &launch_counter() {
@@ -476,7 +477,7 @@ void launch_min_step(const PackView &v, cudaStream_t st, void *ms, int algorithm
     PDGPU_LAUNCH(k_min_dots, dim3(C, v.n_sys), 256, 0, st, v, k.N_per_kcalmolA, C);
   PDGPU_LAUNCH(k_min_control, (v.n_sys + 127) / 128, 128, 0, st, v, m, algorithm, slope_kcal, strict_kcal,
                k.J2kcal * k.Na, nsteps, C);
-  PDGPU_LAUNCH(k_min_update, (v.n_atoms + 255) / 256, 256, 0, st, v, m, k.N_per_kcalmolA, step_size);
+  PDGPU_LAUNCH(k_min_update, (v.n_atoms + 63) / 64, 64, 0, st, v, m, k.N_per_kcalmolA, step_size);
 }
 void launch_min_finish(const PackView &v, cudaStream_t st) {
   if (v.n_atoms) PDGPU_LAUNCH(k_min_restore_best, (v.n_atoms + 255) / 256, 256, 0, st, v);

@@ -37,6 +37,7 @@ constexpr double kForceScale = 4294967296.0;          // 2^32
 constexpr double kInvForceScale = 1.0 / 4294967296.0;
 constexpr double kJScale = 16777216.0;                // 2^24: j-side tile forces and energies
 constexpr double kInvJScale = 1.0 / 16777216.0;
+constexpr int kReduceChunk = 256;                     // items per block of the per-system reductions
 constexpr double kBornScale = 1099511627776.0;        // 2^40
 constexpr double kInvBornScale = 1.0 / 1099511627776.0;
 
@@ -131,7 +132,7 @@ struct PackView {
   double *ene;                // [S * E_COUNT] J-free kcal/mol accumulators
   double *e_part;             // [S * e_chunks * 10] reduction partials
   int *e_done;                // [S] blocks of the energy reduction finished (reset by the last)
-  int e_chunks;               // 1024-item chunks of the largest per-system range
+  int e_chunks;               // kReduceChunk-item chunks of the largest per-system range
   int lpa[3];                 // lanes per atom of the Born, fused-pair and chain kernels
   // backbone torsion moves (Monte Carlo trial conformations)
   const int2 *rot_axis;       // [R]: axis atoms (global) of every phi/psi rotation

@@ -1,11 +1,10 @@
 // Neighbour-list build that allocates no device memory.
 //
-// For callers that cannot allocate: code that runs while a stream is being
-// captured into a CUDA graph (where cudaMalloc is not allowed), and host
-// frameworks that own all device memory themselves (a fixed pool handed out
-// at start-up) and forbid allocation after it.  The caller passes inputs and
-// outputs; every scratch buffer of the build lives in one file-scope static
-// __device__ array, sized for at most kNoAllocMaxAtoms atoms.
+// For callers that cannot allocate: host frameworks that own all device
+// memory themselves (a fixed pool reserved at start-up) and forbid
+// allocation after it.  The caller passes inputs and outputs; every scratch
+// buffer of the build lives in one file-scope static __device__ array, sized
+// for at most kNoAllocMaxAtoms atoms.
 //
 // The array is part of the library image: every GPU that loads libpdgpu
 // holds it until the process exits.  All calls share it and it keeps the

@@ -586,7 +586,7 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
     PALLOC(v.bz, N);
   }
   v.lpa[0] = v.lpa[1] = v.lpa[2] = 8;
-  v.e_chunks = (max_range + 1023) / 1024;
+  v.e_chunks = (max_range + kReduceChunk - 1) / kReduceChunk;
   if (v.e_chunks < 1) v.e_chunks = 1;
   PALLOC(v.e_part, (size_t)S * v.e_chunks * 10);
   PALLOC(v.e_done, S);

@@ -570,12 +570,12 @@ void launch_tiles_build(const PackView &v, cudaStream_t st) {
 void launch_born_radii_tile(const PackView &v, cudaStream_t st, bool zero_first) {
   if (!v.n_sc) return;
   PDGPU_LAUNCH(k_born_tile, v.n_sc, 32 * kTileWarps, 0, st, v);
-  PDGPU_LAUNCH(k_born_finish, (v.n_atoms + 255) / 256, 256, 0, st, v, (int)zero_first);
+  PDGPU_LAUNCH(k_born_finish, (v.n_atoms + 63) / 64, 64, 0, st, v, (int)zero_first);
 }
 void launch_gb_pair_tile(const PackView &v, cudaStream_t st) {
   if (!v.n_sc) return;
   PDGPU_LAUNCH(k_gb_tile, v.n_sc, 32 * kTileWarps, 0, st, v);
-  PDGPU_LAUNCH(k_gb_finish, (v.n_atoms + 255) / 256, 256, 0, st, v);
+  PDGPU_LAUNCH(k_gb_finish, (v.n_atoms + 63) / 64, 64, 0, st, v);
 }
 void launch_gb_chain_tile(const PackView &v, cudaStream_t st) {
   if (!v.n_sc) return;

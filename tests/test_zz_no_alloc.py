@@ -1,8 +1,8 @@
 """GPU: the allocation-free neighbour-list build.
 
-pdgpu_nlist_build_noalloc exists for callers that cannot call cudaMalloc
-(code running under CUDA-graph stream capture, or a host framework that
-hands out all device memory from its own pool after start-up).  It must give
+pdgpu_nlist_build_noalloc exists for callers that cannot call cudaMalloc:
+host frameworks that reserve all device memory for their own pool at
+start-up and forbid allocation afterwards.  It must give
 the same pair set and bond orders as pdgpu_nlist_build -- compared exactly,
 as sorted pair sets, the tolerance every list test uses -- on two calls in a
 row (its static scratch keeps the previous call's contents).
