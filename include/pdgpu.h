@@ -326,8 +326,9 @@ int pdgpu_minimise_run(pdgpu_ctx *ctx, int32_t sys, const pdgpu_min_params *p,
  * kernels overlap with the running jobs'.  All jobs use the same pair-pass layout (and fixed
  * lanes per atom on the row layout), so a job's results are bit-identical
  * alone and in any mix.  A job's memory estimate before admission is
- * natoms * 2048 bytes + 40 bytes per possible 32 x 8 tile + 4 MiB; once its
- * list is sized it is charged max(estimate, real size).  The server is
+ * natoms * 2048 bytes + 1024 bytes per 32-atom cluster + 48 bytes per
+ * possible 32 x 8 tile + 4 MiB; once its list is sized it is charged
+ * max(estimate, real size).  The server is
  * driven from one host thread (the context's). */
 typedef struct pdgpu_server pdgpu_server;
 typedef struct {

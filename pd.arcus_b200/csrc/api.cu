@@ -924,7 +924,6 @@ static int ensure_tuned(pdgpu_ctx *c, Pack &P) {
   t.hy = (long long *)(f + 4 * (size_t)N);
   t.hz = (long long *)(f + 5 * (size_t)N);
   t.ej = (long long *)(f + 6 * (size_t)N);
-  t.deda = f + 10 * (size_t)N;
   t.bsum = (long long *)(f + 11 * (size_t)N);
   t.e_atom = ea;
   t.ene = en;

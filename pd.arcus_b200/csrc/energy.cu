@@ -129,6 +129,7 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode,
       E[E_EKIN] = tot[P_KIN] * J2kcalmol;
       E[E_ETOT] = E[E_EPOT] + E[E_EKIN];
     }
+    if (v.sys_flags[s] & SF_NONFINITE) E[E_EPOT] = __longlong_as_double(0x7ff8000000000000LL);  // NaN
     if (!(E[E_EPOT] == E[E_EPOT])) atomicExch(&v.flags[F_NAN], 1);
     if (mode & EM_RECORD) {
       int k = step_dev[0] - step_dev[1];

@@ -35,7 +35,7 @@ const Consts &consts();
 // kcal/mol/A).  Born sums: A^-1 * 2^40 in int64 (range +-8.3e6).
 constexpr double kForceScale = 4294967296.0;          // 2^32
 constexpr double kInvForceScale = 1.0 / 4294967296.0;
-constexpr double kJScale = 16777216.0;                // 2^24: j-side tile forces and energies
+constexpr double kJScale = 16777216.0;                // 2^24: tile pass forces and energies
 constexpr double kInvJScale = 1.0 / 16777216.0;
 constexpr int kReduceChunk = 256;                     // items per block of the per-system reductions
 constexpr double kBornScale = 1099511627776.0;        // 2^40
@@ -164,22 +164,25 @@ struct PackView {
   int n_sc;                   // i-clusters over all systems
   int max_sys_atoms;          // largest system (sizes the tile build's shared memory)
   const int *sc_atom0, *sc_sys;  // [n_sc] first atom, system
-  int *tile_e0, *tile_e1;     // [n_sc] tile range of each i-cluster
-  int *tile_b0;               // [tile_cap] first atom of each tile's j-cluster
+  int4 *tile_meta;            // [tile_cap] per tile: first j atom, bond-order rows index (-1 none),
+                              // i-cluster's first atom, system << 8 | (i atoms - 1) << 3 | (j atoms - 1)
   unsigned *tile_rows;        // [8*tile_cap] byte l = i lane l's list bits over the 8 j atoms
-  int *tile_spec;             // [tile_cap] bond-order rows index, -1 none
   unsigned *spec_rows;        // [16*spec_cap] bytes 0..31 bond order <= 2, 32..63 == 3
-  int *tile_count;            // [2] tiles, bond-order row sets allocated
+  int *tile_count;            // [2] tiles, bond-order row sets
   long long tile_cap, spec_cap;
+  int tile_blocks[3];         // resident blocks of the three tile passes (persistent grids)
   long long *bsum;            // [N] Born sums of the tile pass, fixed point 2^40
-  long long *hx, *hy, *hz;    // [N] j-side pair forces, fixed point 2^24 kcal/mol/A
-  long long *ej;              // [4*N] j-side LJ, Coulomb, GB energies and dE/da, fixed point 2^24
-  double *deda;               // [N] i-side dE/da of the tile pass
+  long long *hx, *hy, *hz;    // [N] pair forces of the tile passes, fixed point 2^24 kcal/mol/A
+  long long *ej;              // [4*N] LJ, Coulomb, GB energies and dE/da of the tile pass, fixed point 2^24
   int *flags;                 // [8] overflow / nan / etc.
+  int *sys_flags;             // [S] SysFlag bits of the current evaluation
   BondedTerms bt;
 };
 
 enum Flag { F_NL_OVERFLOW = 0, F_NAN = 1, F_CELL_CLAMP = 2, F_COUNT = 8 };
+// per system: a tile pass met a non-finite pair term (its fixed-point sums
+// cannot carry it; the energy record turns it into a NaN potential energy)
+enum SysFlag { SF_NONFINITE = 1 };
 
 // ----------------------------------------------------------------- host side
 struct SystemHost {
@@ -259,14 +262,16 @@ void launch_nlist_fill(Pack &p, cudaStream_t st);
 void launch_born_radii(const PackView &v, cudaStream_t st, bool zero_first = false);
 void launch_gb_pair(const PackView &v, cudaStream_t st);
 void launch_gb_chain(const PackView &v, cudaStream_t st);
-// explicit lanes-per-atom variants (4, 8, 16, 32), used by the autotuner
 // cluster-pair tile versions of the three passes (tiles.cu); the plain
-// launchers above pick them when v.tile_mode is set
+// launchers above pick them when v.tile_mode is set.  tile_launch_shapes
+// sets v.tile_blocks (host only: an occupancy query per pass kernel).
+void tile_launch_shapes(PackView &v);
 void launch_tiles_build(const PackView &v, cudaStream_t st);
 void launch_tile_counts(const PackView &v, cudaStream_t st, unsigned long long *out);
 void launch_born_radii_tile(const PackView &v, cudaStream_t st, bool zero_first);
 void launch_gb_pair_tile(const PackView &v, cudaStream_t st);
 void launch_gb_chain_tile(const PackView &v, cudaStream_t st);
+// explicit lanes-per-atom variants (4, 8, 16, 32), used by the autotuner
 void launch_born_radii_lpa(const PackView &v, cudaStream_t st, bool zero_first, int lpa);
 void launch_gb_pair_lpa(const PackView &v, cudaStream_t st, int lpa);
 void launch_gb_chain_lpa(const PackView &v, cudaStream_t st, int lpa);

@@ -669,12 +669,12 @@ int pdgpu_serve_submit(pdgpu_server *s, int32_t sys, const pdgpu_job *job, const
     j->x0[2 * n + i] = xyz[3 * i + 2];
   }
   // device bytes before the list is sized: per-atom arrays, a list of 256
-  // entries per atom and the worst-case tile store (40 bytes per tile of
+  // entries per atom and the worst-case tile store (48 bytes per tile of
   // 32 x 8 atoms); the pack is charged its real size once sized
   {
     int64_t nsc = ((int64_t)n + 31) / 32, njc = ((int64_t)n + 7) / 8, tiles = 0;
     for (int64_t k = 0; k < nsc; k++) tiles += njc - 4 * k;
-    j->est_bytes = (int64_t)n * (1024 + 256 * 4) + tiles * 40 + nsc * 16 * 64 + (int64_t)4 * 1024 * 1024;
+    j->est_bytes = (int64_t)n * (1024 + 256 * 4) + tiles * 48 + nsc * 16 * 64 + (int64_t)4 * 1024 * 1024;
   }
   if (j->est_bytes > s->prm.hbm_budget) {
     set_error("pdgpu_serve_submit: the job alone exceeds the HBM budget");

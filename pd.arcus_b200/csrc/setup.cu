@@ -236,10 +236,9 @@ static cudaError_t palloc(Pack *p, T **ptr, size_t count) {
 // time a pack uses or times the tile layout.
 int pack_ensure_tiles(Pack *p) {
   PackView &v = p->v;
-  if (v.tile_b0 || v.n_sc == 0) return PDGPU_OK;
-  if (palloc(p, &v.tile_b0, (size_t)v.tile_cap) != cudaSuccess ||
+  if (v.tile_meta || v.n_sc == 0) return PDGPU_OK;
+  if (palloc(p, &v.tile_meta, (size_t)v.tile_cap) != cudaSuccess ||
       palloc(p, &v.tile_rows, 8 * (size_t)v.tile_cap) != cudaSuccess ||
-      palloc(p, &v.tile_spec, (size_t)v.tile_cap) != cudaSuccess ||
       palloc(p, &v.spec_rows, 16 * (size_t)v.spec_cap) != cudaSuccess) {
     set_error("device allocation failed (cluster-pair tiles)");
     return PDGPU_ERR_NOMEM;
@@ -404,6 +403,7 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   PALLOC(v.grid, (size_t)8 * S);
   PALLOC(v.bbox, (size_t)6 * S);
   PALLOC(v.flags, F_COUNT);
+  PALLOC(v.sys_flags, S);
   PALLOC(p->tmp_keys, N);
   PALLOC(p->tmp_vals, N);
   int tiles = (N + 2047) / 2048;
@@ -423,17 +423,15 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
     v.max_sys_atoms = max_sys;
     v.tile_cap = tile_cap;
     v.spec_cap = spec_cap;
+    tile_launch_shapes(v);
     PALLOC(sc_atom0_d, sc_atom0.size());
     PALLOC(sc_sys_d, sc_sys.size());
-    PALLOC(v.tile_e0, sc_atom0.size());
-    PALLOC(v.tile_e1, sc_atom0.size());
     PALLOC(v.tile_count, 2);  // the tile store itself: pack_ensure_tiles, on first use
     PALLOC(v.bsum, N);
     PALLOC(v.hx, N);
     PALLOC(v.hy, N);
     PALLOC(v.hz, N);
     PALLOC(v.ej, 4 * (size_t)N);
-    PALLOC(v.deda, N);
     if (!sc_atom0.empty()) {
       cudaMemcpyAsync(sc_atom0_d, sc_atom0.data(), sizeof(int) * sc_atom0.size(), cudaMemcpyHostToDevice, st);
       cudaMemcpyAsync(sc_sys_d, sc_sys.data(), sizeof(int) * sc_sys.size(), cudaMemcpyHostToDevice, st);

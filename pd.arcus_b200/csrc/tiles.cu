@@ -14,24 +14,32 @@
 // 1-3 or 1-4 partners (bond orders from the list entries) carry two more
 // byte rows: bond order <= 2 and bond order == 3.
 //
-// Each pass runs one block per i-cluster; its warps take the cluster's
-// tiles in turn, prefetching the next tile's 8 j atoms while they work on
-// the current one.  Lane l = 8g + a (one i atom) walks the tile's j atoms in
-// the order (a+t) mod 8: the i side accumulates in registers, the j side
-// goes with one shuffle to the lane of its group that owns the j atom; after
-// the 8 steps the four groups' j sums meet with two xor shuffles and are
-// added to the j atoms with 64-bit fixed-point atomics (order-independent).
-// Per-lane i sums are added in fixed warp order.  Pass results:
-//   K2 k_born_tile   Born sums, i and j side, fixed point 2^40 (exact);
-//                    k_born_finish inverts them (FP64) and zeroes the j-side
+// Each pass runs a persistent grid of G warps over the pack's T tiles
+// (every system's clusters, the tiles of a cluster consecutive): warp g
+// takes the contiguous range [T g / G, T (g+1) / G), so every warp gets the
+// same number of tiles, give or take one, however unequal the clusters'
+// tile counts are.  A warp prefetches the next tile's 8 j atoms while it
+// works on the current one, and reloads its i atoms when the range enters
+// the next cluster.  Lane l = 8g + a (one i atom) walks the tile's j atoms
+// in the order (a+t) mod 8: the i side accumulates in registers, the j
+// side goes with one shuffle to the lane of its group that owns the j
+// atom; after the 8 steps the four groups' j sums meet with two xor
+// shuffles.  Both sides of each tile are then added to their atoms with
+// 64-bit fixed-point atomics.  A tile's sums depend on the tile alone, and
+// fixed-point sums do not depend on the order of the additions, so every
+// result is bit-identical run to run, however the tiles are spread over
+// the warps and whatever other systems share the pack.  Pass results:
+//   K2 k_born_tile   Born sums, fixed point 2^40 (exact per term);
+//                    k_born_finish inverts them (FP64) and zeroes the
 //                    accumulators of the next passes
-//   K3 k_gb_tile     forces (i: FP64 pair force, j: fixed point 2^24),
-//                    per-atom LJ / Coulomb / GB energies and dE/da (i side
-//                    FP64, j side fixed point); k_gb_finish forms the
-//                    reference's per-atom values and the chain-rule weights
-//   K4 k_chain_tile  chain-rule forces (i and j side as K3)
+//   K3 k_gb_tile     forces, per-atom LJ / Coulomb / GB energies and dE/da,
+//                    fixed point 2^24; k_gb_finish forms the reference's
+//                    per-atom values and the chain-rule weights
+//   K4 k_chain_tile  chain-rule forces, fixed point 2^24
 // The per-pair arithmetic is the row kernels' (pairmath.cuh).
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "pairmath.cuh"
 
@@ -133,7 +141,6 @@ __global__ void __launch_bounds__(128) k_tile_build(PackView v) {
     const int nr = min(kBuildChunk, ncand - c0);
     for (int r = tid; r < nr; r += blockDim.x) {
       const int et = base + c0 + r;
-      v.tile_b0[et] = cb0[r];
       unsigned spec_any = 0;
       for (int w = 0; w < 8; w++) {
         v.tile_rows[8 * (size_t)et + w] = rw[r * 8 + w];
@@ -152,13 +159,10 @@ __global__ void __launch_bounds__(128) k_tile_build(PackView v) {
           spec = -1;
         }
       }
-      v.tile_spec[et] = spec;
+      const int nb = min(8, end - cb0[r]);
+      v.tile_meta[et] = make_int4(cb0[r], spec, a0, (s << 8) | ((na - 1) << 3) | (nb - 1));
     }
     __syncthreads();
-  }
-  if (tid == 0) {
-    v.tile_e0[sc] = base;
-    v.tile_e1[sc] = base + ncand;
   }
 }
 
@@ -168,6 +172,14 @@ __device__ __forceinline__ long long to_fixed_j(float f) {
   // stay well inside: 2^39 kcal/mol/A)
   float s = fminf(fmaxf(f * (float)kJScale, -9.0e18f), 9.0e18f);
   return __float2ll_rn(s);
+}
+// Add one FP32 partial to a 2^24 fixed-point sum.  A non-finite partial
+// (coincident atoms) marks its system, whose potential energy then reads
+// NaN as the reference's FP64 sum would.
+__device__ __forceinline__ void add_fixed(const PackView &v, long long *p, float x, int s) {
+  if (x == 0.f) return;
+  if (!(fabsf(x) <= 3.0e38f)) atomicOr(&v.sys_flags[s], SF_NONFINITE);
+  atomicAdd((unsigned long long *)p, (unsigned long long)to_fixed_j(x));
 }
 
 // A lane's row bits of tile e (bits over the 8 j atoms), and of its
@@ -179,90 +191,123 @@ __device__ __forceinline__ unsigned spec_row(const PackView &v, int spec, int wh
   return reinterpret_cast<const unsigned char *>(v.spec_rows)[64 * (size_t)spec + 32 * which + lane];
 }
 
-// Staging of a tile's j atoms: lanes 0..7 hold three records of their j
-// atom in registers (prefetched one tile ahead) and write them to the
-// warp's shared slots before the tile is processed.
+// A tile's metadata, decoded.
+struct TileInfo {
+  int b0, spec, a0, s, na, nb;
+};
+__device__ __forceinline__ TileInfo tile_info(const int4 m) {
+  TileInfo t;
+  t.b0 = m.x;
+  t.spec = m.y;
+  t.a0 = m.z;
+  t.s = m.w >> 8;
+  t.na = ((m.w >> 3) & 31) + 1;
+  t.nb = (m.w & 7) + 1;
+  return t;
+}
+
+// Staging of a tile: its metadata and this lane's row bits, and in lanes
+// 0..7 three records of their j atom, held in registers (prefetched one
+// tile ahead) and written to the warp's shared slots before the tile is
+// processed.
 struct JStage {
   float4 a, b, c;
-  int b0, nb, spec;
+  int4 m;
   unsigned row;
 };
 template <int REC>  // third record: 0 chainp (radius R, volume V, chain weight w), 1 prm (LJ radius, eps)
-__device__ __forceinline__ void stage_load(const PackView &v, int e, int end, int lane, JStage &q) {
-  q.b0 = v.tile_b0[e];
-  q.nb = min(8, end - q.b0);
-  q.spec = v.tile_spec[e];
+__device__ __forceinline__ void stage_load(const PackView &v, int e, int lane, JStage &q) {
+  q.m = v.tile_meta[e];
   q.row = tile_row(v, e, lane);
-  if (lane < q.nb) {
-    const int j = q.b0 + lane;
+  if (lane <= (q.m.w & 7)) {
+    const int j = q.m.x + lane;
     q.a = v.pq[2 * (size_t)j];
     q.b = v.pq[2 * (size_t)j + 1];
     q.c = REC == 0 ? v.chainp[j] : v.prm[j];
   }
 }
 
+// This warp's tile range [e0, e1): an equal share of the pack's tiles.
+__device__ __forceinline__ void warp_range(const PackView &v, int warp, int &e0, int &e1) {
+  const long long T = v.tile_count[0];
+  const long long G = (long long)gridDim.x * kTileWarps;
+  const long long g = (long long)blockIdx.x * kTileWarps + warp;
+  e0 = (int)(T * g / G);
+  e1 = (int)(T * (g + 1) / G);
+}
+
 // --------------------------------------------------------------- K2 tiles
-// (register bounds: five blocks per SM, one wave for a 20k-atom system)
+// (register bounds: five blocks per SM)
 __global__ void __launch_bounds__(32 * kTileWarps, 5) k_born_tile(PackView v) {
   if (v.flags[F_NL_OVERFLOW]) return;
-  const int sc = blockIdx.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g8 = lane & ~7, a = lane & 7;
   __shared__ float4 sA[kTileWarps][8], sB[kTileWarps][8], sC[kTileWarps][8];
-  const int s = v.sc_sys[sc];
-  const SysParams &P = v.sp[s];
-  const int a0 = v.sc_atom0[sc];
-  const int end = v.atom_off[s + 1];
-  const int na = min(32, end - a0);
-  const int i = a0 + (lane < na ? lane : 0);
-  const float4 ia = v.pq[2 * (size_t)i], ib = v.pq[2 * (size_t)i + 1], ic = v.chainp[i];
-  const float s_hi = P.still2 * (1.f + 4e-6f), s_lo = P.still2 * (1.f - 4e-6f);
-  const float invP5 = P.invP5, piP5 = P.piP5, P4s = P.P4 * (float)kBornScale;
-  const double still2_d = P.still2_d;
-  long long acc_i = 0;
-  const int e1 = v.tile_e1[sc];
-  int e = v.tile_e0[sc] + warp;
+  int e, e1;
+  warp_range(v, warp, e, e1);
+  if (e >= e1) return;
   JStage nx;
-  if (e < e1) stage_load<0>(v, e, end, lane, nx);
-  while (e < e1) {
+  stage_load<0>(v, e, lane, nx);
+  int a0 = -1, na = 0, i = 0;
+  float4 ia, ib, ic;
+  float s_hi = 0.f, s_lo = 0.f, invP5 = 0.f, piP5 = 0.f, P4s = 0.f;
+  double still2_d = 0.0;
+  long long acc_i = 0;  // exact per term: added when the range leaves the cluster
+  for (; e < e1; e++) {
     const JStage cur = nx;
-    if (lane < cur.nb) {
+    const TileInfo ti = tile_info(cur.m);
+    if (e + 1 < e1) stage_load<0>(v, e + 1, lane, nx);
+    if (ti.a0 != a0) {
+      if (lane < na && acc_i) atomicAdd((unsigned long long *)&v.bsum[a0 + lane], (unsigned long long)acc_i);
+      acc_i = 0;
+      a0 = ti.a0;
+      na = ti.na;
+      i = a0 + (lane < na ? lane : 0);
+      ia = v.pq[2 * (size_t)i];
+      ib = v.pq[2 * (size_t)i + 1];
+      ic = v.chainp[i];
+      const SysParams &P = v.sp[ti.s];
+      s_hi = P.still2 * (1.f + 4e-6f);
+      s_lo = P.still2 * (1.f - 4e-6f);
+      invP5 = P.invP5;
+      piP5 = P.piP5;
+      P4s = P.P4 * (float)kBornScale;
+      still2_d = P.still2_d;
+    }
+    if (lane < ti.nb) {
       sA[warp][lane] = cur.a;
       sB[warp][lane] = cur.b;
       sC[warp][lane] = cur.c;
     }
     unsigned rows = cur.row;
-    if (cur.spec >= 0) rows &= ~spec_row(v, cur.spec, 0, lane);  // bond order > 2 only
+    if (ti.spec >= 0) rows &= ~spec_row(v, ti.spec, 0, lane);  // bond order > 2 only
     __syncwarp();
-    const int en = e + kTileWarps;
-    if (en < e1) stage_load<0>(v, en, end, lane, nx);
     long long jacc = 0;  // lane (g,a): j atom a, this group's i atoms
 #pragma unroll
     for (int t = 0; t < 8; t++) {
       const int jt = (a + t) & 7;
-      long long ti = 0, tj = 0;
+      long long tI = 0, tJ = 0;
       if ((rows >> jt) & 1u) {
         const float4 ja = sA[warp][jt], jb = sB[warp][jt], jc = sC[warp][jt];
         const Dx d = diff(ia, ib, ja, jb);
         bool ok = d.r2 <= s_lo;
         if (!ok && d.r2 <= s_hi) {
-          const int j = cur.b0 + jt;
+          const int j = ti.b0 + jt;
           ok = !(ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]) > still2_d);
         }
         if (ok) {
           const float term = born_term_noV(d, ic.x, jc.x, invP5, piP5, P4s);
-          ti = __float2ll_rn(__fmul_rn(term, jc.y));
-          tj = __float2ll_rn(__fmul_rn(term, ic.y));
+          tI = __float2ll_rn(__fmul_rn(term, jc.y));
+          tJ = __float2ll_rn(__fmul_rn(term, ic.y));
         }
       }
-      acc_i += ti;
-      jacc += __shfl_sync(0xffffffffu, tj, g8 | ((a - t) & 7));
+      acc_i += tI;
+      jacc += __shfl_sync(0xffffffffu, tJ, g8 | ((a - t) & 7));
     }
     jacc += __shfl_xor_sync(0xffffffffu, jacc, 8);
     jacc += __shfl_xor_sync(0xffffffffu, jacc, 16);
-    if (lane < cur.nb && jacc) atomicAdd((unsigned long long *)&v.bsum[cur.b0 + lane], (unsigned long long)jacc);
+    if (lane < ti.nb && jacc) atomicAdd((unsigned long long *)&v.bsum[ti.b0 + lane], (unsigned long long)jacc);
     __syncwarp();
-    e = en;
   }
   if (lane < na && acc_i) atomicAdd((unsigned long long *)&v.bsum[a0 + lane], (unsigned long long)acc_i);
 }
@@ -293,51 +338,54 @@ __global__ void k_born_finish(PackView v, int zero_first) {
     v.hx[i] = 0;
     v.hy[i] = 0;
     v.hz[i] = 0;
-    if (i == v.atom_off[s])
+    if (i == v.atom_off[s]) {
       for (int k = 0; k < E_COUNT; k++)
         if (k != E_EKIN) v.ene[(size_t)s * E_COUNT + k] = 0.0;
+      v.sys_flags[s] = 0;
+    }
   }
 }
 
 // --------------------------------------------------------------- K3 tiles
 __global__ void __launch_bounds__(32 * kTileWarps, 5) k_gb_tile(PackView v) {
   if (v.flags[F_NL_OVERFLOW]) return;
-  const int sc = blockIdx.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g8 = lane & ~7, a = lane & 7;
   __shared__ float4 sA[kTileWarps][8], sB[kTileWarps][8], sP[kTileWarps][8];
-  __shared__ float red[kTileWarps][7][32];
-  const int s = v.sc_sys[sc];
-  const SysParams &P = v.sp[s];
-  GbSettings gs;
-  gs.load(P);
-  const int a0 = v.sc_atom0[sc];
-  const int end = v.atom_off[s + 1];
-  const int na = min(32, end - a0);
-  const int i = a0 + (lane < na ? lane : 0);
-  const float4 ia = v.pq[2 * (size_t)i], ib = v.pq[2 * (size_t)i + 1], ip = v.prm[i];
-  float fx = 0.f, fy = 0.f, fz = 0.f, e_vdw = 0.f, e_el = 0.f, e_pol = 0.f, deda = 0.f;
+  int e, e1;
+  warp_range(v, warp, e, e1);
+  if (e >= e1) return;
   const int N = v.n_atoms;
-  const int e1 = v.tile_e1[sc];
-  int e = v.tile_e0[sc] + warp;
   JStage nx;
-  if (e < e1) stage_load<1>(v, e, end, lane, nx);
-  while (e < e1) {
+  stage_load<1>(v, e, lane, nx);
+  int a0 = -1, i = 0;
+  float4 ia, ib, ip;
+  GbSettings gs;
+  for (; e < e1; e++) {
     const JStage cur = nx;
-    if (lane < cur.nb) {
+    const TileInfo ti = tile_info(cur.m);
+    if (e + 1 < e1) stage_load<1>(v, e + 1, lane, nx);
+    if (ti.a0 != a0) {
+      a0 = ti.a0;
+      i = a0 + (lane < ti.na ? lane : 0);
+      ia = v.pq[2 * (size_t)i];
+      ib = v.pq[2 * (size_t)i + 1];
+      ip = v.prm[i];
+      gs.load(v.sp[ti.s]);
+    }
+    if (lane < ti.nb) {
       sA[warp][lane] = cur.a;
       sB[warp][lane] = cur.b;
       sP[warp][lane] = cur.c;
     }
     const unsigned rows = cur.row;
     unsigned xrows = 0, brows = 0;  // bond order <= 2, == 3
-    if (cur.spec >= 0) {
-      xrows = spec_row(v, cur.spec, 0, lane);
-      brows = spec_row(v, cur.spec, 1, lane);
+    if (ti.spec >= 0) {
+      xrows = spec_row(v, ti.spec, 0, lane);
+      brows = spec_row(v, ti.spec, 1, lane);
     }
     __syncwarp();
-    const int en = e + kTileWarps;
-    if (en < e1) stage_load<1>(v, en, end, lane, nx);
+    float fx = 0.f, fy = 0.f, fz = 0.f, e_vdw = 0.f, e_el = 0.f, e_pol = 0.f, deda = 0.f;
     float jacc[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll 2
     for (int t = 0; t < 8; t++) {
@@ -350,7 +398,7 @@ __global__ void __launch_bounds__(32 * kTileWarps, 5) k_gb_tile(PackView v) {
         const bool nb3 = !((xrows >> jt) & 1u);
         const bool b14 = (brows >> jt) & 1u;
         const GbPair gp = gb_pair_term(gs, d, nb3, b14, ib.w, jb.w, ia.w, ja.w, ip.x, jp.x, ip.y, jp.y, v, i,
-                                       cur.b0 + jt);
+                                       ti.b0 + jt);
         e_pol += gp.epol;
         deda += gp.dedal * jb.w;
         e_vdw += gp.vdw;
@@ -375,56 +423,40 @@ __global__ void __launch_bounds__(32 * kTileWarps, 5) k_gb_tile(PackView v) {
       jacc[q] += __shfl_xor_sync(0xffffffffu, jacc[q], 8);
       jacc[q] += __shfl_xor_sync(0xffffffffu, jacc[q], 16);
     }
-    if (lane < cur.nb) {
-      const int j = cur.b0 + lane;
-      atomicAdd((unsigned long long *)&v.hx[j], (unsigned long long)to_fixed_j(jacc[0]));
-      atomicAdd((unsigned long long *)&v.hy[j], (unsigned long long)to_fixed_j(jacc[1]));
-      atomicAdd((unsigned long long *)&v.hz[j], (unsigned long long)to_fixed_j(jacc[2]));
+    if (lane < ti.nb) {
+      const int j = ti.b0 + lane;
+      add_fixed(v, &v.hx[j], jacc[0], ti.s);
+      add_fixed(v, &v.hy[j], jacc[1], ti.s);
+      add_fixed(v, &v.hz[j], jacc[2], ti.s);
 #pragma unroll
-      for (int q = 0; q < 4; q++)
-        atomicAdd((unsigned long long *)&v.ej[(size_t)q * N + j], (unsigned long long)to_fixed_j(jacc[3 + q]));
+      for (int q = 0; q < 4; q++) add_fixed(v, &v.ej[(size_t)q * N + j], jacc[3 + q], ti.s);
+    }
+    if (lane < ti.na) {
+      add_fixed(v, &v.hx[i], fx, ti.s);
+      add_fixed(v, &v.hy[i], fy, ti.s);
+      add_fixed(v, &v.hz[i], fz, ti.s);
+      add_fixed(v, &v.ej[i], e_vdw, ti.s);
+      add_fixed(v, &v.ej[(size_t)N + i], e_el, ti.s);
+      add_fixed(v, &v.ej[(size_t)2 * N + i], e_pol, ti.s);
+      add_fixed(v, &v.ej[(size_t)3 * N + i], deda, ti.s);
     }
     __syncwarp();
-    e = en;
-  }
-  // i side: the warps' partials in fixed order
-  red[warp][0][lane] = fx;
-  red[warp][1][lane] = fy;
-  red[warp][2][lane] = fz;
-  red[warp][3][lane] = e_vdw;
-  red[warp][4][lane] = e_el;
-  red[warp][5][lane] = e_pol;
-  red[warp][6][lane] = deda;
-  __syncthreads();
-  if (warp == 0 && lane < na) {
-    double t[7];
-    for (int q = 0; q < 7; q++) {
-      t[q] = 0.0;
-      for (int w = 0; w < kTileWarps; w++) t[q] += (double)red[w][q][lane];
-    }
-    v.gx[i] += t[0];
-    v.gy[i] += t[1];
-    v.gz[i] += t[2];
-    v.e_atom[(size_t)AE_VDW * N + i] = t[3];
-    v.e_atom[(size_t)AE_ELEC * N + i] = t[4];
-    v.e_atom[(size_t)AE_POL * N + i] = t[5];
-    v.deda[i] = t[6];
   }
 }
 
-// Per-atom values of the fused pass from its i and j sides, as the row
-// kernel leaves them: LJ and Coulomb halves, the GB pair sum, the self term,
-// and the chain-rule weight gpi * dE/da_i (gbff.cpp:1731-1757).
+// Per-atom values of the fused pass, as the row kernel leaves them: LJ and
+// Coulomb halves, the GB pair sum, the self term, and the chain-rule
+// weight gpi * dE/da_i (gbff.cpp:1731-1757).
 __global__ void k_gb_finish(PackView v) {
   if (v.flags[F_NL_OVERFLOW]) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= v.n_atoms) return;
   const int N = v.n_atoms;
   const SysParams &P = v.sp[v.sys_of[i]];
-  double dv = v.e_atom[(size_t)AE_VDW * N + i] + (double)v.ej[i] * kInvJScale;
-  double de = v.e_atom[(size_t)AE_ELEC * N + i] + (double)v.ej[(size_t)N + i] * kInvJScale;
-  double dp = v.e_atom[(size_t)AE_POL * N + i] + (double)v.ej[(size_t)2 * N + i] * kInvJScale;
-  double dd = v.deda[i] + (double)v.ej[(size_t)3 * N + i] * kInvJScale;
+  double dv = (double)v.ej[i] * kInvJScale;
+  double de = (double)v.ej[(size_t)N + i] * kInvJScale;
+  double dp = (double)v.ej[(size_t)2 * N + i] * kInvJScale;
+  double dd = (double)v.ej[(size_t)3 * N + i] * kInvJScale;
   double ai_d = v.born_d[i];
   double qd = (double)v.pq[2 * (size_t)i].w;
   double eself = P.premul_d * qd * qd / ai_d;
@@ -438,41 +470,47 @@ __global__ void k_gb_finish(PackView v) {
 }
 
 // --------------------------------------------------------------- K4 tiles
-__global__ void __launch_bounds__(32 * kTileWarps) k_chain_tile(PackView v) {
+__global__ void __launch_bounds__(32 * kTileWarps, 6) k_chain_tile(PackView v) {
   if (v.flags[F_NL_OVERFLOW]) return;
-  const int sc = blockIdx.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g8 = lane & ~7, a = lane & 7;
   __shared__ float4 sA[kTileWarps][8], sB[kTileWarps][8], sC[kTileWarps][8];
-  __shared__ float red[kTileWarps][3][32];
-  const int s = v.sc_sys[sc];
-  const SysParams &P = v.sp[s];
-  const int a0 = v.sc_atom0[sc];
-  const int end = v.atom_off[s + 1];
-  const int na = min(32, end - a0);
-  const int i = a0 + (lane < na ? lane : 0);
-  const float4 ia = v.pq[2 * (size_t)i], ib = v.pq[2 * (size_t)i + 1], ic = v.chainp[i];
-  const float s_hi = P.still2 * (1.f + 4e-6f), s_lo = P.still2 * (1.f - 4e-6f);
-  const float invP5 = P.invP5, piP5 = P.piP5, P4 = P.P4;
-  const double still2_d = P.still2_d;
-  float fx = 0.f, fy = 0.f, fz = 0.f;
-  const int e1 = v.tile_e1[sc];
-  int e = v.tile_e0[sc] + warp;
+  int e, e1;
+  warp_range(v, warp, e, e1);
+  if (e >= e1) return;
   JStage nx;
-  if (e < e1) stage_load<0>(v, e, end, lane, nx);
-  while (e < e1) {
+  stage_load<0>(v, e, lane, nx);
+  int a0 = -1, i = 0;
+  float4 ia, ib, ic;
+  float s_hi = 0.f, s_lo = 0.f, invP5 = 0.f, piP5 = 0.f, P4 = 0.f;
+  double still2_d = 0.0;
+  for (; e < e1; e++) {
     const JStage cur = nx;
-    if (lane < cur.nb) {
+    const TileInfo ti = tile_info(cur.m);
+    if (e + 1 < e1) stage_load<0>(v, e + 1, lane, nx);
+    if (ti.a0 != a0) {
+      a0 = ti.a0;
+      i = a0 + (lane < ti.na ? lane : 0);
+      ia = v.pq[2 * (size_t)i];
+      ib = v.pq[2 * (size_t)i + 1];
+      ic = v.chainp[i];
+      const SysParams &P = v.sp[ti.s];
+      s_hi = P.still2 * (1.f + 4e-6f);
+      s_lo = P.still2 * (1.f - 4e-6f);
+      invP5 = P.invP5;
+      piP5 = P.piP5;
+      P4 = P.P4;
+      still2_d = P.still2_d;
+    }
+    if (lane < ti.nb) {
       sA[warp][lane] = cur.a;
       sB[warp][lane] = cur.b;
       sC[warp][lane] = cur.c;
     }
     unsigned rows = cur.row;
-    if (cur.spec >= 0) rows &= ~spec_row(v, cur.spec, 0, lane);  // bond order > 2 only
+    if (ti.spec >= 0) rows &= ~spec_row(v, ti.spec, 0, lane);  // bond order > 2 only
     __syncwarp();
-    const int en = e + kTileWarps;
-    if (en < e1) stage_load<0>(v, en, end, lane, nx);
-    float j0 = 0.f, j1 = 0.f, j2 = 0.f;
+    float fx = 0.f, fy = 0.f, fz = 0.f, j0 = 0.f, j1 = 0.f, j2 = 0.f;
 #pragma unroll 2
     for (int t = 0; t < 8; t++) {
       const int jt = (a + t) & 7;
@@ -482,7 +520,7 @@ __global__ void __launch_bounds__(32 * kTileWarps) k_chain_tile(PackView v) {
         const Dx d = diff(ia, ib, ja, jb);
         bool ok = d.r2 <= s_lo;
         if (!ok && d.r2 <= s_hi) {
-          const int j = cur.b0 + jt;
+          const int j = ti.b0 + jt;
           ok = !(ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]) > still2_d);
         }
         if (ok) {
@@ -506,28 +544,18 @@ __global__ void __launch_bounds__(32 * kTileWarps) k_chain_tile(PackView v) {
     j0 += __shfl_xor_sync(0xffffffffu, j0, 16);
     j1 += __shfl_xor_sync(0xffffffffu, j1, 16);
     j2 += __shfl_xor_sync(0xffffffffu, j2, 16);
-    if (lane < cur.nb) {
-      const int j = cur.b0 + lane;
-      atomicAdd((unsigned long long *)&v.hx[j], (unsigned long long)to_fixed_j(j0));
-      atomicAdd((unsigned long long *)&v.hy[j], (unsigned long long)to_fixed_j(j1));
-      atomicAdd((unsigned long long *)&v.hz[j], (unsigned long long)to_fixed_j(j2));
+    if (lane < ti.nb) {
+      const int j = ti.b0 + lane;
+      add_fixed(v, &v.hx[j], j0, ti.s);
+      add_fixed(v, &v.hy[j], j1, ti.s);
+      add_fixed(v, &v.hz[j], j2, ti.s);
+    }
+    if (lane < ti.na) {
+      add_fixed(v, &v.hx[i], fx, ti.s);
+      add_fixed(v, &v.hy[i], fy, ti.s);
+      add_fixed(v, &v.hz[i], fz, ti.s);
     }
     __syncwarp();
-    e = en;
-  }
-  red[warp][0][lane] = fx;
-  red[warp][1][lane] = fy;
-  red[warp][2][lane] = fz;
-  __syncthreads();
-  if (warp == 0 && lane < na) {
-    double t[3];
-    for (int q = 0; q < 3; q++) {
-      t[q] = 0.0;
-      for (int w = 0; w < kTileWarps; w++) t[q] += (double)red[w][q][lane];
-    }
-    v.gx[i] += t[0];
-    v.gy[i] += t[1];
-    v.gz[i] += t[2];
   }
 }
 
@@ -556,6 +584,20 @@ size_t tile_build_smem(int max_sys_atoms) {
   int W = (nbits + 31) / 32;
   return sizeof(unsigned) * (2 * (size_t)W + 1 + kBuildChunk + 3 * 8 * (size_t)kBuildChunk);
 }
+// Persistent grids: the blocks one wave holds, and no more warps than the
+// pack can have tiles.
+void tile_launch_shapes(PackView &v) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int occ[3] = {1, 1, 1};
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_born_tile, 32 * kTileWarps, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], k_gb_tile, 32 * kTileWarps, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], k_chain_tile, 32 * kTileWarps, 0);
+  const long long need = (v.tile_cap + kTileWarps - 1) / kTileWarps;
+  for (int p = 0; p < 3; p++)
+    v.tile_blocks[p] = (int)std::max(1LL, std::min((long long)std::max(occ[p], 1) * sms, need));
+}
 void launch_tiles_build(const PackView &v, cudaStream_t st) {
   if (!v.n_sc) return;
   cudaMemsetAsync(v.tile_count, 0, 2 * sizeof(int), st);
@@ -569,17 +611,17 @@ void launch_tiles_build(const PackView &v, cudaStream_t st) {
 }
 void launch_born_radii_tile(const PackView &v, cudaStream_t st, bool zero_first) {
   if (!v.n_sc) return;
-  PDGPU_LAUNCH(k_born_tile, v.n_sc, 32 * kTileWarps, 0, st, v);
+  PDGPU_LAUNCH(k_born_tile, v.tile_blocks[0], 32 * kTileWarps, 0, st, v);
   PDGPU_LAUNCH(k_born_finish, (v.n_atoms + 63) / 64, 64, 0, st, v, (int)zero_first);
 }
 void launch_gb_pair_tile(const PackView &v, cudaStream_t st) {
   if (!v.n_sc) return;
-  PDGPU_LAUNCH(k_gb_tile, v.n_sc, 32 * kTileWarps, 0, st, v);
+  PDGPU_LAUNCH(k_gb_tile, v.tile_blocks[1], 32 * kTileWarps, 0, st, v);
   PDGPU_LAUNCH(k_gb_finish, (v.n_atoms + 63) / 64, 64, 0, st, v);
 }
 void launch_gb_chain_tile(const PackView &v, cudaStream_t st) {
   if (!v.n_sc) return;
-  PDGPU_LAUNCH(k_chain_tile, v.n_sc, 32 * kTileWarps, 0, st, v);
+  PDGPU_LAUNCH(k_chain_tile, v.tile_blocks[2], 32 * kTileWarps, 0, st, v);
 }
 
 }  // namespace pdgpu

@@ -125,7 +125,7 @@ def test_serve_budget_admission(gpu_ctx):
     nsc, njc = (n + 31) // 32, (n + 7) // 8
     tiles = sum(njc - 4 * k for k in range(nsc))
     # the server's admission estimate (include/pdgpu.h, pdgpu_serve_submit)
-    est = n * (1024 + 256 * 4) + tiles * 40 + nsc * 16 * 64 + 4 * 1024 * 1024
+    est = n * (1024 + 256 * 4) + tiles * 48 + nsc * 16 * 64 + 4 * 1024 * 1024
     budget = int(2.5 * est)  # room for two such jobs at a time
     srv = pdgpu.Server(gpu_ctx, hbm_budget=budget, max_active=8, lanes=LANES)
     job = pdgpu.Server.job(pdgpu.Server.MINIMISE, 20)
