@@ -175,6 +175,7 @@ __device__ __forceinline__ void dihedral_term(const PackView &v, int t, double *
 // One launch for every bonded term: threads [0, nb) bonds, then angles,
 // then torsions and impropers.  Per-term energies feed the energy reduction.
 __global__ void k_bonded_all(PackView v) {
+  PDGPU_DEP_ENTRY();
   if (v.flags[F_NL_OVERFLOW]) return;  // the step is being re-planned
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   const BondedTerms &b = v.bt;
@@ -194,7 +195,7 @@ __global__ void k_bonded_all(PackView v) {
 void launch_bonded_terms(const PackView &v, cudaStream_t st) {
   const BondedTerms &b = v.bt;
   int n = b.nb + b.na + b.nt + b.ni;
-  if (n) PDGPU_LAUNCH(k_bonded_all, (n + 127) / 128, 128, 0, st, v);
+  if (n) PDGPU_LAUNCH_DEP(k_bonded_all, (n + 127) / 128, 128, 0, st, v);
 }
 
 }  // namespace pdgpu

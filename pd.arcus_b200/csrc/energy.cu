@@ -16,7 +16,7 @@
 namespace pdgpu {
 
 constexpr int kChunk = kReduceChunk;
-constexpr int kEnergyThreads = 320;  // ten warps: one per partial slot in the final sum
+constexpr int kEnergyThreads = 352;  // eleven warps: one per partial slot in the final sum, one for the record
 // partial slots
 enum { P_VDW = 0, P_ELEC, P_POL, P_SELF, P_NBVIR, P_KIN, P_BOND, P_BVIR, P_ANGLE, P_DIH, P_COUNT };
 static_assert(kEnergyThreads / 32 >= P_COUNT, "one warp per partial slot");
@@ -25,6 +25,7 @@ static_assert(kEnergyThreads / 32 >= P_COUNT, "one warp per partial slot");
 // step_dev[1] first step of the run, step_dev[2] finished-system counter.
 __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode, int C, double J2kcalmol,
                                                            double *hist, int *step_dev) {
+  PDGPU_DEP_ENTRY();
   if (v.flags[F_NL_OVERFLOW]) return;
   const int c = blockIdx.x, s = blockIdx.y, N = v.n_atoms;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -87,58 +88,72 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode,
   if (!last) return;
   __threadfence();
   // warp w adds slot w over the chunks: lane l takes chunks l, l+32, ...
-  // (loads in parallel), then a fixed shuffle tree
+  // (loads in parallel), then a fixed shuffle tree; the record, the step
+  // counters and the system's flags are read in parallel meanwhile
+  __shared__ double sE[E_COUNT];
+  __shared__ int sflag, sk;
+  double *E = v.ene + (size_t)s * E_COUNT;
   if (warp < P_COUNT) {
     double t = 0.0;
     for (int q = lane; q < C; q += 32) t += __ldcg(part + (size_t)q * P_COUNT + warp);
     for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
     if (lane == 0) tot[warp] = t;
+  } else if (warp == P_COUNT) {
+    static_assert(E_COUNT <= 30, "one lane per record slot");
+    if (lane < E_COUNT) sE[lane] = __ldcg(E + lane);
+    if (lane == 30) sflag = __ldcg(v.sys_flags + s);
+    if (lane == 31 && (mode & EM_RECORD)) sk = __ldcg(step_dev) - __ldcg(step_dev + 1);
+  } else {
+    static_assert(kEnergyThreads / 32 > P_COUNT, "a spare warp reads the record");
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     v.e_done[s] = 0;
-    double *E = v.ene + (size_t)s * E_COUNT;
+    double *R = sE;
     if (mode & (EM_PAIR_GB | EM_PAIR_NB)) {
-      E[E_VDW] = tot[P_VDW];
-      E[E_ELEC] = tot[P_ELEC];
-      E[E_EPOT] += tot[P_VDW] + tot[P_ELEC];
+      R[E_VDW] = tot[P_VDW];
+      R[E_ELEC] = tot[P_ELEC];
+      R[E_EPOT] += tot[P_VDW] + tot[P_ELEC];
     }
     if (mode & EM_PAIR_GB) {
-      E[E_POL] += tot[P_POL] + tot[P_SELF];
-      E[E_POL_CROSS] += tot[P_POL];
-      E[E_POL_SELF] += tot[P_SELF];
-      E[E_EPOT] += tot[P_POL] + tot[P_SELF];
+      R[E_POL] += tot[P_POL] + tot[P_SELF];
+      R[E_POL_CROSS] += tot[P_POL];
+      R[E_POL_SELF] += tot[P_SELF];
+      R[E_EPOT] += tot[P_POL] + tot[P_SELF];
     }
-    if (mode & EM_PAIR_NB) E[E_VIRIAL] += tot[P_NBVIR];
+    if (mode & EM_PAIR_NB) R[E_VIRIAL] += tot[P_NBVIR];
     if (mode & EM_BORN_ENERGY) {
       // the energy-only path adds the Born energy to epot alone
       // (gbff.cpp:574-578); the component's own totals go to extra slots
-      E[E_EPOT] += tot[P_POL] + tot[P_SELF];
-      E[E_GB_COMPONENT] = tot[P_POL] + tot[P_SELF];
-      E[E_GB_COMPONENT + 1] = tot[P_POL];
-      E[E_GB_COMPONENT + 2] = tot[P_SELF];
+      R[E_EPOT] += tot[P_POL] + tot[P_SELF];
+      R[E_GB_COMPONENT] = tot[P_POL] + tot[P_SELF];
+      R[E_GB_COMPONENT + 1] = tot[P_POL];
+      R[E_GB_COMPONENT + 2] = tot[P_SELF];
     }
     if (mode & EM_BONDED) {
-      E[E_BOND] += tot[P_BOND];
-      E[E_ANGLE] += tot[P_ANGLE];
-      E[E_TORSION] += tot[P_DIH];
-      E[E_VIRIAL] += tot[P_BVIR];
-      E[E_EPOT] += tot[P_BOND] + tot[P_ANGLE] + tot[P_DIH];
+      R[E_BOND] += tot[P_BOND];
+      R[E_ANGLE] += tot[P_ANGLE];
+      R[E_TORSION] += tot[P_DIH];
+      R[E_VIRIAL] += tot[P_BVIR];
+      R[E_EPOT] += tot[P_BOND] + tot[P_ANGLE] + tot[P_DIH];
     }
     if (mode & EM_KINETIC) {
-      E[E_EKIN] = tot[P_KIN] * J2kcalmol;
-      E[E_ETOT] = E[E_EPOT] + E[E_EKIN];
+      R[E_EKIN] = tot[P_KIN] * J2kcalmol;
+      R[E_ETOT] = R[E_EPOT] + R[E_EKIN];
     }
-    if (v.sys_flags[s] & SF_NONFINITE) E[E_EPOT] = __longlong_as_double(0x7ff8000000000000LL);  // NaN
-    if (!(E[E_EPOT] == E[E_EPOT])) atomicExch(&v.flags[F_NAN], 1);
-    if (mode & EM_RECORD) {
-      int k = step_dev[0] - step_dev[1];
-      double *h = hist + ((size_t)k * v.n_sys + s) * 3;
-      h[0] = E[E_EPOT];
-      h[1] = E[E_EKIN];
-      h[2] = E[E_ETOT];
-      // the last system to finish advances the step (every block has read
-      // step_dev[0] before it counts itself finished)
+    if (sflag & SF_NONFINITE) R[E_EPOT] = __longlong_as_double(0x7ff8000000000000LL);  // NaN
+    if (!(R[E_EPOT] == R[E_EPOT])) atomicExch(&v.flags[F_NAN], 1);
+  }
+  __syncthreads();
+  if (warp == 0) {
+    if (lane < E_COUNT) E[lane] = sE[lane];
+    if ((mode & EM_RECORD) && lane < 3) {
+      double *h = hist + ((size_t)sk * v.n_sys + s) * 3;
+      h[lane] = sE[lane == 0 ? E_EPOT : lane == 1 ? E_EKIN : E_ETOT];
+    }
+    // the last system to finish advances the step (every block has read
+    // step_dev[0] before it counts itself finished)
+    if ((mode & EM_RECORD) && lane == 0) {
       __threadfence();
       int done = atomicAdd(&step_dev[2], 1);
       if (done == v.n_sys - 1) {
@@ -156,7 +171,8 @@ void launch_energy(const PackView &v, cudaStream_t st, int mode, double *hist, i
   if (!v.n_sys) return;
   const Consts &k = consts();
   int C = v.e_chunks;
-  PDGPU_LAUNCH(k_energy, dim3(C, v.n_sys), kEnergyThreads, 0, st, v, mode, C, k.J2kcal * k.Na, hist, step_dev);
+  PDGPU_LAUNCH_DEP(k_energy, dim3(C, v.n_sys), kEnergyThreads, 0, st, v, mode, C, k.J2kcal * k.Na, hist,
+                   step_dev);
 }
 
 }  // namespace pdgpu

@@ -70,6 +70,7 @@ struct MDDev {
 // One integrator step for every atom of the pack.  KE per atom goes to
 // e_atom[AE_KIN] and is reduced per system afterwards.
 __global__ void k_md_step(PackView v, MDDev d, const double *normals, const int *step_dev) {
+  PDGPU_DEP_ENTRY();
   if (v.flags[F_NL_OVERFLOW]) return;  // forces incomplete: keep the state, host re-plans
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= v.n_atoms) return;
@@ -435,7 +436,7 @@ void launch_md_step_impl(const PackView &v, cudaStream_t st, const MDCoef &c, co
   d.is_h = is_h;
   d.sys_seed = seeds;
   // 64-thread blocks: a 20k-atom system spreads over every SM
-  if (v.n_atoms) PDGPU_LAUNCH(k_md_step, (v.n_atoms + 63) / 64, 64, 0, st, v, d, normals, step_dev);
+  if (v.n_atoms) PDGPU_LAUNCH_DEP(k_md_step, (v.n_atoms + 63) / 64, 64, 0, st, v, d, normals, step_dev);
 }
 
 std::atomic<long long> &launch_counter() {
@@ -448,6 +449,13 @@ void count_launch() {
     tl_captured++;
   else
     launch_counter()++;
+}
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char *e = getenv("PDGPU_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
 }
 void begin_capture_count() { tl_captured = 0; }
 long long end_capture_count() {

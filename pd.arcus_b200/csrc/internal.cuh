@@ -357,6 +357,45 @@ long long end_capture_count();
     ::pdgpu::count_launch();                                       \
   } while (0)
 
+// Programmatic dependent launch for the kernels of the evaluation and step
+// chain.  A kernel launched with PDGPU_LAUNCH_DEP may be scheduled while the
+// kernel before it in the stream still runs; it must begin with
+// PDGPU_DEP_ENTRY(), which waits until every earlier kernel of the stream
+// has completed and its memory is visible (griddepcontrol.wait) before the
+// kernel touches global memory, then lets the next kernel be scheduled in
+// turn (griddepcontrol.launch_dependents).  The launch of kernel k+1 thus
+// overlaps the run of kernel k; no kernel reads or writes anything before
+// its predecessors are done.  PDGPU_PDL=0 in the environment turns the
+// overlap off (plain launches).
+#define PDGPU_DEP_ENTRY()                                          \
+  do {                                                             \
+    asm volatile("griddepcontrol.wait;" ::: "memory");             \
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); \
+  } while (0)
+namespace pdgpu {
+bool pdl_enabled();
+template <typename... KArgs, typename... Args>
+inline void launch_dep(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                       Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kern, static_cast<Args &&>(args)...);
+}
+}  // namespace pdgpu
+#define PDGPU_LAUNCH_DEP(kern, grid, block, smem, stream, ...)                       \
+  do {                                                                              \
+    ::pdgpu::launch_dep(kern, dim3(grid), dim3(block), (smem), (stream), __VA_ARGS__); \
+    ::pdgpu::count_launch();                                                        \
+  } while (0)
+
 #define PDGPU_CUDA(call)                                      \
   do {                                                        \
     cudaError_t e_ = (call);                                  \

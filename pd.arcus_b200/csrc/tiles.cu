@@ -239,6 +239,7 @@ __device__ __forceinline__ void warp_range(const PackView &v, int warp, int &e0,
 // --------------------------------------------------------------- K2 tiles
 // (register bounds: five blocks per SM)
 __global__ void __launch_bounds__(32 * kTileWarps, 5) k_born_tile(PackView v) {
+  PDGPU_DEP_ENTRY();
   if (v.flags[F_NL_OVERFLOW]) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g8 = lane & ~7, a = lane & 7;
@@ -315,6 +316,7 @@ __global__ void __launch_bounds__(32 * kTileWarps, 5) k_born_tile(PackView v) {
 // a_i = -halfeconv / (terms123_i + sum) (FP64); zero the accumulators the
 // following passes add into (and, first in an evaluation, the forces)
 __global__ void k_born_finish(PackView v, int zero_first) {
+  PDGPU_DEP_ENTRY();
   if (v.flags[F_NL_OVERFLOW]) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= v.n_atoms) return;
@@ -348,6 +350,7 @@ __global__ void k_born_finish(PackView v, int zero_first) {
 
 // --------------------------------------------------------------- K3 tiles
 __global__ void __launch_bounds__(32 * kTileWarps, 5) k_gb_tile(PackView v) {
+  PDGPU_DEP_ENTRY();
   if (v.flags[F_NL_OVERFLOW]) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g8 = lane & ~7, a = lane & 7;
@@ -448,6 +451,7 @@ __global__ void __launch_bounds__(32 * kTileWarps, 5) k_gb_tile(PackView v) {
 // Coulomb halves, the GB pair sum, the self term, and the chain-rule
 // weight gpi * dE/da_i (gbff.cpp:1731-1757).
 __global__ void k_gb_finish(PackView v) {
+  PDGPU_DEP_ENTRY();
   if (v.flags[F_NL_OVERFLOW]) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= v.n_atoms) return;
@@ -471,6 +475,7 @@ __global__ void k_gb_finish(PackView v) {
 
 // --------------------------------------------------------------- K4 tiles
 __global__ void __launch_bounds__(32 * kTileWarps, 6) k_chain_tile(PackView v) {
+  PDGPU_DEP_ENTRY();
   if (v.flags[F_NL_OVERFLOW]) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g8 = lane & ~7, a = lane & 7;
@@ -611,17 +616,17 @@ void launch_tiles_build(const PackView &v, cudaStream_t st) {
 }
 void launch_born_radii_tile(const PackView &v, cudaStream_t st, bool zero_first) {
   if (!v.n_sc) return;
-  PDGPU_LAUNCH(k_born_tile, v.tile_blocks[0], 32 * kTileWarps, 0, st, v);
-  PDGPU_LAUNCH(k_born_finish, (v.n_atoms + 63) / 64, 64, 0, st, v, (int)zero_first);
+  PDGPU_LAUNCH_DEP(k_born_tile, v.tile_blocks[0], 32 * kTileWarps, 0, st, v);
+  PDGPU_LAUNCH_DEP(k_born_finish, (v.n_atoms + 63) / 64, 64, 0, st, v, (int)zero_first);
 }
 void launch_gb_pair_tile(const PackView &v, cudaStream_t st) {
   if (!v.n_sc) return;
-  PDGPU_LAUNCH(k_gb_tile, v.tile_blocks[1], 32 * kTileWarps, 0, st, v);
-  PDGPU_LAUNCH(k_gb_finish, (v.n_atoms + 63) / 64, 64, 0, st, v);
+  PDGPU_LAUNCH_DEP(k_gb_tile, v.tile_blocks[1], 32 * kTileWarps, 0, st, v);
+  PDGPU_LAUNCH_DEP(k_gb_finish, (v.n_atoms + 63) / 64, 64, 0, st, v);
 }
 void launch_gb_chain_tile(const PackView &v, cudaStream_t st) {
   if (!v.n_sc) return;
-  PDGPU_LAUNCH(k_chain_tile, v.tile_blocks[2], 32 * kTileWarps, 0, st, v);
+  PDGPU_LAUNCH_DEP(k_chain_tile, v.tile_blocks[2], 32 * kTileWarps, 0, st, v);
 }
 
 }  // namespace pdgpu
