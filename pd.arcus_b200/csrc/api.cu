@@ -1150,6 +1150,12 @@ MDCoef pdgpu::md_coef(const pdgpu_md_params *p, int step, int steps) {
                          40967.0 * gt4 / 34406400.0 - 57203.0 * gt5 / 275251200.0 -
                          1429487.0 * gt6 / 13212057600.0);
   }
+  if (gt > 0 && c.c1 != 0) {
+    c.kick1 = (1.0 - c.c0 / c.c1) / gt;
+    c.c0c2_c1 = c.c0 * c.c2 / c.c1;
+    c.inv_gamma = 1.0 / c.gamma;
+    c.sq_crv = sqrt(1.0 - c.crv * c.crv);
+  }
   return c;
 }
 extern "C" {

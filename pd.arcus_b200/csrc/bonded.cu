@@ -21,11 +21,13 @@ __device__ __forceinline__ void bond_term(const PackView &v, int t, double *e_te
   double2 lk = v.bt.blk[t];
   int i = ij.x, j = ij.y;
   double bx = v.x[i] - v.x[j], by = v.y[i] - v.y[j], bz = v.z[i] - v.z[j];
-  double d = sqrt(bx * bx + by * by + bz * bz);
+  double d2 = bx * bx + by * by + bz * bz;
+  double inv_d = rsqrt(d2);
+  double d = d2 * inv_d;
   double fm = 2 * lk.y * (d - lk.x);
   e_term[t] = lk.y * (d - lk.x) * (d - lk.x);
   vir_term[t] = d * fm;
-  double s = fm / d;
+  double s = fm * inv_d;
   add_force(v, i, -bx * s, -by * s, -bz * s);
   add_force(v, j, bx * s, by * s, bz * s);
 }
@@ -38,8 +40,8 @@ __device__ __forceinline__ void angle_term(const PackView &v, int t, double *e_t
   int i = q.x, a = q.y, j = q.z;
   double iv[3] = {v.x[i] - v.x[a], v.y[i] - v.y[a], v.z[i] - v.z[a]};
   double jv[3] = {v.x[j] - v.x[a], v.y[j] - v.y[a], v.z[j] - v.z[a]};
-  double inv_iv = 1 / sqrt(iv[0] * iv[0] + iv[1] * iv[1] + iv[2] * iv[2]);
-  double inv_jv = 1 / sqrt(jv[0] * jv[0] + jv[1] * jv[1] + jv[2] * jv[2]);
+  double inv_iv = rsqrt(iv[0] * iv[0] + iv[1] * iv[1] + iv[2] * iv[2]);
+  double inv_jv = rsqrt(jv[0] * jv[0] + jv[1] * jv[1] + jv[2] * jv[2]);
   double ui[3], uj[3];
   for (int c = 0; c < 3; c++) {
     ui[c] = iv[c] * inv_iv;
@@ -52,9 +54,10 @@ __device__ __forceinline__ void angle_term(const PackView &v, int t, double *e_t
   e_term[t] = kt.x * dth * dth;
   double fm = 2 * kt.x * dth;
   double bi[3], bj[3];
+  const double gi = fm * inv_iv / sn, gj = fm * inv_jv / sn;
   for (int c = 0; c < 3; c++) {
-    bi[c] = fm * inv_iv * (ui[c] * cs - uj[c]) / sn;
-    bj[c] = fm * inv_jv * (uj[c] * cs - ui[c]) / sn;
+    bi[c] = gi * (ui[c] * cs - uj[c]);
+    bj[c] = gj * (uj[c] * cs - ui[c]);
   }
   add_force(v, i, -bi[0], -bi[1], -bi[2]);
   add_force(v, j, -bj[0], -bj[1], -bj[2]);
@@ -64,7 +67,7 @@ __device__ __forceinline__ void angle_term(const PackView &v, int t, double *e_t
 __device__ __forceinline__ void dihedral_term(const PackView &v, int t, double *e_term) {
   int4 q = v.bt.tidx[t];
   int ti = q.x, ta = q.y, tb = q.z, tj = q.w;
-  const double *par = v.bt.tpar + 12 * (size_t)t;
+  const double *par = v.bt.tpar + 20 * (size_t)t;
   int terms = v.bt.tterms[t];
   double a[3] = {v.x[ti] - v.x[ta], v.y[ti] - v.y[ta], v.z[ti] - v.z[ta]};
   double b[3] = {v.x[ta] - v.x[tb], v.y[ta] - v.y[tb], v.z[ta] - v.z[tb]};
@@ -72,16 +75,16 @@ __device__ __forceinline__ void dihedral_term(const PackView &v, int t, double *
   double n1[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
   double n2[3] = {b[1] * c[2] - b[2] * c[1], b[2] * c[0] - b[0] * c[2], b[0] * c[1] - b[1] * c[0]};
   double n3[3] = {b[1] * n1[2] - b[2] * n1[1], b[2] * n1[0] - b[0] * n1[2], b[0] * n1[1] - b[1] * n1[0]};
-  double in1 = 1.0 / sqrt(n1[0] * n1[0] + n1[1] * n1[1] + n1[2] * n1[2]);
-  double in2 = 1.0 / sqrt(n2[0] * n2[0] + n2[1] * n2[1] + n2[2] * n2[2]);
-  double in3 = 1.0 / sqrt(n3[0] * n3[0] + n3[1] * n3[1] + n3[2] * n3[2]);
+  double in1 = rsqrt(n1[0] * n1[0] + n1[1] * n1[1] + n1[2] * n1[2]);
+  double in2 = rsqrt(n2[0] * n2[0] + n2[1] * n2[1] + n2[2] * n2[2]);
+  double in3 = rsqrt(n3[0] * n3[0] + n3[1] * n3[1] + n3[2] * n3[2]);
   double cos_phi = (n1[0] * n2[0] + n1[1] * n2[1] + n1[2] * n2[2]) * in1 * in2;
   double sin_phi = (n3[0] * n2[0] + n3[1] * n2[1] + n3[2] * n2[2]) * in3 * in2;
   for (int k = 0; k < 3; k++) n2[k] *= in2;
   // phi = -atan2(sin_phi, cos_phi) (ffbonded.cpp:1261); the Fourier terms
   // with integer periodicity 1..6 need only cos(n phi) and sin(n phi), from
   // powers of cos(phi) + i sin(phi); phi itself only for the others
-  const double hinv = 1.0 / sqrt(cos_phi * cos_phi + sin_phi * sin_phi);
+  const double hinv = rsqrt(cos_phi * cos_phi + sin_phi * sin_phi);
   const double c1 = cos_phi * hinv, s1 = -sin_phi * hinv;
   bool need_phi = false;
   for (int m = 0; m < terms; m++) {
@@ -104,8 +107,9 @@ __device__ __forceinline__ void dihedral_term(const PackView &v, int t, double *
       d2[k] = in2 * (n2[k] * sin_phi - n3[k]);  // dsin/dn2
     }
   }
-  double fi[3] = {0, 0, 0}, fab[3] = {0, 0, 0}, fj[3] = {0, 0, 0};
-  double e = 0;
+  // the force is linear in dE/dphi: sum it over the Fourier terms, then
+  // apply the geometry once
+  double e = 0, dEs = 0;
   const double PI = 3.14159265358979323846;
   for (int m = 0; m < terms; m++) {
     double k = par[m], n = par[4 + m], gamma = par[8 + m];
@@ -118,8 +122,7 @@ __device__ __forceinline__ void dihedral_term(const PackView &v, int t, double *
         sn = sn * c1 + cn * s1;
         cn = t;
       }
-      double sg, cg;
-      sincos(gamma, &sg, &cg);
+      const double cg = par[12 + m], sg = par[16 + m];
       double cv = cn * cg - sn * sg, sv = sn * cg + cn * sg;
       ep = k * (1.0 + cv);
       dE = -n * k * sv;
@@ -138,32 +141,34 @@ __device__ __forceinline__ void dihedral_term(const PackView &v, int t, double *
       dE = 2.0 * k * diff;
     }
     e += ep;
-    if (use_cos) {
-      dE /= sin_phi;
-      fi[0] += dE * (b[1] * d1[2] - b[2] * d1[1]);
-      fi[1] += dE * (b[2] * d1[0] - b[0] * d1[2]);
-      fi[2] += dE * (b[0] * d1[1] - b[1] * d1[0]);
-      fj[0] += dE * (b[2] * d2[1] - b[1] * d2[2]);
-      fj[1] += dE * (b[0] * d2[2] - b[2] * d2[0]);
-      fj[2] += dE * (b[1] * d2[0] - b[0] * d2[1]);
-      fab[0] += dE * (a[2] * d1[1] - a[1] * d1[2] + c[1] * d2[2] - c[2] * d2[1]);
-      fab[1] += dE * (a[0] * d1[2] - a[2] * d1[0] + c[2] * d2[0] - c[0] * d2[2]);
-      fab[2] += dE * (a[1] * d1[0] - a[0] * d1[1] + c[0] * d2[1] - c[1] * d2[0]);
-    } else {
-      dE /= -cos_phi;
-      fi[0] += dE * ((b[1] * b[1] + b[2] * b[2]) * d1[0] - b[0] * b[1] * d1[1] - b[0] * b[2] * d1[2]);
-      fi[1] += dE * ((b[2] * b[2] + b[0] * b[0]) * d1[1] - b[1] * b[2] * d1[2] - b[1] * b[0] * d1[0]);
-      fi[2] += dE * ((b[0] * b[0] + b[1] * b[1]) * d1[2] - b[2] * b[0] * d1[0] - b[2] * b[1] * d1[1]);
-      fj[0] += dE * (d2[1] * b[2] - d2[2] * b[1]);
-      fj[1] += dE * (d2[2] * b[0] - d2[0] * b[2]);
-      fj[2] += dE * (d2[0] * b[1] - d2[1] * b[0]);
-      fab[0] += dE * (-(b[1] * a[1] + b[2] * a[2]) * d1[0] + (2.0 * b[0] * a[1] - a[0] * b[1]) * d1[1] +
-                      (2.0 * b[0] * a[2] - a[0] * b[2]) * d1[2] + d2[2] * c[1] - d2[1] * c[2]);
-      fab[1] += dE * (-(b[2] * a[2] + b[0] * a[0]) * d1[1] + (2.0 * b[1] * a[2] - a[1] * b[2]) * d1[2] +
-                      (2.0 * b[1] * a[0] - a[1] * b[0]) * d1[0] + d2[0] * c[2] - d2[2] * c[0]);
-      fab[2] += dE * (-(b[0] * a[0] + b[1] * a[1]) * d1[2] + (2.0 * b[2] * a[0] - a[2] * b[0]) * d1[0] +
-                      (2.0 * b[2] * a[1] - a[2] * b[1]) * d1[1] + d2[1] * c[0] - d2[0] * c[1]);
-    }
+    dEs += dE;
+  }
+  double fi[3], fab[3], fj[3];
+  if (use_cos) {
+    const double dE = dEs / sin_phi;
+    fi[0] = dE * (b[1] * d1[2] - b[2] * d1[1]);
+    fi[1] = dE * (b[2] * d1[0] - b[0] * d1[2]);
+    fi[2] = dE * (b[0] * d1[1] - b[1] * d1[0]);
+    fj[0] = dE * (b[2] * d2[1] - b[1] * d2[2]);
+    fj[1] = dE * (b[0] * d2[2] - b[2] * d2[0]);
+    fj[2] = dE * (b[1] * d2[0] - b[0] * d2[1]);
+    fab[0] = dE * (a[2] * d1[1] - a[1] * d1[2] + c[1] * d2[2] - c[2] * d2[1]);
+    fab[1] = dE * (a[0] * d1[2] - a[2] * d1[0] + c[2] * d2[0] - c[0] * d2[2]);
+    fab[2] = dE * (a[1] * d1[0] - a[0] * d1[1] + c[0] * d2[1] - c[1] * d2[0]);
+  } else {
+    const double dE = dEs / -cos_phi;
+    fi[0] = dE * ((b[1] * b[1] + b[2] * b[2]) * d1[0] - b[0] * b[1] * d1[1] - b[0] * b[2] * d1[2]);
+    fi[1] = dE * ((b[2] * b[2] + b[0] * b[0]) * d1[1] - b[1] * b[2] * d1[2] - b[1] * b[0] * d1[0]);
+    fi[2] = dE * ((b[0] * b[0] + b[1] * b[1]) * d1[2] - b[2] * b[0] * d1[0] - b[2] * b[1] * d1[1]);
+    fj[0] = dE * (d2[1] * b[2] - d2[2] * b[1]);
+    fj[1] = dE * (d2[2] * b[0] - d2[0] * b[2]);
+    fj[2] = dE * (d2[0] * b[1] - d2[1] * b[0]);
+    fab[0] = dE * (-(b[1] * a[1] + b[2] * a[2]) * d1[0] + (2.0 * b[0] * a[1] - a[0] * b[1]) * d1[1] +
+                   (2.0 * b[0] * a[2] - a[0] * b[2]) * d1[2] + d2[2] * c[1] - d2[1] * c[2]);
+    fab[1] = dE * (-(b[2] * a[2] + b[0] * a[0]) * d1[1] + (2.0 * b[1] * a[2] - a[1] * b[2]) * d1[2] +
+                   (2.0 * b[1] * a[0] - a[1] * b[0]) * d1[0] + d2[0] * c[2] - d2[2] * c[0]);
+    fab[2] = dE * (-(b[0] * a[0] + b[1] * a[1]) * d1[2] + (2.0 * b[2] * a[0] - a[2] * b[0]) * d1[0] +
+                   (2.0 * b[2] * a[1] - a[2] * b[1]) * d1[1] + d2[1] * c[0] - d2[0] * c[1]);
   }
   e_term[t] = e;
   add_force(v, ti, fi[0], fi[1], fi[2]);

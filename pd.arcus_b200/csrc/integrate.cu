@@ -24,15 +24,27 @@
 namespace pdgpu {
 
 // (Philox4x32-10 and the Box-Muller pair live in internal.cuh)
+// Box-Muller pair in single precision for the thermostat noise: the
+// variates need the normal distribution, not particular bits (24-bit
+// uniforms; the tails are cut at 5.8 sigma, probability 8e-9)
+__device__ __forceinline__ void nrand_pair_f(unsigned ua, unsigned ub, double &n1, double &n2) {
+  const float z1 = ((float)(ua >> 8) + 1.0f) * (1.0f / 16777216.0f);  // (0, 1]
+  const float z2 = (float)(ub >> 8) * (1.0f / 16777216.0f);           // [0, 1)
+  const float l = sqrtf(-2.0f * logf(z1));
+  float s, c;
+  sincospif(-2.0f * z2, &s, &c);
+  n1 = (double)(l * c);
+  n2 = (double)(l * s);
+}
 // six normals for atom `local` at `step`, in the reference's draw order
 // n1x n2y n2x n1z n1y n2z
 __device__ __forceinline__ void six_normals(unsigned long long seed, int local, int step, double *o) {
   unsigned k0 = (unsigned)seed, k1 = (unsigned)(seed >> 32);
   U4 r1 = philox(U4{(unsigned)local, (unsigned)step, 0u, 0x4D44u}, k0, k1);
   U4 r2 = philox(U4{(unsigned)local, (unsigned)step, 1u, 0x4D44u}, k0, k1);
-  nrand_pair(r1.a, r1.b, o[0], o[1]);
-  nrand_pair(r1.c, r1.d, o[2], o[3]);
-  nrand_pair(r2.a, r2.b, o[4], o[5]);
+  nrand_pair_f(r1.a, r1.b, o[0], o[1]);
+  nrand_pair_f(r1.c, r1.d, o[2], o[3]);
+  nrand_pair_f(r2.a, r2.b, o[4], o[5]);
 }
 
 // Total force on atom i along one axis in kcal/mol/A (the caller scales to
@@ -116,10 +128,11 @@ __global__ void k_md_step(PackView v, MDDev d, const double *normals, const int 
         vel[k] += dv;
       }
   } else if (langevin) {
-    double tim = t / m;
-    double gt = c.gamma * t;
+    // md.cpp:1003-1040 with the step's constant quotients formed on the host
+    const double im = 1.0 / m;
+    double tim = t * im;
     if (step > 0)
-      for (int k = 0; k < 3; k++) vel[k] += (1.0 - c.c0 / c.c1) * f[k] * tim / gt;
+      for (int k = 0; k < 3; k++) vel[k] += c.kick1 * f[k] * tim;
     ke = 0.5 * m * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
     if (step < c.steps - 1) {
       double nr[6];
@@ -130,17 +143,17 @@ __global__ void k_md_step(PackView v, MDDev d, const double *normals, const int 
         six_normals(d.sys_seed[s], i - v.atom_off[s], step, nr);
       }
       double n1x = nr[0], n2y = nr[1], n2x = nr[2], n1z = nr[3], n1y = nr[4], n2z = nr[5];
-      double kTdivm = d.kB * c.temp / m;
+      double kTdivm = d.kB * c.temp * im;
       double sigmav = sqrt(kTdivm * c.varv);
-      double sigmar = sqrt(kTdivm * c.varr) / c.gamma;
-      double sq = sqrt(1.0 - c.crv * c.crv);
+      double sigmar = sqrt(kTdivm * c.varr) * c.inv_gamma;
+      double sq = c.sq_crv;
       double dvr[3] = {sigmav * (c.crv * n1x + sq * n2x), sigmav * (c.crv * n1y + sq * n2y),
                        sigmav * (c.crv * n1z + sq * n2z)};
       double drr[3] = {sigmar * n1x, sigmar * n1y, sigmar * n1z};
       for (int k = 0; k < 3; k++) {
         double dr = t * (c.c1 * vel[k] + c.c2 * f[k] * tim) + drr[k];
         dr *= d.inv_angstrom;
-        double dv = (c.c0 * c.c2) * f[k] * tim / c.c1 + dvr[k];
+        double dv = c.c0c2_c1 * f[k] * tim + dvr[k];
         pos[k] += dr;
         vel[k] *= c.c0;
         vel[k] += dv;

@@ -99,7 +99,7 @@ struct BondedTerms {
   double2 *akt = nullptr;     // (k kcal/mol/rad^2, theta0)
   int4 *tidx = nullptr;       // torsions then impropers (i,a,b,j)
   int *tterms = nullptr;
-  double *tpar = nullptr;     // 12 per dihedral: Vn kcal/mol, n, gamma
+  double *tpar = nullptr;     // 20 per dihedral, 4 each: Vn kcal/mol, n, gamma, cos gamma, sin gamma
 };
 
 // Device view of a Pack.  Plain pointers, passed by value to kernels.
@@ -285,6 +285,9 @@ void launch_energy(const PackView &v, cudaStream_t st, int mode, double *hist = 
 // integrators / minimiser
 struct MDCoef {
   double dt, gamma, c0, c1, c2, varv, varr, crv, temp;
+  // per-step constants of the Langevin update, formed once on the host:
+  // (1 - c0/c1)/(gamma dt), c0 c2 / c1, 1/gamma, sqrt(1 - crv^2)
+  double kick1, c0c2_c1, inv_gamma, sq_crv;
   int integrator, step, steps, use_normals, stochastic_h;
   unsigned long long seed;
 };

@@ -509,6 +509,10 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
           double val = h.tpar[12 * q + m];
           tpar.push_back(m < 4 ? val * J2k : val);
         }
+        // cos and sin of each phase, so the kernel needs no transcendental
+        // for the integer periodicities
+        for (int m = 0; m < 4; m++) tpar.push_back(std::cos(h.tpar[12 * q + 8 + m]));
+        for (int m = 0; m < 4; m++) tpar.push_back(std::sin(h.tpar[12 * q + 8 + m]));
       }
     }
   bt.nb = (int)bij.size();
