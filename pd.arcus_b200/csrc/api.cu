@@ -453,6 +453,7 @@ int pdgpu_system_set_params(pdgpu_ctx *c, int32_t sys, const pdgpu_ff_params *pa
   pack_set_params(&P, 0, *params);
   PDGPU_CUDA(cudaMemcpyAsync((void *)P.v.sp, P.sp.data(), sizeof(SysParams), cudaMemcpyHostToDevice, c->st));
   P.have_list = false;  // the list radius may have changed
+  P.csr_stale = false;
   return sync_check(c, "set_params");
 }
 
@@ -825,12 +826,66 @@ static int nlist_enqueue(pdgpu_ctx *c, SysEntry *e, bool size_check) {
   }
   launch_nlist_fill(P, c->st);
   P.have_list = true;
+  P.csr_stale = false;
   return PDGPU_OK;
+}
+
+// A list rebuild for a pack that runs the tile passes makes the tiles
+// straight from the positions (no list, no host synchronisation); the list
+// itself is built later, only if something reads it, at the positions of
+// that rebuild (saved by the search), so it is the list the rebuild would
+// have made.  Packs on the row passes, or with a system too large for the
+// search, rebuild the list (and from it the tiles).
+static bool tile_search_ok(const Pack &P) {
+  return P.v.tile_mode && P.v.tile_meta && P.v.n_sc > 0 && P.v.max_sys_atoms <= kTileSearchMaxAtoms;
+}
+static void rebuild_enqueue(Pack &P, cudaStream_t st) {
+  if (tile_search_ok(P)) {
+    launch_tiles_search(P.v, st);
+    P.csr_stale = true;
+  } else {
+    launch_nlist_count(P, st);
+    launch_nlist_fill(P, st);
+    P.csr_stale = false;
+  }
+}
+// The list (CSR rows), built now at the saved positions when only tiles
+// were made since the last list build.
+static int need_csr(pdgpu_ctx *c, SysEntry *e) {
+  Pack &P = *e->pack;
+  if (!P.have_list) {
+    set_error("no neighbour list: call pdgpu_nlist_build first (NeighbourList::calcNewList)");
+    return PDGPU_ERR_STATE;
+  }
+  if (!P.csr_stale) return PDGPU_OK;
+  PackView &v = P.v;
+  double *x = v.x, *y = v.y, *z = v.z;
+  const size_t N = (size_t)v.n_atoms;
+  v.x = v.xs;
+  v.y = v.xs + N;
+  v.z = v.xs + 2 * N;
+  int r = nlist_enqueue(c, e, true);
+  v.x = x;
+  v.y = y;
+  v.z = z;
+  return r;
+}
+static int need_csr_if(pdgpu_ctx *c, SysEntry *e, bool csr) {
+  if (!e->pack->have_list) {
+    set_error("no neighbour list: call pdgpu_nlist_build first (NeighbourList::calcNewList)");
+    return PDGPU_ERR_STATE;
+  }
+  return csr ? need_csr(c, e) : PDGPU_OK;
 }
 
 int pdgpu_nlist_build(pdgpu_ctx *c, int32_t sys) {
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  if (P.have_list && tile_search_ok(P)) {
+    rebuild_enqueue(P, c->st);
+    return sync_check(c, "nlist_build");
+  }
   int r = nlist_enqueue(c, e, true);
   if (r) return r;
   return sync_check(c, "nlist_build");
@@ -841,10 +896,8 @@ int pdgpu_nlist_export(pdgpu_ctx *c, int32_t sys, int32_t shadow, int32_t *ptr, 
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
   Pack &P = *e->pack;
-  if (!P.have_list) {
-    set_error("no neighbour list: call pdgpu_nlist_build first");
-    return PDGPU_ERR_STATE;
-  }
+  int r0 = need_csr(c, e);
+  if (r0) return r0;
   if (!ptr || !count) {
     set_error("ptr/count is NULL");
     return PDGPU_ERR_ARG;
@@ -885,12 +938,15 @@ int pdgpu_nlist_export(pdgpu_ctx *c, int32_t sys, int32_t shadow, int32_t *ptr, 
   return PDGPU_OK;
 }
 
-static int need_list(Pack &P) {
-  if (!P.have_list) {
-    set_error("no neighbour list: call pdgpu_nlist_build first (NeighbourList::calcNewList)");
-    return PDGPU_ERR_STATE;
-  }
-  return PDGPU_OK;
+static int ensure_tuned(pdgpu_ctx *c, Pack &P);
+// What an evaluation reads: the tiles on the tile passes (current after
+// any rebuild), the list on the row passes and for the autotuner (which
+// times the row passes too).
+static int ready_pairs(pdgpu_ctx *c, SysEntry *e) {
+  Pack &P = *e->pack;
+  int r = need_csr_if(c, e, !P.tuned || !P.v.tile_mode);
+  if (r) return r;
+  return ensure_tuned(c, P);
 }
 
 // Autotuner: lanes per atom (4, 8, 16, 32) of the Born, fused-pair and
@@ -965,16 +1021,32 @@ static int ensure_tuned(pdgpu_ctx *c, Pack &P) {
   // the cluster-pair tile path against the tuned row path (three passes)
   if (r == PDGPU_OK && P.v.n_sc > 0) {
     t.tile_mode = 1;
-    // the tile build comes with every list rebuild: counted at the MD
-    // default cadence (one rebuild per 10 evaluations)
-    float build = 0;
+    // each layout's rebuild comes with every list period: counted at the MD
+    // default cadence (one rebuild per 10 evaluations).  The row passes
+    // rebuild the list; the tile passes search the tiles from the
+    // positions (systems within the search limit), else build the list and
+    // the tiles from it.  Every timed rebuild runs at the current positions
+    // and remakes what is there.
+    const bool search = P.v.max_sys_atoms <= kTileSearchMaxAtoms;
+    float build = 0, list = 0;
     for (int rep = 0; rep < 2 && r == PDGPU_OK; rep++) {
       cudaEventRecord(a, c->st);
-      launch_tiles_build(t, c->st);
+      launch_nlist_count(P, c->st);
+      launch_nlist_fill(P, c->st);  // (on the tile layout also the tiles from it: the same pairs)
+      cudaEventRecord(b, c->st);
+      r = sync_check(c, "autotune list build");
+      cudaEventElapsedTime(&list, a, b);
+      cudaEventRecord(a, c->st);
+      if (search)
+        launch_tiles_search(t, c->st);
+      else
+        launch_tiles_build(t, c->st);
       cudaEventRecord(b, c->st);
       r = sync_check(c, "autotune tile build");
       cudaEventElapsedTime(&build, a, b);
     }
+    if (!search) build += list;
+    row_total += 0.1f * 3.f * list;  // the row timings are sums of three repetitions
     float tot = 0.1f * 3.f * build;  // three timed repetitions below
     for (int rep = 0; rep < 4 && r == PDGPU_OK; rep++) {
       cudaEventRecord(a, c->st);
@@ -1015,9 +1087,8 @@ int pdgpu_gb_forces(pdgpu_ctx *c, int32_t sys) {
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
   Pack &P = *e->pack;
-  int r = need_list(P);
+  int r = ready_pairs(c, e);
   if (r) return r;
-  if ((r = ensure_tuned(c, P))) return r;
   if (!e->host->params.FastMode) {
     set_error("FastMode=false (separate FF_NonBonded + calcBornForces) is not built; use FastMode");
     return PDGPU_ERR_ARG;
@@ -1030,7 +1101,7 @@ int pdgpu_gb_energies(pdgpu_ctx *c, int32_t sys) {
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
   Pack &P = *e->pack;
-  int r = need_list(P);
+  int r = need_csr(c, e);
   if (r) return r;
   // calcEnergies: radii, FF_NonBonded::calcEnergies at Dielectric =
   // DielectricSolute (gbff.cpp:44), then calcBornEnergy
@@ -1057,7 +1128,7 @@ int pdgpu_nonbonded_forces(pdgpu_ctx *c, int32_t sys) {
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
   Pack &P = *e->pack;
-  int r = need_list(P);
+  int r = need_csr(c, e);
   if (r) return r;
   launch_nonbonded(P.v, c->st, P.sp[0].elec_mode);
   launch_energy(P.v, c->st, EM_PAIR_NB);
@@ -1093,9 +1164,8 @@ int pdgpu_calc_forces(pdgpu_ctx *c, int32_t sys) {
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
   Pack &P = *e->pack;
-  int r = need_list(P);
+  int r = ready_pairs(c, e);
   if (r) return r;
-  if ((r = ensure_tuned(c, P))) return r;
   calc_forces_enqueue(c->st, e, true);
   return sync_check(c, "calc_forces");
 }
@@ -1249,7 +1319,7 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
     r = nlist_enqueue(c, e, true);
     if (r) return r;
   }
-  if ((r = ensure_tuned(c, P))) return r;
+  if ((r = ready_pairs(c, e))) return r;
   // A block is one list period: [rebuild] + UpdateNList steps.  If the
   // in-block rebuild overflows the list buffer, every kernel after it skips
   // (device flag), the state stays at the block start, and the host grows
@@ -1275,15 +1345,15 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
       if (use_graph) {
         // graphs are cached per system; the key holds every value baked in
         char key[256];
-        snprintf(key, sizeof key, "%d|%p|%lld|%p|%d|%d|%.17g|%.17g|%.17g|%d|%d|%d|%d%d%d", block, (void *)v.nl,
-                 v.nl_cap, (void *)e->hist, k.integrator, k.steps, k.dt, k.gamma, k.temp, k.stochastic_h,
-                 P.radix_passes, (int)e->host->params.FastMode, v.lpa[0], v.lpa[1], v.lpa[2]);
+        snprintf(key, sizeof key, "%d|%p|%lld|%p|%d|%d|%.17g|%.17g|%.17g|%d|%d|%d|%d%d%d|%d%d", block,
+                 (void *)v.nl, v.nl_cap, (void *)e->hist, k.integrator, k.steps, k.dt, k.gamma, k.temp,
+                 k.stochastic_h, P.radix_passes, (int)e->host->params.FastMode, v.lpa[0], v.lpa[1], v.lpa[2],
+                 v.tile_mode, (int)tile_search_ok(P));
         if (!e->gexec || e->gkey != key) {
           e->drop_graph();
           begin_capture_count();
           PDGPU_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-          launch_nlist_count(P, c->st);
-          launch_nlist_fill(P, c->st);
+          rebuild_enqueue(P, c->st);
           for (int q = 0; q < block; q++) md_step_enqueue(c->st, e, k);
           PDGPU_CUDA(cudaStreamEndCapture(c->st, &e->graph));
           PDGPU_CUDA(cudaGraphInstantiate(&e->gexec, e->graph, 0));
@@ -1292,11 +1362,9 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
         }
         PDGPU_CUDA(cudaGraphLaunch(e->gexec, c->st));
         launch_counter() += e->gnodes;
+        P.csr_stale = tile_search_ok(P);  // what the graph's rebuild made
       } else {
-        if (rebuild) {
-          launch_nlist_count(P, c->st);
-          launch_nlist_fill(P, c->st);
-        }
+        if (rebuild) rebuild_enqueue(P, c->st);
         for (int q = 0; q < block; q++) md_step_enqueue(c->st, e, k);
       }
       int flags[F_COUNT];
@@ -1376,7 +1444,7 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
     r = nlist_enqueue(c, e, true);
     if (r) return r;
   }
-  if ((r = ensure_tuned(c, P))) return r;
+  if ((r = ready_pairs(c, e))) return r;
   cudaEventRecord(P.ev0, c->st);
   // Chunks of up to 16 steps run without a host synchronisation.  A step
   // whose list rebuild overflowed does nothing on the device (flag); the
@@ -1391,10 +1459,7 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
     int chunk = std::min(16, steps - iter);
     for (int q = 0; q < chunk; q++) {
       int cnt = counter0 + iter + q;
-      if (every > 0 && (cnt % every) == 0) {
-        launch_nlist_count(P, c->st);
-        launch_nlist_fill(P, c->st);
-      }
+      if (every > 0 && (cnt % every) == 0) rebuild_enqueue(P, c->st);
       calc_forces_enqueue(c->st, e, true);
       launch_min_step(v, c->st, e->min_state, p->Algorithm, slope, strict, p->StepSize, steps);
     }
@@ -1455,7 +1520,7 @@ int pdgpu_pair_counts(pdgpu_ctx *c, int32_t sys, int64_t *counts) {
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
   Pack &P = *e->pack;
-  int r = need_list(P);
+  int r = need_csr(c, e);
   if (r) return r;
   if (!counts) {
     set_error("counts is NULL");
@@ -1487,9 +1552,8 @@ int pdgpu_profile_pair_kernels(pdgpu_ctx *c, int32_t sys, int32_t reps, double *
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
   Pack &P = *e->pack;
-  int r = need_list(P);
+  int r = ready_pairs(c, e);
   if (r) return r;
-  if ((r = ensure_tuned(c, P))) return r;
   if (!ms || reps <= 0) {
     set_error("ms is NULL or reps <= 0");
     return PDGPU_ERR_ARG;
@@ -1524,7 +1588,7 @@ int pdgpu_autotune(pdgpu_ctx *c, int32_t sys, int32_t *lpa) {
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
   Pack &P = *e->pack;
-  int r = need_list(P);
+  int r = need_csr(c, e);
   if (r) return r;
   P.tuned = false;
   if ((r = ensure_tuned(c, P))) return r;
@@ -1572,7 +1636,8 @@ int pdgpu_pair_path(pdgpu_ctx *c, int32_t sys, int32_t set, int32_t *current) {
       if (set == 1) {
         int re = pack_ensure_tiles(&P);
         if (re) return re;
-        if (P.have_list) launch_tiles_build(P.v, c->st);  // tiles for the current list
+        // tiles for the current list (after a tile search they are current already)
+        if (P.have_list && !P.csr_stale) launch_tiles_build(P.v, c->st);
       }
       int r = sync_check(c, "pair_path");
       if (r) return r;

@@ -164,7 +164,13 @@ struct PackView {
   int n_sc;                   // i-clusters over all systems
   int max_sys_atoms;          // largest system (sizes the tile build's shared memory)
   const int *sc_atom0, *sc_sys;  // [n_sc] first atom, system
-  int4 *tile_meta;            // [tile_cap] per tile: first j atom, bond-order rows index (-1 none),
+  const int *sc_jc0;          // [n_sc] first j-cluster of each i-cluster
+  int n_jc;                   // j-clusters over all systems
+  const int *jc_atom0;        // [n_jc] first atom of each j-cluster
+  const int *jc_off;          // [S+1] first j-cluster of each system
+  double *cbox;               // [6*n_jc] j-cluster boxes at the last search: lo xyz, hi xyz
+  double *xs;                 // [3*N] positions at the last tile search (x block, y block, z block)
+  int4 *tile_meta;           // [tile_cap] per tile: first j atom, bond-order rows index (-1 none),
                               // i-cluster's first atom, system << 8 | (i atoms - 1) << 3 | (j atoms - 1)
   unsigned *tile_rows;        // [8*tile_cap] byte l = i lane l's list bits over the 8 j atoms
   unsigned *spec_rows;        // [16*spec_cap] bytes 0..31 bond order <= 2, 32..63 == 3
@@ -218,7 +224,8 @@ struct Pack {
   cudaStream_t st = nullptr;
   int64_t bytes = 0;
   long long nl_total = -1;       // last known list size (host)
-  bool have_list = false;
+  bool have_list = false;        // a pair structure exists (list, or tiles from a search)
+  bool csr_stale = false;        // the last rebuild made only the tiles (positions saved in v.xs)
   int radix_passes = 3;
   // temporary buffers for scans / sorts
   int *tmp_keys = nullptr, *tmp_vals = nullptr;
@@ -267,6 +274,11 @@ void launch_gb_chain(const PackView &v, cudaStream_t st);
 // sets v.tile_blocks (host only: an occupancy query per pass kernel).
 void tile_launch_shapes(PackView &v);
 void launch_tiles_build(const PackView &v, cudaStream_t st);
+// the tiles straight from the positions (no list); every system of the pack
+// at most kTileSearchMaxAtoms atoms (the search tests every j-cluster box of
+// a system against each of its i-clusters)
+constexpr int kTileSearchMaxAtoms = 65536;
+void launch_tiles_search(const PackView &v, cudaStream_t st);
 void launch_tile_counts(const PackView &v, cudaStream_t st, unsigned long long *out);
 void launch_born_radii_tile(const PackView &v, cudaStream_t st, bool zero_first);
 void launch_gb_pair_tile(const PackView &v, cudaStream_t st);

@@ -239,7 +239,9 @@ int pack_ensure_tiles(Pack *p) {
   if (v.tile_meta || v.n_sc == 0) return PDGPU_OK;
   if (palloc(p, &v.tile_meta, (size_t)v.tile_cap) != cudaSuccess ||
       palloc(p, &v.tile_rows, 8 * (size_t)v.tile_cap) != cudaSuccess ||
-      palloc(p, &v.spec_rows, 16 * (size_t)v.spec_cap) != cudaSuccess) {
+      palloc(p, &v.spec_rows, 16 * (size_t)v.spec_cap) != cudaSuccess ||
+      palloc(p, &v.cbox, 6 * (size_t)v.n_jc) != cudaSuccess ||
+      palloc(p, &v.xs, 3 * (size_t)v.n_atoms) != cudaSuccess) {
     set_error("device allocation failed (cluster-pair tiles)");
     return PDGPU_ERR_NOMEM;
   }
@@ -325,20 +327,24 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   // system in atom order; capacities are worst cases (no overflow path):
   // every j-cluster at or after an i-cluster, and for the bond-order rows
   // every tile within MaxIndexDelta of it plus one per off-diagonal pair
-  std::vector<int> sc_atom0, sc_sys;
+  std::vector<int> sc_atom0, sc_sys, sc_jc0, jc_atom0, jc_off(S + 1, 0);
   long long tile_cap = 0, spec_cap = 0;
   int max_sys = 0;
   for (int s = 0; s < S; s++) {
     int o = p->atom_off[s], n = systems[s]->natoms;
     max_sys = std::max(max_sys, n);
     int nsc = (n + 31) / 32, njc = (n + 7) / 8;
+    jc_off[s] = (int)jc_atom0.size();
     for (int k = 0; k < nsc; k++) {
       sc_atom0.push_back(o + 32 * k);
       sc_sys.push_back(s);
+      sc_jc0.push_back(jc_off[s] + 4 * k);
       tile_cap += njc - 4 * k;
     }
+    for (int k = 0; k < njc; k++) jc_atom0.push_back(o + 8 * k);
     spec_cap += (long long)nsc * ((32 + systems[s]->mid) / 8 + 3);
   }
+  jc_off[S] = (int)jc_atom0.size();
   spec_cap += (long long)off_data.size();
 
   // device allocations
@@ -418,14 +424,26 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   p->radix_passes = (bits + 7) / 8;
   // cluster-pair tiles and the accumulators of the tile passes
   {
-    int *sc_atom0_d, *sc_sys_d;
+    int *sc_atom0_d, *sc_sys_d, *sc_jc0_d, *jc_atom0_d, *jc_off_d;
     v.n_sc = (int)sc_atom0.size();
+    v.n_jc = (int)jc_atom0.size();
     v.max_sys_atoms = max_sys;
     v.tile_cap = tile_cap;
     v.spec_cap = spec_cap;
     tile_launch_shapes(v);
     PALLOC(sc_atom0_d, sc_atom0.size());
     PALLOC(sc_sys_d, sc_sys.size());
+    PALLOC(sc_jc0_d, sc_jc0.size());
+    PALLOC(jc_atom0_d, jc_atom0.size());
+    PALLOC(jc_off_d, jc_off.size());
+    if (!jc_atom0.empty()) {
+      cudaMemcpyAsync(sc_jc0_d, sc_jc0.data(), sizeof(int) * sc_jc0.size(), cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(jc_atom0_d, jc_atom0.data(), sizeof(int) * jc_atom0.size(), cudaMemcpyHostToDevice, st);
+    }
+    cudaMemcpyAsync(jc_off_d, jc_off.data(), sizeof(int) * jc_off.size(), cudaMemcpyHostToDevice, st);
+    v.sc_jc0 = sc_jc0_d;
+    v.jc_atom0 = jc_atom0_d;
+    v.jc_off = jc_off_d;
     PALLOC(v.tile_count, 2);  // the tile store itself: pack_ensure_tiles, on first use
     PALLOC(v.bsum, N);
     PALLOC(v.hx, N);

@@ -166,6 +166,195 @@ __global__ void __launch_bounds__(128) k_tile_build(PackView v) {
   }
 }
 
+// --------------------------------------------------------------- tile search
+// The tiles straight from the positions, without the list.  The pair test
+// is the list's (the reference's FP64 expression without contraction,
+// neighbourlist.cpp:263-266, and j != i) and the bond orders come from the
+// same band and off-diagonal tables, so the tiles hold exactly the pairs a
+// list build at these positions would give them.
+//
+// (1) k_cluster_boxes: one thread per j-cluster folds its <= 8 atoms into
+// an FP64 box (a cluster with a NaN coordinate gets an infinite box: its
+// pairs are decided by the distance test alone) and saves the positions of
+// this rebuild (for a later list build at the same positions).
+// (2) k_tile_search: one block per i-cluster; its warps take the system's
+// j-clusters at or after the i-cluster 32 at a time, one per lane, and keep
+// those whose box lies within the list cutoff of the i-cluster's box (a
+// margin of 1e-9 relative keeps the cull conservative); for each kept
+// j-cluster the warp tests its 32 x 8 atom pairs (lane = i atom) and emits
+// a tile when any pair is in.
+__global__ void k_cluster_boxes(PackView v) {
+  const int jc = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jc >= v.n_jc) return;
+  const int a0 = v.jc_atom0[jc];
+  const int s = v.sys_of[a0];
+  const int n = min(8, v.atom_off[s + 1] - a0);
+  const int N = v.n_atoms;
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  bool wild = false;
+  for (int k = 0; k < n; k++) {
+    const int i = a0 + k;
+    const double p[3] = {v.x[i], v.y[i], v.z[i]};
+    for (int c = 0; c < 3; c++) {
+      wild |= !(p[c] == p[c]);
+      lo[c] = fmin(lo[c], p[c]);
+      hi[c] = fmax(hi[c], p[c]);
+      v.xs[(size_t)c * N + i] = p[c];
+    }
+  }
+  for (int c = 0; c < 3; c++) {
+    v.cbox[6 * (size_t)jc + c] = wild ? -INFINITY : lo[c];
+    v.cbox[6 * (size_t)jc + 3 + c] = wild ? INFINITY : hi[c];
+  }
+}
+
+constexpr int kSearchWarps = 8;  // warps per i-cluster block of the tile search
+
+// One candidate j-cluster against this lane's i atom: the pair bits and
+// the bond-order bits (<= 2, == 3).  The pair tests come first (the 8 j
+// positions load independently), then the bond orders of the pairs in
+// (independent band loads).
+struct SearchRow {
+  unsigned row, xr, br;
+};
+__device__ __forceinline__ SearchRow search_row(const PackView &v, bool live, int i, int li, int a0, double xi,
+                                                double yi, double zi, double lim, int jb0, int nb, int o,
+                                                int mid, const signed char *band, bool has_off, int s) {
+  SearchRow r = {0u, 0u, 0u};
+  if (!live) return r;
+#pragma unroll
+  for (int t = 0; t < 8; t++) {
+    const int j = jb0 + t;
+    // the half list: j > i inside the i-cluster
+    if (t < nb && !(j <= i && j < a0 + 32) && !(ref_d2(xi, yi, zi, v.x[j], v.y[j], v.z[j]) > lim))
+      r.row |= 1u << t;
+  }
+#pragma unroll
+  for (int t = 0; t < 8; t++) {
+    if (!((r.row >> t) & 1u)) continue;
+    const int lj = jb0 + t - o;
+    const int delta = lj > li ? lj - li : li - lj;
+    int bo = 7;
+    if (delta < mid)
+      bo = band[(long long)min(li, lj) * mid + (delta - 1)];
+    else if (has_off)
+      bo = bond_order(v, s, i, jb0 + t);
+    if (bo <= 2)
+      r.xr |= 1u << t;
+    else if (bo == 3)
+      r.br |= 1u << t;
+  }
+  return r;
+}
+// Store one tile (when any pair is in); false when a capacity ran out
+// (cannot happen: the capacities are worst cases).
+__device__ __forceinline__ bool search_emit(const PackView &v, int lane, const SearchRow &r, int jb0, int a0, int s,
+                                            int na, int nb) {
+  if (!__any_sync(0xffffffffu, r.row != 0)) return true;
+  int e = 0;
+  if (lane == 0) e = atomicAdd(&v.tile_count[0], 1);
+  e = __shfl_sync(0xffffffffu, e, 0);
+  if (e >= v.tile_cap) {
+    if (lane == 0) atomicExch(&v.flags[F_NL_OVERFLOW], 1);
+    return false;
+  }
+  reinterpret_cast<unsigned char *>(v.tile_rows)[32 * (size_t)e + lane] = (unsigned char)r.row;
+  int spec = -1;
+  if (__any_sync(0xffffffffu, (r.xr | r.br) != 0)) {
+    if (lane == 0) spec = atomicAdd(&v.tile_count[1], 1);
+    spec = __shfl_sync(0xffffffffu, spec, 0);
+    if (spec >= v.spec_cap) {
+      if (lane == 0) atomicExch(&v.flags[F_NL_OVERFLOW], 1);
+      return false;
+    }
+    reinterpret_cast<unsigned char *>(v.spec_rows)[64 * (size_t)spec + lane] = (unsigned char)r.xr;
+    reinterpret_cast<unsigned char *>(v.spec_rows)[64 * (size_t)spec + 32 + lane] = (unsigned char)r.br;
+  }
+  if (lane == 0) v.tile_meta[e] = make_int4(jb0, spec, a0, (s << 8) | ((na - 1) << 3) | (nb - 1));
+  return true;
+}
+
+__global__ void __launch_bounds__(32 * kSearchWarps) k_tile_search(PackView v) {
+  if (v.flags[F_NL_OVERFLOW]) return;
+  const int sc = blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s = v.sc_sys[sc];
+  const int a0 = v.sc_atom0[sc];
+  const int end = v.atom_off[s + 1];
+  const int na = min(32, end - a0);
+  const int jc0 = v.sc_jc0[sc], jc_end = v.jc_off[s + 1];
+  const double lim = v.sp[s].nl_lim2_d;
+  const double cull = lim * (1.0 + 1e-9);
+  // the i-cluster's box: its (up to four) j-clusters' boxes
+  double ilo[3] = {INFINITY, INFINITY, INFINITY}, ihi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int q = 0; q < 4 && jc0 + q < jc_end; q++)
+    for (int c = 0; c < 3; c++) {
+      ilo[c] = fmin(ilo[c], v.cbox[6 * (size_t)(jc0 + q) + c]);
+      ihi[c] = fmax(ihi[c], v.cbox[6 * (size_t)(jc0 + q) + 3 + c]);
+    }
+  // this lane's i atom and what its bond orders need
+  const bool live = lane < na;
+  const int i = a0 + (live ? lane : 0);
+  const double xi = v.x[i], yi = v.y[i], zi = v.z[i];
+  const int o = v.atom_off[s], mid = v.mid[s], li = i - o;
+  const signed char *band = reinterpret_cast<const signed char *>(v.band) + v.band_off[s];
+  const bool has_off = v.off_ptr[i + 1] > v.off_ptr[i];
+  // the i atoms' positions for the per-atom cull
+  __shared__ double sx[32], sy[32], sz[32];
+  if (warp == 0) {
+    sx[lane] = xi;
+    sy[lane] = yi;
+    sz[lane] = zi;
+  }
+  __syncthreads();
+  for (int base = jc0 + 32 * warp; base < jc_end; base += 32 * kSearchWarps) {
+    bool cand = false;
+    const int jc = base + lane;
+    if (jc < jc_end) {
+      double jlo[3], jhi[3];
+      for (int c = 0; c < 3; c++) {
+        jlo[c] = v.cbox[6 * (size_t)jc + c];
+        jhi[c] = v.cbox[6 * (size_t)jc + 3 + c];
+      }
+      double g2 = 0.0;
+      for (int c = 0; c < 3; c++) {
+        const double gap = fmax(0.0, fmax(jlo[c] - ihi[c], ilo[c] - jhi[c]));
+        g2 += gap * gap;
+      }
+      cand = !(g2 > cull);  // NaN (infinite boxes): a candidate
+      // boxes this close: some i atom must lie within the cutoff of the
+      // j-cluster's box (an i-cluster across two chains has a large box)
+      if (cand) {
+        cand = false;
+        for (int k = 0; k < na && !cand; k++) {
+          const double p[3] = {sx[k], sy[k], sz[k]};
+          double h2 = 0.0;
+          for (int c = 0; c < 3; c++) {
+            const double gap = fmax(0.0, fmax(jlo[c] - p[c], p[c] - jhi[c]));
+            h2 += gap * gap;
+          }
+          cand = !(h2 > cull);
+        }
+      }
+    }
+    unsigned m = __ballot_sync(0xffffffffu, cand);
+    // two candidates at a time: their loads overlap
+    while (m) {
+      const int q1 = __ffs(m) - 1;
+      m &= m - 1;
+      const int q2 = m ? __ffs(m) - 1 : -1;
+      if (m) m &= m - 1;
+      const int jb1 = v.jc_atom0[base + q1], nb1 = min(8, end - jb1);
+      const int jb2 = q2 >= 0 ? v.jc_atom0[base + q2] : jb1, nb2 = min(8, end - jb2);
+      const SearchRow r1 = search_row(v, live, i, li, a0, xi, yi, zi, lim, jb1, nb1, o, mid, band, has_off, s);
+      SearchRow r2 = {0u, 0u, 0u};
+      if (q2 >= 0) r2 = search_row(v, live, i, li, a0, xi, yi, zi, lim, jb2, nb2, o, mid, band, has_off, s);
+      if (!search_emit(v, lane, r1, jb1, a0, s, na, nb1)) return;
+      if (q2 >= 0 && !search_emit(v, lane, r2, jb2, a0, s, na, nb2)) return;
+    }
+  }
+}
+
 // --------------------------------------------------------------- tile passes
 __device__ __forceinline__ long long to_fixed_j(float f) {
   // saturate far outside any physical range (clashing trial structures
@@ -613,6 +802,12 @@ void launch_tiles_build(const PackView &v, cudaStream_t st) {
     opted = smem;
   }
   PDGPU_LAUNCH(k_tile_build, v.n_sc, 128, smem, st, v);
+}
+void launch_tiles_search(const PackView &v, cudaStream_t st) {
+  if (!v.n_sc) return;
+  cudaMemsetAsync(v.tile_count, 0, 2 * sizeof(int), st);
+  PDGPU_LAUNCH(k_cluster_boxes, (v.n_jc + 127) / 128, 128, 0, st, v);
+  PDGPU_LAUNCH(k_tile_search, v.n_sc, 32 * kSearchWarps, 0, st, v);
 }
 void launch_born_radii_tile(const PackView &v, cudaStream_t st, bool zero_first) {
   if (!v.n_sc) return;

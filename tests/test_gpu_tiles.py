@@ -122,3 +122,67 @@ def test_tiles_md_graph_and_eager_agree(gpu_ctx):
         assert ws.setPairPath(-2) == 1
     assert np.array_equal(outs[0][0], outs[1][0])
     assert np.array_equal(outs[0][1], outs[1][1])
+
+
+def _forces_energies(ws, ff):
+    ff.calcForces()
+    return ws.cur.f.copy(), ws._pull_energies().copy(), ws.born_radii().copy()
+
+
+@pytest.mark.parametrize("name", SMALL + ["c2_16x80_s2"])
+def test_tile_search_equals_tiles_from_the_list(name, gpu_ctx):
+    """Tiles searched straight from the positions hold the same pairs as the
+    tiles cut from the list: every result is bit-identical (all tile sums
+    are fixed point, so the tiles' order does not matter)."""
+    arrays, meta = load_fixture(name)
+    ws, ff = build_workspace(arrays, meta, gpu_ctx)
+    assert ws.setPairPath(0) == 0
+    ws.nlist().calcNewList()           # the list
+    assert ws.setPairPath(1) == 1      # tiles cut from it
+    f_l, e_l, b_l = _forces_energies(ws, ff)
+    ws.nlist().calcNewList()           # on the tile layout: the tile search
+    f_s, e_s, b_s = _forces_energies(ws, ff)
+    assert np.array_equal(b_s, b_l)
+    assert np.array_equal(f_s, f_l)
+    assert np.array_equal(e_s, e_l)
+    c = _counts(ws)                    # the list, built now at the same positions
+    assert c[3] == c[2] // 2
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_list_after_a_tile_search_is_the_list(name, gpu_ctx):
+    """After a tile search the list is built when read, at the positions of
+    the search: the same entries as a list build there."""
+    arrays, meta = load_fixture(name)
+    ws, ff = build_workspace(arrays, meta, gpu_ctx)
+    ws.setPairPath(0)
+    ws.nlist().calcNewList()
+    ptr_r, data_r = ws.nlist().getData()
+    ws.setPairPath(1)
+    ws.nlist().calcNewList()           # tiles only
+    ptr_s, data_s = ws.nlist().getData()
+    assert np.array_equal(ptr_s, ptr_r)
+    assert np.array_equal(data_s, data_r)
+
+
+def test_tile_md_rebuilds_keep_list_and_tiles_consistent(gpu_ctx):
+    """MD on the tile layout rebuilds by tile search; the list read
+    afterwards (built at the last rebuild's positions) holds exactly the
+    tiles' pairs, and the row passes then give the tile passes' forces."""
+    import pdgpu
+    arrays, meta = load_fixture("c1_pep64_s0")
+    ws, ff = build_workspace(arrays, meta, gpu_ctx)
+    ws.setPairPath(1)
+    md = pdgpu.MolecularDynamics(ff)
+    md.Integrator = pdgpu.MolecularDynamics.Langevin
+    md.FricCoeff = 1e12
+    md.Steps = 25
+    md.UpdateNList = 10
+    md.Seed = 3
+    md.run()
+    c = _counts(ws)
+    assert c[3] == c[2] // 2 and c[4] > 0
+    f_t, e_t, _ = _forces_energies(ws, ff)
+    ws.setPairPath(0)
+    f_r, e_r, _ = _forces_energies(ws, ff)
+    assert rel_rms(f_t, f_r) <= 1e-6
