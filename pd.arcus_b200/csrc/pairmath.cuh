@@ -119,17 +119,22 @@ __device__ __forceinline__ GbPair gb_pair_term(const GbSettings &g, const Dx &d,
   const bool on = r >= g.rin;
   const float S = on ? sw * sw : 1.f;
   const float dSdd = on ? -4.f * g.inv_sw2 * dr * sw : 0.f;
-  // GB cross term (all bond orders), evaluated for every pair, kept when
-  // the exp approximation applies
-  const float tg = __expf(u);
-  const float fgb = rsqrtf(d.r2 + tg * aiaj);
-  const float l = fgb * fgb;
-  const float epol0 = g.premul * qiqj * fgb;
-  const float dedr0 = -epol0 * (r - 0.25f * r * tg) * l;
-  const float dedal0 = -epol0 * tg * (1.f - u) * l;
-  o.epol = gb ? epol0 * S : 0.f;
-  const float dedr = gb ? S * dedr0 + dSdd * epol0 : 0.f;
-  o.dedal = gb ? dedal0 * S : 0.f;
+  // GB cross term (all bond orders) where the exp approximation applies
+  // (a branch: partners beyond about 4 sqrt(a_i a_j) skip it together)
+  float dedr = 0.f;
+  o.epol = 0.f;
+  o.dedal = 0.f;
+  if (gb) {
+    const float tg = __expf(u);
+    const float fgb = rsqrtf(d.r2 + tg * aiaj);
+    const float l = fgb * fgb;
+    const float epol0 = g.premul * qiqj * fgb;
+    const float dedr0 = -epol0 * (r - 0.25f * r * tg) * l;
+    const float dedal0 = -epol0 * tg * (1.f - u) * l;
+    o.epol = epol0 * S;
+    dedr = S * dedr0 + dSdd * epol0;
+    o.dedal = dedal0 * S;
+  }
   // vacuum Coulomb at the solute (GB branch) or solvent dielectric
   const float ec = nb ? (gb ? g.econv_in : g.econv_out) * (b14 ? g.elec14 : 1.f) * qiqj * invr : 0.f;
   const float elf = S * (-ec * invr) + ec * dSdd;
