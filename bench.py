@@ -294,7 +294,7 @@ def compose(parts, spacing=25.0):
 
 
 def bench_serving(pdgpu, A, ctx, torch, n_requests=300, rate=200.0, budget=120e9, max_active=32, seed=5,
-                  policy=1, tiles=False):
+                  policy=1, tiles=True):
     lib = load_library(LIB_SP)
     meta = lib[0][1]
     rng = np.random.default_rng(seed)
@@ -533,7 +533,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--serve-policy", type=int, default=1, help="0 arrival order, 1 least work first")
     ap.add_argument("--serve-max-active", type=int, default=32)
-    ap.add_argument("--serve-tiles", action="store_true")
+    ap.add_argument("--serve-rows", action="store_true", help="serve on the list-row pair passes")
     args = ap.parse_args()
     rank, world, local = rank_info()
     n_gpus = max(args.gpus, world)
@@ -736,7 +736,7 @@ def main():
         line["batched_md"] = bench_batched_md(pdgpu, A, ctx, torch, steps=args.batched_md_steps)
         line["serving"] = bench_serving(pdgpu, A, ctx, torch, n_requests=args.serve_requests,
                                         policy=args.serve_policy, max_active=args.serve_max_active,
-                                        tiles=args.serve_tiles)
+                                        tiles=not args.serve_rows)
     if rank == 0 and n_gpus == 1 and not args.no_cpu_baseline:
         try:
             cb = run_reference(args, 1)

@@ -7,8 +7,9 @@
 // device side of every admitted job.  Each job gets its own CUDA stream and
 // device state (coordinates, neighbour list, Born radii, integrator or
 // minimiser state stay resident until it finishes) and advances as a small
-// state machine: the worker enqueues one phase of work (a list sizing pass,
-// a single-point evaluation, a chunk of minimiser steps, an MD block replayed
+// state machine: the worker enqueues one phase of work (a tile search or a
+// list sizing pass, a single-point evaluation, a chunk of minimiser steps, an
+// MD block replayed
 // from a CUDA graph), records an event, and moves on to the other jobs; the
 // next phase is enqueued when the event has completed.  Kernels of different
 // jobs therefore overlap on the device, and a job that arrives while others
@@ -154,6 +155,7 @@ struct pdgpu_server {
   void retire(Job *j);
   void fail(Job *j, int status, const std::string &msg);
   void enqueue_size(Job *j, Phase then);
+  void start(Job *j, Phase then);
   void enqueue_min_chunk(Job *j);
   void enqueue_md_block(Job *j);
   void enqueue_results(Job *j);
@@ -176,13 +178,48 @@ void pdgpu_server::fail(Job *j, int status, const std::string &msg) {
   j->phase = PH_FAILED;
 }
 
-// count pass of a list rebuild, its size back to the host
+// A job on the tile layout (systems within the search limit) rebuilds by
+// tile search: no list, no size read-back.
+static bool tile_search_job(const Pack &P) {
+  return P.v.tile_mode && P.v.tile_meta && P.v.n_sc > 0 && P.v.max_sys_atoms <= kTileSearchMaxAtoms;
+}
+static void rebuild_pairs(Pack &P, cudaStream_t st) {
+  if (tile_search_job(P)) {
+    launch_tiles_search(P.v, st);
+    P.csr_stale = true;
+  } else {
+    launch_nlist_count(P, st);
+    launch_nlist_fill(P, st);
+  }
+}
+
+// count pass of a list rebuild, its size back to the host (on the tile
+// layout: the tile search, and straight on to the next phase)
 void pdgpu_server::enqueue_size(Job *j, Phase then) {
   Pack &P = *j->e->pack;
+  if (tile_search_job(P)) {
+    rebuild_pairs(P, j->st);
+    P.have_list = true;
+    start(j, then);
+    return;
+  }
   launch_nlist_count(P, j->st);
   cudaMemcpyAsync(&j->pin->total, P.v.row_start + P.v.n_atoms, sizeof(long long), cudaMemcpyDeviceToHost, j->st);
   j->after_size = then;
   record(j, PH_SIZE);
+}
+
+// The job's work once its pairs exist: one evaluation and the results, or
+// the first minimiser chunk, or the first MD block.
+void pdgpu_server::start(Job *j, Phase then) {
+  if (then == PH_FINISH) {
+    calc_forces_enqueue(j->st, j->e.get(), true);
+    enqueue_results(j);
+  } else if (then == PH_MIN) {
+    enqueue_min_chunk(j);
+  } else {
+    enqueue_md_block(j);
+  }
 }
 
 // Up to 16 minimiser steps without a host round trip (as pdgpu_minimise_run)
@@ -196,10 +233,7 @@ void pdgpu_server::enqueue_min_chunk(Job *j) {
   j->chunk = std::min(16, steps - j->iter);
   for (int q = 0; q < j->chunk; q++) {
     int cnt = j->counter + j->iter + q;
-    if (p.UpdateNList > 0 && (cnt % p.UpdateNList) == 0) {
-      launch_nlist_count(P, j->st);
-      launch_nlist_fill(P, j->st);
-    }
+    if (p.UpdateNList > 0 && (cnt % p.UpdateNList) == 0) rebuild_pairs(P, j->st);
     calc_forces_enqueue(j->st, j->e.get(), true);
     launch_min_step(P.v, j->st, j->e->min_state, p.Algorithm, slope, p.Strictness, p.StepSize, steps);
   }
@@ -235,8 +269,7 @@ void pdgpu_server::enqueue_md_block(Job *j) {
         fail(j, PDGPU_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
         return;
       }
-      launch_nlist_count(P, j->st);
-      launch_nlist_fill(P, j->st);
+      rebuild_pairs(P, j->st);
       for (int q = 0; q < block; q++) md_step_enqueue(j->st, e, j->k);
       ce = cudaStreamEndCapture(j->st, &e->graph);
       e->gnodes = end_capture_count();
@@ -250,10 +283,7 @@ void pdgpu_server::enqueue_md_block(Job *j) {
     cudaGraphLaunch(e->gexec, j->st);
     launch_counter() += e->gnodes;
   } else {
-    if (rebuild) {
-      launch_nlist_count(P, j->st);
-      launch_nlist_fill(P, j->st);
-    }
+    if (rebuild) rebuild_pairs(P, j->st);
     for (int q = 0; q < block; q++) md_step_enqueue(j->st, e, j->k);
   }
   cudaMemcpyAsync(j->pin->flags, v.flags, sizeof(int) * F_COUNT, cudaMemcpyDeviceToHost, j->st);
@@ -390,14 +420,7 @@ void pdgpu_server::advance(Job *j) {
         j->charged = actual;
       }
       e->drop_graph();  // a regrown list buffer invalidates a captured block
-      if (j->after_size == PH_FINISH) {
-        calc_forces_enqueue(j->st, e, true);
-        enqueue_results(j);
-      } else if (j->after_size == PH_MIN) {
-        enqueue_min_chunk(j);
-      } else {
-        enqueue_md_block(j);
-      }
+      start(j, j->after_size);
       return;
     }
     case PH_MIN: {
@@ -592,7 +615,7 @@ void pdgpu_serve_params_default(pdgpu_serve_params *p) {
   p->hbm_budget = 120LL * 1000 * 1000 * 1000;
   p->max_active = 32;
   p->lanes[0] = p->lanes[1] = p->lanes[2] = 8;
-  p->tiles = 0;   // list rows: minimisation rebuilds the list every step
+  p->tiles = 1;   // tile passes; rebuilds by tile search, no list (systems within the search limit)
   p->policy = 1;  // least work first: short jobs do not queue behind long MD runs
 }
 

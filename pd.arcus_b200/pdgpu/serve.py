@@ -21,7 +21,7 @@ class Server:
 
     ARRIVAL, LEAST_WORK = 0, 1
 
-    def __init__(self, ctx, hbm_budget=None, max_active=None, lanes=(8, 8, 8), tiles=False, policy=1):
+    def __init__(self, ctx, hbm_budget=None, max_active=None, lanes=(8, 8, 8), tiles=True, policy=1):
         self.ctx = ctx
         p = A.ServeParams()
         A.lib().pdgpu_serve_params_default(ctypes.byref(p))
