@@ -67,6 +67,23 @@ def rank_info():
     return r, w, lr
 
 
+def max_over_ranks(value, dist, device):
+    """The largest of the ranks' values, on every rank (the value itself
+    without a process group).  Replicas: each rank times its own copy of the
+    workload and the job takes as long as the slowest."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_ns_per_day(n_ranks, steps_per_rank, seconds):
+    """Aggregate simulated time of all replicas per day of wall time."""
+    return n_ranks * steps_per_rank * DT_FS * 1e-6 / seconds * 86400.0
+
+
 def load_fixture():
     z = np.load(FIXTURE)
     arrays = {k: z[k] for k in z.files}
@@ -640,15 +657,8 @@ def main():
     L.pdgpu_launch_count(ctx.ptr, ctypes.byref(lc1))
     if dist:
         dist.barrier()
-    t_local = dev_ms / 1e3
-    if dist:
-        t = torch.tensor([t_local], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    else:
-        t_max = t_local
-    ns_total = n_gpus * args.steps * DT_FS * 1e-6
-    value = ns_total / t_max * 86400.0
+    t_max = max_over_ranks(dev_ms / 1e3, dist, "cuda")
+    value = whole_job_ns_per_day(n_gpus, args.steps, t_max)
 
     # end to end through the public API: per list period, host -> device
     # state (pinned), 10 steps, device -> host state + energies
@@ -680,12 +690,8 @@ def main():
             s2 += k
             done += k
         torch.cuda.synchronize()
-        te = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([te], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = float(t.item())
-        e2e = {"value": n_gpus * e2e_steps * DT_FS * 1e-6 / te * 86400.0, "unit": "ns/day",
+        te = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+        e2e = {"value": whole_job_ns_per_day(n_gpus, e2e_steps, te), "unit": "ns/day",
                "h2d_bytes_per_step": int(2 * n * 24 / BLOCK),
                "d2h_bytes_per_step": int((2 * n * 24 + A.ENE_COUNT * 8) / BLOCK),
                "steps": e2e_steps, "api": "pdgpu_set_positions/velocities + pdgpu_md_run(10) + get_*"}

@@ -1,0 +1,72 @@
+"""CPU: the multi-GPU host path of bench.py with two gloo ranks.
+
+The path shards as replicas (independent systems, no exchange step), so the
+only collective is the timing reduction: every rank gets the slowest rank's
+time, and the whole-job value counts every rank's work.  The reference arm
+runs on rank 0 alone; the other ranks exit 0 without work.
+"""
+import os
+import socket
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, out):
+    import datetime
+    import torch.distributed as dist
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import bench
+    r, w, lr = bench.rank_info()
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        t = bench.max_over_ranks(1.0 + rank, dist, "cpu")  # rank 1 is the slow one
+        value = bench.whole_job_ns_per_day(w, 1000, t)
+        out.put((rank, r, w, lr, t, value))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_take_the_slowest_time():
+    import torch.multiprocessing as mp
+    import bench
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, r, w, lr, t, value in res:
+        assert (r, w, lr) == (rank, 2, rank)
+        assert t == 2.0  # max over ranks, on every rank
+        assert value == pytest.approx(2 * 1000 * 1e-6 / 2.0 * 86400.0)
+    assert bench.max_over_ranks(3.5, None, "cpu") == 3.5
+
+
+def test_reference_arm_exits_without_work_on_other_ranks(monkeypatch):
+    import bench
+    monkeypatch.setenv("RANK", "1")
+    monkeypatch.setenv("WORLD_SIZE", "2")
+    monkeypatch.setenv("LOCAL_RANK", "1")
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--impl", "reference", "--gpus", "2"])
+
+    def no_work(*a, **k):
+        raise AssertionError("rank 1 must not run the reference")
+    monkeypatch.setattr(bench, "run_reference", no_work)
+    assert bench.main() == 0
