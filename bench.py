@@ -58,6 +58,11 @@ REF_PARAM = os.path.join(ROOT, "oracle", "_ref", "param")
 DT_FS = 1.0
 BLOCK = 10  # list period = one timed iteration (L2 flushed between them)
 METRIC = "GB MD ns/day"
+# DRAM bytes (read + write) of one launch of the fused pair kernel on this
+# workload, from one ncu capture (profiles/k_gb_tile_md_20566.md:
+# dram__bytes_read.sum + dram__bytes_write.sum, cold caches); ncu cannot run
+# inside the timed bench, so the figure is carried here with its source
+NCU_TRAFFIC_K3_TILES = 2867200 + 0
 
 
 def rank_info():
@@ -718,7 +723,9 @@ def main():
             "achieved": (k3_flop / t3 / 1e12) if bound == "fp32" else (k3_sfu / t3 / 1e12),
             "peak": (F32 if bound == "fp32" else SFU) / 1e12,
             "unit": "TFLOP/s" if bound == "fp32" else "Top/s (MUFU)",
-            "frac": max(k3_frac_fp32, k3_frac_sfu), "traffic": None,
+            "frac": max(k3_frac_fp32, k3_frac_sfu),
+            "traffic": NCU_TRAFFIC_K3_TILES if path == 1 else None,
+            "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
             "peak_source": "nominal %d SMs x %s/clk at sm_max_mhz %.0f (no measured FP32/SFU peak)" % (
                 sms, "256 flop" if bound == "fp32" else "16 MUFU", f_max / 1e6),
             "pairs": {"P_B": P_B, "P_H": P_H, "list_entries": entries},
