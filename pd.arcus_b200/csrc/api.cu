@@ -1276,9 +1276,8 @@ int pdgpu_md_init_velocities(pdgpu_ctx *c, int32_t sys, double temperature, uint
 void pdgpu::md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k) {
   Pack &P = *e->pack;
   calc_forces_enqueue(st, e, false);
-  launch_md_step_impl(P.v, st, k, nullptr, e->step_dev, P.is_h, e->seeds);
-  launch_energy(P.v, st, EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0) | EM_KINETIC | EM_RECORD, e->hist,
-                e->step_dev);
+  launch_md_step_energy(P.v, st, k, P.is_h, e->seeds,
+                        EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0) | EM_KINETIC | EM_RECORD, e->hist, e->step_dev);
 }
 extern "C" {
 

@@ -11,7 +11,7 @@
 // loop records the step's energies and advances the step.
 #include <cuda_runtime.h>
 
-#include "internal.cuh"
+#include "mdatom.cuh"
 
 namespace pdgpu {
 
@@ -23,11 +23,16 @@ static_assert(kEnergyThreads / 32 >= P_COUNT, "one warp per partial slot");
 
 // hist: [step][sys][3] (epot, ekin, etot); step_dev[0] current step,
 // step_dev[1] first step of the run, step_dev[2] finished-system counter.
+// MD: the block first advances its chunk's atoms by one integrator step
+// (the step kernel's work, md_atom) and sums their kinetic energies, so a
+// step needs no separate integrator launch.
+template <bool MD>
 __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode, int C, double J2kcalmol,
-                                                           double *hist, int *step_dev) {
+                                                           double *hist, int *step_dev, MDDev md) {
   PDGPU_DEP_ENTRY();
   if (v.flags[F_NL_OVERFLOW]) return;
   const int c = blockIdx.x, s = blockIdx.y, N = v.n_atoms;
+  const int md_step = MD ? *step_dev : 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   __shared__ double sh[kEnergyThreads / 32][P_COUNT];
   __shared__ double tot[P_COUNT];
@@ -48,7 +53,13 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode,
         acc[P_SELF] += v.e_atom[(size_t)AE_POL_SELF * N + i];
       }
       if (mode & EM_PAIR_NB) acc[P_NBVIR] += v.e_atom[(size_t)AE_VIR * N + i];
-      if (mode & EM_KINETIC) acc[P_KIN] += v.e_atom[(size_t)AE_KIN * N + i];
+      if (MD) {
+        const double ke = md_atom(v, md, nullptr, md_step, i);  // J
+        v.e_atom[(size_t)AE_KIN * N + i] = ke;
+        acc[P_KIN] += ke;
+      } else if (mode & EM_KINETIC) {
+        acc[P_KIN] += v.e_atom[(size_t)AE_KIN * N + i];
+      }
     }
   if (mode & EM_BONDED) {
     const int S1 = v.n_sys + 1;
@@ -171,8 +182,16 @@ void launch_energy(const PackView &v, cudaStream_t st, int mode, double *hist, i
   if (!v.n_sys) return;
   const Consts &k = consts();
   int C = v.e_chunks;
-  PDGPU_LAUNCH_DEP(k_energy, dim3(C, v.n_sys), kEnergyThreads, 0, st, v, mode, C, k.J2kcal * k.Na, hist,
-                   step_dev);
+  PDGPU_LAUNCH_DEP(k_energy<false>, dim3(C, v.n_sys), kEnergyThreads, 0, st, v, mode, C, k.J2kcal * k.Na, hist,
+                   step_dev, MDDev{});
+}
+void launch_md_step_energy(const PackView &v, cudaStream_t st, const MDCoef &c, const unsigned char *is_h,
+                           const unsigned long long *seeds, int mode, double *hist, int *step_dev) {
+  if (!v.n_sys || !v.n_atoms) return;
+  const Consts &k = consts();
+  int C = v.e_chunks;
+  PDGPU_LAUNCH_DEP(k_energy<true>, dim3(C, v.n_sys), kEnergyThreads, 0, st, v, mode | EM_KINETIC, C,
+                   k.J2kcal * k.Na, hist, step_dev, make_md_dev(c, is_h, seeds));
 }
 
 }  // namespace pdgpu

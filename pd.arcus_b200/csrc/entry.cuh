@@ -11,6 +11,10 @@ namespace pdgpu {
 const char *last_error_cstr();
 void launch_md_step_impl(const PackView &v, cudaStream_t st, const MDCoef &c, const double *normals,
                          const int *step_dev, const unsigned char *is_h, const unsigned long long *seeds);
+// one MD step of every atom fused with the step's energy record (the
+// integrator's work done by the energy reduction's blocks; step_dev needed)
+void launch_md_step_energy(const PackView &v, cudaStream_t st, const MDCoef &c, const unsigned char *is_h,
+                           const unsigned long long *seeds, int mode, double *hist, int *step_dev);
 void launch_pair_counts(const PackView &v, cudaStream_t st, unsigned long long *out);
 void launch_ke_from_velocities(const PackView &v, cudaStream_t st);
 void launch_vel_init_impl(const PackView &v, cudaStream_t st, double temp, const unsigned long long *seeds);

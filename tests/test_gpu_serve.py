@@ -86,16 +86,21 @@ def test_serve_alone_equals_mixed(gpu_ctx, tiles):
         assert info["t_total_ms"] >= info["t_run_ms"] >= 0.0
 
 
-def test_serve_matches_plain_calls_and_reference(gpu_ctx):
+@pytest.mark.parametrize("tiles", [True, False])
+def test_serve_matches_plain_calls_and_reference(gpu_ctx, tiles):
     import pdgpu
     members = _members(gpu_ctx, 6)
     jobs = _jobs(pdgpu)
-    srv = pdgpu.Server(gpu_ctx, max_active=8, lanes=LANES)
+    srv = pdgpu.Server(gpu_ctx, max_active=8, lanes=LANES, tiles=tiles)
     served, infos = _run(srv, members, jobs, together=True)
     srv.close()
     for (ws, ff, a, m), job, res, info in zip(members, jobs, served, infos):
         one = pdgpu.Batch([ws])
-        one.setLanes(LANES)  # the server's layout: list rows with these lanes
+        # the server's layout: tiles, or list rows with these lanes
+        if tiles:
+            one.setPairPath(1)
+        else:
+            one.setLanes(LANES)
         if job.kind == pdgpu.Server.ENERGY:
             f, e = one.evaluate()
             assert np.array_equal(res["forces"], f)
