@@ -1150,13 +1150,27 @@ int pdgpu_bonded_forces(pdgpu_ctx *c, int32_t sys) {
 // Born-radius kernel zeroes forces and record first; one energy reduction.
 // extra_mode adds EM_KINETIC / EM_RECORD inside an MD step.
 }  // extern "C"
+// Forcefield::calcForces for {FF_Bonded, GB}: the bonded terms (zeroing
+// their accumulators first) run on the pack's second stream beside the
+// three pair passes; the stream joins before the energies are read.
 void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce) {
   Pack &P = *e->pack;
-  launch_born_radii(P.v, st, true);
-  if (has_bonded(P)) launch_bonded_terms(P.v, st);
+  const bool bonded = has_bonded(P);
+  if (bonded) {
+    const size_t bytes = sizeof(long long) * (size_t)P.v.n_atoms;
+    cudaEventRecord(P.fork, st);
+    cudaStreamWaitEvent(P.side, P.fork, 0);
+    cudaMemsetAsync(P.v.fx, 0, bytes, P.side);
+    cudaMemsetAsync(P.v.fy, 0, bytes, P.side);
+    cudaMemsetAsync(P.v.fz, 0, bytes, P.side);
+    launch_bonded_terms(P.v, P.side);
+    cudaEventRecord(P.join, P.side);
+  }
+  launch_born_radii(P.v, st, bonded ? ZF_PAIRS : ZF_PAIRS | ZF_BONDED);
   launch_gb_pair(P.v, st);
   launch_gb_chain(P.v, st);
-  if (reduce) launch_energy(P.v, st, EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0));
+  if (bonded) cudaStreamWaitEvent(st, P.join, 0);
+  if (reduce) launch_energy(P.v, st, EM_PAIR_GB | (bonded ? EM_BONDED : 0));
 }
 extern "C" {
 

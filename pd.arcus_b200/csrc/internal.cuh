@@ -240,6 +240,9 @@ struct Pack {
   bool tuned = false;            // lanes-per-atom chosen by the autotuner
   double last_run_ms = 0.0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // the bonded terms run on a second stream beside the pair passes
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   ~Pack();
 };
 
@@ -264,9 +267,11 @@ void launch_zero(const PackView &v, cudaStream_t st);
 // neighbour list: build phases.  count -> (host may read total) -> fill
 void launch_nlist_count(Pack &p, cudaStream_t st);
 void launch_nlist_fill(Pack &p, cudaStream_t st);
-// GB (zero_first: also zero the forces and the potential-energy record,
-// WorkSpace::zeroForces, so the step needs no separate zeroing launch)
-void launch_born_radii(const PackView &v, cudaStream_t st, bool zero_first = false);
+// GB.  zero: ZeroFlags bits; ZF_PAIRS zeroes the pair-force accumulators
+// and the potential-energy record, ZF_BONDED the bonded-force accumulators
+// (together WorkSpace::zeroForces, so a step needs no separate zeroing launch)
+enum ZeroFlags { ZF_PAIRS = 1, ZF_BONDED = 2 };
+void launch_born_radii(const PackView &v, cudaStream_t st, int zero = 0);
 void launch_gb_pair(const PackView &v, cudaStream_t st);
 void launch_gb_chain(const PackView &v, cudaStream_t st);
 // cluster-pair tile versions of the three passes (tiles.cu); the plain
@@ -280,11 +285,11 @@ void launch_tiles_build(const PackView &v, cudaStream_t st);
 constexpr int kTileSearchMaxAtoms = 65536;
 void launch_tiles_search(const PackView &v, cudaStream_t st);
 void launch_tile_counts(const PackView &v, cudaStream_t st, unsigned long long *out);
-void launch_born_radii_tile(const PackView &v, cudaStream_t st, bool zero_first);
+void launch_born_radii_tile(const PackView &v, cudaStream_t st, int zero);
 void launch_gb_pair_tile(const PackView &v, cudaStream_t st);
 void launch_gb_chain_tile(const PackView &v, cudaStream_t st);
 // explicit lanes-per-atom variants (4, 8, 16, 32), used by the autotuner
-void launch_born_radii_lpa(const PackView &v, cudaStream_t st, bool zero_first, int lpa);
+void launch_born_radii_lpa(const PackView &v, cudaStream_t st, int zero, int lpa);
 void launch_gb_pair_lpa(const PackView &v, cudaStream_t st, int lpa);
 void launch_gb_chain_lpa(const PackView &v, cudaStream_t st, int lpa);
 void launch_born_energy(const PackView &v, cudaStream_t st);

@@ -114,12 +114,14 @@ __global__ void __launch_bounds__(256) k_born(PackView v, int zero_first) {
       long long *f = sub == 0 ? v.fx : (sub == 1 ? v.fy : v.fz);
       double *g = sub == 0 ? v.gx : (sub == 1 ? v.gy : v.gz);
       long long *h = sub == 0 ? v.hx : (sub == 1 ? v.hy : v.hz);
-      f[i] = 0;
+      if (zero_first & ZF_BONDED) f[i] = 0;
       g[i] = 0.0;
       h[i] = 0;
-      if (i == v.atom_off[s])
+      if (i == v.atom_off[s]) {
         for (int k = sub; k < E_COUNT; k += 3)
           if (k != E_EKIN) v.ene[(size_t)s * E_COUNT + k] = 0.0;
+        if (sub == 0) v.sys_flags[s] = 0;
+      }
     }
     const float4 ia = v.pq[2 * (size_t)ii], ib = v.pq[2 * (size_t)ii + 1];
     const float Ri = v.chainp[ii].x;
@@ -167,13 +169,13 @@ static int persistent_blocks(K kern, int n_atoms, int lpa) {
   return (int)(need < cap ? need : cap);
 }
 
-void launch_born_radii_lpa(const PackView &v, cudaStream_t st, bool zero_first, int lpa) {
+void launch_born_radii_lpa(const PackView &v, cudaStream_t st, int zero_first, int lpa) {
   if (!v.n_atoms) return;
   switch (lpa) {
-    case 4: PDGPU_LAUNCH(k_born<4>, persistent_blocks(k_born<4>, v.n_atoms, 4), 256, 0, st, v, (int)zero_first); break;
-    case 16: PDGPU_LAUNCH(k_born<16>, persistent_blocks(k_born<16>, v.n_atoms, 16), 256, 0, st, v, (int)zero_first); break;
-    case 32: PDGPU_LAUNCH(k_born<32>, persistent_blocks(k_born<32>, v.n_atoms, 32), 256, 0, st, v, (int)zero_first); break;
-    default: PDGPU_LAUNCH(k_born<8>, persistent_blocks(k_born<8>, v.n_atoms, 8), 256, 0, st, v, (int)zero_first); break;
+    case 4: PDGPU_LAUNCH(k_born<4>, persistent_blocks(k_born<4>, v.n_atoms, 4), 256, 0, st, v, zero_first); break;
+    case 16: PDGPU_LAUNCH(k_born<16>, persistent_blocks(k_born<16>, v.n_atoms, 16), 256, 0, st, v, zero_first); break;
+    case 32: PDGPU_LAUNCH(k_born<32>, persistent_blocks(k_born<32>, v.n_atoms, 32), 256, 0, st, v, zero_first); break;
+    default: PDGPU_LAUNCH(k_born<8>, persistent_blocks(k_born<8>, v.n_atoms, 8), 256, 0, st, v, zero_first); break;
   }
 }
 
@@ -310,7 +312,7 @@ void launch_gb_chain_lpa(const PackView &v, cudaStream_t st, int lpa) {
   }
 }
 
-void launch_born_radii(const PackView &v, cudaStream_t st, bool zero_first) {
+void launch_born_radii(const PackView &v, cudaStream_t st, int zero_first) {
   if (v.tile_mode)
     launch_born_radii_tile(v, st, zero_first);
   else

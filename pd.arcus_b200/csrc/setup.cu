@@ -214,6 +214,9 @@ Pack::~Pack() {
   for (void *a : allocs) cudaFreeAsync(a, st);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
+  if (fork) cudaEventDestroy(fork);
+  if (join) cudaEventDestroy(join);
+  if (side) cudaStreamDestroy(side);
   if (cur >= 0 && cur != device) cudaSetDevice(cur);
 }
 
@@ -632,6 +635,9 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   }
   cudaEventCreate(&p->ev0);
   cudaEventCreate(&p->ev1);
+  cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming);
+  cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking);
   cudaError_t e = sync ? cudaStreamSynchronize(st) : cudaGetLastError();
   if (e != cudaSuccess) {
     if (err) *err = std::string("pack upload failed: ") + cudaGetErrorString(e);

@@ -520,9 +520,11 @@ __global__ void k_born_finish(PackView v, int zero_first) {
   const int N = v.n_atoms;
   for (int q = 0; q < 4; q++) v.ej[(size_t)q * N + i] = 0;
   if (zero_first) {
-    v.fx[i] = 0;
-    v.fy[i] = 0;
-    v.fz[i] = 0;
+    if (zero_first & ZF_BONDED) {
+      v.fx[i] = 0;
+      v.fy[i] = 0;
+      v.fz[i] = 0;
+    }
     v.gx[i] = 0.0;
     v.gy[i] = 0.0;
     v.gz[i] = 0.0;
@@ -809,10 +811,10 @@ void launch_tiles_search(const PackView &v, cudaStream_t st) {
   PDGPU_LAUNCH(k_cluster_boxes, (v.n_jc + 127) / 128, 128, 0, st, v);
   PDGPU_LAUNCH(k_tile_search, v.n_sc, 32 * kSearchWarps, 0, st, v);
 }
-void launch_born_radii_tile(const PackView &v, cudaStream_t st, bool zero_first) {
+void launch_born_radii_tile(const PackView &v, cudaStream_t st, int zero_first) {
   if (!v.n_sc) return;
   PDGPU_LAUNCH_DEP(k_born_tile, v.tile_blocks[0], 32 * kTileWarps, 0, st, v);
-  PDGPU_LAUNCH_DEP(k_born_finish, (v.n_atoms + 63) / 64, 64, 0, st, v, (int)zero_first);
+  PDGPU_LAUNCH_DEP(k_born_finish, (v.n_atoms + 63) / 64, 64, 0, st, v, zero_first);
 }
 void launch_gb_pair_tile(const PackView &v, cudaStream_t st) {
   if (!v.n_sc) return;
