@@ -1166,7 +1166,15 @@ void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce) {
     launch_bonded_terms(P.v, P.side);
     cudaEventRecord(P.join, P.side);
   }
-  launch_born_radii(P.v, st, bonded ? ZF_PAIRS : ZF_PAIRS | ZF_BONDED);
+  // with an MD step's energy record still running beside, the record is
+  // left to it (it forms the record from zero) and the fused pass, which
+  // writes what the record reads, waits for it
+  const bool pending = P.energy_pending;
+  launch_born_radii(P.v, st, ZF_PAIRS | (bonded ? 0 : ZF_BONDED) | (pending ? 0 : ZF_RECORD));
+  if (pending) {
+    cudaStreamWaitEvent(st, P.ene_done, 0);
+    P.energy_pending = false;
+  }
   launch_gb_pair(P.v, st);
   launch_gb_chain(P.v, st);
   if (bonded) cudaStreamWaitEvent(st, P.join, 0);
@@ -1290,8 +1298,25 @@ int pdgpu_md_init_velocities(pdgpu_ctx *c, int32_t sys, double temperature, uint
 void pdgpu::md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k) {
   Pack &P = *e->pack;
   calc_forces_enqueue(st, e, false);
-  launch_md_step_energy(P.v, st, k, P.is_h, e->seeds,
-                        EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0) | EM_KINETIC | EM_RECORD, e->hist, e->step_dev);
+  launch_md_step_impl(P.v, st, k, nullptr, e->step_dev, P.is_h, e->seeds);
+  // the step's energy record on the second stream, beside the next step's
+  // Born pass (its bonded terms queue behind it on that stream)
+  cudaEventRecord(P.fork2, st);
+  cudaStreamWaitEvent(P.side, P.fork2, 0);
+  launch_energy(P.v, P.side,
+                EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0) | EM_KINETIC | EM_RECORD | EM_ASSIGN, e->hist,
+                e->step_dev);
+  cudaEventRecord(P.ene_done, P.side);
+  P.energy_pending = true;
+}
+// The end of a run of MD steps: the last step's energy record joins the
+// main stream.
+void pdgpu::md_steps_end(cudaStream_t st, SysEntry *e) {
+  Pack &P = *e->pack;
+  if (P.energy_pending) {
+    cudaStreamWaitEvent(st, P.ene_done, 0);
+    P.energy_pending = false;
+  }
 }
 extern "C" {
 
@@ -1368,6 +1393,7 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
           PDGPU_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
           rebuild_enqueue(P, c->st);
           for (int q = 0; q < block; q++) md_step_enqueue(c->st, e, k);
+          md_steps_end(c->st, e);
           PDGPU_CUDA(cudaStreamEndCapture(c->st, &e->graph));
           PDGPU_CUDA(cudaGraphInstantiate(&e->gexec, e->graph, 0));
           e->gnodes = end_capture_count();
@@ -1379,6 +1405,7 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
       } else {
         if (rebuild) rebuild_enqueue(P, c->st);
         for (int q = 0; q < block; q++) md_step_enqueue(c->st, e, k);
+        md_steps_end(c->st, e);
       }
       int flags[F_COUNT];
       PDGPU_CUDA(cudaMemcpyAsync(flags, v.flags, sizeof flags, cudaMemcpyDeviceToHost, c->st));

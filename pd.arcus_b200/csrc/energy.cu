@@ -121,6 +121,9 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode,
   if (threadIdx.x == 0) {
     v.e_done[s] = 0;
     double *R = sE;
+    if (mode & EM_ASSIGN)  // as WorkSpace::zeroForces left it
+      for (int k = 0; k < E_COUNT; k++)
+        if (k != E_EKIN) R[k] = 0.0;
     if (mode & (EM_PAIR_GB | EM_PAIR_NB)) {
       R[E_VDW] = tot[P_VDW];
       R[E_ELEC] = tot[P_ELEC];
@@ -158,6 +161,7 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode,
   __syncthreads();
   if (warp == 0) {
     if (lane < E_COUNT) E[lane] = sE[lane];
+    if (lane == 31) v.sys_flags[s] = 0;  // consumed
     if ((mode & EM_RECORD) && lane < 3) {
       double *h = hist + ((size_t)sk * v.n_sys + s) * 3;
       h[lane] = sE[lane == 0 ? E_EPOT : lane == 1 ? E_EKIN : E_ETOT];

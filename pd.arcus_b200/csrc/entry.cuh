@@ -98,6 +98,7 @@ bool has_bonded(const Pack &P);
 void calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce);
 // one MD step: forces, integrator, energy record (+ step counter advance)
 void md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k);
+void md_steps_end(cudaStream_t st, SysEntry *e);
 MDCoef md_coef(const pdgpu_md_params *p, int step, int steps);
 // grow a pack's list buffer to hold `total` entries (stream-ordered)
 int nlist_reserve(Pack &P, long long total, cudaStream_t st);

@@ -86,7 +86,8 @@ enum EnergyMode {
   EM_BORN_ENERGY = 4,  // energy-only Born term
   EM_BONDED = 8,       // bond, angle, torsion, bond virial
   EM_KINETIC = 16,     // ekin, etot
-  EM_RECORD = 32       // history row + step counter advance (step loops)
+  EM_RECORD = 32,      // history row + step counter advance (step loops)
+  EM_ASSIGN = 64       // form the record from zero (its slots were not zeroed before the step)
 };
 
 struct BondedTerms {
@@ -243,6 +244,10 @@ struct Pack {
   // the bonded terms run on a second stream beside the pair passes
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  // an MD step's energy record runs on the second stream beside the next
+  // step's first passes; the next writer of what it reads waits on ene_done
+  cudaEvent_t fork2 = nullptr, ene_done = nullptr;
+  bool energy_pending = false;
   ~Pack();
 };
 
@@ -267,10 +272,11 @@ void launch_zero(const PackView &v, cudaStream_t st);
 // neighbour list: build phases.  count -> (host may read total) -> fill
 void launch_nlist_count(Pack &p, cudaStream_t st);
 void launch_nlist_fill(Pack &p, cudaStream_t st);
-// GB.  zero: ZeroFlags bits; ZF_PAIRS zeroes the pair-force accumulators
-// and the potential-energy record, ZF_BONDED the bonded-force accumulators
-// (together WorkSpace::zeroForces, so a step needs no separate zeroing launch)
-enum ZeroFlags { ZF_PAIRS = 1, ZF_BONDED = 2 };
+// GB.  zero: ZeroFlags bits; ZF_PAIRS zeroes the pair-force accumulators,
+// ZF_BONDED the bonded-force accumulators, ZF_RECORD the potential-energy
+// record and the system flags (together WorkSpace::zeroForces, so a step
+// needs no separate zeroing launch)
+enum ZeroFlags { ZF_PAIRS = 1, ZF_BONDED = 2, ZF_RECORD = 4 };
 void launch_born_radii(const PackView &v, cudaStream_t st, int zero = 0);
 void launch_gb_pair(const PackView &v, cudaStream_t st);
 void launch_gb_chain(const PackView &v, cudaStream_t st);

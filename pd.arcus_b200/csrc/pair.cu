@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(256) k_born(PackView v, int zero_first) {
       if (zero_first & ZF_BONDED) f[i] = 0;
       g[i] = 0.0;
       h[i] = 0;
-      if (i == v.atom_off[s]) {
+      if ((zero_first & ZF_RECORD) && i == v.atom_off[s]) {
         for (int k = sub; k < E_COUNT; k += 3)
           if (k != E_EKIN) v.ene[(size_t)s * E_COUNT + k] = 0.0;
         if (sub == 0) v.sys_flags[s] = 0;

@@ -271,6 +271,7 @@ void pdgpu_server::enqueue_md_block(Job *j) {
       }
       rebuild_pairs(P, j->st);
       for (int q = 0; q < block; q++) md_step_enqueue(j->st, e, j->k);
+      md_steps_end(j->st, e);
       ce = cudaStreamEndCapture(j->st, &e->graph);
       e->gnodes = end_capture_count();
       if (ce == cudaSuccess) ce = cudaGraphInstantiate(&e->gexec, e->graph, 0);
@@ -285,6 +286,7 @@ void pdgpu_server::enqueue_md_block(Job *j) {
   } else {
     if (rebuild) rebuild_pairs(P, j->st);
     for (int q = 0; q < block; q++) md_step_enqueue(j->st, e, j->k);
+    md_steps_end(j->st, e);
   }
   cudaMemcpyAsync(j->pin->flags, v.flags, sizeof(int) * F_COUNT, cudaMemcpyDeviceToHost, j->st);
   record(j, PH_MD);

@@ -216,6 +216,8 @@ Pack::~Pack() {
   if (ev1) cudaEventDestroy(ev1);
   if (fork) cudaEventDestroy(fork);
   if (join) cudaEventDestroy(join);
+  if (fork2) cudaEventDestroy(fork2);
+  if (ene_done) cudaEventDestroy(ene_done);
   if (side) cudaStreamDestroy(side);
   if (cur >= 0 && cur != device) cudaSetDevice(cur);
 }
@@ -637,6 +639,8 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   cudaEventCreate(&p->ev1);
   cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&p->fork2, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&p->ene_done, cudaEventDisableTiming);
   cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking);
   cudaError_t e = sync ? cudaStreamSynchronize(st) : cudaGetLastError();
   if (e != cudaSuccess) {

@@ -531,7 +531,7 @@ __global__ void k_born_finish(PackView v, int zero_first) {
     v.hx[i] = 0;
     v.hy[i] = 0;
     v.hz[i] = 0;
-    if (i == v.atom_off[s]) {
+    if ((zero_first & ZF_RECORD) && i == v.atom_off[s]) {
       for (int k = 0; k < E_COUNT; k++)
         if (k != E_EKIN) v.ene[(size_t)s * E_COUNT + k] = 0.0;
       v.sys_flags[s] = 0;
