@@ -45,7 +45,17 @@
 
 namespace pdgpu {
 
-constexpr int kTileWarps = 4;    // warps per block (one block per i-cluster)
+constexpr int kTileWarps = 4;    // warps per block
+// resident blocks per SM the register allocation must allow, per pass
+#ifndef PDGPU_K2_BLOCKS
+#define PDGPU_K2_BLOCKS 6
+#endif
+#ifndef PDGPU_K3_BLOCKS
+#define PDGPU_K3_BLOCKS 5
+#endif
+#ifndef PDGPU_K4_BLOCKS
+#define PDGPU_K4_BLOCKS 6
+#endif
 constexpr int kBuildChunk = 128; // tiles assembled in shared memory at a time
 
 // --------------------------------------------------------------- tile list
@@ -427,7 +437,7 @@ __device__ __forceinline__ void warp_range(const PackView &v, int warp, int &e0,
 
 // --------------------------------------------------------------- K2 tiles
 // (register bounds: five blocks per SM)
-__global__ void __launch_bounds__(32 * kTileWarps, 5) k_born_tile(PackView v) {
+__global__ void __launch_bounds__(32 * kTileWarps, PDGPU_K2_BLOCKS) k_born_tile(PackView v) {
   PDGPU_DEP_ENTRY();
   if (v.flags[F_NL_OVERFLOW]) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -540,7 +550,7 @@ __global__ void k_born_finish(PackView v, int zero_first) {
 }
 
 // --------------------------------------------------------------- K3 tiles
-__global__ void __launch_bounds__(32 * kTileWarps, 5) k_gb_tile(PackView v) {
+__global__ void __launch_bounds__(32 * kTileWarps, PDGPU_K3_BLOCKS) k_gb_tile(PackView v) {
   PDGPU_DEP_ENTRY();
   if (v.flags[F_NL_OVERFLOW]) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -665,7 +675,7 @@ __global__ void k_gb_finish(PackView v) {
 }
 
 // --------------------------------------------------------------- K4 tiles
-__global__ void __launch_bounds__(32 * kTileWarps, 6) k_chain_tile(PackView v) {
+__global__ void __launch_bounds__(32 * kTileWarps, PDGPU_K4_BLOCKS) k_chain_tile(PackView v) {
   PDGPU_DEP_ENTRY();
   if (v.flags[F_NL_OVERFLOW]) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
