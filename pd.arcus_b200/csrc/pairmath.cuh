@@ -177,7 +177,7 @@ __device__ __forceinline__ float chain_term(const Dx &d, float Ri, float Rj, flo
     const float sq = 0.5f - 0.5f * cs;
     X = 4.f * sq * sq - 2.f * sq * sn * th;
   }
-  const float ir2 = __frcp_rn(d.r2);
+  const float ir2 = __fdividef(1.f, d.r2);  // the fast reciprocal: deterministic, ~1 ulp
   const float ir6 = ir2 * ir2 * ir2;
   return P4 * X * ir6 * (wi * Vj + wj * Vi);
 }
@@ -190,7 +190,7 @@ __device__ __forceinline__ float born_term_noV(const Dx &d, float Ri, float Rj, 
   // explicit roundings: the i and j sides of a pair, in any kernel, get
   // the same bits
   const float Rs = __fadd_rn(Ri, Rj);
-  const float ir2 = __frcp_rn(d.r2);
+  const float ir2 = __fdividef(1.f, d.r2);  // the fast reciprocal: deterministic, ~1 ulp
   float term = __fmul_rn(__fmul_rn(P4scaled, ir2), ir2);
   const float rdivR = __fdividef(d.r2, __fmul_rn(Rs, Rs));
   if (!(rdivR > invP5)) {
