@@ -67,8 +67,9 @@ __device__ __forceinline__ void angle_term(const PackView &v, int t, double *e_t
 __device__ __forceinline__ void dihedral_term(const PackView &v, int t, double *e_term) {
   int4 q = v.bt.tidx[t];
   int ti = q.x, ta = q.y, tb = q.z, tj = q.w;
-  const double *par = v.bt.tpar + 20 * (size_t)t;
-  int terms = v.bt.tterms[t];
+  const int ty = v.bt.ttype[t];
+  const double *par = v.bt.tpar + 20 * (size_t)ty;
+  int terms = v.bt.tterms[ty];
   double a[3] = {v.x[ti] - v.x[ta], v.y[ti] - v.y[ta], v.z[ti] - v.z[ta]};
   double b[3] = {v.x[ta] - v.x[tb], v.y[ta] - v.y[tb], v.z[ta] - v.z[tb]};
   double c[3] = {v.x[tb] - v.x[tj], v.y[tb] - v.y[tj], v.z[tb] - v.z[tj]};

@@ -99,8 +99,9 @@ struct BondedTerms {
   int4 *aiaj = nullptr;       // (i, a, j, -)
   double2 *akt = nullptr;     // (k kcal/mol/rad^2, theta0)
   int4 *tidx = nullptr;       // torsions then impropers (i,a,b,j)
-  int *tterms = nullptr;
-  double *tpar = nullptr;     // 20 per dihedral, 4 each: Vn kcal/mol, n, gamma, cos gamma, sin gamma
+  int *ttype = nullptr;       // [dihedrals] parameter set of each
+  int *tterms = nullptr;      // [sets] Fourier terms
+  double *tpar = nullptr;     // [sets * 20], 4 each: Vn kcal/mol, n, gamma, cos gamma, sin gamma
 };
 
 // Device view of a Pack.  Plain pointers, passed by value to kernels.

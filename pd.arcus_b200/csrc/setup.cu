@@ -502,8 +502,9 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   std::vector<int2> bij;
   std::vector<double2> blk, akt;
   std::vector<int4> aiaj, tidx;
-  std::vector<int> tterms;
+  std::vector<int> tterms, ttype;
   std::vector<double> tpar;
+  std::map<std::vector<double>, int> types;  // dihedral parameter sets (few per forcefield)
   double J2k = c.J2kcal * c.Na;
   for (int s = 0; s < S; s++) {
     const SystemHost &h = *systems[s];
@@ -527,15 +528,24 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
         int q = base + k;
         tidx.push_back(make_int4(o + h.tidx[4 * q], o + h.tidx[4 * q + 1], o + h.tidx[4 * q + 2],
                                  o + h.tidx[4 * q + 3]));
-        tterms.push_back(h.tterms[q]);
-        for (int m = 0; m < 12; m++) {
-          double val = h.tpar[12 * q + m];
-          tpar.push_back(m < 4 ? val * J2k : val);
+        // the dihedral's parameter set, stored once per distinct set: the
+        // kernel reads a 4-byte index per term and the table from cache
+        std::vector<double> key(h.tpar.begin() + 12 * q, h.tpar.begin() + 12 * q + 12);
+        key.push_back((double)h.tterms[q]);
+        auto it = types.find(key);
+        if (it == types.end()) {
+          it = types.emplace(key, (int)tterms.size()).first;
+          tterms.push_back(h.tterms[q]);
+          for (int m = 0; m < 12; m++) {
+            double val = h.tpar[12 * q + m];
+            tpar.push_back(m < 4 ? val * J2k : val);
+          }
+          // cos and sin of each phase, so the kernel needs no transcendental
+          // for the integer periodicities
+          for (int m = 0; m < 4; m++) tpar.push_back(std::cos(h.tpar[12 * q + 8 + m]));
+          for (int m = 0; m < 4; m++) tpar.push_back(std::sin(h.tpar[12 * q + 8 + m]));
         }
-        // cos and sin of each phase, so the kernel needs no transcendental
-        // for the integer periodicities
-        for (int m = 0; m < 4; m++) tpar.push_back(std::cos(h.tpar[12 * q + 8 + m]));
-        for (int m = 0; m < 4; m++) tpar.push_back(std::sin(h.tpar[12 * q + 8 + m]));
+        ttype.push_back(it->second);
       }
     }
   bt.nb = (int)bij.size();
@@ -621,6 +631,7 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   PALLOC(bt.akt, akt.size());
   PALLOC(bt.tidx, tidx.size());
   PALLOC(bt.tterms, tterms.size());
+  PALLOC(bt.ttype, ttype.size());
   PALLOC(bt.tpar, tpar.size());
   if (!bij.empty()) {
     cudaMemcpyAsync(bt.bij, bij.data(), sizeof(int2) * bij.size(), cudaMemcpyHostToDevice, st);
@@ -633,6 +644,7 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   if (!tidx.empty()) {
     cudaMemcpyAsync(bt.tidx, tidx.data(), sizeof(int4) * tidx.size(), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(bt.tterms, tterms.data(), sizeof(int) * tterms.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(bt.ttype, ttype.data(), sizeof(int) * ttype.size(), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(bt.tpar, tpar.data(), sizeof(double) * tpar.size(), cudaMemcpyHostToDevice, st);
   }
   cudaEventCreate(&p->ev0);
