@@ -283,6 +283,20 @@ void pdgpu_md_params_default(pdgpu_md_params *p);
 int pdgpu_md_run(pdgpu_ctx *ctx, int32_t sys, const pdgpu_md_params *p,
                  int32_t first_step, int32_t steps, int32_t total_steps,
                  double *history);
+/* Trajectory snapshots (ProtocolBase::UpdateTra with WorkSpace::outtra.append,
+ * md.cpp:260 and protocolbase.cpp:229-235): with every > 0, pdgpu_md_run
+ * records the positions after each step s with s > 0 and s % every == 0.
+ * The integrator writes them into a device ring inside the step graph, and
+ * each list period's frames are copied to a page-locked host ring of
+ * `capacity` frames on the pack's second stream while the next period runs.
+ * every = 0 stops recording and frees the rings. */
+int pdgpu_md_set_trajectory(pdgpu_ctx *ctx, int32_t sys, int32_t every, int32_t capacity);
+/* Frames recorded since the last call, oldest first: up to max_frames of
+ * frames[max_frames][natoms][3] (A) with their step numbers (steps may be
+ * NULL), *count of them, and *dropped (may be NULL) overwritten in the host
+ * ring before they were read. */
+int pdgpu_md_read_trajectory(pdgpu_ctx *ctx, int32_t sys, double *frames, int64_t *steps, int32_t max_frames,
+                             int32_t *count, int32_t *dropped);
 /* One integrator step with externally supplied normals (normals[6*natoms],
  * per atom in the order the reference's three nrand() pairs draw them:
  * n1x n2y n2x n1z n1y n2z), on the forces already accumulated.  For exact

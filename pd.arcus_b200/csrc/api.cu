@@ -1298,7 +1298,8 @@ int pdgpu_md_init_velocities(pdgpu_ctx *c, int32_t sys, double temperature, uint
 void pdgpu::md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k) {
   Pack &P = *e->pack;
   calc_forces_enqueue(st, e, false);
-  launch_md_step_impl(P.v, st, k, nullptr, e->step_dev, P.is_h, e->seeds);
+  launch_md_step_impl(P.v, st, k, nullptr, e->step_dev, P.is_h, e->seeds, e->traj_dev, e->traj_every,
+                      e->traj_dev_cap);
   // the step's energy record on the second stream, beside the next step's
   // Born pass (its bonded terms queue behind it on that stream)
   cudaEventRecord(P.fork2, st);
@@ -1309,6 +1310,37 @@ void pdgpu::md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k) {
   cudaEventRecord(P.ene_done, P.side);
   P.energy_pending = true;
 }
+// Trajectory frames of steps [s0, s1) (absolute): mirrored from the device
+// ring into the host ring on the pack's second stream once the steps are
+// done.  The step graph of the next list period writes other ring slots
+// (the device ring holds two periods of frames), and before the period
+// after that the main stream waits for this copy.
+static void trajectory_copy(pdgpu_ctx *c, SysEntry *e, int s0, int s1) {
+  if (e->traj_every <= 0) return;
+  Pack &P = *e->pack;
+  const int ev = e->traj_every;
+  const size_t frame = 3 * (size_t)P.v.n_atoms;
+  if (e->traj_pending) cudaStreamWaitEvent(c->st, e->traj_ev, 0);  // the previous period's copy
+  cudaEventRecord(P.fork2, c->st);
+  cudaStreamWaitEvent(P.side, P.fork2, 0);
+  for (int st = std::max(s0, 1); st < s1; st++) {
+    if (st % ev) continue;
+    const long long idx = st / ev - 1;
+    const double *src = e->traj_dev + (size_t)(idx % e->traj_dev_cap) * frame;
+    const long long slot = e->traj_copied % e->traj_host_cap;
+    cudaMemcpyAsync(e->traj_host + (size_t)slot * frame, src, sizeof(double) * frame, cudaMemcpyDeviceToHost,
+                    P.side);
+    e->traj_step[slot] = st;
+    e->traj_copied++;
+  }
+  cudaEventRecord(e->traj_ev, P.side);
+  e->traj_pending = true;
+  // fewer than two periods of frames fit the device ring: the next period
+  // waits for this copy
+  const int per_period = (s1 - s0 + ev - 1) / ev + 1;
+  if (2 * per_period > e->traj_dev_cap) cudaStreamWaitEvent(c->st, e->traj_ev, 0);
+}
+
 // The end of a run of MD steps: the last step's energy record joins the
 // main stream.
 void pdgpu::md_steps_end(cudaStream_t st, SysEntry *e) {
@@ -1319,6 +1351,77 @@ void pdgpu::md_steps_end(cudaStream_t st, SysEntry *e) {
   }
 }
 extern "C" {
+
+int pdgpu_md_set_trajectory(pdgpu_ctx *c, int32_t sys, int32_t every, int32_t capacity) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (every < 0 || (every > 0 && capacity <= 0)) {
+    set_error("md_set_trajectory: need every >= 0 and capacity > 0");
+    return PDGPU_ERR_ARG;
+  }
+  Pack &P = *e->pack;
+  if (e->traj_pending) cudaStreamSynchronize(P.side);
+  e->drop_graph();
+  if (e->traj_dev) {
+    auto it = std::find(e->extra.begin(), e->extra.end(), (void *)e->traj_dev);
+    if (it != e->extra.end()) {
+      cudaFreeAsync(*it, e->st);
+      e->extra.erase(it);
+    }
+  }
+  e->free_trajectory();
+  if (every == 0) return PDGPU_OK;
+  const size_t frame = 3 * (size_t)P.v.n_atoms;
+  // the device ring: two list periods of frames at the most frequent
+  // cadence a run can use (every step), or the host capacity if smaller
+  const int dev_cap = std::max(2, std::min(capacity, 64));
+  if (xalloc(e, &e->traj_dev, frame * dev_cap) != cudaSuccess) {
+    set_error("device allocation failed (trajectory ring)");
+    return PDGPU_ERR_NOMEM;
+  }
+  if (cudaHostAlloc((void **)&e->traj_host, sizeof(double) * frame * capacity, cudaHostAllocDefault) != cudaSuccess) {
+    e->traj_host = nullptr;
+    set_error("page-locked allocation failed (trajectory frames)");
+    return PDGPU_ERR_NOMEM;
+  }
+  cudaEventCreateWithFlags(&e->traj_ev, cudaEventDisableTiming);
+  e->traj_every = every;
+  e->traj_dev_cap = dev_cap;
+  e->traj_host_cap = capacity;
+  e->traj_step.assign(capacity, -1);
+  return sync_check(c, "md_set_trajectory");
+}
+
+int pdgpu_md_read_trajectory(pdgpu_ctx *c, int32_t sys, double *frames, int64_t *steps, int32_t max_frames,
+                             int32_t *count, int32_t *dropped) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (!count || max_frames < 0 || (max_frames > 0 && !frames)) {
+    set_error("md_read_trajectory: bad arguments");
+    return PDGPU_ERR_ARG;
+  }
+  *count = 0;
+  if (dropped) *dropped = 0;
+  if (e->traj_every <= 0) return PDGPU_OK;
+  if (e->traj_pending) {
+    PDGPU_CUDA(cudaEventSynchronize(e->traj_ev));
+  }
+  long long first = e->traj_read;
+  if (e->traj_copied - first > e->traj_host_cap) {  // overwritten before being read
+    if (dropped) *dropped = (int32_t)(e->traj_copied - e->traj_host_cap - first);
+    first = e->traj_copied - e->traj_host_cap;
+  }
+  const size_t frame = 3 * (size_t)e->pack->v.n_atoms;
+  int n = 0;
+  for (long long q = first; q < e->traj_copied && n < max_frames; q++, n++) {
+    const long long slot = q % e->traj_host_cap;
+    std::memcpy(frames + (size_t)n * frame, e->traj_host + (size_t)slot * frame, sizeof(double) * frame);
+    if (steps) steps[n] = e->traj_step[slot];
+  }
+  e->traj_read = first + n;
+  *count = n;
+  return PDGPU_OK;
+}
 
 int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t first_step, int32_t steps,
                  int32_t total_steps, double *history) {
@@ -1383,10 +1486,10 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
       if (use_graph) {
         // graphs are cached per system; the key holds every value baked in
         char key[256];
-        snprintf(key, sizeof key, "%d|%p|%lld|%p|%d|%d|%.17g|%.17g|%.17g|%d|%d|%d|%d%d%d|%d%d", block,
+        snprintf(key, sizeof key, "%d|%p|%lld|%p|%d|%d|%.17g|%.17g|%.17g|%d|%d|%d|%d%d%d|%d%d|%p|%d|%d", block,
                  (void *)v.nl, v.nl_cap, (void *)e->hist, k.integrator, k.steps, k.dt, k.gamma, k.temp,
                  k.stochastic_h, P.radix_passes, (int)e->host->params.FastMode, v.lpa[0], v.lpa[1], v.lpa[2],
-                 v.tile_mode, (int)tile_search_ok(P));
+                 v.tile_mode, (int)tile_search_ok(P), (void *)e->traj_dev, e->traj_every, e->traj_dev_cap);
         if (!e->gexec || e->gkey != key) {
           e->drop_graph();
           begin_capture_count();
@@ -1430,6 +1533,7 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
       break;
     }
     P.nlist_counter = counter0 + block;
+    trajectory_copy(c, e, step, step + block);
     s += block;
   }
   cudaEventRecord(P.ev1, c->st);

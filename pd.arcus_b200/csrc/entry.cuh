@@ -10,7 +10,8 @@
 namespace pdgpu {
 const char *last_error_cstr();
 void launch_md_step_impl(const PackView &v, cudaStream_t st, const MDCoef &c, const double *normals,
-                         const int *step_dev, const unsigned char *is_h, const unsigned long long *seeds);
+                         const int *step_dev, const unsigned char *is_h, const unsigned long long *seeds,
+                         double *frames = nullptr, int frame_every = 0, int frame_cap = 0);
 // one MD step of every atom fused with the step's energy record (the
 // integrator's work done by the energy reduction's blocks; step_dev needed)
 void launch_md_step_energy(const PackView &v, cudaStream_t st, const MDCoef &c, const unsigned char *is_h,
@@ -48,6 +49,27 @@ struct SysEntry {
   int *step_dev = nullptr;
   double *hist = nullptr;
   int hist_cap = 0;
+  // trajectory snapshots (pdgpu_md_set_trajectory): a device ring written by
+  // the integrator, mirrored into a page-locked host ring on the pack's
+  // second stream after each list period
+  int traj_every = 0, traj_dev_cap = 0, traj_host_cap = 0;
+  double *traj_dev = nullptr;
+  double *traj_host = nullptr;
+  std::vector<long long> traj_step;   // [traj_host_cap] step of each host slot
+  long long traj_copied = 0, traj_read = 0;  // frames copied to the host ring / handed out
+  cudaEvent_t traj_ev = nullptr;      // the last copy
+  bool traj_pending = false;
+  void free_trajectory() {
+    if (traj_host) cudaFreeHost(traj_host);
+    if (traj_ev) cudaEventDestroy(traj_ev);
+    traj_host = nullptr;
+    traj_ev = nullptr;
+    traj_dev = nullptr;  // an `extra` allocation, freed with the entry
+    traj_every = traj_dev_cap = traj_host_cap = 0;
+    traj_step.clear();
+    traj_copied = traj_read = 0;
+    traj_pending = false;
+  }
   void *min_state = nullptr;
   std::vector<void *> extra;
   // cached MD block graph
@@ -64,6 +86,8 @@ struct SysEntry {
   }
   void free_device() {
     drop_graph();
+    if (traj_pending && pack) cudaStreamSynchronize(pack->side);
+    free_trajectory();
     for (void *p : extra) cudaFreeAsync(p, st);
     extra.clear();
     seeds = nullptr;

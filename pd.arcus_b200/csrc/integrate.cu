@@ -270,8 +270,12 @@ __global__ void k_min_restore_best(PackView v) {
 
 // --------------------------------------------------------------- launchers
 void launch_md_step_impl(const PackView &v, cudaStream_t st, const MDCoef &c, const double *normals,
-                         const int *step_dev, const unsigned char *is_h, const unsigned long long *seeds) {
-  const MDDev d = make_md_dev(c, is_h, seeds);
+                         const int *step_dev, const unsigned char *is_h, const unsigned long long *seeds,
+                         double *frames, int frame_every, int frame_cap) {
+  MDDev d = make_md_dev(c, is_h, seeds);
+  d.frames = frames;
+  d.frame_every = frames ? frame_every : 0;
+  d.frame_cap = frame_cap;
   // 64-thread blocks: a 20k-atom system spreads over every SM
   if (v.n_atoms) PDGPU_LAUNCH_DEP(k_md_step, (v.n_atoms + 63) / 64, 64, 0, st, v, d, normals, step_dev);
 }

@@ -64,6 +64,11 @@ struct MDDev {
   double kB;
   const unsigned char *is_h;
   const unsigned long long *sys_seed;
+  // trajectory snapshots: with frame_every > 0, the positions after step s
+  // (s > 0, s % frame_every == 0) go to ring slot (s / frame_every - 1) %
+  // frame_cap of frames[frame_cap][N][3]
+  double *frames;
+  int frame_every, frame_cap;
 };
 inline MDDev make_md_dev(const MDCoef &c, const unsigned char *is_h, const unsigned long long *seeds) {
   const Consts &k = consts();
@@ -74,6 +79,9 @@ inline MDDev make_md_dev(const MDCoef &c, const unsigned char *is_h, const unsig
   d.kB = k.kB;
   d.is_h = is_h;
   d.sys_seed = seeds;
+  d.frames = nullptr;
+  d.frame_every = 0;
+  d.frame_cap = 0;
   return d;
 }
 
@@ -194,6 +202,13 @@ __device__ __forceinline__ double md_atom(const PackView &v, const MDDev &d, con
   v.vy[i] = vel[1];
   v.vz[i] = vel[2];
   store_pos(v, i, pos[0], pos[1], pos[2]);
+  if (d.frame_every > 0 && step > 0 && step % d.frame_every == 0) {
+    // WorkSpace::outtra.append after the step (md.cpp:260)
+    double *fr = d.frames + (size_t)((step / d.frame_every - 1) % d.frame_cap) * 3 * (size_t)v.n_atoms + 3 * (size_t)i;
+    fr[0] = pos[0];
+    fr[1] = pos[1];
+    fr[2] = pos[2];
+  }
   return ke;
 }
 

@@ -136,6 +136,10 @@ PROTOTYPES = {
     "pdgpu_calc_forces": (ctypes.c_int, [_CTX, ctypes.c_int32]),
     "pdgpu_md_run": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.POINTER(MDParams), ctypes.c_int32,
                                     ctypes.c_int32, ctypes.c_int32, _D]),
+    "pdgpu_md_set_trajectory": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    "pdgpu_md_read_trajectory": (ctypes.c_int, [_CTX, ctypes.c_int32, _D, ctypes.POINTER(ctypes.c_int64),
+                                                ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                                ctypes.POINTER(ctypes.c_int32)]),
     "pdgpu_md_step_with_normals": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.POINTER(MDParams),
                                                   ctypes.c_int32, ctypes.c_int32, _D]),
     "pdgpu_md_init_velocities": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_double, ctypes.c_uint64]),

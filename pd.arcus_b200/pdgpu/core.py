@@ -600,6 +600,18 @@ class Minimisation(ProtocolBase):
         return taken.value
 
 
+def read_trajectory(ctx, handle, natoms, max_frames):
+    """Frames recorded since the last read: (frames[n][natoms][3] in A,
+    steps[n]) and the number overwritten before they were read."""
+    frames = np.zeros((max_frames, natoms, 3))
+    steps = np.zeros(max_frames, dtype=np.int64)
+    n, dropped = ctypes.c_int32(0), ctypes.c_int32(0)
+    A.check(A.lib().pdgpu_md_read_trajectory(ctx.ptr, handle, A.dptr(frames),
+                                             steps.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                             int(max_frames), ctypes.byref(n), ctypes.byref(dropped)))
+    return (frames[: n.value].copy(), steps[: n.value].copy()), dropped.value
+
+
 class MolecularDynamics(ProtocolBase):
     """MD protocol (protocols/md.h:84-128; md.cpp:202-267) with the step loop
     on the device: list rebuild every UpdateNList steps, forces, integrator,
@@ -622,7 +634,11 @@ class MolecularDynamics(ProtocolBase):
         self.UpdateNList = d.UpdateNList
         self.UseGraph = True
         self.Seed = 0
+        self.UpdateTra = 0            # record a frame every UpdateTra steps (0: none)
+        self.TrajectoryCapacity = 1000
         self.history = None
+        self.frames = None            # (frames[n][natoms][3] A, steps[n]) of the last run
+        self.dropped = 0
 
     def _params(self):
         p = A.md_params_default()
@@ -642,12 +658,19 @@ class MolecularDynamics(ProtocolBase):
         else:
             ws._push_velocities()
         hist = np.zeros(3 * int(self.Steps))
+        every = int(self.UpdateTra)
+        cap = max(1, int(self.TrajectoryCapacity))
+        A.check(L.pdgpu_md_set_trajectory(ws.ctx.ptr, ws._sys, every, cap))
         st = L.pdgpu_md_run(ws.ctx.ptr, ws._sys, ctypes.byref(self._params()), 0, int(self.Steps),
                             int(self.Steps), A.dptr(hist))
         self.history = hist.reshape(-1, 3)
         if st == A.ERR_UNSTABLE:
             raise A.UnstableError(st, A.last_error())
         A.check(st)
+        self.frames, self.dropped = None, 0
+        if every > 0:
+            self.frames, self.dropped = read_trajectory(ws.ctx, ws._sys, ws.nAtoms(), cap)
+            A.check(L.pdgpu_md_set_trajectory(ws.ctx.ptr, ws._sys, 0, 0))
         ws._pull_positions()
         ws._pull_velocities()
         self.ff._sync_out()
