@@ -8,6 +8,7 @@ control flow in Python over the C restatement's kernels:
 * ``minimise``     protocols/minimise.cpp:99-318 (runcore, SD and CG steps)
 * ``md_run``       protocols/md.cpp:202-267 run_core with Langevin / VV / Beeman
 * ``calc_forces``  forcefields/forcefield.cpp:220-247 (zero, then each component)
+* ``lcpo``         forcefields/lcpo.cpp: FF_SASA_LCPO's forces and energies paths
 
 Units follow the reference: Angstrom, J, N, kg.
 """
@@ -96,6 +97,9 @@ def lib():
         L.pdo_beeman_step.argtypes = [ctypes.c_int, _D, _D, _D, _D, _D, ctypes.c_double,
                                       ctypes.c_int, ctypes.c_int]
         L.pdo_beeman_step.restype = ctypes.c_double
+        L.pdo_lcpo.argtypes = [ctypes.c_int, _D, _I, _I, _D, _D, _D, _B, ctypes.c_int, _D, _D,
+                               ctypes.POINTER(ctypes.c_long)]
+        L.pdo_lcpo.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -282,6 +286,29 @@ class System:
         e["epot"] += eg[0]
         e["vdw"], e["elec"], e["pol"], e["pol_cross"], e["pol_self"] = eg[1:6]
         return f, e, born
+
+
+def lcpo(pos, ptr, data, radius, p, sigma, use, energy_only=False):
+    """FF_SASA_LCPO over the neighbour list (ptr, data as the reference
+    packs it): (per-atom SASA in A^2, SASAderiv [n, 3] in sigma units per A
+    (None on the energies path), epot_cav in sigma units, partners that did
+    not fit in the 80-entry overlap lists)."""
+    n = len(radius)
+    sasa = np.zeros(n)
+    deriv = None if energy_only else np.zeros((n, 3))
+    lost = ctypes.c_long(0)
+    sig = np.broadcast_to(np.asarray(sigma, dtype=np.float64), (n,))
+    e = lib().pdo_lcpo(n, _d(_cd(pos)), _i(_ci(ptr)), _i(_ci(data)), _d(_cd(radius)), _d(_cd(p)),
+                       _d(_cd(sig)), _b(np.ascontiguousarray(use, dtype=np.int8)), int(bool(energy_only)),
+                       _d(sasa), None if deriv is None else _d(deriv), ctypes.byref(lost))
+    return sasa, deriv, e, lost.value
+
+
+def lcpo_sigma_J(asp_kcal):
+    """The solvation parameter FF_SASA_LCPO::setup forms from GlobalASP
+    (kcal/mol/A^2 -> J/A^2 per molecule, lcpo.cpp:44-47)."""
+    c = constants()
+    return asp_kcal / c["Na"] / c["J2kcal"]
 
 
 def langevin_step(x, v, f, mass, normals, dt, gamma, temp, step, steps):

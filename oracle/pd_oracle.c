@@ -968,3 +968,180 @@ double pdo_langevin_step(int n, double *x, double *v, const double *f,
     }
   return ekin;
 }
+
+/* ------------------------------------------------------------------ LCPO */
+#define LCPO_NMAX 80 /* lcpo.h: Nlistmax */
+
+/* Maths::sphereSurfaceOverlap (maths/maths.cpp:103-106) */
+static double lcpo_overlap(double ri, double rj, double dij) {
+  return 2.0 * kPI * ri * (ri - dij / 2.0 - (ri * ri - rj * rj) / (2.0 * dij));
+}
+
+/* Distances as the reference's vector helpers form them: the free
+ * function sqrdist(a, b) takes a - b, the member a.sqrdist(b) takes b - a
+ * (maths/maths_vector.h:239-249, 352-368); the squares are the same. */
+static double lcpo_sqrdist(const double *a, const double *b) {
+  double g = a[0] - b[0], h = a[1] - b[1], j = a[2] - b[2];
+  return g * g + h * h + j * j;
+}
+
+double pdo_lcpo(int n, const double *pos, const int *ptr, const int *data,
+                const double *radius, const double *p, const double *sigma,
+                const int8_t *use, int energy_only, double *sasa,
+                double *deriv, long *truncated) {
+  const double TwoPI = 2.0 * kPI, FourPI = 4.0 * kPI;
+  int *cnt = calloc((size_t)n, sizeof(int));
+  int *nl = malloc(sizeof(int) * (size_t)n * LCPO_NMAX);
+  double *sv = malloc(sizeof(double) * (size_t)n * LCPO_NMAX);
+  long lost = 0;
+  /* overlap lists: pairs j < i of the neighbour list, i ascending, both
+   * ends appended while they have room (lcpo.cpp:434-485, 688-746) */
+  for (int i = 0; i < n; i++) {
+    if (!use[i]) continue;
+    const double *pi = pos + 3 * (size_t)i;
+    const double ri = radius[i];
+    for (int q = ptr[i]; q < ptr[i + 1]; q++) {
+      int j = data[q] & 0x00FFFFFF;
+      if (j >= i) break;
+      if (!use[j]) continue;
+      const double *pj = pos + 3 * (size_t)j;
+      const double rj = radius[j];
+      double sij, sji;
+      if (energy_only) {
+        double d = sqrt(lcpo_sqrdist(pi, pj));
+        if (!(d < ri + rj)) continue;
+        sij = lcpo_overlap(ri, rj, d);
+        if (sij < 0) sij = 0;
+        sji = lcpo_overlap(rj, ri, d);
+        if (sji < 0) sji = 0;
+      } else {
+        double d2 = lcpo_sqrdist(pi, pj);
+        if (!(d2 < (ri + rj) * (ri + rj))) continue;
+        double d = sqrt(d2);
+        double inv = 1 / d;
+        double h = 0.5 * (ri * ri - rj * rj) * inv;
+        sij = TwoPI * ri * (ri - d * 0.5 - h);
+        sji = TwoPI * rj * (rj - d * 0.5 + h);
+      }
+      if (cnt[i] < LCPO_NMAX) {
+        nl[(size_t)i * LCPO_NMAX + cnt[i]] = j;
+        sv[(size_t)i * LCPO_NMAX + cnt[i]] = sij;
+        cnt[i]++;
+      } else {
+        lost++;
+      }
+      if (cnt[j] < LCPO_NMAX) {
+        nl[(size_t)j * LCPO_NMAX + cnt[j]] = i;
+        sv[(size_t)j * LCPO_NMAX + cnt[j]] = sji;
+        cnt[j]++;
+      } else {
+        lost++;
+      }
+    }
+  }
+  double epot = 0;
+  for (int i = 0; i < n; i++) {
+    double *di = deriv ? deriv + 3 * (size_t)i : NULL;
+    if (!energy_only) di[0] = di[1] = di[2] = 0;
+    if (!use[i]) {
+      sasa[i] = 0;
+      continue;
+    }
+    const double *pi = pos + 3 * (size_t)i;
+    const double ri = radius[i];
+    const double Si = FourPI * ri * ri; /* sphereSurfaceArea, maths.cpp:97-100 */
+    double Si2 = 0, Si3 = 0, Si4 = 0;
+    double a2[3] = {0, 0, 0}, a4[3] = {0, 0, 0};
+    for (int e = 0; e < cnt[i]; e++) {
+      const int ja = nl[(size_t)i * LCPO_NMAX + e];
+      const double *pj = pos + 3 * (size_t)ja;
+      const double Si2_t = sv[(size_t)i * LCPO_NMAX + e];
+      double Si3_t = 0;
+      if (energy_only) {
+        /* lcpo.cpp:517-537 */
+        for (int k = 0; k < cnt[ja]; k++) {
+          const int ka = nl[(size_t)ja * LCPO_NMAX + k];
+          if (ka == i) continue;
+          if (ri + radius[ka] < sqrt(lcpo_sqrdist(pos + 3 * (size_t)ka, pi))) continue;
+          Si3_t += sv[(size_t)ja * LCPO_NMAX + k];
+        }
+      } else {
+        /* lcpo.cpp:772-901 */
+        const double rj = radius[ja];
+        double Si3ik_t = 0;
+        const double dij = sqrt(lcpo_sqrdist(pj, pi));
+        const double invij = 1 / dij;
+        double h = 0.5 * (ri * ri - rj * rj) * invij;
+        const double sji = TwoPI * rj * (rj - dij * 0.5 + h);
+        h *= 2.0 * invij;
+        double d2[3], d3[3] = {0, 0, 0}, d4[3], d3b[3] = {0, 0, 0}, d4b[3] = {0, 0, 0}, a2t[3], ddd[3];
+        double dAdd = kPI * rj * (-h - 1);
+        for (int c = 0; c < 3; c++) ddd[c] = -(pi[c] - pj[c]) / dij;
+        for (int c = 0; c < 3; c++) d2[c] = dAdd * ddd[c];
+        dAdd = kPI * ri * (h - 1);
+        for (int c = 0; c < 3; c++) a2t[c] = dAdd * ddd[c];
+        for (int k = 0; k < cnt[ja]; k++) {
+          const int ka = nl[(size_t)ja * LCPO_NMAX + k];
+          const double *pk = pos + 3 * (size_t)ka;
+          const double rk = radius[ka];
+          if (ka == i) continue;
+          double dik = lcpo_sqrdist(pk, pi);
+          if ((ri + rk) * (ri + rk) < dik) continue;
+          dik = sqrt(dik);
+          const double invik = 1 / dik;
+          const double hk = (ri * ri - rk * rk) * (invik * invik);
+          dAdd = kPI * ri * (hk - 1);
+          double dk[3];
+          for (int c = 0; c < 3; c++) dk[c] = -(pi[c] - pk[c]) * invik;
+          const double sjk = sv[(size_t)ja * LCPO_NMAX + k];
+          for (int c = 0; c < 3; c++) d3[c] += dAdd * dk[c];
+          dAdd = kPI * rk * (-hk - 1);
+          Si3ik_t += kPI * ri * (2 * ri - dik - dik * hk);
+          for (int c = 0; c < 3; c++) d3b[c] += dAdd * dk[c];
+          for (int c = 0; c < 3; c++) d4b[c] += sjk * dAdd * dk[c];
+          Si3_t += sjk;
+        }
+        for (int c = 0; c < 3; c++) d4[c] = sji * d3[c] + d4b[c];
+        for (int c = 0; c < 3; c++) d3[c] += d3b[c];
+        for (int c = 0; c < 3; c++) d4[c] += d2[c] * Si3ik_t;
+        const double *pj4 = p + 4 * (size_t)ja;
+        const double m2 = pj4[1] * sigma[ja], m3 = pj4[2] * sigma[ja], m4 = pj4[3] * sigma[ja];
+        for (int c = 0; c < 3; c++) {
+          d2[c] *= m2;
+          d3[c] *= m3;
+          d4[c] *= m4;
+        }
+        for (int c = 0; c < 3; c++) di[c] += d2[c];
+        for (int c = 0; c < 3; c++) di[c] += d3[c];
+        for (int c = 0; c < 3; c++) di[c] += d4[c];
+        for (int c = 0; c < 3; c++) a2[c] += a2t[c];
+        for (int c = 0; c < 3; c++) a4[c] += Si3_t * a2t[c];
+      }
+      Si4 += Si3_t * Si2_t;
+      Si3 += Si3_t;
+      Si2 += Si2_t;
+    }
+    const double *pi4 = p + 4 * (size_t)i;
+    double SAi = pi4[0] * Si + pi4[1] * Si2 + pi4[2] * Si3 + pi4[3] * Si4;
+    if (!energy_only) {
+      const double m2 = pi4[1] * sigma[i], m4 = pi4[3] * sigma[i];
+      for (int c = 0; c < 3; c++) {
+        a2[c] *= m2;
+        a4[c] *= m4;
+      }
+      for (int c = 0; c < 3; c++) di[c] += a2[c];
+      for (int c = 0; c < 3; c++) di[c] += a4[c];
+    }
+    if (SAi < 0) {
+      SAi = 0;
+      if (!energy_only) di[0] = di[1] = di[2] = 0;
+    }
+    sasa[i] = SAi;
+    epot += SAi * sigma[i];
+  }
+  free(cnt);
+  free(nl);
+  free(sv);
+  if (truncated) *truncated = lost;
+  return epot;
+}

@@ -112,6 +112,25 @@ double pdo_beeman_step(int n, double *x, double *v, const double *f,
                        double *fold, const double *mass, double dt, int step,
                        int steps);
 
+/* FF_SASA_LCPO (forcefields/lcpo.cpp) over the reference's neighbour list
+ * (ptr/data as pdo_nlist writes them: entries j | bo << 24, ascending j;
+ * only the j < i part of each row is read, lcpo.cpp:446-447).
+ * radius: LCPO type radius + 1.4 (A); p: P1..P4 per atom ([n][4]); sigma:
+ * the atomic solvation parameter per atom (J/A^2 as the reference forms it
+ * from GlobalASP, or any other unit: the results scale with it); use: 0
+ * for the atoms the component ignores.
+ * energy_only = 0: calcLCPOSasaForces(true) (lcpo.cpp:623-946): writes
+ *   sasa[n] (A^2) and deriv[3n] (SASAderiv: sigma units per A, the
+ *   force direction) and returns epot_cav = the sum of sasa * sigma.
+ * energy_only = 1: calcLCPOSasaEnergies(true) (lcpo.cpp:414-566): writes
+ *   sasa and returns epot_cav; deriv is not touched (may be NULL).
+ * The overlap lists hold at most 80 partners per atom (lcpo.h Nlistmax);
+ * *truncated (may be NULL) receives how many partners did not fit. */
+double pdo_lcpo(int n, const double *pos, const int *ptr, const int *data,
+                const double *radius, const double *p, const double *sigma,
+                const int8_t *use, int energy_only, double *sasa,
+                double *deriv, long *truncated);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,6 +33,8 @@
 #include "forcefields/ffparam.h"
 #include "forcefields/ffbonded.h"
 #include "forcefields/gbff.h"
+#include "forcefields/lcpo.h"
+#include "tools/stringtool.h"
 #include "workspace/workspace.h"
 #include "workspace/neighbourlist.h"
 #include "workspace/bondorder.h"
@@ -626,6 +628,136 @@ static void dump_minimise(Built &b, int algo, int nsteps, const std::string &pre
   put_d(pre + "result", r);
 }
 
+// FF_SASA_LCPO (forcefields/lcpo.cpp) on the built system.  The per-atom
+// parameters its setup() derives (lcpo.cpp:16-91) are formed here from the
+// parameter file's LCPOSASAPARAMETERS section with the same rule: the first
+// LCPOSASATYPE line with the atom's force-field type whose neighbour count
+// is -1 or the atom's number of non-hydrogen covalent partners; radius +
+// 1.4; hydrogens unused.  They are not read from the component (its arrays
+// are private); the oracle's energies and forces from them, compared with
+// the component's own, are what checks them.  Dumped: the parameters, the
+// component's forces and energies alone (calcForces at Step 0, calcEnergies),
+// then the whole forcefield with it (single point, velocity-Verlet steps,
+// steepest-descent steps) at UpdateSasa = update.
+struct LcpoType {
+  int attype, nb;
+  double r, p[4];
+};
+static void dump_lcpo(Built &b, const std::vector<double> &allpos, double asp, int update, int steps) {
+  WorkSpace &ws = *b.ws;
+  size_t n = ws.nAtoms();
+  Section sec;
+  if (b.ffps->getSection("LCPOSASAPARAMETERS", sec) != 0) {
+    fprintf(stderr, "no LCPOSASAPARAMETERS section\n");
+    exit(2);
+  }
+  std::vector<LcpoType> types;
+  for (size_t l = 0; l < sec.sectionline.size(); l++) {
+    std::string line = sec.sectionline[l];
+    removecomments(line, "#\12\15");
+    std::vector<std::string> tok = chopstr(line, " \12\15\t");
+    if (tok.size() < 8 || !cmpstring(tok[0], "LCPOSASATYPE")) continue;
+    LcpoType t;
+    t.attype = b.ffps->findAtomType(tok[1]);
+    t.nb = atoi(tok[2].c_str());
+    t.r = strtod(tok[3].c_str(), NULL);
+    for (int k = 0; k < 4; k++) t.p[k] = strtod(tok[4 + k].c_str(), NULL);
+    types.push_back(t);
+  }
+  std::vector<double> rad(n), p4(4 * n);
+  std::vector<int8_t> use(n);
+  for (size_t i = 0; i < n; i++) {
+    const Particle &a = ws.atom[i];
+    int heavy = 0;
+    for (size_t k = 0; k < a.cov12atom.size(); k++)
+      if (ws.atom[a.cov12atom[k].i].Z != 1) heavy++;
+    size_t t = 0;
+    for (; t < types.size(); t++)
+      if (types[t].attype == a.FFType && (types[t].nb < 0 || types[t].nb == heavy)) break;
+    if (t == types.size()) {
+      fprintf(stderr, "no LCPO type for atom %zu\n", i);
+      exit(2);
+    }
+    rad[i] = types[t].r + 1.4;
+    for (int k = 0; k < 4; k++) p4[4 * i + k] = types[t].p[k];
+    use[i] = a.Z == 1 ? 0 : 1;
+  }
+  put_d("lcpo_radius", rad);
+  put_d("lcpo_p", p4, shp(n, 4));
+  put_b("lcpo_use", use);
+  std::vector<double> cfg;
+  cfg.push_back(asp);
+  cfg.push_back(update);
+  put_d("lcpo_cfg", cfg);
+
+  FF_SASA_LCPO *sasa = new FF_SASA_LCPO(ws);
+  sasa->GlobalASP = asp;
+  sasa->UpdateSasa = update;
+  Forcefield *alone = new Forcefield(ws);
+  alone->add(*sasa);
+  set_pos(ws, allpos);
+  alone->ensuresetup(ws);
+  ws.Step = 0;
+  ws.nlist().calcNewList();
+  alone->calcForces();
+  std::vector<double> e = ene_vec(ws.ene);
+  e.push_back(ws.ene.epot_surf);
+  put_d("lcpo_f", get_f(ws), shp(n, 3));
+  put_d("lcpo_ene", e);
+  ws.zeroForces();
+  alone->calcEnergies();
+  e = ene_vec(ws.ene);
+  e.push_back(ws.ene.epot_surf);
+  put_d("lcpo_ene_energypath", e);
+
+  // an artificially dense packing (the coordinates shrunk to 0.35 about
+  // their centroid): atoms with more than 80 overlapping partners, whose
+  // overlap lists the reference truncates (lcpo.cpp:465-482)
+  {
+    std::vector<double> dp(allpos);
+    double c[3] = {0, 0, 0};
+    for (size_t i = 0; i < n; i++)
+      for (int k = 0; k < 3; k++) c[k] += dp[3 * i + k];
+    for (int k = 0; k < 3; k++) c[k] /= (double)n;
+    for (size_t i = 0; i < n; i++)
+      for (int k = 0; k < 3; k++) dp[3 * i + k] = c[k] + 0.35 * (dp[3 * i + k] - c[k]);
+    set_pos(ws, dp);
+    ws.Step = 0;
+    ws.nlist().calcNewList();
+    dump_nlist(b, "lcpo_dense_nl");
+    alone->calcForces();
+    e = ene_vec(ws.ene);
+    e.push_back(ws.ene.epot_surf);
+    put_d("lcpo_dense_pos", dp, shp(n, 3));
+    put_d("lcpo_dense_f", get_f(ws), shp(n, 3));
+    put_d("lcpo_dense_ene", e);
+    ws.zeroForces();
+    alone->calcEnergies();
+    e = ene_vec(ws.ene);
+    e.push_back(ws.ene.epot_surf);
+    put_d("lcpo_dense_ene_energypath", e);
+  }
+
+  b.ff->add(*sasa);
+  b.ff->ensuresetup(ws);
+  set_pos(ws, allpos);
+  ws.Step = 0;
+  ws.nlist().calcNewList();
+  b.ff->calcForces();
+  e = ene_vec(ws.ene);
+  e.push_back(ws.ene.epot_surf);
+  put_d("lcpo_f_total", get_f(ws), shp(n, 3));
+  put_d("lcpo_ene_total", e);
+  if (steps > 0) {
+    set_pos(ws, allpos);
+    dump_md_steps(b, MolecularDynamics::VelocityVerlet, steps, 1e12, "lcpo_mdvv_");
+    set_pos(ws, allpos);
+    ws.Step = 0;
+    dump_minimise(b, Minimisation::SteepestDescent, steps, "lcpo_minsd_");
+  }
+  set_pos(ws, allpos);
+}
+
 static double now() {
   struct timeval tv;
   gettimeofday(&tv, NULL);
@@ -637,6 +769,7 @@ static void usage() {
           "ref_driver build --out DIR --nres N[,N..] --seed S [--cutoff R] "
           "[--inner R] [--grid NX,SPACING] [--premin STEPS] [--param F] "
           "[--md STEPS] [--min STEPS] [--slowmode] [--trials K --trial-sigma DEG]\n"
+          "          [--lcpo-asp KCAL_PER_A2 --lcpo UPDATESASA[,STEPS]]\n"
           "ref_driver time --in DIR --cutoff R --inner R --steps K "
           "[--warmup W] [--nlist-every M] [--param F]\n");
   exit(1);
@@ -661,6 +794,8 @@ int main(int argc, char **argv) {
   uint64_t seed = 0;
   int premin = 500, mdsteps = 0, minsteps = 0, steps = 10, warmup = 1, ntrials = 0;
   double trial_sigma_deg = 15.0;
+  double lcpo_asp = 0.0;
+  int lcpo_update = 5, lcpo_steps = 0;
   int nlist_every = 10;
   int gridx = 0;
   double spacing = 25.0;
@@ -685,6 +820,12 @@ int main(int argc, char **argv) {
     else if (k == "--nlist-every") { nlist_every = atoi(v); a++; }
     else if (k == "--param") { st.param = v; a++; }
     else if (k == "--slowmode") { st.fastmode = false; }
+    else if (k == "--lcpo") {
+      std::vector<int> g = parse_ints(v);
+      lcpo_update = g[0];
+      if (g.size() > 1) lcpo_steps = g[1];
+      a++;
+    } else if (k == "--lcpo-asp") { lcpo_asp = atof(v); a++; }
     else if (k == "--grid") {
       std::vector<int> g = parse_ints(v);
       gridx = g[0];
@@ -757,6 +898,7 @@ int main(int argc, char **argv) {
       set_pos(*b.ws, allpos);
       dump_md_steps(b, MolecularDynamics::Beeman, mdsteps, 1e12, "mdbm_");
     }
+    if (lcpo_asp != 0.0) dump_lcpo(b, allpos, lcpo_asp, lcpo_update, lcpo_steps);
     printf("built %zu atoms\n", b.ws->nAtoms());
     return 0;
   }

@@ -19,6 +19,10 @@ with 500 steepest-descent steps at Rc 12 A unless noted):
   two_chain_s4  two 12-residue chains 12 A apart, Rc 10 (inter-chain pairs),
                 3 phi/psi trial conformations
   c1_pep64_s0   the 64-residue, seed-0 chain of the small plain-MD workload, Rc 12
+  lcpo_pep24_s5 24 residues, Rc 12, with the LCPO surface-area term (FF_SASA_LCPO,
+                GlobalASP 0.005 kcal/mol/A^2, UpdateSasa 5): its per-atom parameters,
+                its forces and energies alone and with {FF_Bonded, GB}, and 12
+                velocity-Verlet and 12 steepest-descent steps of the whole forcefield
   c2_16x80_s2   16 x 80-residue chains on a 4x4 grid 25 A apart (~20.6k atoms),
                 Rc 16: inputs plus reference forces, Born radii and energies
                 (no neighbour list: too large to store)
@@ -43,6 +47,8 @@ SYSTEMS = {
     "pep30_s3_rc16": dict(nres=[30], seed=3, cutoff=16, premin=500),
     "two_chain_s4": dict(nres=[12, 12], seed=4, cutoff=10, premin=500, grid=(2, 12), trials=3),
     "c1_pep64_s0": dict(nres=[64], seed=0, cutoff=12, premin=500),
+    "lcpo_pep24_s5": dict(nres=[24], seed=5, cutoff=12, premin=500, lcpo=(0.005, 5, 12),
+                          drop=("lcpo_mdvv_normals",)),
     "c2_16x80_s2": dict(nres=[80] * 16, seed=2, cutoff=16, premin=500, grid=(4, 25), drop_nl=True),
 }
 
@@ -65,6 +71,9 @@ def build(name, spec, keep_dir=None):
         cmd += ["--min", str(spec["min"])]
     if spec.get("trials"):
         cmd += ["--trials", str(spec["trials"]), "--trial-sigma", "15"]
+    if spec.get("lcpo"):
+        asp, update, steps = spec["lcpo"]
+        cmd += ["--lcpo-asp", repr(asp), "--lcpo", "%d,%d" % (update, steps)]
     env = dict(os.environ, PD_PARAM_PATH=PARAM)
     subprocess.check_call(cmd, env=env, stdout=subprocess.DEVNULL)
     arrays = {}
@@ -86,6 +95,8 @@ def build(name, spec, keep_dir=None):
         for k in list(arrays):
             if k.startswith("nl_") or k in ("f_energypath", "ene_energypath", "atom_epot"):
                 del arrays[k]
+    for k in spec.get("drop", ()):
+        del arrays[k]
     arrays["meta_json"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
     if keep_dir is None:

@@ -174,3 +174,63 @@ def test_trial_forces_match_oracle(name):
         f, e, _ = S.calc_forces(x, ptr, data)
         assert rel_rms(f, arrays["trial_f"][t]) < 1e-12
         assert e["epot"] == pytest.approx(arrays["trial_ene"][t][0], rel=1e-12, abs=1e-30)
+
+
+# ------------------------------------------------------------------ LCPO
+LCPO = [n for n in SMALL if n.startswith("lcpo_")]
+
+
+@pytest.mark.parametrize("name", LCPO)
+@pytest.mark.parametrize("dense", [False, True])
+def test_lcpo_bit_exact(name, dense):
+    """FF_SASA_LCPO alone: calcForces at Step 0 (forces path) and
+    calcEnergies (energies path), on the built chain and on the dense
+    packing whose overlap lists the reference truncates at 80 partners."""
+    a, _ = load_fixture(name)
+    c = O.constants()
+    sig = O.lcpo_sigma_J(float(a["lcpo_cfg"][0]))
+    pre = "lcpo_dense_" if dense else "lcpo_"
+    pos = a["lcpo_dense_pos"] if dense else a["pos"]
+    ptr, data = (a["lcpo_dense_nl_ptr"], a["lcpo_dense_nl_data"]) if dense else (a["nl_ptr"], a["nl_data"])
+    sasa, deriv, e, lost = O.lcpo(pos, ptr, data, a["lcpo_radius"], a["lcpo_p"], sig, a["lcpo_use"])
+    assert (lost > 0) == dense
+    assert np.array_equal(deriv * (1 / c["Angstrom"]), a[pre + "f"])
+    assert e == a[pre + "ene"][10] and e == a[pre + "ene"][0]  # epot_surf, epot
+    assert np.all(sasa[a["lcpo_use"] == 0] == 0)
+    s2, _, e2, _ = O.lcpo(pos, ptr, data, a["lcpo_radius"], a["lcpo_p"], sig, a["lcpo_use"], energy_only=True)
+    assert e2 == a[pre + "ene_energypath"][10]
+
+
+@pytest.mark.parametrize("name", LCPO)
+def test_lcpo_in_the_forcefield_and_update_cadence(name):
+    """{FF_Bonded, GB, LCPO}: the single point, then each velocity-Verlet
+    step's forces from the reference's own positions, with the surface
+    term recomputed only when Step % UpdateSasa == 0 and its forces of that
+    step reused in between (lcpo.cpp:176-190)."""
+    S, a, _ = _system(name)
+    c = O.constants()
+    sig = O.lcpo_sigma_J(float(a["lcpo_cfg"][0]))
+    update = int(a["lcpo_cfg"][1])
+    to_N = 1 / c["Angstrom"]
+
+    def forces(pos, step, held):
+        ptr, data = S.nlist(pos)
+        f, e, _ = S.calc_forces(pos, ptr, data)
+        if step % update == 0:
+            sasa, deriv, esurf, _ = O.lcpo(pos, ptr, data, a["lcpo_radius"], a["lcpo_p"], sig, a["lcpo_use"])
+            held[:] = [deriv, esurf]
+        return f + held[0] * to_N, e["epot"] + held[1], held[1]
+
+    held = [None, None]
+    f, epot, esurf = forces(a["pos"], 0, held)
+    assert rel_rms(f, a["lcpo_f_total"]) <= 1e-14
+    assert esurf == a["lcpo_ene_total"][10]
+    assert epot == pytest.approx(a["lcpo_ene_total"][0], rel=1e-12)
+    x = a["lcpo_mdvv_x0"]
+    K = a["lcpo_mdvv_f"].shape[0]
+    assert K > update
+    for s in range(K):
+        f, epot, _ = forces(x, s, held)
+        assert rel_rms(f, a["lcpo_mdvv_f"][s]) <= 1e-13, s
+        assert epot == pytest.approx(a["lcpo_mdvv_epot"][s], rel=1e-12), s
+        x = a["lcpo_mdvv_x"][s]
