@@ -108,6 +108,29 @@ int pdgpu_system_set_bonded(pdgpu_ctx *ctx, int32_t sys, int32_t nbond,
  * LangevinOnHydrogens=false integrator (md.cpp:1048-1218).  Default: none. */
 int pdgpu_system_set_hydrogens(pdgpu_ctx *ctx, int32_t sys, const int8_t *is_h);
 
+/* FF_SASA_LCPO (forcefields/lcpo.h, lcpo.cpp): the LCPO surface-area term,
+ * epot_surf = sum over atoms of SASA_i * sigma_i.  Replaces the parameter
+ * assignment of FF_SASA_LCPO::setup (lcpo.cpp:16-111): per atom, radius =
+ * the LCPO type's radius + 1.4 (A), p1234 = P1..P4 ([natoms][4]), sigma =
+ * the atomic solvation parameter in kcal/mol/A^2 (GlobalASP for every atom
+ * on the reference's default path), use = 0 for hydrogens.  update_sasa =
+ * UpdateSasa: inside the MD and minimiser loops the term is recomputed when
+ * WorkSpace::Step % UpdateSasa == 0 and otherwise adds the forces of its
+ * last full evaluation (lcpo.cpp:176-190); <= 0 removes the term.  Set it
+ * on a single system before pdgpu_batch_create; batch members then share
+ * one UpdateSasa.  With the term, pdgpu_calc_forces, pdgpu_md_run,
+ * pdgpu_minimise_run and served jobs include it, and list rebuilds always
+ * produce the CSR list (the term reads it). */
+int pdgpu_sasa_lcpo_set(pdgpu_ctx *ctx, int32_t sys, const double *radius,
+                        const double *p1234, const double *sigma,
+                        const uint8_t *use, int32_t update_sasa);
+/* WorkSpace::Step for the calls outside the protocol loops
+ * (pdgpu_calc_forces, pdgpu_sasa_lcpo_forces with step < 0).  Starts at 0;
+ * pdgpu_md_run and pdgpu_minimise_run leave the last step they evaluated,
+ * as the reference's protocols leave WorkSpace::Step. */
+int pdgpu_set_step(pdgpu_ctx *ctx, int32_t sys, int32_t step);
+int pdgpu_get_step(pdgpu_ctx *ctx, int32_t sys, int32_t *step);
+
 /* ------------------------------------------------------------------ batches
  * Many independent systems of uneven size packed into one device pack
  * behind per-system offset tables, so that every kernel of an evaluation,
@@ -179,6 +202,7 @@ int pdgpu_get_atom_epot(pdgpu_ctx *ctx, int32_t sys, double *epot);
 #define PDGPU_ENE_EKIN 10
 #define PDGPU_ENE_ETOT 11
 #define PDGPU_ENE_GB_COMPONENT 12 /* FF_GeneralizedBorn::epot_pol of the energy path */
+#define PDGPU_ENE_SURF 15         /* epot_surf (FF_SASA_LCPO) */
 #define PDGPU_ENE_COUNT 16
 int pdgpu_get_energies(pdgpu_ctx *ctx, int32_t sys, double *ene, int32_t n);
 
@@ -249,8 +273,22 @@ int pdgpu_gb_energies(pdgpu_ctx *ctx, int32_t sys);
 int pdgpu_nonbonded_forces(pdgpu_ctx *ctx, int32_t sys);
 /* FF_Bonded::calcForces (ffbonded.cpp:809-823). */
 int pdgpu_bonded_forces(pdgpu_ctx *ctx, int32_t sys);
+/* FF_SASA_LCPO::calcForces (lcpo.cpp:176-190) at WorkSpace::Step = step
+ * (step < 0: the handle's, pdgpu_set_step): adds its forces and adds
+ * epot_cav to epot and epot_surf.  PDGPU_ERR_STATE if an atom has more than
+ * 256 overlap candidates (a packing far denser than any protein's). */
+int pdgpu_sasa_lcpo_forces(pdgpu_ctx *ctx, int32_t sys, int32_t step);
+/* FF_SASA_LCPO::calcEnergies (lcpo.cpp:168-173, calcLCPOSasaEnergies
+ * :414-566): areas and epot_surf from the energy path's overlap formula;
+ * no forces. */
+int pdgpu_sasa_lcpo_energies(pdgpu_ctx *ctx, int32_t sys);
+/* Per-atom SASA (A^2, SASA_Atom::SASA) of the last LCPO evaluation and
+ * SASAderiv of the last full one in kcal/mol/A ([natoms][3]; the reference
+ * holds it in J/A and adds it / Angstrom to the force); either may be NULL. */
+int pdgpu_sasa_lcpo_get(pdgpu_ctx *ctx, int32_t sys, double *sasa, double *deriv);
 /* Forcefield::calcForces (forcefield.cpp:220-247) for {FF_Bonded,
- * FF_GeneralizedBorn_Still}: zero, bonded, GB.  Reads nothing back. */
+ * FF_GeneralizedBorn_Still[, FF_SASA_LCPO]}: zero, bonded, GB, surface
+ * term at the handle's WorkSpace::Step.  Reads nothing back. */
 int pdgpu_calc_forces(pdgpu_ctx *ctx, int32_t sys);
 
 /* ------------------------------------------------------------------ protocols */

@@ -22,6 +22,9 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
          "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+# per-file flags: the LCPO term's FP64 arithmetic follows the reference's
+# rounding, so it is compiled without fused multiply-adds
+FILE_FLAGS = {"lcpo.cu": ["-fmad=false"]}
 
 
 def _stale(src, obj, deps):
@@ -40,7 +43,8 @@ def build(force=False, ptxas_verbose=False, quiet=False):
     for s in srcs:
         o = os.path.join(OBJ, os.path.basename(s)[:-3] + ".o")
         if force or _stale(s, o, deps):
-            cmd = [NVCC] + ARCH + FLAGS + (["-Xptxas", "-v"] if ptxas_verbose else []) + ["-c", s, "-o", o]
+            cmd = [NVCC] + ARCH + FLAGS + FILE_FLAGS.get(os.path.basename(s), []) + \
+                (["-Xptxas", "-v"] if ptxas_verbose else []) + ["-c", s, "-o", o]
             jobs.append((s, cmd))
 
     def run(job):

@@ -524,6 +524,67 @@ int pdgpu_system_set_hydrogens(pdgpu_ctx *c, int32_t sys, const int8_t *is_h) {
   return sync_check(c, "set_hydrogens");
 }
 
+// FF_SASA_LCPO::setup's per-atom parameters (lcpo.cpp:16-111), formed by
+// the caller; update_sasa <= 0 removes the term.
+int pdgpu_sasa_lcpo_set(pdgpu_ctx *c, int32_t sys, const double *radius, const double *p1234,
+                        const double *sigma, const uint8_t *use, int32_t update_sasa) {
+  CHECK_CTX(c);
+  GET_SYS_HOST(e, c, sys);
+  int r = need_single(e, "pdgpu_sasa_lcpo_set");
+  if (r) return r;
+  SystemHost &h = *e->host;
+  const size_t n = (size_t)h.natoms;
+  if (update_sasa > 0) {
+    if (!radius || !p1234 || !sigma || !use) {
+      set_error("pdgpu_sasa_lcpo_set: NULL parameter array");
+      return PDGPU_ERR_ARG;
+    }
+    for (size_t i = 0; i < n; i++)
+      if (use[i] && !(radius[i] > 0.0)) {
+        set_error("pdgpu_sasa_lcpo_set: an atom in use has a radius <= 0");
+        return PDGPU_ERR_ARG;
+      }
+    h.lcpo_r.assign(radius, radius + n);
+    h.lcpo_p.assign(p1234, p1234 + 4 * n);
+    h.lcpo_sigma.assign(sigma, sigma + n);
+    h.lcpo_use.assign(use, use + n);
+    h.lcpo_update = update_sasa;
+  } else {
+    h.lcpo_update = 0;
+    h.lcpo_r.clear();
+    h.lcpo_p.clear();
+    h.lcpo_sigma.clear();
+    h.lcpo_use.clear();
+  }
+  if (!e->pack) return PDGPU_OK;
+  e->drop_graph();
+  // the term reads the list rows: the calls that run it build them first
+  // when the last rebuild made only the tiles
+  return pack_upload_lcpo(e->pack.get(), e->member_ptrs());
+}
+
+int pdgpu_set_step(pdgpu_ctx *c, int32_t sys, int32_t step) {
+  CHECK_CTX(c);
+  GET_SYS_HOST(e, c, sys);
+  if (step < 0) {
+    set_error("pdgpu_set_step: step < 0");
+    return PDGPU_ERR_ARG;
+  }
+  e->ws_step = step;
+  return PDGPU_OK;
+}
+
+int pdgpu_get_step(pdgpu_ctx *c, int32_t sys, int32_t *step) {
+  CHECK_CTX(c);
+  GET_SYS_HOST(e, c, sys);
+  if (!step) {
+    set_error("step is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  *step = e->ws_step;
+  return PDGPU_OK;
+}
+
 int pdgpu_system_set_torsions(pdgpu_ctx *c, int32_t sys, int32_t nrot, const int32_t *axis) {
   CHECK_CTX(c);
   GET_SYS_HOST(e, c, sys);
@@ -836,8 +897,11 @@ static int nlist_enqueue(pdgpu_ctx *c, SysEntry *e, bool size_check) {
 // that rebuild (saved by the search), so it is the list the rebuild would
 // have made.  Packs on the row passes, or with a system too large for the
 // search, rebuild the list (and from it the tiles).
+// the LCPO term reads the CSR rows, so a pack with it builds them at
+// every rebuild
 static bool tile_search_ok(const Pack &P) {
-  return P.v.tile_mode && P.v.tile_meta && P.v.n_sc > 0 && P.v.max_sys_atoms <= kTileSearchMaxAtoms;
+  return P.v.tile_mode && P.v.tile_meta && P.v.n_sc > 0 && P.v.max_sys_atoms <= kTileSearchMaxAtoms &&
+         P.v.lc.update <= 0;
 }
 static void rebuild_enqueue(Pack &P, cudaStream_t st) {
   if (tile_search_ok(P)) {
@@ -944,7 +1008,7 @@ static int ensure_tuned(pdgpu_ctx *c, Pack &P);
 // times the row passes too).
 static int ready_pairs(pdgpu_ctx *c, SysEntry *e) {
   Pack &P = *e->pack;
-  int r = need_csr_if(c, e, !P.tuned || !P.v.tile_mode);
+  int r = need_csr_if(c, e, !P.tuned || !P.v.tile_mode || P.v.lc.update > 0);
   if (r) return r;
   return ensure_tuned(c, P);
 }
@@ -1150,35 +1214,119 @@ int pdgpu_bonded_forces(pdgpu_ctx *c, int32_t sys) {
 // Born-radius kernel zeroes forces and record first; one energy reduction.
 // extra_mode adds EM_KINETIC / EM_RECORD inside an MD step.
 }  // extern "C"
-// Forcefield::calcForces for {FF_Bonded, GB}: the bonded terms (zeroing
-// their accumulators first) run on the pack's second stream beside the
-// three pair passes; the stream joins before the energies are read.
+// The LCPO component alone: FF_SASA_LCPO::calcForces at WorkSpace::Step =
+// step (lcpo.cpp:176-190) adds its forces and epot_surf; calcEnergies
+// (lcpo.cpp:168-173) recomputes the areas and epot_surf only.
+static int lcpo_ready(pdgpu_ctx *c, SysEntry *e) {
+  Pack &P = *e->pack;
+  if (P.v.lc.update <= 0) {
+    set_error("this system has no LCPO term (pdgpu_sasa_lcpo_set)");
+    return PDGPU_ERR_STATE;
+  }
+  int r = need_csr(c, e);
+  if (r) return r;
+  PDGPU_CUDA(cudaMemsetAsync(P.v.flags + F_LCPO_CAND, 0, sizeof(int), c->st));
+  return PDGPU_OK;
+}
+static int lcpo_done(pdgpu_ctx *c, SysEntry *e, const char *what) {
+  int flag = 0;
+  PDGPU_CUDA(cudaMemcpyAsync(&flag, e->pack->v.flags + F_LCPO_CAND, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  int r = sync_check(c, what);
+  if (r) return r;
+  if (flag) {
+    set_error(kLcpoCandMsg);
+    return PDGPU_ERR_STATE;
+  }
+  return PDGPU_OK;
+}
+extern "C" {
+int pdgpu_sasa_lcpo_forces(pdgpu_ctx *c, int32_t sys, int32_t step) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  int r = lcpo_ready(c, e);
+  if (r) return r;
+  StepSrc src;
+  src.imm = step < 0 ? e->ws_step : step;
+  launch_lcpo(e->pack->v, c->st, src, false);
+  launch_energy(e->pack->v, c->st, EM_SURF);
+  return lcpo_done(c, e, "sasa_lcpo_forces");
+}
+
+int pdgpu_sasa_lcpo_energies(pdgpu_ctx *c, int32_t sys) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  int r = lcpo_ready(c, e);
+  if (r) return r;
+  launch_lcpo(e->pack->v, c->st, StepSrc(), true);
+  launch_energy(e->pack->v, c->st, EM_SURF);
+  return lcpo_done(c, e, "sasa_lcpo_energies");
+}
+
+int pdgpu_sasa_lcpo_get(pdgpu_ctx *c, int32_t sys, double *sasa, double *deriv) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  const LcpoView &lc = e->pack->v.lc;
+  if (lc.update <= 0) {
+    set_error("this system has no LCPO term (pdgpu_sasa_lcpo_set)");
+    return PDGPU_ERR_STATE;
+  }
+  const size_t N = (size_t)e->pack->v.n_atoms;
+  if (sasa) PDGPU_CUDA(cudaMemcpyAsync(sasa, lc.sasa, sizeof(double) * N, cudaMemcpyDeviceToHost, c->st));
+  std::vector<double> d;
+  if (deriv) {
+    d.resize(3 * N);
+    PDGPU_CUDA(cudaMemcpyAsync(d.data(), lc.deriv, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, c->st));
+  }
+  int r = sync_check(c, "sasa_lcpo_get");
+  if (r) return r;
+  for (size_t i = 0; i < N && deriv; i++) {
+    deriv[3 * i] = d[i];
+    deriv[3 * i + 1] = d[N + i];
+    deriv[3 * i + 2] = d[2 * N + i];
+  }
+  return PDGPU_OK;
+}
+}  // extern "C"
+
+// Forcefield::calcForces for {FF_Bonded, GB[, FF_SASA_LCPO]}: the bonded
+// terms and the surface term (zeroing their accumulators first) run on the
+// pack's second stream beside the three pair passes; the stream joins
+// before the energies are read.  The surface term reads the step counter
+// after the previous step's energy record, which runs on that stream too.
 void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce) {
+  StepSrc step;
+  step.imm = e->ws_step;
+  calc_forces_enqueue(st, e, reduce, step);
+}
+void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce, StepSrc step) {
   Pack &P = *e->pack;
   const bool bonded = has_bonded(P);
-  if (bonded) {
+  const bool surf = P.v.lc.update > 0;
+  const bool side = bonded || surf;
+  if (side) {
     const size_t bytes = sizeof(long long) * (size_t)P.v.n_atoms;
     cudaEventRecord(P.fork, st);
     cudaStreamWaitEvent(P.side, P.fork, 0);
     cudaMemsetAsync(P.v.fx, 0, bytes, P.side);
     cudaMemsetAsync(P.v.fy, 0, bytes, P.side);
     cudaMemsetAsync(P.v.fz, 0, bytes, P.side);
-    launch_bonded_terms(P.v, P.side);
+    if (bonded) launch_bonded_terms(P.v, P.side);
+    if (surf) launch_lcpo(P.v, P.side, step, false);
     cudaEventRecord(P.join, P.side);
   }
   // with an MD step's energy record still running beside, the record is
   // left to it (it forms the record from zero) and the fused pass, which
   // writes what the record reads, waits for it
   const bool pending = P.energy_pending;
-  launch_born_radii(P.v, st, ZF_PAIRS | (bonded ? 0 : ZF_BONDED) | (pending ? 0 : ZF_RECORD));
+  launch_born_radii(P.v, st, ZF_PAIRS | (side ? 0 : ZF_BONDED) | (pending ? 0 : ZF_RECORD));
   if (pending) {
     cudaStreamWaitEvent(st, P.ene_done, 0);
     P.energy_pending = false;
   }
   launch_gb_pair(P.v, st);
   launch_gb_chain(P.v, st);
-  if (bonded) cudaStreamWaitEvent(st, P.join, 0);
-  if (reduce) launch_energy(P.v, st, EM_PAIR_GB | (bonded ? EM_BONDED : 0));
+  if (side) cudaStreamWaitEvent(st, P.join, 0);
+  if (reduce) launch_energy(P.v, st, EM_PAIR_GB | (bonded ? EM_BONDED : 0) | (surf ? EM_SURF : 0));
 }
 extern "C" {
 
@@ -1297,7 +1445,9 @@ int pdgpu_md_init_velocities(pdgpu_ctx *c, int32_t sys, double temperature, uint
 }  // extern "C"
 void pdgpu::md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k) {
   Pack &P = *e->pack;
-  calc_forces_enqueue(st, e, false);
+  StepSrc step;
+  step.p = e->step_dev;  // MolecularDynamics::run_core sets WorkSpace::Step = Step (md.cpp:214)
+  calc_forces_enqueue(st, e, false, step);
   launch_md_step_impl(P.v, st, k, nullptr, e->step_dev, P.is_h, e->seeds, e->traj_dev, e->traj_every,
                       e->traj_dev_cap);
   // the step's energy record on the second stream, beside the next step's
@@ -1305,8 +1455,9 @@ void pdgpu::md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k) {
   cudaEventRecord(P.fork2, st);
   cudaStreamWaitEvent(P.side, P.fork2, 0);
   launch_energy(P.v, P.side,
-                EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0) | EM_KINETIC | EM_RECORD | EM_ASSIGN, e->hist,
-                e->step_dev);
+                EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0) | (P.v.lc.update > 0 ? EM_SURF : 0) | EM_KINETIC |
+                    EM_RECORD | EM_ASSIGN,
+                e->hist, e->step_dev);
   cudaEventRecord(P.ene_done, P.side);
   P.energy_pending = true;
 }
@@ -1514,6 +1665,10 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
       PDGPU_CUDA(cudaMemcpyAsync(flags, v.flags, sizeof flags, cudaMemcpyDeviceToHost, c->st));
       r = sync_check(c, "md block");
       if (r) return r;
+      if (flags[F_LCPO_CAND]) {
+        set_error(kLcpoCandMsg);
+        return PDGPU_ERR_STATE;
+      }
       if (flags[F_NL_OVERFLOW]) {
         // state untouched since the block start: grow the list and re-run
         r = nlist_enqueue(c, e, true);
@@ -1539,6 +1694,7 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
   cudaEventRecord(P.ev1, c->st);
   r = sync_check(c, "md_run");
   if (r) return r;
+  if (steps > 0) e->ws_step = first_step + steps - 1;  // WorkSpace::Step as run_core leaves it
   float ms = 0;
   cudaEventElapsedTime(&ms, P.ev0, P.ev1);
   P.last_run_ms = ms;
@@ -1604,13 +1760,17 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
     for (int q = 0; q < chunk; q++) {
       int cnt = counter0 + iter + q;
       if (every > 0 && (cnt % every) == 0) rebuild_enqueue(P, c->st);
-      calc_forces_enqueue(c->st, e, true);
+      calc_forces_enqueue(c->st, e, true, min_step_src(e->min_state, false));
       launch_min_step(v, c->st, e->min_state, p->Algorithm, slope, strict, p->StepSize, steps);
     }
     int flags[F_COUNT];
     PDGPU_CUDA(cudaMemcpyAsync(flags, v.flags, sizeof flags, cudaMemcpyDeviceToHost, c->st));
     r = sync_check(c, "minimise");
     if (r) return r;
+    if (flags[F_LCPO_CAND]) {
+      set_error(kLcpoCandMsg);
+      return PDGPU_ERR_STATE;
+    }
     PDGPU_CUDA(cudaMemcpy(hs.data(), e->min_state, hs.size(), cudaMemcpyDeviceToHost));
     int advanced = 0, nan_count = 0;
     for (int s = 0; s < S; s++) {
@@ -1646,10 +1806,12 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
   P.nlist_counter = counter0 + iter;
   // cur = old; recompute the energies (minimise.cpp:172-176)
   launch_min_finish(v, c->st);
-  calc_forces_enqueue(c->st, e, true);
+  calc_forces_enqueue(c->st, e, true, min_step_src(e->min_state, true));
   cudaEventRecord(P.ev1, c->st);
   r = sync_check(c, "minimise finish");
   if (r) return r;
+  PDGPU_CUDA(cudaMemcpy(hs.data(), e->min_state, hs.size(), cudaMemcpyDeviceToHost));
+  e->ws_step = min_state_last(hs.data(), 0);
   float ms = 0;
   cudaEventElapsedTime(&ms, P.ev0, P.ev1);
   P.last_run_ms = ms;

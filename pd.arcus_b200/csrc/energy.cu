@@ -16,10 +16,11 @@
 namespace pdgpu {
 
 constexpr int kChunk = kReduceChunk;
-constexpr int kEnergyThreads = 352;  // eleven warps: one per partial slot in the final sum, one for the record
+constexpr int kEnergyThreads = 384;  // twelve warps: one per partial slot in the final sum, one for the record
 // partial slots
-enum { P_VDW = 0, P_ELEC, P_POL, P_SELF, P_NBVIR, P_KIN, P_BOND, P_BVIR, P_ANGLE, P_DIH, P_COUNT };
+enum { P_VDW = 0, P_ELEC, P_POL, P_SELF, P_NBVIR, P_KIN, P_BOND, P_BVIR, P_ANGLE, P_DIH, P_SURF, P_COUNT };
 static_assert(kEnergyThreads / 32 >= P_COUNT, "one warp per partial slot");
+static_assert(P_COUNT <= kPartSlots, "partials fit the reduction buffer");
 
 // hist: [step][sys][3] (epot, ekin, etot); step_dev[0] current step,
 // step_dev[1] first step of the run, step_dev[2] finished-system counter.
@@ -41,7 +42,7 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode,
 #pragma unroll
   for (int k = 0; k < P_COUNT; k++) acc[k] = 0.0;
   int a0 = v.atom_off[s] + c * kChunk, a1 = min(a0 + kChunk, v.atom_off[s + 1]);
-  bool atoms = mode & (EM_PAIR_GB | EM_PAIR_NB | EM_BORN_ENERGY | EM_KINETIC);
+  bool atoms = mode & (EM_PAIR_GB | EM_PAIR_NB | EM_BORN_ENERGY | EM_KINETIC | EM_SURF);
   if (atoms)
     for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
       if (mode & (EM_PAIR_GB | EM_PAIR_NB)) {
@@ -53,6 +54,7 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode,
         acc[P_SELF] += v.e_atom[(size_t)AE_POL_SELF * N + i];
       }
       if (mode & EM_PAIR_NB) acc[P_NBVIR] += v.e_atom[(size_t)AE_VIR * N + i];
+      if (mode & EM_SURF) acc[P_SURF] += v.e_atom[(size_t)AE_SURF * N + i];
       if (MD) {
         const double ke = md_atom(v, md, nullptr, md_step, i);  // J
         v.e_atom[(size_t)AE_KIN * N + i] = ke;
@@ -150,6 +152,10 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode,
       R[E_TORSION] += tot[P_DIH];
       R[E_VIRIAL] += tot[P_BVIR];
       R[E_EPOT] += tot[P_BOND] + tot[P_ANGLE] + tot[P_DIH];
+    }
+    if (mode & EM_SURF) {  // FF_SASA_LCPO adds epot_cav to epot and epot_surf
+      R[E_SURF] += tot[P_SURF];
+      R[E_EPOT] += tot[P_SURF];
     }
     if (mode & EM_KINETIC) {
       R[E_EKIN] = tot[P_KIN] * J2kcalmol;

@@ -22,6 +22,10 @@ void launch_vel_init_impl(const PackView &v, cudaStream_t st, double temp, const
 void launch_min_step(const PackView &v, cudaStream_t st, void *ms, int algorithm, double slope_kcal,
                      double strict_kcal, double step_size, int nsteps);
 void launch_min_finish(const PackView &v, cudaStream_t st);
+// where the LCPO term reads each system's WorkSpace::Step inside a
+// minimisation: the step being evaluated, or (last) the last step taken
+StepSrc min_step_src(const void *ms, bool last);
+int min_state_last(const void *host_buf, int s);
 size_t min_state_size();
 void min_state_init(void *host_buf, int n);
 void min_state_read(const void *host_buf, int s, int *taken, int *nan, double *mult);
@@ -47,6 +51,7 @@ struct SysEntry {
     return m;
   }
   int *step_dev = nullptr;
+  int ws_step = 0;  // WorkSpace::Step outside the protocols (pdgpu_set_step; a protocol leaves its last step)
   double *hist = nullptr;
   int hist_cap = 0;
   // trajectory snapshots (pdgpu_md_set_trajectory): a device ring written by
@@ -117,9 +122,12 @@ namespace pdgpu {
 // step counters, enqueued on e->st (with `sync`, waited for).
 int entry_materialize(int device, SysEntry *e, bool sync = true);
 bool has_bonded(const Pack &P);
-// Forcefield::calcForces for {FF_Bonded, FF_GeneralizedBorn_Still}: zero,
-// Born radii, bonded, fused pair, chain rule; one energy reduction if reduce.
+// Forcefield::calcForces for {FF_Bonded, FF_GeneralizedBorn_Still} and the
+// LCPO term where the handle has it: zero, Born radii, bonded, fused pair,
+// chain rule, surface term; one energy reduction if reduce.  `step` is
+// where the surface term reads WorkSpace::Step (default: e->ws_step).
 void calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce);
+void calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce, StepSrc step);
 // one MD step: forces, integrator, energy record (+ step counter advance)
 void md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k);
 void md_steps_end(cudaStream_t st, SysEntry *e);

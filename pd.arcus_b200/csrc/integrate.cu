@@ -18,6 +18,7 @@
 // trajectory does not depend on which other systems share its launch.
 // Roofline: HBM-bound, 152 B/atom/step algorithmic traffic.
 #include <cuda_runtime.h>
+#include <cstddef>
 
 #include "mdatom.cuh"
 
@@ -76,6 +77,7 @@ struct MinState {
   double mult, old_energy, local_old, gamma, fmagold, fmagnew;
   int step, breakcount, done, action;  // action: 0 step, 1 restore-and-skip, 2 restore-then-step
   int taken, nan;
+  int last;  // the last step the loop evaluated (WorkSpace::Step when the loop ends)
 };
 
 // CG dot products: per (chunk, system) partials of fmagold = sum of.of and
@@ -149,6 +151,7 @@ __global__ void k_min_control(PackView v, MinState *ms, int algorithm, double sl
     m.action = -1;
     return;
   }
+  m.last = m.step;
   double epot = v.ene[(size_t)s * E_COUNT + E_EPOT];
   if (!(epot == epot)) {
     m.nan = 1;
@@ -332,6 +335,14 @@ void launch_min_finish(const PackView &v, cudaStream_t st) {
   if (v.n_atoms) PDGPU_LAUNCH(k_min_restore_best, (v.n_atoms + 255) / 256, 256, 0, st, v);
 }
 size_t min_state_size() { return sizeof(MinState); }
+int min_state_last(const void *host_buf, int s) { return ((const MinState *)host_buf)[s].last; }
+StepSrc min_step_src(const void *ms, bool last) {
+  static_assert(sizeof(MinState) % sizeof(int) == 0, "MinState is a whole number of ints");
+  StepSrc r;
+  r.p = (const int *)((const char *)ms + (last ? offsetof(MinState, last) : offsetof(MinState, step)));
+  r.stride = (int)(sizeof(MinState) / sizeof(int));
+  return r;
+}
 void min_state_init(void *host_buf, int n) {
   MinState *m = (MinState *)host_buf;
   for (int s = 0; s < n; s++) {

@@ -38,6 +38,8 @@ constexpr double kInvForceScale = 1.0 / 4294967296.0;
 constexpr double kJScale = 16777216.0;                // 2^24: tile pass forces and energies
 constexpr double kInvJScale = 1.0 / 16777216.0;
 constexpr int kReduceChunk = 256;                     // items per block of the per-system reductions
+constexpr int kPartSlots = 12;                        // reduction partials per (chunk, system)
+constexpr int kLcpoMax = 80;                          // overlap partners kept per atom (lcpo.h Nlistmax)
 constexpr double kBornScale = 1099511627776.0;        // 2^40
 constexpr double kInvBornScale = 1.0 / 1099511627776.0;
 
@@ -72,12 +74,12 @@ struct SysParams {
 
 enum EneSlot {
   E_EPOT = 0, E_VDW, E_ELEC, E_POL, E_POL_CROSS, E_POL_SELF, E_BOND, E_ANGLE,
-  E_TORSION, E_VIRIAL, E_EKIN, E_ETOT, E_GB_COMPONENT, E_COUNT = 16
+  E_TORSION, E_VIRIAL, E_EKIN, E_ETOT, E_GB_COMPONENT, E_SURF = 15, E_COUNT = 16
 };
 
 // Per-atom energy terms written by the pair kernels (kcal/mol), reduced per
 // system in a fixed order so every sum is bit-reproducible.
-enum AtomEne { AE_VDW = 0, AE_ELEC, AE_POL, AE_POL_SELF, AE_VIR, AE_KIN, AE_COUNT };
+enum AtomEne { AE_VDW = 0, AE_ELEC, AE_POL, AE_POL_SELF, AE_VIR, AE_KIN, AE_SURF, AE_COUNT };
 
 // What one energy reduction applies to the record (launch_energy).
 enum EnergyMode {
@@ -87,7 +89,34 @@ enum EnergyMode {
   EM_BONDED = 8,       // bond, angle, torsion, bond virial
   EM_KINETIC = 16,     // ekin, etot
   EM_RECORD = 32,      // history row + step counter advance (step loops)
-  EM_ASSIGN = 64       // form the record from zero (its slots were not zeroed before the step)
+  EM_ASSIGN = 64,      // form the record from zero (its slots were not zeroed before the step)
+  EM_SURF = 128        // LCPO surface term: epot_surf
+};
+
+// FF_SASA_LCPO (forcefields/lcpo.h, lcpo.cpp): per-atom parameters and the
+// state the reference keeps between full evaluations (the overlap lists,
+// each atom's SASA and SASAderiv).  A pack has the term when `update` > 0;
+// batch members without it have `use` 0 on every atom.
+struct LcpoView {
+  int update = 0;                      // UpdateSasa: full evaluation when Step % update == 0
+  const double *r = nullptr;           // [N] LCPO type radius + 1.4 (A)
+  const double4 *p = nullptr;          // [N] P1..P4
+  const double *sigma = nullptr;       // [N] atomic solvation parameter, kcal/mol/A^2
+  const unsigned char *use = nullptr;  // [N]
+  int *cnt = nullptr;                  // [N] partners kept (<= kLcpoMax)
+  int *idx = nullptr;                  // [N * kLcpoMax] partners, ascending
+  double *s = nullptr;                 // [N * kLcpoMax] overlap areas (A^2)
+  double *sasa = nullptr;              // [N] A^2 of the last evaluation
+  double *deriv = nullptr;             // [3N] SASAderiv (kcal/mol/A; x, y, z blocks) of the last full one
+};
+
+// Where an evaluation takes the reference's WorkSpace::Step from: a device
+// counter (the MD step, or each system's minimiser step at `stride` ints
+// per system), else `imm`.
+struct StepSrc {
+  const int *p = nullptr;
+  int stride = 0;
+  int imm = 0;
 };
 
 struct BondedTerms {
@@ -132,7 +161,7 @@ struct PackView {
   double *odx, *ody, *odz;
   double *e_atom;             // [AE_COUNT * N]
   double *ene;                // [S * E_COUNT] J-free kcal/mol accumulators
-  double *e_part;             // [S * e_chunks * 10] reduction partials
+  double *e_part;             // [S * e_chunks * kPartSlots] reduction partials
   int *e_done;                // [S] blocks of the energy reduction finished (reset by the last)
   int e_chunks;               // kReduceChunk-item chunks of the largest per-system range
   int lpa[3];                 // lanes per atom of the Born, fused-pair and chain kernels
@@ -185,9 +214,13 @@ struct PackView {
   int *flags;                 // [8] overflow / nan / etc.
   int *sys_flags;             // [S] SysFlag bits of the current evaluation
   BondedTerms bt;
+  LcpoView lc;
 };
 
-enum Flag { F_NL_OVERFLOW = 0, F_NAN = 1, F_CELL_CLAMP = 2, F_COUNT = 8 };
+// F_LCPO_CAND: an atom had more LCPO overlap candidates than a warp sorts
+enum Flag { F_NL_OVERFLOW = 0, F_NAN = 1, F_CELL_CLAMP = 2, F_LCPO_CAND = 3, F_COUNT = 8 };
+constexpr const char *kLcpoCandMsg =
+    "an atom has more than 256 LCPO overlap candidates (atoms closer than their radii + 2.8 A)";
 // per system: a tile pass met a non-finite pair term (its fixed-point sums
 // cannot carry it; the energy record turns it into a NaN potential energy)
 enum SysFlag { SF_NONFINITE = 1 };
@@ -214,6 +247,10 @@ struct SystemHost {
   std::vector<int> rot_axis, rot_last;
   std::vector<unsigned char> rot_start;
   std::vector<int8_t> is_h;
+  // FF_SASA_LCPO: update 0 = no surface term
+  int lcpo_update = 0;
+  std::vector<double> lcpo_r, lcpo_p, lcpo_sigma;  // lcpo_p: [N][4]
+  std::vector<unsigned char> lcpo_use;
 };
 
 // Owner of device memory for a Pack.
@@ -260,6 +297,8 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
 void pack_set_params(Pack *p, int s, const pdgpu_ff_params &prm);
 // allocate the cluster-pair tile store of a pack (once; enqueued on p->st)
 int pack_ensure_tiles(Pack *p);
+// FF_SASA_LCPO parameters of the members (again after they change)
+int pack_upload_lcpo(Pack *p, const std::vector<const SystemHost *> &systems);
 SysParams make_sys_params(const pdgpu_ff_params &p);
 
 // Host setup computations (restate the reference's setup code).
@@ -302,6 +341,10 @@ void launch_gb_chain_lpa(const PackView &v, cudaStream_t st, int lpa);
 void launch_born_energy(const PackView &v, cudaStream_t st);
 void launch_nonbonded(const PackView &v, cudaStream_t st, int elec_mode);
 void launch_bonded_terms(const PackView &v, cudaStream_t st);
+// FF_SASA_LCPO: overlap lists then areas and derivatives for the systems
+// whose step is due (energy_only: the calcEnergies path, always evaluated);
+// the other systems add their held derivatives to the forces.
+void launch_lcpo(const PackView &v, cudaStream_t st, StepSrc step, bool energy_only);
 // energies: per-atom / per-term energies into the per-system record
 // (mode = EnergyMode bits); hist/step_dev only with EM_RECORD
 void launch_energy(const PackView &v, cudaStream_t st, int mode, double *hist = nullptr,

@@ -1,0 +1,291 @@
+// FF_SASA_LCPO: the LCPO surface-area term (Weiser, Shenkin & Still,
+// J. Comp. Chem. 20:217, 1999) as forcefields/lcpo.cpp evaluates it, with
+// the reference's neighbour list, its 80-partner overlap lists and its
+// UpdateSasa cadence.
+//
+// Two launches per evaluation, one warp per atom:
+//  k_lcpo_list  the atom's overlap partners: the CSR row's atoms j with
+//               use[j] and |xi - xj| < ri + rj, ranked by index, the first
+//               80 kept with their overlap areas.  The reference appends
+//               partners in ascending index from both ends of every pair
+//               and stops at 80 (lcpo.cpp:434-485, 688-746), which keeps
+//               exactly these.
+//  k_lcpo_eval  the atom's area and SASAderiv (lcpo.cpp:751-941): lane e
+//               takes partner e and runs its inner loop over the partner's
+//               own list in the reference's order; the per-partner terms go
+//               to shared memory and twelve lanes then add them in partner
+//               order, one accumulator each, so every sum has the
+//               reference's rounding.  The file is compiled without fused
+//               multiply-adds (build.py), so the FP64 arithmetic matches
+//               the reference compiled without contraction bit for bit.
+// A system whose step is not due (Step % UpdateSasa != 0) adds the
+// derivative it holds from its last full evaluation (lcpo.cpp:641-659).
+// Units: areas A^2, sigma kcal/mol/A^2, SASAderiv kcal/mol/A.
+#include <cuda_runtime.h>
+
+#include "internal.cuh"
+
+namespace pdgpu {
+
+constexpr int kLcpoWarps = 4;    // atoms per block
+constexpr int kLcpoCand = 256;   // overlap candidates one warp ranks
+constexpr int kLcpoQ = 14;       // per-partner terms kept for the ordered sums
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kTwoPi = 2.0 * kPi;
+constexpr double kFourPi = 4.0 * kPi;
+
+__device__ __forceinline__ bool lcpo_due(const LcpoView &lc, const StepSrc &ss, int s) {
+  const int step = ss.p ? __ldcg(ss.p + (size_t)s * ss.stride) : ss.imm;
+  return step % lc.update == 0;
+}
+
+template <bool EO>
+__global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_list(PackView v, StepSrc ss) {
+  __shared__ int cand[kLcpoWarps][kLcpoCand];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kLcpoWarps + warp;
+  if (i >= v.n_atoms || v.flags[F_NL_OVERFLOW]) return;
+  const LcpoView &lc = v.lc;
+  if (!EO && !lcpo_due(lc, ss, v.sys_of[i])) return;
+  if (!lc.use[i]) {
+    if (lane == 0) lc.cnt[i] = 0;
+    return;
+  }
+  const double xi = v.x[i], yi = v.y[i], zi = v.z[i], ri = lc.r[i];
+  const long long r0 = v.row_start[i];
+  const int rn = v.row_cnt[i];
+  int n = 0;
+  for (int q0 = 0; q0 < rn; q0 += 32) {
+    const int q = q0 + lane;
+    bool hit = false;
+    int j = 0;
+    if (q < rn) {
+      j = (int)(v.nl[r0 + q] >> 3);
+      if (lc.use[j]) {
+        const double g = xi - v.x[j], h = yi - v.y[j], k = zi - v.z[j];
+        const double d2 = g * g + h * h + k * k;
+        const double rs = ri + lc.r[j];
+        hit = EO ? sqrt(d2) < rs : d2 < rs * rs;
+      }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, hit);
+    const int at = n + __popc(m & ((1u << lane) - 1u));
+    if (hit && at < kLcpoCand) cand[warp][at] = j;
+    n += __popc(m);
+  }
+  if (n > kLcpoCand) {
+    if (lane == 0) atomicExch(&v.flags[F_LCPO_CAND], 1);
+    n = kLcpoCand;
+  }
+  __syncwarp();
+  if (lane == 0) lc.cnt[i] = min(n, kLcpoMax);
+  const size_t base = (size_t)i * kLcpoMax;
+  for (int q = lane; q < n; q += 32) {
+    const int j = cand[warp][q];
+    int rank = 0;
+    for (int t = 0; t < n; t++) rank += cand[warp][t] < j;
+    if (rank >= kLcpoMax) continue;
+    const double g = xi - v.x[j], h = yi - v.y[j], k = zi - v.z[j];
+    const double d = sqrt(g * g + h * h + k * k);
+    const double rj = lc.r[j];
+    double s;
+    if (EO) {
+      // sphereSurfaceOverlap(ri, rj, d) (maths/maths.cpp:103-106), >= 0
+      s = kTwoPi * ri * (ri - d / 2.0 - (ri * ri - rj * rj) / (2.0 * d));
+      if (s < 0) s = 0;
+    } else {
+      // sij of lcpo.cpp:716-718; from the other end of the pair the same
+      // expression with the half-difference negated, which is this one
+      const double hd = 0.5 * (ri * ri - rj * rj) * (1 / d);
+      s = kTwoPi * ri * (ri - d * 0.5 - hd);
+    }
+    lc.idx[base + rank] = j;
+    lc.s[base + rank] = s;
+  }
+}
+
+__device__ __forceinline__ void lcpo_add_force(const PackView &v, int i, double fx, double fy, double fz) {
+  atomicAdd((unsigned long long *)&v.fx[i], (unsigned long long)__double2ll_rn(fx * kForceScale));
+  atomicAdd((unsigned long long *)&v.fy[i], (unsigned long long)__double2ll_rn(fy * kForceScale));
+  atomicAdd((unsigned long long *)&v.fz[i], (unsigned long long)__double2ll_rn(fz * kForceScale));
+}
+
+// per-partner terms in shared memory: 0-2 dSASA_2 (scaled by P2 sigma of
+// the partner), 3-5 dSASA_3, 6-8 dSASA_4, 9 Si2_t, 10 Si3_t, 11-13
+// dAijdc_2t; a row per term, padded so the twelve summing lanes read
+// different banks
+template <bool EO>
+__global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_eval(PackView v, StepSrc ss) {
+  __shared__ double T[kLcpoWarps][kLcpoQ][kLcpoMax + 1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kLcpoWarps + warp;
+  if (i >= v.n_atoms || v.flags[F_NL_OVERFLOW]) return;
+  const LcpoView &lc = v.lc;
+  const size_t N = (size_t)v.n_atoms;
+  if (!EO && !lcpo_due(lc, ss, v.sys_of[i])) {
+    if (lane == 0) {
+      const double dx = lc.deriv[i], dy = lc.deriv[N + i], dz = lc.deriv[2 * N + i];
+      if (dx != 0.0 || dy != 0.0 || dz != 0.0) lcpo_add_force(v, i, dx, dy, dz);
+    }
+    return;
+  }
+  if (!lc.use[i]) {
+    if (lane == 0) {
+      lc.sasa[i] = 0.0;
+      v.e_atom[AE_SURF * N + i] = 0.0;
+      if (!EO) lc.deriv[i] = lc.deriv[N + i] = lc.deriv[2 * N + i] = 0.0;
+    }
+    return;
+  }
+  double(*W)[kLcpoMax + 1] = T[warp];
+  const double xi = v.x[i], yi = v.y[i], zi = v.z[i], ri = lc.r[i];
+  const int cnt = lc.cnt[i];
+  const size_t base = (size_t)i * kLcpoMax;
+  for (int e = lane; e < cnt; e += 32) {
+    const int ja = lc.idx[base + e];
+    const double si2 = lc.s[base + e];
+    const int nj = lc.cnt[ja];
+    const size_t jb = (size_t)ja * kLcpoMax;
+    double si3 = 0.0;
+    if (EO) {
+      // lcpo.cpp:517-537
+      for (int k = 0; k < nj; k++) {
+        const int ka = lc.idx[jb + k];
+        if (ka == i) continue;
+        const double g = v.x[ka] - xi, h = v.y[ka] - yi, q = v.z[ka] - zi;
+        if (ri + lc.r[ka] < sqrt(g * g + h * h + q * q)) continue;
+        si3 += lc.s[jb + k];
+      }
+    } else {
+      // lcpo.cpp:772-901
+      const double xj = v.x[ja], yj = v.y[ja], zj = v.z[ja], rj = lc.r[ja];
+      const double gx = xj - xi, gy = yj - yi, gz = zj - zi;
+      const double dij = sqrt(gx * gx + gy * gy + gz * gz);
+      const double invij = 1 / dij;
+      double hd = 0.5 * (ri * ri - rj * rj) * invij;
+      const double sji = kTwoPi * rj * (rj - dij * 0.5 + hd);
+      hd *= 2.0 * invij;
+      const double ddx = -(xi - xj) / dij, ddy = -(yi - yj) / dij, ddz = -(zi - zj) / dij;
+      double dAdd = kPi * rj * (-hd - 1);
+      double d2x = dAdd * ddx, d2y = dAdd * ddy, d2z = dAdd * ddz;
+      dAdd = kPi * ri * (hd - 1);
+      const double a2x = dAdd * ddx, a2y = dAdd * ddy, a2z = dAdd * ddz;
+      double d3x = 0, d3y = 0, d3z = 0, d3bx = 0, d3by = 0, d3bz = 0, d4bx = 0, d4by = 0, d4bz = 0;
+      double s3ik = 0.0;
+      for (int k = 0; k < nj; k++) {
+        const int ka = lc.idx[jb + k];
+        const double xk = v.x[ka], yk = v.y[ka], zk = v.z[ka], rk = lc.r[ka];
+        if (ka == i) continue;
+        const double g = xk - xi, h = yk - yi, q = zk - zi;
+        double dik = g * g + h * h + q * q;
+        if ((ri + rk) * (ri + rk) < dik) continue;
+        dik = sqrt(dik);
+        const double invik = 1 / dik;
+        const double hk = (ri * ri - rk * rk) * (invik * invik);
+        dAdd = kPi * ri * (hk - 1);
+        const double dkx = -(xi - xk) * invik, dky = -(yi - yk) * invik, dkz = -(zi - zk) * invik;
+        const double sjk = lc.s[jb + k];
+        d3x += dAdd * dkx;
+        d3y += dAdd * dky;
+        d3z += dAdd * dkz;
+        dAdd = kPi * rk * (-hk - 1);
+        s3ik += kPi * ri * (2 * ri - dik - dik * hk);
+        d3bx += dAdd * dkx;
+        d3by += dAdd * dky;
+        d3bz += dAdd * dkz;
+        d4bx += sjk * dAdd * dkx;
+        d4by += sjk * dAdd * dky;
+        d4bz += sjk * dAdd * dkz;
+        si3 += sjk;
+      }
+      double d4x = sji * d3x + d4bx, d4y = sji * d3y + d4by, d4z = sji * d3z + d4bz;
+      d3x += d3bx;
+      d3y += d3by;
+      d3z += d3bz;
+      d4x += d2x * s3ik;
+      d4y += d2y * s3ik;
+      d4z += d2z * s3ik;
+      const double4 pj = lc.p[ja];
+      const double sj = lc.sigma[ja];
+      const double m2 = pj.y * sj, m3 = pj.z * sj, m4 = pj.w * sj;
+      W[0][e] = d2x * m2;
+      W[1][e] = d2y * m2;
+      W[2][e] = d2z * m2;
+      W[3][e] = d3x * m3;
+      W[4][e] = d3y * m3;
+      W[5][e] = d3z * m3;
+      W[6][e] = d4x * m4;
+      W[7][e] = d4y * m4;
+      W[8][e] = d4z * m4;
+      W[11][e] = a2x;
+      W[12][e] = a2y;
+      W[13][e] = a2z;
+    }
+    W[9][e] = si2;
+    W[10][e] = si3;
+  }
+  __syncwarp();
+  // ordered sums over the partners (lcpo.cpp:903-920): lanes 0-2 SASAderiv
+  // x y z, 3 Si4, 4 Si3, 5 Si2, 6-8 dAijdc_2, 9-11 dAijdc_4
+  double acc = 0.0;
+  if (lane < 3) {
+    if (!EO)
+      for (int e = 0; e < cnt; e++) {
+        acc += W[lane][e];
+        acc += W[3 + lane][e];
+        acc += W[6 + lane][e];
+      }
+  } else if (lane == 3) {
+    for (int e = 0; e < cnt; e++) acc += W[10][e] * W[9][e];
+  } else if (lane == 4) {
+    for (int e = 0; e < cnt; e++) acc += W[10][e];
+  } else if (lane == 5) {
+    for (int e = 0; e < cnt; e++) acc += W[9][e];
+  } else if (lane < 9) {
+    if (!EO)
+      for (int e = 0; e < cnt; e++) acc += W[5 + lane][e];
+  } else if (lane < 12) {
+    if (!EO)
+      for (int e = 0; e < cnt; e++) acc += W[10][e] * W[2 + lane][e];
+  }
+  double R[12];
+#pragma unroll
+  for (int c = 0; c < 12; c++) R[c] = __shfl_sync(0xffffffffu, acc, c);
+  if (lane != 0) return;
+  const double4 pi = lc.p[i];
+  const double sig = lc.sigma[i];
+  const double Si = kFourPi * ri * ri;  // sphereSurfaceArea (maths/maths.cpp:97-100)
+  double SAi = pi.x * Si + pi.y * R[5] + pi.z * R[4] + pi.w * R[3];
+  double D[3] = {R[0], R[1], R[2]};
+  if (!EO) {
+    const double m2 = pi.y * sig, m4 = pi.w * sig;
+    for (int c = 0; c < 3; c++) D[c] += R[6 + c] * m2;
+    for (int c = 0; c < 3; c++) D[c] += R[9 + c] * m4;
+  }
+  if (SAi < 0) {  // lcpo.cpp:926-929
+    SAi = 0;
+    D[0] = D[1] = D[2] = 0.0;
+  }
+  lc.sasa[i] = SAi;
+  v.e_atom[AE_SURF * N + i] = SAi * sig;
+  if (!EO) {
+    lc.deriv[i] = D[0];
+    lc.deriv[N + i] = D[1];
+    lc.deriv[2 * N + i] = D[2];
+    if (D[0] != 0.0 || D[1] != 0.0 || D[2] != 0.0) lcpo_add_force(v, i, D[0], D[1], D[2]);
+  }
+}
+
+void launch_lcpo(const PackView &v, cudaStream_t st, StepSrc step, bool energy_only) {
+  if (v.lc.update <= 0 || !v.n_atoms) return;
+  const int blocks = (v.n_atoms + kLcpoWarps - 1) / kLcpoWarps;
+  if (energy_only) {
+    PDGPU_LAUNCH(k_lcpo_list<true>, blocks, kLcpoWarps * 32, 0, st, v, step);
+    PDGPU_LAUNCH(k_lcpo_eval<true>, blocks, kLcpoWarps * 32, 0, st, v, step);
+  } else {
+    PDGPU_LAUNCH(k_lcpo_list<false>, blocks, kLcpoWarps * 32, 0, st, v, step);
+    PDGPU_LAUNCH(k_lcpo_eval<false>, blocks, kLcpoWarps * 32, 0, st, v, step);
+  }
+}
+
+}  // namespace pdgpu

@@ -181,7 +181,8 @@ void pdgpu_server::fail(Job *j, int status, const std::string &msg) {
 // A job on the tile layout (systems within the search limit) rebuilds by
 // tile search: no list, no size read-back.
 static bool tile_search_job(const Pack &P) {
-  return P.v.tile_mode && P.v.tile_meta && P.v.n_sc > 0 && P.v.max_sys_atoms <= kTileSearchMaxAtoms;
+  return P.v.tile_mode && P.v.tile_meta && P.v.n_sc > 0 && P.v.max_sys_atoms <= kTileSearchMaxAtoms &&
+         P.v.lc.update <= 0;  // the LCPO term reads the CSR rows
 }
 static void rebuild_pairs(Pack &P, cudaStream_t st) {
   if (tile_search_job(P)) {
@@ -234,7 +235,7 @@ void pdgpu_server::enqueue_min_chunk(Job *j) {
   for (int q = 0; q < j->chunk; q++) {
     int cnt = j->counter + j->iter + q;
     if (p.UpdateNList > 0 && (cnt % p.UpdateNList) == 0) rebuild_pairs(P, j->st);
-    calc_forces_enqueue(j->st, j->e.get(), true);
+    calc_forces_enqueue(j->st, j->e.get(), true, min_step_src(j->e->min_state, false));
     launch_min_step(P.v, j->st, j->e->min_state, p.Algorithm, slope, p.Strictness, p.StepSize, steps);
   }
   cudaMemcpyAsync(j->pin->flags, P.v.flags, sizeof(int) * F_COUNT, cudaMemcpyDeviceToHost, j->st);
@@ -436,6 +437,10 @@ void pdgpu_server::advance(Job *j) {
         fail(j, PDGPU_ERR_UNSTABLE, "Simulation unstable (NaN energy during minimisation)");
         return;
       }
+      if (j->pin->flags[F_LCPO_CAND]) {
+        fail(j, PDGPU_ERR_STATE, kLcpoCandMsg);
+        return;
+      }
       bool overflow = j->pin->flags[F_NL_OVERFLOW] != 0;
       bool finished = advanced < j->chunk && !overflow;
       j->iter += advanced;
@@ -451,7 +456,7 @@ void pdgpu_server::advance(Job *j) {
         j->steps_done = j->taken;
         // cur = old; recompute the energies (minimise.cpp:172-176)
         launch_min_finish(P.v, j->st);
-        calc_forces_enqueue(j->st, e, true);
+        calc_forces_enqueue(j->st, e, true, min_step_src(e->min_state, true));
         enqueue_results(j);
         return;
       }
@@ -466,6 +471,10 @@ void pdgpu_server::advance(Job *j) {
           return;
         }
         enqueue_size(j, PH_MD);
+        return;
+      }
+      if (j->pin->flags[F_LCPO_CAND]) {
+        fail(j, PDGPU_ERR_STATE, kLcpoCandMsg);
         return;
       }
       if (j->pin->flags[F_NAN]) {
@@ -695,11 +704,13 @@ int pdgpu_serve_submit(pdgpu_server *s, int32_t sys, const pdgpu_job *job, const
   }
   // device bytes before the list is sized: per-atom arrays, a list of 256
   // entries per atom and the worst-case tile store (48 bytes per tile of
-  // 32 x 8 atoms); the pack is charged its real size once sized
+  // 32 x 8 atoms), the LCPO overlap lists where the system has the term;
+  // the pack is charged its real size once sized
   {
     int64_t nsc = ((int64_t)n + 31) / 32, njc = ((int64_t)n + 7) / 8, tiles = 0;
     for (int64_t k = 0; k < nsc; k++) tiles += njc - 4 * k;
     j->est_bytes = (int64_t)n * (1024 + 256 * 4) + tiles * 48 + nsc * 16 * 64 + (int64_t)4 * 1024 * 1024;
+    if (host->lcpo_update > 0) j->est_bytes += (int64_t)n * (kLcpoMax * 12 + 96);
   }
   if (j->est_bytes > s->prm.hbm_budget) {
     set_error("pdgpu_serve_submit: the job alone exceeds the HBM budget");

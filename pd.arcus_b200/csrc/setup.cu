@@ -253,6 +253,67 @@ int pack_ensure_tiles(Pack *p) {
   return PDGPU_OK;
 }
 
+// FF_SASA_LCPO parameters of every member (members without the term have
+// use 0 on every atom) and the term's state, allocated the first time;
+// enqueued on p->st.  All members share one UpdateSasa.
+int pack_upload_lcpo(Pack *p, const std::vector<const SystemHost *> &systems) {
+  PackView &v = p->v;
+  LcpoView &lc = v.lc;
+  const size_t N = (size_t)v.n_atoms;
+  int update = 0;
+  for (auto *h : systems)
+    if (h->lcpo_update > 0) {
+      if (update && update != h->lcpo_update) {
+        set_error("batch members have different UpdateSasa values");
+        return PDGPU_ERR_ARG;
+      }
+      update = h->lcpo_update;
+    }
+  lc.update = 0;
+  if (!update) return PDGPU_OK;
+  if (!lc.r) {
+    double *r = nullptr, *sig = nullptr;
+    double4 *p4 = nullptr;
+    unsigned char *use = nullptr;
+    if (palloc(p, &r, N) != cudaSuccess || palloc(p, &p4, N) != cudaSuccess || palloc(p, &sig, N) != cudaSuccess ||
+        palloc(p, &use, N) != cudaSuccess || palloc(p, &lc.cnt, N) != cudaSuccess ||
+        palloc(p, &lc.idx, N * kLcpoMax) != cudaSuccess || palloc(p, &lc.s, N * kLcpoMax) != cudaSuccess ||
+        palloc(p, &lc.sasa, N) != cudaSuccess || palloc(p, &lc.deriv, 3 * N) != cudaSuccess) {
+      set_error("device allocation failed (LCPO surface term)");
+      return PDGPU_ERR_NOMEM;
+    }
+    lc.r = r;
+    lc.p = p4;
+    lc.sigma = sig;
+    lc.use = use;
+  }
+  std::vector<double> r(N, 0.0), sig(N, 0.0);
+  std::vector<double4> p4(N, make_double4(0, 0, 0, 0));
+  std::vector<unsigned char> use(N, 0);
+  for (size_t k = 0; k < systems.size(); k++) {
+    const SystemHost &h = *systems[k];
+    if (h.lcpo_update <= 0) continue;
+    const int o = p->atom_off[k];
+    for (int i = 0; i < h.natoms; i++) {
+      r[o + i] = h.lcpo_r[i];
+      p4[o + i] = make_double4(h.lcpo_p[4 * i], h.lcpo_p[4 * i + 1], h.lcpo_p[4 * i + 2], h.lcpo_p[4 * i + 3]);
+      sig[o + i] = h.lcpo_sigma[i];
+      use[o + i] = h.lcpo_use[i];
+    }
+  }
+  cudaStream_t st = p->st;
+  if (cudaMemcpyAsync((void *)lc.r, r.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync((void *)lc.p, p4.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync((void *)lc.sigma, sig.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync((void *)lc.use, use.data(), N, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess) {
+    set_error("LCPO parameter upload failed");
+    return PDGPU_ERR_CUDA;
+  }
+  lc.update = update;
+  return PDGPU_OK;
+}
+
 void pack_set_params(Pack *p, int s, const pdgpu_ff_params &prm) {
   p->sp[s] = make_sys_params(prm);
 }
@@ -623,7 +684,7 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   v.lpa[0] = v.lpa[1] = v.lpa[2] = 8;
   v.e_chunks = (max_range + kReduceChunk - 1) / kReduceChunk;
   if (v.e_chunks < 1) v.e_chunks = 1;
-  PALLOC(v.e_part, (size_t)S * v.e_chunks * 10);
+  PALLOC(v.e_part, (size_t)S * v.e_chunks * kPartSlots);
   PALLOC(v.e_done, S);
   PALLOC(bt.bij, bij.size());
   PALLOC(bt.blk, blk.size());
@@ -646,6 +707,11 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
     cudaMemcpyAsync(bt.tterms, tterms.data(), sizeof(int) * tterms.size(), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(bt.ttype, ttype.data(), sizeof(int) * ttype.size(), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(bt.tpar, tpar.data(), sizeof(double) * tpar.size(), cudaMemcpyHostToDevice, st);
+  }
+  if (pack_upload_lcpo(p, systems) != PDGPU_OK) {
+    if (err) *err = last_error_cstr();
+    delete p;
+    return nullptr;
   }
   cudaEventCreate(&p->ev0);
   cudaEventCreate(&p->ev1);

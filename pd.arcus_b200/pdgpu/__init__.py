@@ -7,7 +7,7 @@ there is no CPU fallback.
 from ._abi import (PdgpuError, UnstableError, lib, last_error, ff_params_default,  # noqa: F401
                    md_params_default, min_params_default, FFParams, MDParams, MinParams)
 from .core import (Context, SystemSpec, WorkSpace, NeighbourList, Hamiltonian,  # noqa: F401
-                   ForcefieldBase, Forcefield, FF_Bonded, FF_NonBonded, FF_GeneralizedBorn_Still,
+                   ForcefieldBase, Forcefield, FF_Bonded, FF_NonBonded, FF_GeneralizedBorn_Still, FF_SASA_LCPO,
                    ProtocolBase, Energy, Minimisation, MolecularDynamics, J2KCAL_NA)
 from .batch import Batch  # noqa: F401
 from .serve import Server  # noqa: F401

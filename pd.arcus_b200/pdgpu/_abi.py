@@ -20,6 +20,7 @@ ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_UNSTABLE, ERR_STATE, ERR_BUDGET, ERR_NODEVICE 
 ENE_EPOT, ENE_VDW, ENE_ELEC, ENE_POL, ENE_POL_CROSS, ENE_POL_SELF = 0, 1, 2, 3, 4, 5
 ENE_BOND, ENE_ANGLE, ENE_TORSION, ENE_VIRIAL, ENE_EKIN, ENE_ETOT = 6, 7, 8, 9, 10, 11
 ENE_GB_COMPONENT = 12
+ENE_SURF = 15
 ENE_COUNT = 16
 
 INTEGRATOR_VERLET, INTEGRATOR_VELOCITY_VERLET, INTEGRATOR_BEEMAN, INTEGRATOR_LANGEVIN = 0, 1, 2, 3
@@ -91,6 +92,7 @@ JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int32)
 _I8 = ctypes.POINTER(ctypes.c_int8)
+_U8 = ctypes.POINTER(ctypes.c_uint8)
 _I64 = ctypes.POINTER(ctypes.c_int64)
 _CTX = ctypes.c_void_p
 
@@ -111,6 +113,9 @@ PROTOTYPES = {
                                                ctypes.c_int32, _I, _D, ctypes.c_int32, _I, _I, _D,
                                                ctypes.c_int32, _I, _I, _D]),
     "pdgpu_system_set_hydrogens": (ctypes.c_int, [_CTX, ctypes.c_int32, _I8]),
+    "pdgpu_sasa_lcpo_set": (ctypes.c_int, [_CTX, ctypes.c_int32, _D, _D, _D, _U8, ctypes.c_int32]),
+    "pdgpu_set_step": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32]),
+    "pdgpu_get_step": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
     "pdgpu_batch_create": (ctypes.c_int, [_CTX, _I, ctypes.c_int32, _I]),
     "pdgpu_batch_info": (ctypes.c_int, [_CTX, ctypes.c_int32, _I, _I]),
     "pdgpu_set_seeds": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64)]),
@@ -133,6 +138,9 @@ PROTOTYPES = {
     "pdgpu_gb_energies": (ctypes.c_int, [_CTX, ctypes.c_int32]),
     "pdgpu_nonbonded_forces": (ctypes.c_int, [_CTX, ctypes.c_int32]),
     "pdgpu_bonded_forces": (ctypes.c_int, [_CTX, ctypes.c_int32]),
+    "pdgpu_sasa_lcpo_forces": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32]),
+    "pdgpu_sasa_lcpo_energies": (ctypes.c_int, [_CTX, ctypes.c_int32]),
+    "pdgpu_sasa_lcpo_get": (ctypes.c_int, [_CTX, ctypes.c_int32, _D, _D]),
     "pdgpu_calc_forces": (ctypes.c_int, [_CTX, ctypes.c_int32]),
     "pdgpu_md_run": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.POINTER(MDParams), ctypes.c_int32,
                                     ctypes.c_int32, ctypes.c_int32, _D]),

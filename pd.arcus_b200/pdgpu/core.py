@@ -94,7 +94,8 @@ class Hamiltonian:
     FIELDS = {"epot": A.ENE_EPOT, "epot_vdw": A.ENE_VDW, "epot_elec": A.ENE_ELEC, "epot_pol": A.ENE_POL,
               "epot_pol_cross": A.ENE_POL_CROSS, "epot_pol_self": A.ENE_POL_SELF,
               "epot_bond": A.ENE_BOND, "epot_angle": A.ENE_ANGLE, "epot_torsion": A.ENE_TORSION,
-              "InternalVirial": A.ENE_VIRIAL, "ekin": A.ENE_EKIN, "etot": A.ENE_ETOT}
+              "InternalVirial": A.ENE_VIRIAL, "ekin": A.ENE_EKIN, "etot": A.ENE_ETOT,
+              "epot_surf": A.ENE_SURF}
 
     def __init__(self):
         self.zero()
@@ -138,6 +139,7 @@ class WorkSpace:
         self._nlist = NeighbourList(self)
         self._pos_dirty = True
         self._ff = None  # the Forcefield whose components set this workspace up
+        self._lcpo_set = False  # the device system has the LCPO term
 
     def nAtoms(self):
         return self.spec.natoms
@@ -209,6 +211,12 @@ class WorkSpace:
         e = np.zeros(A.ENE_COUNT)
         A.check(A.lib().pdgpu_get_energies(self.ctx.ptr, self._sys, A.dptr(e), A.ENE_COUNT))
         return e
+
+    def _pull_step(self):
+        """WorkSpace::Step as the last protocol left it."""
+        st = ctypes.c_int32(0)
+        A.check(A.lib().pdgpu_get_step(self.ctx.ptr, self._sys, ctypes.byref(st)))
+        self.Step = st.value
 
     def born_radii(self):
         b = np.zeros(self.nAtoms())
@@ -433,6 +441,69 @@ class FF_GeneralizedBorn_Still(FF_NonBonded):
         return p
 
 
+class FF_SASA_LCPO(ForcefieldBase):
+    """The LCPO surface-area term (forcefields/lcpo.h; Weiser, Shenkin &
+    Still 1999): epot_surf = sum of SASA_i * sigma_i over the heavy atoms.
+
+    The per-atom LCPO parameters (type radius + 1.4, P1..P4, use) are the
+    ones FF_SASA_LCPO::setup assigns from the parameter file's
+    LCPOSASAPARAMETERS section; the SystemSpec carries them (lcpo_radius,
+    lcpo_p, lcpo_use).  sigma is GlobalASP (kcal/mol/A^2) on every atom, as
+    on the reference's default path, unless ASP holds one value per atom.
+    UpdateSasa: inside MD and minimisation the term is recomputed when
+    WorkSpace.Step % UpdateSasa == 0 and otherwise reuses the forces of its
+    last evaluation (lcpo.cpp:176-190)."""
+
+    name = "LCPO SASA"
+    LIST_CUTOFF = 7.0  # FF_SASA_LCPO::setup requests a 7 A neighbour list (lcpo.cpp:20)
+
+    def __init__(self, wspace):
+        super().__init__(wspace)
+        self.ASPsection_name = ""
+        self.GlobalASP = 0.0
+        self.UpdateSasa = 5
+        self.ASP = None
+        self._key = None
+
+    def _sigma(self):
+        n = self.wspace.nAtoms()
+        if self.ASP is not None:
+            sig = np.ascontiguousarray(self.ASP, dtype=np.float64).reshape(-1)
+            if sig.shape[0] != n:
+                raise ValueError("ASP must hold one value per atom")
+            return sig
+        return np.full(n, float(self.GlobalASP))
+
+    def _setup(self):
+        ws, sp = self.wspace, self.wspace.spec
+        if self.ASPsection_name:
+            raise A.PdgpuError(A.ERR_ARG, "ASP sections are not read; give per-atom values in ASP")
+        for k in ("lcpo_radius", "lcpo_p", "lcpo_use"):
+            if k not in sp:
+                raise A.PdgpuError(A.ERR_ARG, "the system spec has no LCPO parameters (%s)" % k)
+        if int(self.UpdateSasa) < 1:
+            raise ValueError("UpdateSasa must be >= 1")
+        sig = self._sigma()
+        key = (sig.tobytes(), int(self.UpdateSasa), bool(self.Active))
+        if key == self._key and ws._lcpo_set:
+            return
+        use = np.ascontiguousarray(sp["lcpo_use"], dtype=np.uint8)
+        A.check(A.lib().pdgpu_sasa_lcpo_set(
+            ws.ctx.ptr, ws._sys, A.dptr(A.cd(sp["lcpo_radius"])), A.dptr(A.cd(sp["lcpo_p"]).reshape(-1)),
+            A.dptr(sig), use.ctypes.data_as(A._U8), int(self.UpdateSasa) if self.Active else 0))
+        self._key = key
+        ws._lcpo_set = bool(self.Active)
+
+    def sasa(self):
+        """Per-atom SASA (A^2) of the last evaluation and SASAderiv of the
+        last full one (kcal/mol/A, [n, 3])."""
+        ws = self.wspace
+        n = ws.nAtoms()
+        a, d = np.zeros(n), np.zeros((n, 3))
+        A.check(A.lib().pdgpu_sasa_lcpo_get(ws.ctx.ptr, ws._sys, A.dptr(a), A.dptr(d)))
+        return a, d
+
+
 class Forcefield:
     """The component container (forcefield.h:266-319): calcForces zeroes the
     workspace and runs every component (forcefield.cpp:220-247)."""
@@ -451,24 +522,52 @@ class Forcefield:
     def getWSpace(self):
         return self.wspace
 
-    def _nb(self):
+    def _nb(self, required=True):
         nb = [c for c in self.components if isinstance(c, FF_NonBonded) and c.Active]
-        if len(nb) != 1:
+        if len(nb) > 1 or (required and not nb):
             raise A.PdgpuError(A.ERR_ARG, "the GPU path needs exactly one FF_NonBonded / "
                                           "FF_GeneralizedBorn_Still component")
-        return nb[0]
+        return nb[0] if nb else None
 
     def _has_bonded(self):
         return any(isinstance(c, FF_Bonded) and c.Active for c in self.components)
 
+    def _lcpo(self):
+        lc = [c for c in self.components if isinstance(c, FF_SASA_LCPO)]
+        if len(lc) > 1:
+            raise A.PdgpuError(A.ERR_ARG, "more than one FF_SASA_LCPO component")
+        return lc[0] if lc else None
+
     def ensuresetup(self, wspace=None):
-        nb = self._nb()
+        lc = self._lcpo()
+        nb = self._nb(required=lc is None)
         ws = self.wspace
-        ws.nlist().requestCutoff(max(nb.Cutoff, nb.VdwCutoff))
-        if isinstance(nb, FF_GeneralizedBorn_Still):
-            ws.nlist().calcShadow(True)
-        ws._ensure_device(nb._params(), self._has_bonded())
+        if nb is not None:
+            ws.nlist().requestCutoff(max(nb.Cutoff, nb.VdwCutoff))
+            if isinstance(nb, FF_GeneralizedBorn_Still):
+                ws.nlist().calcShadow(True)
+            params = nb._params()
+            if lc is not None and lc.Active and max(nb.Cutoff, nb.VdwCutoff) < lc.LIST_CUTOFF:
+                raise A.PdgpuError(A.ERR_ARG, "FF_SASA_LCPO needs a neighbour list of at least 7 A: "
+                                              "set the non-bonded Cutoff >= 7")
+        else:
+            # the surface term alone: a 7 A list and no pair passes
+            ws.nlist().requestCutoff(lc.LIST_CUTOFF)
+            params = A.ff_params_default()
+            params.Cutoff = params.VdwCutoff = lc.LIST_CUTOFF
+            params.InnerCutoff = params.VdwInnerCutoff = lc.LIST_CUTOFF - 3.0
+            params.Padding = ws.nlist().Padding
+        ws._ensure_device(params, self._has_bonded())
+        if lc is not None:
+            lc._setup()
+        elif ws._lcpo_set:
+            A.check(A.lib().pdgpu_sasa_lcpo_set(ws.ctx.ptr, ws._sys, None, None, None, None, 0))
+            ws._lcpo_set = False
         return 0
+
+    def _lcpo_active(self):
+        lc = self._lcpo()
+        return lc is not None and lc.Active
 
     def _sync_in(self):
         ws = self.wspace
@@ -484,7 +583,7 @@ class Forcefield:
     def calcForces(self):
         self.ensuresetup()
         self._sync_in()
-        nb = self._nb()
+        nb = self._nb(required=self._lcpo() is None)
         ws, L = self.wspace, A.lib()
         if self.wspace.nlist().getFullUpdateCount() == 0:
             self.wspace.nlist().calcNewList()
@@ -493,8 +592,10 @@ class Forcefield:
             A.check(L.pdgpu_bonded_forces(ws.ctx.ptr, ws._sys))
         if isinstance(nb, FF_GeneralizedBorn_Still):
             A.check(L.pdgpu_gb_forces(ws.ctx.ptr, ws._sys))
-        else:
+        elif nb is not None:
             A.check(L.pdgpu_nonbonded_forces(ws.ctx.ptr, ws._sys))
+        if self._lcpo_active():
+            A.check(L.pdgpu_sasa_lcpo_forces(ws.ctx.ptr, ws._sys, int(ws.Step)))
         self._sync_out()
         if not np.isfinite(ws.ene.epot_vdw) or not np.isfinite(ws.ene.epot_elec):
             ws.ene.epot = float("nan")
@@ -502,7 +603,7 @@ class Forcefield:
     def calcEnergies(self):
         self.ensuresetup()
         self._sync_in()
-        nb = self._nb()
+        nb = self._nb(required=self._lcpo() is None)
         ws, L = self.wspace, A.lib()
         if self.wspace.nlist().getFullUpdateCount() == 0:
             self.wspace.nlist().calcNewList()
@@ -511,8 +612,10 @@ class Forcefield:
             A.check(L.pdgpu_bonded_forces(ws.ctx.ptr, ws._sys))
         if isinstance(nb, FF_GeneralizedBorn_Still):
             A.check(L.pdgpu_gb_energies(ws.ctx.ptr, ws._sys))
-        else:
+        elif nb is not None:
             A.check(L.pdgpu_nonbonded_forces(ws.ctx.ptr, ws._sys))
+        if self._lcpo_active():
+            A.check(L.pdgpu_sasa_lcpo_energies(ws.ctx.ptr, ws._sys))
         self._sync_out()
 
     def printEnergySummary(self):
@@ -523,6 +626,8 @@ class Forcefield:
         print(" VdW:           %10.3f kcal/mol" % e.kcal("epot_vdw"))
         print(" Electrostatic: %10.3f kcal/mol" % e.kcal("epot_elec"))
         print(" GB:            %10.3f kcal/mol" % e.kcal("epot_pol"))
+        if self._lcpo_active():
+            print(" SASA Energy:   %10.3f kcal/mol" % e.kcal("epot_surf"))
         print(" Total energy: %10.3f kcal/mol" % e.kcal("epot"))
 
 
@@ -597,6 +702,7 @@ class Minimisation(ProtocolBase):
         ws._pull_positions()
         self.ff._sync_out()
         self.Step = taken.value
+        ws._pull_step()
         return taken.value
 
 
@@ -674,4 +780,5 @@ class MolecularDynamics(ProtocolBase):
         ws._pull_positions()
         ws._pull_velocities()
         self.ff._sync_out()
+        ws._pull_step()
         return int(self.Steps)
