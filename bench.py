@@ -21,6 +21,11 @@ Extra keys of the same JSON line:
               Langevin 1 fs, gamma 1/ps, 300 K, Rc 12 A, list every 10 steps,
               all systems in one CUDA-graph step loop; aggregate ns/day against
               one system alone.
+  lcpo        the headline system with the LCPO surface-area term added
+              (FF_SASA_LCPO, GlobalASP 0.005 kcal/mol/A^2, UpdateSasa 5):
+              parity against the reference, the device time of the term's
+              two launches against the nominal FP64 roof, and MD ns/day with
+              the term (same protocol as the headline).
   serving     a seeded Poisson request stream (200 requests/s) of jobs on
               systems of 500-30,000 atoms (log-uniform; multi-chain systems
               composed from the AMBER99 library peptides, chain axes along z
@@ -257,6 +262,70 @@ def bench_batched_md(pdgpu, A, ctx, torch, copies=16, steps=5000, plain_steps=20
             "finite": bool(np.all(np.isfinite(h))),
             "gpu_launches": int(lc1.value - lc0.value),
             "timing": "CUDA events around the device step loop (pdgpu_last_run_ms)"}
+
+
+# FP64 operations of one (atom, partner, partner's partner) triple of the
+# LCPO inner loop (lcpo.cpp:823-872, sqrt and divide counted as one each):
+# the full body when the third atom overlaps the first, else the distance
+# test alone
+LCPO_FLOP_OVERLAP = 58
+LCPO_FLOP_TEST = 10
+
+
+def bench_lcpo(pdgpu, A, ctx, torch, arrays, meta, f_max, sms, steps=500):
+    """FF_SASA_LCPO on the headline system."""
+    L = A.lib()
+    ws = pdgpu.WorkSpace(pdgpu.SystemSpec(arrays, meta), ctx)
+    ff = pdgpu.Forcefield(ws)
+    ff.add(pdgpu.FF_Bonded(ws))
+    gb = pdgpu.FF_GeneralizedBorn_Still(ws)
+    gb.Cutoff, gb.InnerCutoff = float(meta["cutoff"]), float(meta["inner"])
+    gb.VdwCutoff, gb.VdwInnerCutoff = float(meta["vdwcut"]), float(meta["vdwinner"])
+    ff.add(gb)
+    sasa = pdgpu.FF_SASA_LCPO(ws)
+    sasa.GlobalASP = float(arrays["lcpo_cfg"][0])
+    sasa.UpdateSasa = 5
+    ff.add(sasa)
+    ws.nlist().calcNewList()
+    ff.calcForces()
+    f_ref = arrays["lcpo_f_total"]
+    rms = float(np.sqrt(np.sum((ws.cur.f - f_ref) ** 2) / np.sum(f_ref ** 2)))
+    esurf_rel = float(abs(ws.ene.epot_surf - arrays["lcpo_ene_total"][10]) / abs(arrays["lcpo_ene_total"][10]))
+    prof = np.zeros(5)
+    A.check(L.pdgpu_profile_lcpo(ctx.ptr, ws._sys, 20, A.dptr(prof)))
+    t_list, t_eval = prof[0] / 1e3, prof[1] / 1e3
+    pairs, triples, overl = prof[2], prof[3], prof[4]
+    flop = LCPO_FLOP_OVERLAP * overl + LCPO_FLOP_TEST * (triples - overl)
+    f64_peak = sms * 128 * f_max  # 64 FP64 FMA per SM per clock
+    # MD with the term: the headline protocol
+    p = A.md_params_default()
+    p.Integrator, p.UpdateNList, p.UseGraph = A.INTEGRATOR_LANGEVIN, BLOCK, 1
+    p.Timestep, p.FricCoeff, p.TargetTemp, p.Seed = 1e-15, 1e12, 300.0, 5
+    A.check(L.pdgpu_md_init_velocities(ctx.ptr, ws._sys, 300.0, 5))
+    total = steps + 20
+    A.check(L.pdgpu_md_run(ctx.ptr, ws._sys, ctypes.byref(p), 0, 20, total, None))
+    lc0 = ctypes.c_int64(0)
+    L.pdgpu_launch_count(ctx.ptr, ctypes.byref(lc0))
+    A.check(L.pdgpu_md_run(ctx.ptr, ws._sys, ctypes.byref(p), 20, steps, total, None))
+    ms = ctx.last_run_ms()
+    lc1 = ctypes.c_int64(0)
+    L.pdgpu_launch_count(ctx.ptr, ctypes.byref(lc1))
+    ws.close()
+    return {"metric": "GB/SA (LCPO) MD ns/day", "value": steps * DT_FS * 1e-6 / (ms / 1e3) * 86400.0,
+            "unit": "ns/day", "steps": steps, "ms_per_step": ms / steps,
+            "gpu_launches": int(lc1.value - lc0.value),
+            "parity": {"force_rel_rms_vs_fp64": rms, "epot_surf_rel_err": esurf_rel},
+            "kernels": {"k_lcpo_list_ms": t_list * 1e3, "k_lcpo_eval_ms": t_eval * 1e3,
+                        "overlap_partners": int(pairs), "inner_triples": int(triples),
+                        "overlapping_triples": int(overl)},
+            "roofline": {"kernel": "k_lcpo_eval (areas and derivatives, FP64)", "bound": "fp64",
+                         "achieved": flop / t_eval / 1e12, "peak": f64_peak / 1e12, "unit": "TFLOP/s",
+                         "frac": flop / t_eval / f64_peak,
+                         "peak_source": "nominal %d SMs x 128 FP64 flop/clk at sm_max_mhz %.0f" % (
+                             sms, f_max / 1e6),
+                         "work": "%d flop per overlapping triple, %d per distance test" % (
+                             LCPO_FLOP_OVERLAP, LCPO_FLOP_TEST)},
+            "amortised_ms_per_step": (t_list + t_eval) * 1e3 / 5}
 
 
 # ---------------------------------------------------------------- serving
@@ -745,6 +814,7 @@ def main():
             "gpu_launches": int(lc1.value - lc0.value),
             "clocks": clk, "roofline": roof, "e2e": e2e}
     if not args.no_batched:
+        line["lcpo"] = bench_lcpo(pdgpu, A, ctx, torch, arrays, meta, f_max, sms)
         line["batched_sp"] = bench_batched_sp(pdgpu, A, ctx, torch)
         line["batched_md"] = bench_batched_md(pdgpu, A, ctx, torch, steps=args.batched_md_steps)
         line["serving"] = bench_serving(pdgpu, A, ctx, torch, n_requests=args.serve_requests,

@@ -463,6 +463,14 @@ int pdgpu_pair_counts(pdgpu_ctx *ctx, int32_t sys, int64_t *counts);
  * kernels over `reps` evaluations, each bracketed by CUDA events on the
  * context stream: ms[0..2]. */
 int pdgpu_profile_pair_kernels(pdgpu_ctx *ctx, int32_t sys, int32_t reps, double *ms);
+/* Device times (CUDA events, averaged over reps full evaluations at step 0)
+ * of the LCPO term's two launches and the work they did: out[0] overlap
+ * list ms, out[1] area/derivative ms, out[2] overlap partners kept, out[3]
+ * (atom, partner, partner's partner) triples of the inner loop, out[4] the
+ * triples whose third atom overlaps the first (those run the whole inner
+ * body).  The forces of the timed evaluations are left in the
+ * accumulators. */
+int pdgpu_profile_lcpo(pdgpu_ctx *ctx, int32_t sys, int32_t reps, double *out);
 /* Kernels this context has launched (graph replays count their kernel
  * nodes). */
 int pdgpu_launch_count(pdgpu_ctx *ctx, int64_t *count);

@@ -643,7 +643,8 @@ struct LcpoType {
   int attype, nb;
   double r, p[4];
 };
-static void dump_lcpo(Built &b, const std::vector<double> &allpos, double asp, int update, int steps) {
+static void dump_lcpo(Built &b, const std::vector<double> &allpos, double asp, int update, int steps,
+                      bool dense) {
   WorkSpace &ws = *b.ws;
   size_t n = ws.nAtoms();
   Section sec;
@@ -713,7 +714,7 @@ static void dump_lcpo(Built &b, const std::vector<double> &allpos, double asp, i
   // an artificially dense packing (the coordinates shrunk to 0.35 about
   // their centroid): atoms with more than 80 overlapping partners, whose
   // overlap lists the reference truncates (lcpo.cpp:465-482)
-  {
+  if (dense) {
     std::vector<double> dp(allpos);
     double c[3] = {0, 0, 0};
     for (size_t i = 0; i < n; i++)
@@ -769,7 +770,7 @@ static void usage() {
           "ref_driver build --out DIR --nres N[,N..] --seed S [--cutoff R] "
           "[--inner R] [--grid NX,SPACING] [--premin STEPS] [--param F] "
           "[--md STEPS] [--min STEPS] [--slowmode] [--trials K --trial-sigma DEG]\n"
-          "          [--lcpo-asp KCAL_PER_A2 --lcpo UPDATESASA[,STEPS]]\n"
+          "          [--lcpo-asp KCAL_PER_A2 --lcpo UPDATESASA[,STEPS[,DENSE]]]\n"
           "ref_driver time --in DIR --cutoff R --inner R --steps K "
           "[--warmup W] [--nlist-every M] [--param F]\n");
   exit(1);
@@ -795,7 +796,7 @@ int main(int argc, char **argv) {
   int premin = 500, mdsteps = 0, minsteps = 0, steps = 10, warmup = 1, ntrials = 0;
   double trial_sigma_deg = 15.0;
   double lcpo_asp = 0.0;
-  int lcpo_update = 5, lcpo_steps = 0;
+  int lcpo_update = 5, lcpo_steps = 0, lcpo_dense = 1;
   int nlist_every = 10;
   int gridx = 0;
   double spacing = 25.0;
@@ -824,6 +825,7 @@ int main(int argc, char **argv) {
       std::vector<int> g = parse_ints(v);
       lcpo_update = g[0];
       if (g.size() > 1) lcpo_steps = g[1];
+      if (g.size() > 2) lcpo_dense = g[2];
       a++;
     } else if (k == "--lcpo-asp") { lcpo_asp = atof(v); a++; }
     else if (k == "--grid") {
@@ -898,7 +900,7 @@ int main(int argc, char **argv) {
       set_pos(*b.ws, allpos);
       dump_md_steps(b, MolecularDynamics::Beeman, mdsteps, 1e12, "mdbm_");
     }
-    if (lcpo_asp != 0.0) dump_lcpo(b, allpos, lcpo_asp, lcpo_update, lcpo_steps);
+    if (lcpo_asp != 0.0) dump_lcpo(b, allpos, lcpo_asp, lcpo_update, lcpo_steps, lcpo_dense != 0);
     printf("built %zu atoms\n", b.ws->nAtoms());
     return 0;
   }

@@ -1890,6 +1890,72 @@ int pdgpu_profile_pair_kernels(pdgpu_ctx *c, int32_t sys, int32_t reps, double *
   return PDGPU_OK;
 }
 
+// Device times of the LCPO term's two launches (full evaluations at step
+// 0; the forces they add are left in the accumulators) and the work they
+// did: out[0] list ms, out[1] evaluation ms, out[2] overlap partners kept,
+// out[3] (atom, partner, partner's partner) triples of the inner loop,
+// out[4] those whose third atom overlaps the first (the full inner body).
+int pdgpu_profile_lcpo(pdgpu_ctx *c, int32_t sys, int32_t reps, double *out) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  if (!out || reps <= 0) {
+    set_error("out is NULL or reps <= 0");
+    return PDGPU_ERR_ARG;
+  }
+  int r = lcpo_ready(c, e);
+  if (r) return r;
+  cudaEvent_t ev[3];
+  for (int q = 0; q < 3; q++) cudaEventCreate(&ev[q]);
+  double acc[2] = {0, 0};
+  for (int it = 0; it < reps; it++) {
+    cudaEventRecord(ev[0], c->st);
+    launch_lcpo_part(P.v, c->st, StepSrc(), false, 0);
+    cudaEventRecord(ev[1], c->st);
+    launch_lcpo_part(P.v, c->st, StepSrc(), false, 1);
+    cudaEventRecord(ev[2], c->st);
+    r = sync_check(c, "profile_lcpo");
+    if (r) break;
+    for (int q = 0; q < 2; q++) {
+      float t = 0;
+      cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
+      acc[q] += t;
+    }
+  }
+  for (int q = 0; q < 3; q++) cudaEventDestroy(ev[q]);
+  if (r) return r;
+  if ((r = lcpo_done(c, e, "profile_lcpo"))) return r;
+  const size_t N = (size_t)P.v.n_atoms;
+  std::vector<int> cnt(N), idx(N * kLcpoMax);
+  std::vector<double> x(N), y(N), z(N), rad(N);
+  PDGPU_CUDA(cudaMemcpy(cnt.data(), P.v.lc.cnt, sizeof(int) * N, cudaMemcpyDeviceToHost));
+  PDGPU_CUDA(cudaMemcpy(idx.data(), P.v.lc.idx, sizeof(int) * N * kLcpoMax, cudaMemcpyDeviceToHost));
+  PDGPU_CUDA(cudaMemcpy(x.data(), P.v.x, sizeof(double) * N, cudaMemcpyDeviceToHost));
+  PDGPU_CUDA(cudaMemcpy(y.data(), P.v.y, sizeof(double) * N, cudaMemcpyDeviceToHost));
+  PDGPU_CUDA(cudaMemcpy(z.data(), P.v.z, sizeof(double) * N, cudaMemcpyDeviceToHost));
+  PDGPU_CUDA(cudaMemcpy(rad.data(), P.v.lc.r, sizeof(double) * N, cudaMemcpyDeviceToHost));
+  double pairs = 0, triples = 0, overlapping = 0;
+  for (size_t i = 0; i < N; i++) {
+    pairs += cnt[i];
+    for (int q = 0; q < cnt[i]; q++) {
+      const int j = idx[i * kLcpoMax + q];
+      triples += cnt[j];
+      for (int t = 0; t < cnt[j]; t++) {
+        const int k = idx[(size_t)j * kLcpoMax + t];
+        const double dx = x[k] - x[i], dy = y[k] - y[i], dz = z[k] - z[i];
+        const double rs = rad[i] + rad[k];
+        if (k != (int)i && dx * dx + dy * dy + dz * dz <= rs * rs) overlapping++;
+      }
+    }
+  }
+  out[0] = acc[0] / reps;
+  out[1] = acc[1] / reps;
+  out[2] = pairs;
+  out[3] = triples;
+  out[4] = overlapping;
+  return PDGPU_OK;
+}
+
 int pdgpu_autotune(pdgpu_ctx *c, int32_t sys, int32_t *lpa) {
   CHECK_CTX(c);
   GET_SYS(e, c, sys);

@@ -99,6 +99,8 @@ enum EnergyMode {
 // batch members without it have `use` 0 on every atom.
 struct LcpoView {
   int update = 0;                      // UpdateSasa: full evaluation when Step % update == 0
+  int n_used = 0;                      // atoms with use = 1; the kernels run one warp per such atom
+  const int *atoms = nullptr;          // [n_used] their indices, ascending (the others' state stays 0)
   const double *r = nullptr;           // [N] LCPO type radius + 1.4 (A)
   const double4 *p = nullptr;          // [N] P1..P4
   const double *sigma = nullptr;       // [N] atomic solvation parameter, kcal/mol/A^2
@@ -345,6 +347,8 @@ void launch_bonded_terms(const PackView &v, cudaStream_t st);
 // whose step is due (energy_only: the calcEnergies path, always evaluated);
 // the other systems add their held derivatives to the forces.
 void launch_lcpo(const PackView &v, cudaStream_t st, StepSrc step, bool energy_only);
+// one of the two launches (0: overlap lists, 1: areas and derivatives)
+void launch_lcpo_part(const PackView &v, cudaStream_t st, StepSrc step, bool energy_only, int part);
 // energies: per-atom / per-term energies into the per-system record
 // (mode = EnergyMode bits); hist/step_dev only with EM_RECORD
 void launch_energy(const PackView &v, cudaStream_t st, int mode, double *hist = nullptr,

@@ -3,7 +3,8 @@
 // the reference's neighbour list, its 80-partner overlap lists and its
 // UpdateSasa cadence.
 //
-// Two launches per evaluation, one warp per atom:
+// Two launches per evaluation, one warp per atom the term uses (hydrogens,
+// use 0, keep area, energy and derivative 0 and get no warp):
 //  k_lcpo_list  the atom's overlap partners: the CSR row's atoms j with
 //               use[j] and |xi - xj| < ri + rj, ranked by index, the first
 //               80 kept with their overlap areas.  The reference appends
@@ -43,9 +44,10 @@ template <bool EO>
 __global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_list(PackView v, StepSrc ss) {
   __shared__ int cand[kLcpoWarps][kLcpoCand];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = blockIdx.x * kLcpoWarps + warp;
-  if (i >= v.n_atoms || v.flags[F_NL_OVERFLOW]) return;
   const LcpoView &lc = v.lc;
+  const int w = blockIdx.x * kLcpoWarps + warp;
+  if (w >= lc.n_used || v.flags[F_NL_OVERFLOW]) return;
+  const int i = lc.atoms[w];
   if (!EO && !lcpo_due(lc, ss, v.sys_of[i])) return;
   if (!lc.use[i]) {
     if (lane == 0) lc.cnt[i] = 0;
@@ -118,9 +120,10 @@ template <bool EO>
 __global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_eval(PackView v, StepSrc ss) {
   __shared__ double T[kLcpoWarps][kLcpoQ][kLcpoMax + 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = blockIdx.x * kLcpoWarps + warp;
-  if (i >= v.n_atoms || v.flags[F_NL_OVERFLOW]) return;
   const LcpoView &lc = v.lc;
+  const int w = blockIdx.x * kLcpoWarps + warp;
+  if (w >= lc.n_used || v.flags[F_NL_OVERFLOW]) return;
+  const int i = lc.atoms[w];
   const size_t N = (size_t)v.n_atoms;
   if (!EO && !lcpo_due(lc, ss, v.sys_of[i])) {
     if (lane == 0) {
@@ -276,16 +279,24 @@ __global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_eval(PackView v, StepS
   }
 }
 
-void launch_lcpo(const PackView &v, cudaStream_t st, StepSrc step, bool energy_only) {
-  if (v.lc.update <= 0 || !v.n_atoms) return;
-  const int blocks = (v.n_atoms + kLcpoWarps - 1) / kLcpoWarps;
-  if (energy_only) {
-    PDGPU_LAUNCH(k_lcpo_list<true>, blocks, kLcpoWarps * 32, 0, st, v, step);
-    PDGPU_LAUNCH(k_lcpo_eval<true>, blocks, kLcpoWarps * 32, 0, st, v, step);
+void launch_lcpo_part(const PackView &v, cudaStream_t st, StepSrc step, bool energy_only, int part) {
+  if (v.lc.update <= 0 || !v.lc.n_used) return;
+  const int blocks = (v.lc.n_used + kLcpoWarps - 1) / kLcpoWarps;
+  if (part == 0) {
+    if (energy_only)
+      PDGPU_LAUNCH(k_lcpo_list<true>, blocks, kLcpoWarps * 32, 0, st, v, step);
+    else
+      PDGPU_LAUNCH(k_lcpo_list<false>, blocks, kLcpoWarps * 32, 0, st, v, step);
   } else {
-    PDGPU_LAUNCH(k_lcpo_list<false>, blocks, kLcpoWarps * 32, 0, st, v, step);
-    PDGPU_LAUNCH(k_lcpo_eval<false>, blocks, kLcpoWarps * 32, 0, st, v, step);
+    if (energy_only)
+      PDGPU_LAUNCH(k_lcpo_eval<true>, blocks, kLcpoWarps * 32, 0, st, v, step);
+    else
+      PDGPU_LAUNCH(k_lcpo_eval<false>, blocks, kLcpoWarps * 32, 0, st, v, step);
   }
+}
+void launch_lcpo(const PackView &v, cudaStream_t st, StepSrc step, bool energy_only) {
+  launch_lcpo_part(v, st, step, energy_only, 0);
+  launch_lcpo_part(v, st, step, energy_only, 1);
 }
 
 }  // namespace pdgpu

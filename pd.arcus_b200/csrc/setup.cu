@@ -275,8 +275,9 @@ int pack_upload_lcpo(Pack *p, const std::vector<const SystemHost *> &systems) {
     double *r = nullptr, *sig = nullptr;
     double4 *p4 = nullptr;
     unsigned char *use = nullptr;
+    int *atoms = nullptr;
     if (palloc(p, &r, N) != cudaSuccess || palloc(p, &p4, N) != cudaSuccess || palloc(p, &sig, N) != cudaSuccess ||
-        palloc(p, &use, N) != cudaSuccess || palloc(p, &lc.cnt, N) != cudaSuccess ||
+        palloc(p, &use, N) != cudaSuccess || palloc(p, &atoms, N) != cudaSuccess || palloc(p, &lc.cnt, N) != cudaSuccess ||
         palloc(p, &lc.idx, N * kLcpoMax) != cudaSuccess || palloc(p, &lc.s, N * kLcpoMax) != cudaSuccess ||
         palloc(p, &lc.sasa, N) != cudaSuccess || palloc(p, &lc.deriv, 3 * N) != cudaSuccess) {
       set_error("device allocation failed (LCPO surface term)");
@@ -286,6 +287,7 @@ int pack_upload_lcpo(Pack *p, const std::vector<const SystemHost *> &systems) {
     lc.p = p4;
     lc.sigma = sig;
     lc.use = use;
+    lc.atoms = atoms;
   }
   std::vector<double> r(N, 0.0), sig(N, 0.0);
   std::vector<double4> p4(N, make_double4(0, 0, 0, 0));
@@ -301,8 +303,19 @@ int pack_upload_lcpo(Pack *p, const std::vector<const SystemHost *> &systems) {
       use[o + i] = h.lcpo_use[i];
     }
   }
+  std::vector<int> atoms;
+  for (size_t i = 0; i < N; i++)
+    if (use[i]) atoms.push_back((int)i);
   cudaStream_t st = p->st;
-  if (cudaMemcpyAsync((void *)lc.r, r.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+  // an atom leaving the term keeps no stale area, energy or derivative
+  cudaMemsetAsync(lc.cnt, 0, sizeof(int) * N, st);
+  cudaMemsetAsync(lc.sasa, 0, sizeof(double) * N, st);
+  cudaMemsetAsync(lc.deriv, 0, sizeof(double) * 3 * N, st);
+  cudaMemsetAsync(v.e_atom + (size_t)AE_SURF * N, 0, sizeof(double) * N, st);
+  if ((!atoms.empty() &&
+       cudaMemcpyAsync((void *)lc.atoms, atoms.data(), sizeof(int) * atoms.size(), cudaMemcpyHostToDevice, st) !=
+           cudaSuccess) ||
+      cudaMemcpyAsync((void *)lc.r, r.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync((void *)lc.p, p4.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync((void *)lc.sigma, sig.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync((void *)lc.use, use.data(), N, cudaMemcpyHostToDevice, st) != cudaSuccess ||
@@ -310,6 +323,7 @@ int pack_upload_lcpo(Pack *p, const std::vector<const SystemHost *> &systems) {
     set_error("LCPO parameter upload failed");
     return PDGPU_ERR_CUDA;
   }
+  lc.n_used = (int)atoms.size();
   lc.update = update;
   return PDGPU_OK;
 }

@@ -141,6 +141,7 @@ PROTOTYPES = {
     "pdgpu_sasa_lcpo_forces": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32]),
     "pdgpu_sasa_lcpo_energies": (ctypes.c_int, [_CTX, ctypes.c_int32]),
     "pdgpu_sasa_lcpo_get": (ctypes.c_int, [_CTX, ctypes.c_int32, _D, _D]),
+    "pdgpu_profile_lcpo": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32, _D]),
     "pdgpu_calc_forces": (ctypes.c_int, [_CTX, ctypes.c_int32]),
     "pdgpu_md_run": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.POINTER(MDParams), ctypes.c_int32,
                                     ctypes.c_int32, ctypes.c_int32, _D]),

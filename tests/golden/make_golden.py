@@ -25,7 +25,8 @@ with 500 steepest-descent steps at Rc 12 A unless noted):
                 velocity-Verlet and 12 steepest-descent steps of the whole forcefield
   c2_16x80_s2   16 x 80-residue chains on a 4x4 grid 25 A apart (~20.6k atoms),
                 Rc 16: inputs plus reference forces, Born radii and energies
-                (no neighbour list: too large to store)
+                (no neighbour list: too large to store), and the LCPO term's
+                parameters, forces and energies (GlobalASP 0.005, no dense case)
 """
 import json
 import os
@@ -49,7 +50,8 @@ SYSTEMS = {
     "c1_pep64_s0": dict(nres=[64], seed=0, cutoff=12, premin=500),
     "lcpo_pep24_s5": dict(nres=[24], seed=5, cutoff=12, premin=500, lcpo=(0.005, 5, 12),
                           drop=("lcpo_mdvv_normals",)),
-    "c2_16x80_s2": dict(nres=[80] * 16, seed=2, cutoff=16, premin=500, grid=(4, 25), drop_nl=True),
+    "c2_16x80_s2": dict(nres=[80] * 16, seed=2, cutoff=16, premin=500, grid=(4, 25), drop_nl=True,
+                        lcpo=(0.005, 5, 0, 0)),
 }
 
 # arrays kept for the large system (inputs + a few reference results)
@@ -72,8 +74,9 @@ def build(name, spec, keep_dir=None):
     if spec.get("trials"):
         cmd += ["--trials", str(spec["trials"]), "--trial-sigma", "15"]
     if spec.get("lcpo"):
-        asp, update, steps = spec["lcpo"]
-        cmd += ["--lcpo-asp", repr(asp), "--lcpo", "%d,%d" % (update, steps)]
+        asp, update, steps = spec["lcpo"][:3]
+        dense = spec["lcpo"][3] if len(spec["lcpo"]) > 3 else 1
+        cmd += ["--lcpo-asp", repr(asp), "--lcpo", "%d,%d,%d" % (update, steps, dense)]
     env = dict(os.environ, PD_PARAM_PATH=PARAM)
     subprocess.check_call(cmd, env=env, stdout=subprocess.DEVNULL)
     arrays = {}

@@ -237,3 +237,32 @@ def test_lcpo_batch_members_equal_alone(gpu_ctx):
         assert np.array_equal(deriv[lo:hi], d1)
         assert e[s][A.ENE_SURF] == pytest.approx(e1[A.ENE_SURF], rel=1e-13)
     b.close()
+
+
+def test_lcpo_large_system(gpu_ctx):
+    """The 20,566-atom system with the term, against the reference's
+    forces and surface energy (its list is too large to keep, so the oracle
+    runs on the device's exported list)."""
+    import pdgpu
+    a, meta = load_fixture("c2_16x80_s2")
+    ws = pdgpu.WorkSpace(pdgpu.SystemSpec(a, meta), gpu_ctx)
+    ff = pdgpu.Forcefield(ws)
+    ff.add(pdgpu.FF_Bonded(ws))
+    gb = pdgpu.FF_GeneralizedBorn_Still(ws)
+    gb.Cutoff, gb.InnerCutoff = float(meta["cutoff"]), float(meta["inner"])
+    gb.VdwCutoff, gb.VdwInnerCutoff = float(meta["vdwcut"]), float(meta["vdwinner"])
+    ff.add(gb)
+    sasa = pdgpu.FF_SASA_LCPO(ws)
+    sasa.GlobalASP = float(a["lcpo_cfg"][0])
+    ff.add(sasa)
+    ws.nlist().calcNewList()
+    ff.calcForces()
+    assert rel_rms(ws.cur.f, a["lcpo_f_total"]) <= 1e-5
+    assert ws.ene.epot_surf == pytest.approx(a["lcpo_ene_total"][10], rel=1e-12)
+    area, deriv = sasa.sasa()
+    ptr, data = ws.nlist().getData(shadow=True)
+    o_area, o_deriv, _, _ = O.lcpo(a["pos"], ptr, data, a["lcpo_radius"], a["lcpo_p"], float(a["lcpo_cfg"][0]),
+                                   a["lcpo_use"])
+    assert np.array_equal(area, o_area)
+    assert np.array_equal(deriv, o_deriv)
+    ws.close()
