@@ -119,8 +119,8 @@ int pdgpu_system_set_hydrogens(pdgpu_ctx *ctx, int32_t sys, const int8_t *is_h);
  * last full evaluation (lcpo.cpp:176-190); <= 0 removes the term.  Set it
  * on a single system before pdgpu_batch_create; batch members then share
  * one UpdateSasa.  With the term, pdgpu_calc_forces, pdgpu_md_run,
- * pdgpu_minimise_run and served jobs include it, and list rebuilds always
- * produce the CSR list (the term reads it). */
+ * pdgpu_minimise_run and served jobs include it.  Its overlap partners come
+ * from the neighbour list (the CSR rows, or the tiles of a tile search). */
 int pdgpu_sasa_lcpo_set(pdgpu_ctx *ctx, int32_t sys, const double *radius,
                         const double *p1234, const double *sigma,
                         const uint8_t *use, int32_t update_sasa);

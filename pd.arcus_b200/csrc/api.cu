@@ -897,11 +897,8 @@ static int nlist_enqueue(pdgpu_ctx *c, SysEntry *e, bool size_check) {
 // that rebuild (saved by the search), so it is the list the rebuild would
 // have made.  Packs on the row passes, or with a system too large for the
 // search, rebuild the list (and from it the tiles).
-// the LCPO term reads the CSR rows, so a pack with it builds them at
-// every rebuild
 static bool tile_search_ok(const Pack &P) {
-  return P.v.tile_mode && P.v.tile_meta && P.v.n_sc > 0 && P.v.max_sys_atoms <= kTileSearchMaxAtoms &&
-         P.v.lc.update <= 0;
+  return P.v.tile_mode && P.v.tile_meta && P.v.n_sc > 0 && P.v.max_sys_atoms <= kTileSearchMaxAtoms;
 }
 static void rebuild_enqueue(Pack &P, cudaStream_t st) {
   if (tile_search_ok(P)) {
@@ -1008,7 +1005,7 @@ static int ensure_tuned(pdgpu_ctx *c, Pack &P);
 // times the row passes too).
 static int ready_pairs(pdgpu_ctx *c, SysEntry *e) {
   Pack &P = *e->pack;
-  int r = need_csr_if(c, e, !P.tuned || !P.v.tile_mode || P.v.lc.update > 0);
+  int r = need_csr_if(c, e, !P.tuned || !P.v.tile_mode);
   if (r) return r;
   return ensure_tuned(c, P);
 }
@@ -1223,8 +1220,10 @@ static int lcpo_ready(pdgpu_ctx *c, SysEntry *e) {
     set_error("this system has no LCPO term (pdgpu_sasa_lcpo_set)");
     return PDGPU_ERR_STATE;
   }
-  int r = need_csr(c, e);
-  if (r) return r;
+  if (!P.have_list) {
+    set_error("no neighbour list: call pdgpu_nlist_build first (NeighbourList::calcNewList)");
+    return PDGPU_ERR_STATE;
+  }
   PDGPU_CUDA(cudaMemsetAsync(P.v.flags + F_LCPO_CAND, 0, sizeof(int), c->st));
   return PDGPU_OK;
 }
@@ -1247,7 +1246,7 @@ int pdgpu_sasa_lcpo_forces(pdgpu_ctx *c, int32_t sys, int32_t step) {
   if (r) return r;
   StepSrc src;
   src.imm = step < 0 ? e->ws_step : step;
-  launch_lcpo(e->pack->v, c->st, src, false);
+  launch_lcpo(e->pack->v, c->st, src, false, e->pack->csr_stale);
   launch_energy(e->pack->v, c->st, EM_SURF);
   return lcpo_done(c, e, "sasa_lcpo_forces");
 }
@@ -1257,7 +1256,7 @@ int pdgpu_sasa_lcpo_energies(pdgpu_ctx *c, int32_t sys) {
   GET_SYS(e, c, sys);
   int r = lcpo_ready(c, e);
   if (r) return r;
-  launch_lcpo(e->pack->v, c->st, StepSrc(), true);
+  launch_lcpo(e->pack->v, c->st, StepSrc(), true, e->pack->csr_stale);
   launch_energy(e->pack->v, c->st, EM_SURF);
   return lcpo_done(c, e, "sasa_lcpo_energies");
 }
@@ -1311,7 +1310,7 @@ void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce, StepS
     cudaMemsetAsync(P.v.fy, 0, bytes, P.side);
     cudaMemsetAsync(P.v.fz, 0, bytes, P.side);
     if (bonded) launch_bonded_terms(P.v, P.side);
-    if (surf) launch_lcpo(P.v, P.side, step, false);
+    if (surf) launch_lcpo(P.v, P.side, step, false, P.csr_stale);
     cudaEventRecord(P.join, P.side);
   }
   // with an MD step's energy record still running beside, the record is
@@ -1910,9 +1909,9 @@ int pdgpu_profile_lcpo(pdgpu_ctx *c, int32_t sys, int32_t reps, double *out) {
   double acc[2] = {0, 0};
   for (int it = 0; it < reps; it++) {
     cudaEventRecord(ev[0], c->st);
-    launch_lcpo_part(P.v, c->st, StepSrc(), false, 0);
+    launch_lcpo_part(P.v, c->st, StepSrc(), false, P.csr_stale, 0);
     cudaEventRecord(ev[1], c->st);
-    launch_lcpo_part(P.v, c->st, StepSrc(), false, 1);
+    launch_lcpo_part(P.v, c->st, StepSrc(), false, P.csr_stale, 1);
     cudaEventRecord(ev[2], c->st);
     r = sync_check(c, "profile_lcpo");
     if (r) break;

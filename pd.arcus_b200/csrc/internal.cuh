@@ -40,6 +40,7 @@ constexpr double kInvJScale = 1.0 / 16777216.0;
 constexpr int kReduceChunk = 256;                     // items per block of the per-system reductions
 constexpr int kPartSlots = 12;                        // reduction partials per (chunk, system)
 constexpr int kLcpoMax = 80;                          // overlap partners kept per atom (lcpo.h Nlistmax)
+constexpr int kLcpoCand = 256;                        // overlap candidates an atom may have (ranked, then cut to 80)
 constexpr double kBornScale = 1099511627776.0;        // 2^40
 constexpr double kInvBornScale = 1.0 / 1099511627776.0;
 
@@ -110,6 +111,8 @@ struct LcpoView {
   double *s = nullptr;                 // [N * kLcpoMax] overlap areas (A^2)
   double *sasa = nullptr;              // [N] A^2 of the last evaluation
   double *deriv = nullptr;             // [3N] SASAderiv (kcal/mol/A; x, y, z blocks) of the last full one
+  int *cand_n = nullptr;               // [N] candidates gathered from the tiles (0 between evaluations)
+  int *cand = nullptr;                 // [N * kLcpoCand] their indices, in no order
 };
 
 // Where an evaluation takes the reference's WorkSpace::Step from: a device
@@ -346,9 +349,12 @@ void launch_bonded_terms(const PackView &v, cudaStream_t st);
 // FF_SASA_LCPO: overlap lists then areas and derivatives for the systems
 // whose step is due (energy_only: the calcEnergies path, always evaluated);
 // the other systems add their held derivatives to the forces.
-void launch_lcpo(const PackView &v, cudaStream_t st, StepSrc step, bool energy_only);
-// one of the two launches (0: overlap lists, 1: areas and derivatives)
-void launch_lcpo_part(const PackView &v, cudaStream_t st, StepSrc step, bool energy_only, int part);
+// from_tiles: the overlap candidates come from the cluster-pair tiles of
+// the last tile search (the CSR rows were not built), else from the rows.
+void launch_lcpo(const PackView &v, cudaStream_t st, StepSrc step, bool energy_only, bool from_tiles);
+// one of the two phases (0: overlap lists, 1: areas and derivatives)
+void launch_lcpo_part(const PackView &v, cudaStream_t st, StepSrc step, bool energy_only, bool from_tiles,
+                      int part);
 // energies: per-atom / per-term energies into the per-system record
 // (mode = EnergyMode bits); hist/step_dev only with EM_RECORD
 void launch_energy(const PackView &v, cudaStream_t st, int mode, double *hist = nullptr,

@@ -29,7 +29,6 @@
 namespace pdgpu {
 
 constexpr int kLcpoWarps = 4;    // atoms per block
-constexpr int kLcpoCand = 256;   // overlap candidates one warp ranks
 constexpr int kLcpoQ = 14;       // per-partner terms kept for the ordered sums
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kTwoPi = 2.0 * kPi;
@@ -40,7 +39,49 @@ __device__ __forceinline__ bool lcpo_due(const LcpoView &lc, const StepSrc &ss, 
   return step % lc.update == 0;
 }
 
+// The overlap test of a pair, from either end: the force path compares
+// d^2 with (ri + rj)^2 (lcpo.cpp:713), the energy path d with ri + rj
+// (lcpo.cpp:460); d^2 takes the same value from both ends.
 template <bool EO>
+__device__ __forceinline__ bool lcpo_overlaps(double d2, double rs) {
+  return EO ? sqrt(d2) < rs : d2 < rs * rs;
+}
+
+// Overlap candidates from the tiles of the last tile search: each list pair
+// (one tile bit, stored once) that overlaps is appended to both atoms'
+// candidate buffers; k_lcpo_list ranks them.  One warp per tile, lane l
+// for the i-cluster's atom l.
+template <bool EO>
+__global__ void __launch_bounds__(128) k_lcpo_cand_tiles(PackView v, StepSrc ss) {
+  if (v.flags[F_NL_OVERFLOW]) return;
+  const LcpoView &lc = v.lc;
+  const int lane = threadIdx.x & 31;
+  const int T = v.tile_count[0];
+  const int W = gridDim.x * (blockDim.x >> 5);
+  for (int e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); e < T; e += W) {
+    const int4 m = v.tile_meta[e];
+    const int s = m.w >> 8, na = ((m.w >> 3) & 31) + 1, nb = (m.w & 7) + 1;
+    if (!EO && !lcpo_due(lc, ss, s)) continue;
+    if (lane >= na) continue;
+    const int i = m.z + lane;
+    unsigned row = reinterpret_cast<const unsigned char *>(v.tile_rows)[32 * (size_t)e + lane];
+    if (!row || !lc.use[i]) continue;
+    const double xi = v.x[i], yi = v.y[i], zi = v.z[i], ri = lc.r[i];
+    for (int t = 0; t < nb; t++) {
+      if (!((row >> t) & 1u)) continue;
+      const int j = m.x + t;
+      if (!lc.use[j]) continue;
+      const double g = xi - v.x[j], h = yi - v.y[j], k = zi - v.z[j];
+      if (!lcpo_overlaps<EO>(g * g + h * h + k * k, ri + lc.r[j])) continue;
+      const int qi = atomicAdd(&lc.cand_n[i], 1);
+      if (qi < kLcpoCand) lc.cand[(size_t)i * kLcpoCand + qi] = j;
+      const int qj = atomicAdd(&lc.cand_n[j], 1);
+      if (qj < kLcpoCand) lc.cand[(size_t)j * kLcpoCand + qj] = i;
+    }
+  }
+}
+
+template <bool EO, bool TILES>
 __global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_list(PackView v, StepSrc ss) {
   __shared__ int cand[kLcpoWarps][kLcpoCand];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -54,26 +95,31 @@ __global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_list(PackView v, StepS
     return;
   }
   const double xi = v.x[i], yi = v.y[i], zi = v.z[i], ri = lc.r[i];
-  const long long r0 = v.row_start[i];
-  const int rn = v.row_cnt[i];
   int n = 0;
-  for (int q0 = 0; q0 < rn; q0 += 32) {
-    const int q = q0 + lane;
-    bool hit = false;
-    int j = 0;
-    if (q < rn) {
-      j = (int)(v.nl[r0 + q] >> 3);
-      if (lc.use[j]) {
-        const double g = xi - v.x[j], h = yi - v.y[j], k = zi - v.z[j];
-        const double d2 = g * g + h * h + k * k;
-        const double rs = ri + lc.r[j];
-        hit = EO ? sqrt(d2) < rs : d2 < rs * rs;
+  if (TILES) {
+    n = lc.cand_n[i];
+    for (int q = lane; q < min(n, kLcpoCand); q += 32) cand[warp][q] = lc.cand[(size_t)i * kLcpoCand + q];
+    __syncwarp();
+    if (lane == 0) lc.cand_n[i] = 0;  // clean for the next evaluation
+  } else {
+    const long long r0 = v.row_start[i];
+    const int rn = v.row_cnt[i];
+    for (int q0 = 0; q0 < rn; q0 += 32) {
+      const int q = q0 + lane;
+      bool hit = false;
+      int j = 0;
+      if (q < rn) {
+        j = (int)(v.nl[r0 + q] >> 3);
+        if (lc.use[j]) {
+          const double g = xi - v.x[j], h = yi - v.y[j], k = zi - v.z[j];
+          hit = lcpo_overlaps<EO>(g * g + h * h + k * k, ri + lc.r[j]);
+        }
       }
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
+      const int at = n + __popc(m & ((1u << lane) - 1u));
+      if (hit && at < kLcpoCand) cand[warp][at] = j;
+      n += __popc(m);
     }
-    const unsigned m = __ballot_sync(0xffffffffu, hit);
-    const int at = n + __popc(m & ((1u << lane) - 1u));
-    if (hit && at < kLcpoCand) cand[warp][at] = j;
-    n += __popc(m);
   }
   if (n > kLcpoCand) {
     if (lane == 0) atomicExch(&v.flags[F_LCPO_CAND], 1);
@@ -279,24 +325,45 @@ __global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_eval(PackView v, StepS
   }
 }
 
-void launch_lcpo_part(const PackView &v, cudaStream_t st, StepSrc step, bool energy_only, int part) {
+void launch_lcpo_part(const PackView &v, cudaStream_t st, StepSrc step, bool energy_only, bool from_tiles,
+                      int part) {
   if (v.lc.update <= 0 || !v.lc.n_used) return;
   const int blocks = (v.lc.n_used + kLcpoWarps - 1) / kLcpoWarps;
+  const int tpb = kLcpoWarps * 32;
   if (part == 0) {
-    if (energy_only)
-      PDGPU_LAUNCH(k_lcpo_list<true>, blocks, kLcpoWarps * 32, 0, st, v, step);
-    else
-      PDGPU_LAUNCH(k_lcpo_list<false>, blocks, kLcpoWarps * 32, 0, st, v, step);
+    if (from_tiles) {
+      static int sms = 0;  // a persistent grid: eight 4-warp blocks per SM
+      if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+      }
+      if (energy_only)
+        PDGPU_LAUNCH(k_lcpo_cand_tiles<true>, 8 * sms, 128, 0, st, v, step);
+      else
+        PDGPU_LAUNCH(k_lcpo_cand_tiles<false>, 8 * sms, 128, 0, st, v, step);
+    }
+    if (energy_only) {
+      if (from_tiles)
+        PDGPU_LAUNCH((k_lcpo_list<true, true>), blocks, tpb, 0, st, v, step);
+      else
+        PDGPU_LAUNCH((k_lcpo_list<true, false>), blocks, tpb, 0, st, v, step);
+    } else {
+      if (from_tiles)
+        PDGPU_LAUNCH((k_lcpo_list<false, true>), blocks, tpb, 0, st, v, step);
+      else
+        PDGPU_LAUNCH((k_lcpo_list<false, false>), blocks, tpb, 0, st, v, step);
+    }
   } else {
     if (energy_only)
-      PDGPU_LAUNCH(k_lcpo_eval<true>, blocks, kLcpoWarps * 32, 0, st, v, step);
+      PDGPU_LAUNCH(k_lcpo_eval<true>, blocks, tpb, 0, st, v, step);
     else
-      PDGPU_LAUNCH(k_lcpo_eval<false>, blocks, kLcpoWarps * 32, 0, st, v, step);
+      PDGPU_LAUNCH(k_lcpo_eval<false>, blocks, tpb, 0, st, v, step);
   }
 }
-void launch_lcpo(const PackView &v, cudaStream_t st, StepSrc step, bool energy_only) {
-  launch_lcpo_part(v, st, step, energy_only, 0);
-  launch_lcpo_part(v, st, step, energy_only, 1);
+void launch_lcpo(const PackView &v, cudaStream_t st, StepSrc step, bool energy_only, bool from_tiles) {
+  launch_lcpo_part(v, st, step, energy_only, from_tiles, 0);
+  launch_lcpo_part(v, st, step, energy_only, from_tiles, 1);
 }
 
 }  // namespace pdgpu

@@ -181,8 +181,7 @@ void pdgpu_server::fail(Job *j, int status, const std::string &msg) {
 // A job on the tile layout (systems within the search limit) rebuilds by
 // tile search: no list, no size read-back.
 static bool tile_search_job(const Pack &P) {
-  return P.v.tile_mode && P.v.tile_meta && P.v.n_sc > 0 && P.v.max_sys_atoms <= kTileSearchMaxAtoms &&
-         P.v.lc.update <= 0;  // the LCPO term reads the CSR rows
+  return P.v.tile_mode && P.v.tile_meta && P.v.n_sc > 0 && P.v.max_sys_atoms <= kTileSearchMaxAtoms;
 }
 static void rebuild_pairs(Pack &P, cudaStream_t st) {
   if (tile_search_job(P)) {
@@ -191,6 +190,7 @@ static void rebuild_pairs(Pack &P, cudaStream_t st) {
   } else {
     launch_nlist_count(P, st);
     launch_nlist_fill(P, st);
+    P.csr_stale = false;
   }
 }
 
@@ -710,7 +710,7 @@ int pdgpu_serve_submit(pdgpu_server *s, int32_t sys, const pdgpu_job *job, const
     int64_t nsc = ((int64_t)n + 31) / 32, njc = ((int64_t)n + 7) / 8, tiles = 0;
     for (int64_t k = 0; k < nsc; k++) tiles += njc - 4 * k;
     j->est_bytes = (int64_t)n * (1024 + 256 * 4) + tiles * 48 + nsc * 16 * 64 + (int64_t)4 * 1024 * 1024;
-    if (host->lcpo_update > 0) j->est_bytes += (int64_t)n * (kLcpoMax * 12 + 96);
+    if (host->lcpo_update > 0) j->est_bytes += (int64_t)n * (kLcpoMax * 12 + kLcpoCand * 4 + 96);
   }
   if (j->est_bytes > s->prm.hbm_budget) {
     set_error("pdgpu_serve_submit: the job alone exceeds the HBM budget");

@@ -53,18 +53,23 @@ def _oracle(a, pos, ptr, data, energy_only=False, p=None):
 
 
 @pytest.mark.parametrize("dense", [False, True])
-def test_lcpo_alone_bit_exact(gpu_ctx, dense):
+@pytest.mark.parametrize("path", [0, 1])
+def test_lcpo_alone_bit_exact(gpu_ctx, dense, path):
+    """path 0: overlap candidates from the list rows; 1: from the tiles of a
+    tile search (the rows are then built only for the export below)."""
     ws, ff, sasa, a = _ws(gpu_ctx, with_gb=False)
     pre = "lcpo_dense_" if dense else "lcpo_"
     pos = a["lcpo_dense_pos"] if dense else a["pos"]
     ws.cur.p[:] = pos
     ws._pos_dirty = True
     ws.nlist().calcNewList()
-    ptr, data = ws.nlist().getData(shadow=True)
+    ws.setPairPath(path)
+    ws.nlist().calcNewList()  # on the tile layout: a tile search, no rows
     ref_ptr, ref_data = (a["lcpo_dense_nl_ptr"], a["lcpo_dense_nl_data"]) if dense else (a["nl_ptr"], a["nl_data"])
     ws.Step = 0
     ff.calcForces()
     area, deriv = sasa.sasa()
+    ptr, data = ws.nlist().getData(shadow=True)
     o_area, o_deriv, o_e, lost = _oracle(a, pos, ptr, data)
     assert (lost > 0) == dense  # the dense packing overflows 80-partner lists
     assert np.array_equal(area, o_area)
@@ -76,6 +81,8 @@ def test_lcpo_alone_bit_exact(gpu_ctx, dense):
     assert ws.ene.epot_surf == pytest.approx(a[pre + "ene"][10], rel=1e-12)
     assert ws.ene.epot == pytest.approx(a[pre + "ene"][0], rel=1e-12)
     # the energies path (calcEnergies): its own overlap formula, no forces
+    if path == 1:
+        ws.nlist().calcNewList()  # tiles again
     ff.calcEnergies()
     e_area, _ = sasa.sasa()
     o2, _, _, _ = _oracle(a, pos, ptr, data, energy_only=True)
