@@ -111,6 +111,7 @@ struct LcpoView {
   double *s = nullptr;                 // [N * kLcpoMax] overlap areas (A^2)
   double *sasa = nullptr;              // [N] A^2 of the last evaluation
   double *deriv = nullptr;             // [3N] SASAderiv (kcal/mol/A; x, y, z blocks) of the last full one
+  double4 *xr = nullptr;               // [N] (x, y, z, r) of the heavy atoms at the last evaluation
   int *cand_n = nullptr;               // [N] candidates gathered from the tiles (0 between evaluations)
   int *cand = nullptr;                 // [N * kLcpoCand] their indices, in no order
 };

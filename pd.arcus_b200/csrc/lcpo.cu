@@ -66,12 +66,14 @@ __global__ void __launch_bounds__(128) k_lcpo_cand_tiles(PackView v, StepSrc ss)
     const int i = m.z + lane;
     unsigned row = reinterpret_cast<const unsigned char *>(v.tile_rows)[32 * (size_t)e + lane];
     if (!row || !lc.use[i]) continue;
-    const double xi = v.x[i], yi = v.y[i], zi = v.z[i], ri = lc.r[i];
+    const double4 pi = v.xyzp[i];
+    const double ri = lc.r[i];
     for (int t = 0; t < nb; t++) {
       if (!((row >> t) & 1u)) continue;
       const int j = m.x + t;
       if (!lc.use[j]) continue;
-      const double g = xi - v.x[j], h = yi - v.y[j], k = zi - v.z[j];
+      const double4 pj = v.xyzp[j];
+      const double g = pi.x - pj.x, h = pi.y - pj.y, k = pi.z - pj.z;
       if (!lcpo_overlaps<EO>(g * g + h * h + k * k, ri + lc.r[j])) continue;
       const int qi = atomicAdd(&lc.cand_n[i], 1);
       if (qi < kLcpoCand) lc.cand[(size_t)i * kLcpoCand + qi] = j;
@@ -94,7 +96,9 @@ __global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_list(PackView v, StepS
     if (lane == 0) lc.cnt[i] = 0;
     return;
   }
-  const double xi = v.x[i], yi = v.y[i], zi = v.z[i], ri = lc.r[i];
+  const double4 pi = v.xyzp[i];  // (x, y, z) as in v.x, v.y, v.z
+  const double xi = pi.x, yi = pi.y, zi = pi.z, ri = lc.r[i];
+  if (lane == 0) lc.xr[i] = make_double4(xi, yi, zi, ri);  // for the evaluation's gathers
   int n = 0;
   if (TILES) {
     n = lc.cand_n[i];
@@ -111,7 +115,8 @@ __global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_list(PackView v, StepS
       if (q < rn) {
         j = (int)(v.nl[r0 + q] >> 3);
         if (lc.use[j]) {
-          const double g = xi - v.x[j], h = yi - v.y[j], k = zi - v.z[j];
+          const double4 pj = v.xyzp[j];
+          const double g = xi - pj.x, h = yi - pj.y, k = zi - pj.z;
           hit = lcpo_overlaps<EO>(g * g + h * h + k * k, ri + lc.r[j]);
         }
       }
@@ -133,7 +138,8 @@ __global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_list(PackView v, StepS
     int rank = 0;
     for (int t = 0; t < n; t++) rank += cand[warp][t] < j;
     if (rank >= kLcpoMax) continue;
-    const double g = xi - v.x[j], h = yi - v.y[j], k = zi - v.z[j];
+    const double4 pj = v.xyzp[j];
+    const double g = xi - pj.x, h = yi - pj.y, k = zi - pj.z;
     const double d = sqrt(g * g + h * h + k * k);
     const double rj = lc.r[j];
     double s;
@@ -187,7 +193,8 @@ __global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_eval(PackView v, StepS
     return;
   }
   double(*W)[kLcpoMax + 1] = T[warp];
-  const double xi = v.x[i], yi = v.y[i], zi = v.z[i], ri = lc.r[i];
+  const double4 pi4 = lc.xr[i];
+  const double xi = pi4.x, yi = pi4.y, zi = pi4.z, ri = pi4.w;
   const int cnt = lc.cnt[i];
   const size_t base = (size_t)i * kLcpoMax;
   for (int e = lane; e < cnt; e += 32) {
@@ -201,13 +208,15 @@ __global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_eval(PackView v, StepS
       for (int k = 0; k < nj; k++) {
         const int ka = lc.idx[jb + k];
         if (ka == i) continue;
-        const double g = v.x[ka] - xi, h = v.y[ka] - yi, q = v.z[ka] - zi;
-        if (ri + lc.r[ka] < sqrt(g * g + h * h + q * q)) continue;
+        const double4 pk = lc.xr[ka];
+        const double g = pk.x - xi, h = pk.y - yi, q = pk.z - zi;
+        if (ri + pk.w < sqrt(g * g + h * h + q * q)) continue;
         si3 += lc.s[jb + k];
       }
     } else {
       // lcpo.cpp:772-901
-      const double xj = v.x[ja], yj = v.y[ja], zj = v.z[ja], rj = lc.r[ja];
+      const double4 pj4 = lc.xr[ja];
+      const double xj = pj4.x, yj = pj4.y, zj = pj4.z, rj = pj4.w;
       const double gx = xj - xi, gy = yj - yi, gz = zj - zi;
       const double dij = sqrt(gx * gx + gy * gy + gz * gz);
       const double invij = 1 / dij;
@@ -221,9 +230,20 @@ __global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_eval(PackView v, StepS
       const double a2x = dAdd * ddx, a2y = dAdd * ddy, a2z = dAdd * ddz;
       double d3x = 0, d3y = 0, d3z = 0, d3bx = 0, d3by = 0, d3bz = 0, d4bx = 0, d4by = 0, d4bz = 0;
       double s3ik = 0.0;
+      // the next partner's index, record and overlap are loaded one
+      // iteration ahead
+      int kn = nj > 0 ? lc.idx[jb] : 0;
+      double4 pn = nj > 0 ? lc.xr[kn] : make_double4(0, 0, 0, 0);
+      double sn = nj > 0 ? lc.s[jb] : 0.0;
       for (int k = 0; k < nj; k++) {
-        const int ka = lc.idx[jb + k];
-        const double xk = v.x[ka], yk = v.y[ka], zk = v.z[ka], rk = lc.r[ka];
+        const int ka = kn;
+        const double xk = pn.x, yk = pn.y, zk = pn.z, rk = pn.w;
+        const double sjk = sn;
+        if (k + 1 < nj) {
+          kn = lc.idx[jb + k + 1];
+          pn = lc.xr[kn];
+          sn = lc.s[jb + k + 1];
+        }
         if (ka == i) continue;
         const double g = xk - xi, h = yk - yi, q = zk - zi;
         double dik = g * g + h * h + q * q;
@@ -233,7 +253,6 @@ __global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_eval(PackView v, StepS
         const double hk = (ri * ri - rk * rk) * (invik * invik);
         dAdd = kPi * ri * (hk - 1);
         const double dkx = -(xi - xk) * invik, dky = -(yi - yk) * invik, dkz = -(zi - zk) * invik;
-        const double sjk = lc.s[jb + k];
         d3x += dAdd * dkx;
         d3y += dAdd * dky;
         d3z += dAdd * dkz;

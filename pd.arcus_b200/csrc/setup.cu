@@ -280,7 +280,8 @@ int pack_upload_lcpo(Pack *p, const std::vector<const SystemHost *> &systems) {
         palloc(p, &use, N) != cudaSuccess || palloc(p, &atoms, N) != cudaSuccess || palloc(p, &lc.cnt, N) != cudaSuccess ||
         palloc(p, &lc.idx, N * kLcpoMax) != cudaSuccess || palloc(p, &lc.s, N * kLcpoMax) != cudaSuccess ||
         palloc(p, &lc.sasa, N) != cudaSuccess || palloc(p, &lc.deriv, 3 * N) != cudaSuccess ||
-        palloc(p, &lc.cand_n, N) != cudaSuccess || palloc(p, &lc.cand, N * kLcpoCand) != cudaSuccess) {
+        palloc(p, &lc.cand_n, N) != cudaSuccess || palloc(p, &lc.cand, N * kLcpoCand) != cudaSuccess ||
+        palloc(p, &lc.xr, N) != cudaSuccess) {
       set_error("device allocation failed (LCPO surface term)");
       return PDGPU_ERR_NOMEM;
     }
