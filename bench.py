@@ -15,7 +15,9 @@ Extra keys of the same JSON line:
               x 64 backbone phi/psi trials (sigma 15 deg) drawn on the device:
               32,768 energy+force evaluations, Rc 12 A, in 64 batched
               evaluations of all 512 systems; against the plain path (one
-              system per launch sequence) on a sample.
+              system per launch sequence) on a sample.  device_mc: the same
+              batch through the whole Monte Carlo protocol on the device
+              (64 steps, Metropolis at 300 K, pdgpu_mc_run).
   batched_md  256 peptide systems (16 copies of each of the 16 OPLS-AA
               peptides of tests/golden/lib16_opls_s4.npz, 30-150 residues),
               Langevin 1 fs, gamma 1/ps, 300 K, Rc 12 A, list every 10 steps,
@@ -169,6 +171,16 @@ def bench_batched_sp(pdgpu, A, ctx, torch, copies=32, trials=64, plain_trials=2)
     lc1 = ctypes.c_int64(0)
     L.pdgpu_launch_count(ctx.ptr, ctypes.byref(lc1))
     evals = nsys * trials
+    # the whole Monte Carlo protocol on the device (moves, list, forces,
+    # Metropolis at 300 K per system; one host read per 16 steps)
+    b.setPositions(b.positions())
+    torch.cuda.synchronize()
+    t_mc = time.perf_counter()
+    acc, low = b.runMC(trials, temperature=300.0, sigma=sigma)
+    t_mc = time.perf_counter() - t_mc
+    mc = {"metric": "device Monte Carlo evals/s (pdgpu_mc_run)", "value": nsys * trials / t_mc, "unit": "evals/s",
+          "steps": trials, "acceptance": float(acc.sum()) / (nsys * trials),
+          "device_ms": ctx.last_run_ms(), "timing": "wall clock around the call"}
     # plain path: one system per launch sequence (perturb, list, forces,
     # read); an untimed first evaluation per system tunes its kernels
     plain = []
@@ -200,6 +212,7 @@ def bench_batched_sp(pdgpu, A, ctx, torch, copies=32, trials=64, plain_trials=2)
             "plain_one_system_per_launch": {"value": n_plain / t_plain, "unit": "evals/s", "sample_evals": n_plain,
                                             "latency_ms": {"p50": 1e3 * pctl(plain, 50), "p99": 1e3 * pctl(plain, 99)}},
             "speedup_vs_plain": (evals / t_all) / (n_plain / t_plain),
+            "device_mc": dict(mc, speedup_vs_plain=(nsys * trials / t_mc) / (n_plain / t_plain)),
             "gpu_launches": int(lc1.value - lc0.value),
             "parity": {"force_rel_rms_vs_fp64_max": worst,
                        "case": "reference trial 0 of each of the 16 peptides, angles from the reference run"},

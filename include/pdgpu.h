@@ -174,6 +174,33 @@ int pdgpu_save_base_positions(pdgpu_ctx *ctx, int32_t sys);
 int pdgpu_perturb_torsions(pdgpu_ctx *ctx, int32_t sys, double sigma, uint64_t trial,
                            const double *angles);
 
+/* MonteCarlo (protocols/montecarlo.h:36-125, run_core montecarlo.cpp:24-141)
+ * with the phi/psi moves above as the move set and a list rebuild plus
+ * Forcefield::calcForces as the evaluator, for every system of the handle
+ * at once on the device.  Step 0 evaluates the starting state; step t > 0
+ * perturbs the last accepted state by sigma * N(0,1) per rotation (counter
+ * t, the system's RNG key).  MonteCarlo::accept (montecarlo.cpp:143-159) per
+ * system: non-finite energies are rejected, lower ones accepted, otherwise
+ * d = (E_old - E_new) / kB T is rejected below -50 and else accepted when a
+ * uniform [0, 1) draw (Philox, keyed like the moves; the reference uses
+ * rand()) is below e^d.  Temperature is a constant profile.  The handle
+ * ends in FinalState (Last, LastAcc, LowestEpot) with its forces and
+ * energies evaluated there.  accepted[nsys] receives the acceptances,
+ * lowest[nsys] the lowest accepted epot (J); either may be NULL. */
+#define PDGPU_MC_LAST 0
+#define PDGPU_MC_LAST_ACC 1
+#define PDGPU_MC_LOWEST_EPOT 2
+typedef struct {
+  int32_t Steps;
+  int32_t FinalState;  /* PDGPU_MC_*; default LastAcc (montecarlo.h:53) */
+  double Temperature;  /* K; default 300 */
+  double Sigma;        /* rad, standard deviation of each phi/psi change; default 15 deg */
+  uint64_t Seed;       /* RNG keys base + member index, unless pdgpu_set_seeds gave keys */
+} pdgpu_mc_params;
+void pdgpu_mc_params_default(pdgpu_mc_params *p);
+int pdgpu_mc_run(pdgpu_ctx *ctx, int32_t sys, const pdgpu_mc_params *p, int32_t *accepted,
+                 double *lowest);
+
 /* State transfer (WorkSpace::cur.atom[i].p / .v / .f, snapshot.h:16-22). */
 int pdgpu_set_positions(pdgpu_ctx *ctx, int32_t sys, const double *xyz);
 int pdgpu_get_positions(pdgpu_ctx *ctx, int32_t sys, double *xyz);

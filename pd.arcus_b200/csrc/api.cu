@@ -1,5 +1,6 @@
 // C ABI of libpdgpu (declared in include/pdgpu.h) and the protocol runners.
 #include <algorithm>
+#include <limits>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -1817,6 +1818,127 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
   c->last_ms = ms;
   if (steps_taken)
     for (int s = 0; s < S; s++) steps_taken[s] = taken[s];
+  return PDGPU_OK;
+}
+
+// ------------------------------------------------------------ Monte Carlo
+void pdgpu_mc_params_default(pdgpu_mc_params *p) {
+  if (!p) return;
+  p->Steps = 0;
+  p->FinalState = PDGPU_MC_LAST_ACC;  // montecarlo.h:53
+  p->Temperature = 300.0;             // ConstantProfile(300), montecarlo.h:52
+  p->Sigma = 15.0 * 3.14159265358979323846 / 180.0;
+  p->Seed = 0;
+}
+
+// MonteCarlo::run_core (protocols/montecarlo.cpp:24-141) for every system of
+// the handle at once, on the device: each step perturbs the phi/psi of the
+// last accepted state (step 0 evaluates it unperturbed), rebuilds the list,
+// evaluates the forcefield and applies the Metropolis test per system.  The
+// host reads one flag block per 16 steps.
+int pdgpu_mc_run(pdgpu_ctx *c, int32_t sys, const pdgpu_mc_params *p, int32_t *accepted, double *lowest) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (!p || p->Steps < 1 || !(p->Temperature > 0) || !(p->Sigma >= 0) || p->FinalState < 0 || p->FinalState > 2) {
+    set_error("invalid Monte Carlo parameters (Steps >= 1, Temperature > 0, Sigma >= 0, FinalState 0..2)");
+    return PDGPU_ERR_ARG;
+  }
+  Pack &P = *e->pack;
+  PackView &v = P.v;
+  const int S = e->nsys();
+  const size_t n = (size_t)v.n_atoms;
+  if (!e->mc_state) {
+    unsigned char *m = nullptr;
+    PDGPU_CUDA(xalloc(e, &m, mc_state_size() * S));
+    e->mc_state = m;
+  }
+  PDGPU_CUDA(cudaMemsetAsync(e->mc_state, 0, mc_state_size() * S, c->st));
+  int r = default_seeds(c, e, p->Seed);
+  if (r) return r;
+  if (!P.have_list || P.nl_total < 0) {
+    if ((r = nlist_enqueue(c, e, true))) return r;
+  }
+  if ((r = ready_pairs(c, e))) return r;
+  // the starting state is the first base (and lowest) state
+  PDGPU_CUDA(cudaMemcpyAsync(v.bx, v.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(v.by, v.y, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(v.bz, v.z, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(v.ox, v.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(v.oy, v.y, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
+  PDGPU_CUDA(cudaMemcpyAsync(v.oz, v.z, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
+  PDGPU_CUDA(cudaMemsetAsync(v.flags, 0, sizeof(int) * F_COUNT, c->st));
+  const Consts &k = consts();
+  const double inv_kT = k.J_per_kcalmol / (k.kB * p->Temperature);  // per kcal/mol
+  const int keep_lowest = p->FinalState == PDGPU_MC_LOWEST_EPOT;
+  std::vector<unsigned char> hs(mc_state_size() * S);
+  cudaEventRecord(P.ev0, c->st);
+  int step = 0, regrow = 0;
+  while (step < p->Steps) {
+    const int chunk = std::min(16, p->Steps - step);
+    for (int q = 0; q < chunk; q++) {
+      const int t = step + q;
+      if (t != 0) launch_torsion_moves(v, c->st, p->Sigma, (unsigned long long)t, e->seeds, nullptr);
+      rebuild_enqueue(P, c->st);  // the evaluator's list refresh
+      StepSrc ws;
+      ws.imm = t;  // WorkSpace::Step = Step (montecarlo.cpp:37)
+      calc_forces_enqueue(c->st, e, true, ws);
+      launch_mc_accept(v, c->st, e->mc_state, t, inv_kT, e->seeds, keep_lowest);
+    }
+    int flags[F_COUNT];
+    PDGPU_CUDA(cudaMemcpyAsync(flags, v.flags, sizeof flags, cudaMemcpyDeviceToHost, c->st));
+    PDGPU_CUDA(cudaMemcpyAsync(hs.data(), e->mc_state, hs.size(), cudaMemcpyDeviceToHost, c->st));
+    if ((r = sync_check(c, "mc_run"))) return r;
+    if (flags[F_LCPO_CAND]) {
+      set_error(kLcpoCandMsg);
+      return PDGPU_ERR_STATE;
+    }
+    if (flags[F_NL_OVERFLOW]) {
+      // the steps from the overflowing rebuild on did nothing: grow the list
+      // and go on from the first of them (its base state is untouched)
+      if (++regrow > 8) {
+        set_error("neighbour list kept overflowing during Monte Carlo");
+        return PDGPU_ERR_STATE;
+      }
+      int acc, done, ls;
+      double low;
+      mc_state_read(hs.data(), 0, &acc, &done, &low, &ls);
+      if ((r = nlist_enqueue(c, e, true))) return r;
+      PDGPU_CUDA(cudaMemsetAsync(v.flags + F_NL_OVERFLOW, 0, sizeof(int), c->st));
+      step = done;
+      continue;
+    }
+    step += chunk;
+  }
+  // the final state (montecarlo.cpp:113-133), evaluated again
+  if (p->FinalState == PDGPU_MC_LAST_ACC)
+    launch_mc_restore(v, c->st);
+  else if (p->FinalState == PDGPU_MC_LOWEST_EPOT)
+    launch_min_finish(v, c->st);
+  rebuild_enqueue(P, c->st);
+  StepSrc ws;
+  ws.imm = p->Steps - 1;
+  calc_forces_enqueue(c->st, e, true, ws);
+  cudaEventRecord(P.ev1, c->st);
+  int flags[F_COUNT];
+  PDGPU_CUDA(cudaMemcpyAsync(flags, v.flags, sizeof flags, cudaMemcpyDeviceToHost, c->st));
+  if ((r = sync_check(c, "mc_run final"))) return r;
+  if (flags[F_NL_OVERFLOW]) {  // the final state's list: sized, then evaluated again
+    if ((r = nlist_enqueue(c, e, true))) return r;
+    calc_forces_enqueue(c->st, e, true, ws);
+    if ((r = sync_check(c, "mc_run final"))) return r;
+  }
+  float ms = 0;
+  cudaEventElapsedTime(&ms, P.ev0, P.ev1);
+  P.last_run_ms = ms;
+  c->last_ms = ms;
+  e->ws_step = p->Steps - 1;
+  for (int s = 0; s < S; s++) {
+    int acc, done, ls;
+    double low;
+    mc_state_read(hs.data(), s, &acc, &done, &low, &ls);
+    if (accepted) accepted[s] = acc;
+    if (lowest) lowest[s] = acc ? low * k.J_per_kcalmol : std::numeric_limits<double>::quiet_NaN();
+  }
   return PDGPU_OK;
 }
 

@@ -26,6 +26,12 @@ void launch_min_finish(const PackView &v, cudaStream_t st);
 // minimisation: the step being evaluated, or (last) the last step taken
 StepSrc min_step_src(const void *ms, bool last);
 int min_state_last(const void *host_buf, int s);
+// Monte Carlo (moves.cu): per-system Metropolis state
+size_t mc_state_size();
+void launch_mc_accept(const PackView &v, cudaStream_t st, void *m, int step, double inv_kT,
+                      const unsigned long long *keys, int keep_lowest);
+void launch_mc_restore(const PackView &v, cudaStream_t st);
+void mc_state_read(const void *buf, int s, int *accepted, int *done, double *lowest_kcal, int *low_step);
 size_t min_state_size();
 void min_state_init(void *host_buf, int n);
 void min_state_read(const void *host_buf, int s, int *taken, int *nan, double *mult);
@@ -76,6 +82,7 @@ struct SysEntry {
     traj_pending = false;
   }
   void *min_state = nullptr;
+  void *mc_state = nullptr;
   std::vector<void *> extra;
   // cached MD block graph
   cudaGraph_t graph = nullptr;
@@ -100,6 +107,7 @@ struct SysEntry {
     hist = nullptr;
     hist_cap = 0;
     min_state = nullptr;
+    mc_state = nullptr;
     pack.reset();
   }
   ~SysEntry() { free_device(); }

@@ -114,4 +114,92 @@ void launch_torsion_moves(const PackView &v, cudaStream_t st, double sigma, unsi
   PDGPU_LAUNCH(k_torsion_apply, (v.n_atoms + 255) / 256, 256, 0, st, v);
 }
 
+// ------------------------------------------------------------ Metropolis
+// MonteCarlo::accept (protocols/montecarlo.cpp:143-159) for every system of
+// the pack, on the energy record of the step's evaluation: a non-finite
+// energy is rejected; a lower one accepted; otherwise d = (E_old - E_new) /
+// kB T, rejected when d < -50, else accepted when u < e^d with u uniform in
+// [0, 1) from Philox keyed by the system's key and the step (the reference
+// draws it with rand()).  Step 0 (no move) is accepted when finite.
+// An accepted step moves the system's base positions (the state the next
+// trial perturbs) to the current ones; with keep_lowest the lowest-energy
+// state also goes to the saved positions (o*).
+struct MCSys {
+  double old_e, low_e;  // kcal/mol
+  int acc, last, done, low_step;
+};
+size_t mc_state_size() { return sizeof(MCSys); }
+
+__global__ void k_mc_accept(PackView v, MCSys *m, int step, double inv_kT, const unsigned long long *keys) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= v.n_sys || v.flags[F_NL_OVERFLOW]) return;
+  MCSys &q = m[s];
+  const double e = v.ene[(size_t)s * E_COUNT + E_EPOT];
+  bool ok = e == e && fabs(e) <= 1.79e308;
+  if (ok && step != 0 && !(e < q.old_e)) {
+    const double d = (q.old_e - e) * inv_kT;
+    if (d < -50.0) {
+      ok = false;
+    } else {
+      const unsigned long long k = keys[s];
+      U4 r = philox(U4{(unsigned)step, 0x4D43u, 0x5452u, 0u}, (unsigned)k, (unsigned)(k >> 32));
+      const double u = (double)(((unsigned long long)r.a << 21) ^ (unsigned long long)(r.b >> 11)) *
+                       (1.0 / 9007199254740992.0);  // 53 bits
+      ok = u < exp(d);
+    }
+  }
+  q.last = ok ? 1 : 0;
+  q.done = step + 1;
+  if (ok) {
+    q.old_e = e;
+    q.acc++;
+    if (step == 0 || e < q.low_e) {
+      q.low_e = e;
+      q.low_step = step;
+      q.last = 3;  // accepted and the lowest so far
+    }
+  }
+}
+
+__global__ void k_mc_commit(PackView v, const MCSys *m, int keep_lowest) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v.n_atoms || v.flags[F_NL_OVERFLOW]) return;
+  const int last = m[v.sys_of[i]].last;
+  if (!last) return;
+  const double x = v.x[i], y = v.y[i], z = v.z[i];
+  v.bx[i] = x;
+  v.by[i] = y;
+  v.bz[i] = z;
+  if (keep_lowest && last == 3) {
+    v.ox[i] = x;
+    v.oy[i] = y;
+    v.oz[i] = z;
+  }
+}
+
+// the state a Monte Carlo run ends in: the base positions (last accepted)
+__global__ void k_mc_restore(PackView v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v.n_atoms) return;
+  store_pos_mv(v, i, v.bx[i], v.by[i], v.bz[i]);
+}
+void launch_mc_restore(const PackView &v, cudaStream_t st) {
+  if (v.n_atoms) PDGPU_LAUNCH(k_mc_restore, (v.n_atoms + 255) / 256, 256, 0, st, v);
+}
+
+void launch_mc_accept(const PackView &v, cudaStream_t st, void *m, int step, double inv_kT,
+                      const unsigned long long *keys, int keep_lowest) {
+  if (!v.n_sys) return;
+  PDGPU_LAUNCH(k_mc_accept, (v.n_sys + 127) / 128, 128, 0, st, v, (MCSys *)m, step, inv_kT, keys);
+  if (v.n_atoms) PDGPU_LAUNCH(k_mc_commit, (v.n_atoms + 255) / 256, 256, 0, st, v, (const MCSys *)m, keep_lowest);
+}
+// the host's view of one system's state
+void mc_state_read(const void *buf, int s, int *accepted, int *done, double *lowest_kcal, int *low_step) {
+  const MCSys &q = ((const MCSys *)buf)[s];
+  *accepted = q.acc;
+  *done = q.done;
+  *lowest_kcal = q.low_e;
+  *low_step = q.low_step;
+}
+
 }  // namespace pdgpu

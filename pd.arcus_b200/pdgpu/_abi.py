@@ -64,6 +64,14 @@ class MinParams(ctypes.Structure):
                 ("Strictness", ctypes.c_double)]
 
 
+class MCParams(ctypes.Structure):
+    _fields_ = [("Steps", ctypes.c_int32), ("FinalState", ctypes.c_int32), ("Temperature", ctypes.c_double),
+                ("Sigma", ctypes.c_double), ("Seed", ctypes.c_uint64)]
+
+
+MC_LAST, MC_LAST_ACC, MC_LOWEST_EPOT = 0, 1, 2
+
+
 class ServeParams(ctypes.Structure):
     _fields_ = [("hbm_budget", ctypes.c_int64), ("max_active", ctypes.c_int32), ("lanes", ctypes.c_int32 * 3),
                 ("tiles", ctypes.c_int32), ("policy", ctypes.c_int32), ("_reserved", ctypes.c_int32)]
@@ -101,6 +109,8 @@ PROTOTYPES = {
     "pdgpu_ff_params_default": (None, [ctypes.POINTER(FFParams)]),
     "pdgpu_md_params_default": (None, [ctypes.POINTER(MDParams)]),
     "pdgpu_min_params_default": (None, [ctypes.POINTER(MinParams)]),
+    "pdgpu_mc_params_default": (None, [ctypes.POINTER(MCParams)]),
+    "pdgpu_mc_run": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.POINTER(MCParams), _I, _D]),
     "pdgpu_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_CTX)]),
     "pdgpu_ctx_destroy": (ctypes.c_int, [_CTX]),
     "pdgpu_last_error": (ctypes.c_char_p, []),
@@ -238,4 +248,10 @@ def md_params_default():
 def min_params_default():
     p = MinParams()
     lib().pdgpu_min_params_default(ctypes.byref(p))
+    return p
+
+
+def mc_params_default():
+    p = MCParams()
+    lib().pdgpu_mc_params_default(ctypes.byref(p))
     return p

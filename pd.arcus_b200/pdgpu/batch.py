@@ -125,6 +125,21 @@ class Batch:
         A.check(A.lib().pdgpu_perturb_torsions(self.ctx.ptr, self._id, float(sigma), int(trial), ang))
 
     # -- protocols
+    def runMC(self, steps, temperature=300.0, sigma=None, final_state=None, seed=0):
+        """MonteCarlo for every member on the device (pdgpu_mc_run): phi/psi
+        moves, list rebuild + forces as the evaluator, the Metropolis test.
+        Returns (acceptances per member, lowest accepted epot per member, J)."""
+        p = A.mc_params_default()
+        p.Steps, p.Temperature, p.Seed = int(steps), float(temperature), int(seed)
+        if sigma is not None:
+            p.Sigma = float(sigma)
+        if final_state is not None:
+            p.FinalState = int(final_state)
+        acc = np.zeros(self.nSystems, dtype=np.int32)
+        low = np.zeros(self.nSystems)
+        A.check(A.lib().pdgpu_mc_run(self.ctx.ptr, self._id, ctypes.byref(p), A.iptr(acc), A.dptr(low)))
+        return acc, low
+
     def runMD(self, params: A.MDParams, steps, first_step=0, total_steps=None, init_velocities=None):
         """MolecularDynamics::run_core for every member at once; returns the
         (steps, nSystems, 3) history of epot, ekin, etot (J)."""
