@@ -8,7 +8,7 @@ from ._abi import (PdgpuError, UnstableError, lib, last_error, ff_params_default
                    md_params_default, min_params_default, FFParams, MDParams, MinParams)
 from .core import (Context, SystemSpec, WorkSpace, NeighbourList, Hamiltonian,  # noqa: F401
                    ForcefieldBase, Forcefield, FF_Bonded, FF_NonBonded, FF_GeneralizedBorn_Still, FF_SASA_LCPO,
-                   ProtocolBase, Energy, Minimisation, MolecularDynamics, J2KCAL_NA)
+                   ProtocolBase, Energy, Minimisation, MolecularDynamics, MonteCarlo, J2KCAL_NA)
 from .batch import Batch  # noqa: F401
 from .serve import Server  # noqa: F401
 

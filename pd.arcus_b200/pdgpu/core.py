@@ -706,6 +706,45 @@ class Minimisation(ProtocolBase):
         return taken.value
 
 
+class MonteCarlo(ProtocolBase):
+    """MonteCarlo (protocols/montecarlo.h:36-125) with backbone phi/psi moves
+    of every residue (sigma Sigma rad each) as the move set and the
+    forcefield's calcForces after a list rebuild as the evaluator, run on the
+    device (pdgpu_mc_run).  Temperature is constant (K); FinalState is Last,
+    LastAcc (default) or LowestEpot, as in the reference.  After run():
+    acceptances and lowest (the lowest accepted epot, J)."""
+
+    Last, LastAcc, LowestEpot = A.MC_LAST, A.MC_LAST_ACC, A.MC_LOWEST_EPOT
+
+    def __init__(self, ff):
+        super().__init__(ff)
+        d = A.mc_params_default()
+        self.Temperature = d.Temperature
+        self.Sigma = d.Sigma
+        self.FinalState = d.FinalState
+        self.Seed = 0
+        self.acceptances = 0
+        self.lowest = float("nan")
+
+    def runcore(self):
+        ws = self.getWSpace()
+        self.ff.ensuresetup()
+        self.ff._sync_in()
+        if getattr(ws, "nRotations", 0) == 0:
+            ws.setTorsionMoves()
+        p = A.mc_params_default()
+        p.Steps, p.FinalState = int(self.Steps), int(self.FinalState)
+        p.Temperature, p.Sigma, p.Seed = float(self.Temperature), float(self.Sigma), int(self.Seed)
+        acc = np.zeros(1, dtype=np.int32)
+        low = np.zeros(1)
+        A.check(A.lib().pdgpu_mc_run(ws.ctx.ptr, ws._sys, ctypes.byref(p), A.iptr(acc), A.dptr(low)))
+        self.acceptances, self.lowest = int(acc[0]), float(low[0])
+        ws._pull_positions()
+        self.ff._sync_out()
+        ws._pull_step()
+        return int(self.Steps)
+
+
 def read_trajectory(ctx, handle, natoms, max_frames):
     """Frames recorded since the last read: (frames[n][natoms][3] in A,
     steps[n]) and the number overwritten before they were read."""

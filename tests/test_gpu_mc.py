@@ -93,3 +93,21 @@ def test_mc_lowest_state_and_room_temperature(gpu_ctx):
     acc2, low2 = b.runMC(STEPS, temperature=300.0, sigma=SIGMA, final_state=A.MC_LOWEST_EPOT)
     assert np.array_equal(acc, acc2) and np.array_equal(low, low2)
     b.close()
+
+
+def test_mc_protocol_surface(gpu_ctx):
+    """pdgpu.MonteCarlo on one WorkSpace: ends in its lowest accepted state,
+    re-evaluated, and at 1e-30 K that state is never above the start."""
+    import pdgpu
+    a, m = load_library("lib16_amber_s3")[0]
+    ws, ff = build_workspace(a, m, gpu_ctx)
+    ff.calcForces()
+    e0 = ws.ene.epot
+    mc = pdgpu.MonteCarlo(ff)
+    mc.Steps = 12
+    mc.Temperature = 1e-30
+    mc.FinalState = pdgpu.MonteCarlo.LowestEpot
+    mc.run()
+    assert 1 <= mc.acceptances <= 12
+    assert ws.ene.epot == mc.lowest and mc.lowest <= e0
+    assert ws.Step == 11
