@@ -682,34 +682,25 @@ int pdgpu_perturb_torsions(pdgpu_ctx *c, int32_t sys, double sigma, uint64_t tri
 }
 
 // ------------------------------------------------------------ state
+// The caller's interleaved [n][3] buffer moves as one block to or from a
+// device staging array; the device reshuffles it (a page-locked caller
+// buffer is copied by DMA straight from or into its own memory).
 static int copy_soa_in(pdgpu_ctx *c, Pack &P, const double *xyz, double *X, double *Y, double *Z) {
-  int n = P.v.n_atoms;
-  std::vector<double> a(n), b(n), d(n);
-  for (int i = 0; i < n; i++) {
-    a[i] = xyz[3 * i];
-    b[i] = xyz[3 * i + 1];
-    d[i] = xyz[3 * i + 2];
-  }
-  PDGPU_CUDA(cudaMemcpyAsync(X, a.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
-  PDGPU_CUDA(cudaMemcpyAsync(Y, b.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
-  PDGPU_CUDA(cudaMemcpyAsync(Z, d.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
-  return sync_check(c, "copy in");
+  const int n = P.v.n_atoms;
+  int r = pack_ensure_stage(&P);
+  if (r) return r;
+  PDGPU_CUDA(cudaMemcpyAsync(P.stage, xyz, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, c->st));
+  launch_aos_to_soa(P.stage, X, Y, Z, n, c->st);
+  return PDGPU_OK;
 }
 static int copy_soa_out(pdgpu_ctx *c, Pack &P, double *xyz, const double *X, const double *Y,
                         const double *Z) {
-  int n = P.v.n_atoms;
-  std::vector<double> a(n), b(n), d(n);
-  PDGPU_CUDA(cudaMemcpyAsync(a.data(), X, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
-  PDGPU_CUDA(cudaMemcpyAsync(b.data(), Y, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
-  PDGPU_CUDA(cudaMemcpyAsync(d.data(), Z, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
-  int r = sync_check(c, "copy out");
+  const int n = P.v.n_atoms;
+  int r = pack_ensure_stage(&P);
   if (r) return r;
-  for (int i = 0; i < n; i++) {
-    xyz[3 * i] = a[i];
-    xyz[3 * i + 1] = b[i];
-    xyz[3 * i + 2] = d[i];
-  }
-  return PDGPU_OK;
+  launch_soa_to_aos(P.stage, X, Y, Z, n, c->st);
+  PDGPU_CUDA(cudaMemcpyAsync(xyz, P.stage, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, c->st));
+  return sync_check(c, "copy out");
 }
 
 int pdgpu_set_positions(pdgpu_ctx *c, int32_t sys, const double *xyz) {
@@ -743,7 +734,9 @@ int pdgpu_set_velocities(pdgpu_ctx *c, int32_t sys, const double *v) {
     return PDGPU_ERR_ARG;
   }
   Pack &P = *e->pack;
-  return copy_soa_in(c, P, v, P.v.vx, P.v.vy, P.v.vz);
+  int r = copy_soa_in(c, P, v, P.v.vx, P.v.vy, P.v.vz);
+  if (r) return r;
+  return sync_check(c, "set_velocities");
 }
 int pdgpu_get_velocities(pdgpu_ctx *c, int32_t sys, double *v) {
   CHECK_CTX(c);

@@ -278,6 +278,7 @@ struct Pack {
   long long *scan_tmp = nullptr;
   int scan_tmp_len = 0;
   double *red_tmp = nullptr;     // reductions
+  double *stage = nullptr;       // [3N] interleaved staging of the state transfer calls
   // bookkeeping for protocols
   unsigned char *is_h = nullptr; // Particle::isHydrogen per atom
   long long rot_total = 0;       // backbone rotations over all systems
@@ -303,6 +304,8 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
 void pack_set_params(Pack *p, int s, const pdgpu_ff_params &prm);
 // allocate the cluster-pair tile store of a pack (once; enqueued on p->st)
 int pack_ensure_tiles(Pack *p);
+// the state transfer staging array (once; enqueued on p->st)
+int pack_ensure_stage(Pack *p);
 // FF_SASA_LCPO parameters of the members (again after they change)
 int pack_upload_lcpo(Pack *p, const std::vector<const SystemHost *> &systems);
 SysParams make_sys_params(const pdgpu_ff_params &p);
@@ -314,6 +317,8 @@ void host_gb_fixed_terms(SystemHost &s);
 // ----------------------------------------------------------------- launchers
 // All launchers enqueue on `st` and do not synchronise.
 void launch_pack_positions(const PackView &v, cudaStream_t st);
+void launch_aos_to_soa(const double *aos, double *X, double *Y, double *Z, int n, cudaStream_t st);
+void launch_soa_to_aos(double *aos, const double *X, const double *Y, const double *Z, int n, cudaStream_t st);
 void launch_zero(const PackView &v, cudaStream_t st);
 // neighbour list: build phases.  count -> (host may read total) -> fill
 void launch_nlist_count(Pack &p, cudaStream_t st);

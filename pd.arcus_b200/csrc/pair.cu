@@ -59,6 +59,30 @@ void launch_pack_positions(const PackView &v, cudaStream_t st) {
   if (v.n_atoms) PDGPU_LAUNCH(k_pack_positions, (v.n_atoms + 255) / 256, 256, 0, st, v);
 }
 
+// Interleaved [n][3] <-> three arrays, on the device: the state transfer
+// calls move one contiguous block between the caller's buffer and a device
+// staging array, with no host-side reshuffle.
+__global__ void k_aos_to_soa(const double *aos, double *X, double *Y, double *Z, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  X[i] = aos[3 * (size_t)i];
+  Y[i] = aos[3 * (size_t)i + 1];
+  Z[i] = aos[3 * (size_t)i + 2];
+}
+__global__ void k_soa_to_aos(double *aos, const double *X, const double *Y, const double *Z, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  aos[3 * (size_t)i] = X[i];
+  aos[3 * (size_t)i + 1] = Y[i];
+  aos[3 * (size_t)i + 2] = Z[i];
+}
+void launch_aos_to_soa(const double *aos, double *X, double *Y, double *Z, int n, cudaStream_t st) {
+  if (n > 0) PDGPU_LAUNCH(k_aos_to_soa, (n + 255) / 256, 256, 0, st, aos, X, Y, Z, n);
+}
+void launch_soa_to_aos(double *aos, const double *X, const double *Y, const double *Z, int n, cudaStream_t st) {
+  if (n > 0) PDGPU_LAUNCH(k_soa_to_aos, (n + 255) / 256, 256, 0, st, aos, X, Y, Z, n);
+}
+
 __global__ void k_zero(PackView v) {
   if (v.flags[F_NL_OVERFLOW]) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -330,6 +330,15 @@ int pack_upload_lcpo(Pack *p, const std::vector<const SystemHost *> &systems) {
   return PDGPU_OK;
 }
 
+int pack_ensure_stage(Pack *p) {
+  if (p->stage) return PDGPU_OK;
+  if (palloc(p, &p->stage, 3 * (size_t)p->v.n_atoms) != cudaSuccess || cudaStreamSynchronize(p->st) != cudaSuccess) {
+    set_error("device allocation failed (state staging)");
+    return PDGPU_ERR_NOMEM;
+  }
+  return PDGPU_OK;
+}
+
 void pack_set_params(Pack *p, int s, const pdgpu_ff_params &prm) {
   p->sp[s] = make_sys_params(prm);
 }
