@@ -768,12 +768,7 @@ def main():
         s2 = 0
         while done < e2e_steps:
             k = min(BLOCK, e2e_steps - done)
-            A.check(L.pdgpu_set_positions(ctx.ptr, ws._sys, xp))
-            A.check(L.pdgpu_set_velocities(ctx.ptr, ws._sys, vp))
-            A.check(L.pdgpu_md_run(ctx.ptr, ws._sys, ctypes.byref(p), s2, k, e2e_steps + BLOCK, None))
-            A.check(L.pdgpu_get_positions(ctx.ptr, ws._sys, xp))
-            A.check(L.pdgpu_get_velocities(ctx.ptr, ws._sys, vp))
-            A.check(L.pdgpu_get_energies(ctx.ptr, ws._sys, ep, A.ENE_COUNT))
+            A.check(L.pdgpu_md_run_io(ctx.ptr, ws._sys, ctypes.byref(p), s2, k, e2e_steps + BLOCK, xp, vp, xp, vp, ep))
             s2 += k
             done += k
         torch.cuda.synchronize()
@@ -781,7 +776,7 @@ def main():
         e2e = {"value": whole_job_ns_per_day(n_gpus, e2e_steps, te), "unit": "ns/day",
                "h2d_bytes_per_step": int(2 * n * 24 / BLOCK),
                "d2h_bytes_per_step": int((2 * n * 24 + A.ENE_COUNT * 8) / BLOCK),
-               "steps": e2e_steps, "api": "pdgpu_set_positions/velocities + pdgpu_md_run(10) + get_*"}
+               "steps": e2e_steps, "api": "pdgpu_md_run_io: host positions and velocities in, 10 steps, positions, velocities and energies out"}
 
     # roofline of the pair kernels (FP32/SFU; nominal peaks at the max SM clock)
     P_B, P_H, entries, tile_pairs, n_tiles = (int(c) for c in counts)

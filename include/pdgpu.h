@@ -348,6 +348,17 @@ void pdgpu_md_params_default(pdgpu_md_params *p);
 int pdgpu_md_run(pdgpu_ctx *ctx, int32_t sys, const pdgpu_md_params *p,
                  int32_t first_step, int32_t steps, int32_t total_steps,
                  double *history);
+/* pdgpu_md_run with the state in host memory (MolecularDynamics::run on a
+ * WorkSpace whose cur state the caller owns): positions (A) and velocities
+ * (m/s) in [natoms][3] are loaded first, and after the steps the positions,
+ * velocities and the energy record (J, PDGPU_ENE_COUNT per system) are
+ * written back.  Any pointer may be NULL to skip that transfer.  One host
+ * synchronisation beyond the step loop's; page-locked buffers are copied by
+ * DMA. */
+int pdgpu_md_run_io(pdgpu_ctx *ctx, int32_t sys, const pdgpu_md_params *p,
+                    int32_t first_step, int32_t steps, int32_t total_steps,
+                    const double *x_in, const double *v_in, double *x_out,
+                    double *v_out, double *ene_out);
 /* Trajectory snapshots (ProtocolBase::UpdateTra with WorkSpace::outtra.append,
  * md.cpp:260 and protocolbase.cpp:229-235): with every > 0, pdgpu_md_run
  * records the positions after each step s with s > 0 and s % every == 0.

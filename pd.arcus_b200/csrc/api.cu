@@ -1814,6 +1814,44 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
   return PDGPU_OK;
 }
 
+// MolecularDynamics::run with the state in host memory: the positions and
+// velocities go in, the steps run, and the positions, velocities and energy
+// record come back, with one host synchronisation after the step loop's
+// own (the state calls would add one each).
+int pdgpu_md_run_io(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t first_step, int32_t steps,
+                    int32_t total_steps, const double *x_in, const double *v_in, double *x_out, double *v_out,
+                    double *ene_out) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  int r;
+  if (x_in) {
+    if ((r = copy_soa_in(c, P, x_in, P.v.x, P.v.y, P.v.z))) return r;
+    launch_pack_positions(P.v, c->st);
+  }
+  if (v_in && (r = copy_soa_in(c, P, v_in, P.v.vx, P.v.vy, P.v.vz))) return r;
+  if ((r = pdgpu_md_run(c, sys, p, first_step, steps, total_steps, nullptr))) return r;
+  const int n = P.v.n_atoms;
+  std::vector<double> ene;
+  if ((x_out || v_out) && (r = pack_ensure_stage(&P))) return r;
+  if (x_out) {
+    launch_soa_to_aos(P.stage, P.v.x, P.v.y, P.v.z, n, c->st);
+    PDGPU_CUDA(cudaMemcpyAsync(x_out, P.stage, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, c->st));
+  }
+  if (v_out) {  // the staging block again: stream order puts this after the positions' copy
+    launch_soa_to_aos(P.stage, P.v.vx, P.v.vy, P.v.vz, n, c->st);
+    PDGPU_CUDA(cudaMemcpyAsync(v_out, P.stage, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, c->st));
+  }
+  if (ene_out) {
+    ene.resize((size_t)E_COUNT * e->nsys());
+    PDGPU_CUDA(cudaMemcpyAsync(ene.data(), P.v.ene, sizeof(double) * ene.size(), cudaMemcpyDeviceToHost, c->st));
+  }
+  if ((r = sync_check(c, "md_run_io"))) return r;
+  const double J = consts().J_per_kcalmol;
+  for (size_t k = 0; k < ene.size(); k++) ene_out[k] = ene[k] * J;
+  return PDGPU_OK;
+}
+
 // ------------------------------------------------------------ Monte Carlo
 void pdgpu_mc_params_default(pdgpu_mc_params *p) {
   if (!p) return;

@@ -155,6 +155,8 @@ PROTOTYPES = {
     "pdgpu_calc_forces": (ctypes.c_int, [_CTX, ctypes.c_int32]),
     "pdgpu_md_run": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.POINTER(MDParams), ctypes.c_int32,
                                     ctypes.c_int32, ctypes.c_int32, _D]),
+    "pdgpu_md_run_io": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.POINTER(MDParams), ctypes.c_int32,
+                                       ctypes.c_int32, ctypes.c_int32, _D, _D, _D, _D, _D]),
     "pdgpu_md_set_trajectory": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
     "pdgpu_md_read_trajectory": (ctypes.c_int, [_CTX, ctypes.c_int32, _D, ctypes.POINTER(ctypes.c_int64),
                                                 ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
