@@ -49,6 +49,10 @@ def test_defaults_mirror_reference_constructors():
     assert m.FricCoeff == 10e12
     n = A.min_params_default()
     assert n.Algorithm == A.MIN_CONJUGATE_GRADIENTS and n.StepSize == 2e5 and n.UpdateNList == 1
+    c = A.mc_params_default()
+    # MonteCarlo (montecarlo.h:52-53): ConstantProfile(300), FinalState LastAcc
+    assert c.Temperature == 300.0 and c.FinalState == A.MC_LAST_ACC and c.Steps == 0
+    assert abs(c.Sigma - 15.0 * 3.14159265358979323846 / 180.0) < 1e-15
 
 
 def test_null_arguments_are_rejected_without_a_device():
