@@ -5,9 +5,11 @@
 //
 // Two launches per evaluation, one warp per atom the term uses (hydrogens,
 // use 0, keep area, energy and derivative 0 and get no warp):
-//  k_lcpo_list  the atom's overlap partners: the CSR row's atoms j with
-//               use[j] and |xi - xj| < ri + rj, ranked by index, the first
-//               80 kept with their overlap areas.  The reference appends
+//  k_lcpo_list  the atom's overlap partners: the list partners j with
+//               use[j] and |xi - xj| < ri + rj (from its CSR row, or from
+//               the candidates k_lcpo_cand_tiles gathered off the tiles of a
+//               tile search), ranked by index, the first 80 kept with their
+//               overlap areas.  The reference appends
 //               partners in ascending index from both ends of every pair
 //               and stops at 80 (lcpo.cpp:434-485, 688-746), which keeps
 //               exactly these.
