@@ -65,11 +65,11 @@ REF_PARAM = os.path.join(ROOT, "oracle", "_ref", "param")
 DT_FS = 1.0
 BLOCK = 10  # list period = one timed iteration (L2 flushed between them)
 METRIC = "GB MD ns/day"
-# DRAM bytes (read + write) of one launch of the fused pair kernel on this
-# workload, from one ncu capture (profiles/k_gb_tile_md_20566.md:
-# dram__bytes_read.sum + dram__bytes_write.sum, cold caches); ncu cannot run
-# inside the timed bench, so the figure is carried here with its source
-NCU_TRAFFIC_K3_TILES = 2867200 + 0
+# DRAM bytes (read + write) of one launch of the evaluation kernel on this
+# workload, from one ncu capture of the 20,566-atom MD workload
+# (dram__bytes_read.sum + dram__bytes_write.sum, cold caches); ncu cannot run
+# inside the timed bench, so the figure is carried here
+NCU_TRAFFIC_EVAL = None
 
 
 def rank_info():
@@ -77,6 +77,40 @@ def rank_info():
     w = int(os.environ.get("WORLD_SIZE", "1"))
     lr = int(os.environ.get("LOCAL_RANK", str(r)))
     return r, w, lr
+
+
+def check_world(gpus, world):
+    """The number of GPUs the job runs on: the ranks the launcher started.
+    Each rank is one replica on its own GPU, so asking for more GPUs than
+    there are ranks would count work nobody did; that is refused."""
+    if gpus > world:
+        raise SystemExit("bench.py: --gpus %d needs %d ranks (one process per GPU): launch it with "
+                         "python -m torch.distributed.run --nproc-per-node %d bench.py --gpus %d "
+                         "(WORLD_SIZE is %d)" % (gpus, gpus, gpus, gpus, world))
+    return world
+
+
+def warmup_plan(warmup, steps, block=BLOCK):
+    """Warm-up blocks of the headline MD run: at least max(3, warmup) steps,
+    rounded up to whole list periods so the timed region starts on a period
+    boundary, plus (when the timed steps end inside a period) one partial
+    period and the rest of it, so every step-block graph the timed region
+    replays is captured before it starts.  Returns the block lengths."""
+    w = max(3, warmup)
+    plan = [block] * ((w + block - 1) // block)
+    tail = steps % block
+    if tail:
+        plan += [tail, block - tail]
+    return plan
+
+
+def headline_config(n_atoms, n_gpus):
+    """The workload description both arms print (same keys, same values)."""
+    return {"workload": "16x80-residue chains, 20566 atoms, AMBER99 + Still GB + bonded, Rc 16 A, "
+                        "Langevin 1 fs 300 K gamma 1/ps, list every 10 steps",
+            "atoms": n_atoms, "forcefield": "amber99aa: FF_Bonded + FF_GeneralizedBorn_Still (FastMode)",
+            "parallelism": "replicas" if n_gpus > 1 else "single",
+            "l2": "flushed (256 MiB write) before every 10-step timed block"}
 
 
 def max_over_ranks(value, dist, device):
@@ -578,7 +612,7 @@ def run_reference(args, n_gpus):
     arrays, meta = load_fixture()
     n = arrays["charge"].shape[0]
     steps = max(1, min(args.steps, args.ref_steps))
-    warm = max(1, min(args.warmup, 2))
+    warm = sum(warmup_plan(args.warmup, args.steps))  # the same warm-up as the device arm
     if os.path.exists(REF_DRIVER):
         tmp = tempfile.mkdtemp(prefix="pdref_")
         try:
@@ -617,7 +651,8 @@ def run_reference(args, n_gpus):
         kind = "port"
     ns_day = steps * DT_FS * 1e-6 / secs * 86400.0
     sample = "%d MD steps (1 list rebuild per 10) of the %d-atom workload after %d warm-up" % (steps, n, warm)
-    return {"value": ns_day, "kind": kind, "cores": 1, "sample": sample, "seconds": secs, "steps": steps}
+    return {"value": ns_day, "kind": kind, "cores": 1, "sample": sample, "seconds": secs, "steps": steps,
+            "warmup": warm}
 
 
 # ---------------------------------------------------------------- ours
@@ -640,18 +675,19 @@ def main():
     ap.add_argument("--serve-rows", action="store_true", help="serve on the list-row pair passes")
     args = ap.parse_args()
     rank, world, local = rank_info()
-    n_gpus = max(args.gpus, world)
+    n_gpus = check_world(args.gpus, world)
 
     if args.impl == "reference":
         if rank != 0:
             return 0
         r = run_reference(args, n_gpus)
+        cfg = headline_config(int(load_fixture()[0]["charge"].shape[0]), n_gpus)
+        cfg["threads"] = 1
         line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": "ns/day",
-                "n_gpus": n_gpus, "steps": r["steps"], "warmup": min(args.warmup, 2),
+                "n_gpus": n_gpus, "steps": r["steps"], "warmup": r["warmup"],
                 "ms_per_step": 1e3 * r["seconds"] / r["steps"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "16x80-residue GB MD, 20566 atoms, Rc 16 A, Langevin 1 fs",
-                           "threads": 1},
+                "config": cfg,
                 "cpu_baseline": {"value": r["value"], "unit": "ns/day", "cores": 1, "kind": r["kind"],
                                  "sample": r["sample"]},
                 "e2e": {"value": r["value"], "unit": "ns/day", "h2d_bytes_per_step": 0,
@@ -701,13 +737,16 @@ def main():
     path = ws.setPairPath(-2)  # the layout in use (the autotuner's choice by default)
     kms = np.zeros(3)
     A.check(A.lib().pdgpu_profile_pair_kernels(ctx.ptr, ws._sys, 20, A.dptr(kms)))
+    ems, ecnt = np.zeros(4), np.zeros(2, dtype=np.int64)
+    if path == 1:  # the evaluation kernel: three phases as three launches, then one launch
+        A.check(A.lib().pdgpu_profile_eval(ctx.ptr, ws._sys, 20, A.dptr(ems), ecnt.ctypes.data_as(A._I64)))
 
     p = A.md_params_default()
     p.Integrator, p.UpdateNList, p.UseGraph = A.INTEGRATOR_LANGEVIN, BLOCK, 1
     p.Timestep, p.FricCoeff, p.TargetTemp, p.Seed = 1e-15, 1e12, 300.0, 1000 + rank
     A.check(A.lib().pdgpu_md_init_velocities(ctx.ptr, ws._sys, 300.0, 1000 + rank))
     L = A.lib()
-    total = args.warmup + args.steps + BLOCK
+    total = sum(warmup_plan(args.warmup, args.steps)) + args.steps + BLOCK
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
     def run_block(step0, k):
@@ -715,10 +754,10 @@ def main():
         A.check(st)
         return ctx.last_run_ms()
 
-    warm = max(3, args.warmup)
+    plan = warmup_plan(args.warmup, args.steps)
+    warm = sum(plan)
     s = 0
-    while s < warm:
-        k = min(BLOCK, warm - s)
+    for k in plan:
         run_block(s, k)
         s += k
     # timed: K steps in list-period blocks, L2 flushed before each block
@@ -785,39 +824,61 @@ def main():
     F32 = sms * 256 * f_max
     SFU = sms * 16 * f_max
     t2, t3, t4 = (float(x) / 1e3 for x in kms)
-    k3_flop, k3_sfu = 90.0 * P_H, 5.0 * P_H
-    k3_frac_fp32 = (k3_flop / t3) / F32
-    k3_frac_sfu = (k3_sfu / t3) / SFU
     all_flop, all_sfu = 57.0 * P_B + 90.0 * P_H, 7.0 * P_B + 5.0 * P_H
-    t_pair = t2 + t3 + t4
-    t_roof = max(all_flop / F32, all_sfu / SFU)
-    bound = "fp32" if k3_frac_fp32 >= k3_frac_sfu else "sfu"
-    k3_name = ("k_gb_tile + k_gb_finish (fused GB + LJ + Coulomb on 32x8 cluster-pair tiles, K3)" if path == 1
-               else "k_gb_pair (fused GB + LJ + Coulomb on neighbour-list rows, K3)")
-    roof = {"kernel": k3_name, "bound": bound, "pair_path": "tiles" if path == 1 else "rows",
-            "tiles": {"tiles": n_tiles, "pair_slots": 256 * n_tiles, "list_pairs_held": tile_pairs,
-                      "slot_occupancy": tile_pairs / max(1, 256 * n_tiles)},
-            "achieved": (k3_flop / t3 / 1e12) if bound == "fp32" else (k3_sfu / t3 / 1e12),
-            "peak": (F32 if bound == "fp32" else SFU) / 1e12,
-            "unit": "TFLOP/s" if bound == "fp32" else "Top/s (MUFU)",
-            "frac": max(k3_frac_fp32, k3_frac_sfu),
-            "traffic": NCU_TRAFFIC_K3_TILES if path == 1 else None,
-            "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
-            "peak_source": "nominal %d SMs x %s/clk at sm_max_mhz %.0f (no measured FP32/SFU peak)" % (
-                sms, "256 flop" if bound == "fp32" else "16 MUFU", f_max / 1e6),
-            "pairs": {"P_B": P_B, "P_H": P_H, "list_entries": entries},
-            "kernel_ms": {"born_K2": t2 * 1e3, "pair_K3": t3 * 1e3, "chain_K4": t4 * 1e3},
-            "lanes_per_atom": {"born_K2": int(lpa[0]), "pair_K3": int(lpa[1]), "chain_K4": int(lpa[2])},
-            "pair_kernels_frac_of_roof": t_roof / t_pair}
+    peak_note = "nominal %d SMs x %%s/clk at sm_max_mhz %.0f (no measured FP32/SFU peak)" % (sms, f_max / 1e6)
+    tiles_info = {"tiles": n_tiles, "pair_slots": 256 * n_tiles, "list_pairs_held": tile_pairs,
+                  "slot_occupancy": tile_pairs / max(1, 256 * n_tiles)}
+    if path == 1:
+        # the dominant kernel is the evaluation kernel k_eval_tiles<7>: the
+        # Born sums, the GB + LJ + Coulomb pass and the chain rule in one
+        # cooperative launch; its algorithmic work is all three passes
+        tA, tB, tC, tF = (float(x) / 1e3 for x in ems)
+        fr32, frsfu = (all_flop / tF) / F32, (all_sfu / tF) / SFU
+        bound = "fp32" if fr32 >= frsfu else "sfu"
+        roof = {"kernel": "k_eval_tiles<7> (Born sums + fused GB/LJ/Coulomb + chain rule, one cooperative launch "
+                          "on 32x8 cluster-pair tiles)",
+                "bound": bound, "pair_path": "tiles", "tiles": tiles_info,
+                "achieved": (all_flop / tF / 1e12) if bound == "fp32" else (all_sfu / tF / 1e12),
+                "peak": (F32 if bound == "fp32" else SFU) / 1e12,
+                "unit": "TFLOP/s" if bound == "fp32" else "Top/s (MUFU)",
+                "frac": max(fr32, frsfu),
+                "work": "57 flop + 7 MUFU per P_B pair (Born sum 21+3, chain rule 36+4), 90 flop + 5 MUFU per "
+                        "P_H pair (fused GB/LJ/Coulomb); FMA = 2 flop",
+                "traffic": NCU_TRAFFIC_EVAL if NCU_TRAFFIC_EVAL else None,
+                "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                                "of k_eval_tiles<7> on this workload)",
+                "peak_source": peak_note % ("256 flop" if bound == "fp32" else "16 MUFU"),
+                "pairs": {"P_B": P_B, "P_H": P_H, "list_entries": entries},
+                "kernel_ms": {"eval_one_launch": tF * 1e3, "phase_born_alone": tA * 1e3,
+                              "phase_pair_alone": tB * 1e3, "phase_chain_alone": tC * 1e3},
+                "chain_phase_tiles": {"visited": int(ecnt[1]), "of": int(ecnt[0])},
+                "three_pass_form_ms": {"born_K2": t2 * 1e3, "pair_K3": t3 * 1e3, "chain_K4": t4 * 1e3,
+                                       "frac_of_roof": max(all_flop / F32, all_sfu / SFU) / (t2 + t3 + t4)},
+                "pair_kernels_frac_of_roof": max(all_flop / F32, all_sfu / SFU) / tF}
+    else:
+        k3_flop, k3_sfu = 90.0 * P_H, 5.0 * P_H
+        k3_frac_fp32 = (k3_flop / t3) / F32
+        k3_frac_sfu = (k3_sfu / t3) / SFU
+        t_pair = t2 + t3 + t4
+        t_roof = max(all_flop / F32, all_sfu / SFU)
+        bound = "fp32" if k3_frac_fp32 >= k3_frac_sfu else "sfu"
+        roof = {"kernel": "k_gb_pair (fused GB + LJ + Coulomb on neighbour-list rows, K3)", "bound": bound,
+                "pair_path": "rows", "tiles": tiles_info,
+                "achieved": (k3_flop / t3 / 1e12) if bound == "fp32" else (k3_sfu / t3 / 1e12),
+                "peak": (F32 if bound == "fp32" else SFU) / 1e12,
+                "unit": "TFLOP/s" if bound == "fp32" else "Top/s (MUFU)",
+                "frac": max(k3_frac_fp32, k3_frac_sfu), "traffic": None,
+                "peak_source": peak_note % ("256 flop" if bound == "fp32" else "16 MUFU"),
+                "pairs": {"P_B": P_B, "P_H": P_H, "list_entries": entries},
+                "kernel_ms": {"born_K2": t2 * 1e3, "pair_K3": t3 * 1e3, "chain_K4": t4 * 1e3},
+                "lanes_per_atom": {"born_K2": int(lpa[0]), "pair_K3": int(lpa[1]), "chain_K4": int(lpa[2])},
+                "pair_kernels_frac_of_roof": t_roof / t_pair}
 
     line = {"metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": n_gpus, "steps": args.steps,
             "warmup": warm, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair / f64 state",
             "data": "synthetic (seeded peptides built by the reference's NewProtein)",
-            "config": {"workload": "16x80-residue chains, 20566 atoms, AMBER99 + Still GB + bonded, Rc 16 A, "
-                                   "Langevin 1 fs 300 K gamma 1/ps, list every 10 steps",
-                       "atoms": n, "parallelism": "replicas" if n_gpus > 1 else "single",
-                       "l2": "flushed (256 MiB write) before every 10-step timed block"},
+            "config": headline_config(n, n_gpus),
             "parity": {"force_rel_rms_vs_fp64": force_rms, "epot_abs_err_kcal": de_kcal},
             "gpu_launches": int(lc1.value - lc0.value),
             "clocks": clk, "roofline": roof, "e2e": e2e}

@@ -271,12 +271,18 @@ int pdgpu_nlist_export(pdgpu_ctx *ctx, int32_t sys, int32_t shadow, int32_t *ptr
  *   count          out (host): entries needed; PDGPU_ERR_ARG if > capacity
  *   stream         cudaStream_t to run on (NULL: the default stream)
  * All scratch lives in one static device array sized for 65,536 atoms
- * (about 2.9 MB, held on every GPU that loads the library until exit);
- * larger systems are refused with PDGPU_ERR_ARG.  Calls share that array:
- * calls that overlap on the GPU race and must be serialised by the caller.
- * The first call on each device looks up the array's device address; make
- * that first call outside any stream capture.  The call synchronises
- * `stream` once to read the entry count. */
+ * (about 2.9 MB, held on every GPU where the array's module is loaded, until
+ * exit); larger systems are refused with PDGPU_ERR_ARG.  Calls share that
+ * array: calls that overlap on the GPU race and must be serialised by the
+ * caller.  Under lazy module loading (CUDA_MODULE_LOADING=LAZY, the CUDA
+ * default) the module, and with it the array, is loaded on a device by the
+ * first call there or by pdgpu_ctx_create on that device, whichever comes
+ * first; that is when the 2.9 MB are taken.  A caller that reserves all
+ * device memory for its own pool should make one of those two calls first
+ * (or run with CUDA_MODULE_LOADING=EAGER); after that the call takes no
+ * device memory.  It can never run inside a stream capture: it copies small
+ * host-side parameter blocks and synchronises `stream` once to read the
+ * entry count. */
 int pdgpu_nlist_build_noalloc(const double *x, const double *y, const double *z, int32_t natoms,
                               double list_cutoff, int32_t max_index_delta, const int8_t *band,
                               const int32_t *offdiag_ptr, const int32_t *offdiag_pairs,
@@ -501,6 +507,19 @@ int pdgpu_pair_counts(pdgpu_ctx *ctx, int32_t sys, int64_t *counts);
  * kernels over `reps` evaluations, each bracketed by CUDA events on the
  * context stream: ms[0..2]. */
 int pdgpu_profile_pair_kernels(pdgpu_ctx *ctx, int32_t sys, int32_t reps, double *ms);
+/* Instrumentation (no reference counterpart): device times (CUDA events on
+ * the context stream, averaged over reps) of the evaluation kernel on the
+ * cluster-pair tiles: ms[0..2] its Born-sum, GB + LJ + Coulomb and
+ * chain-rule phases as three launches, ms[3] the three in one cooperative
+ * launch (the form the protocols run).  counts[0] = tiles, counts[1] =
+ * tiles the chain-rule phase visited (a pair inside the Still cutoff).
+ * PDGPU_ERR_STATE unless the handle is on the tile layout. */
+int pdgpu_profile_eval(pdgpu_ctx *ctx, int32_t sys, int32_t reps, double *ms, int64_t *counts);
+/* How an evaluation on the tile layout is launched (no reference
+ * counterpart): 1 = the three passes in one cooperative launch (the
+ * default), 0 = the same three phases as three launches; -1 = only report.
+ * Both give the same bits.  *current (may be NULL) receives the mode. */
+int pdgpu_eval_mode(pdgpu_ctx *ctx, int32_t sys, int32_t set, int32_t *current);
 /* Device times (CUDA events, averaged over reps full evaluations at step 0)
  * of the LCPO term's two launches and the work they did: out[0] overlap
  * list ms, out[1] area/derivative ms, out[2] overlap partners kept, out[3]
@@ -512,6 +531,13 @@ int pdgpu_profile_lcpo(pdgpu_ctx *ctx, int32_t sys, int32_t reps, double *out);
 /* Kernels this context has launched (graph replays count their kernel
  * nodes). */
 int pdgpu_launch_count(pdgpu_ctx *ctx, int64_t *count);
+/* Instrumentation (no reference counterpart): step blocks of pdgpu_md_run
+ * on this handle that replayed a captured graph (replays[0]) and the graphs
+ * cached for it now (replays[1]).  A run cuts its steps at the list periods
+ * (a rebuild every UpdateNList steps, protocolbase.cpp:113-122); every block
+ * of more than one step, a partial first or last period included, replays
+ * a graph when UseGraph is set. */
+int pdgpu_graph_replays(pdgpu_ctx *ctx, int32_t sys, int64_t *replays);
 /* Autotuner (no reference counterpart): re-time the lanes-per-atom choice
  * (4, 8, 16 or 32 lanes walk one atom's neighbour row) of the Born-radius,
  * fused pair and chain-rule kernels on the current list; lpa[0..2] receive

@@ -10,6 +10,13 @@
 //           coordinates and every reference result the parity tests pin
 //   time    rebuild a dumped system's topology, load its coordinates, and
 //           time the reference MD step loop (the CPU baseline)
+//   replay  rebuild a dumped system, load its coordinates and dump what
+//           the reference's protocols give with it: the single-point
+//           results, integrator steps, SD / CG minimisation, and a
+//           MolecularDynamics::runcore run.  Built a second time with
+//           PDGPU_COMPONENT (ref_driver_gpu), the same driver runs the
+//           B200 GB component FF_GeneralizedBorn_Still_GPU in place of
+//           the reference's: the drop-in check.
 //
 // The reference API calls used (all unchanged reference code):
 //   FFParamSet::readLib                 forcefields/ffparam.h:571
@@ -44,6 +51,10 @@
 #include "maths/maths.h"
 #undef private
 #undef protected
+#ifdef PDGPU_COMPONENT
+// the B200 GB component (pd.arcus_b200/plugin) in place of the reference's
+#include "gbff_gpu.h"
+#endif
 
 #include <sys/stat.h>
 #include <sys/time.h>
@@ -202,7 +213,11 @@ static Built make_ws(FFParamSet *ffps, const std::vector<std::string> &seqs,
   b.ws = new WorkSpace(*b.sys);
   b.ff = new Forcefield(*b.ws);
   b.bonded = new FF_Bonded(*b.ws);
+#ifdef PDGPU_COMPONENT
+  b.gb = new FF_GeneralizedBorn_Still_GPU(*b.ws);
+#else
   b.gb = new FF_GeneralizedBorn_Still(*b.ws);
+#endif
   configure_gb(*b.gb, st);
   if (with_bonded) b.ff->add(*b.bonded);
   b.ff->add(*b.gb);
@@ -772,7 +787,9 @@ static void usage() {
           "[--md STEPS] [--min STEPS] [--slowmode] [--trials K --trial-sigma DEG]\n"
           "          [--lcpo-asp KCAL_PER_A2 --lcpo UPDATESASA[,STEPS[,DENSE]]]\n"
           "ref_driver time --in DIR --cutoff R --inner R --steps K "
-          "[--warmup W] [--nlist-every M] [--param F]\n");
+          "[--warmup W] [--nlist-every M] [--param F]\n"
+          "ref_driver replay --in DIR --out DIR --cutoff R --inner R [--md STEPS] [--min STEPS] "
+          "[--steps K] [--param F]\n");
   exit(1);
 }
 
@@ -902,6 +919,63 @@ int main(int argc, char **argv) {
     }
     if (lcpo_asp != 0.0) dump_lcpo(b, allpos, lcpo_asp, lcpo_update, lcpo_steps, lcpo_dense != 0);
     printf("built %zu atoms\n", b.ws->nAtoms());
+    return 0;
+  }
+
+  if (mode == "replay") {
+    if (g_out.empty() || in.empty()) usage();
+    mkdir(g_out.c_str(), 0755);
+    std::vector<std::string> seqs;
+    {
+      std::string path = in + "/meta.txt";
+      FILE *f = fopen(path.c_str(), "r");
+      if (!f) { fprintf(stderr, "no %s\n", path.c_str()); return 2; }
+      char key[64], val[4096];
+      while (fscanf(f, "%63s %4095s", key, val) == 2)
+        if (std::string(key) == "chain") seqs.push_back(val);
+      fclose(f);
+    }
+    size_t n0;
+    std::vector<double> pos = npy_read_d(in + "/pos.npy", &n0);
+    Built b = make_ws(ffps, seqs, st);
+    if (b.ws->nAtoms() != n0) { fprintf(stderr, "atom count mismatch\n"); return 2; }
+    set_pos(*b.ws, pos);
+    b.ff->ensuresetup(*b.ws);
+    dump_single_point(b, "");
+    if (mdsteps > 0) {
+      set_pos(*b.ws, pos);
+      dump_md_steps(b, MolecularDynamics::Langevin, mdsteps, 1e12, "mdlv_");
+      set_pos(*b.ws, pos);
+      dump_md_steps(b, MolecularDynamics::VelocityVerlet, mdsteps, 1e12, "mdvv_");
+    }
+    if (minsteps > 0) {
+      set_pos(*b.ws, pos);
+      dump_minimise(b, Minimisation::SteepestDescent, minsteps, "minsd_");
+      set_pos(*b.ws, pos);
+      dump_minimise(b, Minimisation::ConjugateGradients, minsteps, "mincg_");
+    }
+    if (steps > 0) {
+      // the reference's own protocol loop (md.cpp:202-267) for `steps`
+      // Langevin steps, list every 10, velocities drawn by the reference
+      set_pos(*b.ws, pos);
+      MolecularDynamics md(*b.ff);
+      md.Integrator = MolecularDynamics::Langevin;
+      md.Timestep = 1e-15;
+      md.FricCoeff = 1e12;
+      md.Steps = steps;
+      md.UpdateNList = nlist_every;
+      md.UpdateScr = 0;
+      md.OutputLevel = Verbosity::Silent;
+      srand(4242);
+      md.setInitialSpeeds(300.0);
+      int taken = md.runcore();
+      put_d("proto_md_x", get_pos(*b.ws), shp(b.ws->nAtoms(), 3));
+      std::vector<double> r = ene_vec(b.ws->ene);
+      r.push_back(b.ws->ene.ekin);
+      r.push_back(taken);
+      put_d("proto_md_ene", r);
+    }
+    printf("replayed %zu atoms\n", b.ws->nAtoms());
     return 0;
   }
 

@@ -67,6 +67,28 @@ static int sync_check(pdgpu_ctx *c, const char *what) {
   return PDGPU_OK;
 }
 
+// After an evaluation on the tile layout: a grid barrier of the evaluation
+// kernel that ran out of time (F_BARRIER) is reported, and its counters are
+// cleared so the next evaluation starts clean.
+static int barrier_check(pdgpu_ctx *c, pdgpu::Pack &P, const int *flags_host = nullptr) {
+  using namespace pdgpu;
+  int f = 0;
+  if (flags_host) {
+    f = flags_host[F_BARRIER];
+  } else if (P.v.tile_mode) {
+    PDGPU_CUDA(cudaMemcpyAsync(&f, P.v.flags + F_BARRIER, sizeof f, cudaMemcpyDeviceToHost, c->st));
+    int r = sync_check(c, "evaluation flags");
+    if (r) return r;
+  }
+  if (!f) return PDGPU_OK;
+  cudaMemsetAsync(P.v.flags + F_BARRIER, 0, sizeof(int), c->st);
+  if (P.v.tile_count) cudaMemsetAsync(P.v.tile_count + 2, 0, 2 * sizeof(int), c->st);
+  cudaStreamSynchronize(c->st);
+  set_error("the evaluation kernel's grid barrier timed out (blocks not co-resident); "
+            "set PDGPU_FUSED=0 to run the three passes as separate launches");
+  return PDGPU_ERR_CUDA;
+}
+
 namespace pdgpu {
 int entry_materialize(int device, SysEntry *e, bool sync) {
   std::string err;
@@ -236,6 +258,15 @@ int pdgpu_ctx_create(int device, pdgpu_ctx **out) {
   if (e != cudaSuccess) {
     delete c;
     return cuda_fail(e, "cudaStreamCreate");
+  }
+  // the allocation-free list build's static scratch: loaded now, so a
+  // caller that reserves its device memory after creating a context finds
+  // the array already in place
+  int r = noalloc_prepare_current_device();
+  if (r) {
+    cudaStreamDestroy(c->st);
+    delete c;
+    return r;
   }
   *out = c;
   return PDGPU_OK;
@@ -805,6 +836,9 @@ int pdgpu_get_atom_epot(pdgpu_ctx *c, int32_t sys, double *epot) {
   int n = P.v.n_atoms;
   std::vector<double> ea((size_t)AE_COUNT * n);
   PDGPU_CUDA(cudaMemcpyAsync(ea.data(), P.v.e_atom, sizeof(double) * ea.size(), cudaMemcpyDeviceToHost, c->st));
+  if (P.last_ebuf)  // the last evaluation wrote its pair slots to the second buffer
+    PDGPU_CUDA(cudaMemcpyAsync(ea.data(), P.v.e_pair_alt, sizeof(double) * 4 * (size_t)n, cudaMemcpyDeviceToHost,
+                               c->st));
   int r = sync_check(c, "get_atom_epot");
   if (r) return r;
   double J = consts().J_per_kcalmol;
@@ -1105,9 +1139,7 @@ static int ensure_tuned(pdgpu_ctx *c, Pack &P) {
     float tot = 0.1f * 3.f * build;  // three timed repetitions below
     for (int rep = 0; rep < 4 && r == PDGPU_OK; rep++) {
       cudaEventRecord(a, c->st);
-      launch_born_radii_tile(t, c->st, false);
-      launch_gb_pair_tile(t, c->st);
-      launch_gb_chain_tile(t, c->st);
+      launch_eval_tiles(t, c->st, 0, P.coop);  // the evaluation as the protocols run it
       cudaEventRecord(b, c->st);
       r = sync_check(c, "autotune tiles");
       float ms = 0;
@@ -1128,9 +1160,13 @@ static int ensure_tuned(pdgpu_ctx *c, Pack &P) {
 
 // GB calcForces enqueue (no sync)
 static void gb_forces_enqueue(pdgpu_ctx *c, Pack &P) {
-  launch_born_radii(P.v, c->st);
-  launch_gb_pair(P.v, c->st);
-  launch_gb_chain(P.v, c->st);
+  if (P.v.tile_mode) {
+    launch_eval_tiles(P.v, c->st, 0, P.coop);
+  } else {
+    launch_born_radii(P.v, c->st);
+    launch_gb_pair(P.v, c->st);
+    launch_gb_chain(P.v, c->st);
+  }
   launch_energy(P.v, c->st, EM_PAIR_GB);
 }
 
@@ -1149,7 +1185,8 @@ int pdgpu_gb_forces(pdgpu_ctx *c, int32_t sys) {
     return PDGPU_ERR_ARG;
   }
   gb_forces_enqueue(c, P);
-  return sync_check(c, "gb_forces");
+  r = sync_check(c, "gb_forces");
+  return r ? r : barrier_check(c, P);
 }
 
 int pdgpu_gb_energies(pdgpu_ctx *c, int32_t sys) {
@@ -1291,7 +1328,7 @@ void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce) {
   step.imm = e->ws_step;
   calc_forces_enqueue(st, e, reduce, step);
 }
-void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce, StepSrc step) {
+void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce, StepSrc step, int ebuf) {
   Pack &P = *e->pack;
   const bool bonded = has_bonded(P);
   const bool surf = P.v.lc.update > 0;
@@ -1310,14 +1347,24 @@ void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce, StepS
   // with an MD step's energy record still running beside, the record is
   // left to it (it forms the record from zero) and the fused pass, which
   // writes what the record reads, waits for it
-  const bool pending = P.energy_pending;
-  launch_born_radii(P.v, st, ZF_PAIRS | (side ? 0 : ZF_BONDED) | (pending ? 0 : ZF_RECORD));
-  if (pending) {
-    cudaStreamWaitEvent(st, P.ene_done, 0);
-    P.energy_pending = false;
+  const bool pending = P.energy_pending();
+  const int zero = ZF_PAIRS | (side ? 0 : ZF_BONDED) | (pending ? 0 : ZF_RECORD);
+  if (P.v.tile_mode) {
+    // the tile layout: the three passes as one evaluation into energy
+    // buffer `ebuf`; only a record still reading that buffer is waited for
+    P.wait_energy(st, ebuf);
+    PackView vb = P.v;
+    vb.ebuf = ebuf;
+    launch_eval_tiles(vb, st, zero, P.coop);
+    P.last_ebuf = ebuf;
+  } else {
+    launch_born_radii(P.v, st, zero);
+    P.wait_energy(st, 0);
+    P.wait_energy(st, 1);
+    launch_gb_pair(P.v, st);
+    launch_gb_chain(P.v, st);
+    P.last_ebuf = 0;
   }
-  launch_gb_pair(P.v, st);
-  launch_gb_chain(P.v, st);
   if (side) cudaStreamWaitEvent(st, P.join, 0);
   if (reduce) launch_energy(P.v, st, EM_PAIR_GB | (bonded ? EM_BONDED : 0) | (surf ? EM_SURF : 0));
 }
@@ -1330,7 +1377,8 @@ int pdgpu_calc_forces(pdgpu_ctx *c, int32_t sys) {
   int r = ready_pairs(c, e);
   if (r) return r;
   calc_forces_enqueue(c->st, e, true);
-  return sync_check(c, "calc_forces");
+  r = sync_check(c, "calc_forces");
+  return r ? r : barrier_check(c, P);
 }
 
 // ------------------------------------------------------------ MD
@@ -1436,23 +1484,30 @@ int pdgpu_md_init_velocities(pdgpu_ctx *c, int32_t sys, double temperature, uint
 // one MD step enqueue: forces, integrate, one energy reduction that also
 // records the step and advances the device step counter (7 launches)
 }  // extern "C"
-void pdgpu::md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k) {
+void pdgpu::md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k, int q) {
   Pack &P = *e->pack;
   StepSrc step;
   step.p = e->step_dev;  // MolecularDynamics::run_core sets WorkSpace::Step = Step (md.cpp:214)
-  calc_forces_enqueue(st, e, false, step);
+  const int b = P.v.tile_mode ? (q & 1) : 0;  // this step's energy buffer
+  calc_forces_enqueue(st, e, false, step, b);
+  // the integrator writes the kinetic energies the previous step's record
+  // reads: that record must be done
+  P.wait_energy(st, b ^ 1);
+  P.wait_energy(st, b);
   launch_md_step_impl(P.v, st, k, nullptr, e->step_dev, P.is_h, e->seeds, e->traj_dev, e->traj_every,
                       e->traj_dev_cap);
   // the step's energy record on the second stream, beside the next step's
-  // Born pass (its bonded terms queue behind it on that stream)
+  // evaluation (its bonded terms queue behind it on that stream)
   cudaEventRecord(P.fork2, st);
   cudaStreamWaitEvent(P.side, P.fork2, 0);
-  launch_energy(P.v, P.side,
+  PackView vb = P.v;
+  vb.ebuf = b;
+  launch_energy(vb, P.side,
                 EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0) | (P.v.lc.update > 0 ? EM_SURF : 0) | EM_KINETIC |
                     EM_RECORD | EM_ASSIGN,
                 e->hist, e->step_dev);
-  cudaEventRecord(P.ene_done, P.side);
-  P.energy_pending = true;
+  cudaEventRecord(P.ene_done[b], P.side);
+  P.ene_pending[b] = true;
 }
 // Trajectory frames of steps [s0, s1) (absolute): mirrored from the device
 // ring into the host ring on the pack's second stream once the steps are
@@ -1489,10 +1544,8 @@ static void trajectory_copy(pdgpu_ctx *c, SysEntry *e, int s0, int s1) {
 // main stream.
 void pdgpu::md_steps_end(cudaStream_t st, SysEntry *e) {
   Pack &P = *e->pack;
-  if (P.energy_pending) {
-    cudaStreamWaitEvent(st, P.ene_done, 0);
-    P.energy_pending = false;
-  }
+  P.wait_energy(st, 0);
+  P.wait_energy(st, 1);
 }
 extern "C" {
 
@@ -1615,10 +1668,19 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
   int s = 0;
   while (s < steps) {
     int step = first_step + s;
+    // Blocks follow the list periods (protocolbase.cpp:113-122: a rebuild
+    // when the step counter is a multiple of UpdateNList).  A run that
+    // starts inside a period first finishes that period in one block
+    // without a rebuild; a run that ends inside one ends with a shorter
+    // block that begins with the rebuild.  Every block of more than one
+    // step replays a cached graph of its own shape.
     bool rebuild = every > 0 && (P.nlist_counter % every) == 0;
     int block = 1;
-    if (rebuild && every > 1) block = std::min(every, steps - s);
-    bool use_graph = p->UseGraph && rebuild && block == every && every > 1;
+    if (every > 1) {
+      const int left = rebuild ? every : every - P.nlist_counter % every;
+      block = std::min(left, steps - s);
+    }
+    bool use_graph = p->UseGraph && block > 1;
     int counter0 = P.nlist_counter;
     for (int attempt = 0;; attempt++) {
       if (attempt == 4) {
@@ -1629,35 +1691,59 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
       PDGPU_CUDA(cudaMemcpyAsync(e->step_dev, &step, sizeof(int), cudaMemcpyHostToDevice, c->st));
       if (use_graph) {
         // graphs are cached per system; the key holds every value baked in
-        char key[256];
-        snprintf(key, sizeof key, "%d|%p|%lld|%p|%d|%d|%.17g|%.17g|%.17g|%d|%d|%d|%d%d%d|%d%d|%p|%d|%d", block,
-                 (void *)v.nl, v.nl_cap, (void *)e->hist, k.integrator, k.steps, k.dt, k.gamma, k.temp,
-                 k.stochastic_h, P.radix_passes, (int)e->host->params.FastMode, v.lpa[0], v.lpa[1], v.lpa[2],
-                 v.tile_mode, (int)tile_search_ok(P), (void *)e->traj_dev, e->traj_every, e->traj_dev_cap);
-        if (!e->gexec || e->gkey != key) {
-          e->drop_graph();
+        char key[288];
+        snprintf(key, sizeof key, "%d|%d|%p|%lld|%p|%d|%d|%.17g|%.17g|%.17g|%d|%d|%d|%d%d%d|%d%d|%p|%d|%d", block,
+                 (int)rebuild, (void *)v.nl, v.nl_cap, (void *)e->hist, k.integrator, k.steps, k.dt, k.gamma,
+                 k.temp, k.stochastic_h, P.radix_passes, (int)e->host->params.FastMode, v.lpa[0], v.lpa[1],
+                 v.lpa[2], v.tile_mode, (int)tile_search_ok(P), (void *)e->traj_dev, e->traj_every,
+                 e->traj_dev_cap);
+        SysEntry::GraphSlot *g = nullptr;
+        for (auto &q : e->gslots)
+          if (q.key == key) g = &q;
+        if (!g) {
+          if ((int)e->gslots.size() >= SysEntry::kGraphSlots) {  // evict the least recently used
+            auto lru = std::min_element(e->gslots.begin(), e->gslots.end(),
+                                        [](const SysEntry::GraphSlot &a, const SysEntry::GraphSlot &b) {
+                                          return a.used < b.used;
+                                        });
+            e->drop_slot(*lru);
+            e->gslots.erase(lru);
+          }
+          SysEntry::GraphSlot ng;
+          const bool pend0 = P.ene_pending[0], pend1 = P.ene_pending[1];  // both false between blocks
           begin_capture_count();
           PDGPU_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-          rebuild_enqueue(P, c->st);
-          for (int q = 0; q < block; q++) md_step_enqueue(c->st, e, k);
+          if (rebuild) rebuild_enqueue(P, c->st);
+          for (int q = 0; q < block; q++) md_step_enqueue(c->st, e, k, q);
           md_steps_end(c->st, e);
-          PDGPU_CUDA(cudaStreamEndCapture(c->st, &e->graph));
-          PDGPU_CUDA(cudaGraphInstantiate(&e->gexec, e->graph, 0));
-          e->gnodes = end_capture_count();
-          e->gkey = key;
+          cudaError_t ce = cudaStreamEndCapture(c->st, &ng.graph);
+          ng.nodes = end_capture_count();
+          if (ce == cudaSuccess) ce = cudaGraphInstantiate(&ng.exec, ng.graph, 0);
+          if (ce != cudaSuccess) {
+            e->drop_slot(ng);
+            P.ene_pending[0] = pend0;
+            P.ene_pending[1] = pend1;
+            return cuda_fail(ce, "capture md block");
+          }
+          ng.key = key;
+          e->gslots.push_back(ng);
+          g = &e->gslots.back();
         }
-        PDGPU_CUDA(cudaGraphLaunch(e->gexec, c->st));
-        launch_counter() += e->gnodes;
-        P.csr_stale = tile_search_ok(P);  // what the graph's rebuild made
+        g->used = ++e->gclock;
+        PDGPU_CUDA(cudaGraphLaunch(g->exec, c->st));
+        launch_counter() += g->nodes;
+        e->graph_replays++;
+        if (rebuild) P.csr_stale = tile_search_ok(P);  // what the graph's rebuild made
       } else {
         if (rebuild) rebuild_enqueue(P, c->st);
-        for (int q = 0; q < block; q++) md_step_enqueue(c->st, e, k);
+        for (int q = 0; q < block; q++) md_step_enqueue(c->st, e, k, q);
         md_steps_end(c->st, e);
       }
       int flags[F_COUNT];
       PDGPU_CUDA(cudaMemcpyAsync(flags, v.flags, sizeof flags, cudaMemcpyDeviceToHost, c->st));
       r = sync_check(c, "md block");
       if (r) return r;
+      if ((r = barrier_check(c, P, flags))) return r;
       if (flags[F_LCPO_CAND]) {
         set_error(kLcpoCandMsg);
         return PDGPU_ERR_STATE;
@@ -1760,6 +1846,7 @@ int pdgpu_minimise_run(pdgpu_ctx *c, int32_t sys, const pdgpu_min_params *p, int
     PDGPU_CUDA(cudaMemcpyAsync(flags, v.flags, sizeof flags, cudaMemcpyDeviceToHost, c->st));
     r = sync_check(c, "minimise");
     if (r) return r;
+    if ((r = barrier_check(c, P, flags))) return r;
     if (flags[F_LCPO_CAND]) {
       set_error(kLcpoCandMsg);
       return PDGPU_ERR_STATE;
@@ -1919,6 +2006,7 @@ int pdgpu_mc_run(pdgpu_ctx *c, int32_t sys, const pdgpu_mc_params *p, int32_t *a
     PDGPU_CUDA(cudaMemcpyAsync(flags, v.flags, sizeof flags, cudaMemcpyDeviceToHost, c->st));
     PDGPU_CUDA(cudaMemcpyAsync(hs.data(), e->mc_state, hs.size(), cudaMemcpyDeviceToHost, c->st));
     if ((r = sync_check(c, "mc_run"))) return r;
+    if ((r = barrier_check(c, P, flags))) return r;
     if (flags[F_LCPO_CAND]) {
       set_error(kLcpoCandMsg);
       return PDGPU_ERR_STATE;
@@ -1953,6 +2041,7 @@ int pdgpu_mc_run(pdgpu_ctx *c, int32_t sys, const pdgpu_mc_params *p, int32_t *a
   int flags[F_COUNT];
   PDGPU_CUDA(cudaMemcpyAsync(flags, v.flags, sizeof flags, cudaMemcpyDeviceToHost, c->st));
   if ((r = sync_check(c, "mc_run final"))) return r;
+  if ((r = barrier_check(c, P, flags))) return r;
   if (flags[F_NL_OVERFLOW]) {  // the final state's list: sized, then evaluated again
     if ((r = nlist_enqueue(c, e, true))) return r;
     calc_forces_enqueue(c->st, e, true, ws);
@@ -2047,6 +2136,58 @@ int pdgpu_profile_pair_kernels(pdgpu_ctx *c, int32_t sys, int32_t reps, double *
 // did: out[0] list ms, out[1] evaluation ms, out[2] overlap partners kept,
 // out[3] (atom, partner, partner's partner) triples of the inner loop,
 // out[4] those whose third atom overlaps the first (the full inner body).
+int pdgpu_profile_eval(pdgpu_ctx *c, int32_t sys, int32_t reps, double *ms, int64_t *counts) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  int r = ready_pairs(c, e);
+  if (r) return r;
+  if (!ms || reps <= 0) {
+    set_error("ms is NULL or reps <= 0");
+    return PDGPU_ERR_ARG;
+  }
+  if (!P.v.tile_mode) {
+    set_error("pdgpu_profile_eval: the handle is not on the cluster-pair tile layout");
+    return PDGPU_ERR_STATE;
+  }
+  cudaError_t ce = profile_eval_tiles(P.v, c->st, reps, ms);
+  if (ce != cudaSuccess) return cuda_fail(ce, "profile_eval");
+  if ((r = sync_check(c, "profile_eval"))) return r;
+  if ((r = barrier_check(c, P))) return r;
+  if (counts) {
+    // the still list a Born phase makes (an evaluation's chain phase
+    // clears it, so it is counted after a Born phase alone)
+    int h[4] = {0, 0, 0, 0};
+    PDGPU_CUDA(cudaMemsetAsync(P.v.tile_count + 2, 0, 2 * sizeof(int), c->st));
+    launch_born_phase_only(P.v, c->st);
+    PDGPU_CUDA(cudaMemcpyAsync(h, P.v.tile_count, sizeof h, cudaMemcpyDeviceToHost, c->st));
+    if ((r = sync_check(c, "profile_eval counts"))) return r;
+    counts[0] = h[0];
+    counts[1] = h[2];
+    // clear the list the lone Born phase left, and the sums it added
+    PDGPU_CUDA(cudaMemsetAsync(P.v.tile_count + 2, 0, 2 * sizeof(int), c->st));
+    PDGPU_CUDA(cudaMemsetAsync(P.v.bsum, 0, sizeof(long long) * P.v.n_atoms, c->st));
+    if ((r = sync_check(c, "profile_eval counts"))) return r;
+  }
+  return PDGPU_OK;
+}
+
+int pdgpu_eval_mode(pdgpu_ctx *c, int32_t sys, int32_t set, int32_t *current) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  Pack &P = *e->pack;
+  if (set < -1 || set > 1) {
+    set_error("pdgpu_eval_mode: set must be -1 (query), 0 (three launches) or 1 (one cooperative launch)");
+    return PDGPU_ERR_ARG;
+  }
+  if (set >= 0 && P.coop != (set == 1)) {
+    P.coop = set == 1;
+    e->drop_graph();
+  }
+  if (current) *current = P.coop ? 1 : 0;
+  return PDGPU_OK;
+}
+
 int pdgpu_profile_lcpo(pdgpu_ctx *c, int32_t sys, int32_t reps, double *out) {
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
@@ -2178,6 +2319,18 @@ int pdgpu_launch_count(pdgpu_ctx *c, int64_t *count) {
     return PDGPU_ERR_ARG;
   }
   *count = launch_counter().load();
+  return PDGPU_OK;
+}
+
+int pdgpu_graph_replays(pdgpu_ctx *c, int32_t sys, int64_t *replays) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  if (!replays) {
+    set_error("replays is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  replays[0] = e->graph_replays;
+  replays[1] = (int64_t)e->gslots.size();
   return PDGPU_OK;
 }
 

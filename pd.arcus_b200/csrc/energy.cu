@@ -43,15 +43,17 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode,
   for (int k = 0; k < P_COUNT; k++) acc[k] = 0.0;
   int a0 = v.atom_off[s] + c * kChunk, a1 = min(a0 + kChunk, v.atom_off[s + 1]);
   bool atoms = mode & (EM_PAIR_GB | EM_PAIR_NB | EM_BORN_ENERGY | EM_KINETIC | EM_SURF);
+  const double *ep = v.ebuf ? v.e_pair_alt : v.e_atom;  // the pair slots of this energy buffer
+  int *sflags = v.ebuf ? v.sys_flags_alt : v.sys_flags;
   if (atoms)
     for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
       if (mode & (EM_PAIR_GB | EM_PAIR_NB)) {
-        acc[P_VDW] += v.e_atom[(size_t)AE_VDW * N + i];
-        acc[P_ELEC] += v.e_atom[(size_t)AE_ELEC * N + i];
+        acc[P_VDW] += ep[(size_t)AE_VDW * N + i];
+        acc[P_ELEC] += ep[(size_t)AE_ELEC * N + i];
       }
       if (mode & (EM_PAIR_GB | EM_BORN_ENERGY)) {
-        acc[P_POL] += v.e_atom[(size_t)AE_POL * N + i];
-        acc[P_SELF] += v.e_atom[(size_t)AE_POL_SELF * N + i];
+        acc[P_POL] += ep[(size_t)AE_POL * N + i];
+        acc[P_SELF] += ep[(size_t)AE_POL_SELF * N + i];
       }
       if (mode & EM_PAIR_NB) acc[P_NBVIR] += v.e_atom[(size_t)AE_VIR * N + i];
       if (mode & EM_SURF) acc[P_SURF] += v.e_atom[(size_t)AE_SURF * N + i];
@@ -114,7 +116,7 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode,
   } else if (warp == P_COUNT) {
     static_assert(E_COUNT <= 30, "one lane per record slot");
     if (lane < E_COUNT) sE[lane] = __ldcg(E + lane);
-    if (lane == 30) sflag = __ldcg(v.sys_flags + s);
+    if (lane == 30) sflag = __ldcg(sflags + s);
     if (lane == 31 && (mode & EM_RECORD)) sk = __ldcg(step_dev) - __ldcg(step_dev + 1);
   } else {
     static_assert(kEnergyThreads / 32 > P_COUNT, "a spare warp reads the record");
@@ -167,7 +169,7 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode,
   __syncthreads();
   if (warp == 0) {
     if (lane < E_COUNT) E[lane] = sE[lane];
-    if (lane == 31) v.sys_flags[s] = 0;  // consumed
+    if (lane == 31) sflags[s] = 0;  // consumed
     if ((mode & EM_RECORD) && lane < 3) {
       double *h = hist + ((size_t)sk * v.n_sys + s) * 3;
       h[lane] = sE[lane == 0 ? E_EPOT : lane == 1 ? E_EKIN : E_ETOT];

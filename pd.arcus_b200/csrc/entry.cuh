@@ -9,6 +9,9 @@
 
 namespace pdgpu {
 const char *last_error_cstr();
+// load the allocation-free list build's static scratch on the current
+// device and look up its address (noalloc.cu)
+int noalloc_prepare_current_device();
 void launch_md_step_impl(const PackView &v, cudaStream_t st, const MDCoef &c, const double *normals,
                          const int *step_dev, const unsigned char *is_h, const unsigned long long *seeds,
                          double *frames = nullptr, int frame_every = 0, int frame_cap = 0);
@@ -84,17 +87,40 @@ struct SysEntry {
   void *min_state = nullptr;
   void *mc_state = nullptr;
   std::vector<void *> extra;
-  // cached MD block graph
+  // cached MD block graph (the request loop's job graph)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   std::string gkey;
   long long gnodes = 0;
+  // MD step-block graphs of pdgpu_md_run, keyed by everything baked into
+  // them (block length, whether the block starts with a list rebuild,
+  // buffers, integrator settings).  A run that starts inside a list period,
+  // or ends inside one, replays a graph for its partial head or tail block
+  // as well as the whole-period graph; the few most recent stay cached.
+  struct GraphSlot {
+    std::string key;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long nodes = 0;
+    long long used = 0;
+  };
+  static constexpr int kGraphSlots = 4;
+  std::vector<GraphSlot> gslots;
+  long long gclock = 0;
+  long long graph_replays = 0;  // step-block graph launches (pdgpu_graph_replays)
+  void drop_slot(GraphSlot &g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    g = GraphSlot();
+  }
   void drop_graph() {
     if (gexec) cudaGraphExecDestroy(gexec);
     if (graph) cudaGraphDestroy(graph);
     gexec = nullptr;
     graph = nullptr;
     gkey.clear();
+    for (auto &g : gslots) drop_slot(g);
+    gslots.clear();
   }
   void free_device() {
     drop_graph();
@@ -135,9 +161,10 @@ bool has_bonded(const Pack &P);
 // chain rule, surface term; one energy reduction if reduce.  `step` is
 // where the surface term reads WorkSpace::Step (default: e->ws_step).
 void calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce);
-void calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce, StepSrc step);
-// one MD step: forces, integrator, energy record (+ step counter advance)
-void md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k);
+void calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce, StepSrc step, int ebuf = 0);
+// one MD step: forces, integrator, energy record (+ step counter advance);
+// q = the step's index in its block (its energy buffer is q & 1 on tiles)
+void md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k, int q);
 void md_steps_end(cudaStream_t st, SysEntry *e);
 MDCoef md_coef(const pdgpu_md_params *p, int step, int steps);
 // grow a pack's list buffer to hold `total` entries (stream-ordered)

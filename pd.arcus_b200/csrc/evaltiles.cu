@@ -1,0 +1,716 @@
+// One GB evaluation on the cluster-pair tiles in one persistent launch.
+//
+// FF_GeneralizedBorn_Still::calcForces in FastMode (gbff.cpp:168-180) has
+// three passes over the pairs with a global dependency between each:
+//   A  Born-radius sums (calcBornRadii_PairwiseApprox, gbff.cpp:415-466);
+//      every pair term must be in before a radius can be formed
+//   B  GB + LJ + Coulomb (calcForcesIncludingVacuo loop 1, :1529-1736);
+//      needs every radius, and leaves each atom's dE/da complete only when
+//      every pair is in
+//   C  Born-radius chain rule (loop 2, :1751-1818); needs every dE/da.
+// Here the three are phases of one cooperative launch (every block
+// resident), separated by two grid barriers.  The per-atom steps between
+// them are folded into the phases: phase B forms each atom's Born radius
+// from its fixed-point sum when it stages the atom (the FP64 expression of
+// k_born_finish, so the same bits), and phase C forms each atom's chain
+// weight gpi * dE/da the same way.  The per-atom outputs (Born radii, the
+// per-atom energies) are written by grid-stride epilogues that nothing in
+// the same phase reads.
+//
+// Every warp keeps one contiguous tile range for phases A and B (an equal
+// share of the pack's tiles).  Phase A also notes the tiles that hold a
+// pair inside the Still cutoff (within the guard band); phase C runs over
+// that compacted list only, in equal shares.  As in the separate passes
+// (tiles.cu), a tile's sums depend on the tile alone and are added in
+// 64-bit fixed point, so results do not depend on how the tiles are spread
+// over warps, on the grid, or on the batch a system sits in.
+//
+// The barriers spin with a bounded number of naps; a barrier that runs out
+// sets F_BARRIER, and every block then returns (the host reports it and
+// clears the counter).  The same kernel runs one phase per launch where a
+// cooperative launch is not available (PDGPU_FUSED=0, or a grid that cannot
+// be resident): three launches, the same arithmetic, the same results.
+//
+// Pair arithmetic: the phase-A Born terms are those of the row and tile
+// passes (born_term_noV, explicit roundings: the same Born radii bit for
+// bit); phases B and C follow gb_pair_term and chain_term with every
+// selection branch-free except the GB cross term and the rare FP64
+// re-decisions.  The j records of a tile are stored twice in shared memory
+// (slots 0-7 and 8-15) so lane a reads j atom (a + t) mod 8 at slot a + t
+// with a fixed offset per step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdlib>
+
+#include "tilecommon.cuh"
+
+namespace pdgpu {
+
+constexpr int kEvWarps = 4;  // warps per block
+#ifndef PDGPU_EV_BLOCKS
+#define PDGPU_EV_BLOCKS 5    // resident blocks per SM the register allocation must allow
+#endif
+constexpr unsigned kBarrierNaps = 1u << 22;  // about half a second of 100 ns naps
+
+// ------------------------------------------------------------- barrier
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+  unsigned x;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(x) : "l"(p) : "memory");
+  return x;
+}
+// Grid barrier over a counter that counts arrivals; every block waits for
+// `target` arrivals.  False when the wait ran out (the flag is set).
+__device__ __forceinline__ bool grid_barrier(unsigned *ctr, unsigned target, int *flags) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(ctr, 1u);
+    int ok = 1;
+    unsigned naps = 0;
+    while (ld_acquire_u32(ctr) < target) {
+      if (++naps > kBarrierNaps) {
+        ok = 0;
+        atomicExch(&flags[F_BARRIER], 1);
+        break;
+      }
+      __nanosleep(100);
+    }
+    __threadfence();
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+// This warp's share [e0, e1) of T work items.
+__device__ __forceinline__ void ev_range(long long T, int warp, int &e0, int &e1) {
+  const long long G = (long long)gridDim.x * kEvWarps;
+  const long long g = (long long)blockIdx.x * kEvWarps + warp;
+  e0 = (int)(T * g / G);
+  e1 = (int)(T * (g + 1) / G);
+}
+
+// Born radius of atom i from its fixed-point sum (k_born_finish's FP64
+// expression, gbff.cpp:463-465).
+__device__ __forceinline__ double born_radius(const PackView &v, const SysParams &P, int i) {
+  const double Gpol = v.terms123[i] + (double)v.bsum[i] * kInvBornScale;
+  return -P.halfeconv_d / Gpol + P.born_offset_d;
+}
+
+// A lane's bond-order rows rotated so bit t is j atom (a + t) mod 8.
+__device__ __forceinline__ unsigned rot8(unsigned row, int a) {
+  row &= 0xffu;
+  return ((row >> a) | (row << (8 - a))) & 0xffu;
+}
+
+// Tile staging shared by the phases: the tile's metadata, this lane's row
+// bits and, in lanes 0..7, the j atom's records, prefetched one tile ahead.
+struct EvStage {
+  int4 m;
+  unsigned row;
+  float4 a, b, c;
+};
+
+// ============================================================= phase A
+// Born sums.  Each term is converted to fixed point and added exactly
+// (the row and tile passes' arithmetic).  Tiles with a pair inside the
+// Still cutoff's guard band are appended to the still list in runs of up
+// to 32 (per-warp order inside a run).
+__device__ __forceinline__ void phase_born(const PackView &v, int warp, int lane, float4 (*sA)[16],
+                                           float4 (*sB)[16], float4 (*sC)[16]) {
+  int e, e1;
+  ev_range(v.tile_count[0], warp, e, e1);
+  const int g8 = lane & ~7, a = lane & 7;
+  int a0 = -1, na = 0, i = 0;
+  float4 ia = make_float4(0, 0, 0, 0), ib = ia;
+  float Ri = 0.f, Vi = 0.f, s_hi = 0.f, s_lo = 0.f, invP5 = 0.f, piP5 = 0.f, P4s = 0.f;
+  double still2_d = 0.0;
+  long long acc_i = 0;
+  unsigned near = 0;
+  int run0 = e;
+  EvStage nx;
+  auto load = [&](int t, EvStage &q) {
+    q.m = v.tile_meta[t];
+    q.row = tile_row(v, t, lane);
+    if (lane <= (q.m.w & 7)) {
+      const int j = q.m.x + lane;
+      q.a = v.pq[2 * (size_t)j];
+      q.b = v.pq[2 * (size_t)j + 1];
+      q.c = v.prm[j];
+    }
+  };
+  auto flush_near = [&](int upto) {
+    // tiles [run0, upto) with their bits in `near`
+    const int cnt = __popc(near);
+    if (cnt) {
+      int base = 0;
+      if (lane == 0) base = atomicAdd(&v.tile_count[2], cnt);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if ((near >> lane) & 1u) v.still_list[base + __popc(near & ((1u << lane) - 1u))] = run0 + lane;
+    }
+    near = 0;
+    run0 = upto;
+  };
+  if (e < e1) load(e, nx);
+  for (; e < e1; e++) {
+    const EvStage cur = nx;
+    const TileInfo ti = tile_info(cur.m);
+    if (e + 1 < e1) load(e + 1, nx);
+    if (ti.a0 != a0) {
+      if (lane < na && acc_i) atomicAdd((unsigned long long *)&v.bsum[a0 + lane], (unsigned long long)acc_i);
+      acc_i = 0;
+      a0 = ti.a0;
+      na = ti.na;
+      i = a0 + (lane < na ? lane : 0);
+      ia = v.pq[2 * (size_t)i];
+      ib = v.pq[2 * (size_t)i + 1];
+      const float4 pi = v.prm[i];
+      Ri = pi.z;
+      Vi = pi.w;
+      const SysParams &P = v.sp[ti.s];
+      s_hi = P.still2 * (1.f + 4e-6f);
+      s_lo = P.still2 * (1.f - 4e-6f);
+      invP5 = P.invP5;
+      piP5 = P.piP5;
+      P4s = P.P4 * (float)kBornScale;
+      still2_d = P.still2_d;
+    }
+    if (lane < ti.nb) {
+      sA[warp][lane] = sA[warp][lane + 8] = cur.a;
+      sB[warp][lane] = sB[warp][lane + 8] = cur.b;
+      sC[warp][lane] = sC[warp][lane + 8] = make_float4(cur.c.z, cur.c.w, 0.f, 0.f);
+    }
+    unsigned rows = cur.row;
+    if (ti.spec >= 0) rows &= ~spec_row(v, ti.spec, 0, lane);  // bond order > 2 only
+    rows = rot8(rows, a);
+    __syncwarp();
+    long long jacc = 0;  // lane (g,a): j atom a, this group's i atoms
+    bool any = false;    // a pair inside the Still cutoff's guard band
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+      long long tI = 0, tJ = 0;
+      if ((rows >> t) & 1u) {
+        const float4 ja = sA[warp][a + t], jb = sB[warp][a + t];
+        const Dx d = diff(ia, ib, ja, jb);
+        bool ok = d.r2 <= s_lo;
+        if (!ok && d.r2 <= s_hi) {
+          const int j = ti.b0 + ((a + t) & 7);
+          ok = !(ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]) > still2_d);
+        }
+        any |= d.r2 <= s_hi;
+        if (ok) {
+          const float4 jc = sC[warp][a + t];
+          const float term = born_term_noV(d, Ri, jc.x, invP5, piP5, P4s);
+          tI = __float2ll_rn(__fmul_rn(term, jc.y));
+          tJ = __float2ll_rn(__fmul_rn(term, Vi));
+        }
+      }
+      acc_i += tI;
+      jacc += __shfl_sync(0xffffffffu, tJ, g8 | ((a - t) & 7));
+    }
+    if (__any_sync(0xffffffffu, any)) {
+      near |= 1u << (e - run0);
+      jacc += __shfl_xor_sync(0xffffffffu, jacc, 8);
+      jacc += __shfl_xor_sync(0xffffffffu, jacc, 16);
+      if (lane < ti.nb && jacc) atomicAdd((unsigned long long *)&v.bsum[ti.b0 + lane], (unsigned long long)jacc);
+    }
+    if (e - run0 == 31) flush_near(e + 1);
+    __syncwarp();
+  }
+  if (lane < na && acc_i) atomicAdd((unsigned long long *)&v.bsum[a0 + lane], (unsigned long long)acc_i);
+  flush_near(e1);
+}
+
+// ============================================================= phase B
+// GB + LJ + Coulomb for one pair (gb_pair_term's expressions), every
+// output zero unless `in`.  Selections are branch-free except the GB cross
+// term (skipped by a warp with no pair inside the exp-approximation range)
+// and the FP64 re-decision of that range's edge.
+struct PairOut {
+  float fscal, epol, dedal, vdw, elec;
+};
+__device__ __forceinline__ PairOut pair_gb(const GbSettings &g, float r2, bool in, bool nb, bool b14, float ai,
+                                           float aj, float qiqj, float radsum, float epsij, const PackView &v,
+                                           int i, int j, double ai_d, const SysParams *P) {
+  const float invr = rsqrtf(r2);
+  const float r = r2 * invr;
+  const float aiaj = ai * aj;
+  const float u = __fdividef(-0.25f * r2, aiaj);
+  bool gb = u > g.thr;
+  if (in && fabsf(u - g.thr) <= g.band) {
+    // the FP64 predicate of gbff.cpp:1553-1575 with both radii formed
+    // from their sums (the same values the epilogue stores)
+    const double aj_d = born_radius(v, *P, j);
+    const double srij = ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]);
+    gb = -srij * 0.25 / (ai_d * aj_d) > g.thr_d;
+  }
+  gb = gb && in;
+  const float dr = r - g.rin;
+  const bool on = r >= g.rin;
+  const float sw = 1.f - g.inv_sw2 * dr * dr;
+  const float S = on ? sw * sw : 1.f;
+  const float dSdd = on ? -4.f * g.inv_sw2 * dr * sw : 0.f;
+  float dedr = 0.f, epol = 0.f, dedal = 0.f;
+  if (gb) {
+    const float tg = __expf(u);
+    const float fgb = rsqrtf(r2 + tg * aiaj);
+    const float l = fgb * fgb;
+    const float epol0 = g.premul * qiqj * fgb;
+    const float dedr0 = -epol0 * (r - 0.25f * r * tg) * l;
+    const float dedal0 = -epol0 * tg * (1.f - u) * l;
+    epol = epol0 * S;
+    dedr = S * dedr0 + dSdd * epol0;
+    dedal = dedal0 * S;
+  }
+  const float ec = (gb ? g.econv_in : g.econv_out) * (b14 ? g.elec14 : 1.f) * qiqj * invr;
+  const float elf = S * (-ec * invr) + ec * dSdd;
+  // Lennard-Jones 12-6 with its own switch
+  const float rr = radsum * invr;
+  const float rr2 = rr * rr;
+  const float B = rr2 * rr2 * rr2;
+  const float A = B * B;
+  const float eps = epsij * (b14 ? g.vdw14 : 1.0f);
+  float vdw = (2.f * eps) * (0.5f * A - B);
+  float vdwf = -(12.f * eps * invr) * (A - B);
+  const float vd = r - g.vdw_rin;
+  const float vs = 1.f - g.vdw_inv_sw2 * vd * vd;
+  const bool von = r > g.vdw_rin;
+  const float vS = von ? vs * vs : 1.f;
+  const float vdS = von ? -4.f * g.vdw_inv_sw2 * vd * vs : 0.f;
+  vdwf = vS * vdwf + vdw * vdS;
+  vdw *= vS;
+  const bool lj = in && nb && r < g.vdw_rc;
+  const bool el = in && nb;
+  vdw = lj ? vdw : 0.f;
+  vdwf = lj ? vdwf : 0.f;
+  PairOut o;
+  o.elec = el ? ec * S : 0.f;
+  const float fel = el ? elf : 0.f;
+  o.fscal = in ? dedr * 2.f * invr + (vdwf + fel) * invr : 0.f;
+  o.epol = epol;
+  o.dedal = dedal;
+  o.vdw = vdw;
+  return o;
+}
+
+__device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane, float4 (*sA)[16],
+                                           float4 (*sB)[16], float4 (*sP)[16]) {
+  int e, e1;
+  ev_range(v.tile_count[0], warp, e, e1);
+  const int N = v.n_atoms;
+  const int g8 = lane & ~7, a = lane & 7;
+  int a0 = -1, i = 0, s_cur = -1;
+  float4 ia = make_float4(0, 0, 0, 0), ib = ia, ip = ia;
+  double ai_d = 0.0;
+  const SysParams *P = nullptr;
+  GbSettings gs;
+  EvStage nx;
+  auto load = [&](int t, EvStage &q) {
+    q.m = v.tile_meta[t];
+    q.row = tile_row(v, t, lane);
+    if (lane <= (q.m.w & 7)) {
+      const int j = q.m.x + lane;
+      q.a = v.pq[2 * (size_t)j];
+      q.b = v.pq[2 * (size_t)j + 1];
+      q.c = v.prm[j];
+    }
+  };
+  if (e < e1) load(e, nx);
+  for (; e < e1; e++) {
+    const EvStage cur = nx;
+    const TileInfo ti = tile_info(cur.m);
+    if (e + 1 < e1) load(e + 1, nx);
+    if (ti.s != s_cur) {
+      s_cur = ti.s;
+      P = &v.sp[ti.s];
+      gs.load(*P);
+    }
+    if (ti.a0 != a0) {
+      a0 = ti.a0;
+      i = a0 + (lane < ti.na ? lane : 0);
+      ia = v.pq[2 * (size_t)i];
+      ib = v.pq[2 * (size_t)i + 1];
+      ip = v.prm[i];
+      ai_d = born_radius(v, *P, i);
+      ib.w = (float)ai_d;
+    }
+    if (lane < ti.nb) {
+      float4 b = cur.b;
+      b.w = (float)born_radius(v, *P, ti.b0 + lane);
+      sA[warp][lane] = sA[warp][lane + 8] = cur.a;
+      sB[warp][lane] = sB[warp][lane + 8] = b;
+      sP[warp][lane] = sP[warp][lane + 8] = cur.c;
+    }
+    const unsigned rows = rot8(cur.row, a);
+    unsigned xrows = 0, brows = 0;  // bond order <= 2, == 3
+    if (ti.spec >= 0) {
+      xrows = rot8(spec_row(v, ti.spec, 0, lane), a);
+      brows = rot8(spec_row(v, ti.spec, 1, lane), a);
+    }
+    __syncwarp();
+    float fx = 0.f, fy = 0.f, fz = 0.f, e_vdw = 0.f, e_el = 0.f, e_pol = 0.f, deda = 0.f;
+    float jacc[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+      const float4 ja = sA[warp][a + t], jb = sB[warp][a + t], jp = sP[warp][a + t];
+      const Dx d = diff(ia, ib, ja, jb);
+      const bool in = ((rows >> t) & 1u) && d.r2 <= gs.rc2;
+      const bool nb3 = !((xrows >> t) & 1u);
+      const bool b14 = (brows >> t) & 1u;
+      const PairOut o = pair_gb(gs, d.r2, in, nb3, b14, ib.w, jb.w, ia.w * ja.w, ip.x + jp.x, ip.y * jp.y, v, i,
+                                ti.b0 + ((a + t) & 7), ai_d, P);
+      e_pol += o.epol;
+      deda += o.dedal * jb.w;
+      e_vdw += o.vdw;
+      e_el += o.elec;
+      const float cx = o.fscal * d.x, cy = o.fscal * d.y, cz = o.fscal * d.z;
+      fx -= cx;
+      fy -= cy;
+      fz -= cz;
+      const float c[7] = {cx, cy, cz, o.vdw, o.elec, o.epol, o.dedal * ib.w};
+      const int src = g8 | ((a - t) & 7);
+#pragma unroll
+      for (int q = 0; q < 7; q++) jacc[q] += __shfl_sync(0xffffffffu, c[q], src);
+    }
+#pragma unroll
+    for (int q = 0; q < 7; q++) {
+      jacc[q] += __shfl_xor_sync(0xffffffffu, jacc[q], 8);
+      jacc[q] += __shfl_xor_sync(0xffffffffu, jacc[q], 16);
+    }
+    if (lane < ti.nb) {
+      const int j = ti.b0 + lane;
+      add_fixed(v, &v.hx[j], jacc[0], ti.s);
+      add_fixed(v, &v.hy[j], jacc[1], ti.s);
+      add_fixed(v, &v.hz[j], jacc[2], ti.s);
+#pragma unroll
+      for (int q = 0; q < 4; q++) add_fixed(v, &v.ej[(size_t)q * N + j], jacc[3 + q], ti.s);
+    }
+    if (lane < ti.na) {
+      add_fixed(v, &v.hx[i], fx, ti.s);
+      add_fixed(v, &v.hy[i], fy, ti.s);
+      add_fixed(v, &v.hz[i], fz, ti.s);
+      add_fixed(v, &v.ej[i], e_vdw, ti.s);
+      add_fixed(v, &v.ej[(size_t)N + i], e_el, ti.s);
+      add_fixed(v, &v.ej[(size_t)2 * N + i], e_pol, ti.s);
+      add_fixed(v, &v.ej[(size_t)3 * N + i], deda, ti.s);
+    }
+    __syncwarp();
+  }
+}
+
+// ============================================================= phase C
+// Chain-rule weight of atom i: gpi * dE/da_i, with gpi = a_i^2 / 166.0
+// (the literal of gbff.cpp:1755) and dE/da_i = the pair sum - Eself_i / a_i
+// (gbff.cpp:1731-1757; k_gb_finish's expression).
+__device__ __forceinline__ float chain_weight(const PackView &v, const SysParams &P, int i, int N) {
+  const double ai_d = v.born_d[i];
+  const double dd = (double)v.ej[(size_t)3 * N + i] * kInvJScale;
+  const double qd = (double)v.pq[2 * (size_t)i].w;
+  const double eself = P.premul_d * qd * qd / ai_d;
+  const double deda_i = dd - eself / ai_d;
+  const double gpi = ai_d * ai_d / 166.0;
+  return (float)(gpi * deda_i);
+}
+
+__device__ __forceinline__ void phase_chain(const PackView &v, int warp, int lane, float4 (*sA)[16],
+                                            float4 (*sB)[16], float4 (*sC)[16]) {
+  int q0, q1;
+  ev_range(v.tile_count[2], warp, q0, q1);
+  const int N = v.n_atoms;
+  const int g8 = lane & ~7, a = lane & 7;
+  int a0 = -1, i = 0;
+  float4 ia = make_float4(0, 0, 0, 0), ib = ia, ic = ia;
+  float s_hi = 0.f, s_lo = 0.f, invP5 = 0.f, piP5 = 0.f, P4 = 0.f;
+  double still2_d = 0.0;
+  const SysParams *P = nullptr;
+  EvStage nx;
+  auto load = [&](int q, EvStage &st) {
+    const int t = v.still_list[q];
+    st.m = v.tile_meta[t];
+    st.row = tile_row(v, t, lane);
+    if (lane <= (st.m.w & 7)) {
+      const int j = st.m.x + lane;
+      st.a = v.pq[2 * (size_t)j];
+      st.b = v.pq[2 * (size_t)j + 1];
+      st.c = v.prm[j];
+    }
+  };
+  if (q0 < q1) load(q0, nx);
+  for (int q = q0; q < q1; q++) {
+    const EvStage cur = nx;
+    const TileInfo ti = tile_info(cur.m);
+    if (q + 1 < q1) load(q + 1, nx);
+    if (ti.a0 != a0) {
+      a0 = ti.a0;
+      i = a0 + (lane < ti.na ? lane : 0);
+      ia = v.pq[2 * (size_t)i];
+      ib = v.pq[2 * (size_t)i + 1];
+      const float4 pi = v.prm[i];
+      P = &v.sp[ti.s];
+      ic = make_float4(pi.z, pi.w, chain_weight(v, *P, i, N), 0.f);
+      s_hi = P->still2 * (1.f + 4e-6f);
+      s_lo = P->still2 * (1.f - 4e-6f);
+      invP5 = P->invP5;
+      piP5 = P->piP5;
+      P4 = P->P4;
+      still2_d = P->still2_d;
+    }
+    if (lane < ti.nb) {
+      const float4 c = make_float4(cur.c.z, cur.c.w, chain_weight(v, *P, ti.b0 + lane, N), 0.f);
+      sA[warp][lane] = sA[warp][lane + 8] = cur.a;
+      sB[warp][lane] = sB[warp][lane + 8] = cur.b;
+      sC[warp][lane] = sC[warp][lane + 8] = c;
+    }
+    unsigned rows = cur.row;
+    if (ti.spec >= 0) rows &= ~spec_row(v, ti.spec, 0, lane);  // bond order > 2 only
+    rows = rot8(rows, a);
+    __syncwarp();
+    float fx = 0.f, fy = 0.f, fz = 0.f, j0 = 0.f, j1 = 0.f, j2 = 0.f;
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+      float c0 = 0.f, c1 = 0.f, c2 = 0.f;
+      const float4 ja = sA[warp][a + t], jb = sB[warp][a + t];
+      const Dx d = diff(ia, ib, ja, jb);
+      bool ok = ((rows >> t) & 1u) && d.r2 <= s_lo;
+      if (((rows >> t) & 1u) && !ok && d.r2 <= s_hi) {
+        const int j = ti.b0 + ((a + t) & 7);
+        ok = !(ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]) > still2_d);
+      }
+      if (ok) {
+        const float4 jc = sC[warp][a + t];
+        const float tt = chain_term(d, ic.x, jc.x, ic.y, jc.y, ic.z, jc.z, invP5, piP5, P4);
+        fx += tt * d.x;
+        fy += tt * d.y;
+        fz += tt * d.z;
+        c0 = -tt * d.x;
+        c1 = -tt * d.y;
+        c2 = -tt * d.z;
+      }
+      const int src = g8 | ((a - t) & 7);
+      j0 += __shfl_sync(0xffffffffu, c0, src);
+      j1 += __shfl_sync(0xffffffffu, c1, src);
+      j2 += __shfl_sync(0xffffffffu, c2, src);
+    }
+    j0 += __shfl_xor_sync(0xffffffffu, j0, 8);
+    j1 += __shfl_xor_sync(0xffffffffu, j1, 8);
+    j2 += __shfl_xor_sync(0xffffffffu, j2, 8);
+    j0 += __shfl_xor_sync(0xffffffffu, j0, 16);
+    j1 += __shfl_xor_sync(0xffffffffu, j1, 16);
+    j2 += __shfl_xor_sync(0xffffffffu, j2, 16);
+    if (lane < ti.nb) {
+      const int j = ti.b0 + lane;
+      add_fixed(v, &v.hx[j], j0, ti.s);
+      add_fixed(v, &v.hy[j], j1, ti.s);
+      add_fixed(v, &v.hz[j], j2, ti.s);
+    }
+    if (lane < ti.na) {
+      add_fixed(v, &v.hx[i], fx, ti.s);
+      add_fixed(v, &v.hy[i], fy, ti.s);
+      add_fixed(v, &v.hz[i], fz, ti.s);
+    }
+    __syncwarp();
+  }
+}
+
+// ============================================================= per-atom steps
+// Before phase A: zero what phase B adds into (and, first in an
+// evaluation, the forces and the record; ZeroFlags), as k_born_finish did.
+__device__ __forceinline__ void prologue_zero(const PackView &v, int zero) {
+  const int N = v.n_atoms;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+    for (int q = 0; q < 4; q++) v.ej[(size_t)q * N + i] = 0;
+    if (zero) {
+      if (zero & ZF_BONDED) {
+        v.fx[i] = 0;
+        v.fy[i] = 0;
+        v.fz[i] = 0;
+      }
+      v.gx[i] = 0.0;
+      v.gy[i] = 0.0;
+      v.gz[i] = 0.0;
+      v.hx[i] = 0;
+      v.hy[i] = 0;
+      v.hz[i] = 0;
+      const int s = v.sys_of[i];
+      if ((zero & ZF_RECORD) && i == v.atom_off[s]) {
+        for (int k = 0; k < E_COUNT; k++)
+          if (k != E_EKIN) v.ene[(size_t)s * E_COUNT + k] = 0.0;
+        v.sys_flags[s] = 0;
+        v.sys_flags_alt[s] = 0;
+      }
+    }
+  }
+}
+// After phase B (no phase-B reader of these): the Born radii.
+__device__ __forceinline__ void epilogue_radii(const PackView &v) {
+  const int N = v.n_atoms;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+    const double a = born_radius(v, v.sp[v.sys_of[i]], i);
+    v.born_d[i] = a;
+    reinterpret_cast<float *>(&v.pq[2 * (size_t)i + 1])[3] = (float)a;
+  }
+}
+// After phase C: the per-atom energies (k_gb_finish's values) and the
+// Born sums cleared for the next evaluation.
+__device__ __forceinline__ void epilogue_energies(const PackView &v) {
+  const int N = v.n_atoms;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+    const SysParams &P = v.sp[v.sys_of[i]];
+    const double dv = (double)v.ej[i] * kInvJScale;
+    const double de = (double)v.ej[(size_t)N + i] * kInvJScale;
+    const double dp = (double)v.ej[(size_t)2 * N + i] * kInvJScale;
+    const double ai_d = v.born_d[i];
+    const double qd = (double)v.pq[2 * (size_t)i].w;
+    double *ep = v.ebuf ? v.e_pair_alt : v.e_atom;  // the pair slots of this energy buffer
+    ep[(size_t)AE_VDW * N + i] = 0.5 * dv;
+    ep[(size_t)AE_ELEC * N + i] = 0.5 * de;
+    ep[(size_t)AE_POL * N + i] = dp;
+    ep[(size_t)AE_POL_SELF * N + i] = P.premul_d * qd * qd / ai_d;
+    v.bsum[i] = 0;
+  }
+}
+
+// ============================================================= the kernel
+// PH: which phases (1 A, 2 B, 4 C); more than one needs a cooperative
+// launch.  tile_count[2] is the still-list length, tile_count[3] the
+// barrier / exit counter; the last block out clears both.
+template <int PH>
+__global__ void __launch_bounds__(32 * kEvWarps, PDGPU_EV_BLOCKS) k_eval_tiles(PackView v, int zero) {
+  PDGPU_DEP_ENTRY();
+  if (v.flags[F_NL_OVERFLOW]) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ float4 s0[kEvWarps][16], s1[kEvWarps][16], s2[kEvWarps][16];
+  unsigned *ctr = reinterpret_cast<unsigned *>(&v.tile_count[3]);
+  const unsigned G = gridDim.x;
+  unsigned passed = 0;  // barriers this launch has crossed
+  if (PH & 1) {
+    prologue_zero(v, zero);
+    phase_born(v, warp, lane, s0, s1, s2);
+  }
+  if ((PH & 1) && (PH & 6)) {
+    if (!grid_barrier(ctr, G * ++passed, v.flags)) return;
+  }
+  if (PH & 2) {
+    phase_pair(v, warp, lane, s0, s1, s2);
+    epilogue_radii(v);
+  }
+  if ((PH & 2) && (PH & 4)) {
+    if (!grid_barrier(ctr, G * ++passed, v.flags)) return;
+  }
+  if (PH & 4) {
+    phase_chain(v, warp, lane, s0, s1, s2);
+    epilogue_energies(v);
+    // the last block out clears the still list and the counter
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const unsigned prev = atomicAdd(ctr, 1u);
+      if (prev == G * (passed + 1) - 1) {
+        v.tile_count[2] = 0;
+        atomicExch(ctr, 0u);
+      }
+    }
+  }
+}
+
+// ============================================================= host side
+static int fused_wanted() {
+  static int w = -1;
+  if (w < 0) {
+    const char *s = getenv("PDGPU_FUSED");
+    w = (s && s[0] == '0') ? 0 : 1;
+  }
+  return w;
+}
+
+// Resident blocks of the evaluation kernel on this device (the grid of its
+// cooperative launch), and no more warps than a pack can have tiles.
+int eval_tiles_grid(long long tile_cap) {
+  int dev = 0, sms = 148, occ = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_eval_tiles<7>, 32 * kEvWarps, 0);
+  const long long need = (tile_cap + kEvWarps - 1) / kEvWarps;
+  return (int)std::max(1LL, std::min((long long)std::max(occ, 1) * sms, need));
+}
+
+template <int PH>
+static cudaError_t launch_ev(const PackView &v, cudaStream_t st, int zero, bool coop) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(v.ev_blocks);
+  cfg.blockDim = dim3(32 * kEvWarps);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[2];
+  int na = 0;
+  if (coop) {
+    attr[na].id = cudaLaunchAttributeCooperative;
+    attr[na].val.cooperative = 1;
+    na++;
+  }
+  // programmatic dependent launch for the one-phase launches (a
+  // cooperative launch waits for the kernel before it in the stream)
+  if (!coop && pdl_enabled()) {
+    attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[na].val.programmaticStreamSerializationAllowed = 1;
+    na++;
+  }
+  cfg.attrs = attr;
+  cfg.numAttrs = na;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, k_eval_tiles<PH>, v, zero);
+  count_launch();
+  return e;
+}
+
+// The three GB passes on the tiles: one cooperative launch when allowed,
+// else three launches of the same phases.
+cudaError_t launch_eval_tiles(const PackView &v, cudaStream_t st, int zero, bool coop) {
+  if (!v.n_sc || v.ev_blocks <= 0) return cudaSuccess;
+  if (coop && fused_wanted()) return launch_ev<7>(v, st, zero, true);
+  cudaError_t e = launch_ev<1>(v, st, zero, false);
+  if (e == cudaSuccess) e = launch_ev<2>(v, st, 0, false);
+  if (e == cudaSuccess) e = launch_ev<4>(v, st, 0, false);
+  return e;
+}
+
+cudaError_t launch_born_phase_only(const PackView &v, cudaStream_t st) {
+  if (!v.n_sc || v.ev_blocks <= 0) return cudaSuccess;
+  return launch_ev<1>(v, st, 0, false);
+}
+
+// Device times of the evaluation: the three phases as three launches
+// (ms[0..2]), then the one cooperative launch (ms[3]); averages over reps.
+// The forces of the timed evaluations are left in the accumulators.
+cudaError_t profile_eval_tiles(const PackView &v, cudaStream_t st, int reps, double *ms) {
+  cudaEvent_t ev[5];
+  for (int q = 0; q < 5; q++) cudaEventCreate(&ev[q]);
+  double acc[4] = {0, 0, 0, 0};
+  cudaError_t e = cudaSuccess;
+  for (int it = 0; it < reps && e == cudaSuccess; it++) {
+    cudaEventRecord(ev[0], st);
+    e = launch_ev<1>(v, st, ZF_PAIRS, false);
+    cudaEventRecord(ev[1], st);
+    if (e == cudaSuccess) e = launch_ev<2>(v, st, 0, false);
+    cudaEventRecord(ev[2], st);
+    if (e == cudaSuccess) e = launch_ev<4>(v, st, 0, false);
+    cudaEventRecord(ev[3], st);
+    if (e == cudaSuccess) e = launch_ev<7>(v, st, ZF_PAIRS, true);
+    cudaEventRecord(ev[4], st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    for (int q = 0; q < 4 && e == cudaSuccess; q++) {
+      float t = 0;
+      cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
+      acc[q] += t;
+    }
+  }
+  for (int q = 0; q < 5; q++) cudaEventDestroy(ev[q]);
+  for (int q = 0; q < 4; q++) ms[q] = reps > 0 ? acc[q] / reps : 0.0;
+  return e;
+}
+
+}  // namespace pdgpu

@@ -211,20 +211,30 @@ struct PackView {
                               // i-cluster's first atom, system << 8 | (i atoms - 1) << 3 | (j atoms - 1)
   unsigned *tile_rows;        // [8*tile_cap] byte l = i lane l's list bits over the 8 j atoms
   unsigned *spec_rows;        // [16*spec_cap] bytes 0..31 bond order <= 2, 32..63 == 3
-  int *tile_count;            // [2] tiles, bond-order row sets
+  int *tile_count;            // [4] tiles, bond-order row sets, still-list length, evaluation barrier counter
   long long tile_cap, spec_cap;
   int tile_blocks[3];         // resident blocks of the three tile passes (persistent grids)
+  int *still_list;            // [tile_cap] tiles with a pair inside the Still cutoff (evaluation kernel)
+  int ev_blocks;              // grid of the evaluation kernel (its resident blocks)
   long long *bsum;            // [N] Born sums of the tile pass, fixed point 2^40
   long long *hx, *hy, *hz;    // [N] pair forces of the tile passes, fixed point 2^24 kcal/mol/A
   long long *ej;              // [4*N] LJ, Coulomb, GB energies and dE/da of the tile pass, fixed point 2^24
   int *flags;                 // [8] overflow / nan / etc.
   int *sys_flags;             // [S] SysFlag bits of the current evaluation
+  // energy buffer 1 (ebuf): the evaluation kernel on the tiles and the
+  // energy record of an MD step alternate between two copies of the pair
+  // slots of e_atom (AE_VDW .. AE_POL_SELF) and of sys_flags, so a step's
+  // record can run beside the next step's evaluation
+  double *e_pair_alt;         // [4N]
+  int *sys_flags_alt;         // [S]
+  int ebuf;                   // 0: e_atom / sys_flags, 1: the copies (set per launch)
   BondedTerms bt;
   LcpoView lc;
 };
 
 // F_LCPO_CAND: an atom had more LCPO overlap candidates than a warp sorts
-enum Flag { F_NL_OVERFLOW = 0, F_NAN = 1, F_CELL_CLAMP = 2, F_LCPO_CAND = 3, F_COUNT = 8 };
+// F_BARRIER: a grid barrier of the evaluation kernel ran out of time
+enum Flag { F_NL_OVERFLOW = 0, F_NAN = 1, F_CELL_CLAMP = 2, F_LCPO_CAND = 3, F_BARRIER = 4, F_COUNT = 8 };
 constexpr const char *kLcpoCandMsg =
     "an atom has more than 256 LCPO overlap candidates (atoms closer than their radii + 2.8 A)";
 // per system: a tile pass met a non-finite pair term (its fixed-point sums
@@ -290,9 +300,26 @@ struct Pack {
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   // an MD step's energy record runs on the second stream beside the next
-  // step's first passes; the next writer of what it reads waits on ene_done
-  cudaEvent_t fork2 = nullptr, ene_done = nullptr;
-  bool energy_pending = false;
+  // step's first passes; the next writer of what it reads waits on its
+  // ene_done event.  On the tile layout step q of a block records from
+  // energy buffer q & 1 (PackView::ebuf): the evaluation of step q + 1
+  // writes the other buffer and does not wait; the evaluation of step q + 2
+  // and the integrator of step q + 1 (it writes the kinetic energies the
+  // record reads) do.  The row passes use buffer 0 only and wait for every
+  // pending record before the fused pass.
+  cudaEvent_t fork2 = nullptr, ene_done[2] = {nullptr, nullptr};
+  bool ene_pending[2] = {false, false};
+  int last_ebuf = 0;             // buffer of the last evaluation's per-atom energies
+  bool energy_pending() const { return ene_pending[0] || ene_pending[1]; }
+  void wait_energy(cudaStream_t s, int b) {
+    if (ene_pending[b]) {
+      cudaStreamWaitEvent(s, ene_done[b], 0);
+      ene_pending[b] = false;
+    }
+  }
+  // evaluations may use the cooperative single-launch kernel (not for the
+  // request loop's jobs, whose streams run side by side)
+  bool coop = true;
   ~Pack();
 };
 
@@ -345,6 +372,17 @@ void launch_tile_counts(const PackView &v, cudaStream_t st, unsigned long long *
 void launch_born_radii_tile(const PackView &v, cudaStream_t st, int zero);
 void launch_gb_pair_tile(const PackView &v, cudaStream_t st);
 void launch_gb_chain_tile(const PackView &v, cudaStream_t st);
+// the three tile passes as one evaluation (evaltiles.cu): Born sums, GB +
+// LJ + Coulomb, chain rule, with the finish steps folded in; one
+// cooperative launch when `coop` (and PDGPU_FUSED is not 0), else three
+// launches of the same phases.  zero: ZeroFlags, as launch_born_radii.
+cudaError_t launch_eval_tiles(const PackView &v, cudaStream_t st, int zero, bool coop);
+int eval_tiles_grid(long long tile_cap);
+// the three phases one launch each, timed with events on `st` (ms[0..2]),
+// then the single cooperative launch (ms[3])
+cudaError_t profile_eval_tiles(const PackView &v, cudaStream_t st, int reps, double *ms);
+// the Born-sum phase alone (it fills the still list; instrumentation)
+cudaError_t launch_born_phase_only(const PackView &v, cudaStream_t st);
 // explicit lanes-per-atom variants (4, 8, 16, 32), used by the autotuner
 void launch_born_radii_lpa(const PackView &v, cudaStream_t st, int zero, int lpa);
 void launch_gb_pair_lpa(const PackView &v, cudaStream_t st, int lpa);

@@ -13,7 +13,9 @@
 // must start at zero is cleared by each call.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstring>
+#include <mutex>
 
 #include "internal.cuh"
 
@@ -49,22 +51,42 @@ constexpr size_t kScratchBytes = kOffParams + align256(sizeof(SysParams));
 static __device__ __align__(256) unsigned char g_nlist_scratch[kScratchBytes];
 
 // Device addresses of the array, looked up once per device (host code may
-// not use the symbol itself: on the host it names a stand-in object).
-static void *g_scratch_dev[64];
+// not use the symbol itself: on the host it names a stand-in object).  The
+// lookup runs under a lock; the filled entries are read without it.
+static std::atomic<void *> g_scratch_dev[64];
+static std::mutex g_scratch_lock;
 
 static int scratch_address(int device, unsigned char **out) {
   if (device < 0 || device >= 64) {
     set_error("device index out of range");
     return PDGPU_ERR_ARG;
   }
-  if (!g_scratch_dev[device]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_nlist_scratch);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(nlist scratch)");
-    g_scratch_dev[device] = p;
+  void *p = g_scratch_dev[device].load(std::memory_order_acquire);
+  if (!p) {
+    std::lock_guard<std::mutex> lock(g_scratch_lock);
+    p = g_scratch_dev[device].load(std::memory_order_relaxed);
+    if (!p) {
+      // with lazy module loading (CUDA_MODULE_LOADING=LAZY, the default)
+      // this first lookup on a device loads the module that holds the
+      // array, which is when the device memory for it is taken
+      cudaError_t e = cudaGetSymbolAddress(&p, g_nlist_scratch);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(nlist scratch)");
+      g_scratch_dev[device].store(p, std::memory_order_release);
+    }
   }
-  *out = (unsigned char *)g_scratch_dev[device];
+  *out = (unsigned char *)p;
   return PDGPU_OK;
+}
+
+// Load the array's module on the current device and look its address up
+// (pdgpu_ctx_create calls this, so a caller that creates its context before
+// reserving its memory pool has the array in place before the pool).
+int noalloc_prepare_current_device() {
+  int device = 0;
+  cudaError_t ce = cudaGetDevice(&device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaGetDevice");
+  unsigned char *base = nullptr;
+  return scratch_address(device, &base);
 }
 
 // (j << 3 | bondorder) -> the reference's packed entry j | bondorder << 24

@@ -271,7 +271,7 @@ void pdgpu_server::enqueue_md_block(Job *j) {
         return;
       }
       rebuild_pairs(P, j->st);
-      for (int q = 0; q < block; q++) md_step_enqueue(j->st, e, j->k);
+      for (int q = 0; q < block; q++) md_step_enqueue(j->st, e, j->k, q);
       md_steps_end(j->st, e);
       ce = cudaStreamEndCapture(j->st, &e->graph);
       e->gnodes = end_capture_count();
@@ -286,7 +286,7 @@ void pdgpu_server::enqueue_md_block(Job *j) {
     launch_counter() += e->gnodes;
   } else {
     if (rebuild) rebuild_pairs(P, j->st);
-    for (int q = 0; q < block; q++) md_step_enqueue(j->st, e, j->k);
+    for (int q = 0; q < block; q++) md_step_enqueue(j->st, e, j->k, q);
     md_steps_end(j->st, e);
   }
   cudaMemcpyAsync(j->pin->flags, v.flags, sizeof(int) * F_COUNT, cudaMemcpyDeviceToHost, j->st);
@@ -359,6 +359,7 @@ void pdgpu_server::admit(Job *j) {
   for (int q = 0; q < 3; q++) P.v.lpa[q] = prm.lanes[q];
   P.v.tile_mode = prm.tiles ? 1 : 0;
   P.tuned = true;
+  P.coop = false;  // jobs run side by side on their own streams: no cooperative launches
   if (prm.tiles && (r = pack_ensure_tiles(&P))) {
     fail(j, r, last_error_cstr());
     return;

@@ -217,7 +217,8 @@ Pack::~Pack() {
   if (fork) cudaEventDestroy(fork);
   if (join) cudaEventDestroy(join);
   if (fork2) cudaEventDestroy(fork2);
-  if (ene_done) cudaEventDestroy(ene_done);
+  for (auto &ev : ene_done)
+    if (ev) cudaEventDestroy(ev);
   if (side) cudaStreamDestroy(side);
   if (cur >= 0 && cur != device) cudaSetDevice(cur);
 }
@@ -246,7 +247,8 @@ int pack_ensure_tiles(Pack *p) {
       palloc(p, &v.tile_rows, 8 * (size_t)v.tile_cap) != cudaSuccess ||
       palloc(p, &v.spec_rows, 16 * (size_t)v.spec_cap) != cudaSuccess ||
       palloc(p, &v.cbox, 6 * (size_t)v.n_jc) != cudaSuccess ||
-      palloc(p, &v.xs, 3 * (size_t)v.n_atoms) != cudaSuccess) {
+      palloc(p, &v.xs, 3 * (size_t)v.n_atoms) != cudaSuccess ||
+      palloc(p, &v.still_list, (size_t)v.tile_cap) != cudaSuccess) {
     set_error("device allocation failed (cluster-pair tiles)");
     return PDGPU_ERR_NOMEM;
   }
@@ -501,6 +503,9 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   PALLOC(v.bbox, (size_t)6 * S);
   PALLOC(v.flags, F_COUNT);
   PALLOC(v.sys_flags, S);
+  PALLOC(v.e_pair_alt, (size_t)4 * N);
+  PALLOC(v.sys_flags_alt, S);
+  v.ebuf = 0;
   PALLOC(p->tmp_keys, N);
   PALLOC(p->tmp_vals, N);
   int tiles = (N + 2047) / 2048;
@@ -535,7 +540,7 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
     v.sc_jc0 = sc_jc0_d;
     v.jc_atom0 = jc_atom0_d;
     v.jc_off = jc_off_d;
-    PALLOC(v.tile_count, 2);  // the tile store itself: pack_ensure_tiles, on first use
+    PALLOC(v.tile_count, 4);  // the tile store itself: pack_ensure_tiles, on first use
     PALLOC(v.bsum, N);
     PALLOC(v.hx, N);
     PALLOC(v.hy, N);
@@ -743,7 +748,8 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&p->fork2, cudaEventDisableTiming);
-  cudaEventCreateWithFlags(&p->ene_done, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&p->ene_done[0], cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&p->ene_done[1], cudaEventDisableTiming);
   cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking);
   cudaError_t e = sync ? cudaStreamSynchronize(st) : cudaGetLastError();
   if (e != cudaSuccess) {

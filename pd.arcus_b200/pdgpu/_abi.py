@@ -169,7 +169,10 @@ PROTOTYPES = {
     "pdgpu_last_run_ms": (ctypes.c_int, [_CTX, _D]),
     "pdgpu_pair_counts": (ctypes.c_int, [_CTX, ctypes.c_int32, _I64]),
     "pdgpu_profile_pair_kernels": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32, _D]),
+    "pdgpu_profile_eval": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32, _D, _I64]),
+    "pdgpu_eval_mode": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32, _I]),
     "pdgpu_launch_count": (ctypes.c_int, [_CTX, _I64]),
+    "pdgpu_graph_replays": (ctypes.c_int, [_CTX, ctypes.c_int32, _I64]),
     "pdgpu_autotune": (ctypes.c_int, [_CTX, ctypes.c_int32, _I]),
     "pdgpu_set_lanes": (ctypes.c_int, [_CTX, ctypes.c_int32, _I]),
     "pdgpu_pair_path": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32, _I]),

@@ -91,6 +91,13 @@ class Batch:
         A.check(A.lib().pdgpu_pair_path(self.ctx.ptr, self._id, int(path), ctypes.byref(cur)))
         return cur.value
 
+    def setEvalMode(self, mode):
+        """Launch form of an evaluation on the tile layout: 1 one
+        cooperative launch, 0 three launches, -1 report only."""
+        cur = ctypes.c_int32(0)
+        A.check(A.lib().pdgpu_eval_mode(self.ctx.ptr, self._id, int(mode), ctypes.byref(cur)))
+        return cur.value
+
     def setSeeds(self, seeds=None):
         if seeds is None:
             A.check(A.lib().pdgpu_set_seeds(self.ctx.ptr, self._id, None))

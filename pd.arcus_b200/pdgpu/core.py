@@ -251,6 +251,14 @@ class WorkSpace:
         A.check(A.lib().pdgpu_pair_path(self.ctx.ptr, self._device(), int(path), ctypes.byref(cur)))
         return cur.value
 
+    def setEvalMode(self, mode):
+        """Launch form of an evaluation on the tile layout: 1 one
+        cooperative launch, 0 three launches, -1 report only; returns the
+        form in use."""
+        cur = ctypes.c_int32(0)
+        A.check(A.lib().pdgpu_eval_mode(self.ctx.ptr, self._device(), int(mode), ctypes.byref(cur)))
+        return cur.value
+
     def backboneAxes(self):
         """(N, CA) then (CA, C) of every residue in order: the bonds
         setResiduePhiPsi turns for phi and psi."""

@@ -5,7 +5,9 @@ host frameworks that reserve all device memory for their own pool at
 start-up and forbid allocation afterwards.  It must give
 the same pair set and bond orders as pdgpu_nlist_build -- compared exactly,
 as sorted pair sets, the tolerance every list test uses -- on two calls in a
-row (its static scratch keeps the previous call's contents).
+row (its static scratch keeps the previous call's contents), and the second
+call must leave the device's free memory and the default pool's usage (and
+its high-water mark) where they were.
 """
 import ctypes
 
@@ -15,6 +17,30 @@ import pytest
 from conftest import load_fixture
 
 pytestmark = pytest.mark.gpu
+
+
+def _pool_usage():
+    """(used, high-water) bytes of device 0's default memory pool, through
+    the driver API (the pool stream-ordered allocations come from)."""
+    cu = ctypes.CDLL("libcuda.so.1")
+    dev = ctypes.c_int(0)
+    assert cu.cuDeviceGet(ctypes.byref(dev), 0) == 0
+    pool = ctypes.c_void_p()
+    assert cu.cuDeviceGetDefaultMemPool(ctypes.byref(pool), dev) == 0
+    used, high = ctypes.c_uint64(0), ctypes.c_uint64(0)
+    assert cu.cuMemPoolGetAttribute(pool, 7, ctypes.byref(used)) == 0   # CU_MEMPOOL_ATTR_USED_MEM_CURRENT
+    assert cu.cuMemPoolGetAttribute(pool, 8, ctypes.byref(high)) == 0   # CU_MEMPOOL_ATTR_USED_MEM_HIGH
+    return used.value, high.value
+
+
+def _reset_pool_high():
+    cu = ctypes.CDLL("libcuda.so.1")
+    dev = ctypes.c_int(0)
+    assert cu.cuDeviceGet(ctypes.byref(dev), 0) == 0
+    pool = ctypes.c_void_p()
+    assert cu.cuDeviceGetDefaultMemPool(ctypes.byref(pool), dev) == 0
+    zero = ctypes.c_uint64(0)  # setting the high-water mark to 0 resets it to the current use
+    assert cu.cuMemPoolSetAttribute(pool, 8, ctypes.byref(zero)) == 0
 
 
 def _rows_sorted(ptr, data):
@@ -55,12 +81,21 @@ def test_nlist_noalloc_matches_nlist_build(name):
     stream = torch.cuda.current_stream(dev).cuda_stream
     for call in range(2):
         entries.fill_(-1)
+        torch.cuda.synchronize()
+        if call == 1:  # the first call has run: no further call takes device memory
+            free0 = torch.cuda.mem_get_info(0)[0]
+            _reset_pool_high()
+            used0, _ = _pool_usage()
         count = ctypes.c_int64(0)
         st = A.lib().pdgpu_nlist_build_noalloc(
             x.data_ptr(), y.data_ptr(), z.data_ptr(), n, cutoff, mid, band.data_ptr(), None, None,
             row_start.data_ptr(), entries.data_ptr(), cap, ctypes.byref(count), stream)
         assert st == 0, A.last_error()
         torch.cuda.synchronize()
+        if call == 1:
+            used1, high1 = _pool_usage()
+            assert torch.cuda.mem_get_info(0)[0] == free0, "the call changed the device's free memory"
+            assert used1 == used0 and high1 == used0, "the call allocated from the default pool"
         assert count.value == len(ref_data)
         ptr = row_start.cpu().numpy().astype(np.int32)
         data = entries[: count.value].cpu().numpy()
