@@ -9,6 +9,10 @@ friction 1/ps.  A "step" is one MD step: list refresh (every 10th), bonded +
 Born radii + fused GB/LJ/Coulomb + chain-rule forces, integrator.
 
 Extra keys of the same JSON line:
+  plain_small the plain small method: one 64-residue peptide (1,001 atoms),
+              Rc 12 A, 1,000 Langevin steps at 1 fs (friction 1e13/s, the
+              reference's default), ns/day beside the reference's own CPU MD
+              on one core.
   batched_sp  512 peptide systems (32 copies of each of the 16 reference-built
               AMBER99 peptides of tests/golden/lib16_amber_s3.npz, lengths
               log-uniform 20-200 residues, each copy with its own RNG key)
@@ -240,7 +244,25 @@ def bench_batched_sp(pdgpu, A, ctx, torch, copies=32, trials=64, plain_trials=2)
     b.close()
     for ws, *_ in members:
         ws.close()
-    return {"metric": "batched GB evals/s", "value": evals / t_all, "unit": "evals/s",
+    # the CPU baseline: the reference's list rebuild + calcForces on every
+    # library peptide, one process per host core
+    cpu = None
+    if os.path.exists(REF_DRIVER):
+        cores = host_cores()
+        jobs = []
+        for a, m in lib:
+            nat = a["charge"].shape[0]
+            k = int(max(3, min(60, 0.8 / (2.7e-3 * (nat / 1000.0) ** 2 + 5e-4))))
+            jobs.append((a, m, "evals", ["--steps", k, "--warmup", 1]))
+        res, wall = run_ref_jobs(jobs, cores)
+        t = [r["seconds"] / r["evals"] for r in res if r]
+        if t:
+            v = cores / float(np.mean(t))
+            cpu = {"value": v, "unit": "evals/s", "cores": cores, "kind": "reference",
+                   "sample": "NeighbourList::calcNewList + Forcefield::calcForces of each of the %d library peptides "
+                             "(3-60 evaluations each), concurrent processes on %d cores; aggregate = cores / mean "
+                             "evaluation time" % (len(t), cores)}
+    return {"metric": "batched GB evals/s", "value": evals / t_all, "unit": "evals/s", "cpu_baseline": cpu,
             "evals": evals, "systems": nsys, "trials_per_system": trials, "atoms_packed": atoms,
             "batch_latency_ms": {"p50": 1e3 * pctl(lat, 50), "p99": 1e3 * pctl(lat, 99)},
             "plain_one_system_per_launch": {"value": n_plain / t_plain, "unit": "evals/s", "sample_evals": n_plain,
@@ -253,7 +275,7 @@ def bench_batched_sp(pdgpu, A, ctx, torch, copies=32, trials=64, plain_trials=2)
             "timing": "wall clock around perturb + list + forces + energies read-back, per batched evaluation"}
 
 
-def bench_batched_md(pdgpu, A, ctx, torch, copies=16, steps=5000, plain_steps=200):
+def bench_batched_md(pdgpu, A, ctx, torch, copies=16, steps=5000, plain_steps=200, drift_steps=1000):
     """All systems advanced together in one CUDA-graph step loop."""
     lib = load_library(LIB_MD)
     L = A.lib()
@@ -299,7 +321,50 @@ def bench_batched_md(pdgpu, A, ctx, torch, copies=16, steps=5000, plain_steps=20
     b.close()
     for ws, *_ in members:
         ws.close()
+    # per-system total-energy drift (the reference's least-squares slope,
+    # md.cpp:182-189, 236-240) over the timed steps, and beside it the
+    # reference's own FP64 MD on a sample of members (same start, its own
+    # random draws: the two drifts agree statistically, not step by step)
+    abs_steps = np.arange(20, 20 + steps)
+    drifts = np.array([ls_drift(abs_steps, h[:, s, 2], total) for s in range(nsys)], dtype=np.float64)
+    drift = {"unit": "kcal/mol per 1000 steps",
+             "gpu_all_systems": {"median": float(np.median(drifts)), "p10": float(np.percentile(drifts, 10)),
+                                 "p90": float(np.percentile(drifts, 90)),
+                                 "median_abs": float(np.median(np.abs(drifts)))},
+             "method": "least-squares slope of etot sampled every max(1, Steps/1000) steps after step 50 "
+                       "(MolecularDynamics::run_core)"}
+    cpu = None
+    if os.path.exists(REF_DRIVER):
+        cores = host_cores()
+        sample = list(range(min(len(lib), 2)))
+        opls = [(a, dict(m, param="oplsaal.ff")) for a, m in lib]
+        jobs = [(opls[k][0], opls[k][1], "time", ["--steps", drift_steps, "--warmup", 0, "--nlist-every", 10,
+                                                   "--drift"]) for k in sample]
+        jobs += [(a, m, "time", ["--steps", 30, "--warmup", 10, "--nlist-every", 10]) for a, m in opls]
+        res, wall = run_ref_jobs(jobs, cores)
+        rows = []
+        for k, r in zip(sample, res[:len(sample)]):
+            if not r:
+                continue
+            hk = hist.reshape(steps, nsys, 3)[:drift_steps - 20, k, 2] * pdgpu.J2KCAL_NA
+            rows.append({"member": k, "atoms": int(r["natoms"]), "reference": r.get("drift_kcal_per_1000"),
+                         "gpu": ls_drift(np.arange(20, drift_steps), hk, drift_steps)})
+        drift["vs_reference"] = rows
+        drift["reference_sample"] = ("%d Langevin steps (1/ps, 300 K) of members %s from the fixture coordinates; the "
+                                     "GPU figure is the same member's steps 20-%d of the batched run"
+                                     % (drift_steps, sample, drift_steps))
+        # the CPU baseline: one reference process per host core; each of the
+        # 16 library members timed over 30 MD steps, and a core advancing
+        # the library's mix at the mean step time
+        t = [r["seconds"] / 30 for r in res[len(sample):] if r]
+        if t:
+            cpu = {"value": cores * DT_FS * 1e-6 / float(np.mean(t)) * 86400.0, "unit": "ns/day", "cores": cores,
+                   "kind": "reference",
+                   "sample": "30 reference MD steps (after 10) of each of the %d OPLS-AA library members, run as "
+                             "concurrent processes on %d cores; aggregate = cores x 1 fs / mean step time" % (len(t),
+                                                                                                        cores)}
     return {"metric": "batched GB MD aggregate ns/day", "value": agg, "unit": "ns/day", "systems": nsys,
+            "drift": drift, "cpu_baseline": cpu,
             "steps": steps, "atoms_packed": atoms, "ms_per_step": ms / steps,
             "plain_one_system": {"value": one_nsday, "unit": "ns/day", "atoms": int(a["charge"].shape[0]),
                                  "steps": plain_steps},
@@ -309,6 +374,59 @@ def bench_batched_md(pdgpu, A, ctx, torch, copies=16, steps=5000, plain_steps=20
             "finite": bool(np.all(np.isfinite(h))),
             "gpu_launches": int(lc1.value - lc0.value),
             "timing": "CUDA events around the device step loop (pdgpu_last_run_ms)"}
+
+
+def bench_plain_small(pdgpu, A, ctx, torch, steps=1000, cpu_steps=200):
+    """The plain small method: one seeded 64-residue peptide (1,001 atoms,
+    tests/golden/c1_pep64_s0.npz), AMBER99 + Still GB + bonded, Rc 12 A, list
+    every 10 steps, Langevin at 1 fs and 300 K with the reference's default
+    friction (1e13 /s), 1,000 steps; beside it the reference's own CPU MD on
+    one core (a bounded sample)."""
+    L = A.lib()
+    path = os.path.join(ROOT, "tests", "golden", "c1_pep64_s0.npz")
+    z = np.load(path)
+    arrays = {k: z[k] for k in z.files}
+    meta = json.loads(bytes(arrays.pop("meta_json")).decode())
+    ws, ff = make_ws(pdgpu, arrays, meta, ctx)
+    n = ws.nAtoms()
+    ws.nlist().calcNewList()
+    ff.calcForces()
+    f_rms = float(np.sqrt(np.sum((ws.cur.f - arrays["f_total"]) ** 2) / np.sum(arrays["f_total"] ** 2)))
+    de = float(abs(ws.ene.epot - arrays["ene_total"][0]) * pdgpu.J2KCAL_NA)
+    p = A.md_params_default()
+    p.Integrator, p.UpdateNList, p.UseGraph = A.INTEGRATOR_LANGEVIN, BLOCK, 1
+    p.Timestep, p.FricCoeff, p.TargetTemp, p.Seed = 1e-15, 1e13, 300.0, 0
+    A.check(L.pdgpu_md_init_velocities(ctx.ptr, ws._sys, 300.0, 0))
+    total = steps + 2 * BLOCK
+    A.check(L.pdgpu_md_run(ctx.ptr, ws._sys, ctypes.byref(p), 0, 2 * BLOCK, total, None))  # warm-up + graphs
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist = np.zeros(3 * steps)
+    A.check(L.pdgpu_md_run(ctx.ptr, ws._sys, ctypes.byref(p), 2 * BLOCK, steps, total, A.dptr(hist)))
+    wall = time.perf_counter() - t0
+    ms = ctx.last_run_ms()
+    h = hist.reshape(steps, 3) * pdgpu.J2KCAL_NA
+    nsday = steps * DT_FS * 1e-6 / (ms / 1e3) * 86400.0
+    out = {"metric": "GB MD ns/day", "value": nsday, "unit": "ns/day", "atoms": n, "steps": steps,
+           "ms_per_step": ms / steps,
+           "wall_clock_ns_per_day": steps * DT_FS * 1e-6 / wall * 86400.0,
+           "parity": {"force_rel_rms_vs_fp64": f_rms, "epot_abs_err_kcal": de},
+           "finite": bool(np.all(np.isfinite(h))),
+           "drift_kcal_per_1000_steps": ls_drift(np.arange(2 * BLOCK, 2 * BLOCK + steps), h[:, 2], total),
+           "workload": "64-residue peptide, AMBER99 + Still GB + bonded, Rc 12 A, Langevin 1 fs 300 K, "
+                       "friction 1e13/s, list every 10 steps",
+           "timing": "CUDA events around the device step loop (pdgpu_last_run_ms)"}
+    ws.close()
+    if os.path.exists(REF_DRIVER):
+        res, _ = run_ref_jobs([(arrays, meta, "time", ["--steps", cpu_steps, "--warmup", 10, "--nlist-every", 10,
+                                                        "--fric", "1e13"])], 1)
+        if res[0]:
+            v = cpu_steps * DT_FS * 1e-6 / res[0]["seconds"] * 86400.0
+            out["cpu_baseline"] = {"value": v, "unit": "ns/day", "cores": 1, "kind": "reference",
+                                   "sample": "%d MD steps after 10 warm-up, reference MolecularDynamics step loop"
+                                             % cpu_steps}
+            out["speedup_vs_cpu"] = nsday / v
+    return out
 
 
 # FP64 operations of one (atom, partner, partner's partner) triple of the
@@ -604,6 +722,77 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ---------------------------------------------------------------- reference CPU baselines
+def host_cores():
+    """Host cores this process may use (the CPU baselines run one reference
+    process per core)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
+def _ref_input(arrays, meta):
+    """A directory the reference driver reads: coordinates and the chains'
+    sequences (it rebuilds the topology with the reference's own builder)."""
+    tmp = tempfile.mkdtemp(prefix="pdref_")
+    np.save(os.path.join(tmp, "pos.npy"), arrays["pos"])
+    chains = meta.get("chains") or meta.get("chain") or []
+    if isinstance(chains, str):
+        chains = [chains]
+    with open(os.path.join(tmp, "meta.txt"), "w") as fh:
+        for c in chains:
+            fh.write("chain %s\n" % c)
+    return tmp
+
+
+def run_ref_jobs(jobs, cores):
+    """Run reference-driver jobs, at most `cores` at a time.  jobs: list of
+    (arrays, meta, mode, extra args).  Returns the parsed JSON line of each
+    job (None where the driver failed) and the wall time."""
+    env = dict(os.environ, PD_PARAM_PATH=REF_PARAM)
+    pending = list(enumerate(jobs))
+    running, out = [], [None] * len(jobs)
+    t0 = time.perf_counter()
+    while pending or running:
+        while pending and len(running) < cores:
+            k, (arrays, meta, mode, extra) = pending.pop(0)
+            d = _ref_input(arrays, meta)
+            cmd = [REF_DRIVER, mode, "--in", d, "--cutoff", str(meta["cutoff"]), "--inner", str(meta["inner"]),
+                   "--param", meta.get("param", "amber99aa.ff")] + [str(x) for x in extra]
+            pr = subprocess.Popen(cmd, env=env, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            running.append((k, pr, d))
+        still = []
+        for k, pr, d in running:
+            if pr.poll() is None:
+                still.append((k, pr, d))
+                continue
+            txt = pr.stdout.read()
+            shutil.rmtree(d, ignore_errors=True)
+            try:
+                out[k] = json.loads(txt.strip().splitlines()[-1])
+            except (ValueError, IndexError):
+                out[k] = None
+        running = still
+        if running:
+            time.sleep(0.01)
+    return out, time.perf_counter() - t0
+
+
+def ls_drift(steps, etot_kcal, total_steps):
+    """MolecularDynamics::run_core's total-energy drift (md.cpp:206,
+    236-240, 182-189): etot sampled every max(1, Steps/1000) steps after
+    step 50, least-squares slope, kcal/mol per 1000 steps."""
+    freq = max(1, total_steps // 1000)
+    steps = np.asarray(steps)
+    keep = (steps > 50) & (steps % freq == 0)
+    x, y = steps[keep].astype(np.float64), np.asarray(etot_kcal)[keep]
+    if len(x) < 2:
+        return None
+    mx, my = x.mean(), y.mean()
+    return 1000.0 * float(np.sum((x - mx) * (y - my)) / np.sum((x - mx) ** 2))
+
+
 # ---------------------------------------------------------------- reference arm
 def run_reference(args, n_gpus):
     """The reference's own CPU MD (compiled from its sources with its own
@@ -883,6 +1072,7 @@ def main():
             "gpu_launches": int(lc1.value - lc0.value),
             "clocks": clk, "roofline": roof, "e2e": e2e}
     if not args.no_batched:
+        line["plain_small"] = bench_plain_small(pdgpu, A, ctx, torch)
         line["lcpo"] = bench_lcpo(pdgpu, A, ctx, torch, arrays, meta, f_max, sms)
         line["batched_sp"] = bench_batched_sp(pdgpu, A, ctx, torch)
         line["batched_md"] = bench_batched_md(pdgpu, A, ctx, torch, steps=args.batched_md_steps)

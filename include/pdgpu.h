@@ -424,7 +424,13 @@ int pdgpu_minimise_run(pdgpu_ctx *ctx, int32_t sys, const pdgpu_min_params *p,
  * alone and in any mix.  A job's memory estimate before admission is
  * natoms * 2048 bytes + 1024 bytes per 32-atom cluster + 48 bytes per
  * possible 32 x 8 tile + 4 MiB; once its list is sized it is charged
- * max(estimate, real size).  The server is
+ * max(estimate, real size).  A quarter of the slots (at least two) run on
+ * the device's highest-priority streams and take single-point jobs only, so
+ * those never wait behind long jobs.  With `group` set, single-point jobs
+ * that are queued together, and minimisation jobs with the same settings,
+ * are admitted as one batch: one pack and one launch sequence for all of
+ * them, each member's results the same bits as alone.  A minimisation job's
+ * chunks of 16 steps are replayed from CUDA graphs.  The server is
  * driven from one host thread (the context's). */
 typedef struct pdgpu_server pdgpu_server;
 typedef struct {
@@ -433,7 +439,10 @@ typedef struct {
   int32_t lanes[3];     /* lanes per atom: Born, fused pair, chain (4..32)    */
   int32_t tiles;        /* 1: cluster-pair tile passes, 0: list-row passes    */
   int32_t policy;       /* admission order: 0 arrival, 1 least work first     */
-  int32_t _reserved;
+  int32_t group;        /* 1: single-point jobs queued together, and
+                           minimisation jobs with the same settings, are
+                           admitted as one batch (one pack, one launch
+                           sequence; tile layout only); 0: one job each   */
 } pdgpu_serve_params;
 void pdgpu_serve_params_default(pdgpu_serve_params *p);
 

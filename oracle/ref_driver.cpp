@@ -10,6 +10,8 @@
 //           coordinates and every reference result the parity tests pin
 //   time    rebuild a dumped system's topology, load its coordinates, and
 //           time the reference MD step loop (the CPU baseline)
+//   evals   rebuild a dumped system and time single-point evaluations
+//           (list rebuild + calcForces), the batched scoring's CPU baseline
 //   replay  rebuild a dumped system, load its coordinates and dump what
 //           the reference's protocols give with it: the single-point
 //           results, integrator steps, SD / CG minimisation, and a
@@ -787,7 +789,8 @@ static void usage() {
           "[--md STEPS] [--min STEPS] [--slowmode] [--trials K --trial-sigma DEG]\n"
           "          [--lcpo-asp KCAL_PER_A2 --lcpo UPDATESASA[,STEPS[,DENSE]]]\n"
           "ref_driver time --in DIR --cutoff R --inner R --steps K "
-          "[--warmup W] [--nlist-every M] [--param F]\n"
+          "[--warmup W] [--nlist-every M] [--param F] [--drift] [--fric 1/s]\n"
+          "ref_driver evals --in DIR --cutoff R --inner R --steps K [--warmup W] [--param F]\n"
           "ref_driver replay --in DIR --out DIR --cutoff R --inner R [--md STEPS] [--min STEPS] "
           "[--steps K] [--param F]\n");
   exit(1);
@@ -815,6 +818,8 @@ int main(int argc, char **argv) {
   double lcpo_asp = 0.0;
   int lcpo_update = 5, lcpo_steps = 0, lcpo_dense = 1;
   int nlist_every = 10;
+  bool drift = false;
+  double fric = 1e12;
   int gridx = 0;
   double spacing = 25.0;
   std::string in;
@@ -836,6 +841,8 @@ int main(int argc, char **argv) {
     else if (k == "--steps") { steps = atoi(v); a++; }
     else if (k == "--warmup") { warmup = atoi(v); a++; }
     else if (k == "--nlist-every") { nlist_every = atoi(v); a++; }
+    else if (k == "--drift") { drift = true; }
+    else if (k == "--fric") { fric = atof(v); a++; }
     else if (k == "--param") { st.param = v; a++; }
     else if (k == "--slowmode") { st.fastmode = false; }
     else if (k == "--lcpo") {
@@ -979,6 +986,39 @@ int main(int argc, char **argv) {
     return 0;
   }
 
+  if (mode == "evals") {
+    // single-point evaluations as the batched trial scoring does them:
+    // NeighbourList::calcNewList + Forcefield::calcForces, `steps` times
+    // after `warmup` (the CPU baseline of the batched evaluations)
+    std::vector<std::string> seqs;
+    {
+      std::string path = in + "/meta.txt";
+      FILE *f = fopen(path.c_str(), "r");
+      if (!f) { fprintf(stderr, "no %s\n", path.c_str()); return 2; }
+      char key[64], val[4096];
+      while (fscanf(f, "%63s %4095s", key, val) == 2)
+        if (std::string(key) == "chain") seqs.push_back(val);
+      fclose(f);
+    }
+    size_t n0;
+    std::vector<double> pos = npy_read_d(in + "/pos.npy", &n0);
+    Built b = make_ws(ffps, seqs, st);
+    if (b.ws->nAtoms() != n0) { fprintf(stderr, "atom count mismatch\n"); return 2; }
+    set_pos(*b.ws, pos);
+    b.ff->ensuresetup(*b.ws);
+    double t0 = 0, e = 0;
+    for (int s = 0; s < warmup + steps; s++) {
+      if (s == warmup) t0 = now();
+      b.ws->nlist().calcNewList();
+      b.ff->calcForces();
+      e += b.ws->ene.epot;
+    }
+    double dt = now() - t0;
+    printf("{\"evals\": %d, \"seconds\": %.6f, \"natoms\": %zu, \"epot\": %.9g}\n", steps, dt,
+           b.ws->nAtoms(), e);
+    return 0;
+  }
+
   if (mode == "time") {
     // rebuild the topology from the recorded chains, load coordinates
     std::vector<std::string> seqs;
@@ -1000,15 +1040,21 @@ int main(int argc, char **argv) {
     MolecularDynamics md(*b.ff);
     md.Integrator = MolecularDynamics::Langevin;
     md.Timestep = 1e-15;
-    md.FricCoeff = 1e12;
+    md.FricCoeff = fric;
     md.Steps = warmup + steps;
     md.UpdateNList = nlist_every;
     md.UpdateScr = 0;
     md.OutputLevel = Verbosity::Silent;
     srand(1);
     md.setInitialSpeeds(300.0);
+    // with --drift: MolecularDynamics::run_core's total-energy drift
+    // (md.cpp:206, 231-240, 182-189): etot sampled every max(1, Steps/1000)
+    // steps after step 50, least-squares slope in kcal/mol per 1000 steps
+    const int total = warmup + steps;
+    const int driftfreq = std::max(1, total / 1000);
+    std::vector<double> dx, dy;
     double t0 = 0;
-    for (int s = 0; s < warmup + steps; s++) {
+    for (int s = 0; s < total; s++) {
       if (s == warmup) t0 = now();
       md.Step = s;
       b.ws->Step = s;
@@ -1016,10 +1062,20 @@ int main(int argc, char **argv) {
       b.ff->calcForces();
       md.assertStability();
       md.applyForces();
+      if (drift && s > 50 && s % driftfreq == 0) {
+        dx.push_back(s);
+        dy.push_back((b.ws->ene.epot + b.ws->ene.ekin) * PhysicsConst::J2kcal * PhysicsConst::Na);
+      }
     }
     double dt = now() - t0;
-    printf("{\"steps\": %d, \"seconds\": %.6f, \"natoms\": %zu}\n", steps, dt,
-           b.ws->nAtoms());
+    if (drift && dx.size() > 1) {
+      double da = 0, db = 0, dR = 0;
+      Maths::leastSquaresFit(dx, dy, da, db, dR);
+      printf("{\"steps\": %d, \"seconds\": %.6f, \"natoms\": %zu, \"drift_kcal_per_1000\": %.9g}\n", steps,
+             dt, b.ws->nAtoms(), 1000.0 * db);
+    } else {
+      printf("{\"steps\": %d, \"seconds\": %.6f, \"natoms\": %zu}\n", steps, dt, b.ws->nAtoms());
+    }
     return 0;
   }
   usage();

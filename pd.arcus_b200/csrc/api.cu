@@ -1692,10 +1692,10 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
       if (use_graph) {
         // graphs are cached per system; the key holds every value baked in
         char key[288];
-        snprintf(key, sizeof key, "%d|%d|%p|%lld|%p|%d|%d|%.17g|%.17g|%.17g|%d|%d|%d|%d%d%d|%d%d|%p|%d|%d", block,
+        snprintf(key, sizeof key, "%d|%d|%p|%lld|%p|%d|%d|%.17g|%.17g|%.17g|%d|%d|%d|%d%d%d|%d%d%d|%p|%d|%d", block,
                  (int)rebuild, (void *)v.nl, v.nl_cap, (void *)e->hist, k.integrator, k.steps, k.dt, k.gamma,
                  k.temp, k.stochastic_h, P.radix_passes, (int)e->host->params.FastMode, v.lpa[0], v.lpa[1],
-                 v.lpa[2], v.tile_mode, (int)tile_search_ok(P), (void *)e->traj_dev, e->traj_every,
+                 v.lpa[2], v.tile_mode, (int)tile_search_ok(P), (int)P.coop, (void *)e->traj_dev, e->traj_every,
                  e->traj_dev_cap);
         SysEntry::GraphSlot *g = nullptr;
         for (auto &q : e->gslots)
@@ -1723,6 +1723,13 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
             e->drop_slot(ng);
             P.ene_pending[0] = pend0;
             P.ene_pending[1] = pend1;
+            if (P.coop && P.v.tile_mode) {
+              // a graph that cannot hold the cooperative evaluation: the
+              // same phases as three launches from here on
+              cudaGetLastError();
+              P.coop = false;
+              continue;
+            }
             return cuda_fail(ce, "capture md block");
           }
           ng.key = key;

@@ -118,7 +118,17 @@ struct Job {
   int regrow = 0;
   MDCoef k;
   unsigned char *min_host = nullptr;  // minimiser state read-back (inside pin)
+  // a group: single-point or minimisation jobs admitted together share one
+  // device pack (a batch, one launch sequence for all of them).  The
+  // leader owns the pack, the stream slot and the phases; `group` lists
+  // every member in pack order (the leader first), empty for a lone job.
+  std::vector<Job *> group;
+  int gpos = 0;            // position in the leader's pack
+  bool member_failed = false;
 };
+
+constexpr int kGroupMax = 64;              // jobs per group
+constexpr long long kGroupAtoms = 262144;  // atoms per group
 
 size_t res_doubles(const Job &j) {
   size_t n = (size_t)j.natoms;
@@ -142,7 +152,12 @@ struct pdgpu_server {
   // worker-owned
   std::vector<Job *> queue, active;
   std::vector<cudaStream_t> streams;
-  std::vector<int> free_slots;
+  // slots [0, n_short) run on streams of the device's highest priority and
+  // take single-point jobs only, so a short job never queues behind the
+  // long minimisation and MD jobs holding the other slots, and its kernels
+  // are scheduled ahead of theirs
+  int n_short = 0;
+  std::vector<int> free_slots, free_short;
   int64_t bytes_in_use = 0;
   PinnedPool pool;
   std::thread worker;
@@ -150,7 +165,8 @@ struct pdgpu_server {
   pdgpu_serve_stats stats;
 
   void run();
-  void admit(Job *j);
+  void admit(Job *j, const std::vector<Job *> &more);
+  std::vector<Job *> group_with(Job *j);
   void advance(Job *j);
   void retire(Job *j);
   void fail(Job *j, int status, const std::string &msg);
@@ -223,23 +239,62 @@ void pdgpu_server::start(Job *j, Phase then) {
   }
 }
 
-// Up to 16 minimiser steps without a host round trip (as pdgpu_minimise_run)
+// Up to 16 minimiser steps without a host round trip (as pdgpu_minimise_run),
+// replayed from a graph of the job's (cached by chunk length and the steps
+// of the chunk that rebuild the pairs): one launch instead of some ten per
+// step from the worker thread, whose launch rate bounds the loop.
 void pdgpu_server::enqueue_min_chunk(Job *j) {
-  Pack &P = *j->e->pack;
+  SysEntry *e = j->e.get();
+  Pack &P = *e->pack;
   const pdgpu_min_params &p = j->spec.min;
   const Consts &k = consts();
   double J2k = k.J2kcal * k.Na;
   double slope = p.SlopeCutoff > 0 ? p.SlopeCutoff * J2k : -1.0;
   int steps = j->spec.steps;
   j->chunk = std::min(16, steps - j->iter);
+  std::string key = "min" + std::to_string(j->chunk) + ":";
   for (int q = 0; q < j->chunk; q++) {
     int cnt = j->counter + j->iter + q;
-    if (p.UpdateNList > 0 && (cnt % p.UpdateNList) == 0) rebuild_pairs(P, j->st);
-    calc_forces_enqueue(j->st, j->e.get(), true, min_step_src(j->e->min_state, false));
-    launch_min_step(P.v, j->st, j->e->min_state, p.Algorithm, slope, p.Strictness, p.StepSize, steps);
+    key += (p.UpdateNList > 0 && (cnt % p.UpdateNList) == 0) ? '1' : '0';
+  }
+  auto enqueue = [&]() {
+    for (int q = 0; q < j->chunk; q++) {
+      if (key[key.size() - j->chunk + q] == '1') rebuild_pairs(P, j->st);
+      calc_forces_enqueue(j->st, e, true, min_step_src(e->min_state, false));
+      launch_min_step(P.v, j->st, e->min_state, p.Algorithm, slope, p.Strictness, p.StepSize, steps);
+    }
+  };
+  SysEntry::GraphSlot *g = nullptr;
+  for (auto &x : e->gslots)
+    if (x.key == key) g = &x;
+  if (!g && (int)e->gslots.size() < SysEntry::kGraphSlots) {
+    SysEntry::GraphSlot ng;
+    begin_capture_count();
+    cudaError_t ce = cudaStreamBeginCapture(j->st, cudaStreamCaptureModeThreadLocal);
+    if (ce == cudaSuccess) {
+      enqueue();
+      ce = cudaStreamEndCapture(j->st, &ng.graph);
+    }
+    ng.nodes = end_capture_count();
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&ng.exec, ng.graph, 0);
+    if (ce != cudaSuccess) {
+      e->drop_slot(ng);
+      fail(j, PDGPU_ERR_CUDA, std::string("minimiser graph: ") + cudaGetErrorString(ce));
+      return;
+    }
+    ng.key = key;
+    e->gslots.push_back(ng);
+    g = &e->gslots.back();
+  }
+  if (g) {
+    cudaGraphLaunch(g->exec, j->st);
+    launch_counter() += g->nodes;
+  } else {
+    enqueue();
   }
   cudaMemcpyAsync(j->pin->flags, P.v.flags, sizeof(int) * F_COUNT, cudaMemcpyDeviceToHost, j->st);
-  cudaMemcpyAsync(j->min_host, j->e->min_state, min_state_size(), cudaMemcpyDeviceToHost, j->st);
+  cudaMemcpyAsync(j->min_host, j->e->min_state, min_state_size() * std::max<size_t>(1, j->group.size()),
+                  cudaMemcpyDeviceToHost, j->st);
   record(j, PH_MIN);
 }
 
@@ -296,46 +351,102 @@ void pdgpu_server::enqueue_md_block(Job *j) {
 void pdgpu_server::enqueue_results(Job *j) {
   Pack &P = *j->e->pack;
   PackView &v = P.v;
-  size_t n = (size_t)j->natoms;
-  double *r = j->res;
-  cudaMemcpyAsync(r, v.x, sizeof(double) * n, cudaMemcpyDeviceToHost, j->st);
-  cudaMemcpyAsync(r + n, v.y, sizeof(double) * n, cudaMemcpyDeviceToHost, j->st);
-  cudaMemcpyAsync(r + 2 * n, v.z, sizeof(double) * n, cudaMemcpyDeviceToHost, j->st);
-  cudaMemcpyAsync(r + 3 * n, v.fx, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
-  cudaMemcpyAsync(r + 4 * n, v.fy, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
-  cudaMemcpyAsync(r + 5 * n, v.fz, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
-  cudaMemcpyAsync(r + 6 * n, v.gx, sizeof(double) * n, cudaMemcpyDeviceToHost, j->st);
-  cudaMemcpyAsync(r + 7 * n, v.gy, sizeof(double) * n, cudaMemcpyDeviceToHost, j->st);
-  cudaMemcpyAsync(r + 8 * n, v.gz, sizeof(double) * n, cudaMemcpyDeviceToHost, j->st);
-  cudaMemcpyAsync(r + 9 * n, v.hx, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
-  cudaMemcpyAsync(r + 10 * n, v.hy, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
-  cudaMemcpyAsync(r + 11 * n, v.hz, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
-  cudaMemcpyAsync(r + 12 * n, v.ene, sizeof(double) * E_COUNT, cudaMemcpyDeviceToHost, j->st);
-  if (j->spec.kind == PDGPU_JOB_MD && j->md_done > 0)
-    cudaMemcpyAsync(r + 12 * n + E_COUNT, j->e->hist, sizeof(double) * 3 * (size_t)j->md_done,
-                    cudaMemcpyDeviceToHost, j->st);
-  j->have_results = true;
+  const std::vector<Job *> lone(1, j);
+  const std::vector<Job *> &members = j->group.empty() ? lone : j->group;
+  for (size_t s = 0; s < members.size(); s++) {
+    Job *m = members[s];
+    const size_t n = (size_t)m->natoms, o = (size_t)P.atom_off[s];
+    double *r = m->res;
+    cudaMemcpyAsync(r, v.x + o, sizeof(double) * n, cudaMemcpyDeviceToHost, j->st);
+    cudaMemcpyAsync(r + n, v.y + o, sizeof(double) * n, cudaMemcpyDeviceToHost, j->st);
+    cudaMemcpyAsync(r + 2 * n, v.z + o, sizeof(double) * n, cudaMemcpyDeviceToHost, j->st);
+    cudaMemcpyAsync(r + 3 * n, v.fx + o, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
+    cudaMemcpyAsync(r + 4 * n, v.fy + o, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
+    cudaMemcpyAsync(r + 5 * n, v.fz + o, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
+    cudaMemcpyAsync(r + 6 * n, v.gx + o, sizeof(double) * n, cudaMemcpyDeviceToHost, j->st);
+    cudaMemcpyAsync(r + 7 * n, v.gy + o, sizeof(double) * n, cudaMemcpyDeviceToHost, j->st);
+    cudaMemcpyAsync(r + 8 * n, v.gz + o, sizeof(double) * n, cudaMemcpyDeviceToHost, j->st);
+    cudaMemcpyAsync(r + 9 * n, v.hx + o, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
+    cudaMemcpyAsync(r + 10 * n, v.hy + o, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
+    cudaMemcpyAsync(r + 11 * n, v.hz + o, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
+    cudaMemcpyAsync(r + 12 * n, v.ene + s * E_COUNT, sizeof(double) * E_COUNT, cudaMemcpyDeviceToHost, j->st);
+    if (m->spec.kind == PDGPU_JOB_MD && j->md_done > 0)
+      cudaMemcpyAsync(r + 12 * n + E_COUNT, j->e->hist, sizeof(double) * 3 * (size_t)j->md_done,
+                      cudaMemcpyDeviceToHost, j->st);
+    m->have_results = true;
+  }
   record(j, PH_FINISH);
 }
 
-void pdgpu_server::admit(Job *j) {
-  j->slot = free_slots.back();
-  free_slots.pop_back();
+// Queued jobs that can share a pack with j: the same kind (single point,
+// or minimisation with the same settings and step count), the same
+// surface-term cadence, on the tile layout within the tile search's size
+// limit, fitting the budget; at most kGroupMax jobs and kGroupAtoms atoms.
+// A member's results do not depend on the others (the tile passes and the
+// minimiser are per system), so grouping changes no result.
+std::vector<Job *> pdgpu_server::group_with(Job *j) {
+  std::vector<Job *> more;
+  const int kind = j->spec.kind;
+  if (!prm.tiles || (kind != PDGPU_JOB_ENERGY && kind != PDGPU_JOB_MINIMISE) || j->natoms > kTileSearchMaxAtoms)
+    return more;
+  long long atoms = j->natoms;
+  int64_t bytes = bytes_in_use + j->est_bytes;
+  for (Job *c : queue) {
+    if ((int)more.size() + 1 >= kGroupMax) break;
+    if (c == j || c->spec.kind != kind || c->natoms > kTileSearchMaxAtoms) continue;
+    if (c->host->lcpo_update != j->host->lcpo_update) continue;
+    if (kind == PDGPU_JOB_MINIMISE &&
+        (c->spec.steps != j->spec.steps || std::memcmp(&c->spec.min, &j->spec.min, sizeof j->spec.min) != 0))
+      continue;
+    if (atoms + c->natoms > kGroupAtoms || bytes + c->est_bytes > prm.hbm_budget) continue;
+    atoms += c->natoms;
+    bytes += c->est_bytes;
+    more.push_back(c);
+  }
+  return more;
+}
+
+void pdgpu_server::admit(Job *j, const std::vector<Job *> &more) {
+  if (!more.empty()) {
+    j->group.push_back(j);
+    for (Job *m : more) j->group.push_back(m);
+  }
+  const std::vector<Job *> lone(1, j);
+  const std::vector<Job *> &members = j->group.empty() ? lone : j->group;
+  const int S = (int)members.size();
+  if (j->spec.kind == PDGPU_JOB_ENERGY && !free_short.empty()) {
+    j->slot = free_short.back();
+    free_short.pop_back();
+  } else {
+    j->slot = free_slots.back();
+    free_slots.pop_back();
+  }
   j->st = streams[j->slot];
-  j->t_admit = Clock::now();
+  const auto now = Clock::now();
   {
     std::lock_guard<std::mutex> lk(m);
-    j->state = PDGPU_JOB_RUNNING;
-    stats.active++;
-    stats.queued--;
+    for (Job *x : members) {
+      x->t_admit = now;
+      x->state = PDGPU_JOB_RUNNING;
+      stats.active++;
+      stats.queued--;
+    }
     stats.peak_active = std::max(stats.peak_active, stats.active);
   }
-  j->charged = j->est_bytes;
-  bytes_in_use += j->charged;
-  // page-locked scratch and results
-  j->pin = (PinHead *)pool.get(sizeof(PinHead) + min_state_size(), &j->pin_cap);
-  j->res = (double *)pool.get(sizeof(double) * res_doubles(*j), &j->res_cap);
-  if (!j->pin || !j->res) {
+  for (int q = 0; q < S; q++) {
+    Job *x = members[q];
+    x->gpos = q;
+    x->charged = x->est_bytes;
+    bytes_in_use += x->charged;
+    x->res = (double *)pool.get(sizeof(double) * res_doubles(*x), &x->res_cap);
+    if (!x->res) {
+      fail(j, PDGPU_ERR_NOMEM, "page-locked host allocation failed");
+      return;
+    }
+  }
+  // page-locked scratch (the leader's): flags and every member's minimiser state
+  j->pin = (PinHead *)pool.get(sizeof(PinHead) + min_state_size() * S, &j->pin_cap);
+  if (!j->pin) {
     fail(j, PDGPU_ERR_NOMEM, "page-locked host allocation failed");
     return;
   }
@@ -348,7 +459,7 @@ void pdgpu_server::admit(Job *j) {
   j->e = std::make_unique<SysEntry>();
   SysEntry *e = j->e.get();
   e->host = j->host;
-  e->members.push_back(j->host);
+  for (Job *x : members) e->members.push_back(x->host);
   e->st = j->st;
   int r = entry_materialize(device, e, false);
   if (r) {
@@ -364,22 +475,26 @@ void pdgpu_server::admit(Job *j) {
     fail(j, r, last_error_cstr());
     return;
   }
-  size_t n = (size_t)j->natoms;
-  std::memcpy(j->res, j->x0.data(), sizeof(double) * 3 * n);
-  cudaMemcpyAsync(P.v.x, j->res, sizeof(double) * n, cudaMemcpyHostToDevice, j->st);
-  cudaMemcpyAsync(P.v.y, j->res + n, sizeof(double) * n, cudaMemcpyHostToDevice, j->st);
-  cudaMemcpyAsync(P.v.z, j->res + 2 * n, sizeof(double) * n, cudaMemcpyHostToDevice, j->st);
+  for (int q = 0; q < S; q++) {  // every member's start positions into its slice of the pack
+    Job *x = members[q];
+    const size_t n = (size_t)x->natoms, o = (size_t)P.atom_off[q];
+    std::memcpy(x->res, x->x0.data(), sizeof(double) * 3 * n);
+    cudaMemcpyAsync(P.v.x + o, x->res, sizeof(double) * n, cudaMemcpyHostToDevice, j->st);
+    cudaMemcpyAsync(P.v.y + o, x->res + n, sizeof(double) * n, cudaMemcpyHostToDevice, j->st);
+    cudaMemcpyAsync(P.v.z + o, x->res + 2 * n, sizeof(double) * n, cudaMemcpyHostToDevice, j->st);
+  }
+  const size_t n = (size_t)P.v.n_atoms;
   launch_pack_positions(P.v, j->st);
   cudaMemsetAsync(P.v.flags, 0, sizeof(int) * F_COUNT, j->st);
   if (j->spec.kind == PDGPU_JOB_MINIMISE) {
     unsigned char *ms = nullptr;
-    if (xalloc(e, &ms, min_state_size()) != cudaSuccess) {
+    if (xalloc(e, &ms, min_state_size() * S) != cudaSuccess) {
       fail(j, PDGPU_ERR_NOMEM, "device allocation failed (minimiser state)");
       return;
     }
     e->min_state = ms;
-    min_state_init(j->min_host, 1);
-    cudaMemcpyAsync(ms, j->min_host, min_state_size(), cudaMemcpyHostToDevice, j->st);
+    min_state_init(j->min_host, S);
+    cudaMemcpyAsync(ms, j->min_host, min_state_size() * S, cudaMemcpyHostToDevice, j->st);
     // WorkSpace::old = cur (minimise.cpp:114)
     cudaMemcpyAsync(P.v.ox, P.v.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, j->st);
     cudaMemcpyAsync(P.v.oy, P.v.y, sizeof(double) * n, cudaMemcpyDeviceToDevice, j->st);
@@ -428,13 +543,28 @@ void pdgpu_server::advance(Job *j) {
       return;
     }
     case PH_MIN: {
-      int taken, nan;
-      double mult;
-      min_state_read(j->min_host, 0, &taken, &nan, &mult);
-      int advanced = taken - j->taken;
-      j->taken = taken;
-      if (nan) {
-        j->steps_done = -1;
+      // every member's state; the group goes on while one still advances
+      // (a member that converged or met a NaN sits the rest out, as in
+      // pdgpu_minimise_run on a batch)
+      const std::vector<Job *> lone(1, j);
+      const std::vector<Job *> &members = j->group.empty() ? lone : j->group;
+      int advanced = 0, alive = 0;
+      for (size_t q = 0; q < members.size(); q++) {
+        Job *x = members[q];
+        int taken, nan;
+        double mult;
+        min_state_read(j->min_host, (int)q, &taken, &nan, &mult);
+        advanced = std::max(advanced, taken - x->taken);
+        x->taken = taken;
+        if (nan && !x->member_failed) {
+          x->steps_done = -1;
+          x->member_failed = true;
+          x->status = PDGPU_ERR_UNSTABLE;
+          x->error = "Simulation unstable (NaN energy during minimisation)";
+        }
+        if (!x->member_failed) alive++;
+      }
+      if (!alive) {
         fail(j, PDGPU_ERR_UNSTABLE, "Simulation unstable (NaN energy during minimisation)");
         return;
       }
@@ -454,7 +584,8 @@ void pdgpu_server::advance(Job *j) {
         return;
       }
       if (finished || j->iter >= j->spec.steps) {
-        j->steps_done = j->taken;
+        for (Job *x : members)
+          if (!x->member_failed) x->steps_done = x->taken;
         // cur = old; recompute the energies (minimise.cpp:172-176)
         launch_min_finish(P.v, j->st);
         calc_forces_enqueue(j->st, e, true, min_step_src(e->min_state, true));
@@ -494,7 +625,10 @@ void pdgpu_server::advance(Job *j) {
       return;
     }
     case PH_FINISH:
-      if (j->spec.kind == PDGPU_JOB_ENERGY) j->steps_done = 1;
+      if (j->spec.kind == PDGPU_JOB_ENERGY) {
+        j->steps_done = 1;
+        for (Job *x : j->group) x->steps_done = 1;
+      }
       j->phase = PH_DONE;
       return;
     default:
@@ -511,19 +645,31 @@ void pdgpu_server::retire(Job *j) {
     cudaEventDestroy(j->ev);
     j->ev = nullptr;
   }
-  if (j->slot >= 0) free_slots.push_back(j->slot);
+  if (j->slot >= 0) (j->slot < n_short ? free_short : free_slots).push_back(j->slot);
   j->slot = -1;
-  bytes_in_use -= j->charged;
-  j->charged = 0;
+  const std::vector<Job *> lone(1, j);
+  const std::vector<Job *> members = j->group.empty() ? lone : j->group;
+  for (Job *x : members) {
+    bytes_in_use -= x->charged;
+    x->charged = 0;
+  }
   std::lock_guard<std::mutex> lk(m);
-  j->t_done = Clock::now();
-  bool ok = j->phase == PH_DONE;
-  j->state = ok ? PDGPU_JOB_DONE : PDGPU_JOB_FAILED;
-  stats.active--;
-  if (ok)
-    stats.completed++;
-  else
-    stats.failed++;
+  const auto now = Clock::now();
+  for (Job *x : members) {
+    x->t_done = now;
+    bool ok = j->phase == PH_DONE && !x->member_failed;
+    if (x != j && !ok && !x->member_failed) {  // the group failed as a whole
+      x->status = j->status;
+      x->error = j->error;
+    }
+    if (x != j) x->phase = ok ? PH_DONE : PH_FAILED;
+    x->state = ok ? PDGPU_JOB_DONE : PDGPU_JOB_FAILED;
+    stats.active--;
+    if (ok)
+      stats.completed++;
+    else
+      stats.failed++;
+  }
   stats.bytes_in_use = bytes_in_use;
   cv_done.notify_all();
 }
@@ -579,13 +725,14 @@ void pdgpu_server::run() {
     // than kAgeMs first (in arrival order) and then the least work (atoms x
     // steps) first (policy 1); a job is admitted when a slot is free and its
     // estimate fits the budget.
-    while (!free_slots.empty()) {
+    while (!free_slots.empty() || !free_short.empty()) {
       const auto now = Clock::now();
       int pick = -1;
       double best = 0;
       for (size_t q = 0; q < queue.size(); q++) {
         Job *c = queue[q];
         if (bytes_in_use + c->est_bytes > prm.hbm_budget) continue;
+        if (free_slots.empty() && c->spec.kind != PDGPU_JOB_ENERGY) continue;  // only short slots left
         double waited = ms_between(c->t_submit, now);
         double key = (prm.policy == 0 || waited > kAgeMs)
                          ? -1e30 + (double)q
@@ -597,8 +744,10 @@ void pdgpu_server::run() {
       }
       if (pick < 0) break;
       Job *j = queue[pick];
+      std::vector<Job *> more = prm.group ? group_with(j) : std::vector<Job *>();
       queue.erase(queue.begin() + pick);
-      admit(j);
+      for (Job *x : more) queue.erase(std::find(queue.begin(), queue.end(), x));
+      admit(j, more);
       progressed = true;
       if (j->phase == PH_FAILED)
         retire(j);
@@ -629,6 +778,7 @@ void pdgpu_serve_params_default(pdgpu_serve_params *p) {
   p->lanes[0] = p->lanes[1] = p->lanes[2] = 8;
   p->tiles = 1;   // tile passes; rebuilds by tile search, no list (systems within the search limit)
   p->policy = 1;  // least work first: short jobs do not queue behind long MD runs
+  p->group = 1;   // queued single-point / like minimisation jobs share a pack
 }
 
 int pdgpu_serve_create(pdgpu_ctx *ctx, const pdgpu_serve_params *p, pdgpu_server **out) {
@@ -654,17 +804,21 @@ int pdgpu_serve_create(pdgpu_ctx *ctx, const pdgpu_serve_params *p, pdgpu_server
   s->prm = prm;
   std::memset(&s->stats, 0, sizeof s->stats);
   cudaSetDevice(s->device);
+  int least = 0, greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  s->n_short = prm.max_active >= 4 ? std::max(2, prm.max_active / 4) : 0;
   for (int q = 0; q < prm.max_active; q++) {
     cudaStream_t st;
-    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    const bool short_slot = q < s->n_short;
+    cudaError_t e = cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, short_slot ? greatest : least);
     if (e != cudaSuccess) {
       for (cudaStream_t x : s->streams) cudaStreamDestroy(x);
       delete s;
       return cuda_fail(e, "pdgpu_serve_create: stream");
     }
     s->streams.push_back(st);
-    s->free_slots.push_back(prm.max_active - 1 - q);
   }
+  for (int q = prm.max_active - 1; q >= 0; q--) (q < s->n_short ? s->free_short : s->free_slots).push_back(q);
   s->worker = std::thread([s] { s->run(); });
   *out = s;
   return PDGPU_OK;
