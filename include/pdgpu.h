@@ -289,11 +289,17 @@ int pdgpu_nlist_build_noalloc(const double *x, const double *y, const double *z,
                               int64_t *row_start, uint32_t *entries, int64_t capacity,
                               int64_t *count, void *stream);
 
-/* FF_GeneralizedBorn_Still::calcForces (gbff.cpp:168-180) in FastMode:
- * Born radii (:415-466), then the fused GB + LJ + Coulomb pass (:1529-1736)
- * and the Born-radius chain-rule pass (:1751-1818).  Adds forces; sets the
- * vdw/elec/pol energy slots and adds to EPOT.  FastMode=0 runs
- * FF_NonBonded::calcForces + the same GB terms as calcBornForces. */
+/* FF_GeneralizedBorn_Still::calcForces (gbff.cpp:168-180).  FastMode (the
+ * default): Born radii (:415-466), then the fused GB + LJ + Coulomb pass
+ * (:1529-1736) and the Born-radius chain-rule pass (:1751-1818); adds
+ * forces, sets the vdw/elec energy slots, adds the pol/pol_cross/pol_self
+ * slots and their sum to EPOT.  FastMode=0: FF_NonBonded::calcForces
+ * (nonbonded.cpp:1205-1229, at Dielectric = DielectricSolute, the
+ * component's own switching) + calcBornForces (gbff.cpp:1172-1400: the GB
+ * term without the vacuum terms, keeping its t = 0 limit q_i q_j / r
+ * beyond the exp-approximation range); the LJ/Coulomb slots and the virial
+ * as FF_NonBonded sets them, the GB energy added to EPOT alone (its totals
+ * in the PDGPU_ENE_GB_COMPONENT slots), as the reference does. */
 int pdgpu_gb_forces(pdgpu_ctx *ctx, int32_t sys);
 /* FF_GeneralizedBorn_Still::calcEnergies (gbff.cpp:161-166): radii, the
  * stand-alone LJ/Coulomb pass at the solute dielectric (which, as in the

@@ -776,6 +776,81 @@ static void dump_lcpo(Built &b, const std::vector<double> &allpos, double asp, i
   set_pos(ws, allpos);
 }
 
+// FF_NonBonded alone in each of its calcForces modes (nonbonded.cpp:
+// 1205-1229 selects ForceSwitch over EnergySwitch over plain Coulomb; the
+// DDDielectric flag is not consulted there), at the GB component's cutoffs,
+// and the GB component with FastMode off (calcForces = FF_NonBonded::
+// calcForces + calcBornForces, gbff.cpp:168-180, 1172-1400).
+static void dump_nb_case(Built &b, const std::string &pre, bool fs, bool es, bool ddd, double diel,
+                         bool vdwcor) {
+  WorkSpace &ws = *b.ws;
+  FF_NonBonded *nb = new FF_NonBonded(ws);
+  nb->Cutoff = b.gb->Cutoff;
+  nb->InnerCutoff = b.gb->InnerCutoff;
+  nb->VdwCutoff = b.gb->VdwCutoff;
+  nb->VdwInnerCutoff = b.gb->VdwInnerCutoff;
+  nb->ForceSwitch = fs;
+  nb->EnergySwitch = es;
+  nb->DDDielectric = ddd;
+  nb->Dielectric = diel;
+  if (vdwcor) {
+    nb->VdwCor = true;
+    nb->VdwCorDensity = 0.0334;  // particles / A^3
+    nb->VdwCorEpsilon = 0.152;   // kcal/mol
+    nb->VdwCorRadius = 1.77;     // A
+    nb->VdwCorCutoff = nb->VdwCutoff;
+  }
+  Forcefield ff(ws);
+  ff.add(*nb);
+  ff.ensuresetup(ws);
+  ws.nlist().calcNewList();
+  ff.calcForces();
+  put_d(pre + "f", get_f(ws), shp(ws.nAtoms(), 3));
+  put_d(pre + "ene", ene_vec(ws.ene));
+  std::vector<double> cfg;
+  cfg.push_back(nb->Cutoff);
+  cfg.push_back(nb->InnerCutoff);
+  cfg.push_back(fs);
+  cfg.push_back(es);
+  cfg.push_back(ddd);
+  cfg.push_back(diel);
+  cfg.push_back(vdwcor);
+  cfg.push_back(nb->VdwCorDensity);
+  cfg.push_back(nb->VdwCorEpsilon);
+  cfg.push_back(nb->VdwCorRadius);
+  cfg.push_back(nb->VdwCorCutoff);
+  cfg.push_back(nb->Vdw14Scaling);
+  cfg.push_back(nb->Elec14Scaling);
+  put_d(pre + "cfg", cfg);
+}
+static void dump_nbmodes(Built &b, const std::vector<double> &allpos) {
+  WorkSpace &ws = *b.ws;
+  set_pos(ws, allpos);
+  dump_nb_case(b, "nbfs_", true, false, false, 1.0, false);   // the FF_NonBonded default
+  dump_nb_case(b, "nbes_", false, true, false, 1.0, false);
+  dump_nb_case(b, "nbnorm_", false, false, false, 1.0, false);
+  dump_nb_case(b, "nbddd_", true, false, true, 1.0, false);   // DDDielectric: not consulted by calcForces
+  dump_nb_case(b, "nbdiel4_", false, false, false, 4.0, false);
+  dump_nb_case(b, "nbvdwcor_", true, false, false, 1.0, true);
+  // the GB component with FastMode off, with FF_Bonded, and alone
+  b.gb->FastMode = false;
+  b.ff->ensuresetup(ws);
+  ws.nlist().calcNewList();
+  b.ff->calcForces();
+  put_d("gbslow_f_total", get_f(ws), shp(ws.nAtoms(), 3));
+  put_d("gbslow_ene_total", ene_vec(ws.ene));
+  put_d("gbslow_born", born(b));
+  ws.zeroForces();
+  b.gb->calcForces();
+  put_d("gbslow_f_gb", get_f(ws), shp(ws.nAtoms(), 3));
+  std::vector<double> e = ene_vec(ws.ene);
+  e.push_back(b.gb->epot_pol);
+  e.push_back(b.gb->epot_pol_cross);
+  e.push_back(b.gb->epot_pol_self);
+  put_d("gbslow_ene_gb", e);
+  b.gb->FastMode = true;
+}
+
 static double now() {
   struct timeval tv;
   gettimeofday(&tv, NULL);
@@ -786,7 +861,7 @@ static void usage() {
   fprintf(stderr,
           "ref_driver build --out DIR --nres N[,N..] --seed S [--cutoff R] "
           "[--inner R] [--grid NX,SPACING] [--premin STEPS] [--param F] "
-          "[--md STEPS] [--min STEPS] [--slowmode] [--trials K --trial-sigma DEG]\n"
+          "[--md STEPS] [--min STEPS] [--slowmode] [--trials K --trial-sigma DEG] [--nbmodes]\n"
           "          [--lcpo-asp KCAL_PER_A2 --lcpo UPDATESASA[,STEPS[,DENSE]]]\n"
           "ref_driver time --in DIR --cutoff R --inner R --steps K "
           "[--warmup W] [--nlist-every M] [--param F] [--drift] [--fric 1/s]\n"
@@ -819,6 +894,7 @@ int main(int argc, char **argv) {
   int lcpo_update = 5, lcpo_steps = 0, lcpo_dense = 1;
   int nlist_every = 10;
   bool drift = false;
+  bool nbmodes = false;
   double fric = 1e12;
   int gridx = 0;
   double spacing = 25.0;
@@ -842,6 +918,7 @@ int main(int argc, char **argv) {
     else if (k == "--warmup") { warmup = atoi(v); a++; }
     else if (k == "--nlist-every") { nlist_every = atoi(v); a++; }
     else if (k == "--drift") { drift = true; }
+    else if (k == "--nbmodes") { nbmodes = true; }
     else if (k == "--fric") { fric = atof(v); a++; }
     else if (k == "--param") { st.param = v; a++; }
     else if (k == "--slowmode") { st.fastmode = false; }
@@ -925,6 +1002,7 @@ int main(int argc, char **argv) {
       dump_md_steps(b, MolecularDynamics::Beeman, mdsteps, 1e12, "mdbm_");
     }
     if (lcpo_asp != 0.0) dump_lcpo(b, allpos, lcpo_asp, lcpo_update, lcpo_steps, lcpo_dense != 0);
+    if (nbmodes) dump_nbmodes(b, allpos);
     printf("built %zu atoms\n", b.ws->nAtoms());
     return 0;
   }

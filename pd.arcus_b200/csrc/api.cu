@@ -926,8 +926,11 @@ static int nlist_enqueue(pdgpu_ctx *c, SysEntry *e, bool size_check) {
 // have made.  Packs on the row passes, or with a system too large for the
 // search, rebuild the list (and from it the tiles).
 static bool tile_search_ok(const Pack &P) {
-  return P.v.tile_mode && P.v.tile_meta && P.v.n_sc > 0 && P.v.max_sys_atoms <= kTileSearchMaxAtoms;
+  // (FastMode off needs the list rows for its stand-alone LJ/Coulomb pass)
+  return P.v.tile_mode && P.v.tile_meta && P.v.n_sc > 0 && P.v.max_sys_atoms <= kTileSearchMaxAtoms && !P.slow();
 }
+// the energy-record bits of the pair terms of an evaluation
+static int pair_energy_mode(const Pack &P) { return P.slow() ? (EM_PAIR_NB | EM_PAIR_GB_SLOW) : EM_PAIR_GB; }
 static void rebuild_enqueue(Pack &P, cudaStream_t st) {
   if (tile_search_ok(P)) {
     launch_tiles_search(P.v, st);
@@ -1167,7 +1170,10 @@ static void gb_forces_enqueue(pdgpu_ctx *c, Pack &P) {
     launch_gb_pair(P.v, c->st);
     launch_gb_chain(P.v, c->st);
   }
-  launch_energy(P.v, c->st, EM_PAIR_GB);
+  // FastMode off: FF_NonBonded::calcForces beside calcBornForces
+  // (gbff.cpp:176-177), after the GB passes (they zero what it adds to)
+  if (P.slow()) launch_nonbonded(P.v, c->st, P.sp[0].elec_mode);
+  launch_energy(P.v, c->st, pair_energy_mode(P));
 }
 
 }  // extern "C"
@@ -1180,10 +1186,7 @@ int pdgpu_gb_forces(pdgpu_ctx *c, int32_t sys) {
   Pack &P = *e->pack;
   int r = ready_pairs(c, e);
   if (r) return r;
-  if (!e->host->params.FastMode) {
-    set_error("FastMode=false (separate FF_NonBonded + calcBornForces) is not built; use FastMode");
-    return PDGPU_ERR_ARG;
-  }
+  if (P.slow() && (r = need_csr(c, e))) return r;  // the stand-alone LJ/Coulomb pass reads the rows
   gb_forces_enqueue(c, P);
   r = sync_check(c, "gb_forces");
   return r ? r : barrier_check(c, P);
@@ -1349,10 +1352,14 @@ void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce, StepS
   // writes what the record reads, waits for it
   const bool pending = P.energy_pending();
   const int zero = ZF_PAIRS | (side ? 0 : ZF_BONDED) | (pending ? 0 : ZF_RECORD);
+  const bool slow = P.slow();
   if (P.v.tile_mode) {
     // the tile layout: the three passes as one evaluation into energy
     // buffer `ebuf`; only a record still reading that buffer is waited for
+    // (FastMode off: every pending record, as its LJ/Coulomb pass writes
+    // buffer 0)
     P.wait_energy(st, ebuf);
+    if (slow) P.wait_energy(st, ebuf ^ 1);
     PackView vb = P.v;
     vb.ebuf = ebuf;
     launch_eval_tiles(vb, st, zero, P.coop);
@@ -1365,8 +1372,10 @@ void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce, StepS
     launch_gb_chain(P.v, st);
     P.last_ebuf = 0;
   }
+  // FastMode off: FF_NonBonded::calcForces beside calcBornForces
+  if (slow) launch_nonbonded(P.v, st, P.sp[0].elec_mode);
   if (side) cudaStreamWaitEvent(st, P.join, 0);
-  if (reduce) launch_energy(P.v, st, EM_PAIR_GB | (bonded ? EM_BONDED : 0) | (surf ? EM_SURF : 0));
+  if (reduce) launch_energy(P.v, st, pair_energy_mode(P) | (bonded ? EM_BONDED : 0) | (surf ? EM_SURF : 0));
 }
 extern "C" {
 
@@ -1488,7 +1497,7 @@ void pdgpu::md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k, int q
   Pack &P = *e->pack;
   StepSrc step;
   step.p = e->step_dev;  // MolecularDynamics::run_core sets WorkSpace::Step = Step (md.cpp:214)
-  const int b = P.v.tile_mode ? (q & 1) : 0;  // this step's energy buffer
+  const int b = (P.v.tile_mode && !P.slow()) ? (q & 1) : 0;  // this step's energy buffer
   calc_forces_enqueue(st, e, false, step, b);
   // the integrator writes the kinetic energies the previous step's record
   // reads: that record must be done
@@ -1503,8 +1512,8 @@ void pdgpu::md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k, int q
   PackView vb = P.v;
   vb.ebuf = b;
   launch_energy(vb, P.side,
-                EM_PAIR_GB | (has_bonded(P) ? EM_BONDED : 0) | (P.v.lc.update > 0 ? EM_SURF : 0) | EM_KINETIC |
-                    EM_RECORD | EM_ASSIGN,
+                pair_energy_mode(P) | (has_bonded(P) ? EM_BONDED : 0) | (P.v.lc.update > 0 ? EM_SURF : 0) |
+                    EM_KINETIC | EM_RECORD | EM_ASSIGN,
                 e->hist, e->step_dev);
   cudaEventRecord(P.ene_done[b], P.side);
   P.ene_pending[b] = true;

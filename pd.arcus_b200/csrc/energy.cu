@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode,
         acc[P_VDW] += ep[(size_t)AE_VDW * N + i];
         acc[P_ELEC] += ep[(size_t)AE_ELEC * N + i];
       }
-      if (mode & (EM_PAIR_GB | EM_BORN_ENERGY)) {
+      if (mode & (EM_PAIR_GB | EM_BORN_ENERGY | EM_PAIR_GB_SLOW)) {
         acc[P_POL] += ep[(size_t)AE_POL * N + i];
         acc[P_SELF] += ep[(size_t)AE_POL_SELF * N + i];
       }
@@ -140,6 +140,14 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy(PackView v, int mode,
       R[E_EPOT] += tot[P_POL] + tot[P_SELF];
     }
     if (mode & EM_PAIR_NB) R[E_VIRIAL] += tot[P_NBVIR];
+    if (mode & EM_PAIR_GB_SLOW) {
+      // calcBornForces adds its energy to epot alone (gbff.cpp:1340); the
+      // component's own totals go to the extra slots
+      R[E_EPOT] += tot[P_POL] + tot[P_SELF];
+      R[E_GB_COMPONENT] = tot[P_POL] + tot[P_SELF];
+      R[E_GB_COMPONENT + 1] = tot[P_POL];
+      R[E_GB_COMPONENT + 2] = tot[P_SELF];
+    }
     if (mode & EM_BORN_ENERGY) {
       // the energy-only path adds the Born energy to epot alone
       // (gbff.cpp:574-578); the component's own totals go to extra slots

@@ -263,7 +263,14 @@ __device__ __forceinline__ PairOut pair_gb(const GbSettings &g, float r2, bool i
     epol = epol0 * S;
     dedr = S * dedr0 + dSdd * epol0;
     dedal = dedal0 * S;
+  } else if (g.slow && in) {
+    // FastMode off (calcBornForces, gbff.cpp:1292-1324): the GB term's
+    // t = 0 limit q_i q_j / r beyond the exp-approximation range
+    const float epol0 = g.premul * qiqj * invr;
+    epol = epol0 * S;
+    dedr = S * (-epol0 * invr) + dSdd * epol0;
   }
+  nb = nb && !g.slow;  // FastMode off: the vacuum terms come from FF_NonBonded::calcForces
   const float ec = (gb ? g.econv_in : g.econv_out) * (b14 ? g.elec14 : 1.f) * qiqj * invr;
   const float elf = S * (-ec * invr) + ec * dSdd;
   // Lennard-Jones 12-6 with its own switch

@@ -91,7 +91,9 @@ enum EnergyMode {
   EM_KINETIC = 16,     // ekin, etot
   EM_RECORD = 32,      // history row + step counter advance (step loops)
   EM_ASSIGN = 64,      // form the record from zero (its slots were not zeroed before the step)
-  EM_SURF = 128        // LCPO surface term: epot_surf
+  EM_SURF = 128,       // LCPO surface term: epot_surf
+  EM_PAIR_GB_SLOW = 256  // GB with FastMode off (calcBornForces): pol + self added to epot alone;
+                         // the LJ/Coulomb slots come from EM_PAIR_NB
 };
 
 // FF_SASA_LCPO (forcefields/lcpo.h, lcpo.cpp): per-atom parameters and the
@@ -311,6 +313,13 @@ struct Pack {
   bool ene_pending[2] = {false, false};
   int last_ebuf = 0;             // buffer of the last evaluation's per-atom energies
   bool energy_pending() const { return ene_pending[0] || ene_pending[1]; }
+  // a member has FastMode off: the vacuum LJ/Coulomb come from the
+  // stand-alone pass over the neighbour-list rows
+  bool slow() const {
+    for (const SysParams &q : sp)
+      if (!q.fast_mode) return true;
+    return false;
+  }
   void wait_energy(cudaStream_t s, int b) {
     if (ene_pending[b]) {
       cudaStreamWaitEvent(s, ene_done[b], 0);

@@ -75,7 +75,12 @@ __device__ __forceinline__ bool gb_branch_exact(const double *__restrict__ x, co
 struct GbSettings {
   float thr, band, rc2, rin, inv_sw2, elec14, vdw14, econv_in, econv_out, premul, vdw_rc, vdw_rin, vdw_inv_sw2;
   double thr_d;
+  // FastMode off (calcBornForces, gbff.cpp:1172-1330): no vacuum LJ/Coulomb
+  // in this pass (FF_NonBonded::calcForces gives them), and beyond the
+  // exp-approximation range the GB term keeps its t = 0 limit q_i q_j / r
+  bool slow;
   __device__ __forceinline__ void load(const SysParams &P) {
+    slow = P.fast_mode == 0;
     thr = P.exp_thresh;
     thr_d = P.exp_thresh_d;
     band = 4e-6f * fabsf(thr);
@@ -134,7 +139,12 @@ __device__ __forceinline__ GbPair gb_pair_term(const GbSettings &g, const Dx &d,
     o.epol = epol0 * S;
     dedr = S * dedr0 + dSdd * epol0;
     o.dedal = dedal0 * S;
+  } else if (g.slow) {
+    const float epol0 = g.premul * qiqj * invr;
+    o.epol = epol0 * S;
+    dedr = S * (-epol0 * invr) + dSdd * epol0;
   }
+  if (g.slow) nb = false;  // the vacuum terms come from FF_NonBonded::calcForces
   // vacuum Coulomb at the solute (GB branch) or solvent dielectric
   const float ec = nb ? (gb ? g.econv_in : g.econv_out) * (b14 ? g.elec14 : 1.f) * qiqj * invr : 0.f;
   const float elf = S * (-ec * invr) + ec * dSdd;

@@ -197,7 +197,7 @@ void pdgpu_server::fail(Job *j, int status, const std::string &msg) {
 // A job on the tile layout (systems within the search limit) rebuilds by
 // tile search: no list, no size read-back.
 static bool tile_search_job(const Pack &P) {
-  return P.v.tile_mode && P.v.tile_meta && P.v.n_sc > 0 && P.v.max_sys_atoms <= kTileSearchMaxAtoms;
+  return P.v.tile_mode && P.v.tile_meta && P.v.n_sc > 0 && P.v.max_sys_atoms <= kTileSearchMaxAtoms && !P.slow();
 }
 static void rebuild_pairs(Pack &P, cudaStream_t st) {
   if (tile_search_job(P)) {

@@ -174,10 +174,12 @@ SysParams make_sys_params(const pdgpu_ff_params &p) {
   s.dielectric = (float)p.Dielectric;
   s.ddd_alpha = (float)p.DDDielectricAlpha;
   s.econv_nb = (float)(c.econv / p.Dielectric);
+  // (the DDDielectric flag is not consulted here by the reference: its
+  // calcForces and calcEnergies pick plain, energy-switched or
+  // force-switched Coulomb only)
   int em = 1;
   if (p.EnergySwitch) em = 3;
   if (p.ForceSwitch) em = 4;
-  if (p.DDDielectric) em = 2;
   if (!p.DoElec) em = 0;
   s.elec_mode = em;
   s.vdw_mode = p.DoVdw ? 2 : 0;

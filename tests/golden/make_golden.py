@@ -23,6 +23,11 @@ with 500 steepest-descent steps at Rc 12 A unless noted):
                 GlobalASP 0.005 kcal/mol/A^2, UpdateSasa 5): its per-atom parameters,
                 its forces and energies alone and with {FF_Bonded, GB}, and 12
                 velocity-Verlet and 12 steepest-descent steps of the whole forcefield
+  nb_pep24_s7   24 residues, Rc 12: FF_NonBonded alone in each calcForces mode
+                (force switch -- its default --, energy switch, plain Coulomb,
+                DDDielectric set, dielectric 4, the long-range VdW correction)
+                at the GB cutoffs, and the GB component with FastMode off
+                (FF_NonBonded::calcForces + calcBornForces)
   c2_16x80_s2   16 x 80-residue chains on a 4x4 grid 25 A apart (~20.6k atoms),
                 Rc 16: inputs plus reference forces, Born radii and energies
                 (no neighbour list: too large to store), and the LCPO term's
@@ -52,6 +57,7 @@ SYSTEMS = {
                           drop=("lcpo_mdvv_normals",)),
     "c2_16x80_s2": dict(nres=[80] * 16, seed=2, cutoff=16, premin=500, grid=(4, 25), drop_nl=True,
                         lcpo=(0.005, 5, 0, 0)),
+    "nb_pep24_s7": dict(nres=[24], seed=7, cutoff=12, premin=500, nbmodes=True),
 }
 
 # arrays kept for the large system (inputs + a few reference results)
@@ -73,6 +79,8 @@ def build(name, spec, keep_dir=None):
         cmd += ["--min", str(spec["min"])]
     if spec.get("trials"):
         cmd += ["--trials", str(spec["trials"]), "--trial-sigma", "15"]
+    if spec.get("nbmodes"):
+        cmd += ["--nbmodes"]
     if spec.get("lcpo"):
         asp, update, steps = spec["lcpo"][:3]
         dense = spec["lcpo"][3] if len(spec["lcpo"]) > 3 else 1
