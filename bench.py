@@ -557,22 +557,25 @@ def bench_serving(pdgpu, A, ctx, torch, n_requests=300, rate=200.0, budget=120e9
     # templates: sizes log-uniform in [500, 30000]
     n_tmpl = 24
     targets = np.exp(np.linspace(np.log(500), np.log(30000), n_tmpl))
-    templates = []
+    templates, tmpl_inputs = [], []
     for t in targets:
         parts, tot = [], 0
         while tot < 0.9 * t:
-            a = lib[int(rng.integers(len(lib)))][0]
+            a, am = lib[int(rng.integers(len(lib)))]
             if parts and tot + a["charge"].shape[0] > 1.15 * t:
-                cand = [x for x, _ in lib if tot + x["charge"].shape[0] <= 1.15 * t]
+                cand = [(x, xm) for x, xm in lib if tot + x["charge"].shape[0] <= 1.15 * t]
                 if not cand:
                     break
-                a = cand[int(rng.integers(len(cand)))]
-            parts.append(a)
+                a, am = cand[int(rng.integers(len(cand)))]
+            parts.append((a, am))
             tot += a["charge"].shape[0]
-        arrays = compose(parts)
+        arrays = compose([a for a, _ in parts])
         ws, ff = make_ws(pdgpu, arrays, meta, ctx)
         ws.setLanes((8, 8, 8))
         templates.append(ws)
+        # the template for the reference driver: its chains and coordinates
+        chains = [c for _, am in parts for c in (am["chain"] if isinstance(am["chain"], list) else [am["chain"]])]
+        tmpl_inputs.append(({"pos": arrays["pos"]}, dict(meta, chains=chains)))
     sizes = np.array([ws.nAtoms() for ws in templates])
     # the request stream
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
@@ -649,7 +652,8 @@ def bench_serving(pdgpu, A, ctx, torch, n_requests=300, rate=200.0, budget=120e9
     plain_makespan = time.perf_counter() - t0
     for ws in templates:
         ws.close()
-    return {"metric": "served GB jobs/s", "value": n_requests / makespan, "unit": "jobs/s",
+    cpu = serving_cpu_estimate(tmpl_inputs, sizes, kinds, tmpl, A) if os.path.exists(REF_DRIVER) else None
+    return {"metric": "served GB jobs/s", "value": n_requests / makespan, "unit": "jobs/s", "cpu_baseline": cpu,
             "requests": n_requests, "arrival_rate_per_s": rate,
             "latency_ms": {"p50": pctl(lat, 50), "p99": pctl(lat, 99)}, "by_kind": by_kind,
             "plain_sequential": {"value": n_requests / plain_makespan, "unit": "jobs/s",
@@ -662,6 +666,46 @@ def bench_serving(pdgpu, A, ctx, torch, n_requests=300, rate=200.0, budget=120e9
             "device_max_connections": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS"),
             "peak_bytes": st["peak_bytes"], "failed": st["failed"], "gpu_launches": int(lc1 - lc0),
             "timing": "wall clock: latency = finish - arrival per job; jobs/s = requests / makespan"}
+
+
+def serving_cpu_estimate(tmpl_inputs, sizes, kinds, tmpl, A):
+    """The reference's CPU time for the served job stream, from timed
+    samples: on the smallest, the median and the largest template, the
+    reference's list rebuild + calcForces (a single point, and a
+    steepest-descent step, which rebuilds the list every step) and its MD
+    step (list every 10 steps), each as its own process on the host's cores;
+    a quadratic in the atom count through the three (the reference's list is
+    O(N^2)) gives every job's time, and the stream's jobs/s assumes every
+    core busy with one job after another (an upper bound for the CPU)."""
+    cores = host_cores()
+    order = np.argsort(sizes)
+    pick = [int(order[0]), int(order[len(order) // 2]), int(order[-1])]
+    jobs = []
+    for t in pick:
+        a, m = tmpl_inputs[t]
+        k = 2 if sizes[t] > 10000 else 6
+        jobs.append((a, m, "evals", ["--steps", k, "--warmup", 1]))
+        jobs.append((a, m, "time", ["--steps", k, "--warmup", 1, "--nlist-every", 10]))
+    res, wall = run_ref_jobs(jobs, cores)
+    if any(r is None for r in res):
+        return None
+    n = np.array([float(sizes[t]) for t in pick])
+    t_eval = np.array([res[2 * q]["seconds"] / res[2 * q]["evals"] for q in range(3)])
+    t_md = np.array([res[2 * q + 1]["seconds"] / res[2 * q + 1]["steps"] for q in range(3)])
+    X = np.stack([n, n * n], axis=1)
+    ce = np.linalg.lstsq(X, t_eval, rcond=None)[0]
+    cm = np.linalg.lstsq(X, t_md, rcond=None)[0]
+    total = 0.0
+    for k, kind in enumerate(kinds):
+        N = float(sizes[tmpl[k]])
+        te, tm = max(ce[0] * N + ce[1] * N * N, 0.0), max(cm[0] * N + cm[1] * N * N, 0.0)
+        total += te if kind == A.JOB_ENERGY else (200 * te if kind == A.JOB_MINIMISE else 2000 * tm)
+    return {"value": len(kinds) / (total / cores), "unit": "jobs/s", "cores": cores, "kind": "reference",
+            "estimate": True, "sample_seconds": wall,
+            "sample": "the reference's single point (list + calcForces) and MD step timed on the smallest, "
+                      "median and largest templates (%d, %d, %d atoms); job times from a quadratic in N through "
+                      "them; %d cores each running jobs back to back" % (sizes[pick[0]], sizes[pick[1]],
+                                                                          sizes[pick[2]], cores)}
 
 
 def L_count(L, ctx):

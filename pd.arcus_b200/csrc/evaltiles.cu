@@ -302,13 +302,42 @@ __device__ __forceinline__ PairOut pair_gb(const GbSettings &g, float r2, bool i
   return o;
 }
 
+// The i side of a tile is converted to fixed point per tile (so its sums
+// depend on the tile alone) and kept in 64-bit registers while the warp's
+// range stays in one i-cluster; the sums go to memory when the range moves
+// to the next cluster.  Exact integer sums: the same bits as adding every
+// tile's share to memory at once.
+struct ISide {
+  long long f[7];
+  bool bad;
+  __device__ __forceinline__ void clear() {
+#pragma unroll
+    for (int q = 0; q < 7; q++) f[q] = 0;
+    bad = false;
+  }
+  __device__ __forceinline__ void add(int q, float x) {
+    bad |= !(fabsf(x) <= 3.0e38f);
+    f[q] += to_fixed_j(x);
+  }
+  __device__ __forceinline__ void flush(const PackView &v, int i, int s, int N) {
+    long long *dst[7] = {v.hx + i, v.hy + i, v.hz + i, v.ej + i, v.ej + (size_t)N + i, v.ej + (size_t)2 * N + i,
+                         v.ej + (size_t)3 * N + i};
+#pragma unroll
+    for (int q = 0; q < 7; q++)
+      if (f[q]) atomicAdd((unsigned long long *)dst[q], (unsigned long long)f[q]);
+    if (bad) atomicOr(&(v.ebuf ? v.sys_flags_alt : v.sys_flags)[s], SF_NONFINITE);
+  }
+};
+
 __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane, float4 (*sA)[16],
                                            float4 (*sB)[16], float4 (*sP)[16]) {
   int e, e1;
   ev_range(v.tile_count[0], warp, e, e1);
   const int N = v.n_atoms;
   const int g8 = lane & ~7, a = lane & 7;
-  int a0 = -1, i = 0, s_cur = -1;
+  int a0 = -1, i = 0, s_cur = -1, na = 0, s_i = 0;
+  ISide acc;
+  acc.clear();
   float4 ia = make_float4(0, 0, 0, 0), ib = ia, ip = ia;
   double ai_d = 0.0;
   const SysParams *P = nullptr;
@@ -335,7 +364,11 @@ __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane
       gs.load(*P);
     }
     if (ti.a0 != a0) {
+      if (lane < na) acc.flush(v, i, s_i, N);
+      acc.clear();
       a0 = ti.a0;
+      na = ti.na;
+      s_i = ti.s;
       i = a0 + (lane < ti.na ? lane : 0);
       ia = v.pq[2 * (size_t)i];
       ib = v.pq[2 * (size_t)i + 1];
@@ -394,17 +427,16 @@ __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane
 #pragma unroll
       for (int q = 0; q < 4; q++) add_fixed(v, &v.ej[(size_t)q * N + j], jacc[3 + q], ti.s);
     }
-    if (lane < ti.na) {
-      add_fixed(v, &v.hx[i], fx, ti.s);
-      add_fixed(v, &v.hy[i], fy, ti.s);
-      add_fixed(v, &v.hz[i], fz, ti.s);
-      add_fixed(v, &v.ej[i], e_vdw, ti.s);
-      add_fixed(v, &v.ej[(size_t)N + i], e_el, ti.s);
-      add_fixed(v, &v.ej[(size_t)2 * N + i], e_pol, ti.s);
-      add_fixed(v, &v.ej[(size_t)3 * N + i], deda, ti.s);
-    }
+    acc.add(0, fx);
+    acc.add(1, fy);
+    acc.add(2, fz);
+    acc.add(3, e_vdw);
+    acc.add(4, e_el);
+    acc.add(5, e_pol);
+    acc.add(6, deda);
     __syncwarp();
   }
+  if (lane < na) acc.flush(v, i, s_i, N);
 }
 
 // ============================================================= phase C
@@ -584,10 +616,11 @@ __device__ __forceinline__ void epilogue_energies(const PackView &v) {
 
 // ============================================================= the kernel
 // PH: which phases (1 A, 2 B, 4 C); more than one needs a cooperative
-// launch.  tile_count[2] is the still-list length, tile_count[3] the
+// launch.  MINB: resident blocks per SM the register allocation must allow
+// (PDGPU_EV_BLOCKS, 4 or 5, picks the build at run time).  tile_count[2] is the still-list length, tile_count[3] the
 // barrier / exit counter; the last block out clears both.
-template <int PH>
-__global__ void __launch_bounds__(32 * kEvWarps, PDGPU_EV_BLOCKS) k_eval_tiles(PackView v, int zero) {
+template <int PH, int MINB>
+__global__ void __launch_bounds__(32 * kEvWarps, MINB) k_eval_tiles(PackView v, int zero) {
   PDGPU_DEP_ENTRY();
   if (v.flags[F_NL_OVERFLOW]) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -635,13 +668,25 @@ static int fused_wanted() {
   return w;
 }
 
+static int ev_minb() {
+  static int m = 0;
+  if (!m) {
+    const char *s = getenv("PDGPU_EV_BLOCKS");
+    m = (s && s[0] == '4') ? 4 : PDGPU_EV_BLOCKS;
+  }
+  return m;
+}
+
 // Resident blocks of the evaluation kernel on this device (the grid of its
 // cooperative launch), and no more warps than a pack can have tiles.
 int eval_tiles_grid(long long tile_cap) {
   int dev = 0, sms = 148, occ = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_eval_tiles<7>, 32 * kEvWarps, 0);
+  if (ev_minb() == 4)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_eval_tiles<7, 4>, 32 * kEvWarps, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_eval_tiles<7, PDGPU_EV_BLOCKS>, 32 * kEvWarps, 0);
   const long long need = (tile_cap + kEvWarps - 1) / kEvWarps;
   return (int)std::max(1LL, std::min((long long)std::max(occ, 1) * sms, need));
 }
@@ -669,7 +714,8 @@ static cudaError_t launch_ev(const PackView &v, cudaStream_t st, int zero, bool 
   }
   cfg.attrs = attr;
   cfg.numAttrs = na;
-  cudaError_t e = cudaLaunchKernelEx(&cfg, k_eval_tiles<PH>, v, zero);
+  cudaError_t e = ev_minb() == 4 ? cudaLaunchKernelEx(&cfg, k_eval_tiles<PH, 4>, v, zero)
+                                 : cudaLaunchKernelEx(&cfg, k_eval_tiles<PH, PDGPU_EV_BLOCKS>, v, zero);
   count_launch();
   return e;
 }
