@@ -54,8 +54,13 @@
 #undef private
 #undef protected
 #ifdef PDGPU_COMPONENT
-// the B200 GB component (pd.arcus_b200/plugin) in place of the reference's
+// the B200 GB and LCPO components (pd.arcus_b200/plugin) in place of the
+// reference's
 #include "gbff_gpu.h"
+#include "lcpo_gpu.h"
+typedef Physics::FF_SASA_LCPO_GPU LcpoComponent;
+#else
+typedef Physics::FF_SASA_LCPO LcpoComponent;
 #endif
 
 #include <sys/stat.h>
@@ -861,7 +866,7 @@ static void usage() {
   fprintf(stderr,
           "ref_driver build --out DIR --nres N[,N..] --seed S [--cutoff R] "
           "[--inner R] [--grid NX,SPACING] [--premin STEPS] [--param F] "
-          "[--md STEPS] [--min STEPS] [--slowmode] [--trials K --trial-sigma DEG] [--nbmodes]\n"
+          "[--md STEPS] [--min STEPS] [--slowmode] [--trials K --trial-sigma DEG] [--nbmodes] [--topo-only]\n"
           "          [--lcpo-asp KCAL_PER_A2 --lcpo UPDATESASA[,STEPS[,DENSE]]]\n"
           "ref_driver time --in DIR --cutoff R --inner R --steps K "
           "[--warmup W] [--nlist-every M] [--param F] [--drift] [--fric 1/s]\n"
@@ -895,6 +900,7 @@ int main(int argc, char **argv) {
   int nlist_every = 10;
   bool drift = false;
   bool nbmodes = false;
+  bool topo_only = false;
   double fric = 1e12;
   int gridx = 0;
   double spacing = 25.0;
@@ -919,6 +925,7 @@ int main(int argc, char **argv) {
     else if (k == "--nlist-every") { nlist_every = atoi(v); a++; }
     else if (k == "--drift") { drift = true; }
     else if (k == "--nbmodes") { nbmodes = true; }
+    else if (k == "--topo-only") { topo_only = true; }
     else if (k == "--fric") { fric = atof(v); a++; }
     else if (k == "--param") { st.param = v; a++; }
     else if (k == "--slowmode") { st.fastmode = false; }
@@ -985,6 +992,10 @@ int main(int argc, char **argv) {
     }
     put_d("pos", allpos, shp(b.ws->nAtoms(), 3));
     dump_topology(b, st);
+    if (topo_only) {  // coordinates and topology only (no reference results)
+      printf("built %zu atoms\n", b.ws->nAtoms());
+      return 0;
+    }
     dump_single_point(b, "");
     if (ntrials > 0) dump_trials(b, allpos, ntrials, trial_sigma_deg * 3.14159265358979323846 / 180.0, seed);
     if (minsteps > 0) {
@@ -1038,6 +1049,33 @@ int main(int argc, char **argv) {
       dump_minimise(b, Minimisation::SteepestDescent, minsteps, "minsd_");
       set_pos(*b.ws, pos);
       dump_minimise(b, Minimisation::ConjugateGradients, minsteps, "mincg_");
+    }
+    if (lcpo_asp != 0.0) {
+      // the whole forcefield with the LCPO term: a single point at step 0,
+      // velocity-Verlet and steepest-descent steps (as dump_lcpo records
+      // them for the reference's own component)
+      LcpoComponent *sasa = new LcpoComponent(*b.ws);
+      sasa->GlobalASP = lcpo_asp;
+      sasa->UpdateSasa = lcpo_update;
+      b.ff->add(*sasa);
+      b.ff->ensuresetup(*b.ws);
+      set_pos(*b.ws, pos);
+      b.ws->Step = 0;
+      b.ws->nlist().calcNewList();
+      b.ff->calcForces();
+      std::vector<double> e = ene_vec(b.ws->ene);
+      e.push_back(b.ws->ene.epot_surf);
+      put_d("lcpo_f_total", get_f(*b.ws), shp(b.ws->nAtoms(), 3));
+      put_d("lcpo_ene_total", e);
+      if (lcpo_steps > 0) {
+        set_pos(*b.ws, pos);
+        dump_md_steps(b, MolecularDynamics::VelocityVerlet, lcpo_steps, 1e12, "lcpo_mdvv_");
+        set_pos(*b.ws, pos);
+        b.ws->Step = 0;
+        dump_minimise(b, Minimisation::SteepestDescent, lcpo_steps, "lcpo_minsd_");
+      }
+      printf("replayed %zu atoms\n", b.ws->nAtoms());
+      return 0;
     }
     if (steps > 0) {
       // the reference's own protocol loop (md.cpp:202-267) for `steps`

@@ -23,7 +23,8 @@ std::map<int, pdgpu_ctx *> &contexts() {
   static std::map<int, pdgpu_ctx *> m;
   return m;
 }
-pdgpu_ctx *context_for(int device) {
+}  // namespace
+pdgpu_ctx *plugin_context(int device) {
   std::map<int, pdgpu_ctx *> &m = contexts();
   std::map<int, pdgpu_ctx *>::iterator it = m.find(device);
   if (it != m.end()) return it->second;
@@ -33,7 +34,6 @@ pdgpu_ctx *context_for(int device) {
   m[device] = c;
   return c;
 }
-}  // namespace
 
 FF_GeneralizedBorn_Still_GPU::FF_GeneralizedBorn_Still_GPU(WorkSpace &newwspace, int device)
     : FF_GeneralizedBorn_Still(newwspace), Device(device), m_ctx(0), m_sys(-1), m_listCount(0),
@@ -70,7 +70,7 @@ void FF_GeneralizedBorn_Still_GPU::setup() {
   WorkSpace &wspace = getWSpace();
   const int n = (int)wspace.atom.size();
   release();
-  m_ctx = context_for(Device);
+  m_ctx = plugin_context(Device);
 
   std::vector<double> q(n), rad(n), eps(n), mass(n), gbr(n);
   std::vector<int32_t> ir(n);

@@ -40,6 +40,9 @@ struct pdgpu_ctx;
 
 namespace Physics {
 
+/// the libpdgpu context of a device, shared by the components of a process
+pdgpu_ctx *plugin_context(int device);
+
 class FF_GeneralizedBorn_Still_GPU : public FF_GeneralizedBorn_Still {
  public:
   explicit FF_GeneralizedBorn_Still_GPU(WorkSpace &newwspace, int device = 0);

@@ -1,10 +1,11 @@
-"""GPU: the drop-in component FF_GeneralizedBorn_Still_GPU
-(pd.arcus_b200/plugin) driven by the reference's own C++ protocols.
+"""GPU: the drop-in components FF_GeneralizedBorn_Still_GPU and
+FF_SASA_LCPO_GPU (pd.arcus_b200/plugin) driven by the reference's own C++
+protocols.
 
 oracle/_ref/ref_driver_gpu is the reference driver (oracle/ref_driver.cpp,
 linked with the reference library compiled from its sources) built with
-the B200 component in place of FF_GeneralizedBorn_Still; oracle/_ref/
-ref_driver is the same driver with the reference's own component.  Both
+the B200 components in place of FF_GeneralizedBorn_Still and FF_SASA_LCPO;
+oracle/_ref/ref_driver is the same driver with the reference's own.  Both
 replay one fixture system: single-point forces and energies through
 Forcefield::calcForces / calcEnergies, two integrator steps, 10 SD and 10
 CG steps through Minimisation::runcore, and 20 Langevin steps through
@@ -35,7 +36,7 @@ def energy_close(got_J, ref_J, rel=1e-5, abs_kcal=1e-3):
     return abs(got_J - ref_J) * J2K <= max(rel * abs(ref_J) * J2K, abs_kcal)
 
 
-def _replay(binary, name, out):
+def _replay(binary, name, out, extra=None):
     arrays, meta = load_fixture(name)
     src = tempfile.mkdtemp(prefix="pdplug_in_")
     try:
@@ -44,10 +45,10 @@ def _replay(binary, name, out):
             for c in meta["chains"]:
                 fh.write("chain %s\n" % c)
         env = dict(os.environ, PD_PARAM_PATH=os.path.join(REF, "param"))
+        args = extra if extra is not None else ["--md", "2", "--min", "10", "--steps", "20", "--nlist-every", "10"]
         subprocess.run([os.path.join(REF, binary), "replay", "--in", src, "--out", out, "--cutoff", meta["cutoff"],
-                        "--inner", meta["inner"], "--param", meta["param"], "--md", "2", "--min", "10",
-                        "--steps", "20", "--nlist-every", "10"], env=env, check=True, capture_output=True,
-                       timeout=600)
+                        "--inner", meta["inner"], "--param", meta["param"]] + args, env=env, check=True,
+                       capture_output=True, timeout=600)
     finally:
         shutil.rmtree(src, ignore_errors=True)
     return {f[:-4]: np.load(os.path.join(out, f)) for f in os.listdir(out) if f.endswith(".npy")}, arrays
@@ -95,3 +96,22 @@ def test_component_in_protocols(replays):
     assert int(gpu["proto_md_ene"][-1]) == int(cpu["proto_md_ene"][-1]) == 20
     assert np.max(np.abs(gpu["proto_md_x"] - cpu["proto_md_x"])) <= 1e-4
     assert energy_close(gpu["proto_md_ene"][0], cpu["proto_md_ene"][0], rel=1e-4)
+
+
+def test_lcpo_component_in_protocols():
+    """{FF_Bonded, GB, LCPO} with both B200 components: the single point at
+    step 0, 12 velocity-Verlet steps and 12 steepest-descent steps
+    (UpdateSasa 5: the held forces on the steps between), against the
+    reference's own run of the same (tests/golden/lcpo_pep24_s5.npz)."""
+    tmp = tempfile.mkdtemp(prefix="pdplug_lcpo_")
+    try:
+        gpu, a = _replay("ref_driver_gpu", "lcpo_pep24_s5", os.path.join(tmp, "gpu"),
+                         ["--lcpo-asp", "0.005", "--lcpo", "5,12"])
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    assert rel_rms(gpu["lcpo_f_total"], a["lcpo_f_total"]) <= 1e-5
+    for k in (0, 10):  # epot, epot_surf
+        assert energy_close(gpu["lcpo_ene_total"][k], a["lcpo_ene_total"][k]), k
+    assert np.max(np.abs(gpu["lcpo_mdvv_x"] - a["lcpo_mdvv_x"])) <= 1e-4
+    assert np.max(np.abs(gpu["lcpo_minsd_x"] - a["lcpo_minsd_x"])) <= 1e-4
+    assert gpu["lcpo_minsd_result"][0] == a["lcpo_minsd_result"][0]
