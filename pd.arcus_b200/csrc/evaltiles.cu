@@ -190,7 +190,8 @@ __device__ __forceinline__ void phase_born(const PackView &v, int warp, int lane
     bool any = false;    // a pair inside the Still cutoff's guard band
 #pragma unroll
     for (int t = 0; t < 8; t++) {
-      long long tI = 0, tJ = 0;
+      long long tI = 0;
+      float tJ = 0.f;  // the j side's term, made fixed point by the lane that owns j (the same bits)
       if ((rows >> t) & 1u) {
         const float4 ja = sA[warp][a + t], jb = sB[warp][a + t];
         const Dx d = diff(ia, ib, ja, jb);
@@ -204,11 +205,11 @@ __device__ __forceinline__ void phase_born(const PackView &v, int warp, int lane
           const float4 jc = sC[warp][a + t];
           const float term = born_term_noV(d, Ri, jc.x, invP5, piP5, P4s);
           tI = __float2ll_rn(__fmul_rn(term, jc.y));
-          tJ = __float2ll_rn(__fmul_rn(term, Vi));
+          tJ = __fmul_rn(term, Vi);
         }
       }
       acc_i += tI;
-      jacc += __shfl_sync(0xffffffffu, tJ, g8 | ((a - t) & 7));
+      jacc += __float2ll_rn(__shfl_sync(0xffffffffu, tJ, g8 | ((a - t) & 7)));
     }
     if (__any_sync(0xffffffffu, any)) {
       near |= 1u << (e - run0);
