@@ -395,6 +395,7 @@ std::vector<Job *> pdgpu_server::group_with(Job *j) {
     if ((int)more.size() + 1 >= kGroupMax) break;
     if (c == j || c->spec.kind != kind || c->natoms > kTileSearchMaxAtoms) continue;
     if (c->host->lcpo_update != j->host->lcpo_update) continue;
+    if (c->host->params.FastMode != j->host->params.FastMode) continue;  // one pair-term path per pack
     if (kind == PDGPU_JOB_MINIMISE &&
         (c->spec.steps != j->spec.steps || std::memcmp(&c->spec.min, &j->spec.min, sizeof j->spec.min) != 0))
       continue;
