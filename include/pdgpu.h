@@ -482,7 +482,8 @@ typedef struct {
 
 typedef struct {
   int64_t submitted, completed, failed;
-  int32_t active, queued, peak_active, _reserved;
+  int32_t active, queued, peak_active;
+  int32_t groups;       /* admissions that packed two or more jobs together     */
   int64_t bytes_in_use, peak_bytes;
 } pdgpu_serve_stats;
 

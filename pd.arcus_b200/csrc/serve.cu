@@ -432,6 +432,7 @@ void pdgpu_server::admit(Job *j, const std::vector<Job *> &more) {
       stats.active++;
       stats.queued--;
     }
+    if (S > 1) stats.groups++;
     stats.peak_active = std::max(stats.peak_active, stats.active);
   }
   for (int q = 0; q < S; q++) {

@@ -91,7 +91,7 @@ class JobInfo(ctypes.Structure):
 class ServeStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
                 ("active", ctypes.c_int32), ("queued", ctypes.c_int32), ("peak_active", ctypes.c_int32),
-                ("_reserved", ctypes.c_int32), ("bytes_in_use", ctypes.c_int64), ("peak_bytes", ctypes.c_int64)]
+                ("groups", ctypes.c_int32), ("bytes_in_use", ctypes.c_int64), ("peak_bytes", ctypes.c_int64)]
 
 
 JOB_ENERGY, JOB_MINIMISE, JOB_MD = 0, 1, 2

@@ -172,3 +172,29 @@ def test_serve_failed_job_does_not_disturb_others(gpu_ctx):
         assert np.array_equal(got["positions"], r["positions"])
     assert srv.info(bad)["state"] == 3
     srv.close()
+
+
+@pytest.mark.parametrize("kind", ["energy", "minimise"])
+def test_serve_group_equals_alone(gpu_ctx, kind):
+    """Jobs that queue behind a busy slot are admitted as one group (one
+    pack, one launch sequence); each member's results are the bits it gets
+    served alone."""
+    import pdgpu
+    members = _members(gpu_ctx, 8)
+    S = pdgpu.Server
+    mn = pdgpu.min_params_default()
+    mn.Algorithm = pdgpu.Minimisation.SteepestDescent
+    job = (lambda: S.job(S.ENERGY)) if kind == "energy" else (lambda: S.job(S.MINIMISE, 40, minimiser=mn))
+    srv = pdgpu.Server(gpu_ctx, max_active=1, lanes=LANES, tiles=True)
+    alone, _ = _run(srv, members, [job() for _ in members], together=False)
+    grouped, infos = _run(srv, members, [job() for _ in members], together=True)
+    st = srv.stats()
+    srv.close()
+    assert st["groups"] >= 1  # the queued jobs shared a pack
+    for a, g, (ws, ff, arr, m) in zip(alone, grouped, members):
+        for key in a:
+            assert np.array_equal(a[key], g[key]), key
+        if kind == "energy":
+            assert rel_rms(g["forces"], arr["f_total"]) <= 1e-5
+    for ws, *_ in members:
+        ws.close()
