@@ -383,6 +383,13 @@ __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane
       sA[warp][lane] = sA[warp][lane + 8] = cur.a;
       sB[warp][lane] = sB[warp][lane + 8] = b;
       sP[warp][lane] = sP[warp][lane + 8] = cur.c;
+    } else if (lane < 8) {
+      // a j-cluster shorter than 8 atoms: its empty slots hold zero records,
+      // so the masked-out terms of those slots multiply finite numbers
+      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+      sA[warp][lane] = sA[warp][lane + 8] = z;
+      sB[warp][lane] = sB[warp][lane + 8] = z;
+      sP[warp][lane] = sP[warp][lane + 8] = z;
     }
     const unsigned rows = rot8(cur.row, a);
     unsigned xrows = 0, brows = 0;  // bond order <= 2, == 3
