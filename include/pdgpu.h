@@ -532,9 +532,13 @@ int pdgpu_profile_pair_kernels(pdgpu_ctx *ctx, int32_t sys, int32_t reps, double
  * PDGPU_ERR_STATE unless the handle is on the tile layout. */
 int pdgpu_profile_eval(pdgpu_ctx *ctx, int32_t sys, int32_t reps, double *ms, int64_t *counts);
 /* How an evaluation on the tile layout is launched (no reference
- * counterpart): 1 = the three passes in one cooperative launch (the
- * default), 0 = the same three phases as three launches; -1 = only report.
- * Both give the same bits.  *current (may be NULL) receives the mode. */
+ * counterpart): 1 = the three passes in one cooperative launch everywhere,
+ * 0 = the same three phases as three launches everywhere, 2 (the default) =
+ * one cooperative launch for single evaluations and minimiser / Monte Carlo
+ * steps, three launches inside MD step blocks (where the next step's first
+ * phase can start beside the bonded terms and the previous step's energy
+ * record); -1 = only report.  Every mode gives the same bits.  *current
+ * (may be NULL) receives the mode. */
 int pdgpu_eval_mode(pdgpu_ctx *ctx, int32_t sys, int32_t set, int32_t *current);
 /* Device times (CUDA events, averaged over reps full evaluations at step 0)
  * of the LCPO term's two launches and the work they did: out[0] overlap

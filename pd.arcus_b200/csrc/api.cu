@@ -1331,7 +1331,7 @@ void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce) {
   step.imm = e->ws_step;
   calc_forces_enqueue(st, e, reduce, step);
 }
-void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce, StepSrc step, int ebuf) {
+void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce, StepSrc step, int ebuf, int coop) {
   Pack &P = *e->pack;
   const bool bonded = has_bonded(P);
   const bool surf = P.v.lc.update > 0;
@@ -1362,7 +1362,7 @@ void pdgpu::calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce, StepS
     if (slow) P.wait_energy(st, ebuf ^ 1);
     PackView vb = P.v;
     vb.ebuf = ebuf;
-    launch_eval_tiles(vb, st, zero, P.coop);
+    launch_eval_tiles(vb, st, zero, coop < 0 ? P.coop : coop != 0);
     P.last_ebuf = ebuf;
   } else {
     launch_born_radii(P.v, st, zero);
@@ -1498,7 +1498,7 @@ void pdgpu::md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k, int q
   StepSrc step;
   step.p = e->step_dev;  // MolecularDynamics::run_core sets WorkSpace::Step = Step (md.cpp:214)
   const int b = (P.v.tile_mode && !P.slow()) ? (q & 1) : 0;  // this step's energy buffer
-  calc_forces_enqueue(st, e, false, step, b);
+  calc_forces_enqueue(st, e, false, step, b, P.coop_md ? 1 : 0);
   // the integrator writes the kinetic energies the previous step's record
   // reads: that record must be done
   P.wait_energy(st, b ^ 1);
@@ -1704,7 +1704,7 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
         snprintf(key, sizeof key, "%d|%d|%p|%lld|%p|%d|%d|%.17g|%.17g|%.17g|%d|%d|%d|%d%d%d|%d%d%d|%p|%d|%d", block,
                  (int)rebuild, (void *)v.nl, v.nl_cap, (void *)e->hist, k.integrator, k.steps, k.dt, k.gamma,
                  k.temp, k.stochastic_h, P.radix_passes, (int)e->host->params.FastMode, v.lpa[0], v.lpa[1],
-                 v.lpa[2], v.tile_mode, (int)tile_search_ok(P), (int)P.coop, (void *)e->traj_dev, e->traj_every,
+                 v.lpa[2], v.tile_mode, (int)tile_search_ok(P), (int)P.coop_md, (void *)e->traj_dev, e->traj_every,
                  e->traj_dev_cap);
         SysEntry::GraphSlot *g = nullptr;
         for (auto &q : e->gslots)
@@ -1732,11 +1732,11 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
             e->drop_slot(ng);
             P.ene_pending[0] = pend0;
             P.ene_pending[1] = pend1;
-            if (P.coop && P.v.tile_mode) {
+            if (P.coop_md && P.v.tile_mode) {
               // a graph that cannot hold the cooperative evaluation: the
               // same phases as three launches from here on
               cudaGetLastError();
-              P.coop = false;
+              P.coop_md = false;
               continue;
             }
             return cuda_fail(ce, "capture md block");
@@ -2192,15 +2192,18 @@ int pdgpu_eval_mode(pdgpu_ctx *c, int32_t sys, int32_t set, int32_t *current) {
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
   Pack &P = *e->pack;
-  if (set < -1 || set > 1) {
-    set_error("pdgpu_eval_mode: set must be -1 (query), 0 (three launches) or 1 (one cooperative launch)");
+  if (set < -1 || set > 2) {
+    set_error("pdgpu_eval_mode: set must be -1 (query), 0 (three launches), 1 (one cooperative launch) or 2 "
+              "(cooperative for single evaluations, three launches inside MD step blocks)");
     return PDGPU_ERR_ARG;
   }
-  if (set >= 0 && P.coop != (set == 1)) {
-    P.coop = set == 1;
-    e->drop_graph();
+  if (set >= 0) {
+    const bool one = set >= 1, md = set == 1;
+    if (P.coop_md != md) e->drop_graph();
+    P.coop = one;
+    P.coop_md = md;
   }
-  if (current) *current = P.coop ? 1 : 0;
+  if (current) *current = P.coop ? (P.coop_md ? 1 : 2) : 0;
   return PDGPU_OK;
 }
 

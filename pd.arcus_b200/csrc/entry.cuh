@@ -161,7 +161,8 @@ bool has_bonded(const Pack &P);
 // chain rule, surface term; one energy reduction if reduce.  `step` is
 // where the surface term reads WorkSpace::Step (default: e->ws_step).
 void calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce);
-void calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce, StepSrc step, int ebuf = 0);
+// (coop: -1 = the pack's single-evaluation launch form, else 0/1)
+void calc_forces_enqueue(cudaStream_t st, SysEntry *e, bool reduce, StepSrc step, int ebuf = 0, int coop = -1);
 // one MD step: forces, integrator, energy record (+ step counter advance);
 // q = the step's index in its block (its energy buffer is q & 1 on tiles)
 void md_step_enqueue(cudaStream_t st, SysEntry *e, const MDCoef &k, int q);

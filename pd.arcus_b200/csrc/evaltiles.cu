@@ -48,9 +48,8 @@
 namespace pdgpu {
 
 constexpr int kEvWarps = 4;  // warps per block
-#ifndef PDGPU_EV_BLOCKS
-#define PDGPU_EV_BLOCKS 5    // resident blocks per SM the register allocation must allow
-#endif
+// resident blocks per SM the register allocation must allow: 4 (up to 128
+// registers a thread; the default), or 5 (PDGPU_EV_BLOCKS=5; 102 registers)
 constexpr unsigned kBarrierNaps = 1u << 22;  // about half a second of 100 ns naps
 
 // ------------------------------------------------------------- barrier
@@ -625,7 +624,7 @@ __device__ __forceinline__ void epilogue_energies(const PackView &v) {
 // ============================================================= the kernel
 // PH: which phases (1 A, 2 B, 4 C); more than one needs a cooperative
 // launch.  MINB: resident blocks per SM the register allocation must allow
-// (PDGPU_EV_BLOCKS, 4 or 5, picks the build at run time).  tile_count[2] is the still-list length, tile_count[3] the
+// (PDGPU_EV_BLOCKS, 4 or 5, picks the build at run time; 4 by default).  tile_count[2] is the still-list length, tile_count[3] the
 // barrier / exit counter; the last block out clears both.
 template <int PH, int MINB>
 __global__ void __launch_bounds__(32 * kEvWarps, MINB) k_eval_tiles(PackView v, int zero) {
@@ -680,7 +679,7 @@ static int ev_minb() {
   static int m = 0;
   if (!m) {
     const char *s = getenv("PDGPU_EV_BLOCKS");
-    m = (s && s[0] == '4') ? 4 : PDGPU_EV_BLOCKS;
+    m = (s && s[0] == '5') ? 5 : 4;
   }
   return m;
 }
@@ -694,7 +693,7 @@ int eval_tiles_grid(long long tile_cap) {
   if (ev_minb() == 4)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_eval_tiles<7, 4>, 32 * kEvWarps, 0);
   else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_eval_tiles<7, PDGPU_EV_BLOCKS>, 32 * kEvWarps, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_eval_tiles<7, 5>, 32 * kEvWarps, 0);
   const long long need = (tile_cap + kEvWarps - 1) / kEvWarps;
   return (int)std::max(1LL, std::min((long long)std::max(occ, 1) * sms, need));
 }
@@ -723,7 +722,7 @@ static cudaError_t launch_ev(const PackView &v, cudaStream_t st, int zero, bool 
   cfg.attrs = attr;
   cfg.numAttrs = na;
   cudaError_t e = ev_minb() == 4 ? cudaLaunchKernelEx(&cfg, k_eval_tiles<PH, 4>, v, zero)
-                                 : cudaLaunchKernelEx(&cfg, k_eval_tiles<PH, PDGPU_EV_BLOCKS>, v, zero);
+                                 : cudaLaunchKernelEx(&cfg, k_eval_tiles<PH, 5>, v, zero);
   count_launch();
   return e;
 }

@@ -327,8 +327,12 @@ struct Pack {
     }
   }
   // evaluations may use the cooperative single-launch kernel (not for the
-  // request loop's jobs, whose streams run side by side)
+  // request loop's jobs, whose streams run side by side).  Inside an MD
+  // step block the three-launch form is the default: its first phase starts
+  // while the bonded terms and the previous step's energy record still hold
+  // SMs, where a cooperative grid waits for all of its blocks to fit.
   bool coop = true;
+  bool coop_md = false;
   ~Pack();
 };
 

@@ -473,6 +473,7 @@ void pdgpu_server::admit(Job *j, const std::vector<Job *> &more) {
   P.v.tile_mode = prm.tiles ? 1 : 0;
   P.tuned = true;
   P.coop = false;  // jobs run side by side on their own streams: no cooperative launches
+  P.coop_md = false;
   if (prm.tiles && (r = pack_ensure_tiles(&P))) {
     fail(j, r, last_error_cstr());
     return;

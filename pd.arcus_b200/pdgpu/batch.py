@@ -93,7 +93,8 @@ class Batch:
 
     def setEvalMode(self, mode):
         """Launch form of an evaluation on the tile layout: 1 one
-        cooperative launch, 0 three launches, -1 report only."""
+        cooperative launch, 0 three launches, 2 (the default) cooperative
+        except inside MD step blocks, -1 report only."""
         cur = ctypes.c_int32(0)
         A.check(A.lib().pdgpu_eval_mode(self.ctx.ptr, self._id, int(mode), ctypes.byref(cur)))
         return cur.value

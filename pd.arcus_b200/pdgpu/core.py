@@ -253,8 +253,9 @@ class WorkSpace:
 
     def setEvalMode(self, mode):
         """Launch form of an evaluation on the tile layout: 1 one
-        cooperative launch, 0 three launches, -1 report only; returns the
-        form in use."""
+        cooperative launch, 0 three launches, 2 (the default) cooperative
+        except inside MD step blocks, -1 report only; returns the form in
+        use."""
         cur = ctypes.c_int32(0)
         A.check(A.lib().pdgpu_eval_mode(self.ctx.ptr, self._device(), int(mode), ctypes.byref(cur)))
         return cur.value

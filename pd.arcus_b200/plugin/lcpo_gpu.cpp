@@ -3,6 +3,7 @@
 // linked with the reference library and libpdgpu.so.
 #include "lcpo_gpu.h"
 
+#include <algorithm>
 #include <cstdlib>
 #include <string>
 #include <vector>
@@ -19,12 +20,14 @@ namespace Physics {
 pdgpu_ctx *plugin_context(int device);  // gbff_gpu.cpp: one context per device
 
 FF_SASA_LCPO_GPU::FF_SASA_LCPO_GPU(WorkSpace &newwspace, int device)
-    : FF_SASA_LCPO(newwspace), Device(device), m_ctx(0), m_sys(-1), m_listCount(0), m_haveList(false) {
+    : FF_SASA_LCPO(newwspace), Device(device), m_ctx(0), m_sys(-1), m_listCount(0), m_haveList(false),
+      m_slack(0.0) {
   name = "LCPO SASA, B200";
 }
 
 FF_SASA_LCPO_GPU::FF_SASA_LCPO_GPU(const FF_SASA_LCPO_GPU &other)
-    : FF_SASA_LCPO(other), Device(other.Device), m_ctx(0), m_sys(-1), m_listCount(0), m_haveList(false) {
+    : FF_SASA_LCPO(other), Device(other.Device), m_ctx(0), m_sys(-1), m_listCount(0), m_haveList(false),
+      m_slack(0.0) {
   needsetup = true;
 }
 
@@ -124,6 +127,11 @@ void FF_SASA_LCPO_GPU::setup() {
                             c14i.empty() ? 0 : &c14i[0], &p, &sys),
         "system_create");
   m_sys = sys;
+  double reach = 0.0;  // the largest overlap distance r_i + r_j
+  for (int i = 0; i < n; i++)
+    if (use[i] && 2.0 * rad[i] > reach) reach = 2.0 * rad[i];
+  m_slack = std::max(p.Cutoff, p.VdwCutoff) + p.Padding - reach;
+  m_ref.assign(3 * (size_t)n, 0.0);
   check(pdgpu_sasa_lcpo_set(m_ctx, m_sys, &rad[0], &p4[0], &sigma[0], &use[0], UpdateSasa), "sasa_lcpo_set");
   m_haveList = false;
   m_buf.assign(3 * (size_t)n, 0.0);
@@ -140,8 +148,21 @@ void FF_SASA_LCPO_GPU::upload_and_list() {
   }
   check(pdgpu_set_positions(m_ctx, m_sys, &m_buf[0]), "set_positions");
   const unsigned count = wspace.nlist().getFullUpdateCount();
-  if (!m_haveList || count != m_listCount) {
+  bool stale = !m_haveList || count != m_listCount;
+  if (!stale) {
+    // a pair that was beyond the list cutoff at the build and is now inside
+    // the largest overlap distance has closed by more than the slack: no
+    // atom may have moved by half of it
+    const double lim = 0.25 * m_slack * m_slack;
+    for (size_t i = 0; i < n && !stale; i++) {
+      const double dx = m_buf[3 * i] - m_ref[3 * i], dy = m_buf[3 * i + 1] - m_ref[3 * i + 1],
+                   dz = m_buf[3 * i + 2] - m_ref[3 * i + 2];
+      stale = m_slack <= 0.0 || dx * dx + dy * dy + dz * dz >= lim;
+    }
+  }
+  if (stale) {
     check(pdgpu_nlist_build(m_ctx, m_sys), "nlist_build");
+    m_ref = m_buf;
     m_listCount = count;
     m_haveList = true;
   }

@@ -19,8 +19,15 @@
 //                   ene.epot_surf
 //   calcEnergies()  the energy path's areas and energy, no forces
 // A per-type ASP section (ASPsection_name) is not supported: setup throws.
-// The device list follows the workspace's (NeighbourListBase::
-// getFullUpdateCount), so the overlap partners are the reference's.
+// The device list is rebuilt whenever the workspace's is
+// (NeighbourListBase::getFullUpdateCount) and also whenever an atom has
+// moved far enough since the device list was built that a pair inside the
+// largest overlap distance (twice the largest LCPO radius) could be missing
+// from it: the device list holds pairs within 7 A plus the list padding,
+// where the workspace's list, which the reference's term walks, holds pairs
+// within the largest requested cutoff (the GB cutoff, in practice), so in a
+// minimisation's large steps the 7 A list alone can lose overlap partners
+// that the reference still sees.
 #ifndef PDGPU_LCPO_GPU_H
 #define PDGPU_LCPO_GPU_H
 
@@ -58,6 +65,8 @@ class FF_SASA_LCPO_GPU : public FF_SASA_LCPO {
   int m_sys;
   unsigned m_listCount;
   bool m_haveList;
+  double m_slack;             // list cutoff - the largest overlap distance (A)
+  std::vector<double> m_ref;  // [3N] positions at the last device list build
   std::vector<double> m_buf;
   std::vector<double> m_ene;
 };

@@ -110,10 +110,11 @@ def test_md_one_launch_equals_three(gpu_ctx):
     import ctypes
     arrays, meta = load_fixture("c1_pep64_s0")
     out = []
-    for mode in (1, 0):
+    for mode in (1, 0, 2):
         ws, ff = build_workspace(arrays, meta, gpu_ctx)
         ws.setPairPath(1)
-        ws.setEvalMode(mode)
+        assert ws.setEvalMode(-1) == 2  # the default
+        assert ws.setEvalMode(mode) == mode
         ws.nlist().calcNewList()
         p = A.md_params_default()
         p.Integrator, p.UpdateNList, p.UseGraph = A.INTEGRATOR_LANGEVIN, 10, 1
@@ -130,3 +131,4 @@ def test_md_one_launch_equals_three(gpu_ctx):
     assert np.all(np.isfinite(out[0][0]))
     for q in range(3):
         assert np.array_equal(out[0][q], out[1][q])
+        assert np.array_equal(out[0][q], out[2][q])
