@@ -105,11 +105,84 @@ __device__ __forceinline__ unsigned rot8(unsigned row, int a) {
 }
 
 // Tile staging shared by the phases: the tile's metadata, this lane's row
-// bits and, in lanes 0..7, the j atom's records, prefetched one tile ahead.
+// bits and bond-order rows and, in lanes 0..7, the j atom's records and the
+// per-atom inputs the phase forms from them.  Records are loaded one tile
+// ahead of their use and the metadata two tiles ahead (the records' address
+// depends on it), so no tile waits for a load chain.
 struct EvStage {
   int4 m;
-  unsigned row;
+  unsigned row, x0, x1;  // list bits; bond order <= 2 rows; == 3 rows
   float4 a, b, c;
+  double u;              // phase B: terms123[j]; phase C: born_d[j]
+  long long w;           // phase B: bsum[j]; phase C: the dE/da sum of j
+};
+// PH: the phase (1 A, 2 B, 4 C) the stage is for.
+template <int PH>
+__device__ __forceinline__ void ev_stage(const PackView &v, int t, int lane, EvStage &q) {
+  q.row = tile_row(v, t, lane);
+  q.x0 = q.x1 = 0;
+  if (q.m.y >= 0) {
+    q.x0 = spec_row(v, q.m.y, 0, lane);
+    if (PH == 2) q.x1 = spec_row(v, q.m.y, 1, lane);
+  }
+  if (lane <= (q.m.w & 7)) {
+    const int j = q.m.x + lane;
+    q.a = v.pq[2 * (size_t)j];
+    q.b = v.pq[2 * (size_t)j + 1];
+    q.c = v.prm[j];
+    if (PH == 2) {
+      q.u = v.terms123[j];
+      q.w = v.bsum[j];
+    }
+    if (PH == 4) {
+      q.u = v.born_d[j];
+      q.w = v.ej[(size_t)3 * v.n_atoms + j];
+    }
+  }
+}
+// Walks a warp's tiles [e, e1) (PH 1, 2) or still-list entries (PH 4) with
+// the two-deep prefetch: next() returns the stage of the current tile and
+// its index, and issues the loads for the tiles after it.
+template <int PH>
+struct EvWalk {
+  int e, e1;
+  int t1, t2;   // tiles of items e+1 and e+2
+  int4 m1;      // metadata of item e+1
+  EvStage nx;   // stage of item e
+  __device__ __forceinline__ int tile_of(const PackView &v, int k) const {
+    return PH == 4 ? v.still_list[k] : k;
+  }
+  __device__ __forceinline__ void start(const PackView &v, int lane, int b, int end) {
+    e = b;
+    e1 = end;
+    if (e < e1) {
+      const int t0 = tile_of(v, e);
+      nx.m = v.tile_meta[t0];
+      ev_stage<PH>(v, t0, lane, nx);
+    }
+    if (e + 1 < e1) {
+      t1 = tile_of(v, e + 1);
+      m1 = v.tile_meta[t1];
+    }
+    if (e + 2 < e1) t2 = tile_of(v, e + 2);
+  }
+  // the current item's stage; advances the prefetch by one item
+  __device__ __forceinline__ EvStage next(const PackView &v, int lane, int &tile) {
+    const EvStage cur = nx;
+    tile = PH == 4 ? -1 : e;
+    if (e + 1 < e1) {
+      nx.m = m1;
+      ev_stage<PH>(v, t1, lane, nx);
+    }
+    if (e + 2 < e1) {
+      m1 = v.tile_meta[t2];
+      t1 = t2;
+    }
+    if (PH == 4 && e + 3 < e1) t2 = v.still_list[e + 3];
+    if (PH != 4) t2 = e + 3;
+    e++;
+    return cur;
+  }
 };
 
 // ============================================================= phase A
@@ -129,17 +202,8 @@ __device__ __forceinline__ void phase_born(const PackView &v, int warp, int lane
   long long acc_i = 0;
   unsigned near = 0;
   int run0 = e;
-  EvStage nx;
-  auto load = [&](int t, EvStage &q) {
-    q.m = v.tile_meta[t];
-    q.row = tile_row(v, t, lane);
-    if (lane <= (q.m.w & 7)) {
-      const int j = q.m.x + lane;
-      q.a = v.pq[2 * (size_t)j];
-      q.b = v.pq[2 * (size_t)j + 1];
-      q.c = v.prm[j];
-    }
-  };
+  EvWalk<1> walk;
+  walk.start(v, lane, e, e1);
   auto flush_near = [&](int upto) {
     // tiles [run0, upto) with their bits in `near`
     const int cnt = __popc(near);
@@ -152,11 +216,10 @@ __device__ __forceinline__ void phase_born(const PackView &v, int warp, int lane
     near = 0;
     run0 = upto;
   };
-  if (e < e1) load(e, nx);
   for (; e < e1; e++) {
-    const EvStage cur = nx;
+    int te;
+    const EvStage cur = walk.next(v, lane, te);
     const TileInfo ti = tile_info(cur.m);
-    if (e + 1 < e1) load(e + 1, nx);
     if (ti.a0 != a0) {
       if (lane < na && acc_i) atomicAdd((unsigned long long *)&v.bsum[a0 + lane], (unsigned long long)acc_i);
       acc_i = 0;
@@ -181,9 +244,7 @@ __device__ __forceinline__ void phase_born(const PackView &v, int warp, int lane
       sB[warp][lane] = sB[warp][lane + 8] = cur.b;
       sC[warp][lane] = sC[warp][lane + 8] = make_float4(cur.c.z, cur.c.w, 0.f, 0.f);
     }
-    unsigned rows = cur.row;
-    if (ti.spec >= 0) rows &= ~spec_row(v, ti.spec, 0, lane);  // bond order > 2 only
-    rows = rot8(rows, a);
+    const unsigned rows = rot8(cur.row & ~cur.x0, a);  // bond order > 2 only
     __syncwarp();
     long long jacc = 0;  // lane (g,a): j atom a, this group's i atoms
     bool any = false;    // a pair inside the Still cutoff's guard band
@@ -303,61 +364,56 @@ __device__ __forceinline__ PairOut pair_gb(const GbSettings &g, float r2, bool i
 }
 
 // The i side of a tile is converted to fixed point per tile (so its sums
-// depend on the tile alone) and kept in 64-bit registers while the warp's
-// range stays in one i-cluster; the sums go to memory when the range moves
-// to the next cluster.  Exact integer sums: the same bits as adding every
-// tile's share to memory at once.
+// depend on the tile alone) and kept in this lane's shared-memory slots
+// while the warp's range stays in one i-cluster; the sums go to memory when
+// the range moves to the next cluster.  Exact integer sums: the same bits
+// as adding every tile's share to memory at once.
 struct ISide {
-  long long f[7];
+  long long (*f)[32];  // [7][32]: this warp's slots
+  int lane;
   bool bad;
   __device__ __forceinline__ void clear() {
 #pragma unroll
-    for (int q = 0; q < 7; q++) f[q] = 0;
+    for (int q = 0; q < 7; q++) f[q][lane] = 0;
     bad = false;
   }
   __device__ __forceinline__ void add(int q, float x) {
     bad |= !(fabsf(x) <= 3.0e38f);
-    f[q] += to_fixed_j(x);
+    f[q][lane] += to_fixed_j(x);
   }
   __device__ __forceinline__ void flush(const PackView &v, int i, int s, int N) {
     long long *dst[7] = {v.hx + i, v.hy + i, v.hz + i, v.ej + i, v.ej + (size_t)N + i, v.ej + (size_t)2 * N + i,
                          v.ej + (size_t)3 * N + i};
 #pragma unroll
-    for (int q = 0; q < 7; q++)
-      if (f[q]) atomicAdd((unsigned long long *)dst[q], (unsigned long long)f[q]);
+    for (int q = 0; q < 7; q++) {
+      const long long x = f[q][lane];
+      if (x) atomicAdd((unsigned long long *)dst[q], (unsigned long long)x);
+    }
     if (bad) atomicOr(&(v.ebuf ? v.sys_flags_alt : v.sys_flags)[s], SF_NONFINITE);
   }
 };
 
 __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane, float4 (*sA)[16],
-                                           float4 (*sB)[16], float4 (*sP)[16]) {
+                                           float4 (*sB)[16], float4 (*sP)[16], long long (*sI)[7][32]) {
   int e, e1;
   ev_range(v.tile_count[0], warp, e, e1);
   const int N = v.n_atoms;
   const int g8 = lane & ~7, a = lane & 7;
   int a0 = -1, i = 0, s_cur = -1, na = 0, s_i = 0;
   ISide acc;
+  acc.f = sI[warp];
+  acc.lane = lane;
   acc.clear();
   float4 ia = make_float4(0, 0, 0, 0), ib = ia, ip = ia;
   double ai_d = 0.0;
   const SysParams *P = nullptr;
   GbSettings gs;
-  EvStage nx;
-  auto load = [&](int t, EvStage &q) {
-    q.m = v.tile_meta[t];
-    q.row = tile_row(v, t, lane);
-    if (lane <= (q.m.w & 7)) {
-      const int j = q.m.x + lane;
-      q.a = v.pq[2 * (size_t)j];
-      q.b = v.pq[2 * (size_t)j + 1];
-      q.c = v.prm[j];
-    }
-  };
-  if (e < e1) load(e, nx);
+  EvWalk<2> walk;
+  walk.start(v, lane, e, e1);
   for (; e < e1; e++) {
-    const EvStage cur = nx;
+    int te;
+    const EvStage cur = walk.next(v, lane, te);
     const TileInfo ti = tile_info(cur.m);
-    if (e + 1 < e1) load(e + 1, nx);
     if (ti.s != s_cur) {
       s_cur = ti.s;
       P = &v.sp[ti.s];
@@ -377,8 +433,10 @@ __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane
       ib.w = (float)ai_d;
     }
     if (lane < ti.nb) {
+      // the j atom's Born radius from its staged sum (born_radius's
+      // expression: the same bits)
       float4 b = cur.b;
-      b.w = (float)born_radius(v, *P, ti.b0 + lane);
+      b.w = (float)(-P->halfeconv_d / (cur.u + (double)cur.w * kInvBornScale) + P->born_offset_d);
       sA[warp][lane] = sA[warp][lane + 8] = cur.a;
       sB[warp][lane] = sB[warp][lane + 8] = b;
       sP[warp][lane] = sP[warp][lane + 8] = cur.c;
@@ -391,11 +449,7 @@ __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane
       sP[warp][lane] = sP[warp][lane + 8] = z;
     }
     const unsigned rows = rot8(cur.row, a);
-    unsigned xrows = 0, brows = 0;  // bond order <= 2, == 3
-    if (ti.spec >= 0) {
-      xrows = rot8(spec_row(v, ti.spec, 0, lane), a);
-      brows = rot8(spec_row(v, ti.spec, 1, lane), a);
-    }
+    const unsigned xrows = rot8(cur.x0, a), brows = rot8(cur.x1, a);  // bond order <= 2, == 3
     __syncwarp();
     float fx = 0.f, fy = 0.f, fz = 0.f, e_vdw = 0.f, e_el = 0.f, e_pol = 0.f, deda = 0.f;
     float jacc[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -447,17 +501,15 @@ __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane
 }
 
 // ============================================================= phase C
-// Chain-rule weight of atom i: gpi * dE/da_i, with gpi = a_i^2 / 166.0
-// (the literal of gbff.cpp:1755) and dE/da_i = the pair sum - Eself_i / a_i
-// (gbff.cpp:1731-1757; k_gb_finish's expression).
-__device__ __forceinline__ float chain_weight(const PackView &v, const SysParams &P, int i, int N) {
-  const double ai_d = v.born_d[i];
-  const double dd = (double)v.ej[(size_t)3 * N + i] * kInvJScale;
-  const double qd = (double)v.pq[2 * (size_t)i].w;
-  const double eself = P.premul_d * qd * qd / ai_d;
-  const double deda_i = dd - eself / ai_d;
-  const double gpi = ai_d * ai_d / 166.0;
-  return (float)(gpi * deda_i);
+// Chain-rule weight of an atom: gpi * dE/da with gpi = a^2 / 166.0 (the
+// literal of gbff.cpp:1755) and dE/da = the pair sum - Eself / a, Eself =
+// premul q^2 / a (gbff.cpp:1731-1757; k_gb_finish's expression), here as
+// (a^2 * sum - premul q^2) / 166 in FP64: one rounding apart, and the
+// weight is used in FP32.
+__device__ __forceinline__ float chain_weight(const SysParams &P, double ai_d, long long dsum, float q) {
+  const double dd = (double)dsum * kInvJScale;
+  const double qd = (double)q;
+  return (float)((ai_d * ai_d * dd - P.premul_d * qd * qd) * (1.0 / 166.0));
 }
 
 __device__ __forceinline__ void phase_chain(const PackView &v, int warp, int lane, float4 (*sA)[16],
@@ -471,23 +523,12 @@ __device__ __forceinline__ void phase_chain(const PackView &v, int warp, int lan
   float s_hi = 0.f, s_lo = 0.f, invP5 = 0.f, piP5 = 0.f, P4 = 0.f;
   double still2_d = 0.0;
   const SysParams *P = nullptr;
-  EvStage nx;
-  auto load = [&](int q, EvStage &st) {
-    const int t = v.still_list[q];
-    st.m = v.tile_meta[t];
-    st.row = tile_row(v, t, lane);
-    if (lane <= (st.m.w & 7)) {
-      const int j = st.m.x + lane;
-      st.a = v.pq[2 * (size_t)j];
-      st.b = v.pq[2 * (size_t)j + 1];
-      st.c = v.prm[j];
-    }
-  };
-  if (q0 < q1) load(q0, nx);
+  EvWalk<4> walk;
+  walk.start(v, lane, q0, q1);
   for (int q = q0; q < q1; q++) {
-    const EvStage cur = nx;
+    int te;
+    const EvStage cur = walk.next(v, lane, te);
     const TileInfo ti = tile_info(cur.m);
-    if (q + 1 < q1) load(q + 1, nx);
     if (ti.a0 != a0) {
       a0 = ti.a0;
       i = a0 + (lane < ti.na ? lane : 0);
@@ -495,7 +536,7 @@ __device__ __forceinline__ void phase_chain(const PackView &v, int warp, int lan
       ib = v.pq[2 * (size_t)i + 1];
       const float4 pi = v.prm[i];
       P = &v.sp[ti.s];
-      ic = make_float4(pi.z, pi.w, chain_weight(v, *P, i, N), 0.f);
+      ic = make_float4(pi.z, pi.w, chain_weight(*P, v.born_d[i], v.ej[(size_t)3 * N + i], ia.w), 0.f);
       s_hi = P->still2 * (1.f + 4e-6f);
       s_lo = P->still2 * (1.f - 4e-6f);
       invP5 = P->invP5;
@@ -504,14 +545,12 @@ __device__ __forceinline__ void phase_chain(const PackView &v, int warp, int lan
       still2_d = P->still2_d;
     }
     if (lane < ti.nb) {
-      const float4 c = make_float4(cur.c.z, cur.c.w, chain_weight(v, *P, ti.b0 + lane, N), 0.f);
+      const float4 c = make_float4(cur.c.z, cur.c.w, chain_weight(*P, cur.u, cur.w, cur.a.w), 0.f);
       sA[warp][lane] = sA[warp][lane + 8] = cur.a;
       sB[warp][lane] = sB[warp][lane + 8] = cur.b;
       sC[warp][lane] = sC[warp][lane + 8] = c;
     }
-    unsigned rows = cur.row;
-    if (ti.spec >= 0) rows &= ~spec_row(v, ti.spec, 0, lane);  // bond order > 2 only
-    rows = rot8(rows, a);
+    const unsigned rows = rot8(cur.row & ~cur.x0, a);  // bond order > 2 only
     __syncwarp();
     float fx = 0.f, fy = 0.f, fz = 0.f, j0 = 0.f, j1 = 0.f, j2 = 0.f;
 #pragma unroll
@@ -622,34 +661,39 @@ __device__ __forceinline__ void epilogue_energies(const PackView &v) {
 }
 
 // ============================================================= the kernel
-// PH: which phases (1 A, 2 B, 4 C); more than one needs a cooperative
-// launch.  MINB: resident blocks per SM the register allocation must allow
-// (PDGPU_EV_BLOCKS, 4 or 5, picks the build at run time; 4 by default).  tile_count[2] is the still-list length, tile_count[3] the
-// barrier / exit counter; the last block out clears both.
-template <int PH, int MINB>
-__global__ void __launch_bounds__(32 * kEvWarps, MINB) k_eval_tiles(PackView v, int zero) {
+// ph: which phases (1 A, 2 B, 4 C); more than one needs a cooperative
+// launch.  One compiled kernel serves the single launch and the three
+// one-phase launches, so both forms run the same instructions and give the
+// same bits whatever the compiler's contraction and scheduling choices.
+// MINB: resident blocks per SM the register allocation must allow
+// (PDGPU_EV_BLOCKS, 4 or 5, picks the build at run time; 4 by default).
+// tile_count[2] is the still-list length, tile_count[3] the barrier / exit
+// counter; the last block out clears both.
+template <int MINB>
+__global__ void __launch_bounds__(32 * kEvWarps, MINB) k_eval_tiles(PackView v, int zero, int ph) {
   PDGPU_DEP_ENTRY();
   if (v.flags[F_NL_OVERFLOW]) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   __shared__ float4 s0[kEvWarps][16], s1[kEvWarps][16], s2[kEvWarps][16];
+  __shared__ long long si[kEvWarps][7][32];  // phase B's i-side sums
   unsigned *ctr = reinterpret_cast<unsigned *>(&v.tile_count[3]);
   const unsigned G = gridDim.x;
   unsigned passed = 0;  // barriers this launch has crossed
-  if (PH & 1) {
+  if (ph & 1) {
     prologue_zero(v, zero);
     phase_born(v, warp, lane, s0, s1, s2);
   }
-  if ((PH & 1) && (PH & 6)) {
+  if ((ph & 1) && (ph & 6)) {
     if (!grid_barrier(ctr, G * ++passed, v.flags)) return;
   }
-  if (PH & 2) {
-    phase_pair(v, warp, lane, s0, s1, s2);
+  if (ph & 2) {
+    phase_pair(v, warp, lane, s0, s1, s2, si);
     epilogue_radii(v);
   }
-  if ((PH & 2) && (PH & 4)) {
+  if ((ph & 2) && (ph & 4)) {
     if (!grid_barrier(ctr, G * ++passed, v.flags)) return;
   }
-  if (PH & 4) {
+  if (ph & 4) {
     phase_chain(v, warp, lane, s0, s1, s2);
     epilogue_energies(v);
     // the last block out clears the still list and the counter
@@ -691,15 +735,14 @@ int eval_tiles_grid(long long tile_cap) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (ev_minb() == 4)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_eval_tiles<7, 4>, 32 * kEvWarps, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_eval_tiles<4>, 32 * kEvWarps, 0);
   else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_eval_tiles<7, 5>, 32 * kEvWarps, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_eval_tiles<5>, 32 * kEvWarps, 0);
   const long long need = (tile_cap + kEvWarps - 1) / kEvWarps;
   return (int)std::max(1LL, std::min((long long)std::max(occ, 1) * sms, need));
 }
 
-template <int PH>
-static cudaError_t launch_ev(const PackView &v, cudaStream_t st, int zero, bool coop) {
+static cudaError_t launch_ev(int ph, const PackView &v, cudaStream_t st, int zero, bool coop) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(v.ev_blocks);
   cfg.blockDim = dim3(32 * kEvWarps);
@@ -721,8 +764,8 @@ static cudaError_t launch_ev(const PackView &v, cudaStream_t st, int zero, bool 
   }
   cfg.attrs = attr;
   cfg.numAttrs = na;
-  cudaError_t e = ev_minb() == 4 ? cudaLaunchKernelEx(&cfg, k_eval_tiles<PH, 4>, v, zero)
-                                 : cudaLaunchKernelEx(&cfg, k_eval_tiles<PH, 5>, v, zero);
+  cudaError_t e = ev_minb() == 4 ? cudaLaunchKernelEx(&cfg, k_eval_tiles<4>, v, zero, ph)
+                                 : cudaLaunchKernelEx(&cfg, k_eval_tiles<5>, v, zero, ph);
   count_launch();
   return e;
 }
@@ -731,16 +774,16 @@ static cudaError_t launch_ev(const PackView &v, cudaStream_t st, int zero, bool 
 // else three launches of the same phases.
 cudaError_t launch_eval_tiles(const PackView &v, cudaStream_t st, int zero, bool coop) {
   if (!v.n_sc || v.ev_blocks <= 0) return cudaSuccess;
-  if (coop && fused_wanted()) return launch_ev<7>(v, st, zero, true);
-  cudaError_t e = launch_ev<1>(v, st, zero, false);
-  if (e == cudaSuccess) e = launch_ev<2>(v, st, 0, false);
-  if (e == cudaSuccess) e = launch_ev<4>(v, st, 0, false);
+  if (coop && fused_wanted()) return launch_ev(7, v, st, zero, true);
+  cudaError_t e = launch_ev(1, v, st, zero, false);
+  if (e == cudaSuccess) e = launch_ev(2, v, st, 0, false);
+  if (e == cudaSuccess) e = launch_ev(4, v, st, 0, false);
   return e;
 }
 
 cudaError_t launch_born_phase_only(const PackView &v, cudaStream_t st) {
   if (!v.n_sc || v.ev_blocks <= 0) return cudaSuccess;
-  return launch_ev<1>(v, st, 0, false);
+  return launch_ev(1, v, st, 0, false);
 }
 
 // Device times of the evaluation: the three phases as three launches
@@ -753,13 +796,13 @@ cudaError_t profile_eval_tiles(const PackView &v, cudaStream_t st, int reps, dou
   cudaError_t e = cudaSuccess;
   for (int it = 0; it < reps && e == cudaSuccess; it++) {
     cudaEventRecord(ev[0], st);
-    e = launch_ev<1>(v, st, ZF_PAIRS, false);
+    e = launch_ev(1, v, st, ZF_PAIRS, false);
     cudaEventRecord(ev[1], st);
-    if (e == cudaSuccess) e = launch_ev<2>(v, st, 0, false);
+    if (e == cudaSuccess) e = launch_ev(2, v, st, 0, false);
     cudaEventRecord(ev[2], st);
-    if (e == cudaSuccess) e = launch_ev<4>(v, st, 0, false);
+    if (e == cudaSuccess) e = launch_ev(4, v, st, 0, false);
     cudaEventRecord(ev[3], st);
-    if (e == cudaSuccess) e = launch_ev<7>(v, st, ZF_PAIRS, true);
+    if (e == cudaSuccess) e = launch_ev(7, v, st, ZF_PAIRS, true);
     cudaEventRecord(ev[4], st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     for (int q = 0; q < 4 && e == cudaSuccess; q++) {
