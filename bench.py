@@ -1022,7 +1022,7 @@ def main():
     path = ws.setPairPath(-2)  # the layout in use (the autotuner's choice by default)
     kms = np.zeros(3)
     A.check(A.lib().pdgpu_profile_pair_kernels(ctx.ptr, ws._sys, 20, A.dptr(kms)))
-    ems, ecnt = np.zeros(4), np.zeros(2, dtype=np.int64)
+    ems, ecnt = np.zeros(4), np.zeros(5, dtype=np.int64)
     if path == 1:  # the evaluation kernel: three phases as three launches, then one launch
         A.check(A.lib().pdgpu_profile_eval(ctx.ptr, ws._sys, 20, A.dptr(ems), ecnt.ctypes.data_as(A._I64)))
 
@@ -1144,6 +1144,7 @@ def main():
                                "chain": max(36.0 * P_B / F32, 4.0 * P_B / SFU) / tC,
                                "one_cooperative_launch": max(all_flop / F32, all_sfu / SFU) / tF},
                 "chain_phase_tiles": {"visited": int(ecnt[1]), "of": int(ecnt[0])},
+                "careful_tiles": {"born": int(ecnt[2]), "pair": int(ecnt[3]), "chain": int(ecnt[4])},
                 "three_pass_form_ms": {"born_K2": t2 * 1e3, "pair_K3": t3 * 1e3, "chain_K4": t4 * 1e3,
                                        "frac_of_roof": max(all_flop / F32, all_sfu / SFU) / (t2 + t3 + t4)},
                 "pair_kernels_frac_of_roof": max(all_flop / F32, all_sfu / SFU) / tE}

@@ -527,9 +527,12 @@ int pdgpu_profile_pair_kernels(pdgpu_ctx *ctx, int32_t sys, int32_t reps, double
  * the context stream, averaged over reps) of the evaluation kernel on the
  * cluster-pair tiles: ms[0..2] its Born-sum, GB + LJ + Coulomb and
  * chain-rule phases as three launches, ms[3] the three in one cooperative
- * launch (the form the protocols run).  counts[0] = tiles, counts[1] =
- * tiles the chain-rule phase visited (a pair inside the Still cutoff).
- * PDGPU_ERR_STATE unless the handle is on the tile layout. */
+ * launch (the form the protocols run).  counts (NULL, or 5 entries):
+ * [0] tiles, [1] tiles the chain-rule phase visited (a pair inside the
+ * Still cutoff), [2..4] tiles the Born-sum, GB + LJ + Coulomb and
+ * chain-rule phases redid in their careful form (a pair at a decision
+ * edge decided in FP64).  PDGPU_ERR_STATE unless the handle is on the tile
+ * layout. */
 int pdgpu_profile_eval(pdgpu_ctx *ctx, int32_t sys, int32_t reps, double *ms, int64_t *counts);
 /* How an evaluation on the tile layout is launched (no reference
  * counterpart): 1 = the three passes in one cooperative launch everywhere,

@@ -2183,7 +2183,17 @@ int pdgpu_profile_eval(pdgpu_ctx *c, int32_t sys, int32_t reps, double *ms, int6
     // clear the list the lone Born phase left, and the sums it added
     PDGPU_CUDA(cudaMemsetAsync(P.v.tile_count + 2, 0, 2 * sizeof(int), c->st));
     PDGPU_CUDA(cudaMemsetAsync(P.v.bsum, 0, sizeof(long long) * P.v.n_atoms, c->st));
+    // tiles each phase redid in its careful form (a pair at a decision edge)
+    int *stats = nullptr;
+    PDGPU_CUDA(cudaMallocAsync((void **)&stats, 3 * sizeof(int), c->st));
+    PDGPU_CUDA(cudaMemsetAsync(stats, 0, 3 * sizeof(int), c->st));
+    ce = count_deferred_tiles(P.v, c->st, stats);
+    int d[3] = {0, 0, 0};
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(d, stats, sizeof d, cudaMemcpyDeviceToHost, c->st);
+    cudaFreeAsync(stats, c->st);
+    if (ce != cudaSuccess) return cuda_fail(ce, "profile_eval deferred");
     if ((r = sync_check(c, "profile_eval counts"))) return r;
+    for (int k = 0; k < 3; k++) counts[2 + k] = d[k];
   }
   return PDGPU_OK;
 }

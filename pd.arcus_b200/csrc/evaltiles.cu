@@ -146,17 +146,18 @@ __device__ __forceinline__ void ev_stage(const PackView &v, int t, int lane, EvS
 template <int PH>
 struct EvWalk {
   int e, e1;
-  int t1, t2;   // tiles of items e+1 and e+2
-  int4 m1;      // metadata of item e+1
-  EvStage nx;   // stage of item e
+  int t0, t1, t2;  // tiles of items e, e+1, e+2
+  int4 m1;         // metadata of item e+1
+  EvStage nx;      // stage of item e
   __device__ __forceinline__ int tile_of(const PackView &v, int k) const {
     return PH == 4 ? v.still_list[k] : k;
   }
   __device__ __forceinline__ void start(const PackView &v, int lane, int b, int end) {
     e = b;
     e1 = end;
+    t0 = t1 = t2 = 0;
     if (e < e1) {
-      const int t0 = tile_of(v, e);
+      t0 = tile_of(v, e);
       nx.m = v.tile_meta[t0];
       ev_stage<PH>(v, t0, lane, nx);
     }
@@ -166,42 +167,169 @@ struct EvWalk {
     }
     if (e + 2 < e1) t2 = tile_of(v, e + 2);
   }
-  // the current item's stage; advances the prefetch by one item
+  // the current item's stage and tile; advances the prefetch by one item
   __device__ __forceinline__ EvStage next(const PackView &v, int lane, int &tile) {
     const EvStage cur = nx;
-    tile = PH == 4 ? -1 : e;
+    tile = t0;
     if (e + 1 < e1) {
       nx.m = m1;
       ev_stage<PH>(v, t1, lane, nx);
     }
-    if (e + 2 < e1) {
-      m1 = v.tile_meta[t2];
-      t1 = t2;
-    }
-    if (PH == 4 && e + 3 < e1) t2 = v.still_list[e + 3];
-    if (PH != 4) t2 = e + 3;
+    if (e + 2 < e1) m1 = v.tile_meta[t2];
+    t0 = t1;
+    t1 = t2;
+    if (e + 3 < e1) t2 = tile_of(v, e + 3);
     e++;
     return cur;
   }
 };
+// One tile staged on its own (the deferred tiles' second pass).
+template <int PH>
+__device__ __forceinline__ EvStage ev_stage_one(const PackView &v, int t, int lane) {
+  EvStage q;
+  q.m = v.tile_meta[t];
+  ev_stage<PH>(v, t, lane, q);
+  return q;
+}
+
+// A tile with a pair at a decision edge (the Still cutoff's, or the
+// exp-approximation range's) is not added in a phase's main loop: its index
+// goes to the warp's slots of defer_list ([first, first + n) for a warp
+// whose items start at `first`), and the warp redoes those tiles in the
+// careful form after its main loop, adding their sums then.  A tile's
+// result therefore depends on the tile alone, and the main loop carries
+// neither the FP64 decisions nor the registers they need.
+__device__ __forceinline__ void defer_tile(const PackView &v, int lane, int first, int &n, int t) {
+  if (lane == 0) v.defer_list[first + n] = t;
+  n++;
+}
 
 // ============================================================= phase A
 // Born sums.  Each term is converted to fixed point and added exactly
 // (the row and tile passes' arithmetic).  Tiles with a pair inside the
 // Still cutoff's guard band are appended to the still list in runs of up
 // to 32 (per-warp order inside a run).
+//
+// One tile's terms: the i side's sum (this lane's i atom) and the j side's
+// (lane (g,a): j atom a, this group's i atoms).  A pair in the guard band
+// of the Still cutoff is decided by its FP64 distance: the fast form
+// (CAREFUL false) leaves such pairs out and reports them in `band`, and the
+// caller then redoes the tile in the careful form, which decides them; a
+// tile's result therefore depends on the tile alone.
+// The FP64 inputs of the guard-band decisions (passed by value to the
+// careful forms, which are out of line).
+struct ExactIn {
+  const double *x, *y, *z;
+  const double *terms123;
+  const long long *bsum;
+};
+__device__ __forceinline__ ExactIn exact_in(const PackView &v) {
+  ExactIn x;
+  x.x = v.x;
+  x.y = v.y;
+  x.z = v.z;
+  x.terms123 = v.terms123;
+  x.bsum = v.bsum;
+  return x;
+}
+struct BornTileIn {
+  float4 ia, ib;
+  float Ri, Vi, s_lo, s_hi, invP5, piP5, P4s;
+  double still2_d;
+  int i, b0;
+};
+struct BornTileOut {
+  long long tile_i, jacc;
+  bool any;
+};
+template <bool CAREFUL>
+__device__ __forceinline__ BornTileOut born_tile(const ExactIn &v, const BornTileIn &q, const float4 *sA,
+                                                 const float4 *sB, const float4 *sC, unsigned rows, int a, int g8,
+                                                 bool &band) {
+  long long tile_i = 0, jacc = 0;
+  bool any = false;
+#pragma unroll(CAREFUL ? 1 : 8)
+  for (int t = 0; t < 8; t++) {
+    long long tI = 0;
+    float tJ = 0.f;  // the j side's term, made fixed point by the lane that owns j (the same bits)
+    if ((rows >> t) & 1u) {
+      const float4 ja = sA[a + t], jb = sB[a + t];
+      const Dx d = diff(q.ia, q.ib, ja, jb);
+      bool ok = d.r2 <= q.s_lo;
+      const bool edge = !ok && d.r2 <= q.s_hi;
+      if (CAREFUL) {
+        if (edge) {
+          const int j = q.b0 + ((a + t) & 7), i = q.i;
+          ok = !(ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]) > q.still2_d);
+        }
+      } else {
+        band |= edge;
+      }
+      any |= d.r2 <= q.s_hi;
+      if (ok) {
+        const float4 jc = sC[a + t];
+        const float term = born_term_noV(d, q.Ri, jc.x, q.invP5, q.piP5, q.P4s);
+        tI = __float2ll_rn(__fmul_rn(term, jc.y));
+        tJ = __fmul_rn(term, q.Vi);
+      }
+    }
+    tile_i += tI;
+    jacc += __float2ll_rn(__shfl_sync(0xffffffffu, tJ, g8 | ((a - t) & 7)));
+  }
+  BornTileOut o;
+  o.tile_i = tile_i;
+  o.jacc = jacc;
+  o.any = any;
+  return o;
+}
+// The i-side inputs of atom i of the tile's i-cluster (this lane's).
+__device__ __forceinline__ void born_i_side(const PackView &v, const TileInfo &ti, int lane, BornTileIn &q) {
+  q.i = ti.a0 + (lane < ti.na ? lane : 0);
+  q.ia = v.pq[2 * (size_t)q.i];
+  q.ib = v.pq[2 * (size_t)q.i + 1];
+  const float4 pi = v.prm[q.i];
+  q.Ri = pi.z;
+  q.Vi = pi.w;
+  const SysParams &P = v.sp[ti.s];
+  q.s_hi = P.still2 * (1.f + 4e-6f);
+  q.s_lo = P.still2 * (1.f - 4e-6f);
+  q.invP5 = P.invP5;
+  q.piP5 = P.piP5;
+  q.P4s = P.P4 * (float)kBornScale;
+  q.still2_d = P.still2_d;
+}
+// A tile's j records into this warp's slots.
+__device__ __forceinline__ void born_stage_j(const TileInfo &ti, const EvStage &cur, int lane, float4 *sA,
+                                             float4 *sB, float4 *sC) {
+  if (lane < ti.nb) {
+    sA[lane] = sA[lane + 8] = cur.a;
+    sB[lane] = sB[lane + 8] = cur.b;
+    sC[lane] = sC[lane + 8] = make_float4(cur.c.z, cur.c.w, 0.f, 0.f);
+  }
+}
+// The j side's sums of a tile over the i groups, added to the Born sums.
+__device__ __forceinline__ void born_add_j(const PackView &v, const TileInfo &ti, int lane, long long jacc) {
+  jacc += __shfl_xor_sync(0xffffffffu, jacc, 8);
+  jacc += __shfl_xor_sync(0xffffffffu, jacc, 16);
+  if (lane < ti.nb && jacc) atomicAdd((unsigned long long *)&v.bsum[ti.b0 + lane], (unsigned long long)jacc);
+}
+
 __device__ __forceinline__ void phase_born(const PackView &v, int warp, int lane, float4 (*sA)[16],
                                            float4 (*sB)[16], float4 (*sC)[16]) {
   int e, e1;
   ev_range(v.tile_count[0], warp, e, e1);
+  const int first = e;
   const int g8 = lane & ~7, a = lane & 7;
-  int a0 = -1, na = 0, i = 0;
-  float4 ia = make_float4(0, 0, 0, 0), ib = ia;
-  float Ri = 0.f, Vi = 0.f, s_hi = 0.f, s_lo = 0.f, invP5 = 0.f, piP5 = 0.f, P4s = 0.f;
-  double still2_d = 0.0;
+  int a0 = -1, na = 0, nd = 0;
+  BornTileIn q;
+  q.ia = q.ib = make_float4(0, 0, 0, 0);
+  q.Ri = q.Vi = q.s_lo = q.s_hi = q.invP5 = q.piP5 = q.P4s = 0.f;
+  q.still2_d = 0.0;
+  q.i = 0;
   long long acc_i = 0;
   unsigned near = 0;
   int run0 = e;
+  const ExactIn xin = exact_in(v);
   EvWalk<1> walk;
   walk.start(v, lane, e, e1);
   auto flush_near = [&](int upto) {
@@ -225,63 +353,46 @@ __device__ __forceinline__ void phase_born(const PackView &v, int warp, int lane
       acc_i = 0;
       a0 = ti.a0;
       na = ti.na;
-      i = a0 + (lane < na ? lane : 0);
-      ia = v.pq[2 * (size_t)i];
-      ib = v.pq[2 * (size_t)i + 1];
-      const float4 pi = v.prm[i];
-      Ri = pi.z;
-      Vi = pi.w;
-      const SysParams &P = v.sp[ti.s];
-      s_hi = P.still2 * (1.f + 4e-6f);
-      s_lo = P.still2 * (1.f - 4e-6f);
-      invP5 = P.invP5;
-      piP5 = P.piP5;
-      P4s = P.P4 * (float)kBornScale;
-      still2_d = P.still2_d;
+      born_i_side(v, ti, lane, q);
     }
-    if (lane < ti.nb) {
-      sA[warp][lane] = sA[warp][lane + 8] = cur.a;
-      sB[warp][lane] = sB[warp][lane + 8] = cur.b;
-      sC[warp][lane] = sC[warp][lane + 8] = make_float4(cur.c.z, cur.c.w, 0.f, 0.f);
-    }
+    q.b0 = ti.b0;
+    born_stage_j(ti, cur, lane, sA[warp], sB[warp], sC[warp]);
     const unsigned rows = rot8(cur.row & ~cur.x0, a);  // bond order > 2 only
     __syncwarp();
-    long long jacc = 0;  // lane (g,a): j atom a, this group's i atoms
-    bool any = false;    // a pair inside the Still cutoff's guard band
-#pragma unroll
-    for (int t = 0; t < 8; t++) {
-      long long tI = 0;
-      float tJ = 0.f;  // the j side's term, made fixed point by the lane that owns j (the same bits)
-      if ((rows >> t) & 1u) {
-        const float4 ja = sA[warp][a + t], jb = sB[warp][a + t];
-        const Dx d = diff(ia, ib, ja, jb);
-        bool ok = d.r2 <= s_lo;
-        if (!ok && d.r2 <= s_hi) {
-          const int j = ti.b0 + ((a + t) & 7);
-          ok = !(ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]) > still2_d);
-        }
-        any |= d.r2 <= s_hi;
-        if (ok) {
-          const float4 jc = sC[warp][a + t];
-          const float term = born_term_noV(d, Ri, jc.x, invP5, piP5, P4s);
-          tI = __float2ll_rn(__fmul_rn(term, jc.y));
-          tJ = __fmul_rn(term, Vi);
-        }
-      }
-      acc_i += tI;
-      jacc += __float2ll_rn(__shfl_sync(0xffffffffu, tJ, g8 | ((a - t) & 7)));
-    }
-    if (__any_sync(0xffffffffu, any)) {
-      near |= 1u << (e - run0);
-      jacc += __shfl_xor_sync(0xffffffffu, jacc, 8);
-      jacc += __shfl_xor_sync(0xffffffffu, jacc, 16);
-      if (lane < ti.nb && jacc) atomicAdd((unsigned long long *)&v.bsum[ti.b0 + lane], (unsigned long long)jacc);
+    bool band = false;  // a pair whose inclusion the FP64 distance decides
+    const BornTileOut o = born_tile<false>(xin, q, sA[warp], sB[warp], sC[warp], rows, a, g8, band);
+    // a pair inside the Still cutoff's guard band: the tile goes to the chain-rule phase
+    const bool any = __any_sync(0xffffffffu, o.any);
+    if (any) near |= 1u << (e - run0);
+    if (__any_sync(0xffffffffu, band)) {
+      defer_tile(v, lane, first, nd, e);
+    } else {
+      acc_i += o.tile_i;
+      if (any) born_add_j(v, ti, lane, o.jacc);  // no pair inside the cutoff: no j terms
     }
     if (e - run0 == 31) flush_near(e + 1);
     __syncwarp();
   }
   if (lane < na && acc_i) atomicAdd((unsigned long long *)&v.bsum[a0 + lane], (unsigned long long)acc_i);
   flush_near(e1);
+  if (v.defer_stats && lane == 0 && nd) atomicAdd(&v.defer_stats[0], nd);
+  // the deferred tiles in the careful form
+  __syncwarp();
+  for (int k = 0; k < nd; k++) {
+    const int t = v.defer_list[first + k];
+    const EvStage cur = ev_stage_one<1>(v, t, lane);
+    const TileInfo ti = tile_info(cur.m);
+    born_i_side(v, ti, lane, q);
+    q.b0 = ti.b0;
+    born_stage_j(ti, cur, lane, sA[warp], sB[warp], sC[warp]);
+    const unsigned rows = rot8(cur.row & ~cur.x0, a);
+    __syncwarp();
+    bool band = false;
+    const BornTileOut o = born_tile<true>(xin, q, sA[warp], sB[warp], sC[warp], rows, a, g8, band);
+    if (lane < ti.na && o.tile_i) atomicAdd((unsigned long long *)&v.bsum[q.i], (unsigned long long)o.tile_i);
+    born_add_j(v, ti, lane, o.jacc);
+    __syncwarp();
+  }
 }
 
 // ============================================================= phase B
@@ -292,20 +403,30 @@ __device__ __forceinline__ void phase_born(const PackView &v, int warp, int lane
 struct PairOut {
   float fscal, epol, dedal, vdw, elec;
 };
+// The exp-approximation range's edge is decided by the FP64 predicate: the
+// fast form (CAREFUL false) takes the FP32 decision and reports a pair
+// inside the edge's guard band in `band` (the caller then redoes the tile
+// in the careful form).
+template <bool CAREFUL>
 __device__ __forceinline__ PairOut pair_gb(const GbSettings &g, float r2, bool in, bool nb, bool b14, float ai,
-                                           float aj, float qiqj, float radsum, float epsij, const PackView &v,
-                                           int i, int j, double ai_d, const SysParams *P) {
+                                           float aj, float qiqj, float radsum, float epsij, const ExactIn &v,
+                                           int i, int j, double ai_d, const SysParams *P, bool &band) {
   const float invr = rsqrtf(r2);
   const float r = r2 * invr;
   const float aiaj = ai * aj;
   const float u = __fdividef(-0.25f * r2, aiaj);
   bool gb = u > g.thr;
-  if (in && fabsf(u - g.thr) <= g.band) {
-    // the FP64 predicate of gbff.cpp:1553-1575 with both radii formed
-    // from their sums (the same values the epilogue stores)
-    const double aj_d = born_radius(v, *P, j);
-    const double srij = ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]);
-    gb = -srij * 0.25 / (ai_d * aj_d) > g.thr_d;
+  const bool edge = in && fabsf(u - g.thr) <= g.band;
+  if (CAREFUL) {
+    if (edge) {
+      // the FP64 predicate of gbff.cpp:1553-1575 with both radii formed
+      // from their sums (the same values the epilogue stores)
+      const double aj_d = -P->halfeconv_d / (v.terms123[j] + (double)v.bsum[j] * kInvBornScale) + P->born_offset_d;
+      const double srij = ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]);
+      gb = -srij * 0.25 / (ai_d * aj_d) > g.thr_d;
+    }
+  } else {
+    band |= edge;
   }
   gb = gb && in;
   const float dr = r - g.rin;
@@ -393,21 +514,123 @@ struct ISide {
   }
 };
 
+// One tile's GB + LJ + Coulomb terms: the i side's sums of this lane's i
+// atom (io: force x, y, z, vdw, elec, pol, dE/da) and the j side's (jo,
+// lane (g,a): j atom a, this group's i atoms, before the sum over groups).
+struct PairTileIn {
+  float4 ia, ib, ip;
+  double ai_d;
+  int i, b0;
+};
+struct PairTileOut {
+  float io[7], jo[7];
+};
+template <bool CAREFUL>
+__device__ __forceinline__ PairTileOut pair_tile(const ExactIn &v, const GbSettings &gs, const SysParams *P,
+                                                 const PairTileIn &q, const float4 *sA, const float4 *sB,
+                                                 const float4 *sP, unsigned rows, unsigned xrows, unsigned brows,
+                                                 int a, int g8, bool &band) {
+  float io[7], jo[7];
+#pragma unroll
+  for (int k = 0; k < 7; k++) io[k] = jo[k] = 0.f;
+#pragma unroll(CAREFUL ? 1 : 8)
+  for (int t = 0; t < 8; t++) {
+    const float4 ja = sA[a + t], jb = sB[a + t], jp = sP[a + t];
+    const Dx d = diff(q.ia, q.ib, ja, jb);
+    const bool in = ((rows >> t) & 1u) && d.r2 <= gs.rc2;
+    const bool nb3 = !((xrows >> t) & 1u);
+    const bool b14 = (brows >> t) & 1u;
+    const PairOut o = pair_gb<CAREFUL>(gs, d.r2, in, nb3, b14, q.ib.w, jb.w, q.ia.w * ja.w, q.ip.x + jp.x,
+                                       q.ip.y * jp.y, v, q.i, q.b0 + ((a + t) & 7), q.ai_d, P, band);
+    io[5] += o.epol;
+    io[6] += o.dedal * jb.w;
+    io[3] += o.vdw;
+    io[4] += o.elec;
+    const float cx = o.fscal * d.x, cy = o.fscal * d.y, cz = o.fscal * d.z;
+    io[0] -= cx;
+    io[1] -= cy;
+    io[2] -= cz;
+    const float c[7] = {cx, cy, cz, o.vdw, o.elec, o.epol, o.dedal * q.ib.w};
+    const int src = g8 | ((a - t) & 7);
+#pragma unroll
+    for (int k = 0; k < 7; k++) jo[k] += __shfl_sync(0xffffffffu, c[k], src);
+  }
+  PairTileOut o;
+#pragma unroll
+  for (int k = 0; k < 7; k++) {
+    o.io[k] = io[k];
+    o.jo[k] = jo[k];
+  }
+  return o;
+}
+// The i-side inputs of this lane's atom of the tile's i-cluster.
+__device__ __forceinline__ void pair_i_side(const PackView &v, const TileInfo &ti, const SysParams *P, int lane,
+                                            PairTileIn &q) {
+  q.i = ti.a0 + (lane < ti.na ? lane : 0);
+  q.ia = v.pq[2 * (size_t)q.i];
+  q.ib = v.pq[2 * (size_t)q.i + 1];
+  q.ip = v.prm[q.i];
+  q.ai_d = born_radius(v, *P, q.i);
+  q.ib.w = (float)q.ai_d;
+}
+// A tile's j records into this warp's slots, with each j atom's Born
+// radius formed from its staged sum in FP32 (a few ulp from the FP64
+// value; decisions at the exp-approximation edge use the FP64 radii).
+__device__ __forceinline__ void pair_stage_j(const TileInfo &ti, const EvStage &cur, int lane, float hec,
+                                             float boff, float4 *sA, float4 *sB, float4 *sP) {
+  if (lane < ti.nb) {
+    float4 b = cur.b;
+    b.w = __fdividef(hec, (float)(cur.u + (double)cur.w * kInvBornScale)) + boff;
+    sA[lane] = sA[lane + 8] = cur.a;
+    sB[lane] = sB[lane + 8] = b;
+    sP[lane] = sP[lane + 8] = cur.c;
+  } else if (lane < 8) {
+    // a j-cluster shorter than 8 atoms: its empty slots hold zero records,
+    // so the masked-out terms of those slots multiply finite numbers
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    sA[lane] = sA[lane + 8] = z;
+    sB[lane] = sB[lane + 8] = z;
+    sP[lane] = sP[lane + 8] = z;
+  }
+}
+// The j side's sums of a tile over the i groups, added to the j atoms.
+__device__ __forceinline__ void pair_add_j(const PackView &v, const TileInfo &ti, int lane, float (&jacc)[7]) {
+  const int N = v.n_atoms;
+#pragma unroll
+  for (int k = 0; k < 7; k++) {
+    jacc[k] += __shfl_xor_sync(0xffffffffu, jacc[k], 8);
+    jacc[k] += __shfl_xor_sync(0xffffffffu, jacc[k], 16);
+  }
+  if (lane < ti.nb) {
+    const int j = ti.b0 + lane;
+    add_fixed(v, &v.hx[j], jacc[0], ti.s);
+    add_fixed(v, &v.hy[j], jacc[1], ti.s);
+    add_fixed(v, &v.hz[j], jacc[2], ti.s);
+#pragma unroll
+    for (int k = 0; k < 4; k++) add_fixed(v, &v.ej[(size_t)k * N + j], jacc[3 + k], ti.s);
+  }
+}
+
 __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane, float4 (*sA)[16],
                                            float4 (*sB)[16], float4 (*sP)[16], long long (*sI)[7][32]) {
   int e, e1;
   ev_range(v.tile_count[0], warp, e, e1);
+  const int first = e;
   const int N = v.n_atoms;
   const int g8 = lane & ~7, a = lane & 7;
-  int a0 = -1, i = 0, s_cur = -1, na = 0, s_i = 0;
+  int a0 = -1, s_cur = -1, na = 0, s_i = 0, nd = 0;
   ISide acc;
   acc.f = sI[warp];
   acc.lane = lane;
   acc.clear();
-  float4 ia = make_float4(0, 0, 0, 0), ib = ia, ip = ia;
-  double ai_d = 0.0;
+  PairTileIn q;
+  q.ia = q.ib = q.ip = make_float4(0, 0, 0, 0);
+  q.ai_d = 0.0;
+  q.i = 0;
   const SysParams *P = nullptr;
+  float hec = 0.f, boff = 0.f;  // -halfeconv and the Born radius offset (FP32)
   GbSettings gs;
+  const ExactIn xin = exact_in(v);
   EvWalk<2> walk;
   walk.start(v, lane, e, e1);
   for (; e < e1; e++) {
@@ -418,86 +641,60 @@ __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane
       s_cur = ti.s;
       P = &v.sp[ti.s];
       gs.load(*P);
+      hec = (float)-P->halfeconv_d;
+      boff = (float)P->born_offset_d;
     }
     if (ti.a0 != a0) {
-      if (lane < na) acc.flush(v, i, s_i, N);
+      if (lane < na) acc.flush(v, q.i, s_i, N);
       acc.clear();
       a0 = ti.a0;
       na = ti.na;
       s_i = ti.s;
-      i = a0 + (lane < ti.na ? lane : 0);
-      ia = v.pq[2 * (size_t)i];
-      ib = v.pq[2 * (size_t)i + 1];
-      ip = v.prm[i];
-      ai_d = born_radius(v, *P, i);
-      ib.w = (float)ai_d;
+      pair_i_side(v, ti, P, lane, q);
     }
-    if (lane < ti.nb) {
-      // the j atom's Born radius from its staged sum (born_radius's
-      // expression: the same bits)
-      float4 b = cur.b;
-      b.w = (float)(-P->halfeconv_d / (cur.u + (double)cur.w * kInvBornScale) + P->born_offset_d);
-      sA[warp][lane] = sA[warp][lane + 8] = cur.a;
-      sB[warp][lane] = sB[warp][lane + 8] = b;
-      sP[warp][lane] = sP[warp][lane + 8] = cur.c;
-    } else if (lane < 8) {
-      // a j-cluster shorter than 8 atoms: its empty slots hold zero records,
-      // so the masked-out terms of those slots multiply finite numbers
-      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-      sA[warp][lane] = sA[warp][lane + 8] = z;
-      sB[warp][lane] = sB[warp][lane + 8] = z;
-      sP[warp][lane] = sP[warp][lane + 8] = z;
-    }
+    q.b0 = ti.b0;
+    pair_stage_j(ti, cur, lane, hec, boff, sA[warp], sB[warp], sP[warp]);
     const unsigned rows = rot8(cur.row, a);
     const unsigned xrows = rot8(cur.x0, a), brows = rot8(cur.x1, a);  // bond order <= 2, == 3
     __syncwarp();
-    float fx = 0.f, fy = 0.f, fz = 0.f, e_vdw = 0.f, e_el = 0.f, e_pol = 0.f, deda = 0.f;
-    float jacc[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    bool band = false;
+    PairTileOut o = pair_tile<false>(xin, gs, P, q, sA[warp], sB[warp], sP[warp], rows, xrows, brows, a, g8, band);
+    if (__any_sync(0xffffffffu, band)) {
+      defer_tile(v, lane, first, nd, e);
+    } else {
+      pair_add_j(v, ti, lane, o.jo);
 #pragma unroll
-    for (int t = 0; t < 8; t++) {
-      const float4 ja = sA[warp][a + t], jb = sB[warp][a + t], jp = sP[warp][a + t];
-      const Dx d = diff(ia, ib, ja, jb);
-      const bool in = ((rows >> t) & 1u) && d.r2 <= gs.rc2;
-      const bool nb3 = !((xrows >> t) & 1u);
-      const bool b14 = (brows >> t) & 1u;
-      const PairOut o = pair_gb(gs, d.r2, in, nb3, b14, ib.w, jb.w, ia.w * ja.w, ip.x + jp.x, ip.y * jp.y, v, i,
-                                ti.b0 + ((a + t) & 7), ai_d, P);
-      e_pol += o.epol;
-      deda += o.dedal * jb.w;
-      e_vdw += o.vdw;
-      e_el += o.elec;
-      const float cx = o.fscal * d.x, cy = o.fscal * d.y, cz = o.fscal * d.z;
-      fx -= cx;
-      fy -= cy;
-      fz -= cz;
-      const float c[7] = {cx, cy, cz, o.vdw, o.elec, o.epol, o.dedal * ib.w};
-      const int src = g8 | ((a - t) & 7);
-#pragma unroll
-      for (int q = 0; q < 7; q++) jacc[q] += __shfl_sync(0xffffffffu, c[q], src);
+      for (int k = 0; k < 7; k++) acc.add(k, o.io[k]);
     }
-#pragma unroll
-    for (int q = 0; q < 7; q++) {
-      jacc[q] += __shfl_xor_sync(0xffffffffu, jacc[q], 8);
-      jacc[q] += __shfl_xor_sync(0xffffffffu, jacc[q], 16);
-    }
-    if (lane < ti.nb) {
-      const int j = ti.b0 + lane;
-      add_fixed(v, &v.hx[j], jacc[0], ti.s);
-      add_fixed(v, &v.hy[j], jacc[1], ti.s);
-      add_fixed(v, &v.hz[j], jacc[2], ti.s);
-#pragma unroll
-      for (int q = 0; q < 4; q++) add_fixed(v, &v.ej[(size_t)q * N + j], jacc[3 + q], ti.s);
-    }
-    acc.add(0, fx);
-    acc.add(1, fy);
-    acc.add(2, fz);
-    acc.add(3, e_vdw);
-    acc.add(4, e_el);
-    acc.add(5, e_pol);
-    acc.add(6, deda);
     __syncwarp();
   }
-  if (lane < na) acc.flush(v, i, s_i, N);
+  if (lane < na) acc.flush(v, q.i, s_i, N);
+  if (v.defer_stats && lane == 0 && nd) atomicAdd(&v.defer_stats[1], nd);
+  // the deferred tiles in the careful form; their i sums go to memory at once
+  __syncwarp();
+  for (int k = 0; k < nd; k++) {
+    const int t = v.defer_list[first + k];
+    const EvStage cur = ev_stage_one<2>(v, t, lane);
+    const TileInfo ti = tile_info(cur.m);
+    P = &v.sp[ti.s];
+    gs.load(*P);
+    hec = (float)-P->halfeconv_d;
+    boff = (float)P->born_offset_d;
+    pair_i_side(v, ti, P, lane, q);
+    q.b0 = ti.b0;
+    pair_stage_j(ti, cur, lane, hec, boff, sA[warp], sB[warp], sP[warp]);
+    const unsigned rows = rot8(cur.row, a);
+    const unsigned xrows = rot8(cur.x0, a), brows = rot8(cur.x1, a);
+    __syncwarp();
+    bool band = false;
+    PairTileOut o = pair_tile<true>(xin, gs, P, q, sA[warp], sB[warp], sP[warp], rows, xrows, brows, a, g8, band);
+    pair_add_j(v, ti, lane, o.jo);
+    acc.clear();
+#pragma unroll
+    for (int c = 0; c < 7; c++) acc.add(c, o.io[c]);
+    if (lane < ti.na) acc.flush(v, q.i, ti.s, N);
+    __syncwarp();
+  }
 }
 
 // ============================================================= phase C
@@ -512,89 +709,164 @@ __device__ __forceinline__ float chain_weight(const SysParams &P, double ai_d, l
   return (float)((ai_d * ai_d * dd - P.premul_d * qd * qd) * (1.0 / 166.0));
 }
 
+// One tile's chain-rule terms: the i side's force on this lane's i atom
+// (io) and the j side's (jo, lane (g,a): j atom a, this group's i atoms,
+// before the sum over groups); the Still cutoff's guard band as in phase A.
+struct ChainTileIn {
+  float4 ia, ib, ic;  // ic: R, V, the chain weight
+  float s_lo, s_hi, invP5, piP5, P4;
+  double still2_d;
+  int i, b0;
+};
+struct ChainTileOut {
+  float io[3], jo[3];
+};
+template <bool CAREFUL>
+__device__ __forceinline__ ChainTileOut chain_tile(const ExactIn &v, const ChainTileIn &q, const float4 *sA,
+                                                   const float4 *sB, const float4 *sC, unsigned rows, int a, int g8,
+                                                   bool &band) {
+  float io[3], jo[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) io[k] = jo[k] = 0.f;
+#pragma unroll(CAREFUL ? 1 : 8)
+  for (int t = 0; t < 8; t++) {
+    float c0 = 0.f, c1 = 0.f, c2 = 0.f;
+    const float4 ja = sA[a + t], jb = sB[a + t];
+    const Dx d = diff(q.ia, q.ib, ja, jb);
+    const bool row = (rows >> t) & 1u;
+    bool ok = row && d.r2 <= q.s_lo;
+    const bool edge = row && !ok && d.r2 <= q.s_hi;
+    if (CAREFUL) {
+      if (edge) {
+        const int j = q.b0 + ((a + t) & 7), i = q.i;
+        ok = !(ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]) > q.still2_d);
+      }
+    } else {
+      band |= edge;
+    }
+    if (ok) {
+      const float4 jc = sC[a + t];
+      const float tt = chain_term(d, q.ic.x, jc.x, q.ic.y, jc.y, q.ic.z, jc.z, q.invP5, q.piP5, q.P4);
+      io[0] += tt * d.x;
+      io[1] += tt * d.y;
+      io[2] += tt * d.z;
+      c0 = -tt * d.x;
+      c1 = -tt * d.y;
+      c2 = -tt * d.z;
+    }
+    const int src = g8 | ((a - t) & 7);
+    jo[0] += __shfl_sync(0xffffffffu, c0, src);
+    jo[1] += __shfl_sync(0xffffffffu, c1, src);
+    jo[2] += __shfl_sync(0xffffffffu, c2, src);
+  }
+  ChainTileOut o;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    o.io[k] = io[k];
+    o.jo[k] = jo[k];
+  }
+  return o;
+}
+// The i-side inputs of this lane's atom of the tile's i-cluster.
+__device__ __forceinline__ const SysParams *chain_i_side(const PackView &v, const TileInfo &ti, int lane,
+                                                         ChainTileIn &q) {
+  const int N = v.n_atoms;
+  q.i = ti.a0 + (lane < ti.na ? lane : 0);
+  q.ia = v.pq[2 * (size_t)q.i];
+  q.ib = v.pq[2 * (size_t)q.i + 1];
+  const float4 pi = v.prm[q.i];
+  const SysParams *P = &v.sp[ti.s];
+  q.ic = make_float4(pi.z, pi.w, chain_weight(*P, v.born_d[q.i], v.ej[(size_t)3 * N + q.i], q.ia.w), 0.f);
+  q.s_hi = P->still2 * (1.f + 4e-6f);
+  q.s_lo = P->still2 * (1.f - 4e-6f);
+  q.invP5 = P->invP5;
+  q.piP5 = P->piP5;
+  q.P4 = P->P4;
+  q.still2_d = P->still2_d;
+  return P;
+}
+// A tile's j records (with each j atom's chain weight) into this warp's slots.
+__device__ __forceinline__ void chain_stage_j(const TileInfo &ti, const EvStage &cur, const SysParams *P, int lane,
+                                              float4 *sA, float4 *sB, float4 *sC) {
+  if (lane < ti.nb) {
+    const float4 c = make_float4(cur.c.z, cur.c.w, chain_weight(*P, cur.u, cur.w, cur.a.w), 0.f);
+    sA[lane] = sA[lane + 8] = cur.a;
+    sB[lane] = sB[lane + 8] = cur.b;
+    sC[lane] = sC[lane + 8] = c;
+  }
+}
+// A tile's forces: the j side summed over the i groups, and the i side.
+__device__ __forceinline__ void chain_add(const PackView &v, const TileInfo &ti, int lane, int i,
+                                          const ChainTileOut &o) {
+  float jo[3] = {o.jo[0], o.jo[1], o.jo[2]};
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    jo[c] += __shfl_xor_sync(0xffffffffu, jo[c], 8);
+    jo[c] += __shfl_xor_sync(0xffffffffu, jo[c], 16);
+  }
+  if (lane < ti.nb) {
+    const int j = ti.b0 + lane;
+    add_fixed(v, &v.hx[j], jo[0], ti.s);
+    add_fixed(v, &v.hy[j], jo[1], ti.s);
+    add_fixed(v, &v.hz[j], jo[2], ti.s);
+  }
+  if (lane < ti.na) {
+    add_fixed(v, &v.hx[i], o.io[0], ti.s);
+    add_fixed(v, &v.hy[i], o.io[1], ti.s);
+    add_fixed(v, &v.hz[i], o.io[2], ti.s);
+  }
+}
+
 __device__ __forceinline__ void phase_chain(const PackView &v, int warp, int lane, float4 (*sA)[16],
                                             float4 (*sB)[16], float4 (*sC)[16]) {
   int q0, q1;
   ev_range(v.tile_count[2], warp, q0, q1);
-  const int N = v.n_atoms;
   const int g8 = lane & ~7, a = lane & 7;
-  int a0 = -1, i = 0;
-  float4 ia = make_float4(0, 0, 0, 0), ib = ia, ic = ia;
-  float s_hi = 0.f, s_lo = 0.f, invP5 = 0.f, piP5 = 0.f, P4 = 0.f;
-  double still2_d = 0.0;
+  int a0 = -1, nd = 0;
+  ChainTileIn q;
+  q.ia = q.ib = q.ic = make_float4(0, 0, 0, 0);
+  q.s_hi = q.s_lo = q.invP5 = q.piP5 = q.P4 = 0.f;
+  q.still2_d = 0.0;
+  q.i = 0;
   const SysParams *P = nullptr;
+  const ExactIn xin = exact_in(v);
   EvWalk<4> walk;
   walk.start(v, lane, q0, q1);
-  for (int q = q0; q < q1; q++) {
-    int te;
-    const EvStage cur = walk.next(v, lane, te);
+  for (int k = q0; k < q1; k++) {
+    int t;
+    const EvStage cur = walk.next(v, lane, t);
     const TileInfo ti = tile_info(cur.m);
     if (ti.a0 != a0) {
       a0 = ti.a0;
-      i = a0 + (lane < ti.na ? lane : 0);
-      ia = v.pq[2 * (size_t)i];
-      ib = v.pq[2 * (size_t)i + 1];
-      const float4 pi = v.prm[i];
-      P = &v.sp[ti.s];
-      ic = make_float4(pi.z, pi.w, chain_weight(*P, v.born_d[i], v.ej[(size_t)3 * N + i], ia.w), 0.f);
-      s_hi = P->still2 * (1.f + 4e-6f);
-      s_lo = P->still2 * (1.f - 4e-6f);
-      invP5 = P->invP5;
-      piP5 = P->piP5;
-      P4 = P->P4;
-      still2_d = P->still2_d;
+      P = chain_i_side(v, ti, lane, q);
     }
-    if (lane < ti.nb) {
-      const float4 c = make_float4(cur.c.z, cur.c.w, chain_weight(*P, cur.u, cur.w, cur.a.w), 0.f);
-      sA[warp][lane] = sA[warp][lane + 8] = cur.a;
-      sB[warp][lane] = sB[warp][lane + 8] = cur.b;
-      sC[warp][lane] = sC[warp][lane + 8] = c;
-    }
+    q.b0 = ti.b0;
+    chain_stage_j(ti, cur, P, lane, sA[warp], sB[warp], sC[warp]);
     const unsigned rows = rot8(cur.row & ~cur.x0, a);  // bond order > 2 only
     __syncwarp();
-    float fx = 0.f, fy = 0.f, fz = 0.f, j0 = 0.f, j1 = 0.f, j2 = 0.f;
-#pragma unroll
-    for (int t = 0; t < 8; t++) {
-      float c0 = 0.f, c1 = 0.f, c2 = 0.f;
-      const float4 ja = sA[warp][a + t], jb = sB[warp][a + t];
-      const Dx d = diff(ia, ib, ja, jb);
-      bool ok = ((rows >> t) & 1u) && d.r2 <= s_lo;
-      if (((rows >> t) & 1u) && !ok && d.r2 <= s_hi) {
-        const int j = ti.b0 + ((a + t) & 7);
-        ok = !(ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]) > still2_d);
-      }
-      if (ok) {
-        const float4 jc = sC[warp][a + t];
-        const float tt = chain_term(d, ic.x, jc.x, ic.y, jc.y, ic.z, jc.z, invP5, piP5, P4);
-        fx += tt * d.x;
-        fy += tt * d.y;
-        fz += tt * d.z;
-        c0 = -tt * d.x;
-        c1 = -tt * d.y;
-        c2 = -tt * d.z;
-      }
-      const int src = g8 | ((a - t) & 7);
-      j0 += __shfl_sync(0xffffffffu, c0, src);
-      j1 += __shfl_sync(0xffffffffu, c1, src);
-      j2 += __shfl_sync(0xffffffffu, c2, src);
-    }
-    j0 += __shfl_xor_sync(0xffffffffu, j0, 8);
-    j1 += __shfl_xor_sync(0xffffffffu, j1, 8);
-    j2 += __shfl_xor_sync(0xffffffffu, j2, 8);
-    j0 += __shfl_xor_sync(0xffffffffu, j0, 16);
-    j1 += __shfl_xor_sync(0xffffffffu, j1, 16);
-    j2 += __shfl_xor_sync(0xffffffffu, j2, 16);
-    if (lane < ti.nb) {
-      const int j = ti.b0 + lane;
-      add_fixed(v, &v.hx[j], j0, ti.s);
-      add_fixed(v, &v.hy[j], j1, ti.s);
-      add_fixed(v, &v.hz[j], j2, ti.s);
-    }
-    if (lane < ti.na) {
-      add_fixed(v, &v.hx[i], fx, ti.s);
-      add_fixed(v, &v.hy[i], fy, ti.s);
-      add_fixed(v, &v.hz[i], fz, ti.s);
-    }
+    bool band = false;
+    const ChainTileOut o = chain_tile<false>(xin, q, sA[warp], sB[warp], sC[warp], rows, a, g8, band);
+    if (__any_sync(0xffffffffu, band))
+      defer_tile(v, lane, q0, nd, t);
+    else
+      chain_add(v, ti, lane, q.i, o);
+    __syncwarp();
+  }
+  if (v.defer_stats && lane == 0 && nd) atomicAdd(&v.defer_stats[2], nd);
+  // the deferred tiles in the careful form
+  __syncwarp();
+  for (int k = 0; k < nd; k++) {
+    const int t = v.defer_list[q0 + k];
+    const EvStage cur = ev_stage_one<4>(v, t, lane);
+    const TileInfo ti = tile_info(cur.m);
+    P = chain_i_side(v, ti, lane, q);
+    q.b0 = ti.b0;
+    chain_stage_j(ti, cur, P, lane, sA[warp], sB[warp], sC[warp]);
+    const unsigned rows = rot8(cur.row & ~cur.x0, a);
+    __syncwarp();
+    bool band = false;
+    const ChainTileOut o = chain_tile<true>(xin, q, sA[warp], sB[warp], sC[warp], rows, a, g8, band);
+    chain_add(v, ti, lane, q.i, o);
     __syncwarp();
   }
 }
@@ -784,6 +1056,16 @@ cudaError_t launch_eval_tiles(const PackView &v, cudaStream_t st, int zero, bool
 cudaError_t launch_born_phase_only(const PackView &v, cudaStream_t st) {
   if (!v.n_sc || v.ev_blocks <= 0) return cudaSuccess;
   return launch_ev(1, v, st, 0, false);
+}
+
+// One evaluation (three launches) that counts the tiles each phase
+// deferred to its careful form into stats[0..2] (device memory, zeroed by
+// the caller).
+cudaError_t count_deferred_tiles(const PackView &v, cudaStream_t st, int *stats) {
+  if (!v.n_sc || v.ev_blocks <= 0) return cudaSuccess;
+  PackView w = v;
+  w.defer_stats = stats;
+  return launch_eval_tiles(w, st, ZF_PAIRS, false);
 }
 
 // Device times of the evaluation: the three phases as three launches

@@ -217,6 +217,8 @@ struct PackView {
   long long tile_cap, spec_cap;
   int tile_blocks[3];         // resident blocks of the three tile passes (persistent grids)
   int *still_list;            // [tile_cap] tiles with a pair inside the Still cutoff (evaluation kernel)
+  int *defer_list;            // [tile_cap] tiles a warp redoes in the careful form (evaluation kernel)
+  int *defer_stats;           // [3] deferred tiles per phase, counted when set (profiling only)
   int ev_blocks;              // grid of the evaluation kernel (its resident blocks)
   long long *bsum;            // [N] Born sums of the tile pass, fixed point 2^40
   long long *hx, *hy, *hz;    // [N] pair forces of the tile passes, fixed point 2^24 kcal/mol/A
@@ -396,6 +398,8 @@ int eval_tiles_grid(long long tile_cap);
 cudaError_t profile_eval_tiles(const PackView &v, cudaStream_t st, int reps, double *ms);
 // the Born-sum phase alone (it fills the still list; instrumentation)
 cudaError_t launch_born_phase_only(const PackView &v, cudaStream_t st);
+// one evaluation counting the tiles each phase redid in its careful form
+cudaError_t count_deferred_tiles(const PackView &v, cudaStream_t st, int *stats);
 // explicit lanes-per-atom variants (4, 8, 16, 32), used by the autotuner
 void launch_born_radii_lpa(const PackView &v, cudaStream_t st, int zero, int lpa);
 void launch_gb_pair_lpa(const PackView &v, cudaStream_t st, int lpa);

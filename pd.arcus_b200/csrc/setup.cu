@@ -250,7 +250,8 @@ int pack_ensure_tiles(Pack *p) {
       palloc(p, &v.spec_rows, 16 * (size_t)v.spec_cap) != cudaSuccess ||
       palloc(p, &v.cbox, 6 * (size_t)v.n_jc) != cudaSuccess ||
       palloc(p, &v.xs, 3 * (size_t)v.n_atoms) != cudaSuccess ||
-      palloc(p, &v.still_list, (size_t)v.tile_cap) != cudaSuccess) {
+      palloc(p, &v.still_list, (size_t)v.tile_cap) != cudaSuccess ||
+      palloc(p, &v.defer_list, (size_t)v.tile_cap) != cudaSuccess) {
     set_error("device allocation failed (cluster-pair tiles)");
     return PDGPU_ERR_NOMEM;
   }
