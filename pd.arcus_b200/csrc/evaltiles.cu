@@ -242,6 +242,20 @@ struct BornTileOut {
   long long tile_i, jacc;
   bool any;
 };
+// born_term_noV's value with every step taken on every lane and the
+// results selected (the same bits; no divergent branches, so the eight
+// steps of a tile interleave).
+__device__ __forceinline__ float born_term_sel(const Dx &d, float Ri, float Rj, float invP5, float piP5,
+                                               float P4scaled) {
+  const float Rs = __fadd_rn(Ri, Rj);
+  const float ir2 = __fdividef(1.f, d.r2);
+  const float term = __fmul_rn(__fmul_rn(P4scaled, ir2), ir2);
+  const float rdivR = __fdividef(d.r2, __fmul_rn(Rs, Rs));
+  const float sh = __sinf(__fmul_rn(__fmul_rn(0.5f, piP5), rdivR));
+  const float c = __fmul_rn(sh, sh);
+  const float tc = __fmul_rn(term, __fmul_rn(c, c));
+  return rdivR > invP5 ? term : tc;
+}
 template <bool CAREFUL>
 __device__ __forceinline__ BornTileOut born_tile(const ExactIn &v, const BornTileIn &q, const float4 *sA,
                                                  const float4 *sB, const float4 *sC, unsigned rows, int a, int g8,
@@ -250,30 +264,24 @@ __device__ __forceinline__ BornTileOut born_tile(const ExactIn &v, const BornTil
   bool any = false;
 #pragma unroll(CAREFUL ? 1 : 8)
   for (int t = 0; t < 8; t++) {
-    long long tI = 0;
-    float tJ = 0.f;  // the j side's term, made fixed point by the lane that owns j (the same bits)
-    if ((rows >> t) & 1u) {
-      const float4 ja = sA[a + t], jb = sB[a + t];
-      const Dx d = diff(q.ia, q.ib, ja, jb);
-      bool ok = d.r2 <= q.s_lo;
-      const bool edge = !ok && d.r2 <= q.s_hi;
-      if (CAREFUL) {
-        if (edge) {
-          const int j = q.b0 + ((a + t) & 7), i = q.i;
-          ok = !(ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]) > q.still2_d);
-        }
-      } else {
-        band |= edge;
+    const bool row = (rows >> t) & 1u;
+    const float4 ja = sA[a + t], jb = sB[a + t], jc = sC[a + t];
+    const Dx d = diff(q.ia, q.ib, ja, jb);
+    bool ok = row && d.r2 <= q.s_lo;
+    const bool edge = row && !(d.r2 <= q.s_lo) && d.r2 <= q.s_hi;
+    if (CAREFUL) {
+      if (edge) {
+        const int j = q.b0 + ((a + t) & 7), i = q.i;
+        ok = !(ref_d2(v.x[i], v.y[i], v.z[i], v.x[j], v.y[j], v.z[j]) > q.still2_d);
       }
-      any |= d.r2 <= q.s_hi;
-      if (ok) {
-        const float4 jc = sC[a + t];
-        const float term = born_term_noV(d, q.Ri, jc.x, q.invP5, q.piP5, q.P4s);
-        tI = __float2ll_rn(__fmul_rn(term, jc.y));
-        tJ = __fmul_rn(term, q.Vi);
-      }
+    } else {
+      band |= edge;
     }
-    tile_i += tI;
+    any |= row && d.r2 <= q.s_hi;
+    const float term = born_term_sel(d, q.Ri, jc.x, q.invP5, q.piP5, q.P4s);
+    // the j side's term is made fixed point by the lane that owns j (the same bits)
+    const float tJ = ok ? __fmul_rn(term, q.Vi) : 0.f;
+    tile_i += __float2ll_rn(ok ? __fmul_rn(term, jc.y) : 0.f);
     jacc += __float2ll_rn(__shfl_sync(0xffffffffu, tJ, g8 | ((a - t) & 7)));
   }
   BornTileOut o;
@@ -721,6 +729,22 @@ struct ChainTileIn {
 struct ChainTileOut {
   float io[3], jo[3];
 };
+// chain_term's value with every step taken on every lane and the results
+// selected (no divergent branches, so the eight steps of a tile interleave).
+__device__ __forceinline__ float chain_term_sel(const Dx &d, float Ri, float Rj, float Vi, float Vj, float wi,
+                                                float wj, float invP5, float piP5, float P4) {
+  const float Rs = Ri + Rj;
+  const float rdivR = __fdividef(d.r2, Rs * Rs);
+  const float th = rdivR * piP5;
+  float sn, cs;
+  __sincosf(th, &sn, &cs);
+  const float sq = 0.5f - 0.5f * cs;
+  const float Xc = 4.f * sq * sq - 2.f * sq * sn * th;
+  const float X = rdivR > invP5 ? 4.f : Xc;
+  const float ir2 = __fdividef(1.f, d.r2);  // the fast reciprocal: deterministic, ~1 ulp
+  const float ir6 = ir2 * ir2 * ir2;
+  return P4 * X * ir6 * (wi * Vj + wj * Vi);
+}
 template <bool CAREFUL>
 __device__ __forceinline__ ChainTileOut chain_tile(const ExactIn &v, const ChainTileIn &q, const float4 *sA,
                                                    const float4 *sB, const float4 *sC, unsigned rows, int a, int g8,
@@ -730,8 +754,7 @@ __device__ __forceinline__ ChainTileOut chain_tile(const ExactIn &v, const Chain
   for (int k = 0; k < 3; k++) io[k] = jo[k] = 0.f;
 #pragma unroll(CAREFUL ? 1 : 8)
   for (int t = 0; t < 8; t++) {
-    float c0 = 0.f, c1 = 0.f, c2 = 0.f;
-    const float4 ja = sA[a + t], jb = sB[a + t];
+    const float4 ja = sA[a + t], jb = sB[a + t], jc = sC[a + t];
     const Dx d = diff(q.ia, q.ib, ja, jb);
     const bool row = (rows >> t) & 1u;
     bool ok = row && d.r2 <= q.s_lo;
@@ -744,20 +767,17 @@ __device__ __forceinline__ ChainTileOut chain_tile(const ExactIn &v, const Chain
     } else {
       band |= edge;
     }
-    if (ok) {
-      const float4 jc = sC[a + t];
-      const float tt = chain_term(d, q.ic.x, jc.x, q.ic.y, jc.y, q.ic.z, jc.z, q.invP5, q.piP5, q.P4);
-      io[0] += tt * d.x;
-      io[1] += tt * d.y;
-      io[2] += tt * d.z;
-      c0 = -tt * d.x;
-      c1 = -tt * d.y;
-      c2 = -tt * d.z;
-    }
+    // selected, not multiplied by zero: a lane without a pair may hold a
+    // stale j slot of any value
+    const float tt = chain_term_sel(d, q.ic.x, jc.x, q.ic.y, jc.y, q.ic.z, jc.z, q.invP5, q.piP5, q.P4);
+    const float cx = ok ? tt * d.x : 0.f, cy = ok ? tt * d.y : 0.f, cz = ok ? tt * d.z : 0.f;
+    io[0] += cx;
+    io[1] += cy;
+    io[2] += cz;
     const int src = g8 | ((a - t) & 7);
-    jo[0] += __shfl_sync(0xffffffffu, c0, src);
-    jo[1] += __shfl_sync(0xffffffffu, c1, src);
-    jo[2] += __shfl_sync(0xffffffffu, c2, src);
+    jo[0] += __shfl_sync(0xffffffffu, -cx, src);
+    jo[1] += __shfl_sync(0xffffffffu, -cy, src);
+    jo[2] += __shfl_sync(0xffffffffu, -cz, src);
   }
   ChainTileOut o;
 #pragma unroll
