@@ -58,6 +58,13 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(x) : "l"(p) : "memory");
   return x;
 }
+// The wait of a programmatic dependent launch: every earlier kernel of the
+// stream has completed and its memory is visible; then the next kernel may
+// be scheduled (PDGPU_DEP_ENTRY's two steps, after a launch's static loads).
+__device__ __forceinline__ void griddep_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 // Grid barrier over a counter that counts arrivals; every block waits for
 // `target` arrivals.  False when the wait ran out (the flag is set).
 __device__ __forceinline__ bool grid_barrier(unsigned *ctr, unsigned target, int *flags) {
@@ -116,9 +123,12 @@ struct EvStage {
   double u;              // phase B: terms123[j]; phase C: born_d[j]
   long long w;           // phase B: bsum[j]; phase C: the dE/da sum of j
 };
-// PH: the phase (1 A, 2 B, 4 C) the stage is for.
+// PH: the phase (1 A, 2 B, 4 C) the stage is for.  The static part reads
+// only what the list build and the integrator wrote (the tile records,
+// coordinates, per-atom parameters); the dynamic part what the evaluation's
+// earlier phases wrote (the Born sums; the Born radii and dE/da sums).
 template <int PH>
-__device__ __forceinline__ void ev_stage(const PackView &v, int t, int lane, EvStage &q) {
+__device__ __forceinline__ void ev_stage_static(const PackView &v, int t, int lane, EvStage &q) {
   q.row = tile_row(v, t, lane);
   q.x0 = q.x1 = 0;
   if (q.m.y >= 0) {
@@ -130,19 +140,31 @@ __device__ __forceinline__ void ev_stage(const PackView &v, int t, int lane, EvS
     q.a = v.pq[2 * (size_t)j];
     q.b = v.pq[2 * (size_t)j + 1];
     q.c = v.prm[j];
-    if (PH == 2) {
-      q.u = v.terms123[j];
-      q.w = v.bsum[j];
-    }
+    if (PH == 2) q.u = v.terms123[j];
+  }
+}
+template <int PH>
+__device__ __forceinline__ void ev_stage_dyn(const PackView &v, int lane, EvStage &q) {
+  if (lane <= (q.m.w & 7)) {
+    const int j = q.m.x + lane;
+    if (PH == 2) q.w = v.bsum[j];
     if (PH == 4) {
       q.u = v.born_d[j];
       q.w = v.ej[(size_t)3 * v.n_atoms + j];
     }
   }
 }
+template <int PH>
+__device__ __forceinline__ void ev_stage(const PackView &v, int t, int lane, EvStage &q) {
+  ev_stage_static<PH>(v, t, lane, q);
+  ev_stage_dyn<PH>(v, lane, q);
+}
 // Walks a warp's tiles [e, e1) (PH 1, 2) or still-list entries (PH 4) with
 // the two-deep prefetch: next() returns the stage of the current tile and
-// its index, and issues the loads for the tiles after it.
+// its index, and issues the loads for the tiles after it.  start() is in
+// two parts: the static loads of the first items (which a launch may issue
+// before the earlier phases of its evaluation are done), then the dynamic
+// part of the first item's stage.
 template <int PH>
 struct EvWalk {
   int e, e1;
@@ -152,20 +174,27 @@ struct EvWalk {
   __device__ __forceinline__ int tile_of(const PackView &v, int k) const {
     return PH == 4 ? v.still_list[k] : k;
   }
-  __device__ __forceinline__ void start(const PackView &v, int lane, int b, int end) {
+  __device__ __forceinline__ void start_static(const PackView &v, int lane, int b, int end) {
     e = b;
     e1 = end;
     t0 = t1 = t2 = 0;
     if (e < e1) {
       t0 = tile_of(v, e);
       nx.m = v.tile_meta[t0];
-      ev_stage<PH>(v, t0, lane, nx);
+      ev_stage_static<PH>(v, t0, lane, nx);
     }
     if (e + 1 < e1) {
       t1 = tile_of(v, e + 1);
       m1 = v.tile_meta[t1];
     }
     if (e + 2 < e1) t2 = tile_of(v, e + 2);
+  }
+  __device__ __forceinline__ void start_dyn(const PackView &v, int lane) {
+    if (e < e1) ev_stage_dyn<PH>(v, lane, nx);
+  }
+  __device__ __forceinline__ void start(const PackView &v, int lane, int b, int end) {
+    start_static(v, lane, b, end);
+    start_dyn(v, lane);
   }
   // the current item's stage and tile; advances the prefetch by one item
   __device__ __forceinline__ EvStage next(const PackView &v, int lane, int &tile) {
@@ -620,7 +649,8 @@ __device__ __forceinline__ void pair_add_j(const PackView &v, const TileInfo &ti
 }
 
 __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane, float4 (*sA)[16],
-                                           float4 (*sB)[16], float4 (*sP)[16], long long (*sI)[7][32]) {
+                                           float4 (*sB)[16], float4 (*sP)[16], long long (*sI)[7][32],
+                                           bool early) {
   int e, e1;
   ev_range(v.tile_count[0], warp, e, e1);
   const int first = e;
@@ -640,7 +670,9 @@ __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane
   GbSettings gs;
   const ExactIn xin = exact_in(v);
   EvWalk<2> walk;
-  walk.start(v, lane, e, e1);
+  walk.start_static(v, lane, e, e1);
+  if (early) griddep_wait();
+  walk.start_dyn(v, lane);
   for (; e < e1; e++) {
     int te;
     const EvStage cur = walk.next(v, lane, te);
@@ -838,7 +870,7 @@ __device__ __forceinline__ void chain_add(const PackView &v, const TileInfo &ti,
 }
 
 __device__ __forceinline__ void phase_chain(const PackView &v, int warp, int lane, float4 (*sA)[16],
-                                            float4 (*sB)[16], float4 (*sC)[16]) {
+                                            float4 (*sB)[16], float4 (*sC)[16], bool early) {
   int q0, q1;
   ev_range(v.tile_count[2], warp, q0, q1);
   const int g8 = lane & ~7, a = lane & 7;
@@ -851,7 +883,9 @@ __device__ __forceinline__ void phase_chain(const PackView &v, int warp, int lan
   const SysParams *P = nullptr;
   const ExactIn xin = exact_in(v);
   EvWalk<4> walk;
-  walk.start(v, lane, q0, q1);
+  walk.start_static(v, lane, q0, q1);
+  if (early) griddep_wait();
+  walk.start_dyn(v, lane);
   for (int k = q0; k < q1; k++) {
     int t;
     const EvStage cur = walk.next(v, lane, t);
@@ -963,7 +997,11 @@ __device__ __forceinline__ void epilogue_energies(const PackView &v) {
 // counter; the last block out clears both.
 template <int MINB>
 __global__ void __launch_bounds__(32 * kEvWarps, MINB) k_eval_tiles(PackView v, int zero, int ph) {
-  PDGPU_DEP_ENTRY();
+  // a launch of phase B or C alone follows the launch of the phase before
+  // it: it stages its first tiles while that one still runs, and waits for
+  // it (griddep_wait) before it reads anything the evaluation writes
+  const bool early = ph == 2 || ph == 4;
+  if (!early) PDGPU_DEP_ENTRY();
   if (v.flags[F_NL_OVERFLOW]) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   __shared__ float4 s0[kEvWarps][16], s1[kEvWarps][16], s2[kEvWarps][16];
@@ -979,14 +1017,14 @@ __global__ void __launch_bounds__(32 * kEvWarps, MINB) k_eval_tiles(PackView v, 
     if (!grid_barrier(ctr, G * ++passed, v.flags)) return;
   }
   if (ph & 2) {
-    phase_pair(v, warp, lane, s0, s1, s2, si);
+    phase_pair(v, warp, lane, s0, s1, s2, si, early);
     epilogue_radii(v);
   }
   if ((ph & 2) && (ph & 4)) {
     if (!grid_barrier(ctr, G * ++passed, v.flags)) return;
   }
   if (ph & 4) {
-    phase_chain(v, warp, lane, s0, s1, s2);
+    phase_chain(v, warp, lane, s0, s1, s2, early);
     epilogue_energies(v);
     // the last block out clears the still list and the counter
     __syncthreads();
