@@ -549,8 +549,8 @@ def compose(parts, spacing=25.0):
     return res
 
 
-def bench_serving(pdgpu, A, ctx, torch, n_requests=300, rate=200.0, budget=120e9, max_active=32, seed=5,
-                  policy=1, tiles=True):
+def bench_serving(pdgpu, A, ctx, torch, n_requests=300, rate=200.0, budget=120e9, max_active=16, seed=5,
+                  policy=1, tiles=True, batch_ms=60):
     lib = load_library(LIB_SP)
     meta = lib[0][1]
     rng = np.random.default_rng(seed)
@@ -604,7 +604,7 @@ def bench_serving(pdgpu, A, ctx, torch, n_requests=300, rate=200.0, budget=120e9
     L = A.lib()
     # served: submit at the arrival times, the worker overlaps the jobs
     srv = pdgpu.Server(ctx, hbm_budget=budget, max_active=max_active, lanes=(8, 8, 8), tiles=tiles,
-                       policy=policy)
+                       policy=policy, batch_ms=batch_ms)
     lc0 = L_count(L, ctx)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -660,7 +660,8 @@ def bench_serving(pdgpu, A, ctx, torch, n_requests=300, rate=200.0, budget=120e9
                                  "latency_ms": {"p50": pctl(plat, 50), "p99": pctl(plat, 99)}},
             "speedup_jobs_per_s_vs_plain": (n_requests / makespan) / (n_requests / plain_makespan),
             "system_atoms": {"min": int(sizes.min()), "max": int(sizes.max()), "templates": n_tmpl},
-            "hbm_budget_bytes": int(budget), "max_active": max_active, "peak_active": st["peak_active"],
+            "hbm_budget_bytes": int(budget), "max_active": max_active, "batch_window_ms": batch_ms,
+            "groups": st["groups"], "peak_active": st["peak_active"],
             "admission": "least work first" if policy == 1 else "arrival order",
             "pair_path": "tiles" if tiles else "rows (8 lanes per atom)",
             "device_max_connections": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS"),
@@ -956,7 +957,9 @@ def main():
     ap.add_argument("--batched-md-steps", type=int, default=5000)
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--serve-policy", type=int, default=1, help="0 arrival order, 1 least work first")
-    ap.add_argument("--serve-max-active", type=int, default=32)
+    ap.add_argument("--serve-max-active", type=int, default=16)
+    ap.add_argument("--serve-batch-ms", type=int, default=60,
+                    help="queue time a minimisation / MD job waits for like jobs to share its pack")
     ap.add_argument("--serve-rows", action="store_true", help="serve on the list-row pair passes")
     args = ap.parse_args()
     rank, world, local = rank_info()
@@ -1182,7 +1185,7 @@ def main():
         line["batched_md"] = bench_batched_md(pdgpu, A, ctx, torch, steps=args.batched_md_steps)
         line["serving"] = bench_serving(pdgpu, A, ctx, torch, n_requests=args.serve_requests,
                                         policy=args.serve_policy, max_active=args.serve_max_active,
-                                        tiles=not args.serve_rows)
+                                        tiles=not args.serve_rows, batch_ms=args.serve_batch_ms)
     if rank == 0 and n_gpus == 1 and not args.no_cpu_baseline:
         try:
             cb = run_reference(args, 1)

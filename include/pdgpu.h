@@ -446,9 +446,14 @@ typedef struct {
   int32_t tiles;        /* 1: cluster-pair tile passes, 0: list-row passes    */
   int32_t policy;       /* admission order: 0 arrival, 1 least work first     */
   int32_t group;        /* 1: single-point jobs queued together, and
-                           minimisation jobs with the same settings, are
-                           admitted as one batch (one pack, one launch
-                           sequence; tile layout only); 0: one job each   */
+                           minimisation or MD jobs with the same settings
+                           (an MD member keeps its own seed), are admitted
+                           as one batch (one pack, one launch sequence;
+                           tile layout only); 0: one job each             */
+  int32_t batch_ms;     /* with group: a minimisation or MD job waits in the
+                           queue up to this long (ms) for like jobs to
+                           arrive and share its pack; 0: admitted as soon
+                           as a slot is free                               */
 } pdgpu_serve_params;
 void pdgpu_serve_params_default(pdgpu_serve_params *p);
 

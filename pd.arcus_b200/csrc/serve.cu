@@ -118,8 +118,8 @@ struct Job {
   int regrow = 0;
   MDCoef k;
   unsigned char *min_host = nullptr;  // minimiser state read-back (inside pin)
-  // a group: single-point or minimisation jobs admitted together share one
-  // device pack (a batch, one launch sequence for all of them).  The
+  // a group: single-point, minimisation or MD jobs admitted together share
+  // one device pack (a batch, one launch sequence for all of them).  The
   // leader owns the pack, the stream slot and the phases; `group` lists
   // every member in pack order (the leader first), empty for a lone job.
   std::vector<Job *> group;
@@ -314,6 +314,9 @@ void pdgpu_server::enqueue_md_block(Job *j) {
   j->block = block;
   j->pin->step = j->md_done;
   cudaMemsetAsync(v.flags + F_NL_OVERFLOW, 0, sizeof(int), j->st);
+  // a group goes on past a member's NaN energy (the member is marked failed
+  // from its energy history at the end)
+  if (!j->group.empty()) cudaMemsetAsync(v.flags + F_NAN, 0, sizeof(int), j->st);
   cudaMemcpyAsync(e->step_dev, &j->pin->step, sizeof(int), cudaMemcpyHostToDevice, j->st);
   if (use_graph) {
     if (!e->gexec || e->gkey != "md") {
@@ -370,25 +373,37 @@ void pdgpu_server::enqueue_results(Job *j) {
     cudaMemcpyAsync(r + 10 * n, v.hy + o, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
     cudaMemcpyAsync(r + 11 * n, v.hz + o, sizeof(long long) * n, cudaMemcpyDeviceToHost, j->st);
     cudaMemcpyAsync(r + 12 * n, v.ene + s * E_COUNT, sizeof(double) * E_COUNT, cudaMemcpyDeviceToHost, j->st);
-    if (m->spec.kind == PDGPU_JOB_MD && j->md_done > 0)
-      cudaMemcpyAsync(r + 12 * n + E_COUNT, j->e->hist, sizeof(double) * 3 * (size_t)j->md_done,
-                      cudaMemcpyDeviceToHost, j->st);
+    if (m->spec.kind == PDGPU_JOB_MD && j->md_done > 0)  // member s of the [step][member][3] history
+      cudaMemcpy2DAsync(r + 12 * n + E_COUNT, sizeof(double) * 3, j->e->hist + 3 * s,
+                        sizeof(double) * 3 * members.size(), sizeof(double) * 3, (size_t)j->md_done,
+                        cudaMemcpyDeviceToHost, j->st);
     m->have_results = true;
   }
   record(j, PH_FINISH);
 }
 
-// Queued jobs that can share a pack with j: the same kind (single point,
-// or minimisation with the same settings and step count), the same
-// surface-term cadence, on the tile layout within the tile search's size
-// limit, fitting the budget; at most kGroupMax jobs and kGroupAtoms atoms.
-// A member's results do not depend on the others (the tile passes and the
-// minimiser are per system), so grouping changes no result.
+// MD settings that must agree for jobs to share a pack (the seed is per
+// system: each member keeps its own random stream)
+static bool same_md(const pdgpu_job &a, const pdgpu_job &b) {
+  const pdgpu_md_params &p = a.md, &q = b.md;
+  return a.steps == b.steps && a.init_temp == b.init_temp && p.Integrator == q.Integrator &&
+         p.UpdateNList == q.UpdateNList && p.LangevinOnHydrogens == q.LangevinOnHydrogens &&
+         p.UseGraph == q.UseGraph && p.Timestep == q.Timestep && p.FricCoeff == q.FricCoeff &&
+         p.TargetTemp == q.TargetTemp;
+}
+
+// Queued jobs that can share a pack with j: the same kind (single point;
+// minimisation with the same settings and step count; MD with the same
+// settings, step count and start temperature), the same surface-term
+// cadence, on the tile layout within the tile search's size limit, fitting
+// the budget; at most kGroupMax jobs and kGroupAtoms atoms.  A member's
+// results do not depend on the others (the tile passes, the minimiser and
+// the integrator with its per-system random stream are per system), so
+// grouping changes no result.
 std::vector<Job *> pdgpu_server::group_with(Job *j) {
   std::vector<Job *> more;
   const int kind = j->spec.kind;
-  if (!prm.tiles || (kind != PDGPU_JOB_ENERGY && kind != PDGPU_JOB_MINIMISE) || j->natoms > kTileSearchMaxAtoms)
-    return more;
+  if (!prm.tiles || j->natoms > kTileSearchMaxAtoms) return more;
   long long atoms = j->natoms;
   int64_t bytes = bytes_in_use + j->est_bytes;
   for (Job *c : queue) {
@@ -399,6 +414,7 @@ std::vector<Job *> pdgpu_server::group_with(Job *j) {
     if (kind == PDGPU_JOB_MINIMISE &&
         (c->spec.steps != j->spec.steps || std::memcmp(&c->spec.min, &j->spec.min, sizeof j->spec.min) != 0))
       continue;
+    if (kind == PDGPU_JOB_MD && !same_md(c->spec, j->spec)) continue;
     if (atoms + c->natoms > kGroupAtoms || bytes + c->est_bytes > prm.hbm_budget) continue;
     atoms += c->natoms;
     bytes += c->est_bytes;
@@ -504,15 +520,26 @@ void pdgpu_server::admit(Job *j, const std::vector<Job *> &more) {
     cudaMemcpyAsync(P.v.oz, P.v.z, sizeof(double) * n, cudaMemcpyDeviceToDevice, j->st);
     enqueue_size(j, PH_MIN);
   } else if (j->spec.kind == PDGPU_JOB_MD) {
-    if (xalloc(e, &e->hist, (size_t)3 * j->spec.steps) != cudaSuccess) {
+    // history [step][member][3]
+    if (xalloc(e, &e->hist, (size_t)3 * j->spec.steps * S) != cudaSuccess) {
       fail(j, PDGPU_ERR_NOMEM, "device allocation failed (MD history)");
       return;
     }
     e->hist_cap = j->spec.steps;
     j->pin->step = 0;
-    unsigned long long seed = j->spec.md.Seed;
-    std::memcpy(&j->pin->total, &seed, sizeof seed);  // staged through the pinned block
-    cudaMemcpyAsync(e->seeds, &j->pin->total, sizeof seed, cudaMemcpyHostToDevice, j->st);
+    // every member's seed, staged through the pinned block (the minimiser
+    // state's room, which an MD job does not use)
+    static_assert(sizeof(unsigned long long) <= 8, "seed size");
+    unsigned long long *seeds = reinterpret_cast<unsigned long long *>(j->min_host);
+    if (min_state_size() < sizeof(unsigned long long)) {
+      fail(j, PDGPU_ERR_STATE, "pinned staging too small for the MD seeds");
+      return;
+    }
+    for (int q = 0; q < S; q++) {
+      const unsigned long long seed = members[q]->spec.md.Seed;
+      std::memcpy(seeds + q, &seed, sizeof seed);
+    }
+    cudaMemcpyAsync(e->seeds, seeds, sizeof(unsigned long long) * S, cudaMemcpyHostToDevice, j->st);
     launch_vel_init_impl(P.v, j->st, j->spec.init_temp, e->seeds);
     j->k = md_coef(&j->spec.md, 0, j->spec.steps);
     enqueue_size(j, PH_MD);
@@ -612,7 +639,7 @@ void pdgpu_server::advance(Job *j) {
         fail(j, PDGPU_ERR_STATE, kLcpoCandMsg);
         return;
       }
-      if (j->pin->flags[F_NAN]) {
+      if (j->pin->flags[F_NAN] && j->group.empty()) {
         j->steps_done = j->md_done;
         fail(j, PDGPU_ERR_UNSTABLE, "Simulation unstable or division by zero (NaN energy)");
         return;
@@ -631,6 +658,22 @@ void pdgpu_server::advance(Job *j) {
       if (j->spec.kind == PDGPU_JOB_ENERGY) {
         j->steps_done = 1;
         for (Job *x : j->group) x->steps_done = 1;
+      }
+      if (j->spec.kind == PDGPU_JOB_MD && !j->group.empty()) {
+        // a member whose energy went NaN failed at that step, as alone
+        // (md.cpp's run_core stops at an unstable step)
+        for (Job *x : j->group) {
+          const double *h = x->res + 12 * (size_t)x->natoms + E_COUNT;
+          int bad = -1;
+          for (int k = 0; k < j->md_done && bad < 0; k++)
+            if (!(h[3 * k] == h[3 * k])) bad = k;
+          x->steps_done = bad < 0 ? j->md_done : bad;
+          if (bad >= 0) {
+            x->member_failed = true;
+            x->status = PDGPU_ERR_UNSTABLE;
+            x->error = "Simulation unstable or division by zero (NaN energy)";
+          }
+        }
       }
       j->phase = PH_DONE;
       return;
@@ -737,6 +780,8 @@ void pdgpu_server::run() {
         if (bytes_in_use + c->est_bytes > prm.hbm_budget) continue;
         if (free_slots.empty() && c->spec.kind != PDGPU_JOB_ENERGY) continue;  // only short slots left
         double waited = ms_between(c->t_submit, now);
+        // a minimisation or MD job waits for like jobs to share its pack
+        if (prm.group && c->spec.kind != PDGPU_JOB_ENERGY && waited < prm.batch_ms) continue;
         double key = (prm.policy == 0 || waited > kAgeMs)
                          ? -1e30 + (double)q
                          : (double)c->natoms * (double)std::max(1, c->spec.steps);
@@ -777,11 +822,12 @@ extern "C" {
 void pdgpu_serve_params_default(pdgpu_serve_params *p) {
   std::memset(p, 0, sizeof *p);
   p->hbm_budget = 120LL * 1000 * 1000 * 1000;
-  p->max_active = 32;
+  p->max_active = 16;
   p->lanes[0] = p->lanes[1] = p->lanes[2] = 8;
   p->tiles = 1;   // tile passes; rebuilds by tile search, no list (systems within the search limit)
   p->policy = 1;  // least work first: short jobs do not queue behind long MD runs
-  p->group = 1;   // queued single-point / like minimisation jobs share a pack
+  p->group = 1;   // queued single-point / like minimisation / like MD jobs share a pack
+  p->batch_ms = 60;  // like minimisation / MD jobs gather into groups (a few % of an MD job's run)
 }
 
 int pdgpu_serve_create(pdgpu_ctx *ctx, const pdgpu_serve_params *p, pdgpu_server **out) {

@@ -74,7 +74,8 @@ MC_LAST, MC_LAST_ACC, MC_LOWEST_EPOT = 0, 1, 2
 
 class ServeParams(ctypes.Structure):
     _fields_ = [("hbm_budget", ctypes.c_int64), ("max_active", ctypes.c_int32), ("lanes", ctypes.c_int32 * 3),
-                ("tiles", ctypes.c_int32), ("policy", ctypes.c_int32), ("group", ctypes.c_int32)]
+                ("tiles", ctypes.c_int32), ("policy", ctypes.c_int32), ("group", ctypes.c_int32),
+                ("batch_ms", ctypes.c_int32)]
 
 
 class Job(ctypes.Structure):

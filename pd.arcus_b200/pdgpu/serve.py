@@ -21,7 +21,8 @@ class Server:
 
     ARRIVAL, LEAST_WORK = 0, 1
 
-    def __init__(self, ctx, hbm_budget=None, max_active=None, lanes=(8, 8, 8), tiles=True, policy=1, group=True):
+    def __init__(self, ctx, hbm_budget=None, max_active=None, lanes=(8, 8, 8), tiles=True, policy=1, group=True,
+                 batch_ms=None):
         self.ctx = ctx
         p = A.ServeParams()
         A.lib().pdgpu_serve_params_default(ctypes.byref(p))
@@ -34,6 +35,8 @@ class Server:
         p.tiles = int(bool(tiles))
         p.policy = int(policy)
         p.group = int(bool(group))
+        if batch_ms is not None:
+            p.batch_ms = int(batch_ms)
         self.params = p
         self.ptr = ctypes.c_void_p()
         A.check(A.lib().pdgpu_serve_create(ctx.ptr, ctypes.byref(p), ctypes.byref(self.ptr)))

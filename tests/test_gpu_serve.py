@@ -174,20 +174,34 @@ def test_serve_failed_job_does_not_disturb_others(gpu_ctx):
     srv.close()
 
 
-@pytest.mark.parametrize("kind", ["energy", "minimise"])
+def _md_job(pdgpu, seed, steps=30):
+    md = pdgpu.md_params_default()
+    md.Integrator = pdgpu.MolecularDynamics.Langevin
+    md.FricCoeff = 1e12
+    md.UpdateNList = 10
+    md.Seed = seed
+    return pdgpu.Server.job(pdgpu.Server.MD, steps, md=md)
+
+
+@pytest.mark.parametrize("kind", ["energy", "minimise", "md"])
 def test_serve_group_equals_alone(gpu_ctx, kind):
     """Jobs that queue behind a busy slot are admitted as one group (one
     pack, one launch sequence); each member's results are the bits it gets
-    served alone."""
+    served alone (MD members each with their own seed)."""
     import pdgpu
     members = _members(gpu_ctx, 8)
     S = pdgpu.Server
     mn = pdgpu.min_params_default()
     mn.Algorithm = pdgpu.Minimisation.SteepestDescent
-    job = (lambda: S.job(S.ENERGY)) if kind == "energy" else (lambda: S.job(S.MINIMISE, 40, minimiser=mn))
+    if kind == "energy":
+        jobs = lambda: [S.job(S.ENERGY) for _ in members]
+    elif kind == "minimise":
+        jobs = lambda: [S.job(S.MINIMISE, 40, minimiser=mn) for _ in members]
+    else:
+        jobs = lambda: [_md_job(pdgpu, 100 + k) for k in range(len(members))]
     srv = pdgpu.Server(gpu_ctx, max_active=1, lanes=LANES, tiles=True)
-    alone, _ = _run(srv, members, [job() for _ in members], together=False)
-    grouped, infos = _run(srv, members, [job() for _ in members], together=True)
+    alone, _ = _run(srv, members, jobs(), together=False)
+    grouped, infos = _run(srv, members, jobs(), together=True)
     st = srv.stats()
     srv.close()
     assert st["groups"] >= 1  # the queued jobs shared a pack
@@ -196,5 +210,33 @@ def test_serve_group_equals_alone(gpu_ctx, kind):
             assert np.array_equal(a[key], g[key]), key
         if kind == "energy":
             assert rel_rms(g["forces"], arr["f_total"]) <= 1e-5
+    for ws, *_ in members:
+        ws.close()
+
+
+def test_serve_md_group_member_nan(gpu_ctx):
+    """An MD group goes on past a member whose energy turns NaN: that member
+    fails (UNSTABLE), the others give the bits they get served alone."""
+    import pdgpu
+    members = _members(gpu_ctx, 4)
+    srv = pdgpu.Server(gpu_ctx, max_active=1, lanes=LANES, tiles=True)
+    alone, _ = _run(srv, members[1:], [_md_job(pdgpu, 200 + k) for k in range(1, 4)], together=False)
+    # a busy slot first, so the four queue and are admitted together
+    blocker = srv.submit(members[0][0], _md_job(pdgpu, 7, steps=60))
+    bad_pos = members[0][0].cur.p.copy()
+    bad_pos[5] = np.nan
+    bad = srv.submit(members[0][0], _md_job(pdgpu, 200), positions=bad_pos)
+    ok = [srv.submit(ws, _md_job(pdgpu, 200 + k)) for k, (ws, *_) in enumerate(members[1:], start=1)]
+    assert srv.wait(blocker, 120.0) == 0
+    assert srv.wait(bad, 120.0) == pdgpu._abi.ERR_UNSTABLE
+    assert srv.info(bad)["state"] == 3
+    for jid, a in zip(ok, alone):
+        assert srv.wait(jid, 120.0) == 0
+        got = srv.result(jid)
+        for key in a:
+            assert np.array_equal(a[key], got[key]), key
+    st = srv.stats()
+    srv.close()
+    assert st["groups"] >= 1
     for ws, *_ in members:
         ws.close()
