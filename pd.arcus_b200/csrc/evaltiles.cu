@@ -611,13 +611,18 @@ __device__ __forceinline__ void pair_i_side(const PackView &v, const TileInfo &t
   q.ib.w = (float)q.ai_d;
 }
 // A tile's j records into this warp's slots, with each j atom's Born
-// radius formed from its staged sum in FP32 (a few ulp from the FP64
-// value; decisions at the exp-approximation edge use the FP64 radii).
-__device__ __forceinline__ void pair_stage_j(const TileInfo &ti, const EvStage &cur, int lane, float hec,
-                                             float boff, float4 *sA, float4 *sB, float4 *sP) {
+// radius formed from its staged sum: -halfeconv / G + offset with 1/G from
+// the FP32 reciprocal and one Newton step in FP64 (about 48 bits, so the
+// FP32 radius is born_radius's rounded in all but tie cases; decisions at
+// the exp-approximation edge use the FP64 radii themselves).
+__device__ __forceinline__ void pair_stage_j(const TileInfo &ti, const EvStage &cur, int lane, double hec,
+                                             double boff, float4 *sA, float4 *sB, float4 *sP) {
   if (lane < ti.nb) {
     float4 b = cur.b;
-    b.w = __fdividef(hec, (float)(cur.u + (double)cur.w * kInvBornScale)) + boff;
+    const double G = cur.u + (double)cur.w * kInvBornScale;
+    const double r0 = (double)__frcp_rn((float)G);
+    const double r1 = fma(r0, fma(-G, r0, 1.0), r0);
+    b.w = (float)fma(hec, r1, boff);
     sA[lane] = sA[lane + 8] = cur.a;
     sB[lane] = sB[lane + 8] = b;
     sP[lane] = sP[lane + 8] = cur.c;
@@ -666,7 +671,7 @@ __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane
   q.ai_d = 0.0;
   q.i = 0;
   const SysParams *P = nullptr;
-  float hec = 0.f, boff = 0.f;  // -halfeconv and the Born radius offset (FP32)
+  double hec = 0.0, boff = 0.0;  // -halfeconv and the Born radius offset
   GbSettings gs;
   const ExactIn xin = exact_in(v);
   EvWalk<2> walk;
@@ -681,8 +686,8 @@ __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane
       s_cur = ti.s;
       P = &v.sp[ti.s];
       gs.load(*P);
-      hec = (float)-P->halfeconv_d;
-      boff = (float)P->born_offset_d;
+      hec = -P->halfeconv_d;
+      boff = P->born_offset_d;
     }
     if (ti.a0 != a0) {
       if (lane < na) acc.flush(v, q.i, s_i, N);
@@ -718,8 +723,8 @@ __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane
     const TileInfo ti = tile_info(cur.m);
     P = &v.sp[ti.s];
     gs.load(*P);
-    hec = (float)-P->halfeconv_d;
-    boff = (float)P->born_offset_d;
+    hec = -P->halfeconv_d;
+    boff = P->born_offset_d;
     pair_i_side(v, ti, P, lane, q);
     q.b0 = ti.b0;
     pair_stage_j(ti, cur, lane, hec, boff, sA[warp], sB[warp], sP[warp]);

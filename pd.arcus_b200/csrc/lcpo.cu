@@ -180,7 +180,11 @@ __global__ void __launch_bounds__(kLcpoWarps * 32) k_lcpo_eval(PackView v, StepS
   const int i = lc.atoms[w];
   const size_t N = (size_t)v.n_atoms;
   if (!EO && !lcpo_due(lc, ss, v.sys_of[i])) {
+    // the held step: the energy and forces of the last full evaluation
+    // (lcpo.cpp:641-659 adds SASA * sigma and SASAderiv again), written
+    // afresh so that a zeroed record (WorkSpace::zeroForces) holds them too
     if (lane == 0) {
+      v.e_atom[AE_SURF * N + i] = lc.sasa[i] * lc.sigma[i];
       const double dx = lc.deriv[i], dy = lc.deriv[N + i], dz = lc.deriv[2 * N + i];
       if (dx != 0.0 || dy != 0.0 || dz != 0.0) lcpo_add_force(v, i, dx, dy, dz);
     }
