@@ -444,7 +444,11 @@ struct PairOut {
 // fast form (CAREFUL false) takes the FP32 decision and reports a pair
 // inside the edge's guard band in `band` (the caller then redoes the tile
 // in the careful form).
-template <bool CAREFUL>
+// LEAN: every system of the pack runs FastMode and switches LJ with the
+// GB/Coulomb switch (the same parameters, so the same values): the slow
+// branch and the second switch are left out.  Both builds give the same
+// bits for such a system.
+template <bool CAREFUL, bool LEAN>
 __device__ __forceinline__ PairOut pair_gb(const GbSettings &g, float r2, bool in, bool nb, bool b14, float ai,
                                            float aj, float qiqj, float radsum, float epsij, const ExactIn &v,
                                            int i, int j, double ai_d, const SysParams *P, bool &band) {
@@ -482,14 +486,14 @@ __device__ __forceinline__ PairOut pair_gb(const GbSettings &g, float r2, bool i
     epol = epol0 * S;
     dedr = S * dedr0 + dSdd * epol0;
     dedal = dedal0 * S;
-  } else if (g.slow && in) {
+  } else if (!LEAN && g.slow && in) {
     // FastMode off (calcBornForces, gbff.cpp:1292-1324): the GB term's
     // t = 0 limit q_i q_j / r beyond the exp-approximation range
     const float epol0 = g.premul * qiqj * invr;
     epol = epol0 * S;
     dedr = S * (-epol0 * invr) + dSdd * epol0;
   }
-  nb = nb && !g.slow;  // FastMode off: the vacuum terms come from FF_NonBonded::calcForces
+  if (!LEAN) nb = nb && !g.slow;  // FastMode off: the vacuum terms come from FF_NonBonded::calcForces
   const float ec = (gb ? g.econv_in : g.econv_out) * (b14 ? g.elec14 : 1.f) * qiqj * invr;
   const float elf = S * (-ec * invr) + ec * dSdd;
   // Lennard-Jones 12-6 with its own switch
@@ -500,11 +504,14 @@ __device__ __forceinline__ PairOut pair_gb(const GbSettings &g, float r2, bool i
   const float eps = epsij * (b14 ? g.vdw14 : 1.0f);
   float vdw = (2.f * eps) * (0.5f * A - B);
   float vdwf = -(12.f * eps * invr) * (A - B);
-  const float vd = r - g.vdw_rin;
-  const float vs = 1.f - g.vdw_inv_sw2 * vd * vd;
-  const bool von = r > g.vdw_rin;
-  const float vS = von ? vs * vs : 1.f;
-  const float vdS = von ? -4.f * g.vdw_inv_sw2 * vd * vs : 0.f;
+  float vS = S, vdS = dSdd;
+  if (!LEAN) {
+    const float vd = r - g.vdw_rin;
+    const float vs = 1.f - g.vdw_inv_sw2 * vd * vd;
+    const bool von = r > g.vdw_rin;
+    vS = von ? vs * vs : 1.f;
+    vdS = von ? -4.f * g.vdw_inv_sw2 * vd * vs : 0.f;
+  }
   vdwf = vS * vdwf + vdw * vdS;
   vdw *= vS;
   const bool lj = in && nb && r < g.vdw_rc;
@@ -562,7 +569,7 @@ struct PairTileIn {
 struct PairTileOut {
   float io[7], jo[7];
 };
-template <bool CAREFUL>
+template <bool CAREFUL, bool LEAN>
 __device__ __forceinline__ PairTileOut pair_tile(const ExactIn &v, const GbSettings &gs, const SysParams *P,
                                                  const PairTileIn &q, const float4 *sA, const float4 *sB,
                                                  const float4 *sP, unsigned rows, unsigned xrows, unsigned brows,
@@ -577,7 +584,7 @@ __device__ __forceinline__ PairTileOut pair_tile(const ExactIn &v, const GbSetti
     const bool in = ((rows >> t) & 1u) && d.r2 <= gs.rc2;
     const bool nb3 = !((xrows >> t) & 1u);
     const bool b14 = (brows >> t) & 1u;
-    const PairOut o = pair_gb<CAREFUL>(gs, d.r2, in, nb3, b14, q.ib.w, jb.w, q.ia.w * ja.w, q.ip.x + jp.x,
+    const PairOut o = pair_gb<CAREFUL, LEAN>(gs, d.r2, in, nb3, b14, q.ib.w, jb.w, q.ia.w * ja.w, q.ip.x + jp.x,
                                        q.ip.y * jp.y, v, q.i, q.b0 + ((a + t) & 7), q.ai_d, P, band);
     io[5] += o.epol;
     io[6] += o.dedal * jb.w;
@@ -653,6 +660,7 @@ __device__ __forceinline__ void pair_add_j(const PackView &v, const TileInfo &ti
   }
 }
 
+template <bool LEAN>
 __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane, float4 (*sA)[16],
                                            float4 (*sB)[16], float4 (*sP)[16], long long (*sI)[7][32],
                                            bool early) {
@@ -703,7 +711,7 @@ __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane
     const unsigned xrows = rot8(cur.x0, a), brows = rot8(cur.x1, a);  // bond order <= 2, == 3
     __syncwarp();
     bool band = false;
-    PairTileOut o = pair_tile<false>(xin, gs, P, q, sA[warp], sB[warp], sP[warp], rows, xrows, brows, a, g8, band);
+    PairTileOut o = pair_tile<false, LEAN>(xin, gs, P, q, sA[warp], sB[warp], sP[warp], rows, xrows, brows, a, g8, band);
     if (__any_sync(0xffffffffu, band)) {
       defer_tile(v, lane, first, nd, e);
     } else {
@@ -732,7 +740,7 @@ __device__ __forceinline__ void phase_pair(const PackView &v, int warp, int lane
     const unsigned xrows = rot8(cur.x0, a), brows = rot8(cur.x1, a);
     __syncwarp();
     bool band = false;
-    PairTileOut o = pair_tile<true>(xin, gs, P, q, sA[warp], sB[warp], sP[warp], rows, xrows, brows, a, g8, band);
+    PairTileOut o = pair_tile<true, LEAN>(xin, gs, P, q, sA[warp], sB[warp], sP[warp], rows, xrows, brows, a, g8, band);
     pair_add_j(v, ti, lane, o.jo);
     acc.clear();
 #pragma unroll
@@ -1000,7 +1008,7 @@ __device__ __forceinline__ void epilogue_energies(const PackView &v) {
 // (PDGPU_EV_BLOCKS, 4 or 5, picks the build at run time; 4 by default).
 // tile_count[2] is the still-list length, tile_count[3] the barrier / exit
 // counter; the last block out clears both.
-template <int MINB>
+template <int MINB, bool LEAN>
 __global__ void __launch_bounds__(32 * kEvWarps, MINB) k_eval_tiles(PackView v, int zero, int ph) {
   // a launch of phase B or C alone follows the launch of the phase before
   // it: it stages its first tiles while that one still runs, and waits for
@@ -1022,7 +1030,7 @@ __global__ void __launch_bounds__(32 * kEvWarps, MINB) k_eval_tiles(PackView v, 
     if (!grid_barrier(ctr, G * ++passed, v.flags)) return;
   }
   if (ph & 2) {
-    phase_pair(v, warp, lane, s0, s1, s2, si, early);
+    phase_pair<LEAN>(v, warp, lane, s0, s1, s2, si, early);
     epilogue_radii(v);
   }
   if ((ph & 2) && (ph & 4)) {
@@ -1054,6 +1062,17 @@ static int fused_wanted() {
   return w;
 }
 
+// PDGPU_EV_LEAN=0 runs the general build for every pack (the lean build
+// gives the same bits where it applies; tested)
+static int lean_allowed() {
+  static int w = -1;
+  if (w < 0) {
+    const char *s = getenv("PDGPU_EV_LEAN");
+    w = (s && s[0] == '0') ? 0 : 1;
+  }
+  return w;
+}
+
 static int ev_minb() {
   static int m = 0;
   if (!m) {
@@ -1070,9 +1089,9 @@ int eval_tiles_grid(long long tile_cap) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (ev_minb() == 4)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_eval_tiles<4>, 32 * kEvWarps, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_eval_tiles<4, false>, 32 * kEvWarps, 0);
   else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_eval_tiles<5>, 32 * kEvWarps, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_eval_tiles<5, false>, 32 * kEvWarps, 0);
   const long long need = (tile_cap + kEvWarps - 1) / kEvWarps;
   return (int)std::max(1LL, std::min((long long)std::max(occ, 1) * sms, need));
 }
@@ -1099,8 +1118,14 @@ static cudaError_t launch_ev(int ph, const PackView &v, cudaStream_t st, int zer
   }
   cfg.attrs = attr;
   cfg.numAttrs = na;
-  cudaError_t e = ev_minb() == 4 ? cudaLaunchKernelEx(&cfg, k_eval_tiles<4>, v, zero, ph)
-                                 : cudaLaunchKernelEx(&cfg, k_eval_tiles<5>, v, zero, ph);
+  cudaError_t e;
+  const bool lean = v.ev_lean && lean_allowed();
+  if (ev_minb() == 4)
+    e = lean ? cudaLaunchKernelEx(&cfg, k_eval_tiles<4, true>, v, zero, ph)
+                  : cudaLaunchKernelEx(&cfg, k_eval_tiles<4, false>, v, zero, ph);
+  else
+    e = lean ? cudaLaunchKernelEx(&cfg, k_eval_tiles<5, true>, v, zero, ph)
+                  : cudaLaunchKernelEx(&cfg, k_eval_tiles<5, false>, v, zero, ph);
   count_launch();
   return e;
 }

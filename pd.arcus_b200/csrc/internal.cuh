@@ -220,6 +220,7 @@ struct PackView {
   int *defer_list;            // [tile_cap] tiles a warp redoes in the careful form (evaluation kernel)
   int *defer_stats;           // [3] deferred tiles per phase, counted when set (profiling only)
   int ev_blocks;              // grid of the evaluation kernel (its resident blocks)
+  int ev_lean;                // every system FastMode with one switch for LJ and GB/Coulomb
   long long *bsum;            // [N] Born sums of the tile pass, fixed point 2^40
   long long *hx, *hy, *hz;    // [N] pair forces of the tile passes, fixed point 2^24 kcal/mol/A
   long long *ej;              // [4*N] LJ, Coulomb, GB energies and dE/da of the tile pass, fixed point 2^24

@@ -344,8 +344,17 @@ int pack_ensure_stage(Pack *p) {
   return PDGPU_OK;
 }
 
+// The evaluation kernel's lean build serves a pack whose systems all run
+// FastMode with the LJ switch equal to the GB/Coulomb one.
+static void pack_update_lean(Pack *p) {
+  p->v.ev_lean = 1;
+  for (const SysParams &q : p->sp)
+    if (q.fast_mode == 0 || q.vdw_rin != q.rin || q.vdw_inv_sw2 != q.inv_sw2) p->v.ev_lean = 0;
+}
+
 void pack_set_params(Pack *p, int s, const pdgpu_ff_params &prm) {
   p->sp[s] = make_sys_params(prm);
+  pack_update_lean(p);
 }
 
 #define PALLOC(ptr, n)                                        \
@@ -579,6 +588,7 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   v.atom_off = atom_off_d;
   v.sys_of = sys_of_d;
   v.sp = sp_d;
+  pack_update_lean(p);
   v.mid = mid_d;
   v.band_off = band_off_d;
   v.band = band_d;

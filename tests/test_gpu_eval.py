@@ -134,3 +134,39 @@ def test_md_one_launch_equals_three(gpu_ctx):
     for q in range(3):
         assert np.array_equal(out[0][q], out[1][q])
         assert np.array_equal(out[0][q], out[2][q])
+
+
+_LEAN_SCRIPT = r"""
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1]); sys.path.insert(0, sys.argv[2])
+import pdgpu
+from conftest import build_workspace, load_fixture
+ctx = pdgpu.Context(0)
+arrays, meta = load_fixture("c1_pep64_s0")
+ws, ff = build_workspace(arrays, meta, ctx)
+ws.setPairPath(1)
+ws.nlist().calcNewList()
+ff.calcForces()
+np.save(sys.argv[3], ws.cur.f)
+"""
+
+
+def test_lean_build_equals_general(gpu_ctx, tmp_path):
+    """The evaluation kernel's lean build (FastMode, one switch for LJ and
+    GB/Coulomb) gives the general build's bits: the general build runs in a
+    child process (PDGPU_EV_LEAN=0)."""
+    import os
+    import subprocess
+    import sys
+    from conftest import ROOT
+    arrays, meta = load_fixture("c1_pep64_s0")
+    ws, ff = build_workspace(arrays, meta, gpu_ctx)
+    ws.setPairPath(1)
+    ws.nlist().calcNewList()
+    ff.calcForces()
+    out = str(tmp_path / "f_general.npy")
+    env = dict(os.environ, PDGPU_EV_LEAN="0")
+    subprocess.run([sys.executable, "-c", _LEAN_SCRIPT, os.path.join(ROOT, "pd.arcus_b200"),
+                    os.path.join(ROOT, "tests"), out], env=env, check=True, timeout=300)
+    assert np.array_equal(np.load(out), ws.cur.f)
+    ws.close()
