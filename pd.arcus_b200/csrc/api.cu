@@ -1,5 +1,6 @@
 // C ABI of libpdgpu (declared in include/pdgpu.h) and the protocol runners.
 #include <algorithm>
+#include <functional>
 #include <limits>
 #include <cmath>
 #include <cstring>
@@ -418,6 +419,7 @@ int pdgpu_batch_create(pdgpu_ctx *c, const int32_t *sys_ids, int32_t nsys, int32
   PDGPU_CUDA(cudaMemcpyAsync(e->seeds, keys.data(), sizeof(unsigned long long) * nsys, cudaMemcpyHostToDevice,
                              c->st));
   e->custom_seeds = false;
+  e->seeds_default = false;
   launch_pack_positions(B.v, c->st);
   r = sync_check(c, "batch_create");
   if (r) return r;
@@ -439,6 +441,7 @@ int pdgpu_batch_info(pdgpu_ctx *c, int32_t batch, int32_t *nsys, int32_t *atom_o
 int pdgpu_set_seeds(pdgpu_ctx *c, int32_t sys, const uint64_t *seeds) {
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
+  e->seeds_default = false;
   if (!seeds) {
     e->custom_seeds = false;
     return PDGPU_OK;
@@ -1393,11 +1396,13 @@ int pdgpu_calc_forces(pdgpu_ctx *c, int32_t sys) {
 // ------------------------------------------------------------ MD
 // RNG keys: those given to pdgpu_set_seeds, else base + s for system s
 static int default_seeds(pdgpu_ctx *c, SysEntry *e, unsigned long long base) {
-  if (e->custom_seeds) return PDGPU_OK;
+  if (e->custom_seeds || (e->seeds_default && e->seeds_base == base)) return PDGPU_OK;
   std::vector<unsigned long long> k(e->nsys());
   for (int s = 0; s < e->nsys(); s++) k[s] = base + (unsigned long long)s;
   PDGPU_CUDA(cudaMemcpyAsync(e->seeds, k.data(), sizeof(unsigned long long) * k.size(), cudaMemcpyHostToDevice,
                              c->st));
+  e->seeds_default = true;
+  e->seeds_base = base;
   return PDGPU_OK;
 }
 
@@ -1629,10 +1634,12 @@ int pdgpu_md_read_trajectory(pdgpu_ctx *c, int32_t sys, double *frames, int64_t 
   return PDGPU_OK;
 }
 
-int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t first_step, int32_t steps,
-                 int32_t total_steps, double *history) {
-  CHECK_CTX(c);
-  GET_SYS(e, c, sys);
+// The step loop of pdgpu_md_run.  `tail` (may be empty) enqueues work that
+// follows the run (pdgpu_md_run_io's state copies): it is enqueued behind
+// the last block before that block's one synchronisation, and again behind
+// a block that had to run again.
+static int md_run_impl(pdgpu_ctx *c, SysEntry *e, const pdgpu_md_params *p, int32_t first_step, int32_t steps,
+                       int32_t total_steps, double *history, const std::function<int()> &tail) {
   int r = validate_md(p);
   if (r) return r;
   if (steps < 0 || first_step < 0 || total_steps < first_step + steps) {
@@ -1656,7 +1663,6 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
     e->hist_cap = steps;
   }
   if ((r = default_seeds(c, e, p->Seed))) return r;
-  PDGPU_CUDA(cudaMemcpyAsync(e->step_dev, &first_step, sizeof(int), cudaMemcpyHostToDevice, c->st));
   PDGPU_CUDA(cudaMemsetAsync(v.flags, 0, sizeof(int) * F_COUNT, c->st));
   MDCoef k = md_coef(p, first_step, total_steps);
   int every = p->UpdateNList;
@@ -1671,8 +1677,15 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
   // in-block rebuild overflows the list buffer, every kernel after it skips
   // (device flag), the state stays at the block start, and the host grows
   // the buffer and runs the block again.
-  int steps0[3] = {first_step, first_step, 0};
-  PDGPU_CUDA(cudaMemcpyAsync(e->step_dev, steps0, sizeof steps0, cudaMemcpyHostToDevice, c->st));
+  if (!e->pin_flags && cudaHostAlloc((void **)&e->pin_flags, sizeof(int) * (F_COUNT + 3), 0) != cudaSuccess) {
+    e->pin_flags = nullptr;
+    set_error("page-locked host allocation failed (MD flags)");
+    return PDGPU_ERR_NOMEM;
+  }
+  int *steps0 = e->pin_flags + F_COUNT;  // step counter, first step, finished-system count
+  steps0[0] = steps0[1] = first_step;
+  steps0[2] = 0;
+  PDGPU_CUDA(cudaMemcpyAsync(e->step_dev, steps0, sizeof(int) * 3, cudaMemcpyHostToDevice, c->st));
   cudaEventRecord(P.ev0, c->st);
   int s = 0;
   while (s < steps) {
@@ -1696,8 +1709,11 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
         set_error("neighbour list kept overflowing after regrowth");
         return PDGPU_ERR_STATE;
       }
-      PDGPU_CUDA(cudaMemsetAsync(v.flags + F_NL_OVERFLOW, 0, sizeof(int), c->st));
-      PDGPU_CUDA(cudaMemcpyAsync(e->step_dev, &step, sizeof(int), cudaMemcpyHostToDevice, c->st));
+      if (s > 0 || attempt > 0) {  // the first block starts from the run's own setup
+        PDGPU_CUDA(cudaMemsetAsync(v.flags + F_NL_OVERFLOW, 0, sizeof(int), c->st));
+        steps0[0] = step;
+        PDGPU_CUDA(cudaMemcpyAsync(e->step_dev, steps0, sizeof(int), cudaMemcpyHostToDevice, c->st));
+      }
       if (use_graph) {
         // graphs are cached per system; the key holds every value baked in
         char key[288];
@@ -1755,8 +1771,13 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
         for (int q = 0; q < block; q++) md_step_enqueue(c->st, e, k, q);
         md_steps_end(c->st, e);
       }
-      int flags[F_COUNT];
-      PDGPU_CUDA(cudaMemcpyAsync(flags, v.flags, sizeof flags, cudaMemcpyDeviceToHost, c->st));
+      const bool last = s + block >= steps;
+      if (last) {
+        cudaEventRecord(P.ev1, c->st);
+        if (tail && (r = tail())) return r;
+      }
+      int *flags = e->pin_flags;
+      PDGPU_CUDA(cudaMemcpyAsync(flags, v.flags, sizeof(int) * F_COUNT, cudaMemcpyDeviceToHost, c->st));
       r = sync_check(c, "md block");
       if (r) return r;
       if ((r = barrier_check(c, P, flags))) return r;
@@ -1786,9 +1807,7 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
     trajectory_copy(c, e, step, step + block);
     s += block;
   }
-  cudaEventRecord(P.ev1, c->st);
-  r = sync_check(c, "md_run");
-  if (r) return r;
+  if (e->traj_every > 0 && (r = sync_check(c, "md_run"))) return r;
   if (steps > 0) e->ws_step = first_step + steps - 1;  // WorkSpace::Step as run_core leaves it
   float ms = 0;
   cudaEventElapsedTime(&ms, P.ev0, P.ev1);
@@ -1801,6 +1820,13 @@ int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t fi
     for (size_t q = 0; q < h.size(); q++) history[q] = h[q] * J;
   }
   return PDGPU_OK;
+}
+
+extern "C" int pdgpu_md_run(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t first_step,
+                            int32_t steps, int32_t total_steps, double *history) {
+  CHECK_CTX(c);
+  GET_SYS(e, c, sys);
+  return md_run_impl(c, e, p, first_step, steps, total_steps, history, std::function<int()>());
 }
 
 // ------------------------------------------------------------ minimiser
@@ -1927,31 +1953,41 @@ int pdgpu_md_run_io(pdgpu_ctx *c, int32_t sys, const pdgpu_md_params *p, int32_t
   CHECK_CTX(c);
   GET_SYS(e, c, sys);
   Pack &P = *e->pack;
-  int r;
-  if (x_in) {
-    if ((r = copy_soa_in(c, P, x_in, P.v.x, P.v.y, P.v.z))) return r;
-    launch_pack_positions(P.v, c->st);
-  }
-  if (v_in && (r = copy_soa_in(c, P, v_in, P.v.vx, P.v.vy, P.v.vz))) return r;
-  if ((r = pdgpu_md_run(c, sys, p, first_step, steps, total_steps, nullptr))) return r;
   const int n = P.v.n_atoms;
-  std::vector<double> ene;
-  if ((x_out || v_out) && (r = pack_ensure_stage(&P))) return r;
-  if (x_out) {
-    launch_soa_to_aos(P.stage, P.v.x, P.v.y, P.v.z, n, c->st);
-    PDGPU_CUDA(cudaMemcpyAsync(x_out, P.stage, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, c->st));
+  const size_t blk = sizeof(double) * 3 * (size_t)n;
+  // the state in and out through one device staging block [x | v], one
+  // copy each way per array, and the copies out enqueued behind the last
+  // step block before its synchronisation: one synchronisation per call
+  if ((x_in || v_in || x_out || v_out) && !e->io_stage && xalloc(e, &e->io_stage, 6 * (size_t)n) != cudaSuccess) {
+    set_error("device allocation failed (state staging)");
+    return PDGPU_ERR_NOMEM;
   }
-  if (v_out) {  // the staging block again: stream order puts this after the positions' copy
-    launch_soa_to_aos(P.stage, P.v.vx, P.v.vy, P.v.vz, n, c->st);
-    PDGPU_CUDA(cudaMemcpyAsync(v_out, P.stage, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, c->st));
+  const size_t ne = (size_t)E_COUNT * e->nsys();
+  if (ene_out && !e->pin_ene && cudaHostAlloc((void **)&e->pin_ene, sizeof(double) * ne, 0) != cudaSuccess) {
+    e->pin_ene = nullptr;
+    set_error("page-locked host allocation failed (energies)");
+    return PDGPU_ERR_NOMEM;
+  }
+  double *const X = e->io_stage, *const V = e->io_stage ? e->io_stage + 3 * (size_t)n : nullptr;
+  if (x_in) PDGPU_CUDA(cudaMemcpyAsync(X, x_in, blk, cudaMemcpyHostToDevice, c->st));
+  if (v_in) PDGPU_CUDA(cudaMemcpyAsync(V, v_in, blk, cudaMemcpyHostToDevice, c->st));
+  if (x_in || v_in) launch_state_in(P.v, x_in ? X : nullptr, v_in ? V : nullptr, c->st);
+  auto tail = [&]() -> int {
+    if (x_out || v_out) launch_state_out(P.v, x_out ? X : nullptr, v_out ? V : nullptr, c->st);
+    if (x_out) PDGPU_CUDA(cudaMemcpyAsync(x_out, X, blk, cudaMemcpyDeviceToHost, c->st));
+    if (v_out) PDGPU_CUDA(cudaMemcpyAsync(v_out, V, blk, cudaMemcpyDeviceToHost, c->st));
+    if (ene_out) PDGPU_CUDA(cudaMemcpyAsync(e->pin_ene, P.v.ene, sizeof(double) * ne, cudaMemcpyDeviceToHost, c->st));
+    return PDGPU_OK;
+  };
+  int r = md_run_impl(c, e, p, first_step, steps, total_steps, nullptr, tail);
+  if (r) return r;
+  if (steps == 0) {  // no block ran: the copies out on their own
+    if ((r = tail()) || (r = sync_check(c, "md_run_io"))) return r;
   }
   if (ene_out) {
-    ene.resize((size_t)E_COUNT * e->nsys());
-    PDGPU_CUDA(cudaMemcpyAsync(ene.data(), P.v.ene, sizeof(double) * ene.size(), cudaMemcpyDeviceToHost, c->st));
+    const double J = consts().J_per_kcalmol;
+    for (size_t q = 0; q < ne; q++) ene_out[q] = e->pin_ene[q] * J;
   }
-  if ((r = sync_check(c, "md_run_io"))) return r;
-  const double J = consts().J_per_kcalmol;
-  for (size_t k = 0; k < ene.size(); k++) ene_out[k] = ene[k] * J;
   return PDGPU_OK;
 }
 

@@ -53,6 +53,9 @@ struct SysEntry {
   cudaStream_t st = nullptr;
   unsigned long long *seeds = nullptr;  // [S] RNG keys
   bool custom_seeds = false;
+  // the keys hold base + s from the last default upload (skip re-uploading)
+  bool seeds_default = false;
+  unsigned long long seeds_base = 0;
   int nsys() const { return (int)members.size(); }
   std::vector<const pdgpu::SystemHost *> member_ptrs() const {
     std::vector<const pdgpu::SystemHost *> m;
@@ -87,6 +90,11 @@ struct SysEntry {
   void *min_state = nullptr;
   void *mc_state = nullptr;
   std::vector<void *> extra;
+  // page-locked: an MD run's flag read-back and step-counter upload
+  // ([F_COUNT] flags, then 3 ints); pdgpu_md_run_io's energies
+  int *pin_flags = nullptr;
+  double *pin_ene = nullptr;
+  double *io_stage = nullptr;  // [6N] device staging of pdgpu_md_run_io's state (an `extra` allocation)
   // cached MD block graph (the request loop's job graph)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -126,6 +134,12 @@ struct SysEntry {
     drop_graph();
     if (traj_pending && pack) cudaStreamSynchronize(pack->side);
     free_trajectory();
+    if (pin_flags || pin_ene) cudaStreamSynchronize(st);  // no copy in flight into them
+    if (pin_flags) cudaFreeHost(pin_flags);
+    if (pin_ene) cudaFreeHost(pin_ene);
+    pin_flags = nullptr;
+    pin_ene = nullptr;
+    io_stage = nullptr;
     for (void *p : extra) cudaFreeAsync(p, st);
     extra.clear();
     seeds = nullptr;

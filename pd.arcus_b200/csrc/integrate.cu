@@ -26,13 +26,21 @@ namespace pdgpu {
 
 // One integrator step for every atom of the pack.  KE per atom goes to
 // e_atom[AE_KIN] and is reduced per system afterwards.
+// The thermostat's normals depend on the step, the atom and its system's key
+// only, so they are drawn before the wait for the force passes (under a
+// programmatic dependent launch, beside the last pass's tail).  The step
+// counter is final by then: the step's launch waits on the event of the
+// energy record that advanced it, a full dependency.
 __global__ void k_md_step(PackView v, MDDev d, const double *normals, const int *step_dev) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = i < v.n_atoms;
+  const int step = !live ? 0 : step_dev ? *step_dev : d.c.step;
+  double nr[6];
+  const bool pre = live && !normals && md_draws_normals(v, d, step, i);
+  if (pre) md_normals(v, d, step, i, nr);
   PDGPU_DEP_ENTRY();
-  if (v.flags[F_NL_OVERFLOW]) return;  // forces incomplete: keep the state, host re-plans
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= v.n_atoms) return;
-  const int step = step_dev ? *step_dev : d.c.step;
-  v.e_atom[(size_t)AE_KIN * v.n_atoms + i] = md_atom(v, d, normals, step, i);  // J
+  if (!live || v.flags[F_NL_OVERFLOW]) return;  // forces incomplete: keep the state, host re-plans
+  v.e_atom[(size_t)AE_KIN * v.n_atoms + i] = md_atom(v, d, normals, step, i, pre ? nr : nullptr);  // J
 }
 
 // per-atom kinetic energy from the current velocities (J)

@@ -360,6 +360,9 @@ void host_gb_fixed_terms(SystemHost &s);
 // ----------------------------------------------------------------- launchers
 // All launchers enqueue on `st` and do not synchronise.
 void launch_pack_positions(const PackView &v, cudaStream_t st);
+// pdgpu_md_run_io's state transfer: interleaved [n][3] staging <-> the pack
+void launch_state_in(const PackView &v, const double *X, const double *V, cudaStream_t st);
+void launch_state_out(const PackView &v, double *X, double *V, cudaStream_t st);
 void launch_aos_to_soa(const double *aos, double *X, double *Y, double *Z, int n, cudaStream_t st);
 void launch_soa_to_aos(double *aos, const double *X, const double *Y, const double *Z, int n, cudaStream_t st);
 void launch_zero(const PackView &v, cudaStream_t st);

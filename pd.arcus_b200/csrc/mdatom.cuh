@@ -85,10 +85,25 @@ inline MDDev make_md_dev(const MDCoef &c, const unsigned char *is_h, const unsig
   return d;
 }
 
+// Whether atom i draws thermostat normals at `step` (md_atom's Langevin
+// branch for it).
+__device__ __forceinline__ bool md_draws_normals(const PackView &v, const MDDev &d, int step, int i) {
+  const MDCoef &c = d.c;
+  if (c.integrator != PDGPU_INTEGRATOR_LANGEVIN || c.gamma * c.dt < 0.00001) return false;
+  const bool hyd = d.is_h && d.is_h[i];
+  return (c.stochastic_h || !hyd) && step < c.steps - 1;
+}
+// The six normals of atom i at `step` (its system's key, its local index).
+__device__ __forceinline__ void md_normals(const PackView &v, const MDDev &d, int step, int i, double *nr) {
+  const int s = v.sys_of[i];
+  six_normals(d.sys_seed[s], i - v.atom_off[s], step, nr);
+}
+
 // Advance atom i by one step of the integrator in d.c at `step`; returns
-// its kinetic energy (J) at the point the reference measures it.
+// its kinetic energy (J) at the point the reference measures it.  `pre`:
+// the atom's thermostat normals drawn already (md_normals), or NULL.
 __device__ __forceinline__ double md_atom(const PackView &v, const MDDev &d, const double *normals, int step,
-                                          int i) {
+                                          int i, const double *pre = nullptr) {
   const MDCoef &c = d.c;
   double m = v.mass_si[i];
   double f[3] = {force_N(v.fx[i], v.gx[i], v.hx[i]) * d.N_per_unit, force_N(v.fy[i], v.gy[i], v.hy[i]) * d.N_per_unit,
@@ -140,9 +155,10 @@ __device__ __forceinline__ double md_atom(const PackView &v, const MDDev &d, con
       double nr[6];
       if (normals) {
         for (int k = 0; k < 6; k++) nr[k] = normals[6 * (size_t)i + k];
+      } else if (pre) {
+        for (int k = 0; k < 6; k++) nr[k] = pre[k];
       } else {
-        int s = v.sys_of[i];
-        six_normals(d.sys_seed[s], i - v.atom_off[s], step, nr);
+        md_normals(v, d, step, i, nr);
       }
       double n1x = nr[0], n2y = nr[1], n2x = nr[2], n1z = nr[3], n1y = nr[4], n2z = nr[5];
       double kTdivm = d.kB * c.temp * im;

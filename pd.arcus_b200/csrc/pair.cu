@@ -76,6 +76,54 @@ __global__ void k_soa_to_aos(double *aos, const double *X, const double *Y, cons
   aos[3 * (size_t)i + 1] = Y[i];
   aos[3 * (size_t)i + 2] = Z[i];
 }
+// The MD state in and out of pdgpu_md_run_io in one launch each: positions
+// (with the pair-kernel records) and velocities from / to interleaved
+// [n][3] staging blocks (either may be absent).
+__global__ void k_state_in(PackView v, const double *X, const double *V) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v.n_atoms) return;
+  if (X) {
+    const double x = X[3 * (size_t)i], y = X[3 * (size_t)i + 1], z = X[3 * (size_t)i + 2];
+    v.x[i] = x;
+    v.y[i] = y;
+    v.z[i] = z;
+    float hx = __double2float_rn(x), hy = __double2float_rn(y), hz = __double2float_rn(z);
+    float4 a = v.pq[2 * (size_t)i];
+    a.x = hx;
+    a.y = hy;
+    a.z = hz;
+    v.pq[2 * (size_t)i] = a;
+    v.pq[2 * (size_t)i + 1] = make_float4(__double2float_rn(x - (double)hx), __double2float_rn(y - (double)hy),
+                                          __double2float_rn(z - (double)hz), 0.f);
+    v.xyzp[i] = make_double4(x, y, z, v.pv_d[i]);
+  }
+  if (V) {
+    v.vx[i] = V[3 * (size_t)i];
+    v.vy[i] = V[3 * (size_t)i + 1];
+    v.vz[i] = V[3 * (size_t)i + 2];
+  }
+}
+__global__ void k_state_out(PackView v, double *X, double *V) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v.n_atoms) return;
+  if (X) {
+    X[3 * (size_t)i] = v.x[i];
+    X[3 * (size_t)i + 1] = v.y[i];
+    X[3 * (size_t)i + 2] = v.z[i];
+  }
+  if (V) {
+    V[3 * (size_t)i] = v.vx[i];
+    V[3 * (size_t)i + 1] = v.vy[i];
+    V[3 * (size_t)i + 2] = v.vz[i];
+  }
+}
+void launch_state_in(const PackView &v, const double *X, const double *V, cudaStream_t st) {
+  if (v.n_atoms) PDGPU_LAUNCH(k_state_in, (v.n_atoms + 255) / 256, 256, 0, st, v, X, V);
+}
+void launch_state_out(const PackView &v, double *X, double *V, cudaStream_t st) {
+  if (v.n_atoms) PDGPU_LAUNCH(k_state_out, (v.n_atoms + 255) / 256, 256, 0, st, v, X, V);
+}
+
 void launch_aos_to_soa(const double *aos, double *X, double *Y, double *Z, int n, cudaStream_t st) {
   if (n > 0) PDGPU_LAUNCH(k_aos_to_soa, (n + 255) / 256, 256, 0, st, aos, X, Y, Z, n);
 }
