@@ -13,17 +13,19 @@ Extra keys of the same JSON line:
               Rc 12 A, 1,000 Langevin steps at 1 fs (friction 1e13/s, the
               reference's default), ns/day beside the reference's own CPU MD
               on one core.
-  batched_sp  512 peptide systems (32 copies of each of the 16 reference-built
-              AMBER99 peptides of tests/golden/lib16_amber_s3.npz, lengths
-              log-uniform 20-200 residues, each copy with its own RNG key)
+  batched_sp  512 distinct AMBER99 peptides, lengths log-uniform 20-200
+              residues: the 16 reference-built peptides of
+              tests/golden/lib16_amber_s3.npz and 496 seeded ones spliced from
+              their residue templates (pdgpu.peptides) and relaxed with 500
+              steepest-descent steps on the device; each with its own RNG key,
               x 64 backbone phi/psi trials (sigma 15 deg) drawn on the device:
               32,768 energy+force evaluations, Rc 12 A, in 64 batched
               evaluations of all 512 systems; against the plain path (one
               system per launch sequence) on a sample.  device_mc: the same
               batch through the whole Monte Carlo protocol on the device
               (64 steps, Metropolis at 300 K, pdgpu_mc_run).
-  batched_md  256 peptide systems (16 copies of each of the 16 OPLS-AA
-              peptides of tests/golden/lib16_opls_s4.npz, 30-150 residues),
+  batched_md  256 distinct OPLS-AA peptides of 30-150 residues (the 16 of
+              tests/golden/lib16_opls_s4.npz and 240 spliced as above),
               Langevin 1 fs, gamma 1/ps, 300 K, Rc 12 A, list every 10 steps,
               all systems in one CUDA-graph step loop; aggregate ns/day against
               one system alone.
@@ -165,28 +167,67 @@ def make_ws(pdgpu, arrays, meta, ctx):
     return ws, ff
 
 
+def spliced_members(pdgpu, A, ctx, lib, lengths, seed, premin=500):
+    """Distinct seeded peptides of the given lengths, spliced from the
+    library's reference-built residue templates (pdgpu.peptides) and relaxed
+    with `premin` steepest-descent steps of the device minimiser (all of them
+    as one batch).  Returns (ws, ff, arrays, meta) per peptide and the
+    seconds the splicing and the minimisation took."""
+    from pdgpu.peptides import ResidueLibrary
+    t0 = time.perf_counter()
+    R = ResidueLibrary(lib)
+    rng = np.random.default_rng(seed)
+    out = []
+    for nres in lengths:
+        seq = R.draw_sequence(rng, int(nres))
+        arrays = R.build(seq)
+        meta = dict(lib[0][1], chain=[seq], natoms=str(len(arrays["charge"])), premin=str(premin),
+                    seed=str(seed), spliced="1")
+        ws, ff = make_ws(pdgpu, arrays, meta, ctx)
+        out.append((ws, ff, arrays, meta))
+    t_build = time.perf_counter() - t0
+    b = pdgpu.Batch([ws for ws, *_ in out])
+    mp = A.min_params_default()
+    mp.Algorithm = A.MIN_STEEPEST_DESCENT
+    taken = b.minimise(mp, premin)
+    if np.any(taken < 0):
+        raise RuntimeError("a spliced peptide's energy turned NaN during its relaxation")
+    for (ws, ff, arrays, meta), pos in zip(out, b.split(b.positions())):
+        arrays["pos"] = pos.copy()
+        ws.cur.p[:] = pos
+        ws._push_positions()
+    b.close()
+    return out, {"splice_s": t_build, "minimise_s": time.perf_counter() - t0 - t_build, "premin_sd_steps": premin}
+
+
 def pctl(xs, q):
     return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
 
 
 # ---------------------------------------------------------------- batched workloads
-def bench_batched_sp(pdgpu, A, ctx, torch, copies=32, trials=64, plain_trials=2):
+def bench_batched_sp(pdgpu, A, ctx, torch, n_systems=512, trials=64, plain_trials=2):
     """Batched single-point evaluations of Monte Carlo trial conformations."""
     lib = load_library(LIB_SP)
     L = A.lib()
     sigma = np.deg2rad(15.0)
     members = []
-    for c in range(copies):
-        for k, (a, m) in enumerate(lib):
-            ws, ff = make_ws(pdgpu, a, m, ctx)
-            ws.setTorsionMoves()
-            members.append((ws, ff, a, m, c * len(lib) + k))
+    for k, (a, m) in enumerate(lib):
+        ws, ff = make_ws(pdgpu, a, m, ctx)
+        members.append((ws, ff, a, m))
+    # the other peptides: lengths log-uniform in 20-200 residues (seeded)
+    rng = np.random.default_rng(3003)
+    lens = np.floor(np.exp(rng.uniform(np.log(20), np.log(200), n_systems - len(lib)))).astype(int)
+    extra, prep = spliced_members(pdgpu, A, ctx, lib, lens, seed=3004)
+    members += extra
+    members = [(ws, ff, a, m, s) for s, (ws, ff, a, m) in enumerate(members)]
+    for ws, *_ in members:
+        ws.setTorsionMoves()
     nsys = len(members)
     b = pdgpu.Batch([ws for ws, *_ in members])
     b.setSeeds(np.array([1_000_003 * (s + 1) for *_, s in members], dtype=np.uint64))
     b.saveBasePositions()
     # parity: the reference's first recorded trial of every peptide
-    ang = [a["trial_angles"][0] for ws, ff, a, m, s in members]
+    ang = [a["trial_angles"][0] if "trial_angles" in a else np.zeros(ws.nRotations) for ws, ff, a, m, s in members]
     b.perturbTorsions(angles=ang)
     f, e = b.evaluate()
     worst = 0.0
@@ -265,6 +306,10 @@ def bench_batched_sp(pdgpu, A, ctx, torch, copies=32, trials=64, plain_trials=2)
                              "evaluation time" % (len(t), cores)}
     return {"metric": "batched GB evals/s", "value": evals / t_all, "unit": "evals/s", "cpu_baseline": cpu,
             "evals": evals, "systems": nsys, "trials_per_system": trials, "atoms_packed": atoms,
+            "systems_made": dict(prep, reference_built=len(lib), spliced=nsys - len(lib),
+                                 how="16 library peptides built by the reference's NewProtein, and distinct seeded "
+                                     "peptides (lengths log-uniform 20-200 residues) spliced from their residue "
+                                     "templates and relaxed by the device minimiser"),
             "batch_latency_ms": {"p50": 1e3 * pctl(lat, 50), "p99": 1e3 * pctl(lat, 99)},
             "plain_one_system_per_launch": {"value": n_plain / t_plain, "unit": "evals/s", "sample_evals": n_plain,
                                             "latency_ms": {"p50": 1e3 * pctl(plain, 50), "p99": 1e3 * pctl(plain, 99)}},
@@ -276,15 +321,18 @@ def bench_batched_sp(pdgpu, A, ctx, torch, copies=32, trials=64, plain_trials=2)
             "timing": "wall clock around perturb + list + forces + energies read-back, per batched evaluation"}
 
 
-def bench_batched_md(pdgpu, A, ctx, torch, copies=16, steps=5000, plain_steps=200, drift_steps=1000):
+def bench_batched_md(pdgpu, A, ctx, torch, n_systems=256, steps=5000, plain_steps=200, drift_steps=1000):
     """All systems advanced together in one CUDA-graph step loop."""
     lib = load_library(LIB_MD)
     L = A.lib()
     members = []
-    for c in range(copies):
-        for k, (a, m) in enumerate(lib):
-            ws, ff = make_ws(pdgpu, a, m, ctx)
-            members.append((ws, ff, a, m))
+    for k, (a, m) in enumerate(lib):
+        ws, ff = make_ws(pdgpu, a, m, ctx)
+        members.append((ws, ff, a, m))
+    # the other peptides: lengths uniform in 30-150 residues (seeded)
+    lens = np.random.default_rng(4003).integers(30, 151, n_systems - len(lib))
+    extra, prep = spliced_members(pdgpu, A, ctx, lib, lens, seed=4004)
+    members += extra
     nsys = len(members)
     p = A.md_params_default()
     p.Integrator, p.UpdateNList, p.UseGraph = A.INTEGRATOR_LANGEVIN, 10, 1
@@ -366,6 +414,10 @@ def bench_batched_md(pdgpu, A, ctx, torch, copies=16, steps=5000, plain_steps=20
                                                                                                         cores)}
     return {"metric": "batched GB MD aggregate ns/day", "value": agg, "unit": "ns/day", "systems": nsys,
             "drift": drift, "cpu_baseline": cpu,
+            "systems_made": dict(prep, reference_built=len(lib), spliced=nsys - len(lib),
+                                 how="16 library peptides built by the reference's NewProtein, and distinct seeded "
+                                     "peptides (lengths uniform 30-150 residues) spliced from their residue templates "
+                                     "and relaxed by the device minimiser"),
             "steps": steps, "atoms_packed": atoms, "ms_per_step": ms / steps,
             "plain_one_system": {"value": one_nsday, "unit": "ns/day", "atoms": int(a["charge"].shape[0]),
                                  "steps": plain_steps},
