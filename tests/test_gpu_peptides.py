@@ -1,8 +1,9 @@
 """Spliced peptides (pdgpu.peptides) as device workloads: after relaxation
 by the device minimiser, a batch of seeded spliced AMBER99 and OPLS-AA
-peptides has finite energies, its neighbour lists equal the oracle's pair
-sets, and its forces and Born radii agree with the oracle's FP64 evaluation
-at the same coordinates (relative force RMS 1e-5, Born radii 2e-6)."""
+peptides (2 to 90 residues) has finite energies, its neighbour lists equal
+the oracle's pair sets, and its forces and Born radii agree with the
+oracle's FP64 evaluation at the same coordinates (relative force RMS 1e-5,
+Born radii 2e-6)."""
 import numpy as np
 import pytest
 
@@ -22,7 +23,7 @@ def test_spliced_peptides_relax_and_match_the_oracle(lib_name, gpu_ctx):
     R = ResidueLibrary(lib)
     rng = np.random.default_rng(21)
     built = []
-    for nres in (22, 47, 90):
+    for nres in (2, 22, 47, 90):  # a dipeptide: the smallest chain, one i-cluster
         arrays = R.build(R.draw_sequence(rng, nres))
         meta = dict(lib[0][1], natoms=str(len(arrays["charge"])))
         ws, ff = build_workspace(arrays, meta, gpu_ctx)
