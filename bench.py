@@ -1081,6 +1081,9 @@ def main():
     ems, ecnt = np.zeros(4), np.zeros(5, dtype=np.int64)
     if path == 1:  # the evaluation kernel: three phases as three launches, then one launch
         A.check(A.lib().pdgpu_profile_eval(ctx.ptr, ws._sys, 20, A.dptr(ems), ecnt.ctypes.data_as(A._I64)))
+    # the FP32 (FMA) and special-function (MUFU) pipes' throughput on this device
+    pipes = np.zeros(3)
+    A.check(A.lib().pdgpu_measure_pipe_peaks(ctx.ptr, A.dptr(pipes)))
 
     p = A.md_params_default()
     p.Integrator, p.UpdateNList, p.UseGraph = A.INTEGRATOR_LANGEVIN, BLOCK, 1
@@ -1170,11 +1173,15 @@ def main():
     P_B, P_H, entries, tile_pairs, n_tiles = (int(c) for c in counts)
     f_max = (clk.get("sm_max_mhz") or 1965.0) * 1e6
     sms = torch.cuda.get_device_properties(device).multi_processor_count
-    F32 = sms * 256 * f_max
-    SFU = sms * 16 * f_max
+    F32_nom, SFU_nom = sms * 256 * f_max, sms * 16 * f_max
+    F32 = float(pipes[0]) if pipes[0] > 0 else F32_nom
+    SFU = float(pipes[1]) if pipes[1] > 0 else SFU_nom
     t2, t3, t4 = (float(x) / 1e3 for x in kms)
     all_flop, all_sfu = 57.0 * P_B + 90.0 * P_H, 7.0 * P_B + 5.0 * P_H
-    peak_note = "nominal %d SMs x %%s/clk at sm_max_mhz %.0f (no measured FP32/SFU peak)" % (sms, f_max / 1e6)
+    peak_note = ("measured on this device (pdgpu_measure_pipe_peaks: FP32 FMA and MUFU ex2 chains on every SM): "
+                 "%.1f TFLOP/s FP32, %.2f Top/s MUFU; nominal %d SMs x 256 flop / 16 MUFU per clk at sm_max_mhz "
+                 "%.0f: %.1f / %.2f (%%s)" % (F32 / 1e12, SFU / 1e12, sms, f_max / 1e6, F32_nom / 1e12,
+                                                SFU_nom / 1e12))
     tiles_info = {"tiles": n_tiles, "pair_slots": 256 * n_tiles, "list_pairs_held": tile_pairs,
                   "slot_occupancy": tile_pairs / max(1, 256 * n_tiles)}
     if path == 1:
@@ -1199,7 +1206,7 @@ def main():
                 "traffic": NCU_TRAFFIC_EVAL if NCU_TRAFFIC_EVAL else None,
                 "traffic_unit": "bytes per evaluation (ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
                                 "three one-phase launches on this workload)",
-                "peak_source": peak_note % ("256 flop" if bound == "fp32" else "16 MUFU"),
+                "peak_source": peak_note % ("the binding pipe: " + ("FP32" if bound == "fp32" else "MUFU")),
                 "pairs": {"P_B": P_B, "P_H": P_H, "list_entries": entries},
                 "kernel_ms": {"three_launches": tE * 1e3, "phase_born": tA * 1e3, "phase_pair": tB * 1e3,
                               "phase_chain": tC * 1e3, "one_cooperative_launch": tF * 1e3},
@@ -1225,7 +1232,7 @@ def main():
                 "peak": (F32 if bound == "fp32" else SFU) / 1e12,
                 "unit": "TFLOP/s" if bound == "fp32" else "Top/s (MUFU)",
                 "frac": max(k3_frac_fp32, k3_frac_sfu), "traffic": None,
-                "peak_source": peak_note % ("256 flop" if bound == "fp32" else "16 MUFU"),
+                "peak_source": peak_note % ("the binding pipe: " + ("FP32" if bound == "fp32" else "MUFU")),
                 "pairs": {"P_B": P_B, "P_H": P_H, "list_entries": entries},
                 "kernel_ms": {"born_K2": t2 * 1e3, "pair_K3": t3 * 1e3, "chain_K4": t4 * 1e3},
                 "lanes_per_atom": {"born_K2": int(lpa[0]), "pair_K3": int(lpa[1]), "chain_K4": int(lpa[2])},

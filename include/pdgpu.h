@@ -539,6 +539,12 @@ int pdgpu_profile_pair_kernels(pdgpu_ctx *ctx, int32_t sys, int32_t reps, double
  * edge decided in FP64).  PDGPU_ERR_STATE unless the handle is on the tile
  * layout. */
 int pdgpu_profile_eval(pdgpu_ctx *ctx, int32_t sys, int32_t reps, double *ms, int64_t *counts);
+/* Instrumentation (no reference counterpart): the throughput of the two
+ * pipes the pair kernels are bound by, measured on the context's device
+ * with every SM full of warps: out[0] FP32 flop/s of fused multiply-adds
+ * (2 flop each), out[1] special-function operations/s (ex2.approx), out[2]
+ * the SM count.  The best of three timed launches each (a few ms). */
+int pdgpu_measure_pipe_peaks(pdgpu_ctx *ctx, double *out);
 /* How an evaluation on the tile layout is launched (no reference
  * counterpart): 1 = the three passes in one cooperative launch everywhere,
  * 0 = the same three phases as three launches everywhere, 2 (the default) =

@@ -2234,6 +2234,17 @@ int pdgpu_profile_eval(pdgpu_ctx *c, int32_t sys, int32_t reps, double *ms, int6
   return PDGPU_OK;
 }
 
+int pdgpu_measure_pipe_peaks(pdgpu_ctx *c, double *out) {
+  CHECK_CTX(c);
+  if (!out) {
+    set_error("out is NULL");
+    return PDGPU_ERR_ARG;
+  }
+  cudaError_t ce = measure_pipe_peaks(c->st, out);
+  if (ce != cudaSuccess) return cuda_fail(ce, "measure_pipe_peaks");
+  return sync_check(c, "measure_pipe_peaks");
+}
+
 int pdgpu_eval_mode(pdgpu_ctx *c, int32_t sys, int32_t set, int32_t *current) {
   CHECK_CTX(c);
   GET_SYS(e, c, sys);

@@ -402,6 +402,7 @@ int eval_tiles_grid(long long tile_cap);
 cudaError_t profile_eval_tiles(const PackView &v, cudaStream_t st, int reps, double *ms);
 // the Born-sum phase alone (it fills the still list; instrumentation)
 cudaError_t launch_born_phase_only(const PackView &v, cudaStream_t st);
+cudaError_t measure_pipe_peaks(cudaStream_t st, double *out);
 // one evaluation counting the tiles each phase redid in its careful form
 cudaError_t count_deferred_tiles(const PackView &v, cudaStream_t st, int *stats);
 // explicit lanes-per-atom variants (4, 8, 16, 32), used by the autotuner

@@ -171,6 +171,7 @@ PROTOTYPES = {
     "pdgpu_pair_counts": (ctypes.c_int, [_CTX, ctypes.c_int32, _I64]),
     "pdgpu_profile_pair_kernels": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32, _D]),
     "pdgpu_profile_eval": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32, _D, _I64]),
+    "pdgpu_measure_pipe_peaks": (ctypes.c_int, [_CTX, _D]),
     "pdgpu_eval_mode": (ctypes.c_int, [_CTX, ctypes.c_int32, ctypes.c_int32, _I]),
     "pdgpu_launch_count": (ctypes.c_int, [_CTX, _I64]),
     "pdgpu_graph_replays": (ctypes.c_int, [_CTX, ctypes.c_int32, _I64]),

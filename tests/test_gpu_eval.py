@@ -170,3 +170,21 @@ def test_lean_build_equals_general(gpu_ctx, tmp_path):
                     os.path.join(ROOT, "tests"), out], env=env, check=True, timeout=300)
     assert np.array_equal(np.load(out), ws.cur.f)
     ws.close()
+
+
+def test_measured_pipe_peaks_are_near_nominal(gpu_ctx):
+    """pdgpu_measure_pipe_peaks (the roofline's FP32 and MUFU denominators):
+    every SM counted, and each pipe between half and 1.15 x its nominal
+    rate at the device's maximum clock (128 FMA and 16 MUFU lanes a SM)."""
+    import torch
+    from pdgpu import _abi as A
+    out = np.zeros(3)
+    A.check(A.lib().pdgpu_measure_pipe_peaks(gpu_ctx.ptr, A.dptr(out)))
+    props = torch.cuda.get_device_properties(0)
+    sms = props.multi_processor_count
+    assert int(out[2]) == sms
+    import pynvml
+    pynvml.nvmlInit()
+    f_max = pynvml.nvmlDeviceGetMaxClockInfo(pynvml.nvmlDeviceGetHandleByIndex(0), pynvml.NVML_CLOCK_SM) * 1e6
+    assert 0.5 * sms * 256 * f_max <= out[0] <= 1.15 * sms * 256 * f_max
+    assert 0.5 * sms * 16 * f_max <= out[1] <= 1.15 * sms * 16 * f_max
