@@ -469,16 +469,41 @@ def bench_plain_small(pdgpu, A, ctx, torch, steps=1000, cpu_steps=200):
            "workload": "64-residue peptide, AMBER99 + Still GB + bonded, Rc 12 A, Langevin 1 fs 300 K, "
                        "friction 1e13/s, list every 10 steps",
            "timing": "CUDA events around the device step loop (pdgpu_last_run_ms)"}
-    ws.close()
+    # energy conservation without a thermostat (a friction of 1e3 /s: gamma dt
+    # is below 1e-5, where both codes run velocity Verlet: the Langevin
+    # integrator's fallback, md.cpp:906-1042) from
+    # the fixture's coordinates at 300 K, against the
+    # reference's own run of the same length (its own initial velocities:
+    # the drifts agree statistically, not step by step)
+    ws2, _ = make_ws(pdgpu, arrays, meta, ctx)
+    ws2.nlist().calcNewList()
+    q = A.md_params_default()
+    q.Integrator, q.UpdateNList, q.UseGraph = A.INTEGRATOR_LANGEVIN, BLOCK, 1
+    q.Timestep, q.FricCoeff, q.TargetTemp, q.Seed = 1e-15, 1e3, 300.0, 0
+    A.check(L.pdgpu_md_init_velocities(ctx.ptr, ws2._sys, 300.0, 0))
+    hv = np.zeros(3 * steps)
+    A.check(L.pdgpu_md_run(ctx.ptr, ws2._sys, ctypes.byref(q), 0, steps, steps, A.dptr(hv)))
+    ws2.close()
+    hv = hv.reshape(steps, 3) * pdgpu.J2KCAL_NA
+    out["nve_drift"] = {"unit": "kcal/mol per 1000 steps", "steps": steps,
+                        "gpu": ls_drift(np.arange(steps), hv[:, 2], steps),
+                        "etot_start_kcal": float(hv[0, 2]),
+                        "method": "least-squares slope of etot (MolecularDynamics::run_core), velocity Verlet "
+                                  "(Langevin at 1e3 /s falls back to it), 1 fs, list every 10 steps, initial "
+                                  "velocities at 300 K"}
     if os.path.exists(REF_DRIVER):
-        res, _ = run_ref_jobs([(arrays, meta, "time", ["--steps", cpu_steps, "--warmup", 10, "--nlist-every", 10,
-                                                        "--fric", "1e13"])], 1)
+        jobs = [(arrays, meta, "time", ["--steps", cpu_steps, "--warmup", 10, "--nlist-every", 10, "--fric", "1e13"]),
+                (arrays, meta, "time", ["--steps", steps, "--warmup", 0, "--nlist-every", 10, "--fric", "1e3",
+                                        "--drift"])]
+        res, _ = run_ref_jobs(jobs, 2)
         if res[0]:
             v = cpu_steps * DT_FS * 1e-6 / res[0]["seconds"] * 86400.0
             out["cpu_baseline"] = {"value": v, "unit": "ns/day", "cores": 1, "kind": "reference",
                                    "sample": "%d MD steps after 10 warm-up, reference MolecularDynamics step loop"
                                              % cpu_steps}
             out["speedup_vs_cpu"] = nsday / v
+        if res[1]:
+            out["nve_drift"]["reference"] = res[1].get("drift_kcal_per_1000")
     return out
 
 
