@@ -77,6 +77,9 @@ METRIC = "GB MD ns/day"
 # cold caches: 1,924,352 + 3,327,488 + 3,158,784 bytes read, nothing written);
 # ncu cannot run inside the timed bench, so the figure is carried here
 NCU_TRAFFIC_EVAL = 8410624
+# warp instructions the same three launches executed (smsp__inst_executed.sum
+# of that capture: phases A, B, C), for the issue roof beside the FP32/SFU one
+NCU_INST_EVAL = (5848656, 15501308, 6179253)
 
 
 def rank_info():
@@ -1243,7 +1246,16 @@ def main():
                 "careful_tiles": {"born": int(ecnt[2]), "pair": int(ecnt[3]), "chain": int(ecnt[4])},
                 "three_pass_form_ms": {"born_K2": t2 * 1e3, "pair_K3": t3 * 1e3, "chain_K4": t4 * 1e3,
                                        "frac_of_roof": max(all_flop / F32, all_sfu / SFU) / (t2 + t3 + t4)},
-                "pair_kernels_frac_of_roof": max(all_flop / F32, all_sfu / SFU) / tE}
+                "pair_kernels_frac_of_roof": max(all_flop / F32, all_sfu / SFU) / tE,
+                "issue_roof": {
+                    "warp_instructions": sum(NCU_INST_EVAL),
+                    "per_phase": list(NCU_INST_EVAL),
+                    "roof_ms": 1e3 * sum(NCU_INST_EVAL) / (sms * 4 * f_max),
+                    "frac": (sum(NCU_INST_EVAL) / (sms * 4 * f_max)) / tE,
+                    "frac_one_cooperative_launch": (sum(NCU_INST_EVAL) / (sms * 4 * f_max)) / tF,
+                    "note": "the instructions the kernel executes (ncu, this workload) at one warp instruction "
+                            "per scheduler per clock (4 a SM); the FP32/SFU roof counts only the algorithmic "
+                            "operations of the pairs inside the cutoffs"}}
     else:
         k3_flop, k3_sfu = 90.0 * P_H, 5.0 * P_H
         k3_frac_fp32 = (k3_flop / t3) / F32
