@@ -97,3 +97,31 @@ def test_small_system_md_stays_finite(gpu_ctx):
     md.run()
     assert np.all(np.isfinite(md.history)) and np.all(np.isfinite(ws.cur.p))
     ws.close()
+
+
+def test_batch_with_tiny_members_equals_alone(gpu_ctx):
+    """A batch holding a one-atom system, a pairless system, a peptide and a
+    six-atom system: every member's forces and energies are the bits it
+    gets alone."""
+    import pdgpu
+    a, m = load_library("lib16_amber_s3")[0]
+    specs = [_system(CASES["one_atom"], _PICK[:1]), _system(CASES["no_pair_in_cutoff"], _PICK[:2]),
+             (a, m), _system(CASES["across_the_edges"], _PICK)]
+    alone = []
+    for arrays, meta in specs:
+        ws, ff = build_workspace(arrays, meta, gpu_ctx)
+        ws.setPairPath(1)
+        ws.nlist().calcNewList()
+        ff.calcForces()
+        alone.append((ws.cur.f.copy(), ws.ene.epot))
+        ws.close()
+    members = [build_workspace(arrays, meta, gpu_ctx)[0] for arrays, meta in specs]
+    b = pdgpu.Batch(members)
+    b.setPairPath(1)
+    f, e = b.evaluate()
+    for s, (fa, ea) in enumerate(alone):
+        assert np.array_equal(b.split(f)[s], fa), s
+        assert e[s][0] == ea, s
+    b.close()
+    for ws in members:
+        ws.close()
