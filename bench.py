@@ -203,12 +203,38 @@ def spliced_members(pdgpu, A, ctx, lib, lengths, seed, premin=500):
     return out, {"splice_s": t_build, "minimise_s": time.perf_counter() - t0 - t_build, "premin_sd_steps": premin}
 
 
+def eval_roofline(A, ctx, sid, peaks):
+    """The evaluation kernel's FP32/SFU roofline fraction on handle `sid`
+    (a system or a batch on the tile layout; None otherwise): the same work
+    counts and measured peaks as the headline's, over the three one-phase
+    launches and over the cooperative launch."""
+    L = A.lib()
+    if peaks is None or L.pdgpu_pair_path(ctx.ptr, sid, -2, None) != 0:
+        return None
+    cur = ctypes.c_int32(0)
+    A.check(L.pdgpu_pair_path(ctx.ptr, sid, -2, ctypes.byref(cur)))
+    if cur.value != 1:
+        return None
+    counts = np.zeros(5, dtype=np.int64)
+    A.check(L.pdgpu_pair_counts(ctx.ptr, sid, counts.ctypes.data_as(A._I64)))
+    ems = np.zeros(4)
+    A.check(L.pdgpu_profile_eval(ctx.ptr, sid, 10, A.dptr(ems), None))
+    P_B, P_H, entries, held, tiles = (int(c) for c in counts)
+    F32, SFU = peaks
+    t_roof = max((57.0 * P_B + 90.0 * P_H) / F32, (7.0 * P_B + 5.0 * P_H) / SFU)
+    t3, t1 = sum(float(x) for x in ems[:3]) / 1e3, float(ems[3]) / 1e3
+    return {"frac": t_roof / t3, "frac_one_cooperative_launch": t_roof / t1,
+            "kernel_ms": {"three_launches": 1e3 * t3, "one_cooperative_launch": 1e3 * t1},
+            "pairs": {"P_B": P_B, "P_H": P_H}, "tiles": tiles,
+            "slot_occupancy": held / max(1, 256 * tiles)}
+
+
 def pctl(xs, q):
     return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
 
 
 # ---------------------------------------------------------------- batched workloads
-def bench_batched_sp(pdgpu, A, ctx, torch, n_systems=512, trials=64, plain_trials=2):
+def bench_batched_sp(pdgpu, A, ctx, torch, n_systems=512, trials=64, plain_trials=2, peaks=None):
     """Batched single-point evaluations of Monte Carlo trial conformations."""
     lib = load_library(LIB_SP)
     L = A.lib()
@@ -238,6 +264,7 @@ def bench_batched_sp(pdgpu, A, ctx, torch, n_systems=512, trials=64, plain_trial
         fs = b.split(f)[s]
         ref = a["trial_f"][0]
         worst = max(worst, float(np.sqrt(np.sum((fs - ref) ** 2) / np.sum(ref ** 2))))
+    roof = eval_roofline(A, ctx, b._id, peaks)
     lat = []
     lc0 = ctypes.c_int64(0)
     L.pdgpu_launch_count(ctx.ptr, ctypes.byref(lc0))
@@ -318,13 +345,14 @@ def bench_batched_sp(pdgpu, A, ctx, torch, n_systems=512, trials=64, plain_trial
                                             "latency_ms": {"p50": 1e3 * pctl(plain, 50), "p99": 1e3 * pctl(plain, 99)}},
             "speedup_vs_plain": (evals / t_all) / (n_plain / t_plain),
             "device_mc": dict(mc, speedup_vs_plain=(nsys * trials / t_mc) / (n_plain / t_plain)),
-            "gpu_launches": int(lc1.value - lc0.value),
+            "gpu_launches": int(lc1.value - lc0.value), "roofline": roof,
             "parity": {"force_rel_rms_vs_fp64_max": worst,
                        "case": "reference trial 0 of each of the 16 peptides, angles from the reference run"},
             "timing": "wall clock around perturb + list + forces + energies read-back, per batched evaluation"}
 
 
-def bench_batched_md(pdgpu, A, ctx, torch, n_systems=256, steps=5000, plain_steps=200, drift_steps=1000):
+def bench_batched_md(pdgpu, A, ctx, torch, n_systems=256, steps=5000, plain_steps=200, drift_steps=1000,
+                     peaks=None):
     """All systems advanced together in one CUDA-graph step loop."""
     lib = load_library(LIB_MD)
     L = A.lib()
@@ -353,6 +381,7 @@ def bench_batched_md(pdgpu, A, ctx, torch, n_systems=256, steps=5000, plain_step
     ms = ctx.last_run_ms()
     lc1 = ctypes.c_int64(0)
     L.pdgpu_launch_count(ctx.ptr, ctypes.byref(lc1))
+    roof = eval_roofline(A, ctx, b._id, peaks)  # after the run: its launches are not counted
     h = hist.reshape(steps, nsys, 3) * pdgpu.J2KCAL_NA
     nat = np.diff(b.offsets)
     ek_per_atom = h[-100:, :, 1].mean(axis=0) / nat  # kcal/mol per atom
@@ -416,7 +445,7 @@ def bench_batched_md(pdgpu, A, ctx, torch, n_systems=256, steps=5000, plain_step
                              "concurrent processes on %d cores; aggregate = cores x 1 fs / mean step time" % (len(t),
                                                                                                         cores)}
     return {"metric": "batched GB MD aggregate ns/day", "value": agg, "unit": "ns/day", "systems": nsys,
-            "drift": drift, "cpu_baseline": cpu,
+            "drift": drift, "cpu_baseline": cpu, "roofline": roof,
             "systems_made": dict(prep, reference_built=len(lib), spliced=nsys - len(lib),
                                  how="16 library peptides built by the reference's NewProtein, and distinct seeded "
                                      "peptides (lengths uniform 30-150 residues) spliced from their residue templates "
@@ -1286,8 +1315,9 @@ def main():
     if not args.no_batched:
         line["plain_small"] = bench_plain_small(pdgpu, A, ctx, torch)
         line["lcpo"] = bench_lcpo(pdgpu, A, ctx, torch, arrays, meta, f_max, sms)
-        line["batched_sp"] = bench_batched_sp(pdgpu, A, ctx, torch)
-        line["batched_md"] = bench_batched_md(pdgpu, A, ctx, torch, steps=args.batched_md_steps)
+        line["batched_sp"] = bench_batched_sp(pdgpu, A, ctx, torch, peaks=(F32, SFU))
+        line["batched_md"] = bench_batched_md(pdgpu, A, ctx, torch, steps=args.batched_md_steps,
+                                              peaks=(F32, SFU))
         line["serving"] = bench_serving(pdgpu, A, ctx, torch, n_requests=args.serve_requests,
                                         policy=args.serve_policy, max_active=args.serve_max_active,
                                         tiles=not args.serve_rows, batch_ms=args.serve_batch_ms)
