@@ -256,19 +256,22 @@ __device__ __forceinline__ SearchRow search_row(const PackView &v, bool live, in
   }
   return r;
 }
+// A search block's tiles are staged in shared memory and written to the
+// tile store as one contiguous range when the block is done, so the tiles
+// of an i-cluster sit together and a pass that walks contiguous tile ranges
+// meets few i-cluster changes (each one a reload of the i side).  Tiles
+// beyond the staging capacity go to the store one at a time.
+constexpr int kSearchStage = 256;
+struct SearchStage {
+  int n;                               // tiles emitted into the stage (may pass kSearchStage)
+  int4 meta[kSearchStage];
+  unsigned rows[kSearchStage * 8];     // byte l of tile k's 32 bytes = i lane l's bits
+};
 // Store one tile (when any pair is in); false when a capacity ran out
 // (cannot happen: the capacities are worst cases).
 __device__ __forceinline__ bool search_emit(const PackView &v, int lane, const SearchRow &r, int jb0, int a0, int s,
-                                            int na, int nb) {
+                                            int na, int nb, SearchStage &stage) {
   if (!__any_sync(0xffffffffu, r.row != 0)) return true;
-  int e = 0;
-  if (lane == 0) e = atomicAdd(&v.tile_count[0], 1);
-  e = __shfl_sync(0xffffffffu, e, 0);
-  if (e >= v.tile_cap) {
-    if (lane == 0) atomicExch(&v.flags[F_NL_OVERFLOW], 1);
-    return false;
-  }
-  reinterpret_cast<unsigned char *>(v.tile_rows)[32 * (size_t)e + lane] = (unsigned char)r.row;
   int spec = -1;
   if (__any_sync(0xffffffffu, (r.xr | r.br) != 0)) {
     if (lane == 0) spec = atomicAdd(&v.tile_count[1], 1);
@@ -280,12 +283,28 @@ __device__ __forceinline__ bool search_emit(const PackView &v, int lane, const S
     reinterpret_cast<unsigned char *>(v.spec_rows)[64 * (size_t)spec + lane] = (unsigned char)r.xr;
     reinterpret_cast<unsigned char *>(v.spec_rows)[64 * (size_t)spec + 32 + lane] = (unsigned char)r.br;
   }
-  if (lane == 0) v.tile_meta[e] = make_int4(jb0, spec, a0, (s << 8) | ((na - 1) << 3) | (nb - 1));
+  const int4 meta = make_int4(jb0, spec, a0, (s << 8) | ((na - 1) << 3) | (nb - 1));
+  int k = 0;
+  if (lane == 0) k = atomicAdd(&stage.n, 1);
+  k = __shfl_sync(0xffffffffu, k, 0);
+  if (k < kSearchStage) {
+    reinterpret_cast<unsigned char *>(stage.rows)[32 * k + lane] = (unsigned char)r.row;
+    if (lane == 0) stage.meta[k] = meta;
+    return true;
+  }
+  int e = 0;
+  if (lane == 0) e = atomicAdd(&v.tile_count[0], 1);
+  e = __shfl_sync(0xffffffffu, e, 0);
+  if (e >= v.tile_cap) {
+    if (lane == 0) atomicExch(&v.flags[F_NL_OVERFLOW], 1);
+    return false;
+  }
+  reinterpret_cast<unsigned char *>(v.tile_rows)[32 * (size_t)e + lane] = (unsigned char)r.row;
+  if (lane == 0) v.tile_meta[e] = meta;
   return true;
 }
 
-__global__ void __launch_bounds__(32 * kSearchWarps) k_tile_search(PackView v) {
-  if (v.flags[F_NL_OVERFLOW]) return;
+__global__ void __launch_bounds__(32 * kSearchWarps, 5) k_tile_search(PackView v) {
   const int sc = blockIdx.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int s = v.sc_sys[sc];
@@ -311,13 +330,21 @@ __global__ void __launch_bounds__(32 * kSearchWarps) k_tile_search(PackView v) {
   const bool has_off = v.off_ptr[i + 1] > v.off_ptr[i];
   // the i atoms' positions for the per-atom cull
   __shared__ double sx[32], sy[32], sz[32];
+  __shared__ SearchStage stage;
+  __shared__ int stop_s;  // an earlier overflow, read once so every thread of the block agrees
+  if (threadIdx.x == 0) {
+    stage.n = 0;
+    stop_s = v.flags[F_NL_OVERFLOW];
+  }
   if (warp == 0) {
     sx[lane] = xi;
     sy[lane] = yi;
     sz[lane] = zi;
   }
   __syncthreads();
-  for (int base = jc0 + 32 * warp; base < jc_end; base += 32 * kSearchWarps) {
+  if (stop_s) return;
+  bool ok = true;  // false once a capacity ran out (warp-uniform)
+  for (int base = jc0 + 32 * warp; ok && base < jc_end; base += 32 * kSearchWarps) {
     bool cand = false;
     const int jc = base + lane;
     if (jc < jc_end) {
@@ -349,7 +376,7 @@ __global__ void __launch_bounds__(32 * kSearchWarps) k_tile_search(PackView v) {
     }
     unsigned m = __ballot_sync(0xffffffffu, cand);
     // two candidates at a time: their loads overlap
-    while (m) {
+    while (ok && m) {
       const int q1 = __ffs(m) - 1;
       m &= m - 1;
       const int q2 = m ? __ffs(m) - 1 : -1;
@@ -359,10 +386,24 @@ __global__ void __launch_bounds__(32 * kSearchWarps) k_tile_search(PackView v) {
       const SearchRow r1 = search_row(v, live, i, li, a0, xi, yi, zi, lim, jb1, nb1, o, mid, band, has_off, s);
       SearchRow r2 = {0u, 0u, 0u};
       if (q2 >= 0) r2 = search_row(v, live, i, li, a0, xi, yi, zi, lim, jb2, nb2, o, mid, band, has_off, s);
-      if (!search_emit(v, lane, r1, jb1, a0, s, na, nb1)) return;
-      if (q2 >= 0 && !search_emit(v, lane, r2, jb2, a0, s, na, nb2)) return;
+      ok = search_emit(v, lane, r1, jb1, a0, s, na, nb1, stage);
+      if (ok && q2 >= 0) ok = search_emit(v, lane, r2, jb2, a0, s, na, nb2, stage);
     }
   }
+  // the staged tiles as one range of the tile store
+  __syncthreads();
+  const int n = min(stage.n, kSearchStage);
+  if (n == 0) return;
+  __shared__ int base_s;
+  if (threadIdx.x == 0) base_s = atomicAdd(&v.tile_count[0], n);
+  __syncthreads();
+  const long long b0 = base_s;
+  if (b0 + n > v.tile_cap) {
+    if (threadIdx.x == 0) atomicExch(&v.flags[F_NL_OVERFLOW], 1);
+    return;
+  }
+  for (int w = threadIdx.x; w < 8 * n; w += blockDim.x) v.tile_rows[8 * b0 + w] = stage.rows[w];
+  for (int k = threadIdx.x; k < n; k += blockDim.x) v.tile_meta[b0 + k] = stage.meta[k];
 }
 
 // --------------------------------------------------------------- tile passes
