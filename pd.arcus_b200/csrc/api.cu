@@ -540,6 +540,7 @@ int pdgpu_system_set_bonded(pdgpu_ctx *c, int32_t sys, int32_t nb, const int32_t
   h.tterms.insert(h.tterms.end(), iterms, iterms + ni);
   h.tpar.assign(tpar, tpar + 12 * nt);
   h.tpar.insert(h.tpar.end(), ipar, ipar + 12 * ni);
+  dihedral_sets(h);
   // rebuild the pack with the bonded terms, keeping the state
   return rebuild_pack(c, e, sys);
 }

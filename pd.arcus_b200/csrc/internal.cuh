@@ -263,6 +263,12 @@ struct SystemHost {
   std::vector<int> bij, aiaj, tidx, tterms;
   std::vector<double> blk, akt, tpar;
   int nb = 0, na = 0, nt = 0, ni = 0;
+  // the dihedrals' distinct parameter sets (12 parameters and the term
+  // count, 13 doubles a set, in order of first appearance) and each
+  // dihedral's set, formed once when the terms are set (dihedral_sets) so
+  // that building a pack maps a few sets per system instead of every term
+  std::vector<int> dih_set;
+  std::vector<double> dih_sets;
   // backbone torsion moves: axis atom pairs (local), nest starts and the
   // last rotation (local index, -1 none) that moves each atom
   std::vector<int> rot_axis, rot_last;
@@ -342,6 +348,8 @@ struct Pack {
 // Build a device Pack from host systems (atoms concatenated in order).
 // With `sync` the call waits for the uploads on `st` (reporting their
 // errors); without, everything stays enqueued on `st`.
+// Fill h.dih_set / h.dih_sets from h.tpar and h.tterms.
+void dihedral_sets(SystemHost &h);
 Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHost *> &systems,
                   std::string *err, bool sync = true);
 void pack_set_params(Pack *p, int s, const pdgpu_ff_params &prm);

@@ -21,6 +21,8 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -163,6 +165,27 @@ struct pdgpu_server {
   std::thread worker;
   // statistics (guarded by m)
   pdgpu_serve_stats stats;
+  // host time of the worker's steps (PDGPU_SERVE_TRACE=1: a summary on
+  // stderr when the server is destroyed): [job kind][phase the step left,
+  // kTraceAdmit for the admission], and the worker loop's iterations
+  static constexpr int kTraceAdmit = 7;
+  struct StepClock {
+    long long n = 0;
+    double total_ms = 0.0, max_ms = 0.0;
+    void add(double ms) {
+      n++;
+      total_ms += ms;
+      max_ms = std::max(max_ms, ms);
+    }
+  };
+  bool trace = false;
+  StepClock trace_step[3][8], trace_loop;
+  void trace_add(const Job *j, int phase, Clock::time_point t0) {
+    if (!trace) return;
+    const int k = j->spec.kind == PDGPU_JOB_ENERGY ? 0 : j->spec.kind == PDGPU_JOB_MINIMISE ? 1 : 2;
+    trace_step[k][phase].add(ms_between(t0, Clock::now()));
+  }
+  void trace_print() const;
 
   void run();
   void admit(Job *j, const std::vector<Job *> &more);
@@ -748,6 +771,7 @@ void pdgpu_server::run() {
       }
     }
     bool progressed = false;
+    const auto t_loop = Clock::now();
     for (size_t a = 0; a < active.size();) {
       Job *j = active[a];
       cudaError_t q = cudaEventQuery(j->ev);
@@ -756,10 +780,13 @@ void pdgpu_server::run() {
         continue;
       }
       progressed = true;
+      const auto t_step = Clock::now();
+      const int ph_step = j->phase;
       if (q != cudaSuccess)
         fail(j, PDGPU_ERR_CUDA, std::string("job stream: ") + cudaGetErrorString(q));
       else
         advance(j);
+      trace_add(j, ph_step, t_step);
       if (j->phase == PH_DONE || j->phase == PH_FAILED) {
         retire(j);
         active.erase(active.begin() + a);
@@ -795,7 +822,9 @@ void pdgpu_server::run() {
       std::vector<Job *> more = prm.group ? group_with(j) : std::vector<Job *>();
       queue.erase(queue.begin() + pick);
       for (Job *x : more) queue.erase(std::find(queue.begin(), queue.end(), x));
+      const auto t_admit = Clock::now();
       admit(j, more);
+      trace_add(j, kTraceAdmit, t_admit);
       progressed = true;
       if (j->phase == PH_FAILED)
         retire(j);
@@ -805,8 +834,23 @@ void pdgpu_server::run() {
       stats.bytes_in_use = bytes_in_use;
       stats.peak_bytes = std::max(stats.peak_bytes, bytes_in_use);
     }
+    if (trace && progressed) trace_loop.add(ms_between(t_loop, Clock::now()));
     if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(20));
   }
+}
+
+void pdgpu_server::trace_print() const {
+  static const char *kinds[3] = {"energy", "minimise", "md"};
+  static const char *phases[8] = {"queued", "size", "min", "md", "finish", "done", "failed", "admit"};
+  std::fprintf(stderr, "pdgpu serve trace: worker loop iterations with progress %lld, mean %.3f ms, max %.3f ms\n",
+               trace_loop.n, trace_loop.n ? trace_loop.total_ms / trace_loop.n : 0.0, trace_loop.max_ms);
+  for (int k = 0; k < 3; k++)
+    for (int p = 0; p < 8; p++) {
+      const StepClock &c = trace_step[k][p];
+      if (c.n)
+        std::fprintf(stderr, "  %-8s %-6s steps %6lld  total %9.3f ms  mean %7.3f ms  max %8.3f ms\n", kinds[k],
+                     phases[p], c.n, c.total_ms, c.total_ms / c.n, c.max_ms);
+    }
 }
 
 // ------------------------------------------------------------------ C ABI
@@ -852,6 +896,8 @@ int pdgpu_serve_create(pdgpu_ctx *ctx, const pdgpu_serve_params *p, pdgpu_server
   s->device = ctx_device(ctx);
   s->prm = prm;
   std::memset(&s->stats, 0, sizeof s->stats);
+  const char *trace = std::getenv("PDGPU_SERVE_TRACE");
+  s->trace = trace && trace[0] == '1';
   cudaSetDevice(s->device);
   int least = 0, greatest = 0;
   cudaDeviceGetStreamPriorityRange(&least, &greatest);
@@ -1056,6 +1102,7 @@ int pdgpu_serve_destroy(pdgpu_server *s) {
     s->cv_work.notify_one();
   }
   if (s->worker.joinable()) s->worker.join();
+  if (s->trace) s->trace_print();
   cudaSetDevice(s->device);
   for (cudaStream_t st : s->streams) {
     cudaStreamSynchronize(st);

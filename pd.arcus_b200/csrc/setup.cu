@@ -1,6 +1,7 @@
 // Host-side setup: constants, bond-order band, Still fixed terms, per-system
 // kernel parameters and Pack allocation.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -367,6 +368,24 @@ void pack_set_params(Pack *p, int s, const pdgpu_ff_params &prm) {
     }                                                         \
   } while (0)
 
+void dihedral_sets(SystemHost &h) {
+  const int n = h.nt + h.ni;
+  std::map<std::array<double, 13>, int> seen;
+  h.dih_set.assign(n, 0);
+  h.dih_sets.clear();
+  for (int q = 0; q < n; q++) {
+    std::array<double, 13> key;
+    std::copy(h.tpar.begin() + 12 * (size_t)q, h.tpar.begin() + 12 * (size_t)q + 12, key.begin());
+    key[12] = (double)h.tterms[q];
+    auto it = seen.find(key);
+    if (it == seen.end()) {
+      it = seen.emplace(key, (int)(h.dih_sets.size() / 13)).first;
+      h.dih_sets.insert(h.dih_sets.end(), key.begin(), key.end());
+    }
+    h.dih_set[q] = it->second;
+  }
+}
+
 Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHost *> &systems,
                   std::string *err, bool sync) {
   const Consts &c = consts();
@@ -608,7 +627,23 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
   std::vector<int4> aiaj, tidx;
   std::vector<int> tterms, ttype;
   std::vector<double> tpar;
-  std::map<std::vector<double>, int> types;  // dihedral parameter sets (few per forcefield)
+  // dihedral parameter sets (few per forcefield): the pack's table holds
+  // each once, in order of first appearance over the systems' terms
+  std::map<std::array<double, 13>, int> types;
+  std::vector<std::vector<int>> set_type(S);  // per system: its local sets' pack types (-1 not yet)
+  std::vector<SystemHost> dih_fallback;        // systems whose sets were not formed (none expected)
+  std::vector<const SystemHost *> dih_src(S);
+  for (int s = 0; s < S; s++) {
+    const SystemHost &h = *systems[s];
+    dih_src[s] = &h;
+    if (h.dih_set.size() != (size_t)(h.nt + h.ni)) {
+      dih_fallback.reserve(S);
+      dih_fallback.push_back(h);
+      dihedral_sets(dih_fallback.back());
+      dih_src[s] = &dih_fallback.back();
+    }
+    set_type[s].assign(dih_src[s]->dih_sets.size() / 13, -1);
+  }
   double J2k = c.J2kcal * c.Na;
   for (int s = 0; s < S; s++) {
     const SystemHost &h = *systems[s];
@@ -634,22 +669,29 @@ Pack *pack_create(int device, cudaStream_t st, const std::vector<const SystemHos
                                  o + h.tidx[4 * q + 3]));
         // the dihedral's parameter set, stored once per distinct set: the
         // kernel reads a 4-byte index per term and the table from cache
-        std::vector<double> key(h.tpar.begin() + 12 * q, h.tpar.begin() + 12 * q + 12);
-        key.push_back((double)h.tterms[q]);
-        auto it = types.find(key);
-        if (it == types.end()) {
-          it = types.emplace(key, (int)tterms.size()).first;
-          tterms.push_back(h.tterms[q]);
-          for (int m = 0; m < 12; m++) {
-            double val = h.tpar[12 * q + m];
-            tpar.push_back(m < 4 ? val * J2k : val);
+        const SystemHost &hd = *dih_src[s];
+        const int local = hd.dih_set[q];
+        int &ty = set_type[s][local];
+        if (ty < 0) {
+          std::array<double, 13> key;
+          std::copy(hd.dih_sets.begin() + 13 * (size_t)local, hd.dih_sets.begin() + 13 * (size_t)local + 13,
+                    key.begin());
+          auto it = types.find(key);
+          if (it == types.end()) {
+            it = types.emplace(key, (int)tterms.size()).first;
+            tterms.push_back(h.tterms[q]);
+            for (int m = 0; m < 12; m++) {
+              double val = h.tpar[12 * q + m];
+              tpar.push_back(m < 4 ? val * J2k : val);
+            }
+            // cos and sin of each phase, so the kernel needs no transcendental
+            // for the integer periodicities
+            for (int m = 0; m < 4; m++) tpar.push_back(std::cos(h.tpar[12 * q + 8 + m]));
+            for (int m = 0; m < 4; m++) tpar.push_back(std::sin(h.tpar[12 * q + 8 + m]));
           }
-          // cos and sin of each phase, so the kernel needs no transcendental
-          // for the integer periodicities
-          for (int m = 0; m < 4; m++) tpar.push_back(std::cos(h.tpar[12 * q + 8 + m]));
-          for (int m = 0; m < 4; m++) tpar.push_back(std::sin(h.tpar[12 * q + 8 + m]));
+          ty = it->second;
         }
-        ttype.push_back(it->second);
+        ttype.push_back(ty);
       }
     }
   bt.nb = (int)bij.size();
