@@ -74,12 +74,12 @@ METRIC = "GB MD ns/day"
 # DRAM bytes (read + write) of one evaluation (the evaluation kernel's three
 # one-phase launches of one MD step) on this workload, from one ncu capture
 # of the 20,566-atom MD workload (dram__bytes_read.sum + dram__bytes_write.sum,
-# cold caches: 1,924,352 + 3,327,488 + 3,158,784 bytes read, nothing written);
+# cold caches: 1,924,864 + 3,327,488 + 3,181,312 bytes read, nothing written);
 # ncu cannot run inside the timed bench, so the figure is carried here
-NCU_TRAFFIC_EVAL = 8410624
+NCU_TRAFFIC_EVAL = 8433664
 # warp instructions the same three launches executed (smsp__inst_executed.sum
 # of that capture: phases A, B, C), for the issue roof beside the FP32/SFU one
-NCU_INST_EVAL = (5848656, 15501308, 6179253)
+NCU_INST_EVAL = (5630203, 14581779, 6049203)
 
 
 def rank_info():
