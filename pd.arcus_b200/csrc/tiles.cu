@@ -40,6 +40,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "tilecommon.cuh"
 
@@ -257,13 +258,14 @@ __device__ __forceinline__ SearchRow search_row(const PackView &v, bool live, in
   return r;
 }
 // A search block's tiles are staged in shared memory and written to the
-// tile store as one contiguous range when the block is done, so the tiles
-// of an i-cluster sit together and a pass that walks contiguous tile ranges
-// meets few i-cluster changes (each one a reload of the i side).  Tiles
-// beyond the staging capacity go to the store one at a time.
+// tile store as one contiguous range by the block's last warp to finish, so
+// the tiles of an i-cluster sit together and a pass that walks contiguous
+// tile ranges meets few i-cluster changes (each one a reload of the i side).
+// Tiles beyond the staging capacity go to the store one at a time.
 constexpr int kSearchStage = 256;
 struct SearchStage {
   int n;                               // tiles emitted into the stage (may pass kSearchStage)
+  int done;                            // warps that have finished their j-clusters
   int4 meta[kSearchStage];
   unsigned rows[kSearchStage * 8];     // byte l of tile k's 32 bytes = i lane l's bits
 };
@@ -334,6 +336,7 @@ __global__ void __launch_bounds__(32 * kSearchWarps, 5) k_tile_search(PackView v
   __shared__ int stop_s;  // an earlier overflow, read once so every thread of the block agrees
   if (threadIdx.x == 0) {
     stage.n = 0;
+    stage.done = 0;
     stop_s = v.flags[F_NL_OVERFLOW];
   }
   if (warp == 0) {
@@ -390,20 +393,32 @@ __global__ void __launch_bounds__(32 * kSearchWarps, 5) k_tile_search(PackView v
       if (ok && q2 >= 0) ok = search_emit(v, lane, r2, jb2, a0, s, na, nb2, stage);
     }
   }
-  // the staged tiles as one range of the tile store
-  __syncthreads();
-  const int n = min(stage.n, kSearchStage);
+  // the staged tiles as one range of the tile store, written by the last
+  // warp to finish; the others exit at once (a warp with no j-clusters does
+  // not hold its slot while the block's busy warps run)
+  __syncwarp();
+  __threadfence_block();  // this warp's stage writes before its count
+  int last = 0;
+  if (lane == 0) last = atomicAdd(&stage.done, 1) == kSearchWarps - 1;
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (!last) return;
+  __syncwarp();
+  __threadfence_block();  // every warp's stage writes after the count
+  const int n = min(*(volatile int *)&stage.n, kSearchStage);
   if (n == 0) return;
-  __shared__ int base_s;
-  if (threadIdx.x == 0) base_s = atomicAdd(&v.tile_count[0], n);
-  __syncthreads();
-  const long long b0 = base_s;
+  long long b0 = 0;
+  if (lane == 0) b0 = atomicAdd(&v.tile_count[0], n);
+  b0 = __shfl_sync(0xffffffffu, b0, 0);
   if (b0 + n > v.tile_cap) {
-    if (threadIdx.x == 0) atomicExch(&v.flags[F_NL_OVERFLOW], 1);
+    if (lane == 0) atomicExch(&v.flags[F_NL_OVERFLOW], 1);
     return;
   }
-  for (int w = threadIdx.x; w < 8 * n; w += blockDim.x) v.tile_rows[8 * b0 + w] = stage.rows[w];
-  for (int k = threadIdx.x; k < n; k += blockDim.x) v.tile_meta[b0 + k] = stage.meta[k];
+  const volatile unsigned *rows = stage.rows;
+  for (int w = lane; w < 8 * n; w += 32) v.tile_rows[8 * b0 + w] = rows[w];
+  for (int k = lane; k < n; k += 32) {
+    const volatile int *m = reinterpret_cast<const volatile int *>(&stage.meta[k]);
+    v.tile_meta[b0 + k] = make_int4(m[0], m[1], m[2], m[3]);
+  }
 }
 
 // --------------------------------------------------------------- tile passes
@@ -797,6 +812,16 @@ size_t tile_build_smem(int max_sys_atoms) {
 void tile_launch_shapes(PackView &v) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
+  // the tile search with the largest shared-memory carveout: a search block
+  // holds its 13 KB stage until its last warp is done, and on a pack of many
+  // small systems (thousands of short blocks) a carveout sized for the
+  // register limit would cap the blocks an SM can take as their idle warps
+  // exit.  Set once per device at pack creation (never inside a capture).
+  static std::once_flag carve[64];
+  if (dev >= 0 && dev < 64)
+    std::call_once(carve[dev], [] {
+      cudaFuncSetAttribute(k_tile_search, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    });
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int occ[3] = {1, 1, 1};
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_born_tile, 32 * kTileWarps, 0);
