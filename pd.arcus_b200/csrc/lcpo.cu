@@ -51,16 +51,21 @@ __device__ __forceinline__ bool lcpo_overlaps(double d2, double rs) {
 
 // Overlap candidates from the tiles of the last tile search: each list pair
 // (one tile bit, stored once) that overlaps is appended to both atoms'
-// candidate buffers; k_lcpo_list ranks them.  One warp per tile, lane l
-// for the i-cluster's atom l.
+// candidate buffers; k_lcpo_list ranks them, so the order of the appends
+// does not matter.  A warp takes one tile at a time, lane l for the
+// i-cluster's atom l, over a contiguous range of the tiles: an i-cluster's
+// tiles sit together in the store, so warps that run at once append to
+// different atoms' counters instead of all to the same 32.
 template <bool EO>
 __global__ void __launch_bounds__(128) k_lcpo_cand_tiles(PackView v, StepSrc ss) {
   if (v.flags[F_NL_OVERFLOW]) return;
   const LcpoView &lc = v.lc;
   const int lane = threadIdx.x & 31;
-  const int T = v.tile_count[0];
-  const int W = gridDim.x * (blockDim.x >> 5);
-  for (int e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); e < T; e += W) {
+  const long long T = v.tile_count[0];
+  const long long W = (long long)gridDim.x * (blockDim.x >> 5);
+  const long long g = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int e_end = (int)(T * (g + 1) / W);
+  for (int e = (int)(T * g / W); e < e_end; e++) {
     const int4 m = v.tile_meta[e];
     const int s = m.w >> 8, na = ((m.w >> 3) & 31) + 1, nb = (m.w & 7) + 1;
     if (!EO && !lcpo_due(lc, ss, s)) continue;
