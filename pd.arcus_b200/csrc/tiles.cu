@@ -40,7 +40,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <mutex>
 
 #include "tilecommon.cuh"
 
@@ -812,16 +811,6 @@ size_t tile_build_smem(int max_sys_atoms) {
 void tile_launch_shapes(PackView &v) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
-  // the tile search with the largest shared-memory carveout: a search block
-  // holds its 13 KB stage until its last warp is done, and on a pack of many
-  // small systems (thousands of short blocks) a carveout sized for the
-  // register limit would cap the blocks an SM can take as their idle warps
-  // exit.  Set once per device at pack creation (never inside a capture).
-  static std::once_flag carve[64];
-  if (dev >= 0 && dev < 64)
-    std::call_once(carve[dev], [] {
-      cudaFuncSetAttribute(k_tile_search, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    });
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int occ[3] = {1, 1, 1};
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_born_tile, 32 * kTileWarps, 0);
