@@ -1080,7 +1080,6 @@ def main():
             return 0
         r = run_reference(args, n_gpus)
         cfg = headline_config(int(load_fixture()[0]["charge"].shape[0]), n_gpus)
-        cfg["threads"] = 1
         line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": "ns/day",
                 "n_gpus": n_gpus, "steps": r["steps"], "warmup": r["warmup"],
                 "ms_per_step": 1e3 * r["seconds"] / r["steps"], "higher_is_better": True,
